@@ -1,0 +1,186 @@
+/*
+ * C ABI of the B200 DiffPhD projective-dynamics step and its adjoint.
+ *
+ * This library replaces the device path of the reference's Newton solver
+ * plugin `SolverDiffPhD` (src/newton_solver_diff_phd/_src/solvers/diff_phd/
+ * solver.py). The reference is Python over NVIDIA Warp and exposes no C
+ * interface of its own; each entry point below names the reference call it
+ * stands in for. Host code (the Python package newton_solver_diff_phd_b200)
+ * validates the model exactly like the reference and hands plain arrays here.
+ *
+ * Conventions
+ *  - Every function returns PD_OK (0) or a PD_ERR_* code; pd_last_error()
+ *    returns a thread-local message for the last failure.
+ *  - Device pointers are marked "device"; everything else is host memory.
+ *    Vectors of particles are float32 xyz triples (Newton's wp.vec3) unless
+ *    stated as double.
+ *  - Steps and backward passes are asynchronous on the caller's stream. Solver
+ *    failures never interrupt the device: they set bits of a device status
+ *    word that pd_read_status() returns (the reference's status contract,
+ *    kernels.py:28-31, adjoint.py:64-65).
+ *  - A solver instance serialises its own launches: use one stream per
+ *    instance at a time (the reference's single-stream rule, sparse.py:280-282).
+ */
+#ifndef PD_B200_H
+#define PD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PD_OK 0
+#define PD_ERR_INVALID 1   /* invalid argument; the reference raises ValueError */
+#define PD_ERR_CUDA 2      /* a CUDA runtime call failed */
+#define PD_ERR_NOT_SPD 3   /* the constant matrix is not positive definite (sparse.py:139-140) */
+#define PD_ERR_STATE 4     /* wrong call order, e.g. step before build; RuntimeError in the reference */
+#define PD_ERR_UNSUPPORTED 5 /* NotImplementedError in the reference */
+
+/* Device status bits (solver.py:380-387, kernels.py:28-31, adjoint.py:64-65). */
+#define PD_STATUS_NOT_CONVERGED 1
+#define PD_STATUS_SINGULAR 2
+#define PD_STATUS_ACTIVATION 4
+#define PD_STATUS_ADJOINT_NOT_CONVERGED 8
+#define PD_STATUS_ADJOINT_SAFEGUARD 16
+/* A device barrier gave up waiting (bounded spin); the step result is invalid. */
+#define PD_STATUS_BARRIER_TIMEOUT 1024
+
+#define PD_MATERIAL_PD 0          /* corotated 2 mu + volume lambda */
+#define PD_MATERIAL_NEO_HOOKEAN 1 /* proximal Neo-Hookean, weight 2 mu */
+
+#define PD_PRECISION_FP64 0        /* every solver operation in float64, as the reference */
+#define PD_PRECISION_FP32_REFINE 1 /* fp32 local step and factor, fp64 residual refinement */
+
+#define PD_ADJOINT_REFERENCE 0 /* K with the mean weight per energy (adjoint.py:17-18) */
+#define PD_ADJOINT_EXACT 1     /* K with per-element weights: the derivative of the forward map */
+
+typedef struct PdSolver PdSolver;
+
+typedef struct PdMeshDesc {
+  int32_t n_vertices;
+  int32_t n_elements;
+  int32_t corners;         /* 4: Tet4, 8: Hex8 (eight Gauss samples per cell) */
+  const int32_t* indices;  /* [n_elements][corners] */
+  /* Tet4: [n_elements][4][3] rest shape gradients G (solver.py:218-219).
+     Hex8: [8 samples][8 corners][3] shared Gauss gradients (hex.py:64-79). */
+  const double* gradients;
+  double mean_volume;      /* Vbar: every element's volume and the mass basis */
+  const uint8_t* free;     /* [n_vertices]; 0 marks a Dirichlet (zero inverse mass) particle */
+} PdMeshDesc;
+
+typedef struct PdOptions {
+  int32_t material;          /* PD_MATERIAL_* */
+  int32_t max_iterations;    /* >= 1 */
+  double abs_tol;            /* >= 0 */
+  double rel_tol;            /* >= 0 */
+  int32_t anderson_window;   /* 0..8 */
+  double density;            /* > 0 */
+  int32_t integrate_pinned_velocities;
+  int32_t precision;         /* PD_PRECISION_* */
+  int32_t adjoint_mode;      /* PD_ADJOINT_* */
+  int32_t blocks;            /* persistent grid size; 0 = automatic */
+} PdOptions;
+
+/* Library identity and the message of the last failure on this thread. */
+const char* pd_version(void);
+const char* pd_last_error(void);
+
+/* SolverDiffPhD.__init__ (solver.py:157-333): copies the mesh to the device.
+   `device` is the CUDA ordinal. */
+int pd_create(const PdMeshDesc* mesh, const PdOptions* options, int device, PdSolver** out);
+/* Releases all device memory of the instance. */
+int pd_destroy(PdSolver* solver);
+
+/* Mutable convergence settings (solver.max_iterations / abs_tol / rel_tol). */
+int pd_set_tolerances(PdSolver* solver, int32_t max_iterations, double abs_tol, double rel_tol);
+
+/* Lame parameters [mu, lambda] per element (model.tet_materials columns 0-1,
+   or hex_materials), float64 host array [n_elements][2]. Marks the factor
+   stale (notify_model_changed, solver.py:419-427). */
+int pd_set_materials(PdSolver* solver, const double* mu_lambda);
+
+/* Fibres (solver.py:429-462): unit directions [n_elements][3] (zero rows for
+   disabled fibres) and stiffness [n_elements] in Pa. Pass NULLs to disable. */
+int pd_set_muscles(PdSolver* solver, const double* directions, const double* stiffness);
+
+/* Hex8 native fibre target lengths [n_elements] (solver.muscle_targets).
+   `targets` is a host float64 array. */
+int pd_set_muscle_targets(PdSolver* solver, const double* targets);
+
+/* Tet4 fibre contractions u (target length 1 - u) for the following steps,
+   a device float32 array [n_elements] read at every step
+   (read_activations, kernels.py:136-152). NULL keeps zero contraction. */
+int pd_set_activations(PdSolver* solver, const float* device_contractions);
+
+/* Hex8 vertex-plane energies (hex.py:204-260): vertex indices, stiffness per
+   vertex and the normalised plane (nx, ny, nz, offset). count 0 disables. */
+int pd_set_planar_energies(PdSolver* solver, int32_t count, const int32_t* vertices, const double* stiffness,
+                           const double plane[4]);
+
+/* SolverDiffPhD._build (solver.py:491-552): assembles the constant matrix
+   A = m/h^2 I + sum_e w_e Vbar G_e^T G_e (+ fibres, + plane diagonal) and builds
+   the exact inverse factor A^{-1} = S^T S on the host (sparse.py:291-320),
+   then uploads it. Synchronous; not capturable. */
+int pd_build(PdSolver* solver, double dt);
+
+/* Factor statistics of the last build: rows, nnz(S), nnz(L) incl. diagonal. */
+int pd_factor_stats(const PdSolver* solver, int64_t* rows, int64_t* nnz_s, int64_t* nnz_l);
+
+/* SolverDiffPhD.step (solver.py:689-786) for float32 device states.
+   q, qd, f: device [n][3] float32 inputs; dirichlet: optional device [n][3]
+   prescribed positions of the pinned particles (or NULL); gravity: host [3];
+   q_out, qd_out: device [n][3] float32 outputs (must not alias the inputs);
+   x_record: optional device [n][3] float64 that receives the converged
+   positions for pd_backward (the reference StepRecord.x, adjoint.py:809-841).
+   dt must equal the dt of the last pd_build. `stream` is a cudaStream_t. */
+int pd_step(PdSolver* solver, const float* q, const float* qd, const float* f, const float* dirichlet,
+            const double gravity[3], double dt, float* q_out, float* qd_out, double* x_record, void* stream);
+
+/* Adjoint.backward (adjoint.py:1088-1259) of one recorded step.
+   x_record: device [n][3] float64 positions recorded by pd_step; activations:
+   the device contractions used by that step (or NULL).
+   gq_out, gqd_out: device float32 [n][3] gradients of the step outputs.
+   gq, gqd, gf: device float32 [n][3] accumulators (+=) for the gradients of
+   the step inputs q, qd, f; gdirichlet: optional device float32 [n][3]
+   accumulator when the step used explicit Dirichlet targets.
+   gmaterials: optional device float64 [n_elements][2] accumulator (+=) of
+   dL/dmu, dL/dlambda; gactivations: optional device float32 [n_elements]
+   accumulator of dL/du. Passing gmaterials/gactivations requests z, exactly
+   as a requires_grad material array does in the reference. */
+int pd_backward(PdSolver* solver, const double* x_record, const float* activations, double dt, const float* gq_out,
+                const float* gqd_out, float* gq, float* gqd, float* gf, float* gdirichlet, double* gmaterials,
+                float* gactivations, void* stream);
+
+/* Reads and clears the status word (read_status, solver.py:380-390). Synchronises the stream. */
+int pd_read_status(PdSolver* solver, int32_t* bits, void* stream);
+/* Iteration count of the last step and of the last backward fixed point. Synchronises the stream. */
+int pd_iterations(PdSolver* solver, int32_t* forward, int32_t* backward, void* stream);
+
+/* det(F) at every Hex8 Gauss sample (deformation_determinants, solver.py:360-378):
+   q device float32 [n][3], out device float64 [n_elements][8]. */
+int pd_deformation_determinants(PdSolver* solver, const float* q, double* out, void* stream);
+
+/* Applies the uploaded factor: out = S^T (S rhs), device float64 [n][3] arrays
+   (SparseInverse.apply, sparse.py:350-352). */
+int pd_apply_inverse(PdSolver* solver, const double* rhs, double* out, void* stream);
+
+/* Host factor build for an arbitrary SPD matrix given as full symmetric CSR
+   (SparseInverse.__init__, sparse.py:291-320). Arrays are host memory; the
+   result is freed with pd_inverse_free. */
+typedef struct PdInverseFactor PdInverseFactor;
+int pd_inverse_build(int32_t size, const int32_t* row_offsets, const int32_t* columns, const double* values,
+                     PdInverseFactor** out);
+int pd_inverse_sizes(const PdInverseFactor* factor, int32_t* size, int64_t* nnz, int64_t* factorization_nnz);
+/* Copies the arrays: permutation[size], s_offsets[size+1], s_columns[nnz], s_values[nnz],
+   st_offsets[size+1], st_columns[nnz], st_values[nnz]. Any pointer may be NULL. */
+int pd_inverse_export(const PdInverseFactor* factor, int32_t* permutation, int32_t* s_offsets, int32_t* s_columns,
+                      double* s_values, int32_t* st_offsets, int32_t* st_columns, double* st_values);
+int pd_inverse_free(PdInverseFactor* factor);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PD_B200_H */

@@ -1,0 +1,438 @@
+// Host construction of the exact inverse factor A^{-1} = S^T S.
+//
+// The algorithm and its floating-point evaluation order follow the reference
+// setup in src/newton_solver_diff_phd/_src/solvers/diff_phd/sparse.py, so the
+// CSR arrays are bit-identical to the reference's for the same input rows.
+// The data structures are this file's own: index arrays, marker stamps and
+// an elimination-tree symbolic phase instead of Python sets and dictionaries.
+// Compile without floating-point contraction (-ffp-contract=off): every
+// update must round the product before the subtraction, as NumPy does.
+#include "factor.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <limits>
+#include <numeric>
+#include <string>
+#include <vector>
+
+namespace pdb200 {
+namespace {
+
+using Adjacency = std::vector<std::vector<int32_t>>;
+
+// Minimum-degree elimination order of the subgraph induced by `vertices`
+// (sparse.py:18-28): repeatedly remove the vertex of smallest (degree, index)
+// and join its remaining neighbours into a clique.
+std::vector<int32_t> minimum_degree(const std::vector<int32_t>& vertices, const Adjacency& adjacency,
+                                    std::vector<int32_t>& local) {
+  const int32_t m = static_cast<int32_t>(vertices.size());
+  for (int32_t a = 0; a < m; ++a) local[vertices[a]] = a;
+  std::vector<std::vector<int32_t>> graph(m);
+  for (int32_t a = 0; a < m; ++a) {
+    for (int32_t other : adjacency[vertices[a]]) {
+      const int32_t b = local[other];
+      if (b >= 0 && b < m && vertices[b] == other) graph[a].push_back(b);
+    }
+    std::sort(graph[a].begin(), graph[a].end());
+  }
+  std::vector<char> alive(m, 1);
+  std::vector<int32_t> order;
+  order.reserve(m);
+  std::vector<int32_t> merged;
+  for (int32_t step = 0; step < m; ++step) {
+    int32_t best = -1;
+    size_t best_degree = 0;
+    // Local ids follow ascending vertex ids (vertices is sorted), so the
+    // first minimum of the scan breaks ties by the smallest index.
+    for (int32_t a = 0; a < m; ++a) {
+      if (!alive[a]) continue;
+      if (best < 0 || graph[a].size() < best_degree) {
+        best = a;
+        best_degree = graph[a].size();
+      }
+    }
+    alive[best] = 0;
+    order.push_back(vertices[best]);
+    const std::vector<int32_t> neighbors = graph[best];
+    for (int32_t other : neighbors) {
+      std::vector<int32_t>& list = graph[other];
+      merged.clear();
+      std::set_union(list.begin(), list.end(), neighbors.begin(), neighbors.end(), std::back_inserter(merged));
+      list.clear();
+      for (int32_t value : merged) {
+        if (value != other && value != best) list.push_back(value);
+      }
+    }
+    graph[best].clear();
+  }
+  for (int32_t v : vertices) local[v] = -1;
+  return order;
+}
+
+struct Dissection {
+  const Adjacency& adjacency;
+  std::vector<int32_t> stamp;     // membership token per vertex
+  std::vector<int32_t> distance;  // BFS distance per vertex
+  std::vector<int32_t> local;     // scratch map for minimum_degree
+  int32_t token = 0;
+
+  explicit Dissection(const Adjacency& graph)
+      : adjacency(graph), stamp(graph.size(), -1), distance(graph.size(), -1), local(graph.size(), -1) {}
+
+  // Breadth-first distances from `start` inside the current token's set,
+  // visiting neighbours in ascending order (sparse.py:31-40). Returns the
+  // reached vertices in discovery order.
+  std::vector<int32_t> bfs(int32_t start, int32_t set_token) {
+    std::vector<int32_t> queue;
+    queue.push_back(start);
+    distance[start] = 0;
+    stamp[start] = set_token + 1;  // reached marker
+    for (size_t head = 0; head < queue.size(); ++head) {
+      const int32_t node = queue[head];
+      for (int32_t other : adjacency[node]) {
+        if (stamp[other] == set_token) {
+          stamp[other] = set_token + 1;
+          distance[other] = distance[node] + 1;
+          queue.push_back(other);
+        }
+      }
+    }
+    return queue;
+  }
+
+  int32_t new_token(const std::vector<int32_t>& vertices) {
+    token += 2;
+    for (int32_t v : vertices) stamp[v] = token;
+    return token;
+  }
+
+  void visit(std::vector<int32_t> vertices, std::vector<int32_t>& order) {
+    std::sort(vertices.begin(), vertices.end());
+    if (vertices.size() <= 24) {
+      const std::vector<int32_t> leaf = minimum_degree(vertices, adjacency, local);
+      order.insert(order.end(), leaf.begin(), leaf.end());
+      return;
+    }
+    int32_t set_token = new_token(vertices);
+    // Start at the smallest (degree inside the set, index) (sparse.py:47).
+    int32_t start = -1;
+    size_t start_degree = 0;
+    for (int32_t v : vertices) {
+      size_t degree = 0;
+      for (int32_t other : adjacency[v]) degree += stamp[other] == set_token;
+      if (start < 0 || degree < start_degree) {
+        start = v;
+        start_degree = degree;
+      }
+    }
+    std::vector<int32_t> reached = bfs(start, set_token);
+    if (reached.size() != vertices.size()) {
+      // Components in order: the start's, then by smallest remaining index.
+      std::vector<std::vector<int32_t>> components;
+      components.push_back(reached);
+      for (int32_t v : vertices) {
+        if (stamp[v] == set_token) components.push_back(bfs(v, set_token));
+      }
+      for (auto& component : components) visit(component, order);
+      return;
+    }
+    // Farthest vertex: largest distance, smallest index on ties (sparse.py:57).
+    int32_t farthest = -1;
+    for (int32_t v : vertices) {
+      if (farthest < 0 || distance[v] > distance[farthest]) farthest = v;
+    }
+    set_token = new_token(vertices);
+    bfs(farthest, set_token);
+    int32_t levels_count = 0;
+    for (int32_t v : vertices) levels_count = std::max(levels_count, distance[v] + 1);
+    std::vector<int64_t> cumulative(levels_count, 0);
+    for (int32_t v : vertices) cumulative[distance[v]] += 1;
+    for (int32_t l = 1; l < levels_count; ++l) cumulative[l] += cumulative[l - 1];
+    // np.searchsorted(cumsum, n / 2) with side='left'.
+    const double half = static_cast<double>(vertices.size()) / 2.0;
+    int32_t cut = levels_count;
+    for (int32_t l = 0; l < levels_count; ++l) {
+      if (static_cast<double>(cumulative[l]) >= half) {
+        cut = l;
+        break;
+      }
+    }
+    std::vector<int32_t> lower, upper, separator;
+    for (int32_t v : vertices) {
+      if (distance[v] < cut) {
+        lower.push_back(v);
+      } else if (distance[v] > cut) {
+        upper.push_back(v);
+      } else {
+        separator.push_back(v);
+      }
+    }
+    if (lower.empty() || upper.empty()) {
+      const std::vector<int32_t> all = minimum_degree(vertices, adjacency, local);
+      order.insert(order.end(), all.begin(), all.end());
+      return;
+    }
+    visit(lower, order);
+    visit(upper, order);
+    const std::vector<int32_t> last = minimum_degree(separator, adjacency, local);
+    order.insert(order.end(), last.begin(), last.end());
+  }
+};
+
+}  // namespace
+
+std::vector<int32_t> nested_dissection(const Adjacency& adjacency) {
+  Dissection dissection(adjacency);
+  std::vector<int32_t> all(adjacency.size());
+  std::iota(all.begin(), all.end(), 0);
+  std::vector<int32_t> order;
+  order.reserve(adjacency.size());
+  dissection.visit(all, order);
+  return order;
+}
+
+std::string build_inverse_factor(int32_t size, const int32_t* row_offsets, const int32_t* row_columns,
+                                 const double* row_values, InverseFactor* out) {
+  if (size < 0) return "matrix size must be nonnegative";
+  // --- _validate_rows (sparse.py:73-95) ---------------------------------
+  std::vector<std::vector<std::pair<int32_t, double>>> rows(size);
+  for (int32_t i = 0; i < size; ++i) {
+    if (row_offsets[i + 1] < row_offsets[i]) return "row offsets must be nondecreasing";
+    for (int32_t p = row_offsets[i]; p < row_offsets[i + 1]; ++p) {
+      const int32_t j = row_columns[p];
+      const double value = row_values[p];
+      if (j < 0 || j >= size) return "matrix column indices must be integers in [0, size)";
+      if (!std::isfinite(value)) return "matrix coefficients must be finite";
+      if (value != 0.0) rows[i].emplace_back(j, value);
+    }
+    std::sort(rows[i].begin(), rows[i].end(),
+              [](const auto& a, const auto& b) { return a.first < b.first; });
+    for (size_t p = 1; p < rows[i].size(); ++p) {
+      if (rows[i][p].first == rows[i][p - 1].first) return "matrix rows must not repeat a column";
+    }
+    double diagonal = 0.0;
+    for (const auto& entry : rows[i]) {
+      if (entry.first == i) diagonal = entry.second;
+    }
+    if (!(diagonal > 0.0)) return "matrix must be positive definite with positive diagonal entries";
+  }
+  int64_t matrix_nnz = 0;
+  for (int32_t i = 0; i < size; ++i) {
+    matrix_nnz += static_cast<int64_t>(rows[i].size());
+    for (const auto& entry : rows[i]) {
+      const auto& other = rows[entry.first];
+      auto it = std::lower_bound(other.begin(), other.end(), std::make_pair(i, 0.0),
+                                 [](const auto& a, const auto& b) { return a.first < b.first; });
+      if (it == other.end() || it->first != i || it->second != entry.second) {
+        return "matrix_rows must contain both halves of an exactly symmetric matrix";
+      }
+    }
+  }
+  // --- Ordering -----------------------------------------------------------
+  Adjacency adjacency(size);
+  for (int32_t i = 0; i < size; ++i) {
+    for (const auto& entry : rows[i]) {
+      if (entry.first != i) adjacency[i].push_back(entry.first);
+    }
+  }
+  std::vector<int32_t> permutation = nested_dissection(adjacency);
+  std::vector<int32_t> inverse(size);
+  for (int32_t k = 0; k < size; ++k) inverse[permutation[k]] = k;
+
+  // --- Symbolic fill (sparse.py:98-124) via the elimination tree ----------
+  // Column k of L holds {i > k : A(i,k) != 0} and the columns of its
+  // elimination-tree children; this is the structure the reference's
+  // set-based fill discovery produces.
+  std::vector<std::vector<int32_t>> lower_a(size);  // permuted strict-lower A entries per column
+  for (int32_t i = 0; i < size; ++i) {
+    const int32_t pi = inverse[i];
+    for (const auto& entry : rows[i]) {
+      const int32_t pj = inverse[entry.first];
+      if (pj < pi) lower_a[pj].push_back(pi);
+    }
+  }
+  std::vector<std::vector<int32_t>> columns(size);
+  std::vector<std::vector<int32_t>> children(size);
+  std::vector<int32_t> marker(size, -1);
+  for (int32_t k = 0; k < size; ++k) {
+    std::vector<int32_t>& column = columns[k];
+    for (int32_t i : lower_a[k]) {
+      if (marker[i] != k) {
+        marker[i] = k;
+        column.push_back(i);
+      }
+    }
+    for (int32_t c : children[k]) {
+      for (int32_t i : columns[c]) {
+        if (i > k && marker[i] != k) {
+          marker[i] = k;
+          column.push_back(i);
+        }
+      }
+    }
+    std::sort(column.begin(), column.end());
+    if (!column.empty()) children[column.front()].push_back(k);
+    std::vector<int32_t>().swap(lower_a[k]);
+  }
+  std::vector<std::vector<int32_t>>().swap(children);
+  // Row patterns, each ending with its diagonal.
+  std::vector<int32_t> row_counts(size, 1);
+  for (int32_t k = 0; k < size; ++k) {
+    for (int32_t i : columns[k]) row_counts[i] += 1;
+  }
+  std::vector<int64_t> row_start(size + 1, 0);
+  for (int32_t i = 0; i < size; ++i) row_start[i + 1] = row_start[i] + row_counts[i];
+  const int64_t pattern_nnz = row_start[size];
+  std::vector<int32_t> pattern(pattern_nnz);
+  std::vector<double> values(pattern_nnz, 0.0);
+  {
+    std::vector<int64_t> cursor(row_start.begin(), row_start.end() - 1);
+    for (int32_t k = 0; k < size; ++k) {
+      for (int32_t i : columns[k]) pattern[cursor[i]++] = k;
+    }
+    for (int32_t i = 0; i < size; ++i) pattern[cursor[i]++] = i;
+  }
+  // Positions of column k inside each row of columns[k].
+  std::vector<std::vector<int64_t>> column_positions(size);
+  for (int32_t k = 0; k < size; ++k) column_positions[k].reserve(columns[k].size());
+  for (int32_t i = 0; i < size; ++i) {
+    for (int64_t p = row_start[i]; p < row_start[i + 1] - 1; ++p) column_positions[pattern[p]].push_back(p);
+  }
+  // Initial values: the permuted lower triangle of A.
+  for (int32_t i = 0; i < size; ++i) {
+    const int32_t pi = inverse[i];
+    for (const auto& entry : rows[i]) {
+      const int32_t pj = inverse[entry.first];
+      if (pj <= pi) {
+        const int32_t* first = pattern.data() + row_start[pi];
+        const int32_t* last = pattern.data() + row_start[pi + 1];
+        const int32_t* at = std::lower_bound(first, last, pj);
+        values[row_start[pi] + (at - first)] = entry.second;
+      }
+    }
+  }
+  std::vector<std::vector<std::pair<int32_t, double>>>().swap(rows);
+
+  // --- Numeric right-looking LDL^T (sparse.py:136-151) --------------------
+  std::vector<double> diagonal(size);
+  std::vector<double> entries;
+  std::vector<int64_t> locations;
+  for (int32_t k = 0; k < size; ++k) {
+    const double pivot = values[row_start[k + 1] - 1];
+    if (!std::isfinite(pivot) || pivot <= 0.0) {
+      return "matrix is not positive definite: LDLT pivot " + std::to_string(k) + " is " + std::to_string(pivot);
+    }
+    diagonal[k] = pivot;
+    const std::vector<int32_t>& neighbors = columns[k];
+    const std::vector<int64_t>& positions = column_positions[k];
+    const size_t count = neighbors.size();
+    entries.resize(count);
+    for (size_t o = 0; o < count; ++o) entries[o] = values[positions[o]];
+    for (size_t o = 0; o < count; ++o) {
+      const int32_t i = neighbors[o];
+      const double multiplier = entries[o] / pivot;
+      values[positions[o]] = multiplier;
+      // Walk row i for columns neighbors[0..o]; all lie after column k.
+      int64_t p = positions[o] + 1;
+      for (size_t o2 = 0; o2 <= o; ++o2) {
+        const int32_t j = neighbors[o2];
+        while (pattern[p] < j) ++p;
+        const double product = multiplier * entries[o2];
+        values[p] = values[p] - product;
+      }
+    }
+  }
+  std::vector<std::vector<int64_t>>().swap(column_positions);
+  std::vector<std::vector<int32_t>>().swap(columns);
+
+  // --- Inverse rows (sparse.py:159-177) ----------------------------------
+  // Unscaled rows of L^{-1} in elimination order, stored CSR.
+  std::vector<int64_t> inv_start(1, 0);
+  std::vector<int32_t> inv_columns;
+  std::vector<double> inv_values;
+  std::vector<double> current(size, 0.0);
+  std::vector<int32_t> touched_mark(size, -1);
+  std::vector<int32_t> touched;
+  for (int32_t i = 0; i < size; ++i) {
+    touched.clear();
+    current[i] = 1.0;
+    touched_mark[i] = i;
+    touched.push_back(i);
+    for (int64_t p = row_start[i]; p < row_start[i + 1] - 1; ++p) {
+      const int32_t k = pattern[p];
+      const double coefficient = values[p];
+      if (coefficient == 0.0) continue;  // subtracting a signed zero leaves every entry's value unchanged
+      for (int64_t q = inv_start[k]; q < inv_start[k + 1]; ++q) {
+        const int32_t c = inv_columns[q];
+        if (touched_mark[c] != i) {
+          touched_mark[c] = i;
+          touched.push_back(c);
+        }
+        const double product = coefficient * inv_values[q];
+        current[c] = current[c] - product;
+      }
+    }
+    std::sort(touched.begin(), touched.end());
+    for (int32_t c : touched) {
+      if (current[c] != 0.0) {
+        inv_columns.push_back(c);
+        inv_values.push_back(current[c]);
+      }
+      current[c] = 0.0;
+    }
+    if (inv_columns.size() > static_cast<size_t>(std::numeric_limits<int32_t>::max())) {
+      return "inverse factor fill exceeds int32 sparse indexing";
+    }
+    inv_start.push_back(static_cast<int64_t>(inv_columns.size()));
+  }
+  const int64_t nnz = static_cast<int64_t>(inv_columns.size());
+
+  // --- CSR of S (rows: elimination order, columns: original, sorted) ------
+  out->size = size;
+  out->permutation = permutation;
+  out->diagonal = diagonal;
+  out->factorization_nnz = static_cast<int64_t>(size) + (pattern_nnz - size);
+  out->matrix_nnz = matrix_nnz;
+  Csr& s = out->s;
+  s.offsets.assign(size + 1, 0);
+  s.columns.resize(nnz);
+  s.values.resize(nnz);
+  std::vector<std::pair<int32_t, double>> row;
+  for (int32_t i = 0; i < size; ++i) {
+    const double scale = 1.0 / std::sqrt(diagonal[i]);
+    row.clear();
+    for (int64_t q = inv_start[i]; q < inv_start[i + 1]; ++q) {
+      row.emplace_back(permutation[inv_columns[q]], inv_values[q] * scale);
+    }
+    std::sort(row.begin(), row.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    const int64_t base = inv_start[i];
+    for (size_t q = 0; q < row.size(); ++q) {
+      s.columns[base + q] = row[q].first;
+      s.values[base + q] = row[q].second;
+      if (!std::isfinite(row[q].second)) return "inverse factor overflowed float64";
+    }
+    s.offsets[i + 1] = static_cast<int32_t>(inv_start[i + 1]);
+  }
+  // --- CSR of S^T -----------------------------------------------------------
+  Csr& st = out->st;
+  st.offsets.assign(size + 1, 0);
+  st.columns.resize(nnz);
+  st.values.resize(nnz);
+  for (int64_t q = 0; q < nnz; ++q) st.offsets[s.columns[q] + 1] += 1;
+  for (int32_t i = 0; i < size; ++i) st.offsets[i + 1] += st.offsets[i];
+  {
+    std::vector<int32_t> cursor(st.offsets.begin(), st.offsets.end() - 1);
+    for (int32_t r = 0; r < size; ++r) {
+      for (int32_t q = s.offsets[r]; q < s.offsets[r + 1]; ++q) {
+        const int32_t at = cursor[s.columns[q]]++;
+        st.columns[at] = r;
+        st.values[at] = s.values[q];
+      }
+    }
+  }
+  return std::string();
+}
+
+}  // namespace pdb200

@@ -1,0 +1,44 @@
+// Exact sparse inverse factor A^{-1} = S^T S of a constant SPD scalar matrix.
+//
+// Host-side setup of the DiffPhD global step. It follows the reference's
+// SparseInverse setup (src/newton_solver_diff_phd/_src/solvers/diff_phd/sparse.py):
+// nested dissection with minimum-degree leaves (:18-70), symbolic fill and a
+// right-looking numeric LDL^T in a fixed update order (:98-156), inverse rows
+// with exact-zero omission (:159-177) and CSR output sorted by column
+// (:180-191, :301-314). Every floating-point update is one rounded multiply
+// followed by one rounded subtract, as NumPy evaluates them, so the factor is
+// bit-identical to the reference's for the same input rows.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace pdb200 {
+
+struct Csr {
+  std::vector<int32_t> offsets;
+  std::vector<int32_t> columns;
+  std::vector<double> values;
+};
+
+struct InverseFactor {
+  int32_t size = 0;
+  std::vector<int32_t> permutation;  // elimination order -> original index
+  std::vector<double> diagonal;      // LDL^T pivots in elimination order
+  Csr s;                             // rows: elimination order, columns: original index
+  Csr st;                            // S^T: rows original index, columns elimination order
+  int64_t factorization_nnz = 0;     // size + strict lower nnz(L)
+  int64_t matrix_nnz = 0;
+};
+
+// Validates rows (finite, positive diagonal, exact symmetry) and builds the
+// factor. Returns an empty string on success, otherwise the reason.
+std::string build_inverse_factor(int32_t size, const int32_t* row_offsets, const int32_t* row_columns,
+                                 const double* row_values, InverseFactor* out);
+
+// Nested-dissection order of an undirected graph given as sorted adjacency
+// lists without self loops (the reference _nested_dissection).
+std::vector<int32_t> nested_dissection(const std::vector<std::vector<int32_t>>& adjacency);
+
+}  // namespace pdb200

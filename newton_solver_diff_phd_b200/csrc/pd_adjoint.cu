@@ -1,0 +1,697 @@
+// Persistent backward-step kernel: the reference DiffPhD adjoint of one step
+// (Adjoint.backward, src/newton_solver_diff_phd/_src/solvers/diff_phd/adjoint.py:1088-1259),
+// extended to Hex8 cells (eight Gauss samples, sample weight w Vbar/8) and to
+// an exact mode whose K uses per-element weights.
+//
+//   prologue  seed g = dL/dq+ + dL/dv+/h (:70-81), local Jacobians dP/dF at x+
+//             (9 directional derivatives per sample, :92-137), ||g||^2 partials
+//   loop      A1 K mu per element -> A2 gather + g -> A3 S -> A4 S^T, Dirichlet
+//             zeroing, non-finite scrub, Anderson history -> serial clip / Anderson
+//             -> A5 Anderson apply -> serial clip, stopping rule (:184-321, :927-964)
+//   epilogue  routing guard (:226-261), state gradients (:474-490), Dirichlet
+//             coupling and gradients (:493-553), material and activation gradients
+//             with the parameter guard (:556-659).
+// The norm clip of 1e6 is rare; when it triggers, an extra phase rescales the
+// affected vector and recomputes its partials, so the fast path stays at five
+// grid barriers per iteration.
+#include <cuda_runtime.h>
+
+#include "pd_forward.cuh"
+#include "pd_kernels.h"
+
+namespace pdb200 {
+
+constexpr double kClipNorm = 1.0e6;
+
+template <typename TL>
+__device__ __forceinline__ TL* jacobian_ptr(const AdjointArgs& b);
+template <>
+__device__ __forceinline__ double* jacobian_ptr<double>(const AdjointArgs& b) { return b.jac64; }
+template <>
+__device__ __forceinline__ float* jacobian_ptr<float>(const AdjointArgs& b) { return b.jac32; }
+
+// Directional derivative of the projection stress w.r.t. F, applied to e_r e_c^T,
+// for the nine flattened directions c9 = r + 3 c (Eigen column-major order).
+template <typename TL>
+__device__ void sample_jacobian(const AdjointArgs& b, int e, const M3<TL>& f, TL* out /* [9][9] row-major per direction */) {
+  M3<TL> u, v;
+  V3<TL> sigma;
+  unsigned_svd(f, u, sigma, v);
+  const bool exact = b.exact != 0;
+  const TL wc = static_cast<TL>(exact ? b.wc[e] : b.jwc);
+  const TL wv = static_cast<TL>(exact ? b.wv[e] : b.jwv);
+  const TL wn = static_cast<TL>(exact ? b.wn[e] : b.jwn);
+  const TL mu = static_cast<TL>(b.nh_mu), lame = static_cast<TL>(b.nh_lame), penalty = static_cast<TL>(b.nh_penalty);
+  V3<TL> offset = v3<TL>(TL(0), TL(0), TL(0));
+  V3<TL> stretches = offset;
+  if (b.material == 0) {
+    bool singular;
+    offset = volume_offset(sigma, singular);
+  } else {
+    stretches = nh_prox_stretches(sigma, mu, lame, penalty);
+  }
+  const TL wm = b.has_muscles ? static_cast<TL>(b.wm[e]) : TL(0);
+  V3<TL> m = v3<TL>(TL(0), TL(0), TL(0));
+  TL target = TL(0);
+  if (wm != TL(0)) {
+    m = load3<TL>(b.mdir, e);
+    target = b.activations != nullptr ? static_cast<TL>(1.0 - static_cast<double>(b.activations[e]))
+                                      : static_cast<TL>(b.mtarget[e]);
+  }
+  for (int c9 = 0; c9 < 9; ++c9) {
+    M3<TL> df = zero3<TL>();
+    df.a[c9 % 3][c9 / 3] = TL(1);
+    M3<TL> dp = zero3<TL>();
+    if (b.material == 0) {
+      if (wc != TL(0)) dp = dp + wc * corotated_jvp(u, sigma, v, df);
+      if (wv != TL(0)) dp = dp + wv * volume_jvp(u, sigma, v, offset, df);
+    } else if (wn != TL(0)) {
+      dp = dp + wn * nh_prox_jvp(u, sigma, v, stretches, df, mu, lame, penalty);
+    }
+    if (wm != TL(0)) dp = dp + wm * outer(muscle_jvp(f, m, target, df), m);
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) out[c9 * 9 + r * 3 + c] = dp.a[r][c];
+  }
+}
+
+// ds = sum_c dF[c % 3][c / 3] J_c.
+template <typename TL>
+__device__ __forceinline__ M3<double> apply_jacobian(const TL* jac, const double df[3][3]) {
+  M3<double> ds = zero3<double>();
+  for (int c9 = 0; c9 < 9; ++c9) {
+    const double coefficient = df[c9 % 3][c9 / 3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) ds.a[r][c] += coefficient * static_cast<double>(jac[c9 * 9 + r * 3 + c]);
+  }
+  return ds;
+}
+
+__device__ __forceinline__ void deformation_from(const int* idx, const double* grad, int corners, const double* vec,
+                                                 double out[3][3]) {
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) out[r][c] = 0.0;
+  for (int k = 0; k < corners; ++k) {
+    const int v = idx[k];
+    const double* g = grad + 3 * k;
+    const double px = vec[3 * v], py = vec[3 * v + 1], pz = vec[3 * v + 2];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      out[0][c] += px * g[c];
+      out[1][c] += py * g[c];
+      out[2][c] += pz * g[c];
+    }
+  }
+}
+
+// Per-sample gradient rows: Tet4 element e, or Hex8 sample s (shared).
+__device__ __forceinline__ const double* sample_gradients(const AdjointArgs& b, const double* grad_smem, int e, int s) {
+  return b.hex ? grad_smem + 8 * 3 * s : b.gradients + 12 * e;
+}
+
+// Element phase writing corner contributions of the operator `op` applied to
+// `vec`: op 0 -> K vec (local Jacobian), op 1 -> (A - K) vec without the mass
+// term (Dirichlet coupling, adjoint.py:493-521).
+template <typename TL>
+__device__ void element_operator(const AdjointArgs& b, const double* grad_smem, const double* vec, int op, int gtid,
+                                 int gthreads) {
+  const int samples = b.hex ? 8 : 1;
+  const int corners = b.corners;
+  const int total = b.ne * samples;
+  // Hex8 contributions are summed over the eight samples of a cell in a fixed
+  // order by the thread that owns the cell; Tet4 has one sample per element.
+  for (int e = gtid; e < b.ne; e += gthreads) {
+    double acc[8][3];
+    for (int k = 0; k < corners; ++k) acc[k][0] = acc[k][1] = acc[k][2] = 0.0;
+    for (int s = 0; s < samples; ++s) {
+      const double* g = sample_gradients(b, grad_smem, e, s);
+      double df[3][3];
+      deformation_from(b.indices + corners * e, g, corners, vec, df);
+      const TL* jac = jacobian_ptr<TL>(b) + static_cast<size_t>(e * samples + s) * 81;
+      M3<double> ds = apply_jacobian<TL>(jac, df);
+      if (op == 1) {
+        const double w = b.wc[e] + b.wv[e] + b.wn[e];
+        M3<double> a = zero3<double>();
+        for (int r = 0; r < 3; ++r)
+          for (int c = 0; c < 3; ++c) a.a[r][c] = w * df[r][c];
+        if (b.has_muscles && b.wm[e] != 0.0) {
+          const V3<double> m = load3d(b.mdir, e);
+          V3<double> dfm;
+          for (int r = 0; r < 3; ++r) dfm[r] = df[r][0] * m.x + df[r][1] * m.y + df[r][2] * m.z;
+          a = a + b.wm[e] * outer(dfm, m);
+        }
+        ds = a - ds;
+      }
+      for (int k = 0; k < corners; ++k) {
+        const V3<double> gk = v3<double>(g[3 * k], g[3 * k + 1], g[3 * k + 2]);
+        const V3<double> c = mul(ds, gk);
+        acc[k][0] += c.x;
+        acc[k][1] += c.y;
+        acc[k][2] += c.z;
+      }
+    }
+    (void)total;
+    for (int k = 0; k < corners; ++k) {
+      double* out = b.contrib + (corners * e + k) * 3;
+      out[0] = acc[k][0];
+      out[1] = acc[k][1];
+      out[2] = acc[k][2];
+    }
+  }
+}
+
+__device__ __forceinline__ V3<double> gather_row(const AdjointArgs& b, int i) {
+  double px = 0.0, py = 0.0, pz = 0.0;
+  for (int k = b.inc_offsets[i]; k < b.inc_offsets[i + 1]; ++k) {
+    const double* c = b.contrib + 3 * b.inc_entries[k];
+    px += c[0];
+    py += c[1];
+    pz += c[2];
+  }
+  return v3<double>(px, py, pz);
+}
+
+// Block partial of the Anderson Gram entries (same layout as the forward).
+__device__ void adjoint_gram_partials(const AdjointArgs& b, int r0, int r1, int count, int start, double* block_out,
+                                      double* scratch) {
+  const int entries = count * (count + 1) / 2 + count;
+  const int capacity = b.window + 1;
+  const int groups = entries > 0 ? kBlock / entries : 0;
+  const int t = threadIdx.x;
+  double sum = 0.0;
+  const size_t stride = static_cast<size_t>(3) * b.n;
+  if (entries > 0 && t < groups * entries) {
+    const int entry = t % entries;
+    const int group = t / entries;
+    const int pairs = count * (count + 1) / 2;
+    if (entry < pairs) {
+      int ea, eb;
+      gram_entry_pair(entry, count, ea, eb);
+      const double* ga1 = b.hist_g + ((start + ea + 1) % capacity) * stride;
+      const double* ga0 = b.hist_g + ((start + ea) % capacity) * stride;
+      const double* gb1 = b.hist_g + ((start + eb + 1) % capacity) * stride;
+      const double* gb0 = b.hist_g + ((start + eb) % capacity) * stride;
+      for (int i = r0 + group; i < r1; i += groups)
+        for (int c = 0; c < 3; ++c) sum += (ga1[3 * i + c] - ga0[3 * i + c]) * (gb1[3 * i + c] - gb0[3 * i + c]);
+    } else {
+      const int ea = entry - pairs;
+      const double* ga1 = b.hist_g + ((start + ea + 1) % capacity) * stride;
+      const double* ga0 = b.hist_g + ((start + ea) % capacity) * stride;
+      const double* gn = b.hist_g + ((start + count) % capacity) * stride;
+      for (int i = r0 + group; i < r1; i += groups)
+        for (int c = 0; c < 3; ++c) sum += (ga1[3 * i + c] - ga0[3 * i + c]) * gn[3 * i + c];
+    }
+  }
+  scratch[t] = sum;
+  __syncthreads();
+  if (t < entries) {
+    double total = 0.0;
+    for (int g = 0; g < groups; ++g) total += scratch[g * entries + t];
+    block_out[t] = total;
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ V3<double> adjoint_aa_apply_row(const AdjointArgs& b, int i, int count, int start,
+                                                           const double* gamma) {
+  const int capacity = b.window + 1;
+  const size_t stride = static_cast<size_t>(3) * b.n;
+  const int slot = (start + count) % capacity;
+  V3<double> value;
+  for (int c = 0; c < 3; ++c) value[c] = b.hist_x[slot * stride + 3 * i + c] + b.hist_g[slot * stride + 3 * i + c];
+  for (int k = 0; k < count; ++k) {
+    const int low = (start + k) % capacity;
+    const int high = (start + k + 1) % capacity;
+    for (int c = 0; c < 3; ++c) {
+      const size_t h = high * stride + 3 * i + c;
+      const size_t l = low * stride + 3 * i + c;
+      value[c] -= (b.hist_x[h] - b.hist_x[l] + b.hist_g[h] - b.hist_g[l]) * gamma[k];
+    }
+  }
+  return value;
+}
+
+// Partial slots inside a block's kPartialStride doubles.
+constexpr int kSlotGram = 0;      // .. 43
+constexpr int kSlotRaw = 48;      // ||raw||^2 after the solve
+constexpr int kSlotStep = 49;     // ||raw - prev||^2
+constexpr int kSlotMixed = 50;    // ||raw||^2 after mixing
+constexpr int kSlotRhs = 51;      // ||g||^2 (seed)
+constexpr int kSlotMaterial = 52; // material gradient column sums (2)
+constexpr int kSlotActivation = 54;
+
+template <typename TL, typename TV>
+__global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs b) {
+  __shared__ double s_grad[8 * 8 * 3];
+  __shared__ double s_scratch[kBlock];
+  __shared__ double s_reduced[64];
+  __shared__ int s_control[8];
+  const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int gthreads = gridDim.x * blockDim.x;
+  const int n = b.n;
+  const int samples = b.hex ? 8 : 1;
+  const int corners = b.corners;
+  if (b.hex) {
+    for (int t = threadIdx.x; t < 8 * 8 * 3; t += blockDim.x) s_grad[t] = b.gradients[t];
+    __syncthreads();
+  }
+  const int s_r0 = b.s_part[blockIdx.x], s_r1 = b.s_part[blockIdx.x + 1];
+  const int r0 = b.st_part[blockIdx.x], r1 = b.st_part[blockIdx.x + 1];
+  double* my_partials = b.partials + static_cast<size_t>(blockIdx.x) * kPartialStride;
+  const size_t hstride = static_cast<size_t>(3) * n;
+  const double dt = b.dt;
+
+  // ---- Prologue: seed (own rows), local Jacobians (elements).
+  {
+    double rhs2 = 0.0;
+    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+      V3<double> g;
+      for (int c = 0; c < 3; ++c) {
+        const double velocity = static_cast<double>(b.gqd_out[3 * i + c]) / dt;
+        g[c] = static_cast<double>(b.gq_out[3 * i + c]) + velocity;
+        b.base[3 * i + c] = -velocity;
+      }
+      store3(b.rhs, i, g);
+      store3(b.solution, i, v3<double>(0.0, 0.0, 0.0));
+      rhs2 += dot(g, g);
+    }
+    rhs2 = block_sum(rhs2, s_scratch);
+    if (threadIdx.x == 0) my_partials[kSlotRhs] = rhs2;
+  }
+  for (int t = gtid; t < b.ne * samples; t += gthreads) {
+    const int e = t / samples;
+    const int s = t % samples;
+    double fm[3][3];
+    deformation_from(b.indices + corners * e, sample_gradients(b, s_grad, e, s), corners, b.x, fm);
+    M3<TL> f;
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) f.a[r][c] = static_cast<TL>(fm[r][c]);
+    TL jac[81];
+    sample_jacobian<TL>(b, e, f, jac);
+    TL* out = jacobian_ptr<TL>(b) + static_cast<size_t>(t) * 81;
+    for (int k = 0; k < 81; ++k) out[k] = jac[k];
+  }
+  if (gtid == 0) {
+    b.aa_state[0] = b.aa_state[1] = b.aa_state[2] = b.aa_state[3] = 0;
+    *b.aa_accept = 0;
+    *b.iteration = 0;
+    *b.active = 1;
+  }
+  if (!grid_sync(b.barrier, b.status)) return;
+
+  for (;;) {
+    // ---- A1: K solution per element.
+    element_operator<TL>(b, s_grad, b.solution, 0, gtid, gthreads);
+    if (!grid_sync(b.barrier, b.status)) return;
+
+    // ---- A2: work = g + gather(K solution) (refinement: minus A solution).
+    for (int i = gtid; i < n; i += gthreads) {
+      const V3<double> k = gather_row(b, i);
+      V3<double> w = k + load3d(b.rhs, i);
+      if (b.refine) {
+        for (int q = b.a_off[i]; q < b.a_off[i + 1]; ++q) {
+          const double v = b.a_val[q];
+          const int j = b.a_col[q];
+          w.x -= v * b.solution[3 * j];
+          w.y -= v * b.solution[3 * j + 1];
+          w.z -= v * b.solution[3 * j + 2];
+        }
+      }
+      store3(b.work, i, w);
+    }
+    if (!grid_sync(b.barrier, b.status)) return;
+
+    // ---- A3: y = S work.
+    if (sizeof(TV) == sizeof(double)) {
+      spmv_rows<double>(b.s_off, b.s_col, b.s_val, b.work, b.y, s_r0, s_r1);
+    } else {
+      spmv_rows<float>(b.s_off, b.s_col, b.s_val32, b.work, b.y, s_r0, s_r1);
+    }
+    if (!grid_sync(b.barrier, b.status)) return;
+
+    // ---- A4: raw = S^T y; Dirichlet zeroing and scrub; history; partials.
+    if (sizeof(TV) == sizeof(double)) {
+      spmv_rows<double>(b.st_off, b.st_col, b.st_val, b.y, b.raw, r0, r1);
+    } else {
+      spmv_rows<float>(b.st_off, b.st_col, b.st_val32, b.y, b.raw, r0, r1);
+    }
+    __syncthreads();
+    const int count = b.window > 0 ? b.aa_state[0] : 0;
+    const int start = b.window > 0 ? b.aa_state[1] : 0;
+    const int capacity = b.window + 1;
+    {
+      double raw2 = 0.0, step2 = 0.0;
+      for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+        V3<double> value = load3d(b.raw, i);
+        const V3<double> previous = load3d(b.solution, i);
+        if (b.refine) value = value + previous;
+        if (b.free_[i] == 0) value = v3<double>(0.0, 0.0, 0.0);
+        for (int c = 0; c < 3; ++c) {
+          if (!isfinite(value[c])) {
+            value[c] = 0.0;
+            atomicOr(b.status, kStatusAdjointSafeguard);
+          }
+        }
+        store3(b.raw, i, value);
+        store3(b.prev, i, previous);
+        raw2 += dot(value, value);
+        const V3<double> step = value - previous;
+        step2 += dot(step, step);
+        if (b.window > 0) {
+          const int slot = (start + count) % capacity;
+          double* hx = b.hist_x + slot * hstride + 3 * i;
+          double* hg = b.hist_g + slot * hstride + 3 * i;
+          for (int c = 0; c < 3; ++c) {
+            hx[c] = previous[c];
+            hg[c] = step[c];
+          }
+        }
+      }
+      raw2 = block_sum(raw2, s_scratch);
+      step2 = block_sum(step2, s_scratch);
+      if (threadIdx.x == 0) {
+        my_partials[kSlotRaw] = raw2;
+        my_partials[kSlotStep] = step2;
+      }
+      if (b.window > 0) {
+        __syncthreads();
+        adjoint_gram_partials(b, r0, r1, count, start, my_partials + kSlotGram, s_scratch);
+      }
+      // Serial: norm clip of the solve result (safe_clip, adjoint.py:184-223);
+      // without clipping also the Anderson solve and the step norm.
+      unsigned generation;
+      if (barrier_arrive(b.barrier, generation)) {
+        reduce_partials(b.partials, kSlotRaw, 2, gridDim.x, s_reduced, s_scratch);
+        const double len = sqrt(s_reduced[0]);
+        const bool clip = isfinite(len) && len > kClipNorm;
+        if (threadIdx.x == 0) {
+          b.control_d[0] = clip ? kClipNorm / len : 1.0;
+          b.control_d[1] = s_reduced[1];
+          if (clip) atomicOr(b.status, kStatusAdjointSafeguard);
+        }
+        __syncthreads();
+        if (!clip && b.window > 0) {
+          const int entries = count * (count + 1) / 2 + count;
+          reduce_partials(b.partials, kSlotGram, entries, gridDim.x, s_reduced, s_scratch);
+          if (threadIdx.x == 0) aa_solve(b.aa_state, b.aa_gamma, b.aa_accept, s_reduced, b.window);
+        }
+        barrier_release(b.barrier, generation);
+        __syncthreads();
+      } else if (!barrier_wait(b.barrier, generation, b.status)) {
+        return;
+      }
+    }
+    const double clip1 = *reinterpret_cast<volatile double*>(b.control_d);
+    if (clip1 != 1.0) {
+      // Rare slow path: rescale, then redo the step norm, history and Gram.
+      double step2 = 0.0;
+      for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+        const V3<double> value = clip1 * load3d(b.raw, i);
+        store3(b.raw, i, value);
+        const V3<double> step = value - load3d(b.prev, i);
+        step2 += dot(step, step);
+        if (b.window > 0) {
+          const int slot = (start + count) % capacity;
+          double* hg = b.hist_g + slot * hstride + 3 * i;
+          for (int c = 0; c < 3; ++c) hg[c] = step[c];
+        }
+      }
+      step2 = block_sum(step2, s_scratch);
+      if (threadIdx.x == 0) my_partials[kSlotStep] = step2;
+      if (b.window > 0) {
+        __syncthreads();
+        adjoint_gram_partials(b, r0, r1, count, start, my_partials + kSlotGram, s_scratch);
+      }
+      unsigned generation;
+      if (barrier_arrive(b.barrier, generation)) {
+        if (b.window > 0) {
+          const int entries = count * (count + 1) / 2 + count;
+          reduce_partials(b.partials, kSlotGram, entries, gridDim.x, s_reduced, s_scratch);
+          if (threadIdx.x == 0) aa_solve(b.aa_state, b.aa_gamma, b.aa_accept, s_reduced, b.window);
+          __syncthreads();
+        }
+        reduce_partials(b.partials, kSlotStep, 1, gridDim.x, s_reduced, s_scratch);
+        if (threadIdx.x == 0) b.control_d[1] = s_reduced[0];
+        barrier_release(b.barrier, generation);
+        __syncthreads();
+      } else if (!barrier_wait(b.barrier, generation, b.status)) {
+        return;
+      }
+    }
+
+    // ---- A5: Anderson apply, second clip, stopping rule.
+    {
+      int accept = 0, used_count = 0, used_start = 0;
+      if (b.window > 0) {
+        accept = *reinterpret_cast<volatile int*>(b.aa_accept);
+        used_count = *reinterpret_cast<volatile int*>(b.aa_state + 2);
+        used_start = *reinterpret_cast<volatile int*>(b.aa_state + 3);
+        if (threadIdx.x < kMaxWindow) s_reduced[32 + threadIdx.x] = reinterpret_cast<volatile double*>(b.aa_gamma)[threadIdx.x];
+        __syncthreads();
+      }
+      double mixed2 = 0.0;
+      for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+        V3<double> value = load3d(b.raw, i);
+        if (accept) value = adjoint_aa_apply_row(b, i, used_count, used_start, s_reduced + 32);
+        if (b.free_[i] == 0) value = v3<double>(0.0, 0.0, 0.0);
+        for (int c = 0; c < 3; ++c) {
+          if (!isfinite(value[c])) {
+            value[c] = 0.0;
+            atomicOr(b.status, kStatusAdjointSafeguard);
+          }
+        }
+        store3(b.solution, i, value);
+        mixed2 += dot(value, value);
+      }
+      mixed2 = block_sum(mixed2, s_scratch);
+      if (threadIdx.x == 0) my_partials[kSlotMixed] = mixed2;
+      unsigned generation;
+      if (barrier_arrive(b.barrier, generation)) {
+        reduce_partials(b.partials, kSlotMixed, 1, gridDim.x, s_reduced, s_scratch);
+        if (threadIdx.x == 0) {
+          const double len = sqrt(s_reduced[0]);
+          double scale = 1.0;
+          double solution_norm = len;
+          if (isfinite(len) && len > kClipNorm) {
+            scale = kClipNorm / len;
+            solution_norm = sqrt(scale * scale * s_reduced[0]);
+            atomicOr(b.status, kStatusAdjointSafeguard);
+          }
+          b.control_d[2] = scale;
+          const double step_norm = sqrt(b.control_d[1]);
+          const int k = *b.iteration;
+          *b.iteration = k + 1;
+          int active = 1;
+          if (k > 0 && step_norm < b.rel_tol * solution_norm + b.abs_tol) {
+            active = 0;
+          } else if (k + 1 >= b.max_iterations) {
+            active = 0;
+            atomicOr(b.status, kStatusAdjointNotConverged);
+          }
+          *b.active = active;
+          b.control_d[3] = solution_norm;
+        }
+        barrier_release(b.barrier, generation);
+        __syncthreads();
+      } else if (!barrier_wait(b.barrier, generation, b.status)) {
+        return;
+      }
+      const double clip2 = *reinterpret_cast<volatile double*>(b.control_d + 2);
+      if (clip2 != 1.0) {
+        for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) store3(b.solution, i, clip2 * load3d(b.solution, i));
+        if (!grid_sync(b.barrier, b.status)) return;
+      }
+      if (threadIdx.x == 0) s_control[0] = *reinterpret_cast<volatile int*>(b.active);
+      __syncthreads();
+      if (s_control[0] == 0) break;
+    }
+  }
+
+  // ---- Routing guard (adjoint.py:1125-1138, :226-261), in one serial section.
+  {
+    unsigned generation;
+    if (barrier_arrive(b.barrier, generation)) {
+      reduce_partials(b.partials, kSlotRhs, 1, gridDim.x, s_reduced, s_scratch);
+      if (threadIdx.x == 0) {
+        const double mu_norm = *reinterpret_cast<volatile double*>(b.control_d + 3);
+        const bool failed = kClipNorm > 0.0 && mu_norm >= 0.999 * kClipNorm;
+        double value = 1.0;
+        if (failed) {
+          value = 0.0;
+          atomicOr(b.status, kStatusAdjointSafeguard);
+        } else {
+          const double cap = sqrt(s_reduced[0]) + 1.0;
+          const double injection = b.inertia * mu_norm;
+          if (injection > cap) {
+            value = cap / injection;
+            atomicOr(b.status, kStatusAdjointSafeguard);
+          }
+        }
+        b.control_d[4] = value;
+        b.control_i[0] = failed ? 1 : 0;
+      }
+      barrier_release(b.barrier, generation);
+      __syncthreads();
+    } else if (!barrier_wait(b.barrier, generation, b.status)) {
+      return;
+    }
+  }
+  const double routing = *reinterpret_cast<volatile double*>(b.control_d + 4);
+  const int diverged = *reinterpret_cast<volatile int*>(b.control_i);
+
+  // ---- State gradients (own rows, adjoint.py:474-490).
+  for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+    for (int c = 0; c < 3; ++c) {
+      const double mu = b.solution[3 * i + c];
+      const double injection = routing * b.inertia * mu;
+      b.gq[3 * i + c] = b.gq[3 * i + c] + static_cast<float>(b.base[3 * i + c] + injection);
+      b.gqd[3 * i + c] = b.gqd[3 * i + c] + static_cast<float>(dt * injection);
+      b.gf[3 * i + c] = b.gf[3 * i + c] + static_cast<float>(routing * mu);
+    }
+  }
+
+  // ---- Element epilogue: Dirichlet coupling contributions, material and
+  // activation gradients from z = mu (no contact rows).
+  if (b.has_dirichlet) {
+    if (diverged) {
+      for (int t = gtid; t < b.ne * corners * 3; t += gthreads) b.contrib[t] = 0.0;
+    } else {
+      element_operator<TL>(b, s_grad, b.solution, 1, gtid, gthreads);
+    }
+  }
+  double material0 = 0.0, material1 = 0.0, activation = 0.0;
+  const bool want_material = b.gmaterials != nullptr;
+  const bool want_activation = b.gactivations != nullptr && b.has_muscles;
+  if (want_material || want_activation) {
+    const double volume = b.sample_volume;
+    for (int e = gtid; e < b.ne; e += gthreads) {
+      double first_value = 0.0, second_value = 0.0, act_value = 0.0;
+      for (int s = 0; s < samples; ++s) {
+        const double* g = sample_gradients(b, s_grad, e, s);
+        double fm[3][3];
+        deformation_from(b.indices + corners * e, g, corners, b.x, fm);
+        M3<double> f;
+        for (int r = 0; r < 3; ++r)
+          for (int c = 0; c < 3; ++c) f.a[r][c] = fm[r][c];
+        M3<double> first = zero3<double>(), second = zero3<double>();
+        if (want_material) {
+          if (b.material == 0) {
+            M3<double> u, v;
+            V3<double> sigma;
+            unsigned_svd(f, u, sigma, v);
+            bool singular;
+            const V3<double> offset = volume_offset(sigma, singular);
+            first = f - mul(u, transpose(v));
+            second = f - udvt(u, sigma + offset, v);
+          } else {
+            first = (1.0 / (2.0 * b.nh_mu)) * neo_hookean_stress(f, b.nh_mu, b.nh_lame);
+          }
+        }
+        V3<double> fibre = v3<double>(0.0, 0.0, 0.0);
+        double len = 0.0;
+        V3<double> m = fibre;
+        const bool fibre_on = want_activation && b.wm[e] != 0.0;
+        if (fibre_on) {
+          m = load3d(b.mdir, e);
+          fibre = mul(f, m);
+          len = length(fibre);
+        }
+        for (int k = 0; k < corners; ++k) {
+          const int v = b.indices[corners * e + k];
+          const V3<double> z = load3d(b.solution, v);
+          const V3<double> gk = v3<double>(g[3 * k], g[3 * k + 1], g[3 * k + 2]);
+          first_value -= dot(z, mul(first, gk));
+          second_value -= dot(z, mul(second, gk));
+          if (fibre_on && len > DBL_EPSILON) act_value += dot(z, (b.wm[e] / len * dot(m, gk)) * fibre);
+        }
+      }
+      const double g0 = 2.0 * volume * first_value;
+      const double g1 = b.material == 0 ? volume * second_value : 0.0;
+      if (want_material) {
+        b.material_scratch[2 * e] = g0;
+        b.material_scratch[2 * e + 1] = g1;
+        material0 += g0;
+        material1 += g1;
+      }
+      if (want_activation) {
+        b.activation_scratch[e] = -act_value;
+        activation += -act_value;
+      }
+    }
+  }
+  material0 = block_sum(material0, s_scratch);
+  material1 = block_sum(material1, s_scratch);
+  activation = block_sum(activation, s_scratch);
+  if (threadIdx.x == 0) {
+    my_partials[kSlotMaterial] = material0;
+    my_partials[kSlotMaterial + 1] = material1;
+    my_partials[kSlotActivation] = activation;
+  }
+  // Parameter guard (adjoint.py:622-644).
+  {
+    unsigned generation;
+    if (barrier_arrive(b.barrier, generation)) {
+      reduce_partials(b.partials, kSlotMaterial, 3, gridDim.x, s_reduced, s_scratch);
+      if (threadIdx.x == 0) {
+        const bool material_ok = !b.zero_energy_weight && isfinite(s_reduced[0]) && isfinite(s_reduced[1]);
+        const bool activation_ok = isfinite(s_reduced[2]);
+        b.control_i[1] = (diverged == 0 && material_ok) ? 1 : 0;
+        b.control_i[2] = (diverged == 0 && activation_ok) ? 1 : 0;
+        if ((want_material && !material_ok) || (want_activation && !activation_ok)) {
+          atomicOr(b.status, kStatusAdjointSafeguard);
+        }
+      }
+      barrier_release(b.barrier, generation);
+      __syncthreads();
+    } else if (!barrier_wait(b.barrier, generation, b.status)) {
+      return;
+    }
+  }
+  const int material_valid = *reinterpret_cast<volatile int*>(b.control_i + 1);
+  const int activation_valid = *reinterpret_cast<volatile int*>(b.control_i + 2);
+  if (want_material && material_valid) {
+    for (int e = gtid; e < b.ne; e += gthreads) {
+      b.gmaterials[2 * e] += b.material_scratch[2 * e];
+      b.gmaterials[2 * e + 1] += b.material_scratch[2 * e + 1];
+    }
+  }
+  if (want_activation && activation_valid) {
+    for (int e = gtid; e < b.ne; e += gthreads) {
+      b.gactivations[e] = b.gactivations[e] + static_cast<float>(b.activation_scratch[e]);
+    }
+  }
+  // Dirichlet gradients: dL/dx_D = g_D - (A - K)_DF mu_F (adjoint.py:524-553).
+  if (b.has_dirichlet) {
+    for (int i = gtid; i < n; i += gthreads) {
+      if (b.free_[i] != 0) continue;
+      const V3<double> coupling = gather_row(b, i);
+      for (int c = 0; c < 3; ++c) {
+        const double value = b.rhs[3 * i + c] - coupling[c];
+        if (b.gdirichlet != nullptr) {
+          b.gdirichlet[3 * i + c] = b.gdirichlet[3 * i + c] + static_cast<float>(value);
+        } else {
+          b.gq[3 * i + c] = b.gq[3 * i + c] + static_cast<float>(value);
+          if (b.integrate_pinned) b.gqd[3 * i + c] = b.gqd[3 * i + c] + static_cast<float>(dt * value);
+        }
+      }
+    }
+  }
+}
+
+cudaError_t launch_adjoint_step(const AdjointArgs& args, int blocks, int precision, cudaStream_t stream) {
+  void* params[] = {const_cast<AdjointArgs*>(&args)};
+  const void* kernel = precision == 0 ? reinterpret_cast<const void*>(&adjoint_step_kernel<double, double>)
+                                      : reinterpret_cast<const void*>(&adjoint_step_kernel<float, float>);
+  return cudaLaunchCooperativeKernel(kernel, dim3(blocks), dim3(kBlock), params, 0, stream);
+}
+
+cudaError_t adjoint_step_max_blocks(int precision, int* blocks_per_sm) {
+  const void* kernel = precision == 0 ? reinterpret_cast<const void*>(&adjoint_step_kernel<double, double>)
+                                      : reinterpret_cast<const void*>(&adjoint_step_kernel<float, float>);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kernel, kBlock, 0);
+}
+
+}  // namespace pdb200

@@ -1,0 +1,242 @@
+// Device-side building blocks of the persistent DiffPhD kernels: the bounded
+// grid barrier with a last-arriver serial section, fixed-order reductions,
+// and the argument block shared by the forward and adjoint kernels.
+//
+// One cooperative launch runs every local/global iteration of a step. The
+// grid is co-resident (cudaLaunchCooperativeKernel refuses otherwise), phases
+// are separated by grid barriers, and every wait gives up after a bounded
+// number of polls, raising PD_STATUS_BARRIER_TIMEOUT and unwinding the
+// kernel instead of hanging the device.
+#pragma once
+
+#include <cstdint>
+
+#include "pd_math.cuh"
+
+namespace pdb200 {
+
+constexpr int kBlock = 256;
+constexpr int kWarps = kBlock / 32;
+constexpr int kPartialStride = 64;  // doubles of per-block partial sums
+constexpr int kMaxWindow = 8;
+// Poll budget of one barrier wait (~2^26 polls of >= 32 ns: seconds, far
+// beyond any legitimate phase).
+constexpr unsigned kSpinLimit = 1u << 26;
+
+constexpr int kStatusNotConverged = 1;
+constexpr int kStatusSingular = 2;
+constexpr int kStatusActivation = 4;
+constexpr int kStatusAdjointNotConverged = 8;
+constexpr int kStatusAdjointSafeguard = 16;
+constexpr int kStatusBarrierTimeout = 1024;
+
+struct GridBarrier {
+  unsigned int count;
+  unsigned int generation;
+  unsigned int abort;
+  unsigned int pad;
+};
+
+__device__ __forceinline__ unsigned load_volatile(const unsigned* p) { return *reinterpret_cast<const volatile unsigned*>(p); }
+
+// Arrive at the grid barrier. Returns true in the block that arrived last;
+// that block must run its serial section and then call barrier_release().
+// Every other block must call barrier_wait().
+__device__ __forceinline__ bool barrier_arrive(GridBarrier* bar, unsigned& generation) {
+  __shared__ int s_last;
+  __shared__ unsigned s_generation;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    s_generation = load_volatile(&bar->generation);
+    __threadfence();
+    const unsigned arrived = atomicAdd(&bar->count, 1u) + 1u;
+    s_last = arrived == gridDim.x;
+    if (s_last) __threadfence();
+  }
+  __syncthreads();
+  generation = s_generation;
+  return s_last != 0;
+}
+
+__device__ __forceinline__ void barrier_release(GridBarrier* bar, unsigned generation) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    atomicExch(&bar->count, 0u);
+    __threadfence();
+    atomicExch(&bar->generation, generation + 1u);
+  }
+}
+
+// Returns false when the wait gave up (timeout here or an abort elsewhere).
+__device__ __forceinline__ bool barrier_wait(GridBarrier* bar, unsigned generation, int* status) {
+  __shared__ int s_ok;
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    unsigned spins = 0;
+    while (load_volatile(&bar->generation) == generation) {
+      if (load_volatile(&bar->abort) != 0u) {
+        ok = 0;
+        break;
+      }
+      if (++spins > kSpinLimit) {
+        atomicOr(status, kStatusBarrierTimeout);
+        atomicExch(&bar->abort, 1u);
+        ok = 0;
+        break;
+      }
+      __nanosleep(32);
+    }
+    __threadfence();
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// Plain barrier without a serial section.
+__device__ __forceinline__ bool grid_sync(GridBarrier* bar, int* status) {
+  unsigned generation;
+  if (barrier_arrive(bar, generation)) {
+    barrier_release(bar, generation);
+    __syncthreads();
+    return true;
+  }
+  return barrier_wait(bar, generation, status);
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int offset = 16; offset > 0; offset >>= 1) v += __shfl_xor_sync(0xffffffffu, v, offset);
+  return v;
+}
+
+// Deterministic block-wide sum of one value per thread; result valid in all threads.
+__device__ __forceinline__ double block_sum(double v, double* scratch /* [kWarps] */) {
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) scratch[warp] = v;
+  __syncthreads();
+  double total = 0.0;
+#pragma unroll
+  for (int w = 0; w < kWarps; ++w) total += scratch[w];
+  return total;
+}
+
+// Sums `count` per-block partials (at partials[b*kPartialStride + offset + e])
+// over all blocks in a fixed order. Uses the whole block; results land in
+// out[0..count) (shared memory) for every thread after the call.
+__device__ __forceinline__ void reduce_partials(const double* partials, int offset, int count, int blocks,
+                                                double* out /* shared [count] */,
+                                                double* scratch /* shared [kBlock] */) {
+  const int groups = count > 0 ? kBlock / count : 0;
+  const int t = threadIdx.x;
+  double sum = 0.0;
+  if (count > 0 && t < groups * count) {
+    const int entry = t % count;
+    const int group = t / count;
+    for (int b = group; b < blocks; b += groups) sum += partials[b * kPartialStride + offset + entry];
+  }
+  scratch[t] = sum;
+  __syncthreads();
+  if (t < count) {
+    double total = 0.0;
+    for (int g = 0; g < groups; ++g) total += scratch[g * count + t];
+    out[t] = total;
+  }
+  __syncthreads();
+}
+
+template <typename T>
+__device__ __forceinline__ V3<T> load3(const double* v, int i) {
+  return v3<T>(static_cast<T>(v[3 * i]), static_cast<T>(v[3 * i + 1]), static_cast<T>(v[3 * i + 2]));
+}
+__device__ __forceinline__ V3<double> load3d(const double* v, int i) { return v3<double>(v[3 * i], v[3 * i + 1], v[3 * i + 2]); }
+__device__ __forceinline__ void store3(double* v, int i, V3<double> a) {
+  v[3 * i] = a.x;
+  v[3 * i + 1] = a.y;
+  v[3 * i + 2] = a.z;
+}
+
+// Everything one persistent launch needs. Passed by value as kernel argument.
+struct StepArgs {
+  // Mesh
+  int n;         // vertices
+  int ne;        // elements
+  int corners;   // 4 (Tet4) or 8 (Hex8)
+  int hex;       // 1 when every element has eight shared-gradient samples
+  const int* indices;      // [ne][corners]
+  const double* gradients; // Tet4 [ne][4][3]; Hex8 [8][8][3]
+  const int* free_;        // [n]
+  const int* inc_offsets;  // [n+1]
+  const int* inc_entries;  // element*corners + corner, element-major order
+  const double* plane_weight;  // [n] stiffness of the vertex-plane energy (0: none), or nullptr
+  double plane[4];
+  // Materials (per element; for Hex8 already multiplied by the sample volume)
+  const double* wc;
+  const double* wv;
+  const double* wn;
+  const double* wm;
+  const double* mdir;      // [ne][3]
+  double* mtarget;         // [ne]
+  const float* activations;  // Tet4 contractions [ne] or nullptr
+  int has_muscles;
+  int material;
+  double nh_mu, nh_lame, nh_penalty;
+  // Factor (S: rows in elimination order; S^T: rows in particle order)
+  const int* s_off;
+  const int* s_col;
+  const double* s_val;
+  const float* s_val32;
+  const int* st_off;
+  const int* st_col;
+  const double* st_val;
+  const float* st_val32;
+  const int* s_part;   // [blocks+1] S row partition
+  const int* st_part;  // [blocks+1] S^T row partition (also owns particle rows)
+  const int* a_off;    // constant matrix A (refinement residual)
+  const int* a_col;
+  const double* a_val;
+  int refine;          // 1: delta form x = x_prev + S^T S (b - A x_prev)
+  // Step vectors [n][3] float64
+  double* position;
+  double* velocity;
+  double* target;
+  double* boundary;
+  double* x;
+  double* prev;
+  double* proj;
+  double* prev_proj;
+  double* rhs;
+  double* y;
+  double* contrib;  // [ne][corners][3]
+  // Anderson
+  int window;
+  double* hist_x;   // [(window+1)][3n]
+  double* hist_g;
+  int* aa_state;    // count, start, count_used, start_used
+  double* aa_gamma; // [kMaxWindow]
+  int* aa_accept;
+  double* partials; // [blocks][kPartialStride]
+  // Loop control
+  int* iteration;
+  int* active;
+  int* status;
+  int max_iterations;
+  double abs_tol, rel_tol;
+  GridBarrier* barrier;
+  // Inputs and outputs of the step
+  const float* q_in;
+  const float* qd_in;
+  const float* f_in;
+  const float* dirichlet;
+  float* q_out;
+  float* qd_out;
+  double* x_record;
+  double dt, mass, inertia;
+  double gravity[3];
+  int integrate_pinned;
+};
+
+}  // namespace pdb200

@@ -1,0 +1,404 @@
+// Phases of the forward projective-dynamics step (one persistent launch).
+//
+// Per iteration (reference: SolverDiffPhD._iterate, solver.py:582-659):
+//   P1 local step       elements -> contributions          (kernels.py:222-272, hex.py:122-169)
+//   P2 gather + rhs     particles: p, b = m/h^2 q~ + p       (kernels.py:75-91, hex.py:246-260, :275-284)
+//   P3 y = S b          S rows, nnz-balanced block ranges    (sparse.py:209-227)
+//   P4 x = S^T y        S^T rows + Dirichlet values + Anderson history and Gram partials
+//                       (sparse.py:341-348, kernels.py:287-291, anderson.py:306-354)
+//   serial              Anderson least squares in the last-arriving block (anderson.py:410-475)
+//   P5 Anderson apply + convergence partials                 (anderson.py:478-503, kernels.py:354-401)
+//   serial              dual convergence gate, loop decision
+// Only P1->P2, P2->P3, P3->P4, P4->P5 and P5->P1 cross blocks; particle rows
+// of P4/P5 are owned by one block, so history, previous iterate and previous
+// projection of a particle are only ever touched by that block.
+#pragma once
+
+#include "pd_device.cuh"
+
+namespace pdb200 {
+
+// Deformation gradient of a Tet4 element from float64 positions, as a TL matrix.
+template <typename TL>
+__device__ __forceinline__ void tet_deformation(const StepArgs& a, int e, const double* vec, M3<TL>& f) {
+  double m[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int v = a.indices[4 * e + k];
+    const double* g = a.gradients + (4 * e + k) * 3;
+    const double px = vec[3 * v], py = vec[3 * v + 1], pz = vec[3 * v + 2];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      m[0][c] += px * g[c];
+      m[1][c] += py * g[c];
+      m[2][c] += pz * g[c];
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) f.a[r][c] = static_cast<TL>(m[r][c]);
+}
+
+// Projection stress sum_energies w (P(F) - F_D) of one element sample.
+template <typename TL>
+__device__ __forceinline__ M3<TL> sample_stress(const StepArgs& a, int e, const M3<TL>& f, const M3<TL>& fd) {
+  M3<TL> stress = zero3<TL>();
+  const TL wc = static_cast<TL>(a.wc[e]);
+  const TL wv = static_cast<TL>(a.wv[e]);
+  const TL wn = static_cast<TL>(a.wn[e]);
+  if (wc != TL(0) || wv != TL(0) || wn != TL(0)) {
+    M3<TL> u, v;
+    V3<TL> sigma;
+    unsigned_svd(f, u, sigma, v);
+    if (wc != TL(0)) stress = stress + wc * (mul(u, transpose(v)) - fd);
+    if (wv != TL(0)) {
+      bool singular;
+      const V3<TL> offset = volume_offset(sigma, singular);
+      if (singular) atomicOr(a.status, kStatusSingular);
+      stress = stress + wv * (udvt(u, sigma + offset, v) - fd);
+    }
+    if (wn != TL(0)) {
+      const V3<TL> stretches =
+          nh_prox_stretches(sigma, static_cast<TL>(a.nh_mu), static_cast<TL>(a.nh_lame), static_cast<TL>(a.nh_penalty));
+      stress = stress + wn * (udvt(u, stretches, v) - fd);
+    }
+  }
+  if (a.has_muscles) {
+    const TL wm = static_cast<TL>(a.wm[e]);
+    if (wm != TL(0)) {
+      const V3<TL> m = load3<TL>(a.mdir, e);
+      const V3<TL> fibre = muscle_projection(f, m, static_cast<TL>(a.mtarget[e]));
+      stress = stress + wm * outer(fibre - mul(fd, m), m);
+    }
+  }
+  return stress;
+}
+
+// P1 for Tet4: one thread per element.
+template <typename TL>
+__device__ void local_step_tet(const StepArgs& a, int gtid, int gthreads) {
+  for (int e = gtid; e < a.ne; e += gthreads) {
+    M3<TL> f, fd;
+    tet_deformation<TL>(a, e, a.x, f);
+    tet_deformation<TL>(a, e, a.boundary, fd);
+    const M3<TL> stress = sample_stress<TL>(a, e, f, fd);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const double* g = a.gradients + (4 * e + k) * 3;
+      const V3<TL> gk = v3<TL>(static_cast<TL>(g[0]), static_cast<TL>(g[1]), static_cast<TL>(g[2]));
+      const V3<TL> c = mul(stress, gk);
+      double* out = a.contrib + (4 * e + k) * 3;
+      out[0] = static_cast<double>(c.x);
+      out[1] = static_cast<double>(c.y);
+      out[2] = static_cast<double>(c.z);
+    }
+  }
+}
+
+// P1 for Hex8: eight lanes per cell, one Gauss sample each; the per-corner
+// contributions sum_s stress_s g_sj are reduce-scattered across the eight
+// lanes with shuffles (fixed tree), so lane s ends with corner j = s.
+template <typename TL>
+__device__ void local_step_hex(const StepArgs& a, const double* grad_smem, int gtid, int gthreads) {
+  const int lane = threadIdx.x & 31;
+  const int s = lane & 7;
+  const int group_in_warp = lane >> 3;
+  const int warp_global = gtid >> 5;
+  const int warps_total = gthreads >> 5;
+  for (int base = warp_global * 4; base < a.ne; base += warps_total * 4) {
+    const int e = base + group_in_warp;
+    const bool valid = e < a.ne;
+    const int ec = valid ? e : a.ne - 1;
+    double fm[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    double fdm[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int v = a.indices[8 * ec + j];
+      const double* g = grad_smem + (8 * s + j) * 3;
+      const double px = a.x[3 * v], py = a.x[3 * v + 1], pz = a.x[3 * v + 2];
+      const double bx = a.boundary[3 * v], by = a.boundary[3 * v + 1], bz = a.boundary[3 * v + 2];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        fm[0][c] += px * g[c];
+        fm[1][c] += py * g[c];
+        fm[2][c] += pz * g[c];
+        fdm[0][c] += bx * g[c];
+        fdm[1][c] += by * g[c];
+        fdm[2][c] += bz * g[c];
+      }
+    }
+    M3<TL> f, fd;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        f.a[r][c] = static_cast<TL>(fm[r][c]);
+        fd.a[r][c] = static_cast<TL>(fdm[r][c]);
+      }
+    const M3<TL> stress = sample_stress<TL>(a, ec, f, fd);
+    // v[j] = stress_s g_sj for the eight corners.
+    double vx[8], vy[8], vz[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const double* g = grad_smem + (8 * s + j) * 3;
+      const V3<TL> c = mul(stress, v3<TL>(static_cast<TL>(g[0]), static_cast<TL>(g[1]), static_cast<TL>(g[2])));
+      vx[j] = static_cast<double>(c.x);
+      vy[j] = static_cast<double>(c.y);
+      vz[j] = static_cast<double>(c.z);
+    }
+    // Reduce-scatter over the eight sample lanes: masks 4, 2, 1.
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const bool upper = (s & 4) != 0;
+      const double sx = upper ? vx[t] : vx[4 + t];
+      const double sy = upper ? vy[t] : vy[4 + t];
+      const double sz = upper ? vz[t] : vz[4 + t];
+      const double rx = __shfl_xor_sync(0xffffffffu, sx, 4);
+      const double ry = __shfl_xor_sync(0xffffffffu, sy, 4);
+      const double rz = __shfl_xor_sync(0xffffffffu, sz, 4);
+      vx[t] = (upper ? vx[4 + t] : vx[t]) + rx;
+      vy[t] = (upper ? vy[4 + t] : vy[t]) + ry;
+      vz[t] = (upper ? vz[4 + t] : vz[t]) + rz;
+    }
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      const bool upper = (s & 2) != 0;
+      const double sx = upper ? vx[t] : vx[2 + t];
+      const double sy = upper ? vy[t] : vy[2 + t];
+      const double sz = upper ? vz[t] : vz[2 + t];
+      const double rx = __shfl_xor_sync(0xffffffffu, sx, 2);
+      const double ry = __shfl_xor_sync(0xffffffffu, sy, 2);
+      const double rz = __shfl_xor_sync(0xffffffffu, sz, 2);
+      vx[t] = (upper ? vx[2 + t] : vx[t]) + rx;
+      vy[t] = (upper ? vy[2 + t] : vy[t]) + ry;
+      vz[t] = (upper ? vz[2 + t] : vz[t]) + rz;
+    }
+    {
+      const bool upper = (s & 1) != 0;
+      const double sx = upper ? vx[0] : vx[1];
+      const double sy = upper ? vy[0] : vy[1];
+      const double sz = upper ? vz[0] : vz[1];
+      const double rx = __shfl_xor_sync(0xffffffffu, sx, 1);
+      const double ry = __shfl_xor_sync(0xffffffffu, sy, 1);
+      const double rz = __shfl_xor_sync(0xffffffffu, sz, 1);
+      vx[0] = (upper ? vx[1] : vx[0]) + rx;
+      vy[0] = (upper ? vy[1] : vy[0]) + ry;
+      vz[0] = (upper ? vz[1] : vz[0]) + rz;
+    }
+    if (valid) {
+      double* out = a.contrib + (8 * e + s) * 3;
+      out[0] = vx[0];
+      out[1] = vy[0];
+      out[2] = vz[0];
+    }
+  }
+}
+
+// Row-parallel CSR product out = M vec for rows [r0, r1) of this block,
+// one warp per row, lanes strided over the row, fixed shuffle tree.
+template <typename TV>
+__device__ __forceinline__ void spmv_rows(const int* off, const int* col, const TV* val, const double* vec, double* out,
+                                          int r0, int r1) {
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  for (int row = r0 + warp; row < r1; row += kWarps) {
+    const int begin = off[row];
+    const int end = off[row + 1];
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+#pragma unroll 4
+    for (int k = begin + lane; k < end; k += 32) {
+      const double value = static_cast<double>(val[k]);
+      const int c = col[k];
+      sx += value * vec[3 * c];
+      sy += value * vec[3 * c + 1];
+      sz += value * vec[3 * c + 2];
+    }
+    sx = warp_sum(sx);
+    sy = warp_sum(sy);
+    sz = warp_sum(sz);
+    if (lane == 0) {
+      out[3 * row] = sx;
+      out[3 * row + 1] = sy;
+      out[3 * row + 2] = sz;
+    }
+  }
+}
+
+// Anderson Gram entries for history state (count, start): entries
+// [0, count*(count+1)/2) are dG_a . dG_b (a <= b), then count entries dG_a . g.
+__device__ __forceinline__ int gram_entries(int count) { return count * (count + 1) / 2 + count; }
+
+__device__ __forceinline__ void gram_entry_pair(int entry, int count, int& a, int& b) {
+  // Enumerate (a, b) with a <= b row by row.
+  int k = entry;
+  a = 0;
+  while (k >= count - a) {
+    k -= count - a;
+    ++a;
+  }
+  b = a + k;
+}
+
+// Block partial of the Gram entries over this block's particle rows [r0, r1).
+inline __device__ void gram_partials(const StepArgs& a, int r0, int r1, int count, int start, double* block_out,
+                              double* scratch) {
+  const int entries = gram_entries(count);
+  const int capacity = a.window + 1;
+  const int groups = entries > 0 ? kBlock / entries : 0;
+  const int t = threadIdx.x;
+  double sum = 0.0;
+  if (entries > 0 && t < groups * entries) {
+    const int entry = t % entries;
+    const int group = t / entries;
+    const int pairs = count * (count + 1) / 2;
+    const size_t stride = static_cast<size_t>(3) * a.n;
+    if (entry < pairs) {
+      int ea, eb;
+      gram_entry_pair(entry, count, ea, eb);
+      const double* ga1 = a.hist_g + ((start + ea + 1) % capacity) * stride;
+      const double* ga0 = a.hist_g + ((start + ea) % capacity) * stride;
+      const double* gb1 = a.hist_g + ((start + eb + 1) % capacity) * stride;
+      const double* gb0 = a.hist_g + ((start + eb) % capacity) * stride;
+      for (int i = r0 + group; i < r1; i += groups) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const double da = ga1[3 * i + c] - ga0[3 * i + c];
+          const double db = gb1[3 * i + c] - gb0[3 * i + c];
+          sum += da * db;
+        }
+      }
+    } else {
+      const int ea = entry - pairs;
+      const double* ga1 = a.hist_g + ((start + ea + 1) % capacity) * stride;
+      const double* ga0 = a.hist_g + ((start + ea) % capacity) * stride;
+      const double* gn = a.hist_g + ((start + count) % capacity) * stride;
+      for (int i = r0 + group; i < r1; i += groups) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) sum += (ga1[3 * i + c] - ga0[3 * i + c]) * gn[3 * i + c];
+      }
+    }
+  }
+  scratch[t] = sum;
+  __syncthreads();
+  if (t < entries) {
+    double total = 0.0;
+    for (int g = 0; g < groups; ++g) total += scratch[g * entries + t];
+    block_out[t] = total;
+  }
+  __syncthreads();
+}
+
+// Eigen-style pivoted LDL^T solve of the leading n x n block (anderson.py:357-407).
+inline __device__ void aa_ldlt_solve(double m[kMaxWindow][kMaxWindow], const double* b, int n, double* x) {
+  int perm[kMaxWindow];
+  for (int i = 0; i < n; ++i) perm[i] = i;
+  for (int k = 0; k < n; ++k) {
+    int biggest = k;
+    for (int i = k + 1; i < n; ++i)
+      if (fabs(m[i][i]) > fabs(m[biggest][biggest])) biggest = i;
+    if (biggest != k) {
+      for (int j = 0; j < n; ++j) {
+        const double t = m[k][j];
+        m[k][j] = m[biggest][j];
+        m[biggest][j] = t;
+      }
+      for (int i = 0; i < n; ++i) {
+        const double t = m[i][k];
+        m[i][k] = m[i][biggest];
+        m[i][biggest] = t;
+      }
+      const int t = perm[k];
+      perm[k] = perm[biggest];
+      perm[biggest] = t;
+    }
+    for (int j = 0; j < k; ++j) m[k][k] = m[k][k] - m[k][j] * m[k][j] * m[j][j];
+    for (int i = k + 1; i < n; ++i) {
+      for (int j = 0; j < k; ++j) m[i][k] = m[i][k] - m[i][j] * m[j][j] * m[k][j];
+      if (m[k][k] != 0.0) m[i][k] = m[i][k] / m[k][k];
+    }
+  }
+  double y[kMaxWindow];
+  for (int i = 0; i < n; ++i) y[i] = b[perm[i]];
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < i; ++j) y[i] = y[i] - m[i][j] * y[j];
+  for (int i = 0; i < n; ++i) y[i] = fabs(m[i][i]) > DBL_MIN ? y[i] / m[i][i] : 0.0;
+  for (int r = 0; r < n; ++r) {
+    const int i = n - 1 - r;
+    for (int j = i + 1; j < n; ++j) y[i] = y[i] - m[j][i] * y[j];
+  }
+  for (int i = 0; i < n; ++i) x[perm[i]] = y[i];
+}
+
+// Serial Anderson step (one thread) from the reduced Gram entries (anderson.py:424-475).
+inline __device__ void aa_solve(int* state, double* gamma, int* accept, const double* reduced, int window) {
+  int count = state[0];
+  int start = state[1];
+  const int capacity = window + 1;
+  state[2] = count;
+  state[3] = start;
+  *accept = 0;
+  if (count >= 1) {
+    double gram[kMaxWindow][kMaxWindow];
+    double rhs[kMaxWindow];
+    const int pairs = count * (count + 1) / 2;
+    int entry = 0;
+    for (int i = 0; i < count; ++i)
+      for (int j = i; j < count; ++j) gram[i][j] = reduced[entry++];
+    for (int i = 0; i < count; ++i) rhs[i] = reduced[pairs + i];
+    double trace = 0.0;
+    for (int i = 0; i < count; ++i) {
+      trace += gram[i][i];
+      for (int j = i + 1; j < count; ++j) gram[j][i] = gram[i][j];
+    }
+    const double regularization = fmax(1.0e-6 * trace / static_cast<double>(count), 1.0e-12);
+    for (int i = 0; i < count; ++i) gram[i][i] = gram[i][i] + regularization;
+    double coefficients[kMaxWindow];
+    aa_ldlt_solve(gram, rhs, count, coefficients);
+    double norm = 0.0;
+    for (int i = 0; i < count; ++i) {
+      gamma[i] = coefficients[i];
+      norm += coefficients[i] * coefficients[i];
+    }
+    if (sqrt(norm) >= 10.0) {
+      count = 0;
+      start = 0;
+    } else {
+      *accept = 1;
+      count += 1;
+    }
+  } else {
+    count += 1;
+  }
+  while (count > window) {
+    start = (start + 1) % capacity;
+    count -= 1;
+  }
+  state[0] = count;
+  state[1] = start;
+}
+
+// Anderson-mixed value of particle i (anderson.py:478-503), given the history
+// before trimming (count_used, start_used) and the coefficients.
+__device__ __forceinline__ V3<double> aa_apply_row(const StepArgs& a, int i, int count, int start,
+                                                   const double* gamma) {
+  const int capacity = a.window + 1;
+  const size_t stride = static_cast<size_t>(3) * a.n;
+  const int slot = (start + count) % capacity;
+  V3<double> value;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) value[c] = a.hist_x[slot * stride + 3 * i + c] + a.hist_g[slot * stride + 3 * i + c];
+  for (int k = 0; k < count; ++k) {
+    const int low = (start + k) % capacity;
+    const int high = (start + k + 1) % capacity;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const size_t h = high * stride + 3 * i + c;
+      const size_t l = low * stride + 3 * i + c;
+      value[c] -= (a.hist_x[h] - a.hist_x[l] + a.hist_g[h] - a.hist_g[l]) * gamma[k];
+    }
+  }
+  return value;
+}
+
+}  // namespace pdb200

@@ -1,0 +1,333 @@
+// Persistent forward step kernel, its helpers and small utility kernels.
+#include <cuda_runtime.h>
+
+#include "pd_forward.cuh"
+#include "pd_kernels.h"
+
+namespace pdb200 {
+
+// One projective-dynamics step: prologue, every local/global iteration, epilogue.
+// TL: precision of the local projections; TV: precision of the factor values.
+template <typename TL, typename TV>
+__global__ void __launch_bounds__(kBlock) forward_step_kernel(const StepArgs a) {
+  __shared__ double s_grad[8 * 8 * 3];
+  __shared__ double s_scratch[kBlock];
+  __shared__ double s_reduced[64];
+  __shared__ int s_control[8];
+  const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int gthreads = gridDim.x * blockDim.x;
+  const int n = a.n;
+  if (a.hex) {
+    for (int t = threadIdx.x; t < 8 * 8 * 3; t += blockDim.x) s_grad[t] = a.gradients[t];
+  }
+  // ---- Prologue: begin_step (kernels.py:155-190), explicit_boundary (:199-207),
+  // read_activations (:136-152), begin_solve, Anderson reset.
+  const double dt = a.dt;
+  for (int i = gtid; i < n; i += gthreads) {
+    const V3<double> start = v3<double>(a.q_in[3 * i], a.q_in[3 * i + 1], a.q_in[3 * i + 2]);
+    const V3<double> velocity = v3<double>(a.qd_in[3 * i], a.qd_in[3 * i + 1], a.qd_in[3 * i + 2]);
+    store3(a.position, i, start);
+    store3(a.velocity, i, velocity);
+    V3<double> acceleration;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) acceleration[c] = static_cast<double>(a.f_in[3 * i + c]) / a.mass + a.gravity[c];
+    V3<double> target;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) target[c] = start[c] + dt * velocity[c] + dt * dt * acceleration[c];
+    store3(a.target, i, target);
+    V3<double> boundary = v3<double>(0.0, 0.0, 0.0);
+    if (a.free_[i] == 0) {
+      if (a.dirichlet != nullptr) {
+        boundary = v3<double>(a.dirichlet[3 * i], a.dirichlet[3 * i + 1], a.dirichlet[3 * i + 2]);
+      } else {
+        boundary = start;
+        if (a.integrate_pinned) boundary = boundary + dt * velocity;
+      }
+    }
+    store3(a.boundary, i, boundary);
+    store3(a.x, i, start);
+    store3(a.prev, i, start);
+    store3(a.proj, i, v3<double>(0.0, 0.0, 0.0));
+    store3(a.prev_proj, i, v3<double>(0.0, 0.0, 0.0));
+  }
+  if (a.activations != nullptr) {
+    for (int e = gtid; e < a.ne; e += gthreads) {
+      const double contraction = static_cast<double>(a.activations[e]);
+      if (!isfinite(contraction) || contraction > 1.0 || (a.wm[e] == 0.0 && contraction != 0.0)) {
+        atomicOr(a.status, kStatusActivation);
+      }
+      a.mtarget[e] = 1.0 - contraction;
+    }
+  }
+  if (gtid == 0) {
+    a.aa_state[0] = a.aa_state[1] = a.aa_state[2] = a.aa_state[3] = 0;
+    *a.aa_accept = 0;
+    *a.iteration = 0;
+    *a.active = 1;
+  }
+  if (!grid_sync(a.barrier, a.status)) return;
+
+  const int s_r0 = a.s_part[blockIdx.x], s_r1 = a.s_part[blockIdx.x + 1];
+  const int r0 = a.st_part[blockIdx.x], r1 = a.st_part[blockIdx.x + 1];
+  double* my_partials = a.partials + static_cast<size_t>(blockIdx.x) * kPartialStride;
+  const size_t hstride = static_cast<size_t>(3) * n;
+
+  for (;;) {
+    // ---- P1: local step.
+    if (a.hex) {
+      local_step_hex<TL>(a, s_grad, gtid, gthreads);
+    } else {
+      local_step_tet<TL>(a, gtid, gthreads);
+    }
+    if (!grid_sync(a.barrier, a.status)) return;
+
+    // ---- P2: fixed-order gather, vertex-plane energies, right-hand side.
+    for (int i = gtid; i < n; i += gthreads) {
+      double px = 0.0, py = 0.0, pz = 0.0;
+      for (int k = a.inc_offsets[i]; k < a.inc_offsets[i + 1]; ++k) {
+        const double* c = a.contrib + 3 * a.inc_entries[k];
+        px += c[0];
+        py += c[1];
+        pz += c[2];
+      }
+      if (a.plane_weight != nullptr) {
+        const double w = a.plane_weight[i];
+        if (w != 0.0) {
+          const double nx = a.plane[0], ny = a.plane[1], nz = a.plane[2];
+          const double xx = a.x[3 * i], xy = a.x[3 * i + 1], xz = a.x[3 * i + 2];
+          const double d = nx * xx + ny * xy + nz * xz + a.plane[3];
+          const double m = fmin(0.0, d);
+          px += w * ((xx - m * nx) - a.boundary[3 * i]);
+          py += w * ((xy - m * ny) - a.boundary[3 * i + 1]);
+          pz += w * ((xz - m * nz) - a.boundary[3 * i + 2]);
+        }
+      }
+      a.proj[3 * i] = px;
+      a.proj[3 * i + 1] = py;
+      a.proj[3 * i + 2] = pz;
+      double bx = a.inertia * a.target[3 * i] + px;
+      double by = a.inertia * a.target[3 * i + 1] + py;
+      double bz = a.inertia * a.target[3 * i + 2] + pz;
+      if (a.refine) {
+        // Residual of the linear system at the current iterate, in float64.
+        for (int k = a.a_off[i]; k < a.a_off[i + 1]; ++k) {
+          const double v = a.a_val[k];
+          const int j = a.a_col[k];
+          bx -= v * a.prev[3 * j];
+          by -= v * a.prev[3 * j + 1];
+          bz -= v * a.prev[3 * j + 2];
+        }
+      }
+      a.rhs[3 * i] = bx;
+      a.rhs[3 * i + 1] = by;
+      a.rhs[3 * i + 2] = bz;
+    }
+    if (!grid_sync(a.barrier, a.status)) return;
+
+    // ---- P3: y = S b.
+    if (sizeof(TV) == sizeof(double)) {
+      spmv_rows<double>(a.s_off, a.s_col, a.s_val, a.rhs, a.y, s_r0, s_r1);
+    } else {
+      spmv_rows<float>(a.s_off, a.s_col, a.s_val32, a.rhs, a.y, s_r0, s_r1);
+    }
+    if (!grid_sync(a.barrier, a.status)) return;
+
+    // ---- P4: x = S^T y, Dirichlet values, Anderson history and Gram partials.
+    if (sizeof(TV) == sizeof(double)) {
+      spmv_rows<double>(a.st_off, a.st_col, a.st_val, a.y, a.x, r0, r1);
+    } else {
+      spmv_rows<float>(a.st_off, a.st_col, a.st_val32, a.y, a.x, r0, r1);
+    }
+    __syncthreads();
+    const int count = a.window > 0 ? a.aa_state[0] : 0;
+    const int start = a.window > 0 ? a.aa_state[1] : 0;
+    const int capacity = a.window + 1;
+    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+      V3<double> value = load3d(a.x, i);
+      if (a.refine) value = value + load3d(a.prev, i);
+      if (a.free_[i] == 0) value = load3d(a.boundary, i);
+      store3(a.x, i, value);
+      if (a.window > 0) {
+        const int slot = (start + count) % capacity;
+        const V3<double> previous = load3d(a.prev, i);
+        double* hx = a.hist_x + slot * hstride + 3 * i;
+        double* hg = a.hist_g + slot * hstride + 3 * i;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          hx[c] = previous[c];
+          hg[c] = value[c] - previous[c];
+        }
+      }
+    }
+    if (a.window > 0) {
+      __syncthreads();
+      gram_partials(a, r0, r1, count, start, my_partials, s_scratch);
+      unsigned generation;
+      if (barrier_arrive(a.barrier, generation)) {
+        const int entries = gram_entries(count);
+        reduce_partials(a.partials, 0, entries, gridDim.x, s_reduced, s_scratch);
+        if (threadIdx.x == 0) aa_solve(a.aa_state, a.aa_gamma, a.aa_accept, s_reduced, a.window);
+        barrier_release(a.barrier, generation);
+        __syncthreads();
+      } else if (!barrier_wait(a.barrier, generation, a.status)) {
+        return;
+      }
+    }
+
+    // ---- P5: Anderson apply, Dirichlet re-imposition, convergence partials.
+    {
+      int accept = 0, used_count = 0, used_start = 0;
+      if (a.window > 0) {
+        accept = *reinterpret_cast<volatile int*>(a.aa_accept);
+        used_count = a.aa_state[2];
+        used_start = a.aa_state[3];
+        if (threadIdx.x < kMaxWindow) s_reduced[32 + threadIdx.x] = a.aa_gamma[threadIdx.x];
+        __syncthreads();
+      }
+      double step2 = 0.0, prev2 = 0.0, change2 = 0.0, proj2 = 0.0;
+      for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+        V3<double> value = load3d(a.x, i);
+        if (accept) value = aa_apply_row(a, i, used_count, used_start, s_reduced + 32);
+        if (a.free_[i] == 0) value = load3d(a.boundary, i);
+        store3(a.x, i, value);
+        const V3<double> previous = load3d(a.prev, i);
+        const V3<double> p = load3d(a.proj, i);
+        const V3<double> pp = load3d(a.prev_proj, i);
+        const V3<double> step = value - previous;
+        const V3<double> change = p - pp;
+        step2 += dot(step, step);
+        prev2 += dot(previous, previous);
+        change2 += dot(change, change);
+        proj2 += dot(pp, pp);
+        store3(a.prev, i, value);
+        store3(a.prev_proj, i, p);
+      }
+      step2 = block_sum(step2, s_scratch);
+      prev2 = block_sum(prev2, s_scratch);
+      change2 = block_sum(change2, s_scratch);
+      proj2 = block_sum(proj2, s_scratch);
+      if (threadIdx.x == 0) {
+        my_partials[48] = step2;
+        my_partials[49] = prev2;
+        my_partials[50] = change2;
+        my_partials[51] = proj2;
+      }
+      unsigned generation;
+      if (barrier_arrive(a.barrier, generation)) {
+        reduce_partials(a.partials, 48, 4, gridDim.x, s_reduced, s_scratch);
+        if (threadIdx.x == 0) {
+          const double step_norm = sqrt(s_reduced[0]);
+          const double previous_norm = sqrt(s_reduced[1]);
+          const double change_norm = sqrt(s_reduced[2]);
+          const double projection_norm = sqrt(s_reduced[3]);
+          const int k = *a.iteration;
+          *a.iteration = k + 1;
+          if (k > 0 && step_norm <= a.rel_tol * previous_norm + a.abs_tol &&
+              change_norm <= a.rel_tol * projection_norm + a.abs_tol) {
+            *a.active = 0;
+          } else if (k + 1 >= a.max_iterations) {
+            *a.active = 0;
+            atomicOr(a.status, kStatusNotConverged);
+          } else {
+            *a.active = 1;
+          }
+        }
+        barrier_release(a.barrier, generation);
+        __syncthreads();
+      } else if (!barrier_wait(a.barrier, generation, a.status)) {
+        return;
+      }
+      if (threadIdx.x == 0) s_control[0] = *reinterpret_cast<volatile int*>(a.active);
+      __syncthreads();
+      if (s_control[0] == 0) break;
+    }
+  }
+
+  // ---- Epilogue: write_state (kernels.py:404-414) and the step record.
+  for (int i = gtid; i < n; i += gthreads) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const double value = a.x[3 * i + c];
+      a.q_out[3 * i + c] = static_cast<float>(value);
+      a.qd_out[3 * i + c] = static_cast<float>((value - a.position[3 * i + c]) / dt);
+      if (a.x_record != nullptr) a.x_record[3 * i + c] = value;
+    }
+  }
+}
+
+// Plain out = S^T (S rhs) with separate launches (SparseInverse.apply).
+template <typename TV>
+__global__ void __launch_bounds__(kBlock) spmv_kernel(const int* off, const int* col, const TV* val, const double* vec,
+                                                      double* out, int rows) {
+  const int warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const int warps_total = (gridDim.x * blockDim.x) >> 5;
+  for (int row = warp_global; row < rows; row += warps_total) {
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    for (int k = off[row] + lane; k < off[row + 1]; k += 32) {
+      const double value = static_cast<double>(val[k]);
+      const int c = col[k];
+      sx += value * vec[3 * c];
+      sy += value * vec[3 * c + 1];
+      sz += value * vec[3 * c + 2];
+    }
+    sx = warp_sum(sx);
+    sy = warp_sum(sy);
+    sz = warp_sum(sz);
+    if (lane == 0) {
+      out[3 * row] = sx;
+      out[3 * row + 1] = sy;
+      out[3 * row + 2] = sz;
+    }
+  }
+}
+
+__global__ void hex_determinants_kernel(const float* q, const int* indices, const double* gradients, int ne,
+                                        double* out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ne * 8) return;
+  const int e = t / 8;
+  const int s = t % 8;
+  M3<double> f = zero3<double>();
+  for (int j = 0; j < 8; ++j) {
+    const int v = indices[8 * e + j];
+    const double* g = gradients + (8 * s + j) * 3;
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) f.a[r][c] += static_cast<double>(q[3 * v + r]) * g[c];
+  }
+  out[t] = determinant(f);
+}
+
+// ---------------------------------------------------------------------------
+// Host launchers.
+
+cudaError_t launch_forward_step(const StepArgs& args, int blocks, int precision, cudaStream_t stream) {
+  void* params[] = {const_cast<StepArgs*>(&args)};
+  const void* kernel = precision == 0 ? reinterpret_cast<const void*>(&forward_step_kernel<double, double>)
+                                      : reinterpret_cast<const void*>(&forward_step_kernel<float, float>);
+  return cudaLaunchCooperativeKernel(kernel, dim3(blocks), dim3(kBlock), params, 0, stream);
+}
+
+cudaError_t forward_step_max_blocks(int precision, int* blocks_per_sm) {
+  const void* kernel = precision == 0 ? reinterpret_cast<const void*>(&forward_step_kernel<double, double>)
+                                      : reinterpret_cast<const void*>(&forward_step_kernel<float, float>);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kernel, kBlock, 0);
+}
+
+cudaError_t launch_apply_inverse(const int* s_off, const int* s_col, const double* s_val, const int* st_off,
+                                 const int* st_col, const double* st_val, int rows, const double* rhs, double* work,
+                                 double* out, cudaStream_t stream) {
+  const int blocks = (rows * 32 + kBlock - 1) / kBlock;
+  spmv_kernel<double><<<blocks, kBlock, 0, stream>>>(s_off, s_col, s_val, rhs, work, rows);
+  spmv_kernel<double><<<blocks, kBlock, 0, stream>>>(st_off, st_col, st_val, work, out, rows);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_hex_determinants(const float* q, const int* indices, const double* gradients, int ne, double* out,
+                                    cudaStream_t stream) {
+  const int threads = ne * 8;
+  hex_determinants_kernel<<<(threads + 255) / 256, 256, 0, stream>>>(q, indices, gradients, ne, out);
+  return cudaGetLastError();
+}
+
+}  // namespace pdb200

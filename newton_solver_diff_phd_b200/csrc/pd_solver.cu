@@ -1,0 +1,880 @@
+// Host side of the B200 DiffPhD solver: the C ABI declared in include/pd_b200.h.
+//
+// The solver object owns every device buffer of one instance. pd_build mirrors
+// SolverDiffPhD._build (src/newton_solver_diff_phd/_src/solvers/diff_phd/solver.py:491-552):
+// element weights, assembly of the constant matrix in the reference's
+// accumulation order, the host inverse factor, then the upload. pd_step and
+// pd_backward fill the argument blocks and launch one cooperative kernel each.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <functional>
+#include <string>
+#include <vector>
+
+#include "../../include/pd_b200.h"
+#include "factor.h"
+#include "pd_kernels.h"
+
+using pdb200::AdjointArgs;
+using pdb200::InverseFactor;
+using pdb200::StepArgs;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& message) {
+  g_last_error = message;
+  return code;
+}
+
+#define PD_CUDA(call)                                                                                 \
+  do {                                                                                                \
+    cudaError_t pd_status_ = (call);                                                                  \
+    if (pd_status_ != cudaSuccess) {                                                                  \
+      return fail(PD_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(pd_status_));           \
+    }                                                                                                 \
+  } while (0)
+
+// Owned device allocation.
+struct DeviceBuffer {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  DeviceBuffer() = default;
+  DeviceBuffer(const DeviceBuffer&) = delete;
+  DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+  ~DeviceBuffer() { release(); }
+  void release() {
+    if (ptr != nullptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+  }
+  cudaError_t allocate(size_t size) {
+    release();
+    if (size == 0) size = 16;
+    bytes = size;
+    cudaError_t status = cudaMalloc(&ptr, size);
+    if (status != cudaSuccess) {
+      ptr = nullptr;
+      bytes = 0;
+      return status;
+    }
+    return cudaMemset(ptr, 0, size);
+  }
+  template <typename T>
+  cudaError_t upload(const std::vector<T>& host) {
+    cudaError_t status = allocate(host.size() * sizeof(T));
+    if (status != cudaSuccess || host.empty()) return status;
+    return cudaMemcpy(ptr, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice);
+  }
+  template <typename T>
+  T* as() const {
+    return static_cast<T*>(ptr);
+  }
+};
+
+// Contiguous row ranges with balanced cost (nnz + per-row overhead) per block.
+std::vector<int32_t> partition_rows(const std::vector<int32_t>& offsets, int blocks) {
+  const int rows = static_cast<int>(offsets.size()) - 1;
+  std::vector<int32_t> bounds(blocks + 1, rows);
+  bounds[0] = 0;
+  const double overhead = 16.0;
+  const double total = static_cast<double>(offsets[rows]) + overhead * rows;
+  int b = 1;
+  double cumulative = 0.0;
+  for (int r = 0; r < rows && b < blocks; ++r) {
+    cumulative += static_cast<double>(offsets[r + 1] - offsets[r]) + overhead;
+    while (b < blocks && cumulative >= total * b / blocks) {
+      bounds[b] = r + 1;
+      ++b;
+    }
+  }
+  for (; b < blocks; ++b) bounds[b] = rows;
+  return bounds;
+}
+
+}  // namespace
+
+struct PdSolver {
+  int device = 0;
+  int n = 0, ne = 0, corners = 0, hex = 0;
+  double mean_volume = 0.0;
+  PdOptions options{};
+  std::vector<int32_t> indices;
+  std::vector<double> gradients;
+  std::vector<int32_t> free_;
+  bool has_dirichlet = false;
+  // Materials and energies (host copies).
+  std::vector<double> mu, lame;
+  bool materials_set = false;
+  std::vector<double> muscle_dir, muscle_stiffness;
+  bool has_muscles = false;
+  std::vector<double> muscle_targets;
+  const float* activations = nullptr;
+  std::vector<int32_t> plane_vertices;
+  std::vector<double> plane_stiffness;
+  double plane[4] = {0, 0, 0, 0};
+  // Build state.
+  bool built = false;
+  bool stale = true;
+  double built_dt = 0.0;
+  double inertia = 0.0, mass = 0.0;
+  double nh_mu = 0.0, nh_lame = 0.0, nh_penalty = 0.0;
+  int blocks = 0;
+  int max_blocks = 0;
+  InverseFactor factor;
+  // Device mesh data.
+  DeviceBuffer d_indices, d_gradients, d_free, d_inc_offsets, d_inc_entries, d_plane_weight;
+  DeviceBuffer d_wc, d_wv, d_wn, d_wm, d_mdir, d_mtarget;
+  DeviceBuffer d_s_off, d_s_col, d_s_val, d_s_val32, d_st_off, d_st_col, d_st_val, d_st_val32, d_s_part, d_st_part;
+  DeviceBuffer d_a_off, d_a_col, d_a_val;
+  // Step vectors.
+  DeviceBuffer d_position, d_velocity, d_target, d_boundary, d_x, d_prev, d_proj, d_prev_proj, d_rhs, d_y, d_contrib;
+  DeviceBuffer d_hist_x, d_hist_g, d_aa_state, d_aa_gamma, d_aa_accept, d_partials;
+  DeviceBuffer d_iteration, d_active, d_status, d_barrier;
+  // Adjoint vectors.
+  DeviceBuffer b_rhs, b_base, b_solution, b_prev, b_work, b_y, b_raw, b_contrib, b_jac, b_hist_x, b_hist_g, b_aa_state,
+      b_aa_gamma, b_aa_accept, b_partials, b_iteration, b_active, b_control_d, b_control_i, b_material_scratch,
+      b_activation_scratch, b_zero_gq, b_zero_gqd, b_scratch_gq, b_scratch_gqd, b_scratch_gf;
+};
+
+namespace {
+
+int validate_options(const PdOptions& o) {
+  if (o.material != PD_MATERIAL_PD && o.material != PD_MATERIAL_NEO_HOOKEAN)
+    return fail(PD_ERR_INVALID, "material must be 'pd' or 'neo_hookean'");
+  if (!(o.density > 0.0) || !std::isfinite(o.density)) return fail(PD_ERR_INVALID, "density must be finite and positive");
+  if (!(o.abs_tol >= 0.0) || !std::isfinite(o.abs_tol)) return fail(PD_ERR_INVALID, "abs_tol must be finite and nonnegative");
+  if (!(o.rel_tol >= 0.0) || !std::isfinite(o.rel_tol)) return fail(PD_ERR_INVALID, "rel_tol must be finite and nonnegative");
+  if (o.max_iterations < 1) return fail(PD_ERR_INVALID, "max_iterations must be a positive integer");
+  if (o.anderson_window < 0 || o.anderson_window > pdb200::kMaxWindow)
+    return fail(PD_ERR_INVALID, "anderson_window must be an integer in [0, 8]");
+  if (o.precision != PD_PRECISION_FP64 && o.precision != PD_PRECISION_FP32_REFINE)
+    return fail(PD_ERR_INVALID, "precision must be fp64 or fp32+refine");
+  if (o.adjoint_mode != PD_ADJOINT_REFERENCE && o.adjoint_mode != PD_ADJOINT_EXACT)
+    return fail(PD_ERR_INVALID, "adjoint mode must be reference or exact");
+  if (o.blocks < 0) return fail(PD_ERR_INVALID, "blocks must be nonnegative");
+  return PD_OK;
+}
+
+int samples_of(const PdSolver* s) { return s->hex ? 8 : 1; }
+double sample_volume_of(const PdSolver* s) { return s->mean_volume / static_cast<double>(samples_of(s)); }
+
+// Per-sample gradient rows of element e, sample q.
+const double* sample_rows(const PdSolver* s, int e, int q) {
+  return s->hex ? s->gradients.data() + 8 * 3 * q : s->gradients.data() + 12 * e;
+}
+
+int ensure_adjoint_buffers(PdSolver* s) {
+  const size_t vec = static_cast<size_t>(3) * s->n * sizeof(double);
+  if (s->b_rhs.ptr != nullptr) return PD_OK;
+  for (DeviceBuffer* buffer : {&s->b_rhs, &s->b_base, &s->b_solution, &s->b_prev, &s->b_work, &s->b_y, &s->b_raw})
+    PD_CUDA(buffer->allocate(vec));
+  PD_CUDA(s->b_contrib.allocate(static_cast<size_t>(s->ne) * s->corners * 3 * sizeof(double)));
+  const size_t jac_entries = static_cast<size_t>(s->ne) * samples_of(s) * 81;
+  PD_CUDA(s->b_jac.allocate(jac_entries * (s->options.precision == PD_PRECISION_FP64 ? sizeof(double) : sizeof(float))));
+  const size_t window = static_cast<size_t>(s->options.anderson_window);
+  PD_CUDA(s->b_hist_x.allocate((window + 1) * vec));
+  PD_CUDA(s->b_hist_g.allocate((window + 1) * vec));
+  PD_CUDA(s->b_aa_state.allocate(8 * sizeof(int)));
+  PD_CUDA(s->b_aa_gamma.allocate(pdb200::kMaxWindow * sizeof(double)));
+  PD_CUDA(s->b_aa_accept.allocate(sizeof(int)));
+  PD_CUDA(s->b_iteration.allocate(sizeof(int)));
+  PD_CUDA(s->b_active.allocate(sizeof(int)));
+  PD_CUDA(s->b_control_d.allocate(8 * sizeof(double)));
+  PD_CUDA(s->b_control_i.allocate(8 * sizeof(int)));
+  PD_CUDA(s->b_material_scratch.allocate(static_cast<size_t>(s->ne) * 2 * sizeof(double)));
+  PD_CUDA(s->b_activation_scratch.allocate(static_cast<size_t>(s->ne) * sizeof(double)));
+  const size_t fvec = static_cast<size_t>(3) * s->n * sizeof(float);
+  for (DeviceBuffer* buffer : {&s->b_zero_gq, &s->b_zero_gqd, &s->b_scratch_gq, &s->b_scratch_gqd, &s->b_scratch_gf})
+    PD_CUDA(buffer->allocate(fvec));
+  return PD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* pd_version(void) { return "newton-solver-diff-phd-b200 0.1 (sm_100a)"; }
+
+const char* pd_last_error(void) { return g_last_error.c_str(); }
+
+int pd_create(const PdMeshDesc* mesh, const PdOptions* options, int device, PdSolver** out) {
+  if (mesh == nullptr || options == nullptr || out == nullptr) return fail(PD_ERR_INVALID, "null argument");
+  *out = nullptr;
+  if (int status = validate_options(*options)) return status;
+  if (mesh->corners != 4 && mesh->corners != 8) return fail(PD_ERR_INVALID, "corners must be 4 (Tet4) or 8 (Hex8)");
+  if (mesh->n_vertices <= 0 || mesh->n_elements <= 0)
+    return fail(PD_ERR_INVALID, "SolverDiffPhD requires tetrahedral soft bodies or an explicit hex_mesh");
+  if (mesh->indices == nullptr || mesh->gradients == nullptr || mesh->free == nullptr)
+    return fail(PD_ERR_INVALID, "mesh arrays must not be null");
+  if (!(mesh->mean_volume > 0.0) || !std::isfinite(mesh->mean_volume))
+    return fail(PD_ERR_INVALID, "mean element volume must be finite and positive");
+  auto solver = new PdSolver();
+  solver->device = device;
+  solver->n = mesh->n_vertices;
+  solver->ne = mesh->n_elements;
+  solver->corners = mesh->corners;
+  solver->hex = mesh->corners == 8 ? 1 : 0;
+  solver->mean_volume = mesh->mean_volume;
+  solver->options = *options;
+  const size_t index_count = static_cast<size_t>(solver->ne) * solver->corners;
+  solver->indices.assign(mesh->indices, mesh->indices + index_count);
+  for (int32_t v : solver->indices) {
+    if (v < 0 || v >= solver->n) {
+      delete solver;
+      return fail(PD_ERR_INVALID, "element indices must reference existing particles");
+    }
+  }
+  const size_t gradient_count = solver->hex ? 8 * 8 * 3 : static_cast<size_t>(solver->ne) * 12;
+  solver->gradients.assign(mesh->gradients, mesh->gradients + gradient_count);
+  solver->free_.resize(solver->n);
+  bool any_free = false;
+  for (int i = 0; i < solver->n; ++i) {
+    solver->free_[i] = mesh->free[i] != 0 ? 1 : 0;
+    any_free = any_free || solver->free_[i];
+    solver->has_dirichlet = solver->has_dirichlet || !solver->free_[i];
+  }
+  if (!any_free) {
+    delete solver;
+    return fail(PD_ERR_INVALID, "SolverDiffPhD needs at least one dynamic particle");
+  }
+  solver->muscle_targets.assign(solver->ne, 1.0);
+  cudaError_t status = cudaSetDevice(device);
+  if (status != cudaSuccess) {
+    delete solver;
+    return fail(PD_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(status));
+  }
+  // Incidence lists sorted by element (kernels.py:61-72, hex.py:83-92). Hex8
+  // contributions are pre-summed over the eight samples of a cell.
+  std::vector<int32_t> counts(solver->n + 1, 0);
+  for (int32_t v : solver->indices) counts[v + 1] += 1;
+  for (int i = 0; i < solver->n; ++i) counts[i + 1] += counts[i];
+  std::vector<int32_t> entries(index_count);
+  {
+    std::vector<int32_t> cursor(counts.begin(), counts.end() - 1);
+    for (size_t k = 0; k < index_count; ++k) entries[cursor[solver->indices[k]]++] = static_cast<int32_t>(k);
+  }
+  int rc = PD_OK;
+  auto check = [&](cudaError_t e, const char* what) {
+    if (e != cudaSuccess && rc == PD_OK) rc = fail(PD_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  };
+  check(solver->d_indices.upload(solver->indices), "indices");
+  check(solver->d_gradients.upload(solver->gradients), "gradients");
+  check(solver->d_free.upload(solver->free_), "free");
+  check(solver->d_inc_offsets.upload(counts), "incidence");
+  check(solver->d_inc_entries.upload(entries), "incidence");
+  const size_t vec = static_cast<size_t>(3) * solver->n * sizeof(double);
+  for (DeviceBuffer* buffer : {&solver->d_position, &solver->d_velocity, &solver->d_target, &solver->d_boundary,
+                               &solver->d_x, &solver->d_prev, &solver->d_proj, &solver->d_prev_proj, &solver->d_rhs,
+                               &solver->d_y})
+    check(buffer->allocate(vec), "vectors");
+  check(solver->d_contrib.allocate(index_count * 3 * sizeof(double)), "contributions");
+  const size_t window = static_cast<size_t>(options->anderson_window);
+  check(solver->d_hist_x.allocate((window + 1) * vec), "history");
+  check(solver->d_hist_g.allocate((window + 1) * vec), "history");
+  check(solver->d_aa_state.allocate(8 * sizeof(int)), "anderson");
+  check(solver->d_aa_gamma.allocate(pdb200::kMaxWindow * sizeof(double)), "anderson");
+  check(solver->d_aa_accept.allocate(sizeof(int)), "anderson");
+  check(solver->d_iteration.allocate(sizeof(int)), "iteration");
+  check(solver->d_active.allocate(sizeof(int)), "active");
+  check(solver->d_status.allocate(sizeof(int)), "status");
+  check(solver->d_barrier.allocate(sizeof(pdb200::GridBarrier)), "barrier");
+  check(solver->d_mtarget.upload(solver->muscle_targets), "muscle targets");
+  std::vector<double> zeros(solver->ne, 0.0);
+  check(solver->d_wm.upload(zeros), "muscles");
+  std::vector<double> zeros3(static_cast<size_t>(solver->ne) * 3, 0.0);
+  check(solver->d_mdir.upload(zeros3), "muscles");
+  if (rc != PD_OK) {
+    delete solver;
+    return rc;
+  }
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  int per_sm_forward = 0, per_sm_adjoint = 0;
+  pdb200::forward_step_max_blocks(options->precision, &per_sm_forward);
+  pdb200::adjoint_step_max_blocks(options->precision, &per_sm_adjoint);
+  solver->max_blocks = sms * std::max(1, std::min(per_sm_forward, per_sm_adjoint));
+  *out = solver;
+  return PD_OK;
+}
+
+int pd_destroy(PdSolver* solver) {
+  if (solver == nullptr) return PD_OK;
+  cudaSetDevice(solver->device);
+  delete solver;
+  return PD_OK;
+}
+
+int pd_set_tolerances(PdSolver* solver, int32_t max_iterations, double abs_tol, double rel_tol) {
+  if (solver == nullptr) return fail(PD_ERR_INVALID, "null solver");
+  PdOptions o = solver->options;
+  o.max_iterations = max_iterations;
+  o.abs_tol = abs_tol;
+  o.rel_tol = rel_tol;
+  if (int status = validate_options(o)) return status;
+  solver->options = o;
+  return PD_OK;
+}
+
+int pd_set_materials(PdSolver* solver, const double* mu_lambda) {
+  if (solver == nullptr || mu_lambda == nullptr) return fail(PD_ERR_INVALID, "null argument");
+  solver->mu.resize(solver->ne);
+  solver->lame.resize(solver->ne);
+  for (int e = 0; e < solver->ne; ++e) {
+    solver->mu[e] = mu_lambda[2 * e];
+    solver->lame[e] = mu_lambda[2 * e + 1];
+  }
+  solver->materials_set = true;
+  solver->stale = true;
+  return PD_OK;
+}
+
+int pd_set_muscles(PdSolver* solver, const double* directions, const double* stiffness) {
+  if (solver == nullptr) return fail(PD_ERR_INVALID, "null solver");
+  if ((directions == nullptr) != (stiffness == nullptr))
+    return fail(PD_ERR_INVALID, "muscle_directions and muscle_stiffness must be supplied together");
+  solver->has_muscles = false;
+  solver->muscle_dir.assign(static_cast<size_t>(solver->ne) * 3, 0.0);
+  solver->muscle_stiffness.assign(solver->ne, 0.0);
+  if (directions != nullptr) {
+    for (int e = 0; e < solver->ne; ++e) {
+      const double s = stiffness[e];
+      if (!std::isfinite(s) || s < 0.0) return fail(PD_ERR_INVALID, "Muscle directions and stiffness must be finite, with nonnegative stiffness");
+      solver->muscle_stiffness[e] = s;
+      for (int c = 0; c < 3; ++c) solver->muscle_dir[3 * e + c] = s > 0.0 ? directions[3 * e + c] : 0.0;
+      solver->has_muscles = solver->has_muscles || s > 0.0;
+    }
+  }
+  std::vector<double> weight(solver->ne);
+  const double volume = sample_volume_of(solver);
+  for (int e = 0; e < solver->ne; ++e) weight[e] = solver->muscle_stiffness[e] * volume;
+  PD_CUDA(solver->d_wm.upload(weight));
+  PD_CUDA(solver->d_mdir.upload(solver->muscle_dir));
+  solver->stale = true;
+  return PD_OK;
+}
+
+int pd_set_muscle_targets(PdSolver* solver, const double* targets) {
+  if (solver == nullptr || targets == nullptr) return fail(PD_ERR_INVALID, "null argument");
+  for (int e = 0; e < solver->ne; ++e) {
+    if (!std::isfinite(targets[e]) || targets[e] < 0.0)
+      return fail(PD_ERR_INVALID, "muscle_targets must be finite nonnegative native target lengths");
+  }
+  solver->muscle_targets.assign(targets, targets + solver->ne);
+  PD_CUDA(solver->d_mtarget.upload(solver->muscle_targets));
+  return PD_OK;
+}
+
+int pd_set_activations(PdSolver* solver, const float* device_contractions) {
+  if (solver == nullptr) return fail(PD_ERR_INVALID, "null solver");
+  if (solver->hex && device_contractions != nullptr)
+    return fail(PD_ERR_INVALID, "Hex8 uses solver.muscle_targets; tet_activations cannot control Hex8 fibres");
+  solver->activations = device_contractions;
+  return PD_OK;
+}
+
+int pd_set_planar_energies(PdSolver* solver, int32_t count, const int32_t* vertices, const double* stiffness,
+                           const double plane[4]) {
+  if (solver == nullptr) return fail(PD_ERR_INVALID, "null solver");
+  solver->plane_vertices.clear();
+  solver->plane_stiffness.clear();
+  if (count > 0) {
+    if (vertices == nullptr || stiffness == nullptr || plane == nullptr) return fail(PD_ERR_INVALID, "null argument");
+    for (int k = 0; k < count; ++k) {
+      if (vertices[k] < 0 || vertices[k] >= solver->n) return fail(PD_ERR_INVALID, "planar_energies needs distinct valid particle indices");
+      if (!std::isfinite(stiffness[k]) || stiffness[k] < 0.0)
+        return fail(PD_ERR_INVALID, "planar_energies stiffness must be finite and nonnegative");
+    }
+    solver->plane_vertices.assign(vertices, vertices + count);
+    solver->plane_stiffness.assign(stiffness, stiffness + count);
+    for (int c = 0; c < 4; ++c) solver->plane[c] = plane[c];
+  }
+  std::vector<double> weight(solver->n, 0.0);
+  for (size_t k = 0; k < solver->plane_vertices.size(); ++k) weight[solver->plane_vertices[k]] = solver->plane_stiffness[k];
+  PD_CUDA(solver->d_plane_weight.upload(weight));
+  solver->stale = true;
+  return PD_OK;
+}
+
+int pd_build(PdSolver* s, double dt) {
+  if (s == nullptr) return fail(PD_ERR_INVALID, "null solver");
+  if (!std::isfinite(dt) || dt <= 0.0) return fail(PD_ERR_INVALID, "dt must be finite and positive");
+  if (!s->materials_set) return fail(PD_ERR_STATE, "materials must be set before the build");
+  PD_CUDA(cudaSetDevice(s->device));
+  for (int e = 0; e < s->ne; ++e) {
+    if (!std::isfinite(s->mu[e]) || !std::isfinite(s->lame[e]) || s->mu[e] <= 0.0 || s->lame[e] < 0.0)
+      return fail(PD_ERR_INVALID, "DiffPhD requires positive shear modulus and nonnegative Lame lambda");
+  }
+  const int samples = samples_of(s);
+  const double volume = sample_volume_of(s);
+  // Element weights (kernels.py:112-133, hex.py:95-112).
+  std::vector<double> wc(s->ne, 0.0), wv(s->ne, 0.0), wn(s->ne, 0.0);
+  for (int e = 0; e < s->ne; ++e) {
+    if (s->options.material == PD_MATERIAL_PD) {
+      wc[e] = 2.0 * s->mu[e] * volume;
+      wv[e] = s->lame[e] * volume;
+    } else {
+      wn[e] = 2.0 * s->mu[e] * volume;
+    }
+  }
+  // Mean Lame parameters of the Neo-Hookean projection (solver.py:514-518).
+  // The reference takes NumPy means; the same pairwise summation order
+  // (blocks of 8 below 128 entries, halving above) is used here.
+  auto pairwise = [](const std::vector<double>& v) {
+    // numpy.add.reduce pairwise summation with blocks of 8 (n < 8 sequential).
+    std::function<double(const double*, size_t)> sum = [&](const double* a, size_t n) -> double {
+      if (n < 8) {
+        double r = 0.0;
+        for (size_t i = 0; i < n; ++i) r += a[i];
+        return r;
+      }
+      if (n <= 128) {
+        double r[8];
+        for (int j = 0; j < 8; ++j) r[j] = a[j];
+        size_t i = 8;
+        for (; i + 8 <= n; i += 8)
+          for (int j = 0; j < 8; ++j) r[j] += a[i + j];
+        double result = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
+        for (; i < n; ++i) result += a[i];
+        return result;
+      }
+      size_t half = n / 2;
+      half -= half % 8;
+      return sum(a, half) + sum(a + half, n - half);
+    };
+    return sum(v.data(), v.size()) / static_cast<double>(v.size());
+  };
+  s->nh_mu = pairwise(s->mu);
+  s->nh_lame = pairwise(s->lame);
+  s->nh_penalty = 2.0 * s->nh_mu;
+  s->mass = s->options.density * s->mean_volume;
+  s->inertia = s->mass / (dt * dt);
+  // Constant matrix rows in the reference's accumulation order
+  // (solver.py:521-545). A fixed sparsity pattern (particle adjacency) holds the
+  // running sums; each entry receives the same additions in the same order.
+  std::vector<std::vector<int32_t>> adjacency(s->n);
+  for (int e = 0; e < s->ne; ++e) {
+    const int32_t* nodes = s->indices.data() + s->corners * e;
+    for (int a = 0; a < s->corners; ++a)
+      for (int b = 0; b < s->corners; ++b)
+        if (s->free_[nodes[a]] && s->free_[nodes[b]]) adjacency[nodes[a]].push_back(nodes[b]);
+  }
+  std::vector<int32_t> row_offsets(s->n + 1, 0);
+  for (int i = 0; i < s->n; ++i) {
+    adjacency[i].push_back(i);
+    std::sort(adjacency[i].begin(), adjacency[i].end());
+    adjacency[i].erase(std::unique(adjacency[i].begin(), adjacency[i].end()), adjacency[i].end());
+    row_offsets[i + 1] = row_offsets[i] + static_cast<int32_t>(adjacency[i].size());
+  }
+  std::vector<int32_t> row_columns(row_offsets[s->n]);
+  std::vector<double> row_values(row_offsets[s->n], 0.0);
+  for (int i = 0; i < s->n; ++i) {
+    std::copy(adjacency[i].begin(), adjacency[i].end(), row_columns.begin() + row_offsets[i]);
+    const auto at = std::lower_bound(adjacency[i].begin(), adjacency[i].end(), i) - adjacency[i].begin();
+    row_values[row_offsets[i] + at] = s->free_[i] ? s->inertia : 1.0;
+  }
+  auto add = [&](int i, int j, double value) {
+    const int32_t* first = row_columns.data() + row_offsets[i];
+    const int32_t* last = row_columns.data() + row_offsets[i + 1];
+    row_values[row_offsets[i] + (std::lower_bound(first, last, j) - first)] += value;
+  };
+  const int k = s->corners;
+  std::vector<double> block(static_cast<size_t>(k) * k);
+  std::vector<double> fibre(k);
+  for (int e = 0; e < s->ne; ++e) {
+    const int32_t* nodes = s->indices.data() + k * e;
+    const double weight = (wc[e] + wv[e]) + wn[e];
+    const double muscle = s->muscle_stiffness.empty() ? 0.0 : s->muscle_stiffness[e] * volume;
+    for (int q = 0; q < samples; ++q) {
+      const double* g = sample_rows(s, e, q);
+      for (int a = 0; a < k; ++a)
+        for (int b = 0; b < k; ++b) {
+          const double dot = (g[3 * a] * g[3 * b] + g[3 * a + 1] * g[3 * b + 1]) + g[3 * a + 2] * g[3 * b + 2];
+          block[a * k + b] = weight * dot;
+        }
+      if (s->has_muscles && muscle > 0.0) {
+        const double* m = s->muscle_dir.data() + 3 * e;
+        for (int a = 0; a < k; ++a) fibre[a] = (g[3 * a] * m[0] + g[3 * a + 1] * m[1]) + g[3 * a + 2] * m[2];
+        for (int a = 0; a < k; ++a)
+          for (int b = 0; b < k; ++b) block[a * k + b] += muscle * (fibre[a] * fibre[b]);
+      }
+      for (int a = 0; a < k; ++a) {
+        const int i = nodes[a];
+        if (!s->free_[i]) continue;
+        for (int b = a; b < k; ++b) {
+          const int j = nodes[b];
+          if (!s->free_[j]) continue;
+          const double value = block[a * k + b];
+          add(i, j, value);
+          if (i != j) add(j, i, value);
+        }
+      }
+    }
+  }
+  for (size_t p = 0; p < s->plane_vertices.size(); ++p) {
+    const int i = s->plane_vertices[p];
+    if (s->free_[i]) add(i, i, s->plane_stiffness[p]);
+  }
+  InverseFactor factor;
+  const std::string error =
+      pdb200::build_inverse_factor(s->n, row_offsets.data(), row_columns.data(), row_values.data(), &factor);
+  if (!error.empty()) return fail(error.find("positive definite") != std::string::npos ? PD_ERR_NOT_SPD : PD_ERR_INVALID, error);
+  s->factor = std::move(factor);
+  // Grid size: all SMs for large factors, fewer blocks for small meshes.
+  int blocks = s->options.blocks;
+  if (blocks <= 0) {
+    const int64_t work = std::max<int64_t>(static_cast<int64_t>(s->factor.s.columns.size()) / 2048,
+                                           static_cast<int64_t>(s->ne) * samples / 256);
+    blocks = static_cast<int>(std::max<int64_t>(8, std::min<int64_t>(work, s->max_blocks)));
+  }
+  blocks = std::min(blocks, s->max_blocks);
+  s->blocks = blocks;
+  const std::vector<int32_t> s_part = partition_rows(s->factor.s.offsets, blocks);
+  const std::vector<int32_t> st_part = partition_rows(s->factor.st.offsets, blocks);
+  PD_CUDA(s->d_s_off.upload(s->factor.s.offsets));
+  PD_CUDA(s->d_s_col.upload(s->factor.s.columns));
+  PD_CUDA(s->d_s_val.upload(s->factor.s.values));
+  PD_CUDA(s->d_st_off.upload(s->factor.st.offsets));
+  PD_CUDA(s->d_st_col.upload(s->factor.st.columns));
+  PD_CUDA(s->d_st_val.upload(s->factor.st.values));
+  if (s->options.precision == PD_PRECISION_FP32_REFINE) {
+    std::vector<float> s32(s->factor.s.values.begin(), s->factor.s.values.end());
+    std::vector<float> st32(s->factor.st.values.begin(), s->factor.st.values.end());
+    PD_CUDA(s->d_s_val32.upload(s32));
+    PD_CUDA(s->d_st_val32.upload(st32));
+  }
+  PD_CUDA(s->d_s_part.upload(s_part));
+  PD_CUDA(s->d_st_part.upload(st_part));
+  PD_CUDA(s->d_a_off.upload(row_offsets));
+  PD_CUDA(s->d_a_col.upload(row_columns));
+  PD_CUDA(s->d_a_val.upload(row_values));
+  PD_CUDA(s->d_wc.upload(wc));
+  PD_CUDA(s->d_wv.upload(wv));
+  PD_CUDA(s->d_wn.upload(wn));
+  PD_CUDA(s->d_partials.allocate(static_cast<size_t>(blocks) * pdb200::kPartialStride * sizeof(double)));
+  PD_CUDA(s->b_partials.allocate(static_cast<size_t>(blocks) * pdb200::kPartialStride * sizeof(double)));
+  if (s->d_plane_weight.ptr == nullptr) {
+    std::vector<double> none(s->n, 0.0);
+    PD_CUDA(s->d_plane_weight.upload(none));
+  }
+  s->built = true;
+  s->stale = false;
+  s->built_dt = dt;
+  return PD_OK;
+}
+
+
+int pd_factor_stats(const PdSolver* s, int64_t* rows, int64_t* nnz_s, int64_t* nnz_l) {
+  if (s == nullptr) return fail(PD_ERR_INVALID, "null solver");
+  if (!s->built) return fail(PD_ERR_STATE, "the factor has not been built");
+  if (rows) *rows = s->factor.size;
+  if (nnz_s) *nnz_s = static_cast<int64_t>(s->factor.s.columns.size());
+  if (nnz_l) *nnz_l = s->factor.factorization_nnz;
+  return PD_OK;
+}
+
+int pd_step(PdSolver* s, const float* q, const float* qd, const float* f, const float* dirichlet,
+            const double gravity[3], double dt, float* q_out, float* qd_out, double* x_record, void* stream) {
+  if (s == nullptr || q == nullptr || qd == nullptr || f == nullptr || gravity == nullptr || q_out == nullptr ||
+      qd_out == nullptr)
+    return fail(PD_ERR_INVALID, "null argument");
+  if (!std::isfinite(dt) || dt <= 0.0) return fail(PD_ERR_INVALID, "dt must be finite and positive");
+  if (q == q_out || qd == qd_out || q == qd_out || qd == q_out)
+    return fail(PD_ERR_INVALID, "DiffPhD requires distinct input and output states");
+  if (dirichlet != nullptr && (dirichlet == q_out || dirichlet == qd_out))
+    return fail(PD_ERR_INVALID, "dirichlet_positions must not alias an output state");
+  if (!s->built || s->stale || s->built_dt != dt)
+    return fail(PD_ERR_STATE, "SolverDiffPhD must rebuild its factor (pd_build) for this dt and model");
+  PD_CUDA(cudaSetDevice(s->device));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  StepArgs a{};
+  a.n = s->n;
+  a.ne = s->ne;
+  a.corners = s->corners;
+  a.hex = s->hex;
+  a.indices = s->d_indices.as<int>();
+  a.gradients = s->d_gradients.as<double>();
+  a.free_ = s->d_free.as<int>();
+  a.inc_offsets = s->d_inc_offsets.as<int>();
+  a.inc_entries = s->d_inc_entries.as<int>();
+  a.plane_weight = s->plane_vertices.empty() ? nullptr : s->d_plane_weight.as<double>();
+  {
+    const double* p = s->plane;
+    for (int c = 0; c < 4; ++c) a.plane[c] = p[c];
+  }
+  a.wc = s->d_wc.as<double>();
+  a.wv = s->d_wv.as<double>();
+  a.wn = s->d_wn.as<double>();
+  a.wm = s->d_wm.as<double>();
+  a.mdir = s->d_mdir.as<double>();
+  a.mtarget = s->d_mtarget.as<double>();
+  a.activations = s->hex ? nullptr : s->activations;
+  a.has_muscles = s->has_muscles ? 1 : 0;
+  a.material = s->options.material;
+  a.nh_mu = s->nh_mu;
+  a.nh_lame = s->nh_lame;
+  a.nh_penalty = s->nh_penalty;
+  a.s_off = s->d_s_off.as<int>();
+  a.s_col = s->d_s_col.as<int>();
+  a.s_val = s->d_s_val.as<double>();
+  a.s_val32 = s->d_s_val32.as<float>();
+  a.st_off = s->d_st_off.as<int>();
+  a.st_col = s->d_st_col.as<int>();
+  a.st_val = s->d_st_val.as<double>();
+  a.st_val32 = s->d_st_val32.as<float>();
+  a.s_part = s->d_s_part.as<int>();
+  a.st_part = s->d_st_part.as<int>();
+  a.a_off = s->d_a_off.as<int>();
+  a.a_col = s->d_a_col.as<int>();
+  a.a_val = s->d_a_val.as<double>();
+  a.refine = s->options.precision == PD_PRECISION_FP32_REFINE ? 1 : 0;
+  a.position = s->d_position.as<double>();
+  a.velocity = s->d_velocity.as<double>();
+  a.target = s->d_target.as<double>();
+  a.boundary = s->d_boundary.as<double>();
+  a.x = s->d_x.as<double>();
+  a.prev = s->d_prev.as<double>();
+  a.proj = s->d_proj.as<double>();
+  a.prev_proj = s->d_prev_proj.as<double>();
+  a.rhs = s->d_rhs.as<double>();
+  a.y = s->d_y.as<double>();
+  a.contrib = s->d_contrib.as<double>();
+  a.window = s->options.anderson_window;
+  a.hist_x = s->d_hist_x.as<double>();
+  a.hist_g = s->d_hist_g.as<double>();
+  a.aa_state = s->d_aa_state.as<int>();
+  a.aa_gamma = s->d_aa_gamma.as<double>();
+  a.aa_accept = s->d_aa_accept.as<int>();
+  a.partials = s->d_partials.as<double>();
+  a.iteration = s->d_iteration.as<int>();
+  a.active = s->d_active.as<int>();
+  a.status = s->d_status.as<int>();
+  a.max_iterations = s->options.max_iterations;
+  a.abs_tol = s->options.abs_tol;
+  a.rel_tol = s->options.rel_tol;
+  a.barrier = s->d_barrier.as<pdb200::GridBarrier>();
+  a.q_in = q;
+  a.qd_in = qd;
+  a.f_in = f;
+  a.dirichlet = dirichlet;
+  a.q_out = q_out;
+  a.qd_out = qd_out;
+  a.x_record = x_record;
+  a.dt = dt;
+  a.mass = s->mass;
+  a.inertia = s->inertia;
+  for (int c = 0; c < 3; ++c) a.gravity[c] = gravity[c];
+  a.integrate_pinned = s->options.integrate_pinned_velocities;
+  PD_CUDA(cudaMemsetAsync(s->d_barrier.ptr, 0, sizeof(pdb200::GridBarrier), st));
+  PD_CUDA(pdb200::launch_forward_step(a, s->blocks, s->options.precision, st));
+  return PD_OK;
+}
+
+int pd_backward(PdSolver* s, const double* x_record, const float* activations, double dt, const float* gq_out,
+                const float* gqd_out, float* gq, float* gqd, float* gf, float* gdirichlet, double* gmaterials,
+                float* gactivations, void* stream) {
+  if (s == nullptr || x_record == nullptr) return fail(PD_ERR_INVALID, "null argument");
+  if (!s->built || s->stale || s->built_dt != dt)
+    return fail(PD_ERR_STATE, "the backward pass needs the factor of its recorded step (same dt and model)");
+  PD_CUDA(cudaSetDevice(s->device));
+  if (int status = ensure_adjoint_buffers(s)) return status;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const size_t fvec = static_cast<size_t>(3) * s->n * sizeof(float);
+  // Missing output gradients read as zero; missing input accumulators go to scratch.
+  if (gq_out == nullptr || gqd_out == nullptr) {
+    PD_CUDA(cudaMemsetAsync(s->b_zero_gq.ptr, 0, fvec, st));
+    PD_CUDA(cudaMemsetAsync(s->b_zero_gqd.ptr, 0, fvec, st));
+  }
+  AdjointArgs b{};
+  b.n = s->n;
+  b.ne = s->ne;
+  b.corners = s->corners;
+  b.hex = s->hex;
+  b.indices = s->d_indices.as<int>();
+  b.gradients = s->d_gradients.as<double>();
+  b.free_ = s->d_free.as<int>();
+  b.inc_offsets = s->d_inc_offsets.as<int>();
+  b.inc_entries = s->d_inc_entries.as<int>();
+  b.wc = s->d_wc.as<double>();
+  b.wv = s->d_wv.as<double>();
+  b.wn = s->d_wn.as<double>();
+  b.wm = s->d_wm.as<double>();
+  b.mdir = s->d_mdir.as<double>();
+  b.mtarget = s->d_mtarget.as<double>();
+  b.has_muscles = s->has_muscles ? 1 : 0;
+  b.material = s->options.material;
+  b.exact = s->options.adjoint_mode == PD_ADJOINT_EXACT ? 1 : 0;
+  b.nh_mu = s->nh_mu;
+  b.nh_lame = s->nh_lame;
+  b.nh_penalty = s->nh_penalty;
+  const double volume = sample_volume_of(s);
+  // StepRecord.jacobian_weights (adjoint.py:828-832): the mean weight per energy.
+  b.jwc = s->options.material == PD_MATERIAL_PD ? 2.0 * s->nh_mu * volume : 0.0;
+  b.jwv = s->options.material == PD_MATERIAL_PD ? s->nh_lame * volume : 0.0;
+  b.jwn = s->options.material == PD_MATERIAL_NEO_HOOKEAN ? 2.0 * s->nh_mu * volume : 0.0;
+  b.sample_volume = volume;
+  b.s_off = s->d_s_off.as<int>();
+  b.s_col = s->d_s_col.as<int>();
+  b.s_val = s->d_s_val.as<double>();
+  b.s_val32 = s->d_s_val32.as<float>();
+  b.st_off = s->d_st_off.as<int>();
+  b.st_col = s->d_st_col.as<int>();
+  b.st_val = s->d_st_val.as<double>();
+  b.st_val32 = s->d_st_val32.as<float>();
+  b.s_part = s->d_s_part.as<int>();
+  b.st_part = s->d_st_part.as<int>();
+  b.a_off = s->d_a_off.as<int>();
+  b.a_col = s->d_a_col.as<int>();
+  b.a_val = s->d_a_val.as<double>();
+  b.refine = s->options.precision == PD_PRECISION_FP32_REFINE ? 1 : 0;
+  b.x = x_record;
+  b.rhs = s->b_rhs.as<double>();
+  b.base = s->b_base.as<double>();
+  b.solution = s->b_solution.as<double>();
+  b.prev = s->b_prev.as<double>();
+  b.work = s->b_work.as<double>();
+  b.y = s->b_y.as<double>();
+  b.raw = s->b_raw.as<double>();
+  b.contrib = s->b_contrib.as<double>();
+  b.jac64 = s->b_jac.as<double>();
+  b.jac32 = s->b_jac.as<float>();
+  b.window = s->options.anderson_window;
+  b.hist_x = s->b_hist_x.as<double>();
+  b.hist_g = s->b_hist_g.as<double>();
+  b.aa_state = s->b_aa_state.as<int>();
+  b.aa_gamma = s->b_aa_gamma.as<double>();
+  b.aa_accept = s->b_aa_accept.as<int>();
+  b.partials = s->b_partials.as<double>();
+  b.iteration = s->b_iteration.as<int>();
+  b.active = s->b_active.as<int>();
+  b.status = s->d_status.as<int>();
+  b.max_iterations = s->options.max_iterations;
+  b.abs_tol = s->options.abs_tol;
+  b.rel_tol = s->options.rel_tol;
+  b.barrier = s->d_barrier.as<pdb200::GridBarrier>();
+  b.control_d = s->b_control_d.as<double>();
+  b.control_i = s->b_control_i.as<int>();
+  b.gq_out = gq_out != nullptr ? gq_out : s->b_zero_gq.as<float>();
+  b.gqd_out = gqd_out != nullptr ? gqd_out : s->b_zero_gqd.as<float>();
+  b.gq = gq != nullptr ? gq : s->b_scratch_gq.as<float>();
+  b.gqd = gqd != nullptr ? gqd : s->b_scratch_gqd.as<float>();
+  b.gf = gf != nullptr ? gf : s->b_scratch_gf.as<float>();
+  b.gdirichlet = gdirichlet;
+  b.gmaterials = gmaterials;
+  b.gactivations = s->hex ? nullptr : gactivations;
+  b.material_scratch = s->b_material_scratch.as<double>();
+  b.activation_scratch = s->b_activation_scratch.as<double>();
+  b.has_dirichlet = s->has_dirichlet ? 1 : 0;
+  b.integrate_pinned = s->options.integrate_pinned_velocities;
+  b.zero_energy_weight =
+      (gmaterials != nullptr && s->options.material == PD_MATERIAL_PD && s->nh_lame == 0.0) ? 1 : 0;
+  b.dt = dt;
+  b.inertia = s->inertia;
+  // A Tet4 step's fibre targets are 1 - u of the activations it used.
+  b.activations = (!s->hex && s->has_muscles) ? activations : nullptr;
+  PD_CUDA(cudaMemsetAsync(s->d_barrier.ptr, 0, sizeof(pdb200::GridBarrier), st));
+  PD_CUDA(pdb200::launch_adjoint_step(b, s->blocks, s->options.precision, st));
+  return PD_OK;
+}
+
+int pd_read_status(PdSolver* s, int32_t* bits, void* stream) {
+  if (s == nullptr || bits == nullptr) return fail(PD_ERR_INVALID, "null argument");
+  PD_CUDA(cudaSetDevice(s->device));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int value = 0;
+  PD_CUDA(cudaMemcpyAsync(&value, s->d_status.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
+  PD_CUDA(cudaStreamSynchronize(st));
+  PD_CUDA(cudaMemsetAsync(s->d_status.ptr, 0, sizeof(int), st));
+  PD_CUDA(cudaStreamSynchronize(st));
+  *bits = value;
+  return PD_OK;
+}
+
+int pd_iterations(PdSolver* s, int32_t* forward, int32_t* backward, void* stream) {
+  if (s == nullptr) return fail(PD_ERR_INVALID, "null solver");
+  PD_CUDA(cudaSetDevice(s->device));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int f = 0, b = 0;
+  PD_CUDA(cudaMemcpyAsync(&f, s->d_iteration.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
+  if (s->b_iteration.ptr != nullptr)
+    PD_CUDA(cudaMemcpyAsync(&b, s->b_iteration.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
+  PD_CUDA(cudaStreamSynchronize(st));
+  if (forward) *forward = f;
+  if (backward) *backward = b;
+  return PD_OK;
+}
+
+int pd_deformation_determinants(PdSolver* s, const float* q, double* out, void* stream) {
+  if (s == nullptr || q == nullptr || out == nullptr) return fail(PD_ERR_INVALID, "null argument");
+  if (!s->hex) return fail(PD_ERR_UNSUPPORTED, "deformation_determinants currently requires hex_mesh");
+  PD_CUDA(cudaSetDevice(s->device));
+  PD_CUDA(pdb200::launch_hex_determinants(q, s->d_indices.as<int>(), s->d_gradients.as<double>(), s->ne, out,
+                                          static_cast<cudaStream_t>(stream)));
+  return PD_OK;
+}
+
+int pd_apply_inverse(PdSolver* s, const double* rhs, double* out, void* stream) {
+  if (s == nullptr || rhs == nullptr || out == nullptr) return fail(PD_ERR_INVALID, "null argument");
+  if (!s->built) return fail(PD_ERR_STATE, "the factor has not been built");
+  PD_CUDA(cudaSetDevice(s->device));
+  PD_CUDA(pdb200::launch_apply_inverse(s->d_s_off.as<int>(), s->d_s_col.as<int>(), s->d_s_val.as<double>(),
+                                       s->d_st_off.as<int>(), s->d_st_col.as<int>(), s->d_st_val.as<double>(), s->n,
+                                       rhs, s->d_y.as<double>(), out, static_cast<cudaStream_t>(stream)));
+  return PD_OK;
+}
+
+struct PdInverseFactor {
+  InverseFactor factor;
+};
+
+int pd_inverse_build(int32_t size, const int32_t* row_offsets, const int32_t* columns, const double* values,
+                     PdInverseFactor** out) {
+  if (out == nullptr || row_offsets == nullptr || (size > 0 && (columns == nullptr || values == nullptr)))
+    return fail(PD_ERR_INVALID, "null argument");
+  auto result = new PdInverseFactor();
+  const std::string error = pdb200::build_inverse_factor(size, row_offsets, columns, values, &result->factor);
+  if (!error.empty()) {
+    delete result;
+    *out = nullptr;
+    return fail(error.find("positive definite") != std::string::npos ? PD_ERR_NOT_SPD : PD_ERR_INVALID, error);
+  }
+  *out = result;
+  return PD_OK;
+}
+
+int pd_inverse_sizes(const PdInverseFactor* f, int32_t* size, int64_t* nnz, int64_t* factorization_nnz) {
+  if (f == nullptr) return fail(PD_ERR_INVALID, "null factor");
+  if (size) *size = f->factor.size;
+  if (nnz) *nnz = static_cast<int64_t>(f->factor.s.columns.size());
+  if (factorization_nnz) *factorization_nnz = f->factor.factorization_nnz;
+  return PD_OK;
+}
+
+int pd_inverse_export(const PdInverseFactor* f, int32_t* permutation, int32_t* s_offsets, int32_t* s_columns,
+                      double* s_values, int32_t* st_offsets, int32_t* st_columns, double* st_values) {
+  if (f == nullptr) return fail(PD_ERR_INVALID, "null factor");
+  const InverseFactor& x = f->factor;
+  auto copy = [](auto* dst, const auto& src) {
+    if (dst != nullptr && !src.empty()) std::memcpy(dst, src.data(), src.size() * sizeof(src[0]));
+  };
+  copy(permutation, x.permutation);
+  copy(s_offsets, x.s.offsets);
+  copy(s_columns, x.s.columns);
+  copy(s_values, x.s.values);
+  copy(st_offsets, x.st.offsets);
+  copy(st_columns, x.st.columns);
+  copy(st_values, x.st.values);
+  return PD_OK;
+}
+
+int pd_inverse_free(PdInverseFactor* f) {
+  delete f;
+  return PD_OK;
+}
+
+}  // extern "C"
