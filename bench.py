@@ -1,0 +1,465 @@
+#!/usr/bin/env python
+"""Benchmark of the DiffPhD projective-dynamics step and its adjoint on B200.
+
+Metric: PD forward+adjoint steps per second (one PD time step forward plus its
+adjoint), on the Tet4 block workload: a 32x8x8 block of 0.01 m cubes split
+into 5 tetrahedra each (10,240 Tet4, 2,673 particles), per-tet Young's modulus
+log-uniform in [1e5, 1e7] Pa (seed 0), nu 0.4, density 1000 kg/m^3, gravity
+-9.81 m/s^2, the x=0 face pinned, 50 steps of dt 5e-3 s at relative tolerance
+1e-6, float64. The loss is the squared distance of the final positions to the
+rest pose plus a seeded 1 mm Gaussian displacement; the backward pass returns
+its gradient with respect to every tet's Young's modulus (and the initial
+state and forces). One bench step is one 50-step rollout forward and back.
+
+``--gpus N`` (under torchrun) runs N independent replicas, one per GPU; a
+single instance does not shard (its inverse factor is dense-ish and every
+iteration would need an all-gather). ``value`` is the whole-job rate.
+
+``--impl reference`` times the CPU port of the reference's sparse algorithm
+(oracle/sparse_port.py; the reference's Warp CPU path needs warp-lang and
+newton, which are not installed) on this host's cores, on the same workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+STEPS_PER_ROLLOUT = 50
+DT = 5.0e-3
+REL_TOL = 1.0e-6
+ABS_TOL = 1.0e-9
+NX, NY, NZ, EDGE = 32, 8, 8, 0.01
+METRIC = "PD fwd+adjoint steps/s on 1 B200 at <=1e-6 rel err vs FP64; batched vs plain"
+UNIT = "PD steps/s"
+WORKLOAD = "tet4_block_32x8x8_fwd_adjoint_50steps"
+
+
+def workload_arrays(seed=0):
+    from newton_solver_diff_phd_b200 import meshes
+
+    vertices, tets, _ = meshes.tet_grid(NX, NY, NZ, EDGE)
+    rng = np.random.default_rng(seed)
+    young = np.exp(rng.uniform(np.log(1.0e5), np.log(1.0e7), len(tets)))
+    poisson = 0.4
+    target = vertices + rng.normal(0.0, 1.0e-3, vertices.shape)
+    return vertices, tets, young, poisson, target
+
+
+def build_model(device):
+    import torch
+
+    from newton_solver_diff_phd_b200 import ModelBuilder, meshes
+
+    vertices, tets, young, poisson, target = workload_arrays()
+    builder = ModelBuilder(gravity=(0.0, 0.0, -9.81))
+    builder.add_soft_grid(pos=(0.0, 0.0, 0.0), rot=None, vel=(0.0, 0.0, 0.0), dim_x=NX, dim_y=NY, dim_z=NZ,
+                          cell_x=EDGE, cell_y=EDGE, cell_z=EDGE, density=1000.0, k_mu=1.0, k_lambda=1.0, k_damp=0.0,
+                          fix_left=True)
+    model = builder.finalize(device)
+    mu, lam = meshes.lame_from_young(young, poisson)
+    with torch.no_grad():
+        model.tet_materials.copy_(torch.tensor(np.column_stack((mu, lam, np.zeros_like(mu))), dtype=torch.float32))
+    return model, young, poisson, target
+
+
+def algorithmic_bytes_per_iteration(n, elements, nnz_s, corners=4, window=5, value_bytes=8):
+    """Bytes one local/global iteration must move (SURVEY 8(d) B_iter with b = value bytes)."""
+    b = value_bytes
+    return (2 * (nnz_s * (b + 4) + 4 * (n + 1)) + 2 * (3 * n * b) * 2 + elements * corners * 4 + 3 * elements * 8
+            + 3 * n * b + 3 * n * b + (2 * window + 4) * 3 * n * b + 4 * 3 * n * b)
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        return False
+
+    def summary(self):
+        self.file.flush()
+        rows = []
+        try:
+            for line in Path(self.file.name).read_text().splitlines():
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        finally:
+            os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        max_sm = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        loaded = sorted(sm)[len(sm) // 4:] if len(sm) >= 4 else sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": max(max_sm) if max_sm else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peak():
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        data = json.loads(path.read_text())
+        return float(data["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """Per-launch DRAM bytes of the forward step kernel from the committed ncu summary, if any."""
+    path = ROOT / "profiles" / "forward_step_kernel_tet4_block.md"
+    if not path.exists():
+        return None
+    for line in path.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch_scaled:"):
+            try:
+                return float(line.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
+def run_b200(args):
+    import torch
+
+    from newton_solver_diff_phd_b200 import SolverDiffPhD, meshes
+    from newton_solver_diff_phd_b200.rollout import Rollout
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=device)
+    model, young, poisson, target = build_model(device)
+    solver = SolverDiffPhD(model, density=1000.0, rel_tol=REL_TOL, abs_tol=ABS_TOL, adjoint=args.adjoint,
+                           precision=args.precision)
+    driver = Rollout(solver, STEPS_PER_ROLLOUT, DT)
+    q0 = model.particle_q.clone()
+    qd0 = torch.zeros_like(q0)
+    target_t = torch.tensor(target, dtype=torch.float32, device=device)
+    dmu_de, dlam_de, _, _ = meshes.lame_young_derivatives(poisson)
+    dmu_de_t = torch.tensor(dmu_de, dtype=torch.float64, device=device)
+    dlam_de_t = torch.tensor(dlam_de, dtype=torch.float64, device=device)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+
+    def one_rollout():
+        final = driver.forward(q0, qd0)
+        diff = final.particle_q - target_t
+        loss = (diff.double() ** 2).sum()
+        _, _, _, gml = driver.backward((2.0 * diff).float().contiguous())
+        grad_e = gml[:, 0] * dmu_de_t + gml[:, 1] * dlam_de_t
+        return loss, grad_e
+
+    # Untimed build and warm-up.
+    for _ in range(args.warmup):
+        loss, grad_e = one_rollout()
+    torch.cuda.synchronize()
+    status = solver.read_status()
+    stream = torch.cuda.current_stream()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as sampler:
+        for k in range(args.steps):
+            flush.fill_(float(k))  # evict the factor from L2 between timed rollouts (untimed)
+            starts[k].record(stream)
+            loss, grad_e = one_rollout()
+            ends[k].record(stream)
+        torch.cuda.synchronize()
+    clocks = sampler.summary()
+    elapsed_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    if dist is not None:
+        t = torch.tensor([elapsed_ms], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+    status |= solver.read_status()
+    total_steps = STEPS_PER_ROLLOUT * args.steps * world
+    value = total_steps / (elapsed_ms / 1000.0)
+
+    if args.no_extras:
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                              "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "profiling_run": True}))
+        return
+    # Kernel-level timing of the persistent forward and adjoint launches (outside the timed region).
+    rows, nnz_s, _ = solver.factor_stats()
+    fwd_ms, fwd_iters, bwd_ms, bwd_iters = [], [], [], []
+    import ctypes
+
+    from newton_solver_diff_phd_b200 import _lib
+
+    lib = _lib.library()
+    state_a, state_b = model.state(), model.state()
+    for state in (state_a, state_b):
+        state.requires_grad_(True)
+    with torch.no_grad():
+        state_a.particle_q.copy_(q0)
+    record = torch.zeros((solver._n, 3), dtype=torch.float64, device=device)
+    for t in range(8):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        solver.step(state_a, state_b, None, None, DT, record=record)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        fwd_ms.append(e0.elapsed_time(e1))
+        fwd_iters.append(int(solver.iterations[0]))
+        state_b.particle_q.grad.normal_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        solver.backward_step(record, DT, state_a, state_b)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        bwd_ms.append(e0.elapsed_time(e1))
+        bwd_iters.append(solver.backward_iterations)
+        state_a, state_b = state_b, state_a
+    solver.read_status()
+    per_iter = algorithmic_bytes_per_iteration(rows, solver._element_count, nnz_s)
+    fwd_bytes = per_iter * float(np.mean(fwd_iters))
+    fwd_launch_ms = float(np.mean(fwd_ms))
+    bwd_launch_ms = float(np.mean(bwd_ms))
+    peak, peak_kind = measured_peak()
+    achieved = fwd_bytes / (fwd_launch_ms / 1000.0) / 1e9
+    traffic = profile_traffic()
+
+    result = {
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": elapsed_ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32+f64-refine",
+        "data": "synthetic (seeded Tet4 block; materials log-uniform from default_rng(0))",
+        "config": {
+            "workload": WORKLOAD,
+            "particles": int(solver._n),
+            "tets": int(solver._element_count),
+            "pd_steps_per_bench_step": STEPS_PER_ROLLOUT,
+            "dt": DT,
+            "rel_tol": REL_TOL,
+            "abs_tol": ABS_TOL,
+            "anderson_window": 5,
+            "adjoint": args.adjoint,
+            "precision": args.precision,
+            "nnz_S": int(nnz_s),
+            "l2": "256 MiB write between timed rollouts (flush); the factor re-enters L2 within a rollout",
+            "parallelism": f"replicas x{world}",
+            "forward_iterations_mean": float(np.mean(fwd_iters)),
+            "backward_iterations_mean": float(np.mean(bwd_iters)),
+            "status_bits": int(status),
+        },
+        "gpu_launches": 2 * STEPS_PER_ROLLOUT * args.steps,
+        "clocks": clocks,
+        "roofline": {
+            "bound": "hbm",
+            "kernel": "forward_step_kernel<double,double> (one launch = one PD step, all iterations)",
+            "achieved": achieved,
+            "peak": peak,
+            "peak_kind": f"{peak_kind} burst copy GB/s",
+            "unit": "GB/s",
+            "frac": achieved / peak,
+            "traffic": traffic,
+            "algorithmic_bytes_per_launch": fwd_bytes,
+            "launch_ms": fwd_launch_ms,
+            "adjoint_launch_ms": bwd_launch_ms,
+        },
+    }
+    if rank == 0:
+        result["e2e"] = run_e2e(args, solver, driver, q0, target, young, dmu_de, dlam_de, device)
+        result["cpu_baseline"] = cpu_baseline(args, seconds=args.cpu_seconds)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+
+
+def run_e2e(args, solver, driver, q0, target, young, dmu_de, dlam_de, device):
+    """The same metric through the public API with host buffers (pinned H2D in, D2H out, timed)."""
+    import torch
+
+    from newton_solver_diff_phd_b200.rollout import rollout
+
+    host_q0 = q0.cpu().pin_memory()
+    host_qd0 = torch.zeros_like(host_q0).pin_memory()
+    host_target = torch.tensor(target, dtype=torch.float32).pin_memory()
+    host_young = torch.tensor(young, dtype=torch.float64).pin_memory()
+    out_loss = torch.empty(1, dtype=torch.float64).pin_memory()
+    out_grad = torch.empty(len(young), dtype=torch.float64).pin_memory()
+    nu = 0.4
+    stream = torch.cuda.current_stream()
+    steps = max(1, args.steps)
+
+    def once():
+        q = host_q0.to(device, non_blocking=True)
+        qd = host_qd0.to(device, non_blocking=True)
+        tgt = host_target.to(device, non_blocking=True)
+        e = host_young.to(device, non_blocking=True).requires_grad_(True)
+        mu = e / (2.0 * (1.0 + nu))
+        lam = e * nu / ((1.0 + nu) * (1.0 - 2.0 * nu))
+        q_t, _ = rollout(driver, q, qd, None, torch.stack((mu, lam), dim=1))
+        loss = ((q_t.double() - tgt.double()) ** 2).sum()
+        loss.backward()
+        out_loss.copy_(loss.detach().reshape(1), non_blocking=True)
+        out_grad.copy_(e.grad, non_blocking=True)
+
+    once()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(steps):
+        once()
+    end.record(stream)
+    torch.cuda.synchronize()
+    ms = start.elapsed_time(end)
+    h2d = host_q0.numel() * 4 * 3 + host_young.numel() * 8
+    d2h = 8 + out_grad.numel() * 8
+    return {"value": STEPS_PER_ROLLOUT * steps / (ms / 1000.0), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "grad_wrt": "per-tet Young's modulus (E), loss scalar"}
+
+
+def cpu_sample(steps, threads):
+    """Time the CPU port on the first `steps` PD steps (forward then adjoint); returns (seconds, steps)."""
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    from newton_solver_diff_phd_b200 import _lib, meshes
+    from oracle import pd_oracle
+    from oracle.sparse_port import SparsePort
+
+    vertices, tets, young, poisson, target = workload_arrays()
+    poses = meshes.tet_rest_poses(vertices.astype(np.float32).astype(np.float64), tets).astype(np.float32)
+    mu, lam = meshes.lame_from_young(young, poisson)
+    mu = mu.astype(np.float32).astype(np.float64)
+    lam = lam.astype(np.float32).astype(np.float64)
+    free = vertices[:, 0] > 0
+    body = pd_oracle.Body.tet(tets, poses, free, mu, lam, 1000.0)
+    a = body.matrix(DT)
+    import scipy.sparse as sp
+
+    csr = sp.csr_matrix(a)
+    factor = _lib.inverse_factor((csr.indptr, csr.indices, csr.data))
+    port = SparsePort(body, factor, DT)
+    q = vertices.astype(np.float32).astype(np.float64)
+    v = np.zeros_like(q)
+    gravity = np.array([0.0, 0.0, -9.81], dtype=np.float32).astype(np.float64)
+    start = time.perf_counter()
+    records = []
+    for _ in range(steps):
+        x, _, _ = port.step(q, v, np.zeros_like(q), gravity, max_iterations=10000, abs_tol=ABS_TOL, rel_tol=REL_TOL)
+        records.append(x)
+        v = (x - q) / DT
+        q = x
+    seed = 2.0 * (q - target)
+    for x in reversed(records):
+        mu_adj, _, _ = port.backward(x, seed, np.zeros_like(seed), max_iterations=10000, abs_tol=ABS_TOL,
+                                     rel_tol=REL_TOL, mode="exact")
+        seed = body.mass / DT**2 * mu_adj
+    return time.perf_counter() - start, steps
+
+
+def cpu_baseline(args, seconds=20.0):
+    threads = os.cpu_count() or 1
+    elapsed, steps = cpu_sample(2, threads)
+    return {"value": steps / elapsed, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"first {steps} PD steps of the rollout forward then their adjoints, oracle/sparse_port.py "
+                      "(SciPy CSR S^T S, NumPy projections; SpMV single-threaded)"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_sample(1, threads)
+    total, steps = 0.0, 0
+    for _ in range(args.steps):
+        elapsed, n = cpu_sample(1, threads)
+        total += elapsed
+        steps += n
+    value = steps / total
+    result = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Tet4 block)", "impl": "reference",
+        "config": {"workload": WORKLOAD, "sample": "first PD step forward + adjoint per bench step"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": "first PD step of the Tet4 block rollout, forward then adjoint, per bench step"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(result), flush=True)
+
+
+def main():
+    parser = argparse.ArgumentParser()
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=5)
+    parser.add_argument("--warmup", type=int, default=3)
+    parser.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    parser.add_argument("--adjoint", choices=["reference", "exact"], default="exact")
+    parser.add_argument("--precision", choices=["fp64", "fp32+refine"], default="fp64")
+    parser.add_argument("--cpu-seconds", type=float, default=20.0)
+    parser.add_argument("--no-extras", action="store_true",
+                        help="skip the e2e, CPU-baseline and per-launch timing legs (profiling runs)")
+    args = parser.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -28,6 +28,14 @@ from . import meshes
 PARTICLE_FLAG_ACTIVE = 1
 
 
+def _normalize(device) -> torch.device:
+    """A CUDA device with an explicit index (``cuda`` means the current device)."""
+    device = torch.device(device)
+    if device.type == "cuda" and device.index is None:
+        device = torch.device("cuda", torch.cuda.current_device())
+    return device
+
+
 class State:
     """Particle state: positions, velocities and external forces."""
 
@@ -37,10 +45,16 @@ class State:
         self.particle_f = particle_f
 
     def requires_grad_(self, flag: bool = True) -> "State":
+        """Give every array a zeroed ``.grad`` buffer, as Warp arrays with ``requires_grad``.
+
+        The tensors stay plain (no autograd graph); the solver's backward pass
+        accumulates into their ``.grad`` directly.
+        """
         for tensor in (self.particle_q, self.particle_qd, self.particle_f):
-            tensor.requires_grad_(flag)
             if flag and tensor.grad is None:
                 tensor.grad = torch.zeros_like(tensor)
+            elif not flag:
+                tensor.grad = None
         return self
 
 
@@ -53,7 +67,7 @@ class Control:
 
 class Model:
     def __init__(self, device: str | torch.device = "cuda"):
-        self.device = torch.device(device)
+        self.device = _normalize(device)
         self.particle_q = None
         self.particle_qd = None
         self.particle_inv_mass = None
@@ -138,7 +152,7 @@ class ModelBuilder:
         self._poses.extend(poses)
 
     def finalize(self, device="cuda", requires_grad: bool = False) -> Model:
-        device = torch.device(device)
+        device = _normalize(device)
         model = Model(device)
         q = np.asarray(self.particle_q, dtype=np.float32).reshape(-1, 3)
         model.particle_q = torch.tensor(q, device=device)
@@ -156,6 +170,5 @@ class ModelBuilder:
             model.tet_activations = torch.zeros(len(self.tet_indices), dtype=torch.float32, device=device)
         model.requires_grad = requires_grad
         if requires_grad and model.tet_materials is not None:
-            model.tet_materials.requires_grad_(True)
             model.tet_materials.grad = torch.zeros_like(model.tet_materials)
         return model

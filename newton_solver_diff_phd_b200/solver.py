@@ -421,6 +421,9 @@ class SolverDiffPhD:
         self._nh_mu = float(materials[:, 0].mean())
         self._nh_lame = float(materials[:, 1].mean())
         self._inertia = self.particle_mass / dt**2
+        self._gravity = np.ascontiguousarray(
+            self.model.gravity[self._gravity_world].detach().cpu().numpy().astype(np.float64)
+        )
         self._factor_key = dt
         self._model_changed = False
 
@@ -517,8 +520,13 @@ class SolverDiffPhD:
             self._targets_host = targets.copy()
             _lib.check(self._lib.pd_set_muscle_targets(self._handle, _lib.ptr(np.ascontiguousarray(targets))))
 
-    def step(self, state_in, state_out, control, contacts, dt: float, *, dirichlet_positions=None) -> None:
-        """Advance one step of length ``dt`` [s] on the current CUDA stream."""
+    def step(self, state_in, state_out, control, contacts, dt: float, *, dirichlet_positions=None,
+             record: torch.Tensor | None = None) -> None:
+        """Advance one step of length ``dt`` [s] on the current CUDA stream.
+
+        ``record`` (added): an optional float64 ``(N, 3)`` device tensor that
+        receives the converged positions for :meth:`backward_step`.
+        """
         if contacts is not None:
             raise NotImplementedError("SolverDiffPhD does not consume Newton contacts; pass contacts=None")
         if not np.isfinite(dt) or dt <= 0:
@@ -547,7 +555,7 @@ class SolverDiffPhD:
         self._sync_hex_targets()
         activations = self._activations(control)
         _lib.check(self._lib.pd_set_activations(self._handle, _lib.ptr(activations)))
-        gravity = self.model.gravity[self._gravity_world].detach().cpu().numpy().astype(np.float64)
+        gravity = self._gravity
         q = state_in.particle_q.detach()
         qd = state_in.particle_qd.detach()
         f = state_in.particle_f.detach()
@@ -562,14 +570,15 @@ class SolverDiffPhD:
                 _lib.ptr(qd),
                 _lib.ptr(f),
                 _lib.ptr(dirichlet),
-                _lib.ptr(np.ascontiguousarray(gravity)),
+                _lib.ptr(gravity),
                 dt,
                 _lib.ptr(state_out.particle_q.detach()),
                 _lib.ptr(state_out.particle_qd.detach()),
-                _lib.ptr(self._x),
+                _lib.ptr(self._x if record is None else record),
                 _stream(),
             )
         )
+        self._last_record = self._x if record is None else record
         if tape is not None:
             self._record(tape, state_in, state_out, activations, dirichlet_positions, dt)
 
@@ -585,7 +594,7 @@ class SolverDiffPhD:
         self._recorded = tape
 
     def _record(self, tape, state_in, state_out, activations, dirichlet_positions, dt):
-        x_record = self._x.clone()
+        x_record = self._last_record.clone()
         factor_key = self._factor_key
         materials = self.model.tet_materials if self._hex is None else self.hex_materials
         activation_source = None
@@ -625,8 +634,13 @@ class SolverDiffPhD:
         gf = _grad(state_in.particle_f)
         gdirichlet = _grad(dirichlet_positions) if dirichlet_positions is not None else None
         material_grad = None
-        if materials is not None and materials.requires_grad and materials.grad is not None:
-            material_grad = torch.zeros((self._element_count, 2), dtype=torch.float64, device=self.device)
+        direct = False
+        if materials is not None and materials.grad is not None:
+            grad = materials.grad
+            direct = (grad.dtype == torch.float64 and tuple(grad.shape) == (self._element_count, 2)
+                      and grad.is_contiguous())
+            material_grad = grad if direct else torch.zeros((self._element_count, 2), dtype=torch.float64,
+                                                            device=self.device)
         _lib.check(
             self._lib.pd_backward(
                 self._handle,
@@ -644,7 +658,7 @@ class SolverDiffPhD:
                 _stream(),
             )
         )
-        if material_grad is not None:
+        if material_grad is not None and not direct:
             materials.grad[:, :2] += material_grad.to(materials.grad.dtype)
 
     def __del__(self):

@@ -1,0 +1,122 @@
+"""CPU port of the reference's sparse DiffPhD path, used as the timed CPU baseline.
+
+TEST INFRASTRUCTURE ONLY (imported by tests/ and by bench.py's CPU-baseline
+leg). It follows the reference's CPU code path step for step: the local step
+over all elements, the fixed-order gather, ``x = S^T (S b)`` with the exact
+inverse factor (``sparse.py:322-352``), Dirichlet values, type-II Anderson
+with a ring history (``anderson.py``), the dual stopping gate
+(``kernels.py:294-347``), and the backward fixed point ``mu <- A^{-1}(g + K mu)``
+with Anderson and the dual-norm stop (``adjoint.py:927-964, 1054-1086``).
+
+The reference's own CPU path (Warp CPU kernels) needs warp-lang and newton,
+which are not installed; this port runs the same algorithm with NumPy/SciPy
+(SpMV in SciPy's compiled CSR kernels, projections vectorised over elements).
+The factor arrays come from the caller (they are bit-identical to the
+reference's ``sparse.py`` output).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import scipy.sparse as sp
+
+from . import pd_oracle
+
+
+class SparsePort:
+    def __init__(self, body: pd_oracle.Body, factor: dict, dt: float, window: int = 5):
+        n = body.n
+        self.body = body
+        self.dt = dt
+        self.window = window
+        self.inertia = body.mass / dt**2
+        self.s = sp.csr_matrix((factor["s_values"], factor["s_columns"], factor["s_offsets"]), shape=(n, n))
+        self.st = sp.csr_matrix((factor["st_values"], factor["st_columns"], factor["st_offsets"]), shape=(n, n))
+
+    def solve(self, rhs):
+        return self.st @ (self.s @ rhs)
+
+    def _anderson(self):
+        return {"x": [], "g": []}
+
+    @staticmethod
+    def _mix(history, x, previous, window):
+        g = x - previous
+        history["x"].append(previous)
+        history["g"].append(g)
+        m = len(history["g"]) - 1
+        if m >= 1:
+            dg = np.stack([(history["g"][i + 1] - history["g"][i]).ravel() for i in range(m)], axis=1)
+            dx = np.stack([(history["x"][i + 1] - history["x"][i]).ravel() for i in range(m)], axis=1)
+            gram = dg.T @ dg
+            gram += max(1.0e-6 * np.trace(gram) / m, 1.0e-12) * np.eye(m)
+            gamma = np.linalg.solve(gram, dg.T @ g.ravel())
+            if np.linalg.norm(gamma) >= 10.0:
+                history["x"].clear()
+                history["g"].clear()
+            else:
+                x = ((previous + g).ravel() - (dx + dg) @ gamma).reshape(-1, 3)
+        del history["x"][:-window]
+        del history["g"][:-window]
+        return x
+
+    def step(self, q, v, f_ext, gravity, *, max_iterations, abs_tol, rel_tol, boundary=None, targets=None):
+        body, dt = self.body, self.dt
+        q = np.asarray(q, dtype=np.float64)
+        v = np.asarray(v, dtype=np.float64)
+        free = body.free
+        if boundary is None:
+            boundary = np.where(free[:, None], 0.0, q)
+        q_tilde = q + dt * v + dt**2 * (np.asarray(f_ext, np.float64) / body.mass + np.asarray(gravity, np.float64))
+        x = q.copy()
+        previous_p = np.zeros_like(x)
+        history = self._anderson()
+        for iteration in range(max_iterations):
+            previous = x
+            p = body.projection_rhs(x, boundary, targets)
+            x = self.solve(self.inertia * q_tilde + p)
+            x[~free] = boundary[~free]
+            if self.window:
+                x = self._mix(history, x, previous, self.window)
+            x[~free] = boundary[~free]
+            step_norm = np.linalg.norm(x - previous)
+            change = np.linalg.norm(p - previous_p)
+            done = (iteration > 0 and step_norm <= rel_tol * np.linalg.norm(previous) + abs_tol
+                    and change <= rel_tol * np.linalg.norm(previous_p) + abs_tol)
+            previous_p = p
+            if done:
+                return x, iteration + 1, True
+        return x, max_iterations, False
+
+    def backward(self, x_next, dl_dq, dl_dv, *, max_iterations, abs_tol, rel_tol, targets=None, mode="reference"):
+        """Adjoint fixed point of one step; returns ``mu`` and the material gradient."""
+        body, dt = self.body, self.dt
+        free = body.free
+        k_matrix = sp.csr_matrix(pd_oracle.stiffness_matrix_blocks(body, x_next, targets, mode))
+        rhs = np.asarray(dl_dq, np.float64) + np.asarray(dl_dv, np.float64) / dt
+        solution = np.zeros_like(rhs)
+        history = self._anderson()
+        for iteration in range(max_iterations):
+            previous = solution
+            work = rhs + (k_matrix @ solution.ravel()).reshape(-1, 3)
+            raw = self.solve(work)
+            raw[~free] = 0.0
+            step_norm = np.linalg.norm(raw - previous)
+            if self.window:
+                raw = self._mix(history, raw, previous, self.window)
+            raw[~free] = 0.0
+            solution = raw
+            if iteration > 0 and step_norm < rel_tol * np.linalg.norm(raw) + abs_tol:
+                break
+        f = body.deformation(x_next)
+        material = np.zeros((len(body.elements), 2))
+        for name, _weight in body.energies():
+            if name == "corotated":
+                stress = f - pd_oracle.corotated(f)
+            elif name == "volume":
+                stress = f - pd_oracle.volume_projection(f)
+            else:
+                continue
+            value = -np.einsum("eki,esij,eskj,es->e", solution[body.elements], stress, body.gradients, body.sample_volume)
+            material[:, 1 if name == "volume" else 0] += value if name == "volume" else 2.0 * value
+        return solution, material, iteration + 1

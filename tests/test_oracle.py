@@ -1,0 +1,98 @@
+"""The oracle restatement against the reference's own outputs (tests/golden)."""
+
+import numpy as np
+import pytest
+
+from newton_solver_diff_phd_b200 import meshes
+from oracle import pd_oracle
+from tests.helpers import golden
+
+
+def _tet_fixture():
+    vertices, tets, _ = meshes.tet_grid(3, 2, 2, 0.1, origin=(0.0, 0.0, 1.0))
+    return vertices, tets, meshes.tet_rest_poses(vertices, tets), vertices[:, 0] > 0
+
+
+GRAVITY = np.array([0.0, 0.0, -9.81], dtype=np.float32).astype(np.float64)
+
+
+@pytest.mark.parametrize("contrast,material,label", [
+    (1.0, "pd", "fixed"), (1.0, "pd", "converged"), (1.0, "neo_hookean", "fixed"), (1.0, "neo_hookean", "converged"),
+    (10.0, "pd", "converged"), (10.0, "neo_hookean", "converged"), (100.0, "pd", "converged"),
+    (100.0, "neo_hookean", "converged"),
+])
+def test_tet_forward_matches_reference_oracle(contrast, material, label):
+    g = golden("tet_forward.npz")
+    vertices, tets, poses, free = _tet_fixture()
+    c = f"c{int(contrast)}"
+    key = f"{c}_{material}_{label}"
+    options = g[key + "__options"]
+    body = pd_oracle.Body.tet(tets, poses, free, g[c + "__mu"], g[c + "__lame"], 1000.0, material=material)
+    x, iterations, converged = pd_oracle.step(
+        body, g[c + "__q"], g[c + "__v"], np.zeros((len(vertices), 3)), GRAVITY, 0.004,
+        max_iterations=int(options[0]), abs_tol=float(options[1]), rel_tol=float(options[2]),
+    )
+    reference = g[key + "__x"]
+    np.testing.assert_allclose(x, reference, rtol=0.0, atol=1.0e-10 * np.abs(reference).max())
+    assert iterations == int(g[key + "__iterations"])
+    assert converged == bool(g[key + "__converged"])
+
+
+def test_tet_muscle_forward_matches_reference_oracle():
+    g = golden("tet_forward.npz")
+    vertices, tets, poses, free = _tet_fixture()
+    body = pd_oracle.Body.tet(
+        tets, poses, free, g["c1__mu"], g["c1__lame"], 1000.0,
+        muscle_directions=g["muscle__directions"], muscle_stiffness=g["muscle__stiffness"],
+    )
+    x, _, converged = pd_oracle.step(
+        body, g["muscle__q"], g["muscle__v"], np.zeros((len(vertices), 3)), [0.0, 0.0, -9.81], 0.004,
+        max_iterations=500, abs_tol=1e-11, rel_tol=1e-10, targets=1.0 - g["muscle__contraction"].astype(np.float64),
+    )
+    assert converged
+    np.testing.assert_allclose(x, g["muscle__x"], rtol=0.0, atol=1e-10 * np.abs(g["muscle__x"]).max())
+
+
+@pytest.mark.parametrize("material", ["pd", "neo_hookean"])
+def test_hex_forward_matches_reference_hex_oracle(material):
+    h = golden("hex_forward.npz")
+    elements = np.array([np.arange(8), np.arange(4, 12)])
+    body = pd_oracle.Body.hex(
+        h["vertices"], elements, np.arange(12) >= 4, h["materials"][:, 0], h["materials"][:, 1], 1000.0,
+        material=material, muscle_directions=[[1.0, 0, 0], [0, 1.0, 0]], muscle_stiffness=[1000.0, 300.0],
+        planes=(np.array([0, 8, 9]), 120.0, (0.0, 0.0, 2.0, -0.08)),
+    )
+    x, iterations, _ = pd_oracle.step(
+        body, h["q"], h["v"], h["f"], np.zeros(3), 0.003, max_iterations=1000, abs_tol=1e-12, rel_tol=1e-10,
+        window=0, targets=np.array([0.0, 0.8]),
+    )
+    np.testing.assert_allclose(x, h[material + "__x"], rtol=0, atol=1e-12)
+    assert iterations == int(h[material + "__iterations"])
+    np.testing.assert_allclose(np.linalg.inv(body.matrix(0.003)), h[material + "__inverse"], rtol=1e-12, atol=1e-16)
+
+
+@pytest.mark.parametrize("key", ["c2_pd", "c1_pd", "c1_neo_hookean"])
+def test_backward_matches_reference_backward(key):
+    b = golden("tet_backward.npz")
+    vertices, tets, poses, free = _tet_fixture()
+    material = key.split("_", 1)[1]
+    ml = b[key + "__mu_lame"]
+    body = pd_oracle.Body.tet(tets, poses, free, ml[:, 0], ml[:, 1], 1000.0, material=material)
+    out = pd_oracle.backward(body, b[key + "__x"], 0.004, b[key + "__gq"], b[key + "__gv"], mode="reference")
+    for name in ("mu", "q", "qd", "f", "materials"):
+        reference = b[key + "__out_" + name]
+        np.testing.assert_allclose(out[name], reference, rtol=0, atol=1e-8 * np.abs(reference).max())
+
+
+def test_projections_follow_unsigned_svd_conventions():
+    # diag(1, 0, 1): Eigen keeps U = V, so the polar factor is the identity (reference test :181-204).
+    f = np.diag([1.0, 0.0, 1.0])
+    np.testing.assert_allclose(pd_oracle.corotated(f[None])[0] @ pd_oracle.corotated(f[None])[0].T, np.eye(3), atol=1e-14)
+    # Reflections: U V^T has determinant -1 when det F < 0.
+    r = pd_oracle.corotated(np.diag([1.0, 1.0, -0.5])[None])[0]
+    assert abs(np.linalg.det(r) + 1.0) < 1e-12
+    # The volume projection lands on det = 1.
+    rng = np.random.default_rng(7)
+    mats = np.eye(3) + 0.3 * rng.standard_normal((16, 3, 3))
+    mats = mats[np.linalg.det(mats) > 0.1]
+    np.testing.assert_allclose(np.linalg.det(pd_oracle.volume_projection(mats)), 1.0, atol=1e-9)
