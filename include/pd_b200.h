@@ -153,6 +153,11 @@ int pd_backward(PdSolver* solver, const double* x_record, const float* activatio
                 const float* gqd_out, float* gq, float* gqd, float* gf, float* gdirichlet, double* gmaterials,
                 float* gactivations, void* stream);
 
+/* Device buffer of 8 uint64 nanosecond accumulators for the per-phase timers
+   of a library built with -DPD_PHASE_TIMERS (profiling); ignored otherwise.
+   NULL disables. */
+int pd_set_phase_timers(PdSolver* solver, unsigned long long* device_timers);
+
 /* Reads and clears the status word (read_status, solver.py:380-390). Synchronises the stream. */
 int pd_read_status(PdSolver* solver, int32_t* bits, void* stream);
 /* Iteration count of the last step and of the last backward fixed point. Synchronises the stream. */

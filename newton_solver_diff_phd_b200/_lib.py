@@ -7,12 +7,13 @@ path, and a missing library raises :class:`LibraryMissing` on first use.
 from __future__ import annotations
 
 import ctypes
+import os
 import threading
 from pathlib import Path
 
 import numpy as np
 
-LIBRARY = Path(__file__).resolve().parent / "_build" / "libpdb200.so"
+LIBRARY = Path(os.environ.get("PD_B200_LIBRARY", Path(__file__).resolve().parent / "_build" / "libpdb200.so"))
 
 PD_OK = 0
 PD_ERR_INVALID = 1
@@ -85,6 +86,7 @@ SIGNATURES = {
     "pd_factor_stats": ([_P, ctypes.POINTER(_I64), ctypes.POINTER(_I64), ctypes.POINTER(_I64)], ctypes.c_int),
     "pd_step": ([_P, _P, _P, _P, _P, _P, _D, _P, _P, _P, _P], ctypes.c_int),
     "pd_backward": ([_P, _P, _P, _D, _P, _P, _P, _P, _P, _P, _P, _P, _P], ctypes.c_int),
+    "pd_set_phase_timers": ([_P, _P], ctypes.c_int),
     "pd_read_status": ([_P, ctypes.POINTER(_I32), _P], ctypes.c_int),
     "pd_iterations": ([_P, ctypes.POINTER(_I32), ctypes.POINTER(_I32), _P], ctypes.c_int),
     "pd_deformation_determinants": ([_P, _P, _P, _P], ctypes.c_int),

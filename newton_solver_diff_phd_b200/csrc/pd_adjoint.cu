@@ -210,7 +210,7 @@ __device__ void adjoint_gram_partials(const AdjointArgs& b, int r0, int r1, int 
   if (t < entries) {
     double total = 0.0;
     for (int g = 0; g < groups; ++g) total += scratch[g * entries + t];
-    block_out[t] = total;
+    block_out[t * gridDim.x] = total;
   }
   __syncthreads();
 }
@@ -260,7 +260,7 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
   }
   const int s_r0 = b.s_part[blockIdx.x], s_r1 = b.s_part[blockIdx.x + 1];
   const int r0 = b.st_part[blockIdx.x], r1 = b.st_part[blockIdx.x + 1];
-  double* my_partials = b.partials + static_cast<size_t>(blockIdx.x) * kPartialStride;
+  double* my_partials = b.partials + blockIdx.x;  // slot-major: [slot * gridDim.x]
   const size_t hstride = static_cast<size_t>(3) * n;
   const double dt = b.dt;
 
@@ -279,7 +279,7 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
       rhs2 += dot(g, g);
     }
     rhs2 = block_sum(rhs2, s_scratch);
-    if (threadIdx.x == 0) my_partials[kSlotRhs] = rhs2;
+    if (threadIdx.x == 0) my_partials[(kSlotRhs) * gridDim.x] = rhs2;
   }
   for (int t = gtid; t < b.ne * samples; t += gthreads) {
     const int e = t / samples;
@@ -307,20 +307,47 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
     element_operator<TL>(b, s_grad, b.solution, 0, gtid, gthreads);
     if (!grid_sync(b.barrier, b.status)) return;
 
-    // ---- A2: work = g + gather(K solution) (refinement: minus A solution).
-    for (int i = gtid; i < n; i += gthreads) {
-      const V3<double> k = gather_row(b, i);
-      V3<double> w = k + load3d(b.rhs, i);
-      if (b.refine) {
-        for (int q = b.a_off[i]; q < b.a_off[i + 1]; ++q) {
-          const double v = b.a_val[q];
-          const int j = b.a_col[q];
-          w.x -= v * b.solution[3 * j];
-          w.y -= v * b.solution[3 * j + 1];
-          w.z -= v * b.solution[3 * j + 2];
+    // ---- A2: work = g + gather(K solution) (refinement: minus A solution),
+    // four lanes per particle with a fixed shuffle tree.
+    {
+      const int sub = threadIdx.x & 3;
+      const int groups_total = gthreads >> 2;
+      const int lane_group = (threadIdx.x & 31) >> 2;
+      for (int base = (gtid >> 5) * 8; base < n; base += groups_total) {
+        const int i = base + lane_group;
+        const bool valid = i < n;
+        double px = 0.0, py = 0.0, pz = 0.0;
+        if (valid) {
+          const int k0 = b.inc_offsets[i], k1 = b.inc_offsets[i + 1];
+#pragma unroll 4
+          for (int k = k0 + sub; k < k1; k += 4) {
+            const double* c = b.contrib + 3 * b.inc_entries[k];
+            px += c[0];
+            py += c[1];
+            pz += c[2];
+          }
+          if (b.refine) {
+            for (int q = b.a_off[i] + sub; q < b.a_off[i + 1]; q += 4) {
+              const double v = b.a_val[q];
+              const int j = b.a_col[q];
+              px -= v * b.solution[3 * j];
+              py -= v * b.solution[3 * j + 1];
+              pz -= v * b.solution[3 * j + 2];
+            }
+          }
+        }
+#pragma unroll
+        for (int mask = 1; mask < 4; mask <<= 1) {
+          px += __shfl_xor_sync(0xffffffffu, px, mask);
+          py += __shfl_xor_sync(0xffffffffu, py, mask);
+          pz += __shfl_xor_sync(0xffffffffu, pz, mask);
+        }
+        if (valid && sub == 0) {
+          b.work[3 * i] = px + b.rhs[3 * i];
+          b.work[3 * i + 1] = py + b.rhs[3 * i + 1];
+          b.work[3 * i + 2] = pz + b.rhs[3 * i + 2];
         }
       }
-      store3(b.work, i, w);
     }
     if (!grid_sync(b.barrier, b.status)) return;
 
@@ -373,12 +400,12 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
       raw2 = block_sum(raw2, s_scratch);
       step2 = block_sum(step2, s_scratch);
       if (threadIdx.x == 0) {
-        my_partials[kSlotRaw] = raw2;
-        my_partials[kSlotStep] = step2;
+        my_partials[(kSlotRaw) * gridDim.x] = raw2;
+        my_partials[(kSlotStep) * gridDim.x] = step2;
       }
       if (b.window > 0) {
         __syncthreads();
-        adjoint_gram_partials(b, r0, r1, count, start, my_partials + kSlotGram, s_scratch);
+        adjoint_gram_partials(b, r0, r1, count, start, my_partials + kSlotGram * gridDim.x, s_scratch);
       }
       // Serial: norm clip of the solve result (safe_clip, adjoint.py:184-223);
       // without clipping also the Anderson solve and the step norm.
@@ -420,10 +447,10 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
         }
       }
       step2 = block_sum(step2, s_scratch);
-      if (threadIdx.x == 0) my_partials[kSlotStep] = step2;
+      if (threadIdx.x == 0) my_partials[(kSlotStep) * gridDim.x] = step2;
       if (b.window > 0) {
         __syncthreads();
-        adjoint_gram_partials(b, r0, r1, count, start, my_partials + kSlotGram, s_scratch);
+        adjoint_gram_partials(b, r0, r1, count, start, my_partials + kSlotGram * gridDim.x, s_scratch);
       }
       unsigned generation;
       if (barrier_arrive(b.barrier, generation)) {
@@ -467,7 +494,7 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
         mixed2 += dot(value, value);
       }
       mixed2 = block_sum(mixed2, s_scratch);
-      if (threadIdx.x == 0) my_partials[kSlotMixed] = mixed2;
+      if (threadIdx.x == 0) my_partials[(kSlotMixed) * gridDim.x] = mixed2;
       unsigned generation;
       if (barrier_arrive(b.barrier, generation)) {
         reduce_partials(b.partials, kSlotMixed, 1, gridDim.x, s_reduced, s_scratch);
@@ -626,9 +653,9 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
   material1 = block_sum(material1, s_scratch);
   activation = block_sum(activation, s_scratch);
   if (threadIdx.x == 0) {
-    my_partials[kSlotMaterial] = material0;
-    my_partials[kSlotMaterial + 1] = material1;
-    my_partials[kSlotActivation] = activation;
+    my_partials[(kSlotMaterial) * gridDim.x] = material0;
+    my_partials[(kSlotMaterial + 1) * gridDim.x] = material1;
+    my_partials[(kSlotActivation) * gridDim.x] = activation;
   }
   // Parameter guard (adjoint.py:622-644).
   {

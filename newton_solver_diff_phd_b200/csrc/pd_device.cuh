@@ -17,7 +17,7 @@ namespace pdb200 {
 
 constexpr int kBlock = 256;
 constexpr int kWarps = kBlock / 32;
-constexpr int kPartialStride = 64;  // doubles of per-block partial sums
+constexpr int kPartialStride = 64;  // partial-sum slots per block
 constexpr int kMaxWindow = 8;
 // Poll budget of one barrier wait (~2^26 polls of >= 32 ns: seconds, far
 // beyond any legitimate phase).
@@ -124,26 +124,27 @@ __device__ __forceinline__ double block_sum(double v, double* scratch /* [kWarps
   return total;
 }
 
-// Sums `count` per-block partials (at partials[b*kPartialStride + offset + e])
-// over all blocks in a fixed order. Uses the whole block; results land in
-// out[0..count) (shared memory) for every thread after the call.
+// Per-block partial sums live slot-major: partials[slot * blocks + block], so
+// the partials of one slot over all blocks are contiguous.
+__device__ __forceinline__ double* partial_slot(double* partials, int slot) { return partials + slot * gridDim.x; }
+
+// Sums slots [offset, offset + count) over all blocks in a fixed order: one
+// warp per slot, lanes strided over blocks (coalesced, all loads in flight),
+// then a fixed shuffle tree. Uses the whole block; results land in out[0..count)
+// (shared memory) for every thread after the call.
 __device__ __forceinline__ void reduce_partials(const double* partials, int offset, int count, int blocks,
                                                 double* out /* shared [count] */,
-                                                double* scratch /* shared [kBlock] */) {
-  const int groups = count > 0 ? kBlock / count : 0;
-  const int t = threadIdx.x;
-  double sum = 0.0;
-  if (count > 0 && t < groups * count) {
-    const int entry = t % count;
-    const int group = t / count;
-    for (int b = group; b < blocks; b += groups) sum += partials[b * kPartialStride + offset + entry];
-  }
-  scratch[t] = sum;
-  __syncthreads();
-  if (t < count) {
-    double total = 0.0;
-    for (int g = 0; g < groups; ++g) total += scratch[g * count + t];
-    out[t] = total;
+                                                double* scratch /* unused, kept for the call sites */) {
+  (void)scratch;
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  for (int slot = warp; slot < count; slot += kWarps) {
+    const double* row = partials + (offset + slot) * blocks;
+    double sum = 0.0;
+#pragma unroll 8
+    for (int b = lane; b < blocks; b += 32) sum += row[b];
+    sum = warp_sum(sum);
+    if (lane == 0) out[slot] = sum;
   }
   __syncthreads();
 }
@@ -218,7 +219,8 @@ struct StepArgs {
   int* aa_state;    // count, start, count_used, start_used
   double* aa_gamma; // [kMaxWindow]
   int* aa_accept;
-  double* partials; // [blocks][kPartialStride]
+  double* partials; // [kPartialStride][blocks], slot-major
+  unsigned long long* timers;  // optional phase timers (PD_PHASE_TIMERS builds)
   // Loop control
   int* iteration;
   int* active;

@@ -284,7 +284,7 @@ inline __device__ void gram_partials(const StepArgs& a, int r0, int r1, int coun
   if (t < entries) {
     double total = 0.0;
     for (int g = 0; g < groups; ++g) total += scratch[g * entries + t];
-    block_out[t] = total;
+    block_out[t * gridDim.x] = total;
   }
   __syncthreads();
 }
@@ -385,17 +385,23 @@ __device__ __forceinline__ V3<double> aa_apply_row(const StepArgs& a, int i, int
   const int capacity = a.window + 1;
   const size_t stride = static_cast<size_t>(3) * a.n;
   const int slot = (start + count) % capacity;
+  const double* hx = a.hist_x + 3 * static_cast<size_t>(i);
+  const double* hg = a.hist_g + 3 * static_cast<size_t>(i);
   V3<double> value;
 #pragma unroll
-  for (int c = 0; c < 3; ++c) value[c] = a.hist_x[slot * stride + 3 * i + c] + a.hist_g[slot * stride + 3 * i + c];
-  for (int k = 0; k < count; ++k) {
-    const int low = (start + k) % capacity;
-    const int high = (start + k + 1) % capacity;
+  for (int c = 0; c < 3; ++c) value[c] = hx[slot * stride + c] + hg[slot * stride + c];
+  // Fully unrolled and predicated so every history load is issued up front.
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const size_t h = high * stride + 3 * i + c;
-      const size_t l = low * stride + 3 * i + c;
-      value[c] -= (a.hist_x[h] - a.hist_x[l] + a.hist_g[h] - a.hist_g[l]) * gamma[k];
+  for (int k = 0; k < kMaxWindow; ++k) {
+    if (k < count) {
+      const int low = (start + k) % capacity;
+      const int high = (start + k + 1) % capacity;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const size_t h = high * stride + c;
+        const size_t l = low * stride + c;
+        value[c] -= (hx[h] - hx[l] + hg[h] - hg[l]) * gamma[k];
+      }
     }
   }
   return value;

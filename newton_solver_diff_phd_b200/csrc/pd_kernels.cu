@@ -4,6 +4,30 @@
 #include "pd_forward.cuh"
 #include "pd_kernels.h"
 
+// Phase timers of the persistent loop (block 0, thread 0), compiled in only
+// with -DPD_PHASE_TIMERS; the timing probe builds such a variant.
+#ifdef PD_PHASE_TIMERS
+#define PD_TIMER(slot)                                                              \
+  do {                                                                             \
+    if (blockIdx.x == 0 && threadIdx.x == 0 && a.timers != nullptr) {             \
+      unsigned long long now_;                                                     \
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now_));                     \
+      a.timers[slot] += now_ - timer_last_;                                        \
+      timer_last_ = now_;                                                          \
+    }                                                                              \
+  } while (0)
+#define PD_TIMER_START()                                                           \
+  unsigned long long timer_last_ = 0;                                              \
+  if (blockIdx.x == 0 && threadIdx.x == 0) asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(timer_last_))
+#else
+#define PD_TIMER(slot) \
+  do {                 \
+  } while (0)
+#define PD_TIMER_START() \
+  do {                   \
+  } while (0)
+#endif
+
 namespace pdb200 {
 
 // One projective-dynamics step: prologue, every local/global iteration, epilogue.
@@ -69,9 +93,11 @@ __global__ void __launch_bounds__(kBlock) forward_step_kernel(const StepArgs a) 
 
   const int s_r0 = a.s_part[blockIdx.x], s_r1 = a.s_part[blockIdx.x + 1];
   const int r0 = a.st_part[blockIdx.x], r1 = a.st_part[blockIdx.x + 1];
-  double* my_partials = a.partials + static_cast<size_t>(blockIdx.x) * kPartialStride;
+  // This block's partial-sum slots: my_partials[slot * gridDim.x].
+  double* my_partials = a.partials + blockIdx.x;
   const size_t hstride = static_cast<size_t>(3) * n;
 
+  PD_TIMER_START();
   for (;;) {
     // ---- P1: local step.
     if (a.hex) {
@@ -79,58 +105,89 @@ __global__ void __launch_bounds__(kBlock) forward_step_kernel(const StepArgs a) 
     } else {
       local_step_tet<TL>(a, gtid, gthreads);
     }
+    PD_TIMER(0);
     if (!grid_sync(a.barrier, a.status)) return;
+    PD_TIMER(5);
 
     // ---- P2: fixed-order gather, vertex-plane energies, right-hand side.
-    for (int i = gtid; i < n; i += gthreads) {
-      double px = 0.0, py = 0.0, pz = 0.0;
-      for (int k = a.inc_offsets[i]; k < a.inc_offsets[i + 1]; ++k) {
-        const double* c = a.contrib + 3 * a.inc_entries[k];
-        px += c[0];
-        py += c[1];
-        pz += c[2];
-      }
-      if (a.plane_weight != nullptr) {
-        const double w = a.plane_weight[i];
-        if (w != 0.0) {
-          const double nx = a.plane[0], ny = a.plane[1], nz = a.plane[2];
-          const double xx = a.x[3 * i], xy = a.x[3 * i + 1], xz = a.x[3 * i + 2];
-          const double d = nx * xx + ny * xy + nz * xz + a.plane[3];
-          const double m = fmin(0.0, d);
-          px += w * ((xx - m * nx) - a.boundary[3 * i]);
-          py += w * ((xy - m * ny) - a.boundary[3 * i + 1]);
-          pz += w * ((xz - m * nz) - a.boundary[3 * i + 2]);
+    // Four lanes per particle: lane q sums entries q, q+4, ... of the
+    // particle's element-ordered incidence list; a fixed shuffle tree joins
+    // them, so the sum order is the same on every run.
+    {
+      const int sub = threadIdx.x & 3;
+      const int groups_total = gthreads >> 2;
+      const int lane_group = (threadIdx.x & 31) >> 2;
+      const int warp_first = (gtid >> 5) * 8;
+      for (int base = warp_first; base < n; base += groups_total) {
+        const int i = base + lane_group;
+        const bool valid = i < n;
+        double px = 0.0, py = 0.0, pz = 0.0;
+        double ax = 0.0, ay = 0.0, az = 0.0;
+        if (valid) {
+          const int k0 = a.inc_offsets[i], k1 = a.inc_offsets[i + 1];
+#pragma unroll 4
+          for (int k = k0 + sub; k < k1; k += 4) {
+            const double* c = a.contrib + 3 * a.inc_entries[k];
+            px += c[0];
+            py += c[1];
+            pz += c[2];
+          }
+          if (a.refine) {
+            for (int k = a.a_off[i] + sub; k < a.a_off[i + 1]; k += 4) {
+              const double v = a.a_val[k];
+              const int j = a.a_col[k];
+              ax += v * a.prev[3 * j];
+              ay += v * a.prev[3 * j + 1];
+              az += v * a.prev[3 * j + 2];
+            }
+          }
+        }
+#pragma unroll
+        for (int mask = 1; mask < 4; mask <<= 1) {
+          px += __shfl_xor_sync(0xffffffffu, px, mask);
+          py += __shfl_xor_sync(0xffffffffu, py, mask);
+          pz += __shfl_xor_sync(0xffffffffu, pz, mask);
+          if (a.refine) {
+            ax += __shfl_xor_sync(0xffffffffu, ax, mask);
+            ay += __shfl_xor_sync(0xffffffffu, ay, mask);
+            az += __shfl_xor_sync(0xffffffffu, az, mask);
+          }
+        }
+        if (valid && sub == 0) {
+          if (a.plane_weight != nullptr) {
+            const double w = a.plane_weight[i];
+            if (w != 0.0) {
+              const double nx = a.plane[0], ny = a.plane[1], nz = a.plane[2];
+              const double xx = a.x[3 * i], xy = a.x[3 * i + 1], xz = a.x[3 * i + 2];
+              const double d = nx * xx + ny * xy + nz * xz + a.plane[3];
+              const double m = fmin(0.0, d);
+              px += w * ((xx - m * nx) - a.boundary[3 * i]);
+              py += w * ((xy - m * ny) - a.boundary[3 * i + 1]);
+              pz += w * ((xz - m * nz) - a.boundary[3 * i + 2]);
+            }
+          }
+          a.proj[3 * i] = px;
+          a.proj[3 * i + 1] = py;
+          a.proj[3 * i + 2] = pz;
+          // Residual form with refinement: b - A x_prev, in float64.
+          a.rhs[3 * i] = a.inertia * a.target[3 * i] + px - ax;
+          a.rhs[3 * i + 1] = a.inertia * a.target[3 * i + 1] + py - ay;
+          a.rhs[3 * i + 2] = a.inertia * a.target[3 * i + 2] + pz - az;
         }
       }
-      a.proj[3 * i] = px;
-      a.proj[3 * i + 1] = py;
-      a.proj[3 * i + 2] = pz;
-      double bx = a.inertia * a.target[3 * i] + px;
-      double by = a.inertia * a.target[3 * i + 1] + py;
-      double bz = a.inertia * a.target[3 * i + 2] + pz;
-      if (a.refine) {
-        // Residual of the linear system at the current iterate, in float64.
-        for (int k = a.a_off[i]; k < a.a_off[i + 1]; ++k) {
-          const double v = a.a_val[k];
-          const int j = a.a_col[k];
-          bx -= v * a.prev[3 * j];
-          by -= v * a.prev[3 * j + 1];
-          bz -= v * a.prev[3 * j + 2];
-        }
-      }
-      a.rhs[3 * i] = bx;
-      a.rhs[3 * i + 1] = by;
-      a.rhs[3 * i + 2] = bz;
     }
+    PD_TIMER(1);
     if (!grid_sync(a.barrier, a.status)) return;
-
+    PD_TIMER(5);
     // ---- P3: y = S b.
     if (sizeof(TV) == sizeof(double)) {
       spmv_rows<double>(a.s_off, a.s_col, a.s_val, a.rhs, a.y, s_r0, s_r1);
     } else {
       spmv_rows<float>(a.s_off, a.s_col, a.s_val32, a.rhs, a.y, s_r0, s_r1);
     }
+    PD_TIMER(2);
     if (!grid_sync(a.barrier, a.status)) return;
+    PD_TIMER(5);
 
     // ---- P4: x = S^T y, Dirichlet values, Anderson history and Gram partials.
     if (sizeof(TV) == sizeof(double)) {
@@ -162,6 +219,7 @@ __global__ void __launch_bounds__(kBlock) forward_step_kernel(const StepArgs a) 
     if (a.window > 0) {
       __syncthreads();
       gram_partials(a, r0, r1, count, start, my_partials, s_scratch);
+      PD_TIMER(3);
       unsigned generation;
       if (barrier_arrive(a.barrier, generation)) {
         const int entries = gram_entries(count);
@@ -172,6 +230,7 @@ __global__ void __launch_bounds__(kBlock) forward_step_kernel(const StepArgs a) 
       } else if (!barrier_wait(a.barrier, generation, a.status)) {
         return;
       }
+      PD_TIMER(6);
     }
 
     // ---- P5: Anderson apply, Dirichlet re-imposition, convergence partials.
@@ -206,11 +265,12 @@ __global__ void __launch_bounds__(kBlock) forward_step_kernel(const StepArgs a) 
       prev2 = block_sum(prev2, s_scratch);
       change2 = block_sum(change2, s_scratch);
       proj2 = block_sum(proj2, s_scratch);
+      PD_TIMER(4);
       if (threadIdx.x == 0) {
-        my_partials[48] = step2;
-        my_partials[49] = prev2;
-        my_partials[50] = change2;
-        my_partials[51] = proj2;
+        my_partials[48 * gridDim.x] = step2;
+        my_partials[49 * gridDim.x] = prev2;
+        my_partials[50 * gridDim.x] = change2;
+        my_partials[51 * gridDim.x] = proj2;
       }
       unsigned generation;
       if (barrier_arrive(a.barrier, generation)) {
@@ -237,6 +297,7 @@ __global__ void __launch_bounds__(kBlock) forward_step_kernel(const StepArgs a) 
       } else if (!barrier_wait(a.barrier, generation, a.status)) {
         return;
       }
+      PD_TIMER(7);
       if (threadIdx.x == 0) s_control[0] = *reinterpret_cast<volatile int*>(a.active);
       __syncthreads();
       if (s_control[0] == 0) break;

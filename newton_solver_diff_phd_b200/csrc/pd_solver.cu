@@ -126,6 +126,7 @@ struct PdSolver {
   double nh_mu = 0.0, nh_lame = 0.0, nh_penalty = 0.0;
   int blocks = 0;
   int max_blocks = 0;
+  unsigned long long* timers = nullptr;  // phase timers of PD_PHASE_TIMERS builds
   InverseFactor factor;
   // Device mesh data.
   DeviceBuffer d_indices, d_gradients, d_free, d_inc_offsets, d_inc_entries, d_plane_weight;
@@ -670,6 +671,7 @@ int pd_step(PdSolver* s, const float* q, const float* qd, const float* f, const 
   a.inertia = s->inertia;
   for (int c = 0; c < 3; ++c) a.gravity[c] = gravity[c];
   a.integrate_pinned = s->options.integrate_pinned_velocities;
+  a.timers = s->timers;
   PD_CUDA(cudaMemsetAsync(s->d_barrier.ptr, 0, sizeof(pdb200::GridBarrier), st));
   PD_CUDA(pdb200::launch_forward_step(a, s->blocks, s->options.precision, st));
   return PD_OK;
@@ -779,6 +781,12 @@ int pd_backward(PdSolver* s, const double* x_record, const float* activations, d
   b.activations = (!s->hex && s->has_muscles) ? activations : nullptr;
   PD_CUDA(cudaMemsetAsync(s->d_barrier.ptr, 0, sizeof(pdb200::GridBarrier), st));
   PD_CUDA(pdb200::launch_adjoint_step(b, s->blocks, s->options.precision, st));
+  return PD_OK;
+}
+
+int pd_set_phase_timers(PdSolver* s, unsigned long long* device_timers) {
+  if (s == nullptr) return fail(PD_ERR_INVALID, "null solver");
+  s->timers = device_timers;
   return PD_OK;
 }
 

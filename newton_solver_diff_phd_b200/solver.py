@@ -332,6 +332,7 @@ class SolverDiffPhD:
         self._factor_key = None
         self._model_changed = True
         self._recorded = None
+        self._activation_source = None
 
     # ------------------------------------------------------------------ setup
     def _initialize_muscles(self, directions, stiffness):
@@ -510,6 +511,7 @@ class SolverDiffPhD:
             source = control.tet_activations
         if source is None or tuple(source.shape) != (len(self._tets),) or source.dtype != torch.float32:
             raise ValueError("Muscle activations must be a float32 (tet_count,) array")
+        self._activation_source = source
         return source.detach().contiguous()
 
     def _sync_hex_targets(self):
@@ -597,11 +599,8 @@ class SolverDiffPhD:
         x_record = self._last_record.clone()
         factor_key = self._factor_key
         materials = self.model.tet_materials if self._hex is None else self.hex_materials
-        activation_source = None
-        if activations is not None:
-            activation_source = self.model.tet_activations
-            # The control's tensor is the one whose gradient the user reads.
-            activation_source = activations
+        # The control's (or model's) tensor is the one whose gradient the user reads.
+        activation_source = self._activation_source if activations is not None else None
 
         def backward():
             if self._factor_key != factor_key or self._model_changed:
