@@ -171,6 +171,16 @@ int pd_deformation_determinants(PdSolver* solver, const float* q, double* out, v
    (SparseInverse.apply, sparse.py:350-352). */
 int pd_apply_inverse(PdSolver* solver, const double* rhs, double* out, void* stream);
 
+/* out = S^T (S rhs) without any allocation; no counterpart in the reference.
+   For callers that cannot allocate device memory when they solve (inside a
+   stream capture, under a host-owned allocator, in a real-time loop): the
+   intermediate vector lives in a file-scope device array of at most 65536
+   particles (1.5 MiB, resident on each GPU that loads the library until
+   exit). Rejects larger solvers with PD_ERR_INVALID. The first call on a
+   device resolves the array's address and must come before any stream
+   capture. All calls share the array: calls that overlap on the GPU race. */
+int pd_apply_inverse_static(PdSolver* solver, const double* rhs, double* out, void* stream);
+
 /* Host factor build for an arbitrary SPD matrix given as full symmetric CSR
    (SparseInverse.__init__, sparse.py:291-320). Arrays are host memory; the
    result is freed with pd_inverse_free. */

@@ -91,6 +91,7 @@ SIGNATURES = {
     "pd_iterations": ([_P, ctypes.POINTER(_I32), ctypes.POINTER(_I32), _P], ctypes.c_int),
     "pd_deformation_determinants": ([_P, _P, _P, _P], ctypes.c_int),
     "pd_apply_inverse": ([_P, _P, _P, _P], ctypes.c_int),
+    "pd_apply_inverse_static": ([_P, _P, _P, _P], ctypes.c_int),
     "pd_inverse_build": ([_I32, _P, _P, _P, ctypes.POINTER(_P)], ctypes.c_int),
     "pd_inverse_sizes": ([_P, ctypes.POINTER(_I32), ctypes.POINTER(_I64), ctypes.POINTER(_I64)], ctypes.c_int),
     "pd_inverse_export": ([_P, _P, _P, _P, _P, _P, _P, _P], ctypes.c_int),

@@ -836,6 +836,27 @@ int pd_apply_inverse(PdSolver* s, const double* rhs, double* out, void* stream) 
   return PD_OK;
 }
 
+}  // extern "C"
+
+// Internal hooks for pd_noalloc.cu (C++ linkage, not part of the ABI).
+int pd_internal_fail(int code, const char* message) { return fail(code, message); }
+
+int pd_internal_factor(PdSolver* s, int* device, int* rows, const int** s_off, const int** s_col, const double** s_val,
+                       const int** st_off, const int** st_col, const double** st_val) {
+  if (!s->built) return fail(PD_ERR_STATE, "the factor has not been built");
+  *device = s->device;
+  *rows = s->n;
+  *s_off = s->d_s_off.as<int>();
+  *s_col = s->d_s_col.as<int>();
+  *s_val = s->d_s_val.as<double>();
+  *st_off = s->d_st_off.as<int>();
+  *st_col = s->d_st_col.as<int>();
+  *st_val = s->d_st_val.as<double>();
+  return PD_OK;
+}
+
+extern "C" {
+
 struct PdInverseFactor {
   InverseFactor factor;
 };
