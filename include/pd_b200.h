@@ -81,6 +81,8 @@ typedef struct PdOptions {
   int32_t precision;         /* PD_PRECISION_* */
   int32_t adjoint_mode;      /* PD_ADJOINT_* */
   int32_t blocks;            /* persistent grid size; 0 = automatic */
+  int32_t resident;          /* 1: keep factor slices in shared memory when they fit (default) */
+  int32_t svd_warm_start;    /* 1: warm-start each sample's SVD from the previous iteration (default) */
 } PdOptions;
 
 /* Library identity and the message of the last failure on this thread. */

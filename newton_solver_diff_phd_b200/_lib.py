@@ -63,6 +63,8 @@ class PdOptions(ctypes.Structure):
         ("precision", ctypes.c_int32),
         ("adjoint_mode", ctypes.c_int32),
         ("blocks", ctypes.c_int32),
+        ("resident", ctypes.c_int32),
+        ("svd_warm_start", ctypes.c_int32),
     ]
 
 

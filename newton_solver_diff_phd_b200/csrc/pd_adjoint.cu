@@ -245,6 +245,7 @@ constexpr int kSlotActivation = 54;
 
 template <typename TL, typename TV>
 __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs b) {
+  extern __shared__ __align__(16) char dyn_smem[];
   __shared__ double s_grad[8 * 8 * 3];
   __shared__ double s_scratch[kBlock];
   __shared__ double s_reduced[64];
@@ -258,7 +259,6 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
     for (int t = threadIdx.x; t < 8 * 8 * 3; t += blockDim.x) s_grad[t] = b.gradients[t];
     __syncthreads();
   }
-  const int s_r0 = b.s_part[blockIdx.x], s_r1 = b.s_part[blockIdx.x + 1];
   const int r0 = b.st_part[blockIdx.x], r1 = b.st_part[blockIdx.x + 1];
   double* my_partials = b.partials + blockIdx.x;  // slot-major: [slot * gridDim.x]
   const size_t hstride = static_cast<size_t>(3) * n;
@@ -300,6 +300,15 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
     *b.iteration = 0;
     *b.active = 1;
   }
+  const TV* s_values = sizeof(TV) == sizeof(double) ? reinterpret_cast<const TV*>(b.s_val)
+                                                    : reinterpret_cast<const TV*>(b.s_val32);
+  const TV* st_values = sizeof(TV) == sizeof(double) ? reinterpret_cast<const TV*>(b.st_val)
+                                                     : reinterpret_cast<const TV*>(b.st_val32);
+  if (b.resident) {
+    load_slice<TV>(b.plan_s, s_values, dyn_smem);
+    load_slice<TV>(b.plan_st, st_values, dyn_smem);
+  }
+  double* vector_smem = reinterpret_cast<double*>(dyn_smem + b.vector_smem_offset);
   if (!grid_sync(b.barrier, b.status)) return;
 
   for (;;) {
@@ -352,18 +361,24 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
     if (!grid_sync(b.barrier, b.status)) return;
 
     // ---- A3: y = S work.
-    if (sizeof(TV) == sizeof(double)) {
-      spmv_rows<double>(b.s_off, b.s_col, b.s_val, b.work, b.y, s_r0, s_r1);
-    } else {
-      spmv_rows<float>(b.s_off, b.s_col, b.s_val32, b.work, b.y, s_r0, s_r1);
+    {
+      const double* in = b.work;
+      if (b.stage_vector) {
+        stage_vector(b.work, vector_smem, n);
+        in = vector_smem;
+      }
+      spmv_block<TV>(b.plan_s, s_values, b.resident != 0, dyn_smem, in, b.y);
     }
     if (!grid_sync(b.barrier, b.status)) return;
 
     // ---- A4: raw = S^T y; Dirichlet zeroing and scrub; history; partials.
-    if (sizeof(TV) == sizeof(double)) {
-      spmv_rows<double>(b.st_off, b.st_col, b.st_val, b.y, b.raw, r0, r1);
-    } else {
-      spmv_rows<float>(b.st_off, b.st_col, b.st_val32, b.y, b.raw, r0, r1);
+    {
+      const double* in = b.y;
+      if (b.stage_vector) {
+        stage_vector(b.y, vector_smem, n);
+        in = vector_smem;
+      }
+      spmv_block<TV>(b.plan_st, st_values, b.resident != 0, dyn_smem, in, b.raw);
     }
     __syncthreads();
     const int count = b.window > 0 ? b.aa_state[0] : 0;
@@ -708,17 +723,21 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
   }
 }
 
-cudaError_t launch_adjoint_step(const AdjointArgs& args, int blocks, int precision, cudaStream_t stream) {
-  void* params[] = {const_cast<AdjointArgs*>(&args)};
-  const void* kernel = precision == 0 ? reinterpret_cast<const void*>(&adjoint_step_kernel<double, double>)
-                                      : reinterpret_cast<const void*>(&adjoint_step_kernel<float, float>);
-  return cudaLaunchCooperativeKernel(kernel, dim3(blocks), dim3(kBlock), params, 0, stream);
+static const void* adjoint_kernel(int precision) {
+  return precision == 0 ? reinterpret_cast<const void*>(&adjoint_step_kernel<double, double>)
+                        : reinterpret_cast<const void*>(&adjoint_step_kernel<float, float>);
 }
 
-cudaError_t adjoint_step_max_blocks(int precision, int* blocks_per_sm) {
-  const void* kernel = precision == 0 ? reinterpret_cast<const void*>(&adjoint_step_kernel<double, double>)
-                                      : reinterpret_cast<const void*>(&adjoint_step_kernel<float, float>);
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kernel, kBlock, 0);
+cudaError_t launch_adjoint_step(const AdjointArgs& args, int blocks, int precision, size_t smem, cudaStream_t stream) {
+  void* params[] = {const_cast<AdjointArgs*>(&args)};
+  return cudaLaunchCooperativeKernel(adjoint_kernel(precision), dim3(blocks), dim3(kBlock), params, smem, stream);
+}
+
+cudaError_t adjoint_step_max_blocks(int precision, size_t smem, int* blocks_per_sm) {
+  const void* kernel = adjoint_kernel(precision);
+  cudaError_t status = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (status != cudaSuccess) return status;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kernel, kBlock, smem);
 }
 
 }  // namespace pdb200

@@ -39,19 +39,33 @@ struct GridBarrier {
 
 __device__ __forceinline__ unsigned load_volatile(const unsigned* p) { return *reinterpret_cast<const volatile unsigned*>(p); }
 
+__device__ __forceinline__ unsigned load_acquire(const unsigned* p) {
+  unsigned value;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(value) : "l"(p) : "memory");
+  return value;
+}
+__device__ __forceinline__ unsigned add_release(unsigned* p, unsigned value) {
+  unsigned old;
+  asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(value) : "memory");
+  return old;
+}
+__device__ __forceinline__ void store_release(unsigned* p, unsigned value) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(value) : "memory");
+}
+
 // Arrive at the grid barrier. Returns true in the block that arrived last;
 // that block must run its serial section and then call barrier_release().
-// Every other block must call barrier_wait().
+// Every other block must call barrier_wait(). The arrival is an acq_rel
+// atomic: this block's writes (ordered before it by __syncthreads and the
+// cumulative release) are visible to the block that observes the count.
 __device__ __forceinline__ bool barrier_arrive(GridBarrier* bar, unsigned& generation) {
   __shared__ int s_last;
   __shared__ unsigned s_generation;
   __syncthreads();
   if (threadIdx.x == 0) {
-    s_generation = load_volatile(&bar->generation);
-    __threadfence();
-    const unsigned arrived = atomicAdd(&bar->count, 1u) + 1u;
+    s_generation = load_acquire(&bar->generation);
+    const unsigned arrived = add_release(&bar->count, 1u) + 1u;
     s_last = arrived == gridDim.x;
-    if (s_last) __threadfence();
   }
   __syncthreads();
   generation = s_generation;
@@ -62,8 +76,7 @@ __device__ __forceinline__ void barrier_release(GridBarrier* bar, unsigned gener
   __syncthreads();
   if (threadIdx.x == 0) {
     atomicExch(&bar->count, 0u);
-    __threadfence();
-    atomicExch(&bar->generation, generation + 1u);
+    store_release(&bar->generation, generation + 1u);
   }
 }
 
@@ -73,7 +86,7 @@ __device__ __forceinline__ bool barrier_wait(GridBarrier* bar, unsigned generati
   if (threadIdx.x == 0) {
     int ok = 1;
     unsigned spins = 0;
-    while (load_volatile(&bar->generation) == generation) {
+    while (load_acquire(&bar->generation) == generation) {
       if (load_volatile(&bar->abort) != 0u) {
         ok = 0;
         break;
@@ -84,9 +97,8 @@ __device__ __forceinline__ bool barrier_wait(GridBarrier* bar, unsigned generati
         ok = 0;
         break;
       }
-      __nanosleep(32);
+      if (spins > 256) __nanosleep(20);
     }
-    __threadfence();
     s_ok = ok;
   }
   __syncthreads();
@@ -160,6 +172,27 @@ __device__ __forceinline__ void store3(double* v, int i, V3<double> a) {
   v[3 * i + 2] = a.z;
 }
 
+// One sparse product (S or S^T) split into per-block row ranges.
+struct SpmvPlan {
+  const int* off;       // CSR row offsets (global)
+  const int* col;       // CSR columns
+  const double* val64;  // CSR values (float64)
+  const float* val32;   // CSR values (float32 copy, fp32+refine)
+  const int* part;      // [blocks+1] row range of each block, balanced by nnz
+  const int* rowlist;   // rows of each block's range: short rows first (one thread each), then long rows (one warp each)
+  const int* nshort;    // [blocks] number of short rows of each block
+  int smem_offset;      // byte offset of this product's slice in dynamic shared memory (resident plans)
+  int max_nnz;          // largest per-block nnz (slice layout size)
+  int max_rows;         // largest per-block row count
+};
+
+// Shared-memory layout of one resident slice: values, columns, relative row
+// offsets, row list; every section 16-byte aligned.
+__host__ __device__ __forceinline__ int align16(int bytes) { return (bytes + 15) & ~15; }
+__host__ __device__ __forceinline__ int slice_bytes(int max_nnz, int max_rows, int value_bytes) {
+  return align16(max_nnz * value_bytes) + align16(max_nnz * 4) + align16((max_rows + 1) * 4) + align16(max_rows * 4);
+}
+
 // Everything one persistent launch needs. Passed by value as kernel argument.
 struct StepArgs {
   // Mesh
@@ -196,6 +229,13 @@ struct StepArgs {
   const float* st_val32;
   const int* s_part;   // [blocks+1] S row partition
   const int* st_part;  // [blocks+1] S^T row partition (also owns particle rows)
+  SpmvPlan plan_s;
+  SpmvPlan plan_st;
+  int resident;        // 1: factor slices live in dynamic shared memory for the launch
+  int stage_vector;    // 1: the SpMV input vector is staged in shared memory
+  int vector_smem_offset;
+  double* svd_u;       // warm-start singular vectors per element sample [E*S][9] (or nullptr)
+  double* svd_v;
   const int* a_off;    // constant matrix A (refinement residual)
   const int* a_col;
   const double* a_val;

@@ -41,8 +41,44 @@ __device__ __forceinline__ void tet_deformation(const StepArgs& a, int e, const 
 }
 
 // Projection stress sum_energies w (P(F) - F_D) of one element sample.
+// SVD of F, warm-started from the singular vectors of the same sample in the
+// previous iteration of this step: B = U0^T F V0 is nearly diagonal, so the
+// Jacobi sweeps on B converge in one rotation sweep; U = U0 Ub, V = V0 Vb. The
+// first iteration of a step starts cold (Eigen's conventions on F itself).
 template <typename TL>
-__device__ __forceinline__ M3<TL> sample_stress(const StepArgs& a, int e, const M3<TL>& f, const M3<TL>& fd) {
+__device__ __forceinline__ void sample_svd(const StepArgs& a, int sample, bool warm, const M3<TL>& f, M3<TL>& u,
+                                           V3<TL>& sigma, M3<TL>& v) {
+  if (a.svd_u == nullptr || sample < 0) {
+    unsigned_svd(f, u, sigma, v);
+    return;
+  }
+  double* su = a.svd_u + 9 * static_cast<size_t>(sample);
+  double* sv = a.svd_v + 9 * static_cast<size_t>(sample);
+  if (warm) {
+    M3<TL> u0, v0;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      u0.a[k / 3][k % 3] = static_cast<TL>(su[k]);
+      v0.a[k / 3][k % 3] = static_cast<TL>(sv[k]);
+    }
+    const M3<TL> b = mul(mul(transpose(u0), f), v0);
+    M3<TL> ub, vb;
+    unsigned_svd(b, ub, sigma, vb);
+    u = mul(u0, ub);
+    v = mul(v0, vb);
+  } else {
+    unsigned_svd(f, u, sigma, v);
+  }
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    su[k] = static_cast<double>(u.a[k / 3][k % 3]);
+    sv[k] = static_cast<double>(v.a[k / 3][k % 3]);
+  }
+}
+
+template <typename TL>
+__device__ __forceinline__ M3<TL> sample_stress(const StepArgs& a, int e, int sample, bool warm, const M3<TL>& f,
+                                                const M3<TL>& fd) {
   M3<TL> stress = zero3<TL>();
   const TL wc = static_cast<TL>(a.wc[e]);
   const TL wv = static_cast<TL>(a.wv[e]);
@@ -50,7 +86,7 @@ __device__ __forceinline__ M3<TL> sample_stress(const StepArgs& a, int e, const 
   if (wc != TL(0) || wv != TL(0) || wn != TL(0)) {
     M3<TL> u, v;
     V3<TL> sigma;
-    unsigned_svd(f, u, sigma, v);
+    sample_svd<TL>(a, sample, warm, f, u, sigma, v);
     if (wc != TL(0)) stress = stress + wc * (mul(u, transpose(v)) - fd);
     if (wv != TL(0)) {
       bool singular;
@@ -77,12 +113,12 @@ __device__ __forceinline__ M3<TL> sample_stress(const StepArgs& a, int e, const 
 
 // P1 for Tet4: one thread per element.
 template <typename TL>
-__device__ void local_step_tet(const StepArgs& a, int gtid, int gthreads) {
+__device__ void local_step_tet(const StepArgs& a, bool warm, int gtid, int gthreads) {
   for (int e = gtid; e < a.ne; e += gthreads) {
     M3<TL> f, fd;
     tet_deformation<TL>(a, e, a.x, f);
     tet_deformation<TL>(a, e, a.boundary, fd);
-    const M3<TL> stress = sample_stress<TL>(a, e, f, fd);
+    const M3<TL> stress = sample_stress<TL>(a, e, e, warm, f, fd);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       const double* g = a.gradients + (4 * e + k) * 3;
@@ -100,7 +136,7 @@ __device__ void local_step_tet(const StepArgs& a, int gtid, int gthreads) {
 // contributions sum_s stress_s g_sj are reduce-scattered across the eight
 // lanes with shuffles (fixed tree), so lane s ends with corner j = s.
 template <typename TL>
-__device__ void local_step_hex(const StepArgs& a, const double* grad_smem, int gtid, int gthreads) {
+__device__ void local_step_hex(const StepArgs& a, const double* grad_smem, bool warm, int gtid, int gthreads) {
   const int lane = threadIdx.x & 31;
   const int s = lane & 7;
   const int group_in_warp = lane >> 3;
@@ -136,7 +172,8 @@ __device__ void local_step_hex(const StepArgs& a, const double* grad_smem, int g
         f.a[r][c] = static_cast<TL>(fm[r][c]);
         fd.a[r][c] = static_cast<TL>(fdm[r][c]);
       }
-    const M3<TL> stress = sample_stress<TL>(a, ec, f, fd);
+    // Padding lanes (e >= ne) neither read nor write the warm-start state.
+    const M3<TL> stress = sample_stress<TL>(a, ec, valid ? 8 * ec + s : -1, warm, f, fd);
     // v[j] = stress_s g_sj for the eight corners.
     double vx[8], vy[8], vz[8];
 #pragma unroll
@@ -218,6 +255,110 @@ __device__ __forceinline__ void spmv_rows(const int* off, const int* col, const 
     sy = warp_sum(sy);
     sz = warp_sum(sz);
     if (lane == 0) {
+      out[3 * row] = sx;
+      out[3 * row + 1] = sy;
+      out[3 * row + 2] = sz;
+    }
+  }
+}
+
+// Copies this block's rows of one product into shared memory (once per launch).
+template <typename TV>
+__device__ void load_slice(const SpmvPlan& plan, const TV* global_values, char* smem) {
+  const int r0 = plan.part[blockIdx.x], r1 = plan.part[blockIdx.x + 1];
+  const int k0 = plan.off[r0], k1 = plan.off[r1];
+  const int nnz = k1 - k0, rows = r1 - r0;
+  char* base = smem + plan.smem_offset;
+  TV* val = reinterpret_cast<TV*>(base);
+  int* col = reinterpret_cast<int*>(base + align16(plan.max_nnz * static_cast<int>(sizeof(TV))));
+  int* off = col + align16(plan.max_nnz * 4) / 4;
+  int* rowlist = off + align16((plan.max_rows + 1) * 4) / 4;
+  for (int k = threadIdx.x; k < nnz; k += blockDim.x) {
+    val[k] = global_values[k0 + k];
+    col[k] = plan.col[k0 + k];
+  }
+  for (int r = threadIdx.x; r <= rows; r += blockDim.x) off[r] = plan.off[r0 + r] - k0;
+  for (int r = threadIdx.x; r < rows; r += blockDim.x) rowlist[r] = plan.rowlist[r0 + r] - r0;
+}
+
+// Copies a particle vector [n][3] float64 into shared memory.
+__device__ __forceinline__ void stage_vector(const double* vec, double* smem_vec, int n) {
+  const int count = 3 * n;
+  const double2* src = reinterpret_cast<const double2*>(vec);
+  double2* dst = reinterpret_cast<double2*>(smem_vec);
+  const int pairs = count / 2;
+#pragma unroll 4
+  for (int k = threadIdx.x; k < pairs; k += blockDim.x) dst[k] = src[k];
+  if ((count & 1) && threadIdx.x == 0) smem_vec[count - 1] = vec[count - 1];
+  __syncthreads();
+}
+
+// out = M vec for this block's rows of one product. Short rows (<= 32 nnz)
+// are summed sequentially by one thread, long rows by one warp (lane-strided,
+// fixed shuffle tree); each row always by the same unit, so the result is
+// bitwise reproducible. Slice data comes from shared memory when resident.
+template <typename TV>
+__device__ void spmv_block(const SpmvPlan& plan, const TV* global_values, bool resident, const char* smem,
+                           const double* vec, double* out) {
+  const int r0 = plan.part[blockIdx.x], r1 = plan.part[blockIdx.x + 1];
+  const int rows = r1 - r0;
+  const int nshort = plan.nshort[blockIdx.x];
+  // Resident: row ids, offsets and entries are relative to the block's first
+  // row and first entry. Global: absolute.
+  const TV* val;
+  const int* col;
+  const int* off;
+  const int* rowlist;
+  int row_shift;
+  if (resident) {
+    const char* base = smem + plan.smem_offset;
+    val = reinterpret_cast<const TV*>(base);
+    col = reinterpret_cast<const int*>(base + align16(plan.max_nnz * static_cast<int>(sizeof(TV))));
+    off = col + align16(plan.max_nnz * 4) / 4;
+    rowlist = off + align16((plan.max_rows + 1) * 4) / 4;
+    row_shift = r0;
+  } else {
+    val = global_values;
+    col = plan.col;
+    off = plan.off;
+    rowlist = plan.rowlist + r0;
+    row_shift = 0;
+  }
+  for (int t = threadIdx.x; t < nshort; t += blockDim.x) {
+    const int r = rowlist[t];
+    const int begin = off[r], end = off[r + 1];
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    for (int k = begin; k < end; ++k) {
+      const double value = static_cast<double>(val[k]);
+      const int c = col[k];
+      sx += value * vec[3 * c];
+      sy += value * vec[3 * c + 1];
+      sz += value * vec[3 * c + 2];
+    }
+    const int row = r + row_shift;
+    out[3 * row] = sx;
+    out[3 * row + 1] = sy;
+    out[3 * row + 2] = sz;
+  }
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  for (int w = nshort + warp; w < rows; w += kWarps) {
+    const int r = rowlist[w];
+    const int begin = off[r], end = off[r + 1];
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+#pragma unroll 4
+    for (int k = begin + lane; k < end; k += 32) {
+      const double value = static_cast<double>(val[k]);
+      const int c = col[k];
+      sx += value * vec[3 * c];
+      sy += value * vec[3 * c + 1];
+      sz += value * vec[3 * c + 2];
+    }
+    sx = warp_sum(sx);
+    sy = warp_sum(sy);
+    sz = warp_sum(sz);
+    if (lane == 0) {
+      const int row = r + row_shift;
       out[3 * row] = sx;
       out[3 * row + 1] = sy;
       out[3 * row + 2] = sz;

@@ -34,6 +34,7 @@ namespace pdb200 {
 // TL: precision of the local projections; TV: precision of the factor values.
 template <typename TL, typename TV>
 __global__ void __launch_bounds__(kBlock) forward_step_kernel(const StepArgs a) {
+  extern __shared__ __align__(16) char dyn_smem[];
   __shared__ double s_grad[8 * 8 * 3];
   __shared__ double s_scratch[kBlock];
   __shared__ double s_reduced[64];
@@ -89,21 +90,30 @@ __global__ void __launch_bounds__(kBlock) forward_step_kernel(const StepArgs a) 
     *a.iteration = 0;
     *a.active = 1;
   }
+  // Factor slices of this block stay in shared memory for the whole step.
+  const TV* s_values = sizeof(TV) == sizeof(double) ? reinterpret_cast<const TV*>(a.s_val)
+                                                    : reinterpret_cast<const TV*>(a.s_val32);
+  const TV* st_values = sizeof(TV) == sizeof(double) ? reinterpret_cast<const TV*>(a.st_val)
+                                                     : reinterpret_cast<const TV*>(a.st_val32);
+  if (a.resident) {
+    load_slice<TV>(a.plan_s, s_values, dyn_smem);
+    load_slice<TV>(a.plan_st, st_values, dyn_smem);
+  }
+  double* vector_smem = reinterpret_cast<double*>(dyn_smem + a.vector_smem_offset);
   if (!grid_sync(a.barrier, a.status)) return;
 
-  const int s_r0 = a.s_part[blockIdx.x], s_r1 = a.s_part[blockIdx.x + 1];
   const int r0 = a.st_part[blockIdx.x], r1 = a.st_part[blockIdx.x + 1];
   // This block's partial-sum slots: my_partials[slot * gridDim.x].
   double* my_partials = a.partials + blockIdx.x;
   const size_t hstride = static_cast<size_t>(3) * n;
 
   PD_TIMER_START();
-  for (;;) {
-    // ---- P1: local step.
+  for (int iter = 0;; ++iter) {
+    // ---- P1: local step (warm-started SVD after the first iteration).
     if (a.hex) {
-      local_step_hex<TL>(a, s_grad, gtid, gthreads);
+      local_step_hex<TL>(a, s_grad, iter > 0, gtid, gthreads);
     } else {
-      local_step_tet<TL>(a, gtid, gthreads);
+      local_step_tet<TL>(a, iter > 0, gtid, gthreads);
     }
     PD_TIMER(0);
     if (!grid_sync(a.barrier, a.status)) return;
@@ -180,20 +190,26 @@ __global__ void __launch_bounds__(kBlock) forward_step_kernel(const StepArgs a) 
     if (!grid_sync(a.barrier, a.status)) return;
     PD_TIMER(5);
     // ---- P3: y = S b.
-    if (sizeof(TV) == sizeof(double)) {
-      spmv_rows<double>(a.s_off, a.s_col, a.s_val, a.rhs, a.y, s_r0, s_r1);
-    } else {
-      spmv_rows<float>(a.s_off, a.s_col, a.s_val32, a.rhs, a.y, s_r0, s_r1);
+    {
+      const double* in = a.rhs;
+      if (a.stage_vector) {
+        stage_vector(a.rhs, vector_smem, n);
+        in = vector_smem;
+      }
+      spmv_block<TV>(a.plan_s, s_values, a.resident != 0, dyn_smem, in, a.y);
     }
     PD_TIMER(2);
     if (!grid_sync(a.barrier, a.status)) return;
     PD_TIMER(5);
 
     // ---- P4: x = S^T y, Dirichlet values, Anderson history and Gram partials.
-    if (sizeof(TV) == sizeof(double)) {
-      spmv_rows<double>(a.st_off, a.st_col, a.st_val, a.y, a.x, r0, r1);
-    } else {
-      spmv_rows<float>(a.st_off, a.st_col, a.st_val32, a.y, a.x, r0, r1);
+    {
+      const double* in = a.y;
+      if (a.stage_vector) {
+        stage_vector(a.y, vector_smem, n);
+        in = vector_smem;
+      }
+      spmv_block<TV>(a.plan_st, st_values, a.resident != 0, dyn_smem, in, a.x);
     }
     __syncthreads();
     const int count = a.window > 0 ? a.aa_state[0] : 0;
@@ -362,17 +378,21 @@ __global__ void hex_determinants_kernel(const float* q, const int* indices, cons
 // ---------------------------------------------------------------------------
 // Host launchers.
 
-cudaError_t launch_forward_step(const StepArgs& args, int blocks, int precision, cudaStream_t stream) {
-  void* params[] = {const_cast<StepArgs*>(&args)};
-  const void* kernel = precision == 0 ? reinterpret_cast<const void*>(&forward_step_kernel<double, double>)
-                                      : reinterpret_cast<const void*>(&forward_step_kernel<float, float>);
-  return cudaLaunchCooperativeKernel(kernel, dim3(blocks), dim3(kBlock), params, 0, stream);
+static const void* forward_kernel(int precision) {
+  return precision == 0 ? reinterpret_cast<const void*>(&forward_step_kernel<double, double>)
+                        : reinterpret_cast<const void*>(&forward_step_kernel<float, float>);
 }
 
-cudaError_t forward_step_max_blocks(int precision, int* blocks_per_sm) {
-  const void* kernel = precision == 0 ? reinterpret_cast<const void*>(&forward_step_kernel<double, double>)
-                                      : reinterpret_cast<const void*>(&forward_step_kernel<float, float>);
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kernel, kBlock, 0);
+cudaError_t launch_forward_step(const StepArgs& args, int blocks, int precision, size_t smem, cudaStream_t stream) {
+  void* params[] = {const_cast<StepArgs*>(&args)};
+  return cudaLaunchCooperativeKernel(forward_kernel(precision), dim3(blocks), dim3(kBlock), params, smem, stream);
+}
+
+cudaError_t forward_step_max_blocks(int precision, size_t smem, int* blocks_per_sm) {
+  const void* kernel = forward_kernel(precision);
+  cudaError_t status = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (status != cudaSuccess) return status;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kernel, kBlock, smem);
 }
 
 cudaError_t launch_apply_inverse(const int* s_off, const int* s_col, const double* s_val, const int* st_off,

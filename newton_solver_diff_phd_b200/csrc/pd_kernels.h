@@ -38,6 +38,11 @@ struct AdjointArgs {
   const float* st_val32;
   const int* s_part;
   const int* st_part;
+  SpmvPlan plan_s;
+  SpmvPlan plan_st;
+  int resident;
+  int stage_vector;
+  int vector_smem_offset;
   const int* a_off;
   const int* a_col;
   const double* a_val;
@@ -84,10 +89,10 @@ struct AdjointArgs {
   double dt, inertia;
 };
 
-cudaError_t launch_forward_step(const StepArgs& args, int blocks, int precision, cudaStream_t stream);
-cudaError_t forward_step_max_blocks(int precision, int* blocks_per_sm);
-cudaError_t launch_adjoint_step(const AdjointArgs& args, int blocks, int precision, cudaStream_t stream);
-cudaError_t adjoint_step_max_blocks(int precision, int* blocks_per_sm);
+cudaError_t launch_forward_step(const StepArgs& args, int blocks, int precision, size_t smem, cudaStream_t stream);
+cudaError_t forward_step_max_blocks(int precision, size_t smem, int* blocks_per_sm);
+cudaError_t launch_adjoint_step(const AdjointArgs& args, int blocks, int precision, size_t smem, cudaStream_t stream);
+cudaError_t adjoint_step_max_blocks(int precision, size_t smem, int* blocks_per_sm);
 cudaError_t launch_apply_inverse(const int* s_off, const int* s_col, const double* s_val, const int* st_off,
                                  const int* st_col, const double* st_val, int rows, const double* rhs, double* work,
                                  double* out, cudaStream_t stream);

@@ -97,6 +97,39 @@ std::vector<int32_t> partition_rows(const std::vector<int32_t>& offsets, int blo
   return bounds;
 }
 
+// Per-block row order for the SpMV: rows with at most kShortRow entries first
+// (one thread each), then the longer rows by decreasing length (one warp each).
+constexpr int kShortRow = 32;
+
+void plan_rows(const std::vector<int32_t>& offsets, const std::vector<int32_t>& part, std::vector<int32_t>& rowlist,
+               std::vector<int32_t>& nshort, int& max_nnz, int& max_rows) {
+  const int blocks = static_cast<int>(part.size()) - 1;
+  rowlist.assign(offsets.size() - 1, 0);
+  nshort.assign(blocks, 0);
+  max_nnz = 0;
+  max_rows = 0;
+  std::vector<int32_t> longs;
+  for (int b = 0; b < blocks; ++b) {
+    const int r0 = part[b], r1 = part[b + 1];
+    int cursor = r0;
+    longs.clear();
+    for (int r = r0; r < r1; ++r) {
+      if (offsets[r + 1] - offsets[r] <= kShortRow) {
+        rowlist[cursor++] = r;
+      } else {
+        longs.push_back(r);
+      }
+    }
+    nshort[b] = cursor - r0;
+    std::stable_sort(longs.begin(), longs.end(), [&](int x, int y) {
+      return offsets[x + 1] - offsets[x] > offsets[y + 1] - offsets[y];
+    });
+    for (int r : longs) rowlist[cursor++] = r;
+    max_nnz = std::max(max_nnz, offsets[r1] - offsets[r0]);
+    max_rows = std::max(max_rows, r1 - r0);
+  }
+}
+
 }  // namespace
 
 struct PdSolver {
@@ -126,6 +159,11 @@ struct PdSolver {
   double nh_mu = 0.0, nh_lame = 0.0, nh_penalty = 0.0;
   int blocks = 0;
   int max_blocks = 0;
+  // Launch plan of the sparse products.
+  pdb200::SpmvPlan plan_s{}, plan_st{};
+  int resident = 0, stage_vector = 0, vector_smem_offset = 0;
+  size_t smem = 0;
+  DeviceBuffer d_s_rowlist, d_s_nshort, d_st_rowlist, d_st_nshort, d_svd_u, d_svd_v;
   unsigned long long* timers = nullptr;  // phase timers of PD_PHASE_TIMERS builds
   InverseFactor factor;
   // Device mesh data.
@@ -296,9 +334,15 @@ int pd_create(const PdMeshDesc* mesh, const PdOptions* options, int device, PdSo
   }
   int sms = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  check(solver->d_svd_u.allocate(index_count / solver->corners * (solver->hex ? 8 : 1) * 9 * sizeof(double)), "svd");
+  check(solver->d_svd_v.allocate(index_count / solver->corners * (solver->hex ? 8 : 1) * 9 * sizeof(double)), "svd");
+  if (rc != PD_OK) {
+    delete solver;
+    return rc;
+  }
   int per_sm_forward = 0, per_sm_adjoint = 0;
-  pdb200::forward_step_max_blocks(options->precision, &per_sm_forward);
-  pdb200::adjoint_step_max_blocks(options->precision, &per_sm_adjoint);
+  pdb200::forward_step_max_blocks(options->precision, 0, &per_sm_forward);
+  pdb200::adjoint_step_max_blocks(options->precision, 0, &per_sm_adjoint);
   solver->max_blocks = sms * std::max(1, std::min(per_sm_forward, per_sm_adjoint));
   *out = solver;
   return PD_OK;
@@ -551,6 +595,60 @@ int pd_build(PdSolver* s, double dt) {
   }
   PD_CUDA(s->d_s_part.upload(s_part));
   PD_CUDA(s->d_st_part.upload(st_part));
+  {
+    std::vector<int32_t> rowlist, nshort;
+    int max_nnz = 0, max_rows = 0;
+    plan_rows(s->factor.s.offsets, s_part, rowlist, nshort, max_nnz, max_rows);
+    PD_CUDA(s->d_s_rowlist.upload(rowlist));
+    PD_CUDA(s->d_s_nshort.upload(nshort));
+    s->plan_s.max_nnz = max_nnz;
+    s->plan_s.max_rows = max_rows;
+    plan_rows(s->factor.st.offsets, st_part, rowlist, nshort, max_nnz, max_rows);
+    PD_CUDA(s->d_st_rowlist.upload(rowlist));
+    PD_CUDA(s->d_st_nshort.upload(nshort));
+    s->plan_st.max_nnz = max_nnz;
+    s->plan_st.max_rows = max_rows;
+  }
+  // Shared memory: keep the factor slices resident for the whole launch when
+  // they fit, and stage the SpMV input vector when it fits as well.
+  {
+    int optin = 0;
+    PD_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, s->device));
+    const int budget = optin - 8 * 1024;  // static shared memory of the kernels
+    const int value_bytes = s->options.precision == PD_PRECISION_FP64 ? 8 : 4;
+    const int slice_s = pdb200::slice_bytes(s->plan_s.max_nnz, s->plan_s.max_rows, value_bytes);
+    const int slice_st = pdb200::slice_bytes(s->plan_st.max_nnz, s->plan_st.max_rows, value_bytes);
+    const int vector_bytes = pdb200::align16(3 * s->n * 8);
+    s->resident = s->options.resident != 0 && slice_s + slice_st <= budget ? 1 : 0;
+    const int slices = s->resident ? slice_s + slice_st : 0;
+    s->stage_vector = s->options.resident != 0 && slices + vector_bytes <= budget ? 1 : 0;
+    s->plan_s.smem_offset = 0;
+    s->plan_st.smem_offset = slice_s;
+    s->vector_smem_offset = slices;
+    s->smem = static_cast<size_t>(slices + (s->stage_vector ? vector_bytes : 0));
+    int per_sm_forward = 0, per_sm_adjoint = 0;
+    PD_CUDA(pdb200::forward_step_max_blocks(s->options.precision, s->smem, &per_sm_forward));
+    PD_CUDA(pdb200::adjoint_step_max_blocks(s->options.precision, s->smem, &per_sm_adjoint));
+    int sms = 0;
+    PD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device));
+    if (std::min(per_sm_forward, per_sm_adjoint) * sms < blocks) {
+      return fail(PD_ERR_CUDA, "the persistent step kernels cannot keep the requested grid co-resident");
+    }
+  }
+  auto fill_plan = [&](pdb200::SpmvPlan& plan, const DeviceBuffer& off, const DeviceBuffer& col, const DeviceBuffer& val,
+                       const DeviceBuffer& val32, const DeviceBuffer& part, const DeviceBuffer& rowlist,
+                       const DeviceBuffer& nshort) {
+    plan.off = off.as<int>();
+    plan.col = col.as<int>();
+    plan.val64 = val.as<double>();
+    plan.val32 = val32.as<float>();
+    plan.part = part.as<int>();
+    plan.rowlist = rowlist.as<int>();
+    plan.nshort = nshort.as<int>();
+  };
+  fill_plan(s->plan_s, s->d_s_off, s->d_s_col, s->d_s_val, s->d_s_val32, s->d_s_part, s->d_s_rowlist, s->d_s_nshort);
+  fill_plan(s->plan_st, s->d_st_off, s->d_st_col, s->d_st_val, s->d_st_val32, s->d_st_part, s->d_st_rowlist,
+            s->d_st_nshort);
   PD_CUDA(s->d_a_off.upload(row_offsets));
   PD_CUDA(s->d_a_col.upload(row_columns));
   PD_CUDA(s->d_a_val.upload(row_values));
@@ -672,8 +770,15 @@ int pd_step(PdSolver* s, const float* q, const float* qd, const float* f, const 
   for (int c = 0; c < 3; ++c) a.gravity[c] = gravity[c];
   a.integrate_pinned = s->options.integrate_pinned_velocities;
   a.timers = s->timers;
+  a.plan_s = s->plan_s;
+  a.plan_st = s->plan_st;
+  a.resident = s->resident;
+  a.stage_vector = s->stage_vector;
+  a.vector_smem_offset = s->vector_smem_offset;
+  a.svd_u = s->options.svd_warm_start ? s->d_svd_u.as<double>() : nullptr;
+  a.svd_v = s->options.svd_warm_start ? s->d_svd_v.as<double>() : nullptr;
   PD_CUDA(cudaMemsetAsync(s->d_barrier.ptr, 0, sizeof(pdb200::GridBarrier), st));
-  PD_CUDA(pdb200::launch_forward_step(a, s->blocks, s->options.precision, st));
+  PD_CUDA(pdb200::launch_forward_step(a, s->blocks, s->options.precision, s->smem, st));
   return PD_OK;
 }
 
@@ -779,8 +884,13 @@ int pd_backward(PdSolver* s, const double* x_record, const float* activations, d
   b.inertia = s->inertia;
   // A Tet4 step's fibre targets are 1 - u of the activations it used.
   b.activations = (!s->hex && s->has_muscles) ? activations : nullptr;
+  b.plan_s = s->plan_s;
+  b.plan_st = s->plan_st;
+  b.resident = s->resident;
+  b.stage_vector = s->stage_vector;
+  b.vector_smem_offset = s->vector_smem_offset;
   PD_CUDA(cudaMemsetAsync(s->d_barrier.ptr, 0, sizeof(pdb200::GridBarrier), st));
-  PD_CUDA(pdb200::launch_adjoint_step(b, s->blocks, s->options.precision, st));
+  PD_CUDA(pdb200::launch_adjoint_step(b, s->blocks, s->options.precision, s->smem, st));
   return PD_OK;
 }
 

@@ -185,6 +185,8 @@ class SolverDiffPhD:
         precision: str = "fp64",
         adjoint: str = "reference",
         blocks: int = 0,
+        resident: bool = True,
+        svd_warm_start: bool = True,
     ):
         if material not in MATERIALS:
             raise ValueError("material must be 'pd' or 'neo_hookean'")
@@ -310,6 +312,8 @@ class SolverDiffPhD:
             PRECISIONS[precision],
             ADJOINTS[adjoint],
             int(blocks),
+            int(bool(resident)),
+            int(bool(svd_warm_start)),
         )
         handle = ctypes.c_void_p()
         device_index = self.device.index if self.device.index is not None else torch.cuda.current_device()
