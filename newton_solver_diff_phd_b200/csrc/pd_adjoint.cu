@@ -123,7 +123,8 @@ __device__ void element_operator(const AdjointArgs& b, const double* grad_smem, 
   const int total = b.ne * samples;
   // Hex8 contributions are summed over the eight samples of a cell in a fixed
   // order by the thread that owns the cell; Tet4 has one sample per element.
-  for (int e = gtid; e < b.ne; e += gthreads) {
+  (void)gtid;
+  for (int e = threadIdx.x * gridDim.x + blockIdx.x; e < b.ne; e += gthreads) {
     double acc[8][3];
     for (int k = 0; k < corners; ++k) acc[k][0] = acc[k][1] = acc[k][2] = 0.0;
     for (int s = 0; s < samples; ++s) {

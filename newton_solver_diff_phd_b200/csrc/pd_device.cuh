@@ -30,12 +30,17 @@ constexpr int kStatusAdjointNotConverged = 8;
 constexpr int kStatusAdjointSafeguard = 16;
 constexpr int kStatusBarrierTimeout = 1024;
 
+// Grid barrier state: one 32-bit word, generation in the high 16 bits and the
+// arrival count in the low 16 bits, so arriving is a single atomic and the
+// release (generation + 1, count reset) is another.
 struct GridBarrier {
-  unsigned int count;
-  unsigned int generation;
+  unsigned int state;
   unsigned int abort;
-  unsigned int pad;
+  unsigned int pad[2];
 };
+
+constexpr unsigned kCountBits = 16;
+constexpr unsigned kCountMask = (1u << kCountBits) - 1u;
 
 __device__ __forceinline__ unsigned load_volatile(const unsigned* p) { return *reinterpret_cast<const volatile unsigned*>(p); }
 
@@ -44,40 +49,39 @@ __device__ __forceinline__ unsigned load_acquire(const unsigned* p) {
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(value) : "l"(p) : "memory");
   return value;
 }
-__device__ __forceinline__ unsigned add_release(unsigned* p, unsigned value) {
+__device__ __forceinline__ unsigned add_acq_rel(unsigned* p, unsigned value) {
   unsigned old;
   asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(value) : "memory");
   return old;
 }
-__device__ __forceinline__ void store_release(unsigned* p, unsigned value) {
-  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(value) : "memory");
+__device__ __forceinline__ void red_release(unsigned* p, unsigned value) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(value) : "memory");
 }
 
 // Arrive at the grid barrier. Returns true in the block that arrived last;
 // that block must run its serial section and then call barrier_release().
 // Every other block must call barrier_wait(). The arrival is an acq_rel
 // atomic: this block's writes (ordered before it by __syncthreads and the
-// cumulative release) are visible to the block that observes the count.
+// cumulative release) are visible to the block that completes the count,
+// which acquires them.
 __device__ __forceinline__ bool barrier_arrive(GridBarrier* bar, unsigned& generation) {
   __shared__ int s_last;
   __shared__ unsigned s_generation;
   __syncthreads();
   if (threadIdx.x == 0) {
-    s_generation = load_acquire(&bar->generation);
-    const unsigned arrived = add_release(&bar->count, 1u) + 1u;
-    s_last = arrived == gridDim.x;
+    const unsigned old = add_acq_rel(&bar->state, 1u);
+    s_generation = old >> kCountBits;
+    s_last = (old & kCountMask) + 1u == gridDim.x;
   }
   __syncthreads();
   generation = s_generation;
   return s_last != 0;
 }
 
+// Last arriver: next generation and a zero count in one release atomic.
 __device__ __forceinline__ void barrier_release(GridBarrier* bar, unsigned generation) {
   __syncthreads();
-  if (threadIdx.x == 0) {
-    atomicExch(&bar->count, 0u);
-    store_release(&bar->generation, generation + 1u);
-  }
+  if (threadIdx.x == 0) red_release(&bar->state, (1u << kCountBits) - gridDim.x);
 }
 
 // Returns false when the wait gave up (timeout here or an abort elsewhere).
@@ -86,7 +90,7 @@ __device__ __forceinline__ bool barrier_wait(GridBarrier* bar, unsigned generati
   if (threadIdx.x == 0) {
     int ok = 1;
     unsigned spins = 0;
-    while (load_acquire(&bar->generation) == generation) {
+    while ((load_acquire(&bar->state) >> kCountBits) == (generation & (kCountMask))) {
       if (load_volatile(&bar->abort) != 0u) {
         ok = 0;
         break;
@@ -140,25 +144,43 @@ __device__ __forceinline__ double block_sum(double v, double* scratch /* [kWarps
 // the partials of one slot over all blocks are contiguous.
 __device__ __forceinline__ double* partial_slot(double* partials, int slot) { return partials + slot * gridDim.x; }
 
-// Sums slots [offset, offset + count) over all blocks in a fixed order: one
-// warp per slot, lanes strided over blocks (coalesced, all loads in flight),
-// then a fixed shuffle tree. Uses the whole block; results land in out[0..count)
-// (shared memory) for every thread after the call.
+// Sums slots [offset, offset + count) over all blocks in a fixed order. The
+// blocks of a slot are cut into kReduceChunks contiguous chunks; one thread
+// sums a chunk (all its loads issued together), then one thread per slot adds
+// the chunk sums in chunk order. Every load of the reduction is in flight at
+// once, so the latency is about one L2 round trip. Uses the whole block;
+// results land in out[0..count) (shared memory) for every thread.
+constexpr int kReduceChunks = 8;
+constexpr int kReduceChunkMax = 32;  // blocks per chunk: grids up to 256 blocks
+
 __device__ __forceinline__ void reduce_partials(const double* partials, int offset, int count, int blocks,
                                                 double* out /* shared [count] */,
-                                                double* scratch /* unused, kept for the call sites */) {
-  (void)scratch;
-  const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
-  for (int slot = warp; slot < count; slot += kWarps) {
-    const double* row = partials + (offset + slot) * blocks;
+                                                double* scratch /* shared [>= kBlock] */) {
+  const int chunk = (blocks + kReduceChunks - 1) / kReduceChunks;
+  for (int base = 0; base < count * kReduceChunks; base += blockDim.x) {
+    const int t = base + threadIdx.x;
     double sum = 0.0;
-#pragma unroll 8
-    for (int b = lane; b < blocks; b += 32) sum += row[b];
-    sum = warp_sum(sum);
-    if (lane == 0) out[slot] = sum;
+    if (t < count * kReduceChunks) {
+      const int slot = t / kReduceChunks;
+      const int c = t % kReduceChunks;
+      const double* row = partials + (offset + slot) * blocks;
+      const int b0 = c * chunk;
+      double values[kReduceChunkMax];
+#pragma unroll
+      for (int k = 0; k < kReduceChunkMax; ++k) values[k] = (k < chunk && b0 + k < blocks) ? row[b0 + k] : 0.0;
+#pragma unroll
+      for (int k = 0; k < kReduceChunkMax; ++k) sum += values[k];
+    }
+    scratch[threadIdx.x] = sum;
+    __syncthreads();
+    if (threadIdx.x * kReduceChunks < blockDim.x && base / kReduceChunks + threadIdx.x < count) {
+      double total = 0.0;
+#pragma unroll
+      for (int c = 0; c < kReduceChunks; ++c) total += scratch[threadIdx.x * kReduceChunks + c];
+      out[base / kReduceChunks + threadIdx.x] = total;
+    }
+    __syncthreads();
   }
-  __syncthreads();
 }
 
 template <typename T>

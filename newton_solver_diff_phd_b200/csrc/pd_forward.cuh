@@ -112,9 +112,12 @@ __device__ __forceinline__ M3<TL> sample_stress(const StepArgs& a, int e, int sa
 }
 
 // P1 for Tet4: one thread per element.
+// Element e belongs to block e % blocks: the local step is spread over every
+// SM instead of filling the first ones.
 template <typename TL>
 __device__ void local_step_tet(const StepArgs& a, bool warm, int gtid, int gthreads) {
-  for (int e = gtid; e < a.ne; e += gthreads) {
+  (void)gtid;
+  for (int e = threadIdx.x * gridDim.x + blockIdx.x; e < a.ne; e += gthreads) {
     M3<TL> f, fd;
     tet_deformation<TL>(a, e, a.x, f);
     tet_deformation<TL>(a, e, a.boundary, fd);
@@ -140,9 +143,11 @@ __device__ void local_step_hex(const StepArgs& a, const double* grad_smem, bool 
   const int lane = threadIdx.x & 31;
   const int s = lane & 7;
   const int group_in_warp = lane >> 3;
-  const int warp_global = gtid >> 5;
   const int warps_total = gthreads >> 5;
-  for (int base = warp_global * 4; base < a.ne; base += warps_total * 4) {
+  (void)gtid;
+  // Cell groups are interleaved over blocks (group g lives in block g % blocks).
+  const int warp_in_block = threadIdx.x >> 5;
+  for (int base = (warp_in_block * gridDim.x + blockIdx.x) * 4; base < a.ne; base += warps_total * 4) {
     const int e = base + group_in_warp;
     const bool valid = e < a.ne;
     const int ec = valid ? e : a.ne - 1;

@@ -30,6 +30,41 @@
 
 namespace pdb200 {
 
+// Dual convergence gate of the previous iteration (kernels.py:354-401), by one
+// warp while the other warps run the next local step: a fixed-order warp
+// reduction of the per-block partials, then the decision. All blocks read it
+// after the next barrier, so its latency leaves the critical path; a
+// converged step costs one extra local step whose output is discarded.
+__device__ void warp_convergence(const StepArgs& a) {
+  const int lane = threadIdx.x & 31;
+  const int blocks = gridDim.x;
+  double sums[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const double* row = a.partials + (48 + q) * blocks;
+    double v = 0.0;
+    for (int b = lane; b < blocks; b += 32) v += row[b];
+    sums[q] = warp_sum(v);
+  }
+  if (lane == 0) {
+    const double step_norm = sqrt(sums[0]);
+    const double previous_norm = sqrt(sums[1]);
+    const double change_norm = sqrt(sums[2]);
+    const double projection_norm = sqrt(sums[3]);
+    const int k = *a.iteration;
+    *a.iteration = k + 1;
+    if (k > 0 && step_norm <= a.rel_tol * previous_norm + a.abs_tol &&
+        change_norm <= a.rel_tol * projection_norm + a.abs_tol) {
+      *a.active = 0;
+    } else if (k + 1 >= a.max_iterations) {
+      *a.active = 0;
+      atomicOr(a.status, kStatusNotConverged);
+    } else {
+      *a.active = 1;
+    }
+  }
+}
+
 // One projective-dynamics step: prologue, every local/global iteration, epilogue.
 // TL: precision of the local projections; TV: precision of the factor values.
 template <typename TL, typename TV>
@@ -109,6 +144,8 @@ __global__ void __launch_bounds__(kBlock) forward_step_kernel(const StepArgs a) 
 
   PD_TIMER_START();
   for (int iter = 0;; ++iter) {
+    // Decision for the previous iteration, overlapped with this local step.
+    if (iter > 0 && blockIdx.x == 0 && (threadIdx.x >> 5) == kWarps - 1) warp_convergence(a);
     // ---- P1: local step (warm-started SVD after the first iteration).
     if (a.hex) {
       local_step_hex<TL>(a, s_grad, iter > 0, gtid, gthreads);
@@ -118,6 +155,11 @@ __global__ void __launch_bounds__(kBlock) forward_step_kernel(const StepArgs a) 
     PD_TIMER(0);
     if (!grid_sync(a.barrier, a.status)) return;
     PD_TIMER(5);
+    if (iter > 0) {
+      if (threadIdx.x == 0) s_control[0] = *reinterpret_cast<volatile int*>(a.active);
+      __syncthreads();
+      if (s_control[0] == 0) break;  // converged at iter - 1; x is that iterate
+    }
 
     // ---- P2: fixed-order gather, vertex-plane energies, right-hand side.
     // Four lanes per particle: lane q sums entries q, q+4, ... of the
@@ -288,35 +330,9 @@ __global__ void __launch_bounds__(kBlock) forward_step_kernel(const StepArgs a) 
         my_partials[50 * gridDim.x] = change2;
         my_partials[51 * gridDim.x] = proj2;
       }
-      unsigned generation;
-      if (barrier_arrive(a.barrier, generation)) {
-        reduce_partials(a.partials, 48, 4, gridDim.x, s_reduced, s_scratch);
-        if (threadIdx.x == 0) {
-          const double step_norm = sqrt(s_reduced[0]);
-          const double previous_norm = sqrt(s_reduced[1]);
-          const double change_norm = sqrt(s_reduced[2]);
-          const double projection_norm = sqrt(s_reduced[3]);
-          const int k = *a.iteration;
-          *a.iteration = k + 1;
-          if (k > 0 && step_norm <= a.rel_tol * previous_norm + a.abs_tol &&
-              change_norm <= a.rel_tol * projection_norm + a.abs_tol) {
-            *a.active = 0;
-          } else if (k + 1 >= a.max_iterations) {
-            *a.active = 0;
-            atomicOr(a.status, kStatusNotConverged);
-          } else {
-            *a.active = 1;
-          }
-        }
-        barrier_release(a.barrier, generation);
-        __syncthreads();
-      } else if (!barrier_wait(a.barrier, generation, a.status)) {
-        return;
-      }
+      // The decision is taken by one warp during the next local step.
+      if (!grid_sync(a.barrier, a.status)) return;
       PD_TIMER(7);
-      if (threadIdx.x == 0) s_control[0] = *reinterpret_cast<volatile int*>(a.active);
-      __syncthreads();
-      if (s_control[0] == 0) break;
     }
   }
 

@@ -211,7 +211,20 @@ PD_HD void rotate_columns(M3<T>& m, int p, int q, T c, T s) {
     m.a[i][q] = s * x + c * y;
   }
 }
-// Symmetric 2x2 Jacobi rotation (Eigen JacobiRotation::makeJacobi for reals).
+// 1 / sqrt(x) (a hardware-seeded reciprocal square root on the device).
+template <typename T>
+PD_HD T reciprocal_sqrt(T x) {
+#ifdef __CUDA_ARCH__
+  return rsqrt(x);
+#else
+  return T(1) / sqrt(x);
+#endif
+}
+
+// Symmetric 2x2 Jacobi rotation (Eigen JacobiRotation::makeJacobi for reals):
+// tau = (x - z) / 2|y|, t = 1 / (tau +- sqrt(tau^2 + 1)), c = 1 / sqrt(t^2 + 1),
+// s = -sign(t) sign(y) |t| c. The reciprocal square root and the sign copy
+// replace two of Eigen's divisions; results agree to rounding.
 template <typename T>
 PD_HD void make_jacobi(T x, T y, T z, T& c, T& s) {
   c = T(1);
@@ -222,13 +235,30 @@ PD_HD void make_jacobi(T x, T y, T z, T& c, T& s) {
     const T w = sqrt(tau * tau + T(1));
     const T t = tau > T(0) ? T(1) / (tau + w) : T(1) / (tau - w);
     const T sign = t > T(0) ? T(1) : T(-1);
-    const T n = T(1) / sqrt(t * t + T(1));
-    s = -sign * (y / fabs(y)) * fabs(t) * n;
+    const T n = reciprocal_sqrt(t * t + T(1));
+    s = -sign * copysign(T(1), y) * fabs(t) * n;
     c = n;
   }
 }
 
 constexpr int kJacobiMaxSweeps = 64;
+
+// Swap entries I and J of sigma and columns I and J of U and V.
+template <typename T, int I, int J>
+PD_HD void swap_columns(V3<T>& sigma, M3<T>& u, M3<T>& v) {
+  const T value = sigma[I];
+  sigma[I] = sigma[J];
+  sigma[J] = value;
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    T t = u.a[r][I];
+    u.a[r][I] = u.a[r][J];
+    u.a[r][J] = t;
+    t = v.a[r][I];
+    v.a[r][I] = v.a[r][J];
+    v.a[r][J] = t;
+  }
+}
 
 // F = U diag(sigma) V^T with sigma >= 0 sorted descending.
 template <typename T>
@@ -263,9 +293,9 @@ PD_HD void unsigned_svd(const M3<T>& f, M3<T>& u, V3<T>& sigma, M3<T>& v) {
         T s1 = T(0);
         if (fabs(d) >= Limits<T>::min_normal()) {
           const T ratio = t / d;
-          const T root = sqrt(T(1) + ratio * ratio);
-          s1 = T(1) / root;
-          c1 = ratio / root;
+          const T inverse_root = reciprocal_sqrt(T(1) + ratio * ratio);
+          s1 = inverse_root;
+          c1 = ratio * inverse_root;
         }
         const T m00 = c1 * w.a[p][p] + s1 * w.a[q][p];
         const T m01 = c1 * w.a[p][q] + s1 * w.a[q][q];
@@ -292,25 +322,22 @@ PD_HD void unsigned_svd(const M3<T>& f, M3<T>& u, V3<T>& sigma, M3<T>& v) {
       for (int r = 0; r < 3; ++r) u.a[r][i] = -u.a[r][i];
     }
   }
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    int position = i;
-#pragma unroll
-    for (int j = i + 1; j < 3; ++j)
-      if (sigma[j] > sigma[position]) position = j;
-    if (sigma[position] == T(0)) break;
-    if (position != i) {
-      const T value = sigma[i];
-      sigma[i] = sigma[position];
-      sigma[position] = value;
-#pragma unroll
-      for (int r = 0; r < 3; ++r) {
-        T t = u.a[r][i];
-        u.a[r][i] = u.a[r][position];
-        u.a[r][position] = t;
-        t = v.a[r][i];
-        v.a[r][i] = v.a[r][position];
-        v.a[r][position] = t;
+  // Descending selection sort that stops at the first zero maximum (Eigen),
+  // written with compile-time column indices so U and V stay in registers.
+  {
+    int position = 0;
+    if (sigma.y > sigma[position]) position = 1;
+    if (sigma.z > sigma[position]) position = 2;
+    if (sigma[position] != T(0)) {
+      if (position == 1) {
+        swap_columns<T, 0, 1>(sigma, u, v);
+      } else if (position == 2) {
+        swap_columns<T, 0, 2>(sigma, u, v);
+      }
+      if (sigma.z > sigma.y) {
+        if (sigma.z != T(0)) swap_columns<T, 1, 2>(sigma, u, v);
+      } else if (sigma.y == T(0)) {
+        // The maximum of the remaining entries is zero: the sort stops.
       }
     }
   }
@@ -322,7 +349,7 @@ template <typename T>
 PD_HD V3<T> volume_offset(V3<T> sigma, bool& singular) {
   singular = sigma.z < Limits<T>::eps();
   const T product = sigma.x * sigma.y * sigma.z;
-  const T root = pow(product, T(1) / T(3));
+  const T root = cbrt(product);
   V3<T> d = v3<T>(sigma.x / root - sigma.x, sigma.y / root - sigma.y, sigma.z / root - sigma.z);
   for (int iteration = 0; iteration < 50; ++iteration) {
     const V3<T> s = sigma + d;

@@ -577,7 +577,8 @@ int pd_build(PdSolver* s, double dt) {
                                            static_cast<int64_t>(s->ne) * samples / 256);
     blocks = static_cast<int>(std::max<int64_t>(8, std::min<int64_t>(work, s->max_blocks)));
   }
-  blocks = std::min(blocks, s->max_blocks);
+  // Fixed-order reductions handle up to 256 blocks (8 chunks of 32).
+  blocks = std::min(std::min(blocks, s->max_blocks), 256);
   s->blocks = blocks;
   const std::vector<int32_t> s_part = partition_rows(s->factor.s.offsets, blocks);
   const std::vector<int32_t> st_part = partition_rows(s->factor.st.offsets, blocks);
