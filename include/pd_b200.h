@@ -56,6 +56,10 @@ extern "C" {
 #define PD_ADJOINT_REFERENCE 0 /* K with the mean weight per energy (adjoint.py:17-18) */
 #define PD_ADJOINT_EXACT 1     /* K with per-element weights: the derivative of the forward map */
 
+#define PD_ADJOINT_SOLVER_AUTO 0        /* fixed point for the reference mode, CG for the exact mode */
+#define PD_ADJOINT_SOLVER_FIXED_POINT 1 /* mu <- A^{-1}(g + K mu) with Anderson and safeguards (adjoint.py:927-1086) */
+#define PD_ADJOINT_SOLVER_CG 2          /* CG on (A - K) mu = g preconditioned by A^{-1} = S^T S */
+
 typedef struct PdSolver PdSolver;
 
 typedef struct PdMeshDesc {
@@ -83,6 +87,7 @@ typedef struct PdOptions {
   int32_t blocks;            /* persistent grid size; 0 = automatic */
   int32_t resident;          /* 1: keep factor slices in shared memory when they fit (default) */
   int32_t svd_warm_start;    /* 1: warm-start each sample's SVD from the previous iteration (default) */
+  int32_t adjoint_solver;    /* PD_ADJOINT_SOLVER_* */
 } PdOptions;
 
 /* Library identity and the message of the last failure on this thread. */

@@ -65,6 +65,7 @@ class PdOptions(ctypes.Structure):
         ("blocks", ctypes.c_int32),
         ("resident", ctypes.c_int32),
         ("svd_warm_start", ctypes.c_int32),
+        ("adjoint_solver", ctypes.c_int32),
     ]
 
 

@@ -107,6 +107,26 @@ __device__ __forceinline__ void deformation_from(const int* idx, const double* g
   }
 }
 
+// Deformation of the combination vec + beta * vec2 (a CG search direction formed on the fly).
+__device__ __forceinline__ void deformation_combined(const int* idx, const double* grad, int corners, const double* vec,
+                                                     const double* vec2, double beta, double out[3][3]) {
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) out[r][c] = 0.0;
+  for (int k = 0; k < corners; ++k) {
+    const int v = idx[k];
+    const double* g = grad + 3 * k;
+    const double px = vec[3 * v] + beta * vec2[3 * v];
+    const double py = vec[3 * v + 1] + beta * vec2[3 * v + 1];
+    const double pz = vec[3 * v + 2] + beta * vec2[3 * v + 2];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      out[0][c] += px * g[c];
+      out[1][c] += py * g[c];
+      out[2][c] += pz * g[c];
+    }
+  }
+}
+
 // Per-sample gradient rows: Tet4 element e, or Hex8 sample s (shared).
 __device__ __forceinline__ const double* sample_gradients(const AdjointArgs& b, const double* grad_smem, int e, int s) {
   return b.hex ? grad_smem + 8 * 3 * s : b.gradients + 12 * e;
@@ -117,7 +137,7 @@ __device__ __forceinline__ const double* sample_gradients(const AdjointArgs& b, 
 // term (Dirichlet coupling, adjoint.py:493-521).
 template <typename TL>
 __device__ void element_operator(const AdjointArgs& b, const double* grad_smem, const double* vec, int op, int gtid,
-                                 int gthreads) {
+                                 int gthreads, const double* vec2 = nullptr, double beta = 0.0) {
   const int samples = b.hex ? 8 : 1;
   const int corners = b.corners;
   const int total = b.ne * samples;
@@ -130,7 +150,11 @@ __device__ void element_operator(const AdjointArgs& b, const double* grad_smem, 
     for (int s = 0; s < samples; ++s) {
       const double* g = sample_gradients(b, grad_smem, e, s);
       double df[3][3];
-      deformation_from(b.indices + corners * e, g, corners, vec, df);
+      if (vec2 != nullptr) {
+        deformation_combined(b.indices + corners * e, g, corners, vec, vec2, beta, df);
+      } else {
+        deformation_from(b.indices + corners * e, g, corners, vec, df);
+      }
       const TL* jac = jacobian_ptr<TL>(b) + static_cast<size_t>(e * samples + s) * 81;
       M3<double> ds = apply_jacobian<TL>(jac, df);
       if (op == 1) {
@@ -243,6 +267,10 @@ constexpr int kSlotMixed = 50;    // ||raw||^2 after mixing
 constexpr int kSlotRhs = 51;      // ||g||^2 (seed)
 constexpr int kSlotMaterial = 52; // material gradient column sums (2)
 constexpr int kSlotActivation = 54;
+constexpr int kSlotRZ = 56;   // CG: r^T z
+constexpr int kSlotZZ = 57;   // CG: z^T z (the fixed-point step norm)
+constexpr int kSlotMM = 58;   // CG: mu^T mu
+constexpr int kSlotPQ = 59;   // CG: p^T (A - K) p
 
 template <typename TL, typename TV>
 __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs b) {
@@ -312,6 +340,188 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
   double* vector_smem = reinterpret_cast<double*>(dyn_smem + b.vector_smem_offset);
   if (!grid_sync(b.barrier, b.status)) return;
 
+  if (b.pcg) {
+    // ---- Preconditioned conjugate gradients on (A - K) mu = g over the free
+    // rows, preconditioned by the factor A^{-1} = S^T S. The reference's
+    // fixed-point step A^{-1}(g + K mu) - mu equals the preconditioned residual
+    // z = A^{-1} r, so the stop rule ||z|| < rel ||mu|| + abs is the reference's.
+    // Per iteration: S | S^T (+ serial: beta, stop) | K p | A p - K p (+ serial:
+    // alpha) | updates; the new direction p = z + beta p is formed where read.
+    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+      V3<double> g = load3d(b.rhs, i);
+      if (b.free_[i] == 0) g = v3<double>(0.0, 0.0, 0.0);
+      store3(b.work, i, g);                                  // r
+      store3(b.prev, i, v3<double>(0.0, 0.0, 0.0));          // p
+    }
+    if (threadIdx.x == 0) my_partials[kSlotMM * gridDim.x] = 0.0;
+    if (!grid_sync(b.barrier, b.status)) return;
+    for (;;) {
+      // z = A^{-1} r.
+      {
+        const double* in = b.work;
+        if (b.stage_vector) {
+          stage_vector(b.work, vector_smem, n);
+          in = vector_smem;
+        }
+        spmv_block<TV>(b.plan_s, s_values, b.resident != 0, dyn_smem, in, b.y);
+      }
+      if (!grid_sync(b.barrier, b.status)) return;
+      {
+        const double* in = b.y;
+        if (b.stage_vector) {
+          stage_vector(b.y, vector_smem, n);
+          in = vector_smem;
+        }
+        spmv_block<TV>(b.plan_st, st_values, b.resident != 0, dyn_smem, in, b.raw);
+      }
+      __syncthreads();
+      double rz = 0.0, zz = 0.0;
+      for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+        V3<double> z = load3d(b.raw, i);
+        if (b.free_[i] == 0) z = v3<double>(0.0, 0.0, 0.0);
+        for (int c = 0; c < 3; ++c) {
+          if (!isfinite(z[c])) {
+            z[c] = 0.0;
+            atomicOr(b.status, kStatusAdjointSafeguard);
+          }
+        }
+        store3(b.raw, i, z);
+        rz += dot(load3d(b.work, i), z);
+        zz += dot(z, z);
+      }
+      rz = block_sum(rz, s_scratch);
+      zz = block_sum(zz, s_scratch);
+      if (threadIdx.x == 0) {
+        my_partials[kSlotRZ * gridDim.x] = rz;
+        my_partials[kSlotZZ * gridDim.x] = zz;
+      }
+      {
+        unsigned generation;
+        if (barrier_arrive(b.barrier, generation)) {
+          reduce_partials(b.partials, kSlotRZ, 3, gridDim.x, s_reduced, s_scratch);
+          if (threadIdx.x == 0) {
+            const double rho = s_reduced[0];
+            const double step_norm = sqrt(s_reduced[1]);
+            const double mu_norm = sqrt(s_reduced[2]);
+            const int k = *b.iteration;
+            *b.iteration = k + 1;
+            int active = 1;
+            if (k > 0 && step_norm < b.rel_tol * mu_norm + b.abs_tol) {
+              active = 0;
+            } else if (k + 1 >= b.max_iterations) {
+              active = 0;
+              atomicOr(b.status, kStatusAdjointNotConverged);
+            } else if (!(rho > 0.0) || !isfinite(rho)) {
+              // Zero residual (exact solve) or a non-positive preconditioned norm.
+              active = 0;
+              if (!(rho == 0.0)) atomicOr(b.status, kStatusAdjointSafeguard);
+            }
+            const double previous_rho = b.control_d[5];
+            b.control_d[6] = (k == 0 || !(previous_rho > 0.0)) ? 0.0 : rho / previous_rho;  // beta
+            b.control_d[5] = rho;
+            b.control_d[3] = mu_norm;
+            *b.active = active;
+          }
+          barrier_release(b.barrier, generation);
+          __syncthreads();
+        } else if (!barrier_wait(b.barrier, generation, b.status)) {
+          return;
+        }
+      }
+      if (threadIdx.x == 0) s_control[0] = *reinterpret_cast<volatile int*>(b.active);
+      __syncthreads();
+      if (s_control[0] == 0) break;
+      const double beta = *reinterpret_cast<volatile double*>(b.control_d + 6);
+      // K p with p = z + beta p_old formed on the fly.
+      element_operator<TL>(b, s_grad, b.raw, 0, gtid, gthreads, b.prev, beta);
+      if (!grid_sync(b.barrier, b.status)) return;
+      // q = A p - K p on the free rows; p^T q partials.
+      double pq = 0.0;
+      {
+        const int sub = threadIdx.x & 3;
+        const int groups_total = gthreads >> 2;
+        const int lane_group = (threadIdx.x & 31) >> 2;
+        for (int base = (gtid >> 5) * 8; base < n; base += groups_total) {
+          const int i = base + lane_group;
+          const bool valid = i < n;
+          double qx = 0.0, qy = 0.0, qz = 0.0;
+          if (valid) {
+            const int k0 = b.inc_offsets[i], k1 = b.inc_offsets[i + 1];
+            for (int k = k0 + sub; k < k1; k += 4) {
+              const double* c = b.contrib + 3 * b.inc_entries[k];
+              qx -= c[0];
+              qy -= c[1];
+              qz -= c[2];
+            }
+            for (int q = b.a_off[i] + sub; q < b.a_off[i + 1]; q += 4) {
+              const double v = b.a_val[q];
+              const int j = b.a_col[q];
+              qx += v * (b.raw[3 * j] + beta * b.prev[3 * j]);
+              qy += v * (b.raw[3 * j + 1] + beta * b.prev[3 * j + 1]);
+              qz += v * (b.raw[3 * j + 2] + beta * b.prev[3 * j + 2]);
+            }
+          }
+#pragma unroll
+          for (int mask = 1; mask < 4; mask <<= 1) {
+            qx += __shfl_xor_sync(0xffffffffu, qx, mask);
+            qy += __shfl_xor_sync(0xffffffffu, qy, mask);
+            qz += __shfl_xor_sync(0xffffffffu, qz, mask);
+          }
+          if (valid && sub == 0) {
+            if (b.free_[i] == 0) qx = qy = qz = 0.0;
+            b.y[3 * i] = qx;
+            b.y[3 * i + 1] = qy;
+            b.y[3 * i + 2] = qz;
+            pq += (b.raw[3 * i] + beta * b.prev[3 * i]) * qx + (b.raw[3 * i + 1] + beta * b.prev[3 * i + 1]) * qy +
+                  (b.raw[3 * i + 2] + beta * b.prev[3 * i + 2]) * qz;
+          }
+        }
+      }
+      pq = block_sum(pq, s_scratch);
+      if (threadIdx.x == 0) my_partials[kSlotPQ * gridDim.x] = pq;
+      {
+        unsigned generation;
+        if (barrier_arrive(b.barrier, generation)) {
+          reduce_partials(b.partials, kSlotPQ, 1, gridDim.x, s_reduced, s_scratch);
+          if (threadIdx.x == 0) {
+            const double curvature = s_reduced[0];
+            double alpha = 0.0;
+            if (curvature > 0.0 && isfinite(curvature)) {
+              alpha = b.control_d[5] / curvature;
+            } else {
+              // (A - K) is not positive definite along p: keep mu and stop.
+              atomicOr(b.status, kStatusAdjointSafeguard);
+              *b.active = 0;
+            }
+            b.control_d[7] = alpha;
+          }
+          barrier_release(b.barrier, generation);
+          __syncthreads();
+        } else if (!barrier_wait(b.barrier, generation, b.status)) {
+          return;
+        }
+      }
+      const double alpha = *reinterpret_cast<volatile double*>(b.control_d + 7);
+      // mu += alpha p, r -= alpha q, p stored (own rows).
+      double mm = 0.0;
+      for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+        V3<double> p = load3d(b.raw, i) + beta * load3d(b.prev, i);
+        if (b.free_[i] == 0) p = v3<double>(0.0, 0.0, 0.0);
+        const V3<double> mu = load3d(b.solution, i) + alpha * p;
+        const V3<double> r = load3d(b.work, i) - alpha * load3d(b.y, i);
+        store3(b.prev, i, p);
+        store3(b.solution, i, mu);
+        store3(b.work, i, r);
+        mm += dot(mu, mu);
+      }
+      mm = block_sum(mm, s_scratch);
+      if (threadIdx.x == 0) my_partials[kSlotMM * gridDim.x] = mm;
+      if (!grid_sync(b.barrier, b.status)) return;
+      if (threadIdx.x == 0) s_control[0] = *reinterpret_cast<volatile int*>(b.active);
+      __syncthreads();
+      if (s_control[0] == 0) break;
+    }
+  } else {
   for (;;) {
     // ---- A1: K solution per element.
     element_operator<TL>(b, s_grad, b.solution, 0, gtid, gthreads);
@@ -551,6 +761,8 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
       __syncthreads();
       if (s_control[0] == 0) break;
     }
+  }
+
   }
 
   // ---- Routing guard (adjoint.py:1125-1138, :226-261), in one serial section.

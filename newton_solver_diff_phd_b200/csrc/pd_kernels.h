@@ -25,6 +25,7 @@ struct AdjointArgs {
   int has_muscles;
   int material;
   int exact;               // K with per-element weights instead of the mean weights
+  int pcg;                 // solve (A - K) mu = g by CG preconditioned with A^{-1} instead of the fixed point
   double nh_mu, nh_lame, nh_penalty;
   double jwc, jwv, jwn;    // mean weights of K (reference mode), per sample
   double sample_volume;    // Vbar (Tet4) or Vbar/8 (Hex8)

@@ -197,6 +197,8 @@ int validate_options(const PdOptions& o) {
   if (o.adjoint_mode != PD_ADJOINT_REFERENCE && o.adjoint_mode != PD_ADJOINT_EXACT)
     return fail(PD_ERR_INVALID, "adjoint mode must be reference or exact");
   if (o.blocks < 0) return fail(PD_ERR_INVALID, "blocks must be nonnegative");
+  if (o.adjoint_solver < PD_ADJOINT_SOLVER_AUTO || o.adjoint_solver > PD_ADJOINT_SOLVER_CG)
+    return fail(PD_ERR_INVALID, "adjoint solver must be auto, fixed point or CG");
   return PD_OK;
 }
 
@@ -817,6 +819,10 @@ int pd_backward(PdSolver* s, const double* x_record, const float* activations, d
   b.has_muscles = s->has_muscles ? 1 : 0;
   b.material = s->options.material;
   b.exact = s->options.adjoint_mode == PD_ADJOINT_EXACT ? 1 : 0;
+  b.pcg = s->options.adjoint_solver == PD_ADJOINT_SOLVER_CG ||
+                  (s->options.adjoint_solver == PD_ADJOINT_SOLVER_AUTO && b.exact)
+              ? 1
+              : 0;
   b.nh_mu = s->nh_mu;
   b.nh_lame = s->nh_lame;
   b.nh_penalty = s->nh_penalty;

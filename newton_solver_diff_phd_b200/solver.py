@@ -13,7 +13,10 @@ pointers to the library. There is no CPU fallback.
 Added keywords: ``precision`` (``"fp64"`` as the reference, or
 ``"fp32+refine"``), ``adjoint`` (``"reference"``: the reference's mean-weight
 local Jacobian; ``"exact"``: per-element weights, the derivative of the
-forward map) and ``blocks`` (persistent grid size, 0 = automatic).
+forward map), ``adjoint_solver`` (``"auto"``: the reference's Anderson fixed
+point for ``"reference"``, conjugate gradients preconditioned by the factor for
+``"exact"``; or ``"fixed_point"`` / ``"cg"``), ``blocks`` (persistent grid
+size, 0 = automatic), ``resident`` and ``svd_warm_start`` (kernel tuning).
 
 Differences from the reference: frictional boundaries and ``mesh_contact`` are
 not available in this build (``NotImplementedError``); gravity is taken from
@@ -35,6 +38,7 @@ from .meshes import Mesh
 MATERIALS = {"pd": 0, "neo_hookean": 1}
 PRECISIONS = {"fp64": _lib.PRECISION_FP64, "fp32+refine": _lib.PRECISION_FP32_REFINE}
 ADJOINTS = {"reference": _lib.ADJOINT_REFERENCE, "exact": _lib.ADJOINT_EXACT}
+ADJOINT_SOLVERS = {"auto": 0, "fixed_point": 1, "cg": 2}
 MAX_WINDOW = 8
 
 
@@ -187,6 +191,7 @@ class SolverDiffPhD:
         blocks: int = 0,
         resident: bool = True,
         svd_warm_start: bool = True,
+        adjoint_solver: str = "auto",
     ):
         if material not in MATERIALS:
             raise ValueError("material must be 'pd' or 'neo_hookean'")
@@ -219,6 +224,8 @@ class SolverDiffPhD:
             raise ValueError("precision must be 'fp64' or 'fp32+refine'")
         if adjoint not in ADJOINTS:
             raise ValueError("adjoint must be 'reference' or 'exact'")
+        if adjoint_solver not in ADJOINT_SOLVERS:
+            raise ValueError("adjoint_solver must be 'auto', 'fixed_point' or 'cg'")
         self.model = model
         self.device = model.device
         if self.device.type != "cuda":
@@ -314,6 +321,7 @@ class SolverDiffPhD:
             int(blocks),
             int(bool(resident)),
             int(bool(svd_warm_start)),
+            ADJOINT_SOLVERS[adjoint_solver],
         )
         handle = ctypes.c_void_p()
         device_index = self.device.index if self.device.index is not None else torch.cuda.current_device()
