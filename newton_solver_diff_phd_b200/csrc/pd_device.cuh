@@ -34,9 +34,10 @@ constexpr int kStatusBarrierTimeout = 1024;
 // arrival count in the low 16 bits, so arriving is a single atomic and the
 // release (generation + 1, count reset) is another.
 struct GridBarrier {
-  unsigned int state;
+  unsigned int state;  // serial-section barriers
   unsigned int abort;
-  unsigned int pad[2];
+  unsigned int flip;   // plain barriers: arrival count with a flipping high bit
+  unsigned int pad;
 };
 
 constexpr unsigned kCountBits = 16;
@@ -109,15 +110,35 @@ __device__ __forceinline__ bool barrier_wait(GridBarrier* bar, unsigned generati
   return s_ok != 0;
 }
 
-// Plain barrier without a serial section.
+// Plain barrier without a serial section: block 0 adds 2^31 - (blocks - 1),
+// every other block adds 1, so the arrival that completes the count also
+// flips the high bit and resets the low bits; waiters poll for the flip. One
+// atomic per block and no separate release.
 __device__ __forceinline__ bool grid_sync(GridBarrier* bar, int* status) {
-  unsigned generation;
-  if (barrier_arrive(bar, generation)) {
-    barrier_release(bar, generation);
-    __syncthreads();
-    return true;
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned increment = blockIdx.x == 0 ? 0x80000000u - (gridDim.x - 1u) : 1u;
+    const unsigned old = add_acq_rel(&bar->flip, increment);
+    int ok = 1;
+    unsigned spins = 0;
+    while (((old ^ load_acquire(&bar->flip)) & 0x80000000u) == 0u) {
+      if (load_volatile(&bar->abort) != 0u) {
+        ok = 0;
+        break;
+      }
+      if (++spins > kSpinLimit) {
+        atomicOr(status, kStatusBarrierTimeout);
+        atomicExch(&bar->abort, 1u);
+        ok = 0;
+        break;
+      }
+      if (spins > 256) __nanosleep(20);
+    }
+    s_ok = ok;
   }
-  return barrier_wait(bar, generation, status);
+  __syncthreads();
+  return s_ok != 0;
 }
 
 __device__ __forceinline__ double warp_sum(double v) {

