@@ -88,6 +88,7 @@ typedef struct PdOptions {
   int32_t resident;          /* 1: keep factor slices in shared memory when they fit (default) */
   int32_t svd_warm_start;    /* 1: warm-start each sample's SVD from the previous iteration (default) */
   int32_t adjoint_solver;    /* PD_ADJOINT_SOLVER_* */
+  int32_t state_precision;   /* 0: float32 particle states (Newton's), 1: float64 states and gradients */
 } PdOptions;
 
 /* Library identity and the message of the last failure on this thread. */
@@ -135,15 +136,18 @@ int pd_build(PdSolver* solver, double dt);
 /* Factor statistics of the last build: rows, nnz(S), nnz(L) incl. diagonal. */
 int pd_factor_stats(const PdSolver* solver, int64_t* rows, int64_t* nnz_s, int64_t* nnz_l);
 
-/* SolverDiffPhD.step (solver.py:689-786) for float32 device states.
-   q, qd, f: device [n][3] float32 inputs; dirichlet: optional device [n][3]
+/* SolverDiffPhD.step (solver.py:689-786).
+   Particle arrays are float32 (Newton's states), or float64 when the solver
+   was created with state_precision 1 (the same holds for the gradient arrays
+   of pd_backward).
+   q, qd, f: device [n][3] inputs; dirichlet: optional device [n][3]
    prescribed positions of the pinned particles (or NULL); gravity: host [3];
    q_out, qd_out: device [n][3] float32 outputs (must not alias the inputs);
    x_record: optional device [n][3] float64 that receives the converged
    positions for pd_backward (the reference StepRecord.x, adjoint.py:809-841).
    dt must equal the dt of the last pd_build. `stream` is a cudaStream_t. */
-int pd_step(PdSolver* solver, const float* q, const float* qd, const float* f, const float* dirichlet,
-            const double gravity[3], double dt, float* q_out, float* qd_out, double* x_record, void* stream);
+int pd_step(PdSolver* solver, const void* q, const void* qd, const void* f, const void* dirichlet,
+            const double gravity[3], double dt, void* q_out, void* qd_out, double* x_record, void* stream);
 
 /* Adjoint.backward (adjoint.py:1088-1259) of one recorded step.
    x_record: device [n][3] float64 positions recorded by pd_step; activations:
@@ -156,8 +160,8 @@ int pd_step(PdSolver* solver, const float* q, const float* qd, const float* f, c
    dL/dmu, dL/dlambda; gactivations: optional device float32 [n_elements]
    accumulator of dL/du. Passing gmaterials/gactivations requests z, exactly
    as a requires_grad material array does in the reference. */
-int pd_backward(PdSolver* solver, const double* x_record, const float* activations, double dt, const float* gq_out,
-                const float* gqd_out, float* gq, float* gqd, float* gf, float* gdirichlet, double* gmaterials,
+int pd_backward(PdSolver* solver, const double* x_record, const float* activations, double dt, const void* gq_out,
+                const void* gqd_out, void* gq, void* gqd, void* gf, void* gdirichlet, double* gmaterials,
                 float* gactivations, void* stream);
 
 /* Device buffer of 8 uint64 nanosecond accumulators for the per-phase timers

@@ -66,6 +66,7 @@ class PdOptions(ctypes.Structure):
         ("resident", ctypes.c_int32),
         ("svd_warm_start", ctypes.c_int32),
         ("adjoint_solver", ctypes.c_int32),
+        ("state_precision", ctypes.c_int32),
     ]
 
 

@@ -299,8 +299,8 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
     for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
       V3<double> g;
       for (int c = 0; c < 3; ++c) {
-        const double velocity = static_cast<double>(b.gqd_out[3 * i + c]) / dt;
-        g[c] = static_cast<double>(b.gq_out[3 * i + c]) + velocity;
+        const double velocity = state_load(b.gqd_out, b.state_f64, 3 * i + c) / dt;
+        g[c] = state_load(b.gq_out, b.state_f64, 3 * i + c) + velocity;
         b.base[3 * i + c] = -velocity;
       }
       store3(b.rhs, i, g);
@@ -802,9 +802,9 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
     for (int c = 0; c < 3; ++c) {
       const double mu = b.solution[3 * i + c];
       const double injection = routing * b.inertia * mu;
-      b.gq[3 * i + c] = b.gq[3 * i + c] + static_cast<float>(b.base[3 * i + c] + injection);
-      b.gqd[3 * i + c] = b.gqd[3 * i + c] + static_cast<float>(dt * injection);
-      b.gf[3 * i + c] = b.gf[3 * i + c] + static_cast<float>(routing * mu);
+      state_add(b.gq, b.state_f64, 3 * i + c, b.base[3 * i + c] + injection);
+      state_add(b.gqd, b.state_f64, 3 * i + c, dt * injection);
+      state_add(b.gf, b.state_f64, 3 * i + c, routing * mu);
     }
   }
 
@@ -926,10 +926,10 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
       for (int c = 0; c < 3; ++c) {
         const double value = b.rhs[3 * i + c] - coupling[c];
         if (b.gdirichlet != nullptr) {
-          b.gdirichlet[3 * i + c] = b.gdirichlet[3 * i + c] + static_cast<float>(value);
+          state_add(b.gdirichlet, b.state_f64, 3 * i + c, value);
         } else {
-          b.gq[3 * i + c] = b.gq[3 * i + c] + static_cast<float>(value);
-          if (b.integrate_pinned) b.gqd[3 * i + c] = b.gqd[3 * i + c] + static_cast<float>(dt * value);
+          state_add(b.gq, b.state_f64, 3 * i + c, value);
+          if (b.integrate_pinned) state_add(b.gqd, b.state_f64, 3 * i + c, dt * value);
         }
       }
     }

@@ -204,6 +204,27 @@ __device__ __forceinline__ void reduce_partials(const double* partials, int offs
   }
 }
 
+// Particle state arrays are float32 (Newton's wp.vec3) or float64.
+__device__ __forceinline__ double state_load(const void* p, int f64, int k) {
+  return f64 ? static_cast<const double*>(p)[k] : static_cast<double>(static_cast<const float*>(p)[k]);
+}
+__device__ __forceinline__ void state_store(void* p, int f64, int k, double v) {
+  if (f64) {
+    static_cast<double*>(p)[k] = v;
+  } else {
+    static_cast<float*>(p)[k] = static_cast<float>(v);
+  }
+}
+// Accumulate as the reference does: in the array's own precision.
+__device__ __forceinline__ void state_add(void* p, int f64, int k, double v) {
+  if (f64) {
+    static_cast<double*>(p)[k] += v;
+  } else {
+    float* f = static_cast<float*>(p);
+    f[k] = f[k] + static_cast<float>(v);
+  }
+}
+
 template <typename T>
 __device__ __forceinline__ V3<T> load3(const double* v, int i) {
   return v3<T>(static_cast<T>(v[3 * i]), static_cast<T>(v[3 * i + 1]), static_cast<T>(v[3 * i + 2]));
@@ -311,13 +332,14 @@ struct StepArgs {
   int max_iterations;
   double abs_tol, rel_tol;
   GridBarrier* barrier;
-  // Inputs and outputs of the step
-  const float* q_in;
-  const float* qd_in;
-  const float* f_in;
-  const float* dirichlet;
-  float* q_out;
-  float* qd_out;
+  // Inputs and outputs of the step (float32, or float64 when state_f64)
+  const void* q_in;
+  const void* qd_in;
+  const void* f_in;
+  const void* dirichlet;
+  void* q_out;
+  void* qd_out;
+  int state_f64;
   double* x_record;
   double dt, mass, inertia;
   double gravity[3];

@@ -84,13 +84,16 @@ __global__ void __launch_bounds__(kBlock) forward_step_kernel(const StepArgs a) 
   // read_activations (:136-152), begin_solve, Anderson reset.
   const double dt = a.dt;
   for (int i = gtid; i < n; i += gthreads) {
-    const V3<double> start = v3<double>(a.q_in[3 * i], a.q_in[3 * i + 1], a.q_in[3 * i + 2]);
-    const V3<double> velocity = v3<double>(a.qd_in[3 * i], a.qd_in[3 * i + 1], a.qd_in[3 * i + 2]);
+    const int f64 = a.state_f64;
+    const V3<double> start =
+        v3<double>(state_load(a.q_in, f64, 3 * i), state_load(a.q_in, f64, 3 * i + 1), state_load(a.q_in, f64, 3 * i + 2));
+    const V3<double> velocity = v3<double>(state_load(a.qd_in, f64, 3 * i), state_load(a.qd_in, f64, 3 * i + 1),
+                                           state_load(a.qd_in, f64, 3 * i + 2));
     store3(a.position, i, start);
     store3(a.velocity, i, velocity);
     V3<double> acceleration;
 #pragma unroll
-    for (int c = 0; c < 3; ++c) acceleration[c] = static_cast<double>(a.f_in[3 * i + c]) / a.mass + a.gravity[c];
+    for (int c = 0; c < 3; ++c) acceleration[c] = state_load(a.f_in, f64, 3 * i + c) / a.mass + a.gravity[c];
     V3<double> target;
 #pragma unroll
     for (int c = 0; c < 3; ++c) target[c] = start[c] + dt * velocity[c] + dt * dt * acceleration[c];
@@ -98,7 +101,8 @@ __global__ void __launch_bounds__(kBlock) forward_step_kernel(const StepArgs a) 
     V3<double> boundary = v3<double>(0.0, 0.0, 0.0);
     if (a.free_[i] == 0) {
       if (a.dirichlet != nullptr) {
-        boundary = v3<double>(a.dirichlet[3 * i], a.dirichlet[3 * i + 1], a.dirichlet[3 * i + 2]);
+        boundary = v3<double>(state_load(a.dirichlet, f64, 3 * i), state_load(a.dirichlet, f64, 3 * i + 1),
+                              state_load(a.dirichlet, f64, 3 * i + 2));
       } else {
         boundary = start;
         if (a.integrate_pinned) boundary = boundary + dt * velocity;
@@ -341,8 +345,8 @@ __global__ void __launch_bounds__(kBlock) forward_step_kernel(const StepArgs a) 
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const double value = a.x[3 * i + c];
-      a.q_out[3 * i + c] = static_cast<float>(value);
-      a.qd_out[3 * i + c] = static_cast<float>((value - a.position[3 * i + c]) / dt);
+      state_store(a.q_out, a.state_f64, 3 * i + c, value);
+      state_store(a.qd_out, a.state_f64, 3 * i + c, (value - a.position[3 * i + c]) / dt);
       if (a.x_record != nullptr) a.x_record[3 * i + c] = value;
     }
   }

@@ -74,12 +74,13 @@ struct AdjointArgs {
   GridBarrier* barrier;
   double* control_d;       // [8]
   int* control_i;          // [8]
-  const float* gq_out;
-  const float* gqd_out;
-  float* gq;
-  float* gqd;
-  float* gf;
-  float* gdirichlet;
+  const void* gq_out;    // float32, or float64 when state_f64
+  const void* gqd_out;
+  void* gq;
+  void* gqd;
+  void* gf;
+  void* gdirichlet;
+  int state_f64;
   double* gmaterials;
   float* gactivations;
   double* material_scratch;    // [ne][2]

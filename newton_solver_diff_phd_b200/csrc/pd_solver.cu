@@ -197,6 +197,7 @@ int validate_options(const PdOptions& o) {
   if (o.adjoint_mode != PD_ADJOINT_REFERENCE && o.adjoint_mode != PD_ADJOINT_EXACT)
     return fail(PD_ERR_INVALID, "adjoint mode must be reference or exact");
   if (o.blocks < 0) return fail(PD_ERR_INVALID, "blocks must be nonnegative");
+  if (o.state_precision != 0 && o.state_precision != 1) return fail(PD_ERR_INVALID, "state precision must be 0 or 1");
   if (o.adjoint_solver < PD_ADJOINT_SOLVER_AUTO || o.adjoint_solver > PD_ADJOINT_SOLVER_CG)
     return fail(PD_ERR_INVALID, "adjoint solver must be auto, fixed point or CG");
   return PD_OK;
@@ -230,7 +231,7 @@ int ensure_adjoint_buffers(PdSolver* s) {
   PD_CUDA(s->b_control_i.allocate(8 * sizeof(int)));
   PD_CUDA(s->b_material_scratch.allocate(static_cast<size_t>(s->ne) * 2 * sizeof(double)));
   PD_CUDA(s->b_activation_scratch.allocate(static_cast<size_t>(s->ne) * sizeof(double)));
-  const size_t fvec = static_cast<size_t>(3) * s->n * sizeof(float);
+  const size_t fvec = static_cast<size_t>(3) * s->n * sizeof(double);  // fits float32 and float64 states
   for (DeviceBuffer* buffer : {&s->b_zero_gq, &s->b_zero_gqd, &s->b_scratch_gq, &s->b_scratch_gqd, &s->b_scratch_gf})
     PD_CUDA(buffer->allocate(fvec));
   return PD_OK;
@@ -680,8 +681,8 @@ int pd_factor_stats(const PdSolver* s, int64_t* rows, int64_t* nnz_s, int64_t* n
   return PD_OK;
 }
 
-int pd_step(PdSolver* s, const float* q, const float* qd, const float* f, const float* dirichlet,
-            const double gravity[3], double dt, float* q_out, float* qd_out, double* x_record, void* stream) {
+int pd_step(PdSolver* s, const void* q, const void* qd, const void* f, const void* dirichlet,
+            const double gravity[3], double dt, void* q_out, void* qd_out, double* x_record, void* stream) {
   if (s == nullptr || q == nullptr || qd == nullptr || f == nullptr || gravity == nullptr || q_out == nullptr ||
       qd_out == nullptr)
     return fail(PD_ERR_INVALID, "null argument");
@@ -772,6 +773,7 @@ int pd_step(PdSolver* s, const float* q, const float* qd, const float* f, const 
   a.inertia = s->inertia;
   for (int c = 0; c < 3; ++c) a.gravity[c] = gravity[c];
   a.integrate_pinned = s->options.integrate_pinned_velocities;
+  a.state_f64 = s->options.state_precision;
   a.timers = s->timers;
   a.plan_s = s->plan_s;
   a.plan_st = s->plan_st;
@@ -785,8 +787,8 @@ int pd_step(PdSolver* s, const float* q, const float* qd, const float* f, const 
   return PD_OK;
 }
 
-int pd_backward(PdSolver* s, const double* x_record, const float* activations, double dt, const float* gq_out,
-                const float* gqd_out, float* gq, float* gqd, float* gf, float* gdirichlet, double* gmaterials,
+int pd_backward(PdSolver* s, const double* x_record, const float* activations, double dt, const void* gq_out,
+                const void* gqd_out, void* gq, void* gqd, void* gf, void* gdirichlet, double* gmaterials,
                 float* gactivations, void* stream) {
   if (s == nullptr || x_record == nullptr) return fail(PD_ERR_INVALID, "null argument");
   if (!s->built || s->stale || s->built_dt != dt)
@@ -794,7 +796,7 @@ int pd_backward(PdSolver* s, const double* x_record, const float* activations, d
   PD_CUDA(cudaSetDevice(s->device));
   if (int status = ensure_adjoint_buffers(s)) return status;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const size_t fvec = static_cast<size_t>(3) * s->n * sizeof(float);
+  const size_t fvec = static_cast<size_t>(3) * s->n * (s->options.state_precision ? sizeof(double) : sizeof(float));
   // Missing output gradients read as zero; missing input accumulators go to scratch.
   if (gq_out == nullptr || gqd_out == nullptr) {
     PD_CUDA(cudaMemsetAsync(s->b_zero_gq.ptr, 0, fvec, st));
@@ -873,11 +875,12 @@ int pd_backward(PdSolver* s, const double* x_record, const float* activations, d
   b.barrier = s->d_barrier.as<pdb200::GridBarrier>();
   b.control_d = s->b_control_d.as<double>();
   b.control_i = s->b_control_i.as<int>();
-  b.gq_out = gq_out != nullptr ? gq_out : s->b_zero_gq.as<float>();
-  b.gqd_out = gqd_out != nullptr ? gqd_out : s->b_zero_gqd.as<float>();
-  b.gq = gq != nullptr ? gq : s->b_scratch_gq.as<float>();
-  b.gqd = gqd != nullptr ? gqd : s->b_scratch_gqd.as<float>();
-  b.gf = gf != nullptr ? gf : s->b_scratch_gf.as<float>();
+  b.gq_out = gq_out != nullptr ? gq_out : s->b_zero_gq.ptr;
+  b.gqd_out = gqd_out != nullptr ? gqd_out : s->b_zero_gqd.ptr;
+  b.gq = gq != nullptr ? gq : s->b_scratch_gq.ptr;
+  b.gqd = gqd != nullptr ? gqd : s->b_scratch_gqd.ptr;
+  b.gf = gf != nullptr ? gf : s->b_scratch_gf.ptr;
+  b.state_f64 = s->options.state_precision;
   b.gdirichlet = gdirichlet;
   b.gmaterials = gmaterials;
   b.gactivations = s->hex ? nullptr : gactivations;

@@ -34,13 +34,14 @@ class Rollout:
         self.every = int(checkpoint_every)
         n = solver._n
         device = solver.device
+        dtype = solver.state_dtype
         kept = self.steps + 1 if self.every == 1 else self.steps // self.every + 2
 
         def state():
             s = State(
-                torch.zeros((n, 3), dtype=torch.float32, device=device),
-                torch.zeros((n, 3), dtype=torch.float32, device=device),
-                torch.zeros((n, 3), dtype=torch.float32, device=device),
+                torch.zeros((n, 3), dtype=dtype, device=device),
+                torch.zeros((n, 3), dtype=dtype, device=device),
+                torch.zeros((n, 3), dtype=dtype, device=device),
             )
             for tensor in (s.particle_q, s.particle_qd, s.particle_f):
                 tensor.grad = torch.zeros_like(tensor)
@@ -51,7 +52,7 @@ class Rollout:
         self.records = torch.zeros((self.steps if self.every == 1 else self.every, n, 3), dtype=torch.float64,
                                    device=device)
         self.segment = [state() for _ in range(self.every + 1)] if self.every > 1 else None
-        self.force_grad = torch.zeros((self.steps, n, 3), dtype=torch.float32, device=device)
+        self.force_grad = torch.zeros((self.steps, n, 3), dtype=dtype, device=device)
         self.material_grad = torch.zeros((solver._element_count, 2), dtype=torch.float64, device=device)
         self._forces = None
 
@@ -62,7 +63,7 @@ class Rollout:
         return forces[t] if forces.dim() == 3 else forces
 
     def forward(self, q0: torch.Tensor, qd0: torch.Tensor, forces: torch.Tensor | None = None) -> State:
-        """Run all steps; returns the final state. ``forces`` is ``(N,3)`` or ``(steps,N,3)`` float32."""
+        """Run all steps; returns the final state. ``forces`` is ``(N,3)`` or ``(steps,N,3)`` in the state dtype."""
         self._forces = forces
         first = self.checkpoints[0]
         first.particle_q.copy_(q0)

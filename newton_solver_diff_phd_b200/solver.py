@@ -18,6 +18,9 @@ point for ``"reference"``, conjugate gradients preconditioned by the factor for
 ``"exact"``; or ``"fixed_point"`` / ``"cg"``), ``blocks`` (persistent grid
 size, 0 = automatic), ``resident`` and ``svd_warm_start`` (kernel tuning).
 
+``state_dtype=torch.float64`` (added) keeps particle states and their
+gradients in float64 between steps; the default float32 matches Newton.
+
 Differences from the reference: frictional boundaries and ``mesh_contact`` are
 not available in this build (``NotImplementedError``); gravity is taken from
 one world; Hex8 steps can be recorded for the backward pass (the reference
@@ -192,6 +195,7 @@ class SolverDiffPhD:
         resident: bool = True,
         svd_warm_start: bool = True,
         adjoint_solver: str = "auto",
+        state_dtype: torch.dtype = torch.float32,
     ):
         if material not in MATERIALS:
             raise ValueError("material must be 'pd' or 'neo_hookean'")
@@ -226,6 +230,9 @@ class SolverDiffPhD:
             raise ValueError("adjoint must be 'reference' or 'exact'")
         if adjoint_solver not in ADJOINT_SOLVERS:
             raise ValueError("adjoint_solver must be 'auto', 'fixed_point' or 'cg'")
+        if state_dtype not in (torch.float32, torch.float64):
+            raise ValueError("state_dtype must be torch.float32 (Newton states) or torch.float64")
+        self.state_dtype = state_dtype
         self.model = model
         self.device = model.device
         if self.device.type != "cuda":
@@ -322,6 +329,7 @@ class SolverDiffPhD:
             int(bool(resident)),
             int(bool(svd_warm_start)),
             ADJOINT_SOLVERS[adjoint_solver],
+            1 if state_dtype == torch.float64 else 0,
         )
         handle = ctypes.c_void_p()
         device_index = self.device.index if self.device.index is not None else torch.cuda.current_device()
@@ -550,8 +558,8 @@ class SolverDiffPhD:
         if dirichlet_positions is not None:
             if not isinstance(dirichlet_positions, torch.Tensor):
                 raise TypeError("dirichlet_positions must be a tensor")
-            if dirichlet_positions.dtype != torch.float32 or tuple(dirichlet_positions.shape) != (self._n, 3):
-                raise ValueError("dirichlet_positions must have dtype float32 and shape (particle_count, 3)")
+            if dirichlet_positions.dtype != self.state_dtype or tuple(dirichlet_positions.shape) != (self._n, 3):
+                raise ValueError("dirichlet_positions must have the state dtype and shape (particle_count, 3)")
             if dirichlet_positions.device != self.device:
                 raise ValueError("dirichlet_positions must be on the solver device")
             if dirichlet_positions.data_ptr() in (state_out.particle_q.data_ptr(), state_out.particle_qd.data_ptr()):
@@ -573,9 +581,10 @@ class SolverDiffPhD:
         q = state_in.particle_q.detach()
         qd = state_in.particle_qd.detach()
         f = state_in.particle_f.detach()
-        for name, tensor in (("particle_q", q), ("particle_qd", qd), ("particle_f", f)):
-            if tensor.dtype != torch.float32 or tuple(tensor.shape) != (self._n, 3) or not tensor.is_contiguous():
-                raise ValueError(f"state {name} must be a contiguous float32 (particle_count, 3) tensor")
+        for name, tensor in (("particle_q", q), ("particle_qd", qd), ("particle_f", f),
+                             ("particle_q out", state_out.particle_q), ("particle_qd out", state_out.particle_qd)):
+            if tensor.dtype != self.state_dtype or tuple(tensor.shape) != (self._n, 3) or not tensor.is_contiguous():
+                raise ValueError(f"state {name} must be a contiguous {self.state_dtype} (particle_count, 3) tensor")
         dirichlet = None if dirichlet_positions is None else dirichlet_positions.detach().contiguous()
         _lib.check(
             self._lib.pd_step(

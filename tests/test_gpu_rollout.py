@@ -63,21 +63,22 @@ def test_young_modulus_gradient_matches_finite_differences(adjoint_solver):
 
     def loss_of(young_values, with_grad):
         mu, lam = _set_young(model, young_values, nu)
-        solver = SolverDiffPhD(model, density=1000.0, adjoint="exact", adjoint_solver=adjoint_solver, **TIGHT)
+        # float64 states: a 1e-4 relative change of E moves positions by ~1e-10 m,
+        # far below the float32 state rounding (~2e-9 m) between steps.
+        solver = SolverDiffPhD(model, density=1000.0, adjoint="exact", adjoint_solver=adjoint_solver,
+                               state_dtype=torch.float64, **TIGHT)
         driver = Rollout(solver, steps, dt)
-        q0 = model.particle_q.clone()
+        q0 = model.particle_q.double()
         e = torch.tensor(young_values, dtype=torch.float64, device="cuda", requires_grad=with_grad)
         mu_t = e / (2.0 * (1.0 + nu))
         lam_t = e * nu / ((1.0 + nu) * (1.0 - 2.0 * nu))
         q_t, _ = rollout(driver, q0, torch.zeros_like(q0), None, torch.stack((mu_t, lam_t), dim=1))
         # Loss on the float64 recorded positions of the last step (no float32 output rounding).
-        x_t = driver.records[-1]
-        loss = ((x_t - target_t) ** 2).sum() + 0.0 * (q_t.double().sum())
+        loss = ((q_t - target_t) ** 2).sum()
         if with_grad:
-            loss_q = ((q_t.double() - target_t) ** 2).sum()
-            loss_q.backward()
+            loss.backward()
         solver.check_status()
-        return float(loss), (e.grad.cpu().numpy() if with_grad else None)
+        return float(loss.detach()), (e.grad.cpu().numpy() if with_grad else None)
 
     _, grad = loss_of(young, True)
     scale = np.abs(grad).max()
@@ -89,9 +90,10 @@ def test_young_modulus_gradient_matches_finite_differences(adjoint_solver):
         plus[element] += eps
         minus[element] -= eps
         numeric = (loss_of(plus, False)[0] - loss_of(minus, False)[0]) / (2 * eps)
-        # Relative 1e-3 for the dominant entries; small entries sit at the FD noise
-        # floor of a 1e-12-converged solve, so they get a floor of 1e-2 of the largest.
-        assert abs(grad[element] - numeric) <= 1e-3 * max(abs(numeric), 10.0 * scale * (element not in largest)), (
+        # Relative 1e-4 (the gradient target) for the dominant entries; small
+        # entries sit at the FD noise floor of a 1e-12-converged solve, so they
+        # get an absolute floor of 1e-4 of the largest entry.
+        assert abs(grad[element] - numeric) <= 1e-4 * max(abs(numeric), scale * (element not in largest)), (
             element, grad[element], numeric)
 
 
