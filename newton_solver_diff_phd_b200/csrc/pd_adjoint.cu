@@ -136,15 +136,15 @@ __device__ __forceinline__ const double* sample_gradients(const AdjointArgs& b, 
 // `vec`: op 0 -> K vec (local Jacobian), op 1 -> (A - K) vec without the mass
 // term (Dirichlet coupling, adjoint.py:493-521).
 template <typename TL>
-__device__ void element_operator(const AdjointArgs& b, const double* grad_smem, const double* vec, int op, int gtid,
-                                 int gthreads, const double* vec2 = nullptr, double beta = 0.0) {
+__device__ void element_operator(const AdjointArgs& b, const double* grad_smem, const double* vec, int op, Team team,
+                                 const double* vec2 = nullptr, double beta = 0.0) {
   const int samples = b.hex ? 8 : 1;
   const int corners = b.corners;
   const int total = b.ne * samples;
   // Hex8 contributions are summed over the eight samples of a cell in a fixed
   // order by the thread that owns the cell; Tet4 has one sample per element.
-  (void)gtid;
-  for (int e = threadIdx.x * gridDim.x + blockIdx.x; e < b.ne; e += gthreads) {
+  const int gthreads = team.size * blockDim.x;
+  for (int e = threadIdx.x * team.size + team.rank; e < b.ne; e += gthreads) {
     double acc[8][3];
     for (int k = 0; k < corners; ++k) acc[k][0] = acc[k][1] = acc[k][2] = 0.0;
     for (int s = 0; s < samples; ++s) {
@@ -201,7 +201,7 @@ __device__ __forceinline__ V3<double> gather_row(const AdjointArgs& b, int i) {
 
 // Block partial of the Anderson Gram entries (same layout as the forward).
 __device__ void adjoint_gram_partials(const AdjointArgs& b, int r0, int r1, int count, int start, double* block_out,
-                                      double* scratch) {
+                                      double* scratch, int blocks) {
   const int entries = count * (count + 1) / 2 + count;
   const int capacity = b.window + 1;
   const int groups = entries > 0 ? kBlock / entries : 0;
@@ -235,7 +235,7 @@ __device__ void adjoint_gram_partials(const AdjointArgs& b, int r0, int r1, int 
   if (t < entries) {
     double total = 0.0;
     for (int g = 0; g < groups; ++g) total += scratch[g * entries + t];
-    block_out[t * gridDim.x] = total;
+    block_out[t * blocks] = total;
   }
   __syncthreads();
 }
@@ -272,15 +272,16 @@ constexpr int kSlotZZ = 57;   // CG: z^T z (the fixed-point step norm)
 constexpr int kSlotMM = 58;   // CG: mu^T mu
 constexpr int kSlotPQ = 59;   // CG: p^T (A - K) p
 
+// One adjoint step of one instance by one team of blocks. Returns false when
+// a team barrier gave up (the status word says why).
 template <typename TL, typename TV>
-__global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs b) {
-  extern __shared__ __align__(16) char dyn_smem[];
+__device__ __forceinline__ bool adjoint_step_body(const AdjointArgs& b, const Team team, char* dyn_smem) {
   __shared__ double s_grad[8 * 8 * 3];
   __shared__ double s_scratch[kBlock];
   __shared__ double s_reduced[64];
   __shared__ int s_control[8];
-  const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
-  const int gthreads = gridDim.x * blockDim.x;
+  const int gtid = team.rank * blockDim.x + threadIdx.x;
+  const int gthreads = team.size * blockDim.x;
   const int n = b.n;
   const int samples = b.hex ? 8 : 1;
   const int corners = b.corners;
@@ -288,8 +289,8 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
     for (int t = threadIdx.x; t < 8 * 8 * 3; t += blockDim.x) s_grad[t] = b.gradients[t];
     __syncthreads();
   }
-  const int r0 = b.st_part[blockIdx.x], r1 = b.st_part[blockIdx.x + 1];
-  double* my_partials = b.partials + blockIdx.x;  // slot-major: [slot * gridDim.x]
+  const int r0 = b.st_part[team.rank], r1 = b.st_part[team.rank + 1];
+  double* my_partials = b.partials + team.rank;  // slot-major: [slot * team.size]
   const size_t hstride = static_cast<size_t>(3) * n;
   const double dt = b.dt;
 
@@ -308,7 +309,7 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
       rhs2 += dot(g, g);
     }
     rhs2 = block_sum(rhs2, s_scratch);
-    if (threadIdx.x == 0) my_partials[(kSlotRhs) * gridDim.x] = rhs2;
+    if (threadIdx.x == 0) my_partials[(kSlotRhs) * team.size] = rhs2;
   }
   for (int t = gtid; t < b.ne * samples; t += gthreads) {
     const int e = t / samples;
@@ -334,11 +335,11 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
   const TV* st_values = sizeof(TV) == sizeof(double) ? reinterpret_cast<const TV*>(b.st_val)
                                                      : reinterpret_cast<const TV*>(b.st_val32);
   if (b.resident) {
-    load_slice<TV>(b.plan_s, s_values, dyn_smem);
-    load_slice<TV>(b.plan_st, st_values, dyn_smem);
+    load_slice<TV>(b.plan_s, s_values, dyn_smem, team.rank);
+    load_slice<TV>(b.plan_st, st_values, dyn_smem, team.rank);
   }
   double* vector_smem = reinterpret_cast<double*>(dyn_smem + b.vector_smem_offset);
-  if (!grid_sync(b.barrier, b.status)) return;
+  if (!grid_sync(b.barrier, b.status, team.size, team.rank)) return false;
 
   if (b.pcg) {
     // ---- Preconditioned conjugate gradients on (A - K) mu = g over the free
@@ -353,8 +354,8 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
       store3(b.work, i, g);                                  // r
       store3(b.prev, i, v3<double>(0.0, 0.0, 0.0));          // p
     }
-    if (threadIdx.x == 0) my_partials[kSlotMM * gridDim.x] = 0.0;
-    if (!grid_sync(b.barrier, b.status)) return;
+    if (threadIdx.x == 0) my_partials[kSlotMM * team.size] = 0.0;
+    if (!grid_sync(b.barrier, b.status, team.size, team.rank)) return false;
     for (;;) {
       // z = A^{-1} r.
       {
@@ -363,16 +364,16 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
           stage_vector(b.work, vector_smem, n);
           in = vector_smem;
         }
-        spmv_block<TV>(b.plan_s, s_values, b.resident != 0, dyn_smem, in, b.y);
+        spmv_block<TV>(b.plan_s, s_values, b.resident != 0, dyn_smem, in, b.y, team.rank);
       }
-      if (!grid_sync(b.barrier, b.status)) return;
+      if (!grid_sync(b.barrier, b.status, team.size, team.rank)) return false;
       {
         const double* in = b.y;
         if (b.stage_vector) {
           stage_vector(b.y, vector_smem, n);
           in = vector_smem;
         }
-        spmv_block<TV>(b.plan_st, st_values, b.resident != 0, dyn_smem, in, b.raw);
+        spmv_block<TV>(b.plan_st, st_values, b.resident != 0, dyn_smem, in, b.raw, team.rank);
       }
       __syncthreads();
       double rz = 0.0, zz = 0.0;
@@ -392,13 +393,13 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
       rz = block_sum(rz, s_scratch);
       zz = block_sum(zz, s_scratch);
       if (threadIdx.x == 0) {
-        my_partials[kSlotRZ * gridDim.x] = rz;
-        my_partials[kSlotZZ * gridDim.x] = zz;
+        my_partials[kSlotRZ * team.size] = rz;
+        my_partials[kSlotZZ * team.size] = zz;
       }
       {
         unsigned generation;
-        if (barrier_arrive(b.barrier, generation)) {
-          reduce_partials(b.partials, kSlotRZ, 3, gridDim.x, s_reduced, s_scratch);
+        if (barrier_arrive(b.barrier, generation, team.size)) {
+          reduce_partials(b.partials, kSlotRZ, 3, team.size, s_reduced, s_scratch);
           if (threadIdx.x == 0) {
             const double rho = s_reduced[0];
             const double step_norm = sqrt(s_reduced[1]);
@@ -422,10 +423,10 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
             b.control_d[3] = mu_norm;
             *b.active = active;
           }
-          barrier_release(b.barrier, generation);
+          barrier_release(b.barrier, generation, team.size);
           __syncthreads();
         } else if (!barrier_wait(b.barrier, generation, b.status)) {
-          return;
+          return false;
         }
       }
       if (threadIdx.x == 0) s_control[0] = *reinterpret_cast<volatile int*>(b.active);
@@ -433,8 +434,8 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
       if (s_control[0] == 0) break;
       const double beta = *reinterpret_cast<volatile double*>(b.control_d + 6);
       // K p with p = z + beta p_old formed on the fly.
-      element_operator<TL>(b, s_grad, b.raw, 0, gtid, gthreads, b.prev, beta);
-      if (!grid_sync(b.barrier, b.status)) return;
+      element_operator<TL>(b, s_grad, b.raw, 0, team, b.prev, beta);
+      if (!grid_sync(b.barrier, b.status, team.size, team.rank)) return false;
       // q = A p - K p on the free rows; p^T q partials.
       double pq = 0.0;
       {
@@ -478,11 +479,11 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
         }
       }
       pq = block_sum(pq, s_scratch);
-      if (threadIdx.x == 0) my_partials[kSlotPQ * gridDim.x] = pq;
+      if (threadIdx.x == 0) my_partials[kSlotPQ * team.size] = pq;
       {
         unsigned generation;
-        if (barrier_arrive(b.barrier, generation)) {
-          reduce_partials(b.partials, kSlotPQ, 1, gridDim.x, s_reduced, s_scratch);
+        if (barrier_arrive(b.barrier, generation, team.size)) {
+          reduce_partials(b.partials, kSlotPQ, 1, team.size, s_reduced, s_scratch);
           if (threadIdx.x == 0) {
             const double curvature = s_reduced[0];
             double alpha = 0.0;
@@ -495,10 +496,10 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
             }
             b.control_d[7] = alpha;
           }
-          barrier_release(b.barrier, generation);
+          barrier_release(b.barrier, generation, team.size);
           __syncthreads();
         } else if (!barrier_wait(b.barrier, generation, b.status)) {
-          return;
+          return false;
         }
       }
       const double alpha = *reinterpret_cast<volatile double*>(b.control_d + 7);
@@ -515,8 +516,8 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
         mm += dot(mu, mu);
       }
       mm = block_sum(mm, s_scratch);
-      if (threadIdx.x == 0) my_partials[kSlotMM * gridDim.x] = mm;
-      if (!grid_sync(b.barrier, b.status)) return;
+      if (threadIdx.x == 0) my_partials[kSlotMM * team.size] = mm;
+      if (!grid_sync(b.barrier, b.status, team.size, team.rank)) return false;
       if (threadIdx.x == 0) s_control[0] = *reinterpret_cast<volatile int*>(b.active);
       __syncthreads();
       if (s_control[0] == 0) break;
@@ -524,8 +525,8 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
   } else {
   for (;;) {
     // ---- A1: K solution per element.
-    element_operator<TL>(b, s_grad, b.solution, 0, gtid, gthreads);
-    if (!grid_sync(b.barrier, b.status)) return;
+    element_operator<TL>(b, s_grad, b.solution, 0, team);
+    if (!grid_sync(b.barrier, b.status, team.size, team.rank)) return false;
 
     // ---- A2: work = g + gather(K solution) (refinement: minus A solution),
     // four lanes per particle with a fixed shuffle tree.
@@ -569,7 +570,7 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
         }
       }
     }
-    if (!grid_sync(b.barrier, b.status)) return;
+    if (!grid_sync(b.barrier, b.status, team.size, team.rank)) return false;
 
     // ---- A3: y = S work.
     {
@@ -578,9 +579,9 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
         stage_vector(b.work, vector_smem, n);
         in = vector_smem;
       }
-      spmv_block<TV>(b.plan_s, s_values, b.resident != 0, dyn_smem, in, b.y);
+      spmv_block<TV>(b.plan_s, s_values, b.resident != 0, dyn_smem, in, b.y, team.rank);
     }
-    if (!grid_sync(b.barrier, b.status)) return;
+    if (!grid_sync(b.barrier, b.status, team.size, team.rank)) return false;
 
     // ---- A4: raw = S^T y; Dirichlet zeroing and scrub; history; partials.
     {
@@ -589,7 +590,7 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
         stage_vector(b.y, vector_smem, n);
         in = vector_smem;
       }
-      spmv_block<TV>(b.plan_st, st_values, b.resident != 0, dyn_smem, in, b.raw);
+      spmv_block<TV>(b.plan_st, st_values, b.resident != 0, dyn_smem, in, b.raw, team.rank);
     }
     __syncthreads();
     const int count = b.window > 0 ? b.aa_state[0] : 0;
@@ -626,18 +627,18 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
       raw2 = block_sum(raw2, s_scratch);
       step2 = block_sum(step2, s_scratch);
       if (threadIdx.x == 0) {
-        my_partials[(kSlotRaw) * gridDim.x] = raw2;
-        my_partials[(kSlotStep) * gridDim.x] = step2;
+        my_partials[(kSlotRaw) * team.size] = raw2;
+        my_partials[(kSlotStep) * team.size] = step2;
       }
       if (b.window > 0) {
         __syncthreads();
-        adjoint_gram_partials(b, r0, r1, count, start, my_partials + kSlotGram * gridDim.x, s_scratch);
+        adjoint_gram_partials(b, r0, r1, count, start, my_partials + kSlotGram * team.size, s_scratch, team.size);
       }
       // Serial: norm clip of the solve result (safe_clip, adjoint.py:184-223);
       // without clipping also the Anderson solve and the step norm.
       unsigned generation;
-      if (barrier_arrive(b.barrier, generation)) {
-        reduce_partials(b.partials, kSlotRaw, 2, gridDim.x, s_reduced, s_scratch);
+      if (barrier_arrive(b.barrier, generation, team.size)) {
+        reduce_partials(b.partials, kSlotRaw, 2, team.size, s_reduced, s_scratch);
         const double len = sqrt(s_reduced[0]);
         const bool clip = isfinite(len) && len > kClipNorm;
         if (threadIdx.x == 0) {
@@ -648,13 +649,13 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
         __syncthreads();
         if (!clip && b.window > 0) {
           const int entries = count * (count + 1) / 2 + count;
-          reduce_partials(b.partials, kSlotGram, entries, gridDim.x, s_reduced, s_scratch);
+          reduce_partials(b.partials, kSlotGram, entries, team.size, s_reduced, s_scratch);
           if (threadIdx.x == 0) aa_solve(b.aa_state, b.aa_gamma, b.aa_accept, s_reduced, b.window);
         }
-        barrier_release(b.barrier, generation);
+        barrier_release(b.barrier, generation, team.size);
         __syncthreads();
       } else if (!barrier_wait(b.barrier, generation, b.status)) {
-        return;
+        return false;
       }
     }
     const double clip1 = *reinterpret_cast<volatile double*>(b.control_d);
@@ -673,25 +674,25 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
         }
       }
       step2 = block_sum(step2, s_scratch);
-      if (threadIdx.x == 0) my_partials[(kSlotStep) * gridDim.x] = step2;
+      if (threadIdx.x == 0) my_partials[(kSlotStep) * team.size] = step2;
       if (b.window > 0) {
         __syncthreads();
-        adjoint_gram_partials(b, r0, r1, count, start, my_partials + kSlotGram * gridDim.x, s_scratch);
+        adjoint_gram_partials(b, r0, r1, count, start, my_partials + kSlotGram * team.size, s_scratch, team.size);
       }
       unsigned generation;
-      if (barrier_arrive(b.barrier, generation)) {
+      if (barrier_arrive(b.barrier, generation, team.size)) {
         if (b.window > 0) {
           const int entries = count * (count + 1) / 2 + count;
-          reduce_partials(b.partials, kSlotGram, entries, gridDim.x, s_reduced, s_scratch);
+          reduce_partials(b.partials, kSlotGram, entries, team.size, s_reduced, s_scratch);
           if (threadIdx.x == 0) aa_solve(b.aa_state, b.aa_gamma, b.aa_accept, s_reduced, b.window);
           __syncthreads();
         }
-        reduce_partials(b.partials, kSlotStep, 1, gridDim.x, s_reduced, s_scratch);
+        reduce_partials(b.partials, kSlotStep, 1, team.size, s_reduced, s_scratch);
         if (threadIdx.x == 0) b.control_d[1] = s_reduced[0];
-        barrier_release(b.barrier, generation);
+        barrier_release(b.barrier, generation, team.size);
         __syncthreads();
       } else if (!barrier_wait(b.barrier, generation, b.status)) {
-        return;
+        return false;
       }
     }
 
@@ -720,10 +721,10 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
         mixed2 += dot(value, value);
       }
       mixed2 = block_sum(mixed2, s_scratch);
-      if (threadIdx.x == 0) my_partials[(kSlotMixed) * gridDim.x] = mixed2;
+      if (threadIdx.x == 0) my_partials[(kSlotMixed) * team.size] = mixed2;
       unsigned generation;
-      if (barrier_arrive(b.barrier, generation)) {
-        reduce_partials(b.partials, kSlotMixed, 1, gridDim.x, s_reduced, s_scratch);
+      if (barrier_arrive(b.barrier, generation, team.size)) {
+        reduce_partials(b.partials, kSlotMixed, 1, team.size, s_reduced, s_scratch);
         if (threadIdx.x == 0) {
           const double len = sqrt(s_reduced[0]);
           double scale = 1.0;
@@ -747,15 +748,15 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
           *b.active = active;
           b.control_d[3] = solution_norm;
         }
-        barrier_release(b.barrier, generation);
+        barrier_release(b.barrier, generation, team.size);
         __syncthreads();
       } else if (!barrier_wait(b.barrier, generation, b.status)) {
-        return;
+        return false;
       }
       const double clip2 = *reinterpret_cast<volatile double*>(b.control_d + 2);
       if (clip2 != 1.0) {
         for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) store3(b.solution, i, clip2 * load3d(b.solution, i));
-        if (!grid_sync(b.barrier, b.status)) return;
+        if (!grid_sync(b.barrier, b.status, team.size, team.rank)) return false;
       }
       if (threadIdx.x == 0) s_control[0] = *reinterpret_cast<volatile int*>(b.active);
       __syncthreads();
@@ -768,8 +769,8 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
   // ---- Routing guard (adjoint.py:1125-1138, :226-261), in one serial section.
   {
     unsigned generation;
-    if (barrier_arrive(b.barrier, generation)) {
-      reduce_partials(b.partials, kSlotRhs, 1, gridDim.x, s_reduced, s_scratch);
+    if (barrier_arrive(b.barrier, generation, team.size)) {
+      reduce_partials(b.partials, kSlotRhs, 1, team.size, s_reduced, s_scratch);
       if (threadIdx.x == 0) {
         const double mu_norm = *reinterpret_cast<volatile double*>(b.control_d + 3);
         const bool failed = kClipNorm > 0.0 && mu_norm >= 0.999 * kClipNorm;
@@ -788,10 +789,10 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
         b.control_d[4] = value;
         b.control_i[0] = failed ? 1 : 0;
       }
-      barrier_release(b.barrier, generation);
+      barrier_release(b.barrier, generation, team.size);
       __syncthreads();
     } else if (!barrier_wait(b.barrier, generation, b.status)) {
-      return;
+      return false;
     }
   }
   const double routing = *reinterpret_cast<volatile double*>(b.control_d + 4);
@@ -814,7 +815,7 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
     if (diverged) {
       for (int t = gtid; t < b.ne * corners * 3; t += gthreads) b.contrib[t] = 0.0;
     } else {
-      element_operator<TL>(b, s_grad, b.solution, 1, gtid, gthreads);
+      element_operator<TL>(b, s_grad, b.solution, 1, team);
     }
   }
   double material0 = 0.0, material1 = 0.0, activation = 0.0;
@@ -881,15 +882,15 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
   material1 = block_sum(material1, s_scratch);
   activation = block_sum(activation, s_scratch);
   if (threadIdx.x == 0) {
-    my_partials[(kSlotMaterial) * gridDim.x] = material0;
-    my_partials[(kSlotMaterial + 1) * gridDim.x] = material1;
-    my_partials[(kSlotActivation) * gridDim.x] = activation;
+    my_partials[(kSlotMaterial) * team.size] = material0;
+    my_partials[(kSlotMaterial + 1) * team.size] = material1;
+    my_partials[(kSlotActivation) * team.size] = activation;
   }
   // Parameter guard (adjoint.py:622-644).
   {
     unsigned generation;
-    if (barrier_arrive(b.barrier, generation)) {
-      reduce_partials(b.partials, kSlotMaterial, 3, gridDim.x, s_reduced, s_scratch);
+    if (barrier_arrive(b.barrier, generation, team.size)) {
+      reduce_partials(b.partials, kSlotMaterial, 3, team.size, s_reduced, s_scratch);
       if (threadIdx.x == 0) {
         const bool material_ok = !b.zero_energy_weight && isfinite(s_reduced[0]) && isfinite(s_reduced[1]);
         const bool activation_ok = isfinite(s_reduced[2]);
@@ -899,10 +900,10 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
           atomicOr(b.status, kStatusAdjointSafeguard);
         }
       }
-      barrier_release(b.barrier, generation);
+      barrier_release(b.barrier, generation, team.size);
       __syncthreads();
     } else if (!barrier_wait(b.barrier, generation, b.status)) {
-      return;
+      return false;
     }
   }
   const int material_valid = *reinterpret_cast<volatile int*>(b.control_i + 1);
@@ -934,6 +935,14 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
       }
     }
   }
+  return true;
+}
+
+// Plain launch: the whole cooperative grid is one team solving one instance.
+template <typename TL, typename TV>
+__global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs b) {
+  extern __shared__ __align__(16) char dyn_smem[];
+  adjoint_step_body<TL, TV>(b, Team{static_cast<int>(blockIdx.x), static_cast<int>(gridDim.x)}, dyn_smem);
 }
 
 static const void* adjoint_kernel(int precision) {

@@ -65,14 +65,18 @@ __device__ __forceinline__ void red_release(unsigned* p, unsigned value) {
 // atomic: this block's writes (ordered before it by __syncthreads and the
 // cumulative release) are visible to the block that completes the count,
 // which acquires them.
-__device__ __forceinline__ bool barrier_arrive(GridBarrier* bar, unsigned& generation) {
+__device__ __forceinline__ bool barrier_arrive(GridBarrier* bar, unsigned& generation, int blocks) {
   __shared__ int s_last;
   __shared__ unsigned s_generation;
   __syncthreads();
+  if (blocks == 1) {
+    generation = 0;
+    return true;
+  }
   if (threadIdx.x == 0) {
     const unsigned old = add_acq_rel(&bar->state, 1u);
     s_generation = old >> kCountBits;
-    s_last = (old & kCountMask) + 1u == gridDim.x;
+    s_last = (old & kCountMask) + 1u == static_cast<unsigned>(blocks);
   }
   __syncthreads();
   generation = s_generation;
@@ -80,9 +84,9 @@ __device__ __forceinline__ bool barrier_arrive(GridBarrier* bar, unsigned& gener
 }
 
 // Last arriver: next generation and a zero count in one release atomic.
-__device__ __forceinline__ void barrier_release(GridBarrier* bar, unsigned generation) {
+__device__ __forceinline__ void barrier_release(GridBarrier* bar, unsigned generation, int blocks) {
   __syncthreads();
-  if (threadIdx.x == 0) red_release(&bar->state, (1u << kCountBits) - gridDim.x);
+  if (blocks > 1 && threadIdx.x == 0) red_release(&bar->state, (1u << kCountBits) - static_cast<unsigned>(blocks));
 }
 
 // Returns false when the wait gave up (timeout here or an abort elsewhere).
@@ -114,11 +118,12 @@ __device__ __forceinline__ bool barrier_wait(GridBarrier* bar, unsigned generati
 // every other block adds 1, so the arrival that completes the count also
 // flips the high bit and resets the low bits; waiters poll for the flip. One
 // atomic per block and no separate release.
-__device__ __forceinline__ bool grid_sync(GridBarrier* bar, int* status) {
+__device__ __forceinline__ bool grid_sync(GridBarrier* bar, int* status, int blocks, int rank) {
   __shared__ int s_ok;
   __syncthreads();
+  if (blocks == 1) return true;
   if (threadIdx.x == 0) {
-    const unsigned increment = blockIdx.x == 0 ? 0x80000000u - (gridDim.x - 1u) : 1u;
+    const unsigned increment = rank == 0 ? 0x80000000u - static_cast<unsigned>(blocks - 1) : 1u;
     const unsigned old = add_acq_rel(&bar->flip, increment);
     int ok = 1;
     unsigned spins = 0;
@@ -161,9 +166,6 @@ __device__ __forceinline__ double block_sum(double v, double* scratch /* [kWarps
   return total;
 }
 
-// Per-block partial sums live slot-major: partials[slot * blocks + block], so
-// the partials of one slot over all blocks are contiguous.
-__device__ __forceinline__ double* partial_slot(double* partials, int slot) { return partials + slot * gridDim.x; }
 
 // Sums slots [offset, offset + count) over all blocks in a fixed order. The
 // blocks of a slot are cut into kReduceChunks contiguous chunks; one thread
@@ -256,6 +258,14 @@ __host__ __device__ __forceinline__ int align16(int bytes) { return (bytes + 15)
 __host__ __device__ __forceinline__ int slice_bytes(int max_nnz, int max_rows, int value_bytes) {
   return align16(max_nnz * value_bytes) + align16(max_nnz * 4) + align16((max_rows + 1) * 4) + align16(max_rows * 4);
 }
+
+// The blocks that solve one instance: the whole grid in the plain launch, or
+// one block per instance in the batched launch (then every barrier is a
+// __syncthreads and the serial sections run in that block).
+struct Team {
+  int rank;
+  int size;
+};
 
 // Everything one persistent launch needs. Passed by value as kernel argument.
 struct StepArgs {

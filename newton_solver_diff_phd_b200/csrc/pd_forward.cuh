@@ -40,20 +40,19 @@ __device__ __forceinline__ void tet_deformation(const StepArgs& a, int e, const 
     for (int c = 0; c < 3; ++c) f.a[r][c] = static_cast<TL>(m[r][c]);
 }
 
-// Projection stress sum_energies w (P(F) - F_D) of one element sample.
 // SVD of F, warm-started from the singular vectors of the same sample in the
 // previous iteration of this step: B = U0^T F V0 is nearly diagonal, so the
 // Jacobi sweeps on B converge in one rotation sweep; U = U0 Ub, V = V0 Vb. The
 // first iteration of a step starts cold (Eigen's conventions on F itself).
-template <typename TL>
-__device__ __forceinline__ void sample_svd(const StepArgs& a, int sample, bool warm, const M3<TL>& f, M3<TL>& u,
-                                           V3<TL>& sigma, M3<TL>& v) {
-  if (a.svd_u == nullptr || sample < 0) {
+// su, sv: this sample's stored U and V (row-major, TS precision), or nullptr
+// for a cold SVD without stored state.
+template <typename TL, typename TS>
+__device__ __forceinline__ void warm_svd(TS* su, TS* sv, bool warm, const M3<TL>& f, M3<TL>& u, V3<TL>& sigma,
+                                         M3<TL>& v) {
+  if (su == nullptr) {
     unsigned_svd(f, u, sigma, v);
     return;
   }
-  double* su = a.svd_u + 9 * static_cast<size_t>(sample);
-  double* sv = a.svd_v + 9 * static_cast<size_t>(sample);
   if (warm) {
     M3<TL> u0, v0;
 #pragma unroll
@@ -71,13 +70,23 @@ __device__ __forceinline__ void sample_svd(const StepArgs& a, int sample, bool w
   }
 #pragma unroll
   for (int k = 0; k < 9; ++k) {
-    su[k] = static_cast<double>(u.a[k / 3][k % 3]);
-    sv[k] = static_cast<double>(v.a[k / 3][k % 3]);
+    su[k] = static_cast<TS>(u.a[k / 3][k % 3]);
+    sv[k] = static_cast<TS>(v.a[k / 3][k % 3]);
   }
 }
 
-template <typename TL>
-__device__ __forceinline__ M3<TL> sample_stress(const StepArgs& a, int e, int sample, bool warm, const M3<TL>& f,
+// Warm-start state pointers of element sample `sample` (nullptr when the
+// solver keeps none or the lane is padding, sample < 0).
+template <typename TS>
+__device__ __forceinline__ TS* svd_state(TS* base, int sample) {
+  return (base == nullptr || sample < 0) ? nullptr : base + 9 * static_cast<size_t>(sample);
+}
+
+// Projection stress sum_energies w (P(F) - F_D) of one element sample.
+// Args: any argument block with the per-element weights, muscle data, the
+// Neo-Hookean parameters and the status word (StepArgs, BatchInstance).
+template <typename TL, typename Args, typename TS>
+__device__ __forceinline__ M3<TL> sample_stress(const Args& a, int e, TS* su, TS* sv, bool warm, const M3<TL>& f,
                                                 const M3<TL>& fd) {
   M3<TL> stress = zero3<TL>();
   const TL wc = static_cast<TL>(a.wc[e]);
@@ -86,7 +95,7 @@ __device__ __forceinline__ M3<TL> sample_stress(const StepArgs& a, int e, int sa
   if (wc != TL(0) || wv != TL(0) || wn != TL(0)) {
     M3<TL> u, v;
     V3<TL> sigma;
-    sample_svd<TL>(a, sample, warm, f, u, sigma, v);
+    warm_svd<TL, TS>(su, sv, warm, f, u, sigma, v);
     if (wc != TL(0)) stress = stress + wc * (mul(u, transpose(v)) - fd);
     if (wv != TL(0)) {
       bool singular;
@@ -115,13 +124,13 @@ __device__ __forceinline__ M3<TL> sample_stress(const StepArgs& a, int e, int sa
 // Element e belongs to block e % blocks: the local step is spread over every
 // SM instead of filling the first ones.
 template <typename TL>
-__device__ void local_step_tet(const StepArgs& a, bool warm, int gtid, int gthreads) {
-  (void)gtid;
-  for (int e = threadIdx.x * gridDim.x + blockIdx.x; e < a.ne; e += gthreads) {
+__device__ void local_step_tet(const StepArgs& a, bool warm, Team team) {
+  const int gthreads = team.size * blockDim.x;
+  for (int e = threadIdx.x * team.size + team.rank; e < a.ne; e += gthreads) {
     M3<TL> f, fd;
     tet_deformation<TL>(a, e, a.x, f);
     tet_deformation<TL>(a, e, a.boundary, fd);
-    const M3<TL> stress = sample_stress<TL>(a, e, e, warm, f, fd);
+    const M3<TL> stress = sample_stress<TL>(a, e, svd_state(a.svd_u, e), svd_state(a.svd_v, e), warm, f, fd);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       const double* g = a.gradients + (4 * e + k) * 3;
@@ -139,15 +148,14 @@ __device__ void local_step_tet(const StepArgs& a, bool warm, int gtid, int gthre
 // contributions sum_s stress_s g_sj are reduce-scattered across the eight
 // lanes with shuffles (fixed tree), so lane s ends with corner j = s.
 template <typename TL>
-__device__ void local_step_hex(const StepArgs& a, const double* grad_smem, bool warm, int gtid, int gthreads) {
+__device__ void local_step_hex(const StepArgs& a, const double* grad_smem, bool warm, Team team) {
   const int lane = threadIdx.x & 31;
   const int s = lane & 7;
   const int group_in_warp = lane >> 3;
-  const int warps_total = gthreads >> 5;
-  (void)gtid;
+  const int warps_total = (team.size * blockDim.x) >> 5;
   // Cell groups are interleaved over blocks (group g lives in block g % blocks).
   const int warp_in_block = threadIdx.x >> 5;
-  for (int base = (warp_in_block * gridDim.x + blockIdx.x) * 4; base < a.ne; base += warps_total * 4) {
+  for (int base = (warp_in_block * team.size + team.rank) * 4; base < a.ne; base += warps_total * 4) {
     const int e = base + group_in_warp;
     const bool valid = e < a.ne;
     const int ec = valid ? e : a.ne - 1;
@@ -178,7 +186,9 @@ __device__ void local_step_hex(const StepArgs& a, const double* grad_smem, bool 
         fd.a[r][c] = static_cast<TL>(fdm[r][c]);
       }
     // Padding lanes (e >= ne) neither read nor write the warm-start state.
-    const M3<TL> stress = sample_stress<TL>(a, ec, valid ? 8 * ec + s : -1, warm, f, fd);
+    const int sample = valid ? 8 * ec + s : -1;
+    const M3<TL> stress =
+        sample_stress<TL>(a, ec, svd_state(a.svd_u, sample), svd_state(a.svd_v, sample), warm, f, fd);
     // v[j] = stress_s g_sj for the eight corners.
     double vx[8], vy[8], vz[8];
 #pragma unroll
@@ -269,8 +279,8 @@ __device__ __forceinline__ void spmv_rows(const int* off, const int* col, const 
 
 // Copies this block's rows of one product into shared memory (once per launch).
 template <typename TV>
-__device__ void load_slice(const SpmvPlan& plan, const TV* global_values, char* smem) {
-  const int r0 = plan.part[blockIdx.x], r1 = plan.part[blockIdx.x + 1];
+__device__ void load_slice(const SpmvPlan& plan, const TV* global_values, char* smem, int rank) {
+  const int r0 = plan.part[rank], r1 = plan.part[rank + 1];
   const int k0 = plan.off[r0], k1 = plan.off[r1];
   const int nnz = k1 - k0, rows = r1 - r0;
   char* base = smem + plan.smem_offset;
@@ -304,10 +314,10 @@ __device__ __forceinline__ void stage_vector(const double* vec, double* smem_vec
 // bitwise reproducible. Slice data comes from shared memory when resident.
 template <typename TV>
 __device__ void spmv_block(const SpmvPlan& plan, const TV* global_values, bool resident, const char* smem,
-                           const double* vec, double* out) {
-  const int r0 = plan.part[blockIdx.x], r1 = plan.part[blockIdx.x + 1];
+                           const double* vec, double* out, int rank) {
+  const int r0 = plan.part[rank], r1 = plan.part[rank + 1];
   const int rows = r1 - r0;
-  const int nshort = plan.nshort[blockIdx.x];
+  const int nshort = plan.nshort[rank];
   // Resident: row ids, offsets and entries are relative to the block's first
   // row and first entry. Global: absolute.
   const TV* val;
@@ -388,7 +398,7 @@ __device__ __forceinline__ void gram_entry_pair(int entry, int count, int& a, in
 
 // Block partial of the Gram entries over this block's particle rows [r0, r1).
 inline __device__ void gram_partials(const StepArgs& a, int r0, int r1, int count, int start, double* block_out,
-                              double* scratch) {
+                              double* scratch, int blocks) {
   const int entries = gram_entries(count);
   const int capacity = a.window + 1;
   const int groups = entries > 0 ? kBlock / entries : 0;
@@ -430,7 +440,7 @@ inline __device__ void gram_partials(const StepArgs& a, int r0, int r1, int coun
   if (t < entries) {
     double total = 0.0;
     for (int g = 0; g < groups; ++g) total += scratch[g * entries + t];
-    block_out[t * gridDim.x] = total;
+    block_out[t * blocks] = total;
   }
   __syncthreads();
 }

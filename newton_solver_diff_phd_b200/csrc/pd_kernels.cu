@@ -35,9 +35,8 @@ namespace pdb200 {
 // reduction of the per-block partials, then the decision. All blocks read it
 // after the next barrier, so its latency leaves the critical path; a
 // converged step costs one extra local step whose output is discarded.
-__device__ void warp_convergence(const StepArgs& a) {
+__device__ void warp_convergence(const StepArgs& a, int blocks) {
   const int lane = threadIdx.x & 31;
-  const int blocks = gridDim.x;
   double sums[4];
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
@@ -65,17 +64,18 @@ __device__ void warp_convergence(const StepArgs& a) {
   }
 }
 
-// One projective-dynamics step: prologue, every local/global iteration, epilogue.
+// One projective-dynamics step of one instance by one team of blocks:
+// prologue, every local/global iteration, epilogue. Returns false when a team
+// barrier gave up (the status word says why).
 // TL: precision of the local projections; TV: precision of the factor values.
 template <typename TL, typename TV>
-__global__ void __launch_bounds__(kBlock) forward_step_kernel(const StepArgs a) {
-  extern __shared__ __align__(16) char dyn_smem[];
+__device__ __forceinline__ bool forward_step_body(const StepArgs& a, const Team team, char* dyn_smem) {
   __shared__ double s_grad[8 * 8 * 3];
   __shared__ double s_scratch[kBlock];
   __shared__ double s_reduced[64];
   __shared__ int s_control[8];
-  const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
-  const int gthreads = gridDim.x * blockDim.x;
+  const int gtid = team.rank * blockDim.x + threadIdx.x;
+  const int gthreads = team.size * blockDim.x;
   const int n = a.n;
   if (a.hex) {
     for (int t = threadIdx.x; t < 8 * 8 * 3; t += blockDim.x) s_grad[t] = a.gradients[t];
@@ -135,29 +135,29 @@ __global__ void __launch_bounds__(kBlock) forward_step_kernel(const StepArgs a) 
   const TV* st_values = sizeof(TV) == sizeof(double) ? reinterpret_cast<const TV*>(a.st_val)
                                                      : reinterpret_cast<const TV*>(a.st_val32);
   if (a.resident) {
-    load_slice<TV>(a.plan_s, s_values, dyn_smem);
-    load_slice<TV>(a.plan_st, st_values, dyn_smem);
+    load_slice<TV>(a.plan_s, s_values, dyn_smem, team.rank);
+    load_slice<TV>(a.plan_st, st_values, dyn_smem, team.rank);
   }
   double* vector_smem = reinterpret_cast<double*>(dyn_smem + a.vector_smem_offset);
-  if (!grid_sync(a.barrier, a.status)) return;
+  if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
 
-  const int r0 = a.st_part[blockIdx.x], r1 = a.st_part[blockIdx.x + 1];
-  // This block's partial-sum slots: my_partials[slot * gridDim.x].
-  double* my_partials = a.partials + blockIdx.x;
+  const int r0 = a.st_part[team.rank], r1 = a.st_part[team.rank + 1];
+  // This block's partial-sum slots: my_partials[slot * team.size].
+  double* my_partials = a.partials + team.rank;
   const size_t hstride = static_cast<size_t>(3) * n;
 
   PD_TIMER_START();
   for (int iter = 0;; ++iter) {
     // Decision for the previous iteration, overlapped with this local step.
-    if (iter > 0 && blockIdx.x == 0 && (threadIdx.x >> 5) == kWarps - 1) warp_convergence(a);
+    if (iter > 0 && team.rank == 0 && (threadIdx.x >> 5) == kWarps - 1) warp_convergence(a, team.size);
     // ---- P1: local step (warm-started SVD after the first iteration).
     if (a.hex) {
-      local_step_hex<TL>(a, s_grad, iter > 0, gtid, gthreads);
+      local_step_hex<TL>(a, s_grad, iter > 0, team);
     } else {
-      local_step_tet<TL>(a, iter > 0, gtid, gthreads);
+      local_step_tet<TL>(a, iter > 0, team);
     }
     PD_TIMER(0);
-    if (!grid_sync(a.barrier, a.status)) return;
+    if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
     PD_TIMER(5);
     if (iter > 0) {
       if (threadIdx.x == 0) s_control[0] = *reinterpret_cast<volatile int*>(a.active);
@@ -233,7 +233,7 @@ __global__ void __launch_bounds__(kBlock) forward_step_kernel(const StepArgs a) 
       }
     }
     PD_TIMER(1);
-    if (!grid_sync(a.barrier, a.status)) return;
+    if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
     PD_TIMER(5);
     // ---- P3: y = S b.
     {
@@ -242,10 +242,10 @@ __global__ void __launch_bounds__(kBlock) forward_step_kernel(const StepArgs a) 
         stage_vector(a.rhs, vector_smem, n);
         in = vector_smem;
       }
-      spmv_block<TV>(a.plan_s, s_values, a.resident != 0, dyn_smem, in, a.y);
+      spmv_block<TV>(a.plan_s, s_values, a.resident != 0, dyn_smem, in, a.y, team.rank);
     }
     PD_TIMER(2);
-    if (!grid_sync(a.barrier, a.status)) return;
+    if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
     PD_TIMER(5);
 
     // ---- P4: x = S^T y, Dirichlet values, Anderson history and Gram partials.
@@ -255,7 +255,7 @@ __global__ void __launch_bounds__(kBlock) forward_step_kernel(const StepArgs a) 
         stage_vector(a.y, vector_smem, n);
         in = vector_smem;
       }
-      spmv_block<TV>(a.plan_st, st_values, a.resident != 0, dyn_smem, in, a.x);
+      spmv_block<TV>(a.plan_st, st_values, a.resident != 0, dyn_smem, in, a.x, team.rank);
     }
     __syncthreads();
     const int count = a.window > 0 ? a.aa_state[0] : 0;
@@ -280,17 +280,17 @@ __global__ void __launch_bounds__(kBlock) forward_step_kernel(const StepArgs a) 
     }
     if (a.window > 0) {
       __syncthreads();
-      gram_partials(a, r0, r1, count, start, my_partials, s_scratch);
+      gram_partials(a, r0, r1, count, start, my_partials, s_scratch, team.size);
       PD_TIMER(3);
       unsigned generation;
-      if (barrier_arrive(a.barrier, generation)) {
+      if (barrier_arrive(a.barrier, generation, team.size)) {
         const int entries = gram_entries(count);
-        reduce_partials(a.partials, 0, entries, gridDim.x, s_reduced, s_scratch);
+        reduce_partials(a.partials, 0, entries, team.size, s_reduced, s_scratch);
         if (threadIdx.x == 0) aa_solve(a.aa_state, a.aa_gamma, a.aa_accept, s_reduced, a.window);
-        barrier_release(a.barrier, generation);
+        barrier_release(a.barrier, generation, team.size);
         __syncthreads();
       } else if (!barrier_wait(a.barrier, generation, a.status)) {
-        return;
+        return false;
       }
       PD_TIMER(6);
     }
@@ -329,13 +329,13 @@ __global__ void __launch_bounds__(kBlock) forward_step_kernel(const StepArgs a) 
       proj2 = block_sum(proj2, s_scratch);
       PD_TIMER(4);
       if (threadIdx.x == 0) {
-        my_partials[48 * gridDim.x] = step2;
-        my_partials[49 * gridDim.x] = prev2;
-        my_partials[50 * gridDim.x] = change2;
-        my_partials[51 * gridDim.x] = proj2;
+        my_partials[48 * team.size] = step2;
+        my_partials[49 * team.size] = prev2;
+        my_partials[50 * team.size] = change2;
+        my_partials[51 * team.size] = proj2;
       }
       // The decision is taken by one warp during the next local step.
-      if (!grid_sync(a.barrier, a.status)) return;
+      if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
       PD_TIMER(7);
     }
   }
@@ -350,6 +350,14 @@ __global__ void __launch_bounds__(kBlock) forward_step_kernel(const StepArgs a) 
       if (a.x_record != nullptr) a.x_record[3 * i + c] = value;
     }
   }
+  return true;
+}
+
+// Plain launch: the whole cooperative grid is one team solving one instance.
+template <typename TL, typename TV>
+__global__ void __launch_bounds__(kBlock) forward_step_kernel(const StepArgs a) {
+  extern __shared__ __align__(16) char dyn_smem[];
+  forward_step_body<TL, TV>(a, Team{static_cast<int>(blockIdx.x), static_cast<int>(gridDim.x)}, dyn_smem);
 }
 
 // Plain out = S^T (S rhs) with separate launches (SparseInverse.apply).
