@@ -19,8 +19,8 @@
 namespace pdb200 {
 
 // Deformation gradient of a Tet4 element from float64 positions, as a TL matrix.
-template <typename TL>
-__device__ __forceinline__ void tet_deformation(const StepArgs& a, int e, const double* vec, M3<TL>& f) {
+template <typename TL, typename Args>
+__device__ __forceinline__ void tet_deformation(const Args& a, int e, const double* vec, M3<TL>& f) {
   double m[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
@@ -120,130 +120,141 @@ __device__ __forceinline__ M3<TL> sample_stress(const Args& a, int e, TS* su, TS
   return stress;
 }
 
-// P1 for Tet4: one thread per element.
-// Element e belongs to block e % blocks: the local step is spread over every
-// SM instead of filling the first ones.
-template <typename TL>
-__device__ void local_step_tet(const StepArgs& a, bool warm, Team team) {
-  const int gthreads = team.size * blockDim.x;
-  for (int e = threadIdx.x * team.size + team.rank; e < a.ne; e += gthreads) {
-    M3<TL> f, fd;
-    tet_deformation<TL>(a, e, a.x, f);
-    tet_deformation<TL>(a, e, a.boundary, fd);
-    const M3<TL> stress = sample_stress<TL>(a, e, svd_state(a.svd_u, e), svd_state(a.svd_v, e), warm, f, fd);
+// Local step of Tet4 element e: corner contributions stress g_k.
+template <typename TL, typename Args, typename TS>
+__device__ __forceinline__ void tet_element(const Args& a, int e, bool warm, TS* svd_u, TS* svd_v) {
+  M3<TL> f, fd;
+  tet_deformation<TL>(a, e, a.x, f);
+  tet_deformation<TL>(a, e, a.boundary, fd);
+  const M3<TL> stress = sample_stress<TL>(a, e, svd_state(svd_u, e), svd_state(svd_v, e), warm, f, fd);
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const double* g = a.gradients + (4 * e + k) * 3;
-      const V3<TL> gk = v3<TL>(static_cast<TL>(g[0]), static_cast<TL>(g[1]), static_cast<TL>(g[2]));
-      const V3<TL> c = mul(stress, gk);
-      double* out = a.contrib + (4 * e + k) * 3;
-      out[0] = static_cast<double>(c.x);
-      out[1] = static_cast<double>(c.y);
-      out[2] = static_cast<double>(c.z);
-    }
+  for (int k = 0; k < 4; ++k) {
+    const double* g = a.gradients + (4 * e + k) * 3;
+    const V3<TL> gk = v3<TL>(static_cast<TL>(g[0]), static_cast<TL>(g[1]), static_cast<TL>(g[2]));
+    const V3<TL> c = mul(stress, gk);
+    double* out = a.contrib + (4 * e + k) * 3;
+    out[0] = static_cast<double>(c.x);
+    out[1] = static_cast<double>(c.y);
+    out[2] = static_cast<double>(c.z);
   }
 }
 
-// P1 for Hex8: eight lanes per cell, one Gauss sample each; the per-corner
-// contributions sum_s stress_s g_sj are reduce-scattered across the eight
-// lanes with shuffles (fixed tree), so lane s ends with corner j = s.
+// P1 for Tet4: one thread per element. Element e belongs to block
+// e % blocks: the local step is spread over every SM instead of filling the
+// first ones.
+template <typename TL>
+__device__ void local_step_tet(const StepArgs& a, bool warm, Team team) {
+  const int gthreads = team.size * blockDim.x;
+  for (int e = threadIdx.x * team.size + team.rank; e < a.ne; e += gthreads) tet_element<TL>(a, e, warm, a.svd_u, a.svd_v);
+}
+
+// Local step of Hex8 cell e by the eight lanes (lane & 7 = Gauss sample) of
+// one lane group: the per-corner contributions sum_s stress_s g_sj are
+// reduce-scattered across the eight lanes with shuffles (fixed tree), so lane
+// s ends with corner j = s. Every lane of the warp must call this (the
+// shuffles span the warp); lanes with e >= ne compute on a clamped cell,
+// neither read nor write warm-start state and store nothing.
+template <typename TL, typename Args, typename TS>
+__device__ __forceinline__ void hex_cell(const Args& a, const double* grad_smem, int e, bool warm, TS* svd_u,
+                                         TS* svd_v) {
+  const int s = threadIdx.x & 7;
+  const bool valid = e < a.ne;
+  const int ec = valid ? e : a.ne - 1;
+  double fm[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+  double fdm[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const int v = a.indices[8 * ec + j];
+    const double* g = grad_smem + (8 * s + j) * 3;
+    const double px = a.x[3 * v], py = a.x[3 * v + 1], pz = a.x[3 * v + 2];
+    const double bx = a.boundary[3 * v], by = a.boundary[3 * v + 1], bz = a.boundary[3 * v + 2];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      fm[0][c] += px * g[c];
+      fm[1][c] += py * g[c];
+      fm[2][c] += pz * g[c];
+      fdm[0][c] += bx * g[c];
+      fdm[1][c] += by * g[c];
+      fdm[2][c] += bz * g[c];
+    }
+  }
+  M3<TL> f, fd;
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      f.a[r][c] = static_cast<TL>(fm[r][c]);
+      fd.a[r][c] = static_cast<TL>(fdm[r][c]);
+    }
+  const int sample = valid ? 8 * ec + s : -1;
+  const M3<TL> stress = sample_stress<TL>(a, ec, svd_state(svd_u, sample), svd_state(svd_v, sample), warm, f, fd);
+  // v[j] = stress_s g_sj for the eight corners.
+  double vx[8], vy[8], vz[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const double* g = grad_smem + (8 * s + j) * 3;
+    const V3<TL> c = mul(stress, v3<TL>(static_cast<TL>(g[0]), static_cast<TL>(g[1]), static_cast<TL>(g[2])));
+    vx[j] = static_cast<double>(c.x);
+    vy[j] = static_cast<double>(c.y);
+    vz[j] = static_cast<double>(c.z);
+  }
+  // Reduce-scatter over the eight sample lanes: masks 4, 2, 1.
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    const bool upper = (s & 4) != 0;
+    const double sx = upper ? vx[t] : vx[4 + t];
+    const double sy = upper ? vy[t] : vy[4 + t];
+    const double sz = upper ? vz[t] : vz[4 + t];
+    const double rx = __shfl_xor_sync(0xffffffffu, sx, 4);
+    const double ry = __shfl_xor_sync(0xffffffffu, sy, 4);
+    const double rz = __shfl_xor_sync(0xffffffffu, sz, 4);
+    vx[t] = (upper ? vx[4 + t] : vx[t]) + rx;
+    vy[t] = (upper ? vy[4 + t] : vy[t]) + ry;
+    vz[t] = (upper ? vz[4 + t] : vz[t]) + rz;
+  }
+#pragma unroll
+  for (int t = 0; t < 2; ++t) {
+    const bool upper = (s & 2) != 0;
+    const double sx = upper ? vx[t] : vx[2 + t];
+    const double sy = upper ? vy[t] : vy[2 + t];
+    const double sz = upper ? vz[t] : vz[2 + t];
+    const double rx = __shfl_xor_sync(0xffffffffu, sx, 2);
+    const double ry = __shfl_xor_sync(0xffffffffu, sy, 2);
+    const double rz = __shfl_xor_sync(0xffffffffu, sz, 2);
+    vx[t] = (upper ? vx[2 + t] : vx[t]) + rx;
+    vy[t] = (upper ? vy[2 + t] : vy[t]) + ry;
+    vz[t] = (upper ? vz[2 + t] : vz[t]) + rz;
+  }
+  {
+    const bool upper = (s & 1) != 0;
+    const double sx = upper ? vx[0] : vx[1];
+    const double sy = upper ? vy[0] : vy[1];
+    const double sz = upper ? vz[0] : vz[1];
+    const double rx = __shfl_xor_sync(0xffffffffu, sx, 1);
+    const double ry = __shfl_xor_sync(0xffffffffu, sy, 1);
+    const double rz = __shfl_xor_sync(0xffffffffu, sz, 1);
+    vx[0] = (upper ? vx[1] : vx[0]) + rx;
+    vy[0] = (upper ? vy[1] : vy[0]) + ry;
+    vz[0] = (upper ? vz[1] : vz[0]) + rz;
+  }
+  if (valid) {
+    double* out = a.contrib + (8 * e + s) * 3;
+    out[0] = vx[0];
+    out[1] = vy[0];
+    out[2] = vz[0];
+  }
+}
+
+// P1 for Hex8: eight lanes per cell, four cells per warp. Cell groups are
+// interleaved over the team's blocks (group g lives in block g % blocks).
 template <typename TL>
 __device__ void local_step_hex(const StepArgs& a, const double* grad_smem, bool warm, Team team) {
   const int lane = threadIdx.x & 31;
-  const int s = lane & 7;
   const int group_in_warp = lane >> 3;
   const int warps_total = (team.size * blockDim.x) >> 5;
-  // Cell groups are interleaved over blocks (group g lives in block g % blocks).
   const int warp_in_block = threadIdx.x >> 5;
   for (int base = (warp_in_block * team.size + team.rank) * 4; base < a.ne; base += warps_total * 4) {
-    const int e = base + group_in_warp;
-    const bool valid = e < a.ne;
-    const int ec = valid ? e : a.ne - 1;
-    double fm[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-    double fdm[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const int v = a.indices[8 * ec + j];
-      const double* g = grad_smem + (8 * s + j) * 3;
-      const double px = a.x[3 * v], py = a.x[3 * v + 1], pz = a.x[3 * v + 2];
-      const double bx = a.boundary[3 * v], by = a.boundary[3 * v + 1], bz = a.boundary[3 * v + 2];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        fm[0][c] += px * g[c];
-        fm[1][c] += py * g[c];
-        fm[2][c] += pz * g[c];
-        fdm[0][c] += bx * g[c];
-        fdm[1][c] += by * g[c];
-        fdm[2][c] += bz * g[c];
-      }
-    }
-    M3<TL> f, fd;
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        f.a[r][c] = static_cast<TL>(fm[r][c]);
-        fd.a[r][c] = static_cast<TL>(fdm[r][c]);
-      }
-    // Padding lanes (e >= ne) neither read nor write the warm-start state.
-    const int sample = valid ? 8 * ec + s : -1;
-    const M3<TL> stress =
-        sample_stress<TL>(a, ec, svd_state(a.svd_u, sample), svd_state(a.svd_v, sample), warm, f, fd);
-    // v[j] = stress_s g_sj for the eight corners.
-    double vx[8], vy[8], vz[8];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const double* g = grad_smem + (8 * s + j) * 3;
-      const V3<TL> c = mul(stress, v3<TL>(static_cast<TL>(g[0]), static_cast<TL>(g[1]), static_cast<TL>(g[2])));
-      vx[j] = static_cast<double>(c.x);
-      vy[j] = static_cast<double>(c.y);
-      vz[j] = static_cast<double>(c.z);
-    }
-    // Reduce-scatter over the eight sample lanes: masks 4, 2, 1.
-#pragma unroll
-    for (int t = 0; t < 4; ++t) {
-      const bool upper = (s & 4) != 0;
-      const double sx = upper ? vx[t] : vx[4 + t];
-      const double sy = upper ? vy[t] : vy[4 + t];
-      const double sz = upper ? vz[t] : vz[4 + t];
-      const double rx = __shfl_xor_sync(0xffffffffu, sx, 4);
-      const double ry = __shfl_xor_sync(0xffffffffu, sy, 4);
-      const double rz = __shfl_xor_sync(0xffffffffu, sz, 4);
-      vx[t] = (upper ? vx[4 + t] : vx[t]) + rx;
-      vy[t] = (upper ? vy[4 + t] : vy[t]) + ry;
-      vz[t] = (upper ? vz[4 + t] : vz[t]) + rz;
-    }
-#pragma unroll
-    for (int t = 0; t < 2; ++t) {
-      const bool upper = (s & 2) != 0;
-      const double sx = upper ? vx[t] : vx[2 + t];
-      const double sy = upper ? vy[t] : vy[2 + t];
-      const double sz = upper ? vz[t] : vz[2 + t];
-      const double rx = __shfl_xor_sync(0xffffffffu, sx, 2);
-      const double ry = __shfl_xor_sync(0xffffffffu, sy, 2);
-      const double rz = __shfl_xor_sync(0xffffffffu, sz, 2);
-      vx[t] = (upper ? vx[2 + t] : vx[t]) + rx;
-      vy[t] = (upper ? vy[2 + t] : vy[t]) + ry;
-      vz[t] = (upper ? vz[2 + t] : vz[t]) + rz;
-    }
-    {
-      const bool upper = (s & 1) != 0;
-      const double sx = upper ? vx[0] : vx[1];
-      const double sy = upper ? vy[0] : vy[1];
-      const double sz = upper ? vz[0] : vz[1];
-      const double rx = __shfl_xor_sync(0xffffffffu, sx, 1);
-      const double ry = __shfl_xor_sync(0xffffffffu, sy, 1);
-      const double rz = __shfl_xor_sync(0xffffffffu, sz, 1);
-      vx[0] = (upper ? vx[1] : vx[0]) + rx;
-      vy[0] = (upper ? vy[1] : vy[0]) + ry;
-      vz[0] = (upper ? vz[1] : vz[0]) + rz;
-    }
-    if (valid) {
-      double* out = a.contrib + (8 * e + s) * 3;
-      out[0] = vx[0];
-      out[1] = vy[0];
-      out[2] = vz[0];
-    }
+    hex_cell<TL>(a, grad_smem, base + group_in_warp, warm, a.svd_u, a.svd_v);
   }
 }
 

@@ -18,64 +18,16 @@
 #include "../../include/pd_b200.h"
 #include "factor.h"
 #include "pd_kernels.h"
+#include "solver_state.h"
 
 using pdb200::AdjointArgs;
-using pdb200::InverseFactor;
 using pdb200::StepArgs;
 
 namespace {
 
 thread_local std::string g_last_error;
 
-int fail(int code, const std::string& message) {
-  g_last_error = message;
-  return code;
-}
-
-#define PD_CUDA(call)                                                                                 \
-  do {                                                                                                \
-    cudaError_t pd_status_ = (call);                                                                  \
-    if (pd_status_ != cudaSuccess) {                                                                  \
-      return fail(PD_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(pd_status_));           \
-    }                                                                                                 \
-  } while (0)
-
-// Owned device allocation.
-struct DeviceBuffer {
-  void* ptr = nullptr;
-  size_t bytes = 0;
-  DeviceBuffer() = default;
-  DeviceBuffer(const DeviceBuffer&) = delete;
-  DeviceBuffer& operator=(const DeviceBuffer&) = delete;
-  ~DeviceBuffer() { release(); }
-  void release() {
-    if (ptr != nullptr) cudaFree(ptr);
-    ptr = nullptr;
-    bytes = 0;
-  }
-  cudaError_t allocate(size_t size) {
-    release();
-    if (size == 0) size = 16;
-    bytes = size;
-    cudaError_t status = cudaMalloc(&ptr, size);
-    if (status != cudaSuccess) {
-      ptr = nullptr;
-      bytes = 0;
-      return status;
-    }
-    return cudaMemset(ptr, 0, size);
-  }
-  template <typename T>
-  cudaError_t upload(const std::vector<T>& host) {
-    cudaError_t status = allocate(host.size() * sizeof(T));
-    if (status != cudaSuccess || host.empty()) return status;
-    return cudaMemcpy(ptr, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice);
-  }
-  template <typename T>
-  T* as() const {
-    return static_cast<T*>(ptr);
-  }
-};
+int fail(int code, const std::string& message) { return pd_set_error(code, message); }
 
 // Contiguous row ranges with balanced cost (nnz + per-row overhead) per block.
 std::vector<int32_t> partition_rows(const std::vector<int32_t>& offsets, int blocks) {
@@ -132,54 +84,11 @@ void plan_rows(const std::vector<int32_t>& offsets, const std::vector<int32_t>& 
 
 }  // namespace
 
-struct PdSolver {
-  int device = 0;
-  int n = 0, ne = 0, corners = 0, hex = 0;
-  double mean_volume = 0.0;
-  PdOptions options{};
-  std::vector<int32_t> indices;
-  std::vector<double> gradients;
-  std::vector<int32_t> free_;
-  bool has_dirichlet = false;
-  // Materials and energies (host copies).
-  std::vector<double> mu, lame;
-  bool materials_set = false;
-  std::vector<double> muscle_dir, muscle_stiffness;
-  bool has_muscles = false;
-  std::vector<double> muscle_targets;
-  const float* activations = nullptr;
-  std::vector<int32_t> plane_vertices;
-  std::vector<double> plane_stiffness;
-  double plane[4] = {0, 0, 0, 0};
-  // Build state.
-  bool built = false;
-  bool stale = true;
-  double built_dt = 0.0;
-  double inertia = 0.0, mass = 0.0;
-  double nh_mu = 0.0, nh_lame = 0.0, nh_penalty = 0.0;
-  int blocks = 0;
-  int max_blocks = 0;
-  // Launch plan of the sparse products.
-  pdb200::SpmvPlan plan_s{}, plan_st{};
-  int resident = 0, stage_vector = 0, vector_smem_offset = 0;
-  size_t smem = 0;
-  DeviceBuffer d_s_rowlist, d_s_nshort, d_st_rowlist, d_st_nshort, d_svd_u, d_svd_v;
-  unsigned long long* timers = nullptr;  // phase timers of PD_PHASE_TIMERS builds
-  InverseFactor factor;
-  // Device mesh data.
-  DeviceBuffer d_indices, d_gradients, d_free, d_inc_offsets, d_inc_entries, d_plane_weight;
-  DeviceBuffer d_wc, d_wv, d_wn, d_wm, d_mdir, d_mtarget;
-  DeviceBuffer d_s_off, d_s_col, d_s_val, d_s_val32, d_st_off, d_st_col, d_st_val, d_st_val32, d_s_part, d_st_part;
-  DeviceBuffer d_a_off, d_a_col, d_a_val;
-  // Step vectors.
-  DeviceBuffer d_position, d_velocity, d_target, d_boundary, d_x, d_prev, d_proj, d_prev_proj, d_rhs, d_y, d_contrib;
-  DeviceBuffer d_hist_x, d_hist_g, d_aa_state, d_aa_gamma, d_aa_accept, d_partials;
-  DeviceBuffer d_iteration, d_active, d_status, d_barrier;
-  // Adjoint vectors.
-  DeviceBuffer b_rhs, b_base, b_solution, b_prev, b_work, b_y, b_raw, b_contrib, b_jac, b_hist_x, b_hist_g, b_aa_state,
-      b_aa_gamma, b_aa_accept, b_partials, b_iteration, b_active, b_control_d, b_control_i, b_material_scratch,
-      b_activation_scratch, b_zero_gq, b_zero_gqd, b_scratch_gq, b_scratch_gqd, b_scratch_gf;
-};
+int pd_set_error(int code, const std::string& message) {
+  g_last_error = message;
+  return code;
+}
+
 
 namespace {
 
