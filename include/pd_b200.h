@@ -51,7 +51,10 @@ extern "C" {
 #define PD_MATERIAL_NEO_HOOKEAN 1 /* proximal Neo-Hookean, weight 2 mu */
 
 #define PD_PRECISION_FP64 0        /* every solver operation in float64, as the reference */
-#define PD_PRECISION_FP32_REFINE 1 /* fp32 local step and factor, fp64 residual refinement */
+#define PD_PRECISION_FP32_REFINE 1 /* fp32 factor products with fp64 residual refinement; fp64 local step:
+                                      the converged positions are the fp64 solver's */
+#define PD_PRECISION_FP32 2        /* fp32+refine with fp32 local projections and adjoint Jacobians: fastest;
+                                      the fixed point moves by about cond(A) * 6e-8 relative */
 
 #define PD_ADJOINT_REFERENCE 0 /* K with the mean weight per energy (adjoint.py:17-18) */
 #define PD_ADJOINT_EXACT 1     /* K with per-element weights: the derivative of the forward map */
@@ -192,6 +195,56 @@ int pd_apply_inverse(PdSolver* solver, const double* rhs, double* out, void* str
    capture. All calls share the array: calls that overlap on the GPU race. */
 int pd_apply_inverse_static(PdSolver* solver, const double* rhs, double* out, void* stream);
 
+/* ---- Batched rollouts.
+   Many independent built solvers (uneven sizes allowed) advanced together:
+   one CUDA graph per rollout, every PD step a WHILE loop of per-phase kernels
+   over all instances that still iterate. Each instance follows the same
+   algorithm as pd_step (solver.py:582-687: local step, gather, S^T S solve,
+   Anderson, dual convergence gate) with its own tolerances and iteration
+   limit; the factor is the instance's own, stored in postorder run format.
+   The reference steps one model at a time; batching has no counterpart there.
+   Instances do not wait for each other between steps: an instance whose
+   step has converged writes it out and starts its next step while others
+   are still iterating.
+   Every solver must be built for the same dt, on one device, with one
+   precision and one state precision, without Dirichlet targets or Tet4
+   activations. The solvers must outlive the batch and must not step on
+   their own while a batched rollout runs (the batch uses their buffers). */
+typedef struct PdBatch PdBatch;
+typedef struct PdBatchOptions {
+  int32_t svd_warm_start; /* 1: warm-started SVD of every element sample after the first iteration */
+  int32_t task_nnz;       /* factor entries per product task (>= 256; default 32768) */
+  int32_t run_gap;        /* omitted zeros bridged inside a run (default 2) */
+  int32_t local_cells;    /* Hex8 cells per local-step task (>= 4; default 64) */
+} PdBatchOptions;
+/* options may be NULL (defaults). */
+int pd_batch_create(PdSolver* const* solvers, int32_t count, const PdBatchOptions* options, PdBatch** out);
+int pd_batch_destroy(PdBatch* batch);
+/* First particle / element of each instance in the concatenated arrays, [count + 1] each. */
+int pd_batch_layout(const PdBatch* batch, int64_t* particle_offsets, int64_t* element_offsets);
+/* Stored factor values (S and S^T), runs, and task counts [local, gather, S, S^T]. */
+int pd_batch_factor_stats(const PdBatch* batch, int64_t* values, int64_t* runs, int64_t* tasks);
+/* Rollout of `steps` PD steps of every instance (SolverDiffPhD.step repeated,
+   solver.py:689-786). q0, qd0: device [P][3] in the state precision (P = all
+   particles); forces: device [P][3] per step, step t at forces + t *
+   force_step_stride elements (0: the same forces every step); q_traj,
+   qd_traj: device [steps][P][3] outputs; x_record: device float64
+   [steps][P][3] or NULL. The graph is rebuilt when any pointer, steps, dt or
+   gravity differs from the previous call. */
+int pd_batch_forward(PdBatch* batch, int32_t steps, double dt, const double gravity[3], const void* q0,
+                     const void* qd0, const void* forces, int64_t force_step_stride, void* q_traj, void* qd_traj,
+                     double* x_record, void* stream);
+/* The same rollout without a graph: every kernel launched on its own, the
+   loop decided on the host every 16 passes (synchronises). For profilers
+   that follow plain launches; results equal pd_batch_forward's. */
+int pd_batch_forward_stepwise(PdBatch* batch, int32_t steps, double dt, const double gravity[3], const void* q0,
+                              const void* qd0, const void* forces, int64_t force_step_stride, void* q_traj,
+                              void* qd_traj, double* x_record, void* stream);
+/* Status bits per instance (accumulated, not cleared), [count], and the
+   iteration count of every step of the last rollout, [steps][count]. Either
+   pointer may be NULL. Synchronises the stream. */
+int pd_batch_read(PdBatch* batch, int32_t* status, int32_t* iterations, void* stream);
+
 /* Host factor build for an arbitrary SPD matrix given as full symmetric CSR
    (SparseInverse.__init__, sparse.py:291-320). Arrays are host memory; the
    result is freed with pd_inverse_free. */
@@ -204,6 +257,17 @@ int pd_inverse_sizes(const PdInverseFactor* factor, int32_t* size, int64_t* nnz,
 int pd_inverse_export(const PdInverseFactor* factor, int32_t* permutation, int32_t* s_offsets, int32_t* s_columns,
                       double* s_values, int32_t* st_offsets, int32_t* st_columns, double* st_values);
 int pd_inverse_free(PdInverseFactor* factor);
+/* The factor in postorder run format (the storage of the batched path): rows
+   of S and S^T as runs of consecutive labels, omitted zeros bridged inside a
+   run when at most max_gap of them lie between two stored entries. Sizes
+   first; then label_of[size], s_row_runs[size+1], s_run_col[s_runs],
+   s_run_off[s_runs+1], s_values[s_values], and the same for S^T. No
+   counterpart in the reference (sparse.py keeps CSR only). */
+int pd_inverse_run_sizes(const PdInverseFactor* factor, int32_t max_gap, int64_t* s_runs, int64_t* s_values,
+                         int64_t* st_runs, int64_t* st_values);
+int pd_inverse_run_export(const PdInverseFactor* factor, int32_t max_gap, int32_t* label_of, int32_t* s_row_runs,
+                          int32_t* s_run_col, int32_t* s_run_off, double* s_values, int32_t* st_row_runs,
+                          int32_t* st_run_col, int32_t* st_run_off, double* st_values);
 
 #ifdef __cplusplus
 }

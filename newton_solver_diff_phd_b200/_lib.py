@@ -31,6 +31,7 @@ STATUS_BARRIER_TIMEOUT = 1024
 
 PRECISION_FP64 = 0
 PRECISION_FP32_REFINE = 1
+PRECISION_FP32 = 2
 ADJOINT_REFERENCE = 0
 ADJOINT_EXACT = 1
 
@@ -70,6 +71,15 @@ class PdOptions(ctypes.Structure):
     ]
 
 
+class PdBatchOptions(ctypes.Structure):
+    _fields_ = [
+        ("svd_warm_start", ctypes.c_int32),
+        ("task_nnz", ctypes.c_int32),
+        ("run_gap", ctypes.c_int32),
+        ("local_cells", ctypes.c_int32),
+    ]
+
+
 _P = ctypes.c_void_p
 _I32 = ctypes.c_int32
 _I64 = ctypes.c_int64
@@ -96,10 +106,20 @@ SIGNATURES = {
     "pd_deformation_determinants": ([_P, _P, _P, _P], ctypes.c_int),
     "pd_apply_inverse": ([_P, _P, _P, _P], ctypes.c_int),
     "pd_apply_inverse_static": ([_P, _P, _P, _P], ctypes.c_int),
+    "pd_batch_create": ([_P, _I32, ctypes.POINTER(PdBatchOptions), ctypes.POINTER(_P)], ctypes.c_int),
+    "pd_batch_destroy": ([_P], ctypes.c_int),
+    "pd_batch_layout": ([_P, _P, _P], ctypes.c_int),
+    "pd_batch_factor_stats": ([_P, ctypes.POINTER(_I64), ctypes.POINTER(_I64), _P], ctypes.c_int),
+    "pd_batch_forward": ([_P, _I32, _D, _P, _P, _P, _P, _I64, _P, _P, _P, _P], ctypes.c_int),
+    "pd_batch_forward_stepwise": ([_P, _I32, _D, _P, _P, _P, _P, _I64, _P, _P, _P, _P], ctypes.c_int),
+    "pd_batch_read": ([_P, _P, _P, _P], ctypes.c_int),
     "pd_inverse_build": ([_I32, _P, _P, _P, ctypes.POINTER(_P)], ctypes.c_int),
     "pd_inverse_sizes": ([_P, ctypes.POINTER(_I32), ctypes.POINTER(_I64), ctypes.POINTER(_I64)], ctypes.c_int),
     "pd_inverse_export": ([_P, _P, _P, _P, _P, _P, _P, _P], ctypes.c_int),
     "pd_inverse_free": ([_P], ctypes.c_int),
+    "pd_inverse_run_sizes": ([_P, _I32, ctypes.POINTER(_I64), ctypes.POINTER(_I64), ctypes.POINTER(_I64),
+                              ctypes.POINTER(_I64)], ctypes.c_int),
+    "pd_inverse_run_export": ([_P, _I32] + [_P] * 9, ctypes.c_int),
 }
 
 _lock = threading.Lock()
@@ -151,11 +171,12 @@ def ptr(array) -> int | None:
     return array.data_ptr()
 
 
-def inverse_factor(matrix_csr):
+def inverse_factor(matrix_csr, run_gap=None):
     """Build the exact inverse factor of an SPD CSR matrix with the C++ host builder.
 
     ``matrix_csr`` is ``(offsets, columns, values)`` of the full symmetric matrix.
-    Returns a dict with ``permutation`` and the CSR arrays of S and S^T.
+    Returns a dict with ``permutation`` and the CSR arrays of S and S^T; with
+    ``run_gap`` also ``runs``, the postorder run format of both.
     """
     offsets, columns, values = (
         np.ascontiguousarray(matrix_csr[0], dtype=np.int32),
@@ -185,6 +206,23 @@ def inverse_factor(matrix_csr):
             )
         )
         out["factorization_nnz"] = factorization.value
+        if run_gap is not None:
+            counts = [_I64() for _ in range(4)]
+            check(lib.pd_inverse_run_sizes(handle, int(run_gap), *(ctypes.byref(c) for c in counts)))
+            s_runs, s_values, st_runs, st_values = (c.value for c in counts)
+            runs = {
+                "label_of": np.empty(n, np.int32),
+                "s_row_runs": np.empty(n + 1, np.int32),
+                "s_run_col": np.empty(s_runs, np.int32),
+                "s_run_off": np.empty(s_runs + 1, np.int32),
+                "s_values": np.empty(s_values, np.float64),
+                "st_row_runs": np.empty(n + 1, np.int32),
+                "st_run_col": np.empty(st_runs, np.int32),
+                "st_run_off": np.empty(st_runs + 1, np.int32),
+                "st_values": np.empty(st_values, np.float64),
+            }
+            check(lib.pd_inverse_run_export(handle, int(run_gap), *(ptr(runs[k]) for k in runs)))
+            out["runs"] = runs
         return out
     finally:
         lib.pd_inverse_free(handle)

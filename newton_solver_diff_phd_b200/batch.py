@@ -1,0 +1,159 @@
+"""Batched rollouts: many independent :class:`SolverDiffPhD` instances in one CUDA graph.
+
+The reference advances one Newton model per ``SolverDiffPhD.step`` call
+(``src/newton_solver_diff_phd/_src/solvers/diff_phd/solver.py:689-786``). For
+many small meshes of uneven size that leaves a B200 idle, so this module runs
+the steps of every instance together: per PD step, each phase of the
+local/global iteration is one kernel over the work of all instances still
+iterating, repeated by a device-side loop of a CUDA graph. An instance whose step has
+passed its convergence gate writes it out and starts its next step at once,
+so instances never wait for each other between steps. Each instance keeps its own
+materials, tolerances, iteration limit, Anderson window and factor; the
+result of an instance equals its single-instance ``step`` to rounding.
+
+States are concatenated: instance ``i`` owns particles
+``particle_offsets[i]:particle_offsets[i+1]`` of every ``(P, 3)`` array.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from .solver import SolverDiffPhD, _stream
+
+
+class BatchedSolver:
+    """A fixed set of solvers stepped together (``pd_batch_*`` in ``include/pd_b200.h``).
+
+    Every solver is built for ``dt`` here (as its first ``step`` would). The
+    solvers must share device, precision and state dtype, must outlive the
+    batch, and must not be stepped on their own while a batched rollout runs.
+    Dirichlet targets and Tet4 muscle activations are not supported.
+    """
+
+    def __init__(self, solvers: list[SolverDiffPhD], dt: float, *, svd_warm_start: bool = True,
+                 task_nnz: int = 32768, run_gap: int = 2, local_cells: int = 64):
+        if not solvers:
+            raise ValueError("BatchedSolver needs at least one solver")
+        if not np.isfinite(dt) or dt <= 0:
+            raise ValueError("dt must be finite and positive")
+        first = solvers[0]
+        for solver in solvers:
+            if not isinstance(solver, SolverDiffPhD):
+                raise TypeError("BatchedSolver takes SolverDiffPhD instances")
+            if solver.device != first.device or solver.state_dtype != first.state_dtype:
+                raise ValueError("batched solvers must share device and state dtype")
+        self.dt = float(dt)
+        self.device = first.device
+        self.state_dtype = first.state_dtype
+        for solver in solvers:
+            if solver._model_changed or solver._factor_key != self.dt:
+                solver._build(self.dt)
+            solver._sync_hex_targets()
+        gravities = np.stack([s._gravity for s in solvers])
+        if not np.all(gravities == gravities[0]):
+            raise ValueError("batched solvers must share gravity")
+        self._gravity = np.ascontiguousarray(gravities[0])
+        self.solvers = list(solvers)
+        self._lib = _lib.library()
+        handles = (ctypes.c_void_p * len(solvers))(*[ctypes.cast(s._handle, ctypes.c_void_p).value for s in solvers])
+        options = _lib.PdBatchOptions(int(svd_warm_start), int(task_nnz), int(run_gap), int(local_cells))
+        handle = ctypes.c_void_p()
+        _lib.check(self._lib.pd_batch_create(ctypes.cast(handles, ctypes.c_void_p), len(solvers), ctypes.byref(options), ctypes.byref(handle)))
+        self._handle = handle
+        particles = np.zeros(len(solvers) + 1, np.int64)
+        elements = np.zeros(len(solvers) + 1, np.int64)
+        _lib.check(self._lib.pd_batch_layout(self._handle, _lib.ptr(particles), _lib.ptr(elements)))
+        self.particle_offsets = particles
+        self.element_offsets = elements
+        self.particle_count = int(particles[-1])
+        self._steps = 0
+
+    @property
+    def count(self) -> int:
+        return len(self.solvers)
+
+    def factor_stats(self) -> dict:
+        values, runs = ctypes.c_int64(), ctypes.c_int64()
+        tasks = np.zeros(4, np.int64)
+        _lib.check(self._lib.pd_batch_factor_stats(self._handle, ctypes.byref(values), ctypes.byref(runs),
+                                                   _lib.ptr(tasks)))
+        return {"values": values.value, "runs": runs.value, "tasks": dict(zip(("local", "gather", "s", "st"),
+                                                                                tasks.tolist()))}
+
+    def concat(self, tensors) -> torch.Tensor:
+        """Concatenate per-instance ``(n_i, 3)`` tensors into one ``(P, 3)`` state array."""
+        out = torch.cat([t.to(self.device, self.state_dtype) for t in tensors]).contiguous()
+        if out.shape != (self.particle_count, 3):
+            raise ValueError("per-instance tensors must match the instance particle counts")
+        return out
+
+    def split(self, tensor: torch.Tensor) -> list[torch.Tensor]:
+        """Per-instance views of the last axis-(-2) ``P`` rows of a concatenated array."""
+        o = self.particle_offsets
+        return [tensor[..., o[i]:o[i + 1], :] for i in range(self.count)]
+
+    def rollout(self, q0: torch.Tensor, qd0: torch.Tensor, forces: torch.Tensor, steps: int, *,
+                record: bool = True, out=None, stepwise: bool = False):
+        """Run ``steps`` PD steps of every instance in one graph launch.
+
+        ``q0``, ``qd0``: ``(P, 3)``; ``forces``: ``(P, 3)`` applied every step or
+        ``(steps, P, 3)``. Returns ``(q, qd, x_record)`` with ``q``, ``qd`` of
+        shape ``(steps, P, 3)`` (state dtype) and ``x_record`` float64
+        ``(steps, P, 3)`` (or ``None``). ``out`` may pass those three arrays
+        to reuse them (the captured graph is reused while every pointer matches).
+        ``stepwise=True`` launches the same kernels one by one instead of as
+        one graph (for profilers; slower, same results).
+        """
+        steps = int(steps)
+        if steps < 1:
+            raise ValueError("steps must be positive")
+        shape = (self.particle_count, 3)
+        for name, tensor in (("q0", q0), ("qd0", qd0)):
+            if tensor.dtype != self.state_dtype or tuple(tensor.shape) != shape or not tensor.is_contiguous():
+                raise ValueError(f"{name} must be a contiguous {self.state_dtype} (P, 3) tensor")
+            if tensor.device != self.device:
+                raise ValueError(f"{name} must be on the solver device")
+        if forces.dtype != self.state_dtype or not forces.is_contiguous() or forces.device != self.device:
+            raise ValueError("forces must be a contiguous tensor of the state dtype on the solver device")
+        if tuple(forces.shape) == shape:
+            stride = 0
+        elif tuple(forces.shape) == (steps,) + shape:
+            stride = 3 * self.particle_count
+        else:
+            raise ValueError("forces must have shape (P, 3) or (steps, P, 3)")
+        if out is None:
+            q = torch.empty((steps,) + shape, dtype=self.state_dtype, device=self.device)
+            qd = torch.empty_like(q)
+            x_record = torch.empty((steps,) + shape, dtype=torch.float64, device=self.device) if record else None
+        else:
+            q, qd, x_record = out
+        self._steps = steps
+        _lib.check(
+            (self._lib.pd_batch_forward_stepwise if stepwise else self._lib.pd_batch_forward)(
+                self._handle, steps, self.dt, _lib.ptr(self._gravity), _lib.ptr(q0), _lib.ptr(qd0), _lib.ptr(forces),
+                stride, _lib.ptr(q), _lib.ptr(qd), _lib.ptr(x_record), _stream(),
+            )
+        )
+        return q, qd, x_record
+
+    def read(self):
+        """``(status bits per instance, iterations (steps, count) of the last rollout)``; synchronises."""
+        status = np.zeros(self.count, np.int32)
+        iterations = np.zeros((max(self._steps, 0), self.count), np.int32)
+        _lib.check(self._lib.pd_batch_read(self._handle, _lib.ptr(status), _lib.ptr(iterations) if self._steps else None,
+                                           _stream()))
+        return status, iterations
+
+    def __del__(self):
+        handle = getattr(self, "_handle", None)
+        if handle is not None and handle.value:
+            try:
+                self._lib.pd_batch_destroy(handle)
+            except Exception:
+                pass
+            self._handle = None

@@ -20,7 +20,7 @@ INCLUDE = PACKAGE.parent / "include"
 BUILD = PACKAGE / "_build"
 LIBRARY = BUILD / "libpdb200.so"
 
-CUDA_SOURCES = ("pd_kernels.cu", "pd_adjoint.cu", "pd_solver.cu", "pd_noalloc.cu")
+CUDA_SOURCES = ("pd_kernels.cu", "pd_adjoint.cu", "pd_solver.cu", "pd_noalloc.cu", "pd_batch.cu")
 HOST_SOURCES = ("factor.cpp", "runs.cpp")
 HEADERS = ("factor.h", "pd_math.cuh", "pd_device.cuh", "pd_forward.cuh", "pd_kernels.h")
 ARCH = ("-gencode", "arch=compute_100a,code=sm_100a")

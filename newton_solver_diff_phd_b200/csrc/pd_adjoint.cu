@@ -945,9 +945,11 @@ __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs 
   adjoint_step_body<TL, TV>(b, Team{static_cast<int>(blockIdx.x), static_cast<int>(gridDim.x)}, dyn_smem);
 }
 
+// precision 0: FP64; 1: FP64 Jacobians, FP32 factor products; 2: FP32 Jacobians and factor.
 static const void* adjoint_kernel(int precision) {
-  return precision == 0 ? reinterpret_cast<const void*>(&adjoint_step_kernel<double, double>)
-                        : reinterpret_cast<const void*>(&adjoint_step_kernel<float, float>);
+  if (precision == 0) return reinterpret_cast<const void*>(&adjoint_step_kernel<double, double>);
+  if (precision == 1) return reinterpret_cast<const void*>(&adjoint_step_kernel<double, float>);
+  return reinterpret_cast<const void*>(&adjoint_step_kernel<float, float>);
 }
 
 cudaError_t launch_adjoint_step(const AdjointArgs& args, int blocks, int precision, size_t smem, cudaStream_t stream) {
@@ -955,9 +957,21 @@ cudaError_t launch_adjoint_step(const AdjointArgs& args, int blocks, int precisi
   return cudaLaunchCooperativeKernel(adjoint_kernel(precision), dim3(blocks), dim3(kBlock), params, smem, stream);
 }
 
+// Allows the device's largest dynamic shared memory for the kernel (an
+// attribute of the function, shared by every solver on the device, so it is
+// never lowered to one solver's need) and returns the occupancy at `smem`.
 cudaError_t adjoint_step_max_blocks(int precision, size_t smem, int* blocks_per_sm) {
   const void* kernel = adjoint_kernel(precision);
-  cudaError_t status = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  int device = 0, optin = 0;
+  cudaError_t status = cudaGetDevice(&device);
+  if (status != cudaSuccess) return status;
+  status = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+  if (status != cudaSuccess) return status;
+  cudaFuncAttributes attributes{};
+  status = cudaFuncGetAttributes(&attributes, kernel);
+  if (status != cudaSuccess) return status;
+  status = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                optin - static_cast<int>(attributes.sharedSizeBytes));
   if (status != cudaSuccess) return status;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kernel, kBlock, smem);
 }

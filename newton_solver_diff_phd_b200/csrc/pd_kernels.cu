@@ -406,9 +406,11 @@ __global__ void hex_determinants_kernel(const float* q, const int* indices, cons
 // ---------------------------------------------------------------------------
 // Host launchers.
 
+// precision 0: FP64; 1: FP64 local step, FP32 factor products; 2: FP32 local step and factor.
 static const void* forward_kernel(int precision) {
-  return precision == 0 ? reinterpret_cast<const void*>(&forward_step_kernel<double, double>)
-                        : reinterpret_cast<const void*>(&forward_step_kernel<float, float>);
+  if (precision == 0) return reinterpret_cast<const void*>(&forward_step_kernel<double, double>);
+  if (precision == 1) return reinterpret_cast<const void*>(&forward_step_kernel<double, float>);
+  return reinterpret_cast<const void*>(&forward_step_kernel<float, float>);
 }
 
 cudaError_t launch_forward_step(const StepArgs& args, int blocks, int precision, size_t smem, cudaStream_t stream) {
@@ -416,9 +418,21 @@ cudaError_t launch_forward_step(const StepArgs& args, int blocks, int precision,
   return cudaLaunchCooperativeKernel(forward_kernel(precision), dim3(blocks), dim3(kBlock), params, smem, stream);
 }
 
+// Allows the device's largest dynamic shared memory for the kernel (an
+// attribute of the function, shared by every solver on the device, so it is
+// never lowered to one solver's need) and returns the occupancy at `smem`.
 cudaError_t forward_step_max_blocks(int precision, size_t smem, int* blocks_per_sm) {
   const void* kernel = forward_kernel(precision);
-  cudaError_t status = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  int device = 0, optin = 0;
+  cudaError_t status = cudaGetDevice(&device);
+  if (status != cudaSuccess) return status;
+  status = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+  if (status != cudaSuccess) return status;
+  cudaFuncAttributes attributes{};
+  status = cudaFuncGetAttributes(&attributes, kernel);
+  if (status != cudaSuccess) return status;
+  status = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                optin - static_cast<int>(attributes.sharedSizeBytes));
   if (status != cudaSuccess) return status;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kernel, kBlock, smem);
 }

@@ -17,6 +17,7 @@
 
 #include "../../include/pd_b200.h"
 #include "factor.h"
+#include "runs.h"
 #include "pd_kernels.h"
 #include "solver_state.h"
 
@@ -101,8 +102,8 @@ int validate_options(const PdOptions& o) {
   if (o.max_iterations < 1) return fail(PD_ERR_INVALID, "max_iterations must be a positive integer");
   if (o.anderson_window < 0 || o.anderson_window > pdb200::kMaxWindow)
     return fail(PD_ERR_INVALID, "anderson_window must be an integer in [0, 8]");
-  if (o.precision != PD_PRECISION_FP64 && o.precision != PD_PRECISION_FP32_REFINE)
-    return fail(PD_ERR_INVALID, "precision must be fp64 or fp32+refine");
+  if (o.precision != PD_PRECISION_FP64 && o.precision != PD_PRECISION_FP32_REFINE && o.precision != PD_PRECISION_FP32)
+    return fail(PD_ERR_INVALID, "precision must be fp64, fp32+refine or fp32");
   if (o.adjoint_mode != PD_ADJOINT_REFERENCE && o.adjoint_mode != PD_ADJOINT_EXACT)
     return fail(PD_ERR_INVALID, "adjoint mode must be reference or exact");
   if (o.blocks < 0) return fail(PD_ERR_INVALID, "blocks must be nonnegative");
@@ -127,7 +128,7 @@ int ensure_adjoint_buffers(PdSolver* s) {
     PD_CUDA(buffer->allocate(vec));
   PD_CUDA(s->b_contrib.allocate(static_cast<size_t>(s->ne) * s->corners * 3 * sizeof(double)));
   const size_t jac_entries = static_cast<size_t>(s->ne) * samples_of(s) * 81;
-  PD_CUDA(s->b_jac.allocate(jac_entries * (s->options.precision == PD_PRECISION_FP64 ? sizeof(double) : sizeof(float))));
+  PD_CUDA(s->b_jac.allocate(jac_entries * (s->options.precision == PD_PRECISION_FP32 ? sizeof(float) : sizeof(double))));
   const size_t window = static_cast<size_t>(s->options.anderson_window);
   PD_CUDA(s->b_hist_x.allocate((window + 1) * vec));
   PD_CUDA(s->b_hist_g.allocate((window + 1) * vec));
@@ -500,7 +501,7 @@ int pd_build(PdSolver* s, double dt) {
   PD_CUDA(s->d_st_off.upload(s->factor.st.offsets));
   PD_CUDA(s->d_st_col.upload(s->factor.st.columns));
   PD_CUDA(s->d_st_val.upload(s->factor.st.values));
-  if (s->options.precision == PD_PRECISION_FP32_REFINE) {
+  if (s->options.precision != PD_PRECISION_FP64) {
     std::vector<float> s32(s->factor.s.values.begin(), s->factor.s.values.end());
     std::vector<float> st32(s->factor.st.values.begin(), s->factor.st.values.end());
     PD_CUDA(s->d_s_val32.upload(s32));
@@ -644,7 +645,7 @@ int pd_step(PdSolver* s, const void* q, const void* qd, const void* f, const voi
   a.a_off = s->d_a_off.as<int>();
   a.a_col = s->d_a_col.as<int>();
   a.a_val = s->d_a_val.as<double>();
-  a.refine = s->options.precision == PD_PRECISION_FP32_REFINE ? 1 : 0;
+  a.refine = s->options.precision != PD_PRECISION_FP64 ? 1 : 0;
   a.position = s->d_position.as<double>();
   a.velocity = s->d_velocity.as<double>();
   a.target = s->d_target.as<double>();
@@ -756,7 +757,7 @@ int pd_backward(PdSolver* s, const double* x_record, const float* activations, d
   b.a_off = s->d_a_off.as<int>();
   b.a_col = s->d_a_col.as<int>();
   b.a_val = s->d_a_val.as<double>();
-  b.refine = s->options.precision == PD_PRECISION_FP32_REFINE ? 1 : 0;
+  b.refine = s->options.precision != PD_PRECISION_FP64 ? 1 : 0;
   b.x = x_record;
   b.rhs = s->b_rhs.as<double>();
   b.base = s->b_base.as<double>();
@@ -932,6 +933,37 @@ int pd_inverse_export(const PdInverseFactor* f, int32_t* permutation, int32_t* s
 
 int pd_inverse_free(PdInverseFactor* f) {
   delete f;
+  return PD_OK;
+}
+
+int pd_inverse_run_sizes(const PdInverseFactor* f, int32_t max_gap, int64_t* s_runs, int64_t* s_values,
+                         int64_t* st_runs, int64_t* st_values) {
+  if (f == nullptr || max_gap < 0) return fail(PD_ERR_INVALID, "null factor or negative gap");
+  const pdb200::RunFactor runs = pdb200::build_run_factor(f->factor, max_gap);
+  if (s_runs) *s_runs = static_cast<int64_t>(runs.s.run_col.size());
+  if (s_values) *s_values = static_cast<int64_t>(runs.s.values.size());
+  if (st_runs) *st_runs = static_cast<int64_t>(runs.st.run_col.size());
+  if (st_values) *st_values = static_cast<int64_t>(runs.st.values.size());
+  return PD_OK;
+}
+
+int pd_inverse_run_export(const PdInverseFactor* f, int32_t max_gap, int32_t* label_of, int32_t* s_row_runs,
+                          int32_t* s_run_col, int32_t* s_run_off, double* s_values, int32_t* st_row_runs,
+                          int32_t* st_run_col, int32_t* st_run_off, double* st_values) {
+  if (f == nullptr || max_gap < 0) return fail(PD_ERR_INVALID, "null factor or negative gap");
+  const pdb200::RunFactor runs = pdb200::build_run_factor(f->factor, max_gap);
+  auto copy = [](auto* dst, const auto& src) {
+    if (dst != nullptr && !src.empty()) std::memcpy(dst, src.data(), src.size() * sizeof(src[0]));
+  };
+  copy(label_of, runs.label_of);
+  copy(s_row_runs, runs.s.row_runs);
+  copy(s_run_col, runs.s.run_col);
+  copy(s_run_off, runs.s.run_off);
+  copy(s_values, runs.s.values);
+  copy(st_row_runs, runs.st.row_runs);
+  copy(st_run_col, runs.st.run_col);
+  copy(st_run_off, runs.st.run_off);
+  copy(st_values, runs.st.values);
   return PD_OK;
 }
 

@@ -10,8 +10,11 @@ the C ABI (``include/pd_b200.h``); this module validates inputs with NumPy
 exactly like the reference, computes the rest-shape data, and hands device
 pointers to the library. There is no CPU fallback.
 
-Added keywords: ``precision`` (``"fp64"`` as the reference, or
-``"fp32+refine"``), ``adjoint`` (``"reference"``: the reference's mean-weight
+Added keywords: ``precision`` (``"fp64"`` as the reference; ``"fp32+refine"``:
+float32 factor products corrected by a float64 residual every iteration, so
+the converged positions are the float64 solver's; ``"fp32"``: float32 local
+projections as well, whose fixed point moves by about cond(A) times the
+float32 rounding), ``adjoint`` (``"reference"``: the reference's mean-weight
 local Jacobian; ``"exact"``: per-element weights, the derivative of the
 forward map), ``adjoint_solver`` (``"auto"``: the reference's Anderson fixed
 point for ``"reference"``, conjugate gradients preconditioned by the factor for
@@ -39,7 +42,7 @@ from . import _lib
 from .meshes import Mesh
 
 MATERIALS = {"pd": 0, "neo_hookean": 1}
-PRECISIONS = {"fp64": _lib.PRECISION_FP64, "fp32+refine": _lib.PRECISION_FP32_REFINE}
+PRECISIONS = {"fp64": _lib.PRECISION_FP64, "fp32+refine": _lib.PRECISION_FP32_REFINE, "fp32": _lib.PRECISION_FP32}
 ADJOINTS = {"reference": _lib.ADJOINT_REFERENCE, "exact": _lib.ADJOINT_EXACT}
 ADJOINT_SOLVERS = {"auto": 0, "fixed_point": 1, "cg": 2}
 MAX_WINDOW = 8
@@ -225,7 +228,7 @@ class SolverDiffPhD:
         if int(anderson_window) != anderson_window or not 0 <= anderson_window <= MAX_WINDOW:
             raise ValueError(f"anderson_window must be an integer in [0, {MAX_WINDOW}]")
         if precision not in PRECISIONS:
-            raise ValueError("precision must be 'fp64' or 'fp32+refine'")
+            raise ValueError("precision must be 'fp64', 'fp32+refine' or 'fp32'")
         if adjoint not in ADJOINTS:
             raise ValueError("adjoint must be 'reference' or 'exact'")
         if adjoint_solver not in ADJOINT_SOLVERS:

@@ -64,3 +64,56 @@ def test_isolated_dirichlet_rows_are_identity():
         lo, hi = out["s_offsets"][r], out["s_offsets"][r + 1]
         if out["permutation"][r] >= 3:
             np.testing.assert_array_equal(out["s_values"][lo:hi], [1.0])
+
+
+def _dense_from_runs(row_runs, run_col, run_off, values, n):
+    m = np.zeros((n, n))
+    for r in range(n):
+        for k in range(row_runs[r], row_runs[r + 1]):
+            lo, hi = run_off[k], run_off[k + 1]
+            m[r, run_col[k]:run_col[k] + hi - lo] = values[lo:hi]
+    return m
+
+
+def _hex_cantilever_matrix(nx, ny):
+    from newton_solver_diff_phd_b200 import meshes
+    from oracle import pd_oracle
+
+    vertices, hexes, _ = meshes.hex_grid(nx, ny, ny, 0.01)
+    free = vertices[:, 0] > 1e-9
+    mu, lam = meshes.lame_from_young(np.full(len(hexes), 1e6), 0.4)
+    return pd_oracle.Body.hex(vertices, hexes, free, mu, lam, 1000.0).matrix(0.01)
+
+
+@pytest.mark.parametrize("name", NAMES + ["cantilever"])
+@pytest.mark.parametrize("gap", [0, 2])
+def test_run_format_is_the_same_factor(name, gap):
+    """The postorder run matrices hold exactly the CSR factor: S_run = S[rows, cols] relabelled."""
+    matrix = _hex_cantilever_matrix(8, 2) if name == "cantilever" else golden("sparse_factors.npz")[name + "__matrix"]
+    out = _lib.inverse_factor(_lib.dense_to_csr(matrix), run_gap=gap)
+    runs = out["runs"]
+    n = len(matrix)
+    label = runs["label_of"]
+    assert sorted(label.tolist()) == list(range(n))
+    s = np.zeros((n, n))
+    for r in range(n):
+        lo, hi = out["s_offsets"][r], out["s_offsets"][r + 1]
+        s[r, out["s_columns"][lo:hi]] = out["s_values"][lo:hi]
+    # Row r of S (elimination order) is run-format row label[permutation[r]].
+    particle_of = np.empty(n, np.int64)
+    particle_of[label] = np.arange(n)
+    s_run = _dense_from_runs(runs["s_row_runs"], runs["s_run_col"], runs["s_run_off"], runs["s_values"], n)
+    position = np.empty(n, np.int64)
+    position[out["permutation"]] = np.arange(n)
+    rows = np.array([position[particle_of[u]] for u in range(n)])
+    np.testing.assert_array_equal(s_run, s[rows][:, particle_of])
+    st_run = _dense_from_runs(runs["st_row_runs"], runs["st_run_col"], runs["st_run_off"], runs["st_values"], n)
+    np.testing.assert_array_equal(st_run, s_run.T)
+    # S^T S applied through the run format equals the inverse.
+    rhs = np.random.default_rng(0).standard_normal((n, 3))
+    x = np.empty_like(rhs)
+    x[particle_of] = st_run @ (s_run @ rhs[particle_of])
+    np.testing.assert_allclose(matrix @ x, rhs, atol=1e-9 * np.abs(rhs).max())
+    if gap >= 2 and name == "cantilever":
+        # Postorder labels make every row of S a single contiguous run.
+        assert np.all(np.diff(runs["s_row_runs"]) <= 1)

@@ -1,0 +1,184 @@
+"""Batched rollouts against the single-instance path, instance by instance."""
+
+import numpy as np
+import pytest
+import torch
+
+from newton_solver_diff_phd_b200 import SolverDiffPhD
+from newton_solver_diff_phd_b200.batch import BatchedSolver
+from newton_solver_diff_phd_b200.scenes import Cantilever, cantilever_model
+from tests.helpers import tet_grid_model
+
+pytestmark = pytest.mark.gpu
+
+DT = 0.01
+STEPS = 4
+
+
+def _specs():
+    rng = np.random.default_rng(5)
+    sizes = [(4, 2), (7, 2), (12, 3), (9, 2), (5, 2)]
+    youngs = [3e5, 2e6, 1e6, 5e6, 1e5]
+    poissons = [0.35, 0.4, 0.45, 0.3, 0.42]
+    return [Cantilever(nx, ny, ny, e, nu, rng.uniform(0.0, 5.0, (ny + 1) ** 2))
+            for (nx, ny), e, nu in zip(sizes, youngs, poissons)]
+
+
+def _instances(precision, window=5, with_tet=False):
+    out = []
+    for spec in _specs():
+        model, mesh, materials, forces = cantilever_model(spec)
+        solver = SolverDiffPhD(model, density=1000.0, hex_mesh=mesh, hex_materials=materials, precision=precision,
+                               anderson_window=window, rel_tol=1e-6, abs_tol=1e-9, max_iterations=3000)
+        out.append((model, solver, torch.as_tensor(forces, device="cuda")))
+    if with_tet:
+        model = tet_grid_model(gravity=0.0)
+        solver = SolverDiffPhD(model, density=1000.0, precision=precision, anderson_window=window, rel_tol=1e-6,
+                               abs_tol=1e-9, max_iterations=3000)
+        forces = torch.zeros_like(model.particle_q)
+        forces[:, 2] = 0.5
+        out.append((model, solver, forces))
+    return out
+
+
+def _plain(model, solver, forces):
+    state, out = model.state(), model.state()
+    trajectory, iterations = [], []
+    for _ in range(STEPS):
+        state.particle_f.copy_(forces)
+        solver.step(state, out, None, None, DT)
+        trajectory.append(out.particle_q.clone())
+        iterations.append(int(solver.iterations[0]))
+        state, out = out, state
+    solver.check_status()
+    return torch.stack(trajectory), iterations
+
+
+def _batched(instances, **options):
+    batch = BatchedSolver([s for _, s, _ in instances], DT, **options)
+    q0 = batch.concat([m.particle_q for m, _, _ in instances])
+    qd0 = torch.zeros_like(q0)
+    forces = batch.concat([f for _, _, f in instances])
+    q, qd, x = batch.rollout(q0, qd0, forces, STEPS)
+    status, iterations = batch.read()
+    return batch, q, qd, x, status, iterations
+
+
+def test_batched_fp64_matches_single_instance_steps():
+    plain = [_plain(*inst) for inst in _instances("fp64", with_tet=True)]
+    instances = _instances("fp64", with_tet=True)
+    batch, q, qd, x, status, iterations = _batched(instances)
+    assert np.all(status == 0), status
+    for i, (trajectory, its) in enumerate(plain):
+        got = batch.split(q)[i]
+        scale = float(trajectory.abs().max())
+        err = float((got - trajectory).abs().max())
+        # Same algorithm, different reduction order: equal to rounding when the
+        # iteration counts agree, within the convergence tolerance otherwise.
+        assert np.all(np.abs(iterations[:, i] - np.asarray(its)) <= 1), (i, iterations[:, i], its)
+        assert err <= 1e-6 * scale, (i, err, scale)
+        np.testing.assert_allclose(batch.split(x)[i][-1].float().cpu(), got[-1].cpu(), rtol=0, atol=1e-6 * scale)
+
+
+def _instances64(precision, rel_tol, max_iterations, abs_tol=1e-12):
+    """The cantilevers with float64 states (no state rounding between steps)."""
+    out = []
+    for spec in _specs():
+        model, mesh, materials, forces = cantilever_model(spec)
+        solver = SolverDiffPhD(model, density=1000.0, hex_mesh=mesh, hex_materials=materials, precision=precision,
+                               anderson_window=5, rel_tol=rel_tol, abs_tol=abs_tol, max_iterations=max_iterations,
+                               state_dtype=torch.float64)
+        out.append((model, solver, torch.as_tensor(forces, device="cuda", dtype=torch.float64)))
+    return out
+
+
+def _plain64(model, solver, forces):
+    state, out = model.state(), model.state()
+    for s in (state, out):
+        s.particle_q, s.particle_qd, s.particle_f = s.particle_q.double(), s.particle_qd.double(), s.particle_f.double()
+    trajectory = []
+    for _ in range(STEPS):
+        state.particle_f.copy_(forces)
+        solver.step(state, out, None, None, DT)
+        trajectory.append(solver._x.clone())
+        state, out = out, state
+    return torch.stack(trajectory)
+
+
+def _relative(a, b):
+    return float((a - b).abs().max()) / float(b.abs().max())
+
+
+def test_batched_fp32_refine_arithmetic_error_below_1e6():
+    """Same iterations (no convergence stop): float32 factor products with
+    float64 residual refinement stay within 1e-6 of the float64 iterates."""
+    plain = [_plain64(*inst) for inst in _instances64("fp64", 0.0, 40, abs_tol=0.0)]
+    batch, q, qd, x, status, iterations = _batched(_instances64("fp32+refine", 0.0, 40, abs_tol=0.0))
+    assert np.all(iterations == 40), iterations
+    for i, reference in enumerate(plain):
+        assert _relative(batch.split(x)[i], reference) <= 1e-6, i
+
+
+def test_batched_fp32_refine_fixed_point_is_the_fp64_solution():
+    """Converged tightly, float32 factor products reach the float64 solution
+    (within 1e-6); at the working tolerance they land as close to it as the
+    float64 solver itself. Float32 local projections move the fixed point by
+    about cond(A) * 6e-8, bounded here at 1e-4."""
+    truth = [_plain64(*inst) for inst in _instances64("fp64", 1e-12, 50000, abs_tol=0.0)]
+    fp64 = [_plain64(*inst) for inst in _instances64("fp64", 1e-6, 20000)]
+    tight = _batched(_instances64("fp32+refine", 1e-10, 50000, abs_tol=0.0))
+    loose = _batched(_instances64("fp32+refine", 1e-6, 20000))
+    fast = _batched(_instances64("fp32", 1e-8, 20000, abs_tol=0.0))
+    assert np.all(tight[4] == 0) and np.all(loose[4] == 0) and np.all(fast[4] == 0)
+    for i, (t, r) in enumerate(zip(truth, fp64)):
+        assert _relative(tight[0].split(tight[3])[i], t) <= 1e-6, i
+        e32 = _relative(loose[0].split(loose[3])[i], t)
+        e64 = _relative(r, t)
+        assert e32 <= 2.0 * e64 + 1e-6, (i, e32, e64)
+        assert _relative(fast[0].split(fast[3])[i], t) <= 1e-4, i
+
+
+def test_batched_rollout_is_bitwise_deterministic_and_graph_is_reused():
+    instances = _instances("fp32+refine", window=3)
+    batch = BatchedSolver([s for _, s, _ in instances], DT)
+    q0 = batch.concat([m.particle_q for m, _, _ in instances])
+    qd0 = torch.zeros_like(q0)
+    forces = batch.concat([f for _, _, f in instances])
+    first = batch.rollout(q0, qd0, forces, STEPS)
+    snapshot = [t.clone() for t in first]
+    second = batch.rollout(q0, qd0, forces, STEPS, out=first)
+    for a, b in zip(snapshot, second):
+        assert torch.equal(a, b)
+
+
+def test_batched_per_step_forces_and_cold_svd():
+    instances = _instances("fp64", window=0)
+    batch = BatchedSolver([s for _, s, _ in instances], DT, svd_warm_start=False, task_nnz=512)
+    q0 = batch.concat([m.particle_q for m, _, _ in instances])
+    qd0 = torch.zeros_like(q0)
+    forces = batch.concat([f for _, _, f in instances])
+    per_step = torch.stack([forces * (t + 1) / STEPS for t in range(STEPS)]).contiguous()
+    q, _, _ = batch.rollout(q0, qd0, per_step, STEPS)
+    for i, (model, solver, f) in enumerate(instances):
+        state, out = model.state(), model.state()
+        for t in range(STEPS):
+            state.particle_f.copy_(f * (t + 1) / STEPS)
+            solver.step(state, out, None, None, DT)
+            state, out = out, state
+        expected = state.particle_q
+        scale = float(expected.abs().max())
+        assert float((batch.split(q)[i][-1] - expected).abs().max()) <= 1e-6 * scale
+
+
+def test_stepwise_launches_equal_the_graph():
+    instances = _instances("fp32+refine")
+    batch = BatchedSolver([s for _, s, _ in instances], DT)
+    q0 = batch.concat([m.particle_q for m, _, _ in instances])
+    qd0 = torch.zeros_like(q0)
+    forces = batch.concat([f for _, _, f in instances])
+    graph = [t.clone() for t in batch.rollout(q0, qd0, forces, STEPS)]
+    graph_iterations = batch.read()[1]
+    stepwise = batch.rollout(q0, qd0, forces, STEPS, stepwise=True)
+    assert np.array_equal(batch.read()[1], graph_iterations)
+    for a, b in zip(graph, stepwise):
+        assert torch.equal(a, b)
