@@ -211,11 +211,23 @@ int pd_apply_inverse_static(PdSolver* solver, const double* rhs, double* out, vo
    activations. The solvers must outlive the batch and must not step on
    their own while a batched rollout runs (the batch uses their buffers). */
 typedef struct PdBatch PdBatch;
+/* Schedules of a batch.
+   TEAMS: one persistent cooperative launch per rollout; every instance runs
+   all its steps on a team of blocks sized to its factor and element count,
+   with the single-instance step body (and adjoint body) and its own team
+   barriers; teams form from a queue as blocks finish earlier instances.
+   PHASES: per-phase kernels over all instances inside a graph WHILE loop,
+   the factor in postorder run format (forward only). */
+#define PD_BATCH_TEAMS 0
+#define PD_BATCH_PHASES 1
 typedef struct PdBatchOptions {
-  int32_t svd_warm_start; /* 1: warm-started SVD of every element sample after the first iteration */
-  int32_t task_nnz;       /* factor entries per product task (>= 256; default 32768) */
-  int32_t run_gap;        /* omitted zeros bridged inside a run (default 2) */
-  int32_t local_cells;    /* Hex8 cells per local-step task (>= 4; default 64) */
+  int32_t svd_warm_start; /* phases: 1 = warm-started SVD after the first iteration */
+  int32_t task_nnz;       /* phases: factor entries per product task (>= 256; default 32768) */
+  int32_t run_gap;        /* phases: omitted zeros bridged inside a run (default 2) */
+  int32_t local_cells;    /* phases: Hex8 cells per local-step task (>= 4; default 64) */
+  int32_t schedule;       /* PD_BATCH_TEAMS (default) or PD_BATCH_PHASES */
+  int32_t team_nnz;       /* teams: factor entries of S per block of a team (default 65536) */
+  int32_t team_samples;   /* teams: element samples per block of a team (default 512) */
 } PdBatchOptions;
 /* options may be NULL (defaults). */
 int pd_batch_create(PdSolver* const* solvers, int32_t count, const PdBatchOptions* options, PdBatch** out);
@@ -234,9 +246,28 @@ int pd_batch_factor_stats(const PdBatch* batch, int64_t* values, int64_t* runs, 
 int pd_batch_forward(PdBatch* batch, int32_t steps, double dt, const double gravity[3], const void* q0,
                      const void* qd0, const void* forces, int64_t force_step_stride, void* q_traj, void* qd_traj,
                      double* x_record, void* stream);
+/* Adjoint of the last rollout (teams schedule), last step first (the
+   reference's tape replay, adjoint.py:1088-1259, per step): x_record the
+   forward's float64 [steps][P][3] record; grad_q_final / grad_qd_final the
+   loss gradient w.r.t. the final state [P][3]; grad_q / grad_qd scratch of
+   [2][P][3] each, where dL/dq0 and dL/dqd0 end in slot (steps - 1) & 1;
+   grad_forces [steps][P][3] receives dL/df of every step; grad_materials
+   float64 [E][2] (or NULL) receives dL/d(mu, lambda) per element. State
+   arrays use the state precision. iterations (host [steps][count], or NULL)
+   receives every adjoint step's solver iterations and synchronises. */
+int pd_batch_backward(PdBatch* batch, int32_t steps, double dt, const double* x_record, const void* grad_q_final,
+                      const void* grad_qd_final, void* grad_q, void* grad_qd, void* grad_forces,
+                      double* grad_materials, int32_t* iterations, void* stream);
+/* Global-timer nanoseconds [count][2] at which each instance's last forward
+   and adjoint rollout started and ended on its lane (teams schedule). Either
+   pointer may be NULL. Synchronises. */
+int pd_batch_timeline(PdBatch* batch, uint64_t* forward, uint64_t* adjoint, void* stream);
+/* Team size of every instance (0 under the phases schedule) and the grid of the team launch. */
+int pd_batch_team_sizes(const PdBatch* batch, int32_t* sizes, int32_t* grid);
 /* The same rollout without a graph: every kernel launched on its own, the
    loop decided on the host every 16 passes (synchronises). For profilers
-   that follow plain launches; results equal pd_batch_forward's. */
+   that follow plain launches; results equal pd_batch_forward's. Phases
+   schedule only. */
 int pd_batch_forward_stepwise(PdBatch* batch, int32_t steps, double dt, const double gravity[3], const void* q0,
                               const void* qd0, const void* forces, int64_t force_step_stride, void* q_traj,
                               void* qd_traj, double* x_record, void* stream);

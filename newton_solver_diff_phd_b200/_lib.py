@@ -32,6 +32,8 @@ STATUS_BARRIER_TIMEOUT = 1024
 PRECISION_FP64 = 0
 PRECISION_FP32_REFINE = 1
 PRECISION_FP32 = 2
+BATCH_TEAMS = 0
+BATCH_PHASES = 1
 ADJOINT_REFERENCE = 0
 ADJOINT_EXACT = 1
 
@@ -77,6 +79,9 @@ class PdBatchOptions(ctypes.Structure):
         ("task_nnz", ctypes.c_int32),
         ("run_gap", ctypes.c_int32),
         ("local_cells", ctypes.c_int32),
+        ("schedule", ctypes.c_int32),
+        ("team_nnz", ctypes.c_int32),
+        ("team_samples", ctypes.c_int32),
     ]
 
 
@@ -113,6 +118,9 @@ SIGNATURES = {
     "pd_batch_forward": ([_P, _I32, _D, _P, _P, _P, _P, _I64, _P, _P, _P, _P], ctypes.c_int),
     "pd_batch_forward_stepwise": ([_P, _I32, _D, _P, _P, _P, _P, _I64, _P, _P, _P, _P], ctypes.c_int),
     "pd_batch_read": ([_P, _P, _P, _P], ctypes.c_int),
+    "pd_batch_backward": ([_P, _I32, _D, _P, _P, _P, _P, _P, _P, _P, _P, _P], ctypes.c_int),
+    "pd_batch_team_sizes": ([_P, _P, _P], ctypes.c_int),
+    "pd_batch_timeline": ([_P, _P, _P, _P], ctypes.c_int),
     "pd_inverse_build": ([_I32, _P, _P, _P, ctypes.POINTER(_P)], ctypes.c_int),
     "pd_inverse_sizes": ([_P, ctypes.POINTER(_I32), ctypes.POINTER(_I64), ctypes.POINTER(_I64)], ctypes.c_int),
     "pd_inverse_export": ([_P, _P, _P, _P, _P, _P, _P, _P], ctypes.c_int),

@@ -26,6 +26,9 @@ from . import _lib
 from .solver import SolverDiffPhD, _stream
 
 
+SCHEDULES = {"teams": _lib.BATCH_TEAMS, "phases": _lib.BATCH_PHASES}
+
+
 class BatchedSolver:
     """A fixed set of solvers stepped together (``pd_batch_*`` in ``include/pd_b200.h``).
 
@@ -33,14 +36,23 @@ class BatchedSolver:
     solvers must share device, precision and state dtype, must outlive the
     batch, and must not be stepped on their own while a batched rollout runs.
     Dirichlet targets and Tet4 muscle activations are not supported.
+
+    ``schedule="teams"`` (default) runs each instance's whole rollout on a
+    team of blocks of one persistent launch, with the single-instance step
+    and adjoint bodies; ``"phases"`` runs per-phase kernels over all
+    instances in a graph loop (forward only).
     """
 
-    def __init__(self, solvers: list[SolverDiffPhD], dt: float, *, svd_warm_start: bool = True,
+    def __init__(self, solvers: list[SolverDiffPhD], dt: float, *, schedule: str = "teams",
+                 team_nnz: int = 65536, team_samples: int = 512, svd_warm_start: bool = True,
                  task_nnz: int = 32768, run_gap: int = 2, local_cells: int = 64):
         if not solvers:
             raise ValueError("BatchedSolver needs at least one solver")
         if not np.isfinite(dt) or dt <= 0:
             raise ValueError("dt must be finite and positive")
+        if schedule not in SCHEDULES:
+            raise ValueError("schedule must be 'teams' or 'phases'")
+        self.schedule = schedule
         first = solvers[0]
         for solver in solvers:
             if not isinstance(solver, SolverDiffPhD):
@@ -61,7 +73,8 @@ class BatchedSolver:
         self.solvers = list(solvers)
         self._lib = _lib.library()
         handles = (ctypes.c_void_p * len(solvers))(*[ctypes.cast(s._handle, ctypes.c_void_p).value for s in solvers])
-        options = _lib.PdBatchOptions(int(svd_warm_start), int(task_nnz), int(run_gap), int(local_cells))
+        options = _lib.PdBatchOptions(int(svd_warm_start), int(task_nnz), int(run_gap), int(local_cells),
+                                      SCHEDULES[schedule], int(team_nnz), int(team_samples))
         handle = ctypes.c_void_p()
         _lib.check(self._lib.pd_batch_create(ctypes.cast(handles, ctypes.c_void_p), len(solvers), ctypes.byref(options), ctypes.byref(handle)))
         self._handle = handle
@@ -84,6 +97,63 @@ class BatchedSolver:
                                                    _lib.ptr(tasks)))
         return {"values": values.value, "runs": runs.value, "tasks": dict(zip(("local", "gather", "s", "st"),
                                                                                 tasks.tolist()))}
+
+    def team_sizes(self):
+        """``(blocks per instance, blocks of the team launch)`` (teams schedule)."""
+        sizes = np.zeros(self.count, np.int32)
+        grid = ctypes.c_int32()
+        _lib.check(self._lib.pd_batch_team_sizes(self._handle, _lib.ptr(sizes), ctypes.byref(grid)))
+        return sizes, grid.value
+
+    def backward(self, x_record: torch.Tensor, grad_q: torch.Tensor, grad_qd: torch.Tensor | None = None, *,
+                 materials: bool = True):
+        """Adjoint of the last rollout (teams schedule).
+
+        ``x_record``: the rollout's float64 ``(steps, P, 3)`` record;
+        ``grad_q``/``grad_qd``: loss gradients w.r.t. the final ``(P, 3)`` state.
+        Returns ``(dL/dq0, dL/dqd0, dL/dforces (steps, P, 3), dL/d(mu, lambda)
+        (E, 2) float64 or None, adjoint iterations (steps, count))``.
+        """
+        steps = int(x_record.shape[0])
+        shape = (self.particle_count, 3)
+        if x_record.dtype != torch.float64 or tuple(x_record.shape) != (steps,) + shape or not x_record.is_contiguous():
+            raise ValueError("x_record must be the rollout's contiguous float64 (steps, P, 3) record")
+        grad_q = grad_q.detach().to(self.device, self.state_dtype).contiguous()
+        grad_qd = (torch.zeros_like(grad_q) if grad_qd is None
+                   else grad_qd.detach().to(self.device, self.state_dtype).contiguous())
+        if tuple(grad_q.shape) != shape or tuple(grad_qd.shape) != shape:
+            raise ValueError("final-state gradients must have shape (P, 3)")
+        key = (steps, materials)
+        if getattr(self, "_adjoint_key", None) != key:
+            self._adjoint_buffers = (
+                torch.empty((2,) + shape, dtype=self.state_dtype, device=self.device),
+                torch.empty((2,) + shape, dtype=self.state_dtype, device=self.device),
+                torch.empty((steps,) + shape, dtype=self.state_dtype, device=self.device),
+                torch.empty((int(self.element_offsets[-1]), 2), dtype=torch.float64, device=self.device)
+                if materials else None,
+                torch.empty((2,) + shape, dtype=self.state_dtype, device=self.device),
+            )
+            self._adjoint_key = key
+        gq, gqd, gf, gm, final = self._adjoint_buffers
+        final[0].copy_(grad_q)
+        final[1].copy_(grad_qd)
+        iterations = np.zeros((steps, self.count), np.int32)
+        _lib.check(
+            self._lib.pd_batch_backward(
+                self._handle, steps, self.dt, _lib.ptr(x_record), _lib.ptr(final[0]), _lib.ptr(final[1]),
+                _lib.ptr(gq), _lib.ptr(gqd), _lib.ptr(gf), _lib.ptr(gm), _lib.ptr(iterations), _stream(),
+            )
+        )
+        slot = (steps - 1) & 1
+        return gq[slot], gqd[slot], gf, gm, iterations
+
+    def timeline(self):
+        """Start and end (global-timer ns) of each instance's last forward and
+        adjoint rollout on its lane: two ``(count, 2)`` uint64 arrays."""
+        forward = np.zeros((self.count, 2), np.uint64)
+        adjoint = np.zeros((self.count, 2), np.uint64)
+        _lib.check(self._lib.pd_batch_timeline(self._handle, _lib.ptr(forward), _lib.ptr(adjoint), _stream()))
+        return forward, adjoint
 
     def concat(self, tensors) -> torch.Tensor:
         """Concatenate per-instance ``(n_i, 3)`` tensors into one ``(P, 3)`` state array."""

@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include "pd_forward.cuh"
+#include "pd_team.cuh"
 #include "pd_kernels.h"
 
 namespace pdb200 {
@@ -943,6 +944,100 @@ template <typename TL, typename TV>
 __global__ void __launch_bounds__(kBlock) adjoint_step_kernel(const AdjointArgs b) {
   extern __shared__ __align__(16) char dyn_smem[];
   adjoint_step_body<TL, TV>(b, Team{static_cast<int>(blockIdx.x), static_cast<int>(gridDim.x)}, dyn_smem);
+}
+
+// Whole adjoint rollouts (last step first) of many instances, each by a team
+// of blocks: the single-instance adjoint body per step. dL/dq and dL/dqd of
+// consecutive steps alternate between two buffers; a team clears its slice
+// of the buffer a step accumulates into before the step.
+template <typename TL, typename TV>
+__global__ void __launch_bounds__(kBlock) team_adjoint_kernel(const TeamLaunch launch) {
+  extern __shared__ __align__(16) char dyn_smem[];
+  __shared__ AdjointArgs s_args;
+  Team team;
+  const int lane = lane_of_block(launch, team);
+  GridBarrier* barrier = &launch.lane_barrier[lane];
+  const int f64 = launch.state_f64;
+  const long long step_elements = 3 * launch.particles;
+  for (;;) {
+    const int instance = next_instance(launch, lane, team, launch.status);
+    if (instance < 0) return;
+    copy_arguments(launch.adjoint + instance, &s_args);
+    if (launch.timeline != nullptr && team.rank == 0 && threadIdx.x == 0) {
+      unsigned long long now;
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+      launch.timeline[2 * instance] = now;
+    }
+    const long long offset = 3 * launch.particle_offset[instance];
+    const int n3 = 3 * launch.adjoint[instance].n;
+    __syncthreads();
+    for (int t = launch.steps - 1; t >= 0; --t) {
+      const int write = (launch.steps - 1 - t) & 1;
+      void* gq = state_offset(launch.grad_q, f64, write * step_elements + offset);
+      void* gqd = state_offset(launch.grad_qd, f64, write * step_elements + offset);
+      for (int k = team.rank * blockDim.x + threadIdx.x; k < n3; k += team.size * blockDim.x) {
+        state_store(gq, f64, k, 0.0);
+        state_store(gqd, f64, k, 0.0);
+      }
+      if (threadIdx.x == 0) {
+        const bool last = t == launch.steps - 1;
+        s_args.barrier = barrier;
+        s_args.x = launch.x_record + t * step_elements + offset;
+        s_args.gq_out = last ? state_offset(launch.grad_q_final, f64, offset)
+                             : state_offset(static_cast<const void*>(launch.grad_q), f64, (1 - write) * step_elements + offset);
+        s_args.gqd_out = last ? state_offset(launch.grad_qd_final, f64, offset)
+                              : state_offset(static_cast<const void*>(launch.grad_qd), f64, (1 - write) * step_elements + offset);
+        s_args.gq = gq;
+        s_args.gqd = gqd;
+        s_args.gf = state_offset(launch.grad_forces, f64, t * step_elements + offset);
+        s_args.gdirichlet = nullptr;
+        s_args.gmaterials = launch.grad_materials != nullptr ? launch.grad_materials + 2 * launch.element_offset[instance]
+                                                             : nullptr;
+        s_args.gactivations = nullptr;
+        s_args.activations = nullptr;
+        s_args.dt = launch.dt;
+      }
+      __syncthreads();
+      // The cleared accumulators are complete before any rank adds into them.
+      if (!grid_sync(barrier, s_args.status, team.size, team.rank)) return;
+      if (!adjoint_step_body<TL, TV>(s_args, team, dyn_smem)) return;
+      if (team.rank == 0 && threadIdx.x == 0 && launch.iteration_log != nullptr)
+        launch.iteration_log[t * launch.count + instance] = *s_args.iteration;
+      if (!grid_sync(barrier, s_args.status, team.size, team.rank)) return;
+    }
+    if (launch.timeline != nullptr && team.rank == 0 && threadIdx.x == 0) {
+      unsigned long long now;
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+      launch.timeline[2 * instance + 1] = now;
+    }
+  }
+}
+
+static const void* team_adjoint(int precision) {
+  if (precision == 0) return reinterpret_cast<const void*>(&team_adjoint_kernel<double, double>);
+  if (precision == 1) return reinterpret_cast<const void*>(&team_adjoint_kernel<double, float>);
+  return reinterpret_cast<const void*>(&team_adjoint_kernel<float, float>);
+}
+
+cudaError_t launch_team_adjoint(const TeamLaunch& launch, int blocks, int precision, size_t smem, cudaStream_t stream) {
+  void* params[] = {const_cast<TeamLaunch*>(&launch)};
+  return cudaLaunchCooperativeKernel(team_adjoint(precision), dim3(blocks), dim3(kBlock), params, smem, stream);
+}
+
+cudaError_t team_adjoint_max_blocks(int precision, size_t smem, int* blocks_per_sm) {
+  const void* kernel = team_adjoint(precision);
+  int device = 0, optin = 0;
+  cudaError_t status = cudaGetDevice(&device);
+  if (status != cudaSuccess) return status;
+  status = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+  if (status != cudaSuccess) return status;
+  cudaFuncAttributes attributes{};
+  status = cudaFuncGetAttributes(&attributes, kernel);
+  if (status != cudaSuccess) return status;
+  status = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                optin - static_cast<int>(attributes.sharedSizeBytes));
+  if (status != cudaSuccess) return status;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kernel, kBlock, smem);
 }
 
 // precision 0: FP64; 1: FP64 Jacobians, FP32 factor products; 2: FP32 Jacobians and factor.

@@ -24,6 +24,7 @@
 
 #include "pd_batch.cuh"
 #include "pd_forward.cuh"
+#include "pd_kernels.h"
 #include "runs.h"
 #include "solver_state.h"
 
@@ -658,6 +659,7 @@ struct GraphKey {
 }  // namespace
 
 struct PdBatch {
+  int schedule = PD_BATCH_TEAMS;
   int device = 0;
   int count = 0;
   int precision = 0;
@@ -676,9 +678,21 @@ struct PdBatch {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   GraphKey key;
+  // Teams schedule: per-instance team sizes and argument blocks, the queue.
+  std::vector<int> team_size;
+  DeviceBuffer d_forward_args, d_adjoint_args, d_lane_start, d_lane_class, d_class_begin, d_class_order,
+      d_particle_offset, d_element_offset, d_class_head, d_lane_slot, d_barriers, d_team_status, d_adjoint_log,
+      d_timeline;
+  int team_blocks = 0, lanes = 0, classes = 0;
+  size_t team_smem = 0;
+  cudaStream_t capture = nullptr;  // private stream the rollout graphs are captured on
+  cudaGraphExec_t adjoint_exec = nullptr;
+  GraphKey adjoint_key;
   ~PdBatch() {
     if (exec != nullptr) cudaGraphExecDestroy(exec);
     if (graph != nullptr) cudaGraphDestroy(graph);
+    if (adjoint_exec != nullptr) cudaGraphExecDestroy(adjoint_exec);
+    if (capture != nullptr) cudaStreamDestroy(capture);
   }
 };
 
@@ -768,35 +782,10 @@ cudaError_t add_kernel(cudaGraphNode_t* node, cudaGraph_t graph, const cudaGraph
 
 }  // namespace
 
-extern "C" int pd_batch_create(PdSolver* const* solvers, int32_t count, const PdBatchOptions* options,
-                               PdBatch** out) {
-  if (solvers == nullptr || out == nullptr || count < 1) return pd_set_error(PD_ERR_INVALID, "batch needs solvers");
-  *out = nullptr;
-  PdBatchOptions opts{};
-  opts.svd_warm_start = 1;
-  opts.task_nnz = 32768;
-  opts.run_gap = 2;
-  opts.local_cells = 64;
-  if (options != nullptr) opts = *options;
-  if (opts.task_nnz < 256 || opts.run_gap < 0 || opts.local_cells < 4)
-    return pd_set_error(PD_ERR_INVALID, "batch options out of range");
-  auto batch = std::make_unique<PdBatch>();
-  batch->count = count;
-  batch->solvers.assign(solvers, solvers + count);
-  for (int i = 0; i < count; ++i) {
-    const PdSolver* s = solvers[i];
-    if (s == nullptr) return pd_set_error(PD_ERR_INVALID, "null solver in batch");
-    if (!s->built || s->stale) return pd_set_error(PD_ERR_STATE, "every batched solver must be built (pd_build)");
-    if (s->device != solvers[0]->device || s->options.precision != solvers[0]->options.precision ||
-        s->options.state_precision != solvers[0]->options.state_precision || s->built_dt != solvers[0]->built_dt)
-      return pd_set_error(PD_ERR_INVALID, "batched solvers must share device, precision, state precision and dt");
-    if (s->activations != nullptr && !s->hex)
-      return pd_set_error(PD_ERR_UNSUPPORTED, "muscle activations are not supported by the batched path");
-  }
-  batch->device = solvers[0]->device;
-  batch->precision = solvers[0]->options.precision;
-  batch->state_f64 = solvers[0]->options.state_precision;
-  PD_CUDA(cudaSetDevice(batch->device));
+// The phases schedule: run-format factors, work-list tasks and the
+// instance table of the per-phase kernels.
+int create_phases(PdBatch* batch, const PdBatchOptions& opts) {
+  const int count = batch->count;
   const bool fp64 = batch->precision == PD_PRECISION_FP64;
   const size_t tv = fp64 ? sizeof(double) : sizeof(float);
   const size_t tl = batch->precision == PD_PRECISION_FP32 ? sizeof(float) : sizeof(double);
@@ -811,9 +800,7 @@ extern "C" int pd_batch_create(PdSolver* const* solvers, int32_t count, const Pd
   int64_t particles = 0, elements = 0;
   int max_iterations = 0;
   for (int i = 0; i < count; ++i) {
-    PdSolver* s = solvers[i];
-    batch->particle_offsets.push_back(particles);
-    batch->element_offsets.push_back(elements);
+    PdSolver* s = batch->solvers[i];
     auto buffers = std::make_unique<InstanceBuffers>();
     const pdb200::RunFactor runs = pdb200::build_run_factor(s->factor, opts.run_gap);
     PD_CUDA(buffers->s_row_runs.upload(runs.s.row_runs));
@@ -921,8 +908,6 @@ extern "C" int pd_batch_create(PdSolver* const* solvers, int32_t count, const Pd
     elements += s->ne;
     batch->buffers.push_back(std::move(buffers));
   }
-  batch->particle_offsets.push_back(particles);
-  batch->element_offsets.push_back(elements);
   PD_CUDA(batch->d_instances.upload(instances));
   PD_CUDA(batch->d_local_tasks.upload(local_tasks));
   PD_CUDA(batch->d_gather_tasks.upload(gather_tasks));
@@ -966,6 +951,205 @@ extern "C" int pd_batch_create(PdSolver* const* solvers, int32_t count, const Pd
       batch->grid[k] = std::max(1, std::min(tasks[k], std::max(1, per_sm) * sms));
     }
   }
+  return PD_OK;
+}
+
+// The teams schedule. Each instance wants a team of about
+// max(nnz(S) / team_nnz, samples / team_samples) blocks, rounded to a power of
+// two: its size class. The grid is cut into lanes of each class's size, with
+// a share of blocks per class proportional to the class's work (factor
+// entries plus element samples); every solver is planned for its class's
+// team size, and the queues list each class's instances by decreasing work.
+int create_teams(PdBatch* batch, const PdBatchOptions& opts) {
+  const int count = batch->count;
+  int sms = 0, optin = 0;
+  PD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, batch->device));
+  PD_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, batch->device));
+  int per_sm_forward = 0, per_sm_adjoint = 0;
+  PD_CUDA(pdb200::team_forward_max_blocks(batch->precision, 0, &per_sm_forward));
+  PD_CUDA(pdb200::team_adjoint_max_blocks(batch->precision, 0, &per_sm_adjoint));
+  const int grid_cap = std::max(1, std::min(per_sm_forward, per_sm_adjoint)) * sms;
+  // Largest class: a power of two that leaves room for one lane of every smaller class.
+  int largest = 1;
+  while (largest * 4 <= grid_cap && largest < 64) largest *= 2;
+  const int budget = optin - 10 * 1024;  // static shared memory of the team kernels
+  std::vector<double> cost(count);
+  std::vector<int> cls_of(count);
+  batch->team_size.assign(count, 1);
+  for (int i = 0; i < count; ++i) {
+    const PdSolver* s = batch->solvers[i];
+    const double nnz = static_cast<double>(s->factor.s.columns.size());
+    const double samples = static_cast<double>(s->ne) * (s->hex ? 8 : 1);
+    const double want = std::max(1.0, std::max(nnz / opts.team_nnz, samples / opts.team_samples));
+    int size = 1;
+    while (size < largest && size * 1.5 < want) size *= 2;
+    batch->team_size[i] = size;
+    cost[i] = nnz + 64.0 * samples;
+  }
+  // Classes present, ascending size. A class whose share of the grid (by
+  // work) is smaller than one of its teams moves down to half the size, so
+  // that no class with much work is left with a single serial lane.
+  std::vector<int> sizes;
+  std::vector<double> work;
+  std::vector<int> members;
+  int classes = 0;
+  for (;;) {
+    sizes.clear();
+    for (int i = 0; i < count; ++i) sizes.push_back(batch->team_size[i]);
+    std::sort(sizes.begin(), sizes.end());
+    sizes.erase(std::unique(sizes.begin(), sizes.end()), sizes.end());
+    classes = static_cast<int>(sizes.size());
+    work.assign(classes, 0.0);
+    members.assign(classes, 0);
+    double total = 0.0;
+    for (int i = 0; i < count; ++i) {
+      cls_of[i] = static_cast<int>(std::lower_bound(sizes.begin(), sizes.end(), batch->team_size[i]) - sizes.begin());
+      work[cls_of[i]] += cost[i];
+      members[cls_of[i]] += 1;
+      total += cost[i];
+    }
+    int shrink = -1;
+    for (int c = classes - 1; c >= 0; --c) {
+      const double share = grid_cap * work[c] / total;
+      if (sizes[c] > 1 && share < 2.0 * sizes[c] && members[c] > 1) {
+        shrink = sizes[c];
+        break;
+      }
+    }
+    if (shrink < 0) break;
+    for (int i = 0; i < count; ++i)
+      if (batch->team_size[i] == shrink) batch->team_size[i] = shrink / 2;
+  }
+  double total_work = 0.0;
+  for (double w : work) total_work += w;
+  std::vector<int> teams(classes, 1);
+  auto used = [&]() {
+    int blocks = 0;
+    for (int c = 0; c < classes; ++c) blocks += teams[c] * sizes[c];
+    return blocks;
+  };
+  if (used() > grid_cap) return pd_set_error(PD_ERR_UNSUPPORTED, "the team classes do not fit the co-resident grid");
+  // Add lanes where a class's share of the grid is furthest below its share of the work.
+  for (;;) {
+    int best = -1;
+    double best_gap = 0.0;
+    for (int c = 0; c < classes; ++c) {
+      if (teams[c] >= members[c] || used() + sizes[c] > grid_cap) continue;
+      const double gap = work[c] / total_work - static_cast<double>(teams[c] * sizes[c]) / grid_cap;
+      if (best < 0 || gap > best_gap) {
+        best = c;
+        best_gap = gap;
+      }
+    }
+    if (best < 0) break;
+    teams[best] += 1;
+  }
+  // Plans, argument blocks and queues.
+  size_t smem = 0;
+  for (int i = 0; i < count; ++i) {
+    PdSolver* s = batch->solvers[i];
+    if (int status = pd_plan_launch(s, batch->team_size[i], budget)) return status;
+    if (int status = pd_ensure_adjoint_buffers(s)) return status;
+    smem = std::max(smem, s->smem);
+  }
+  std::vector<pdb200::StepArgs> forward(count);
+  std::vector<pdb200::AdjointArgs> adjoint(count);
+  for (int i = 0; i < count; ++i) {
+    fill_step_args(batch->solvers[i], &forward[i]);
+    fill_adjoint_args(batch->solvers[i], &adjoint[i]);
+    forward[i].timers = nullptr;
+  }
+  std::vector<int> class_begin(classes + 1, 0), class_order;
+  for (int c = 0; c < classes; ++c) {
+    std::vector<int> list;
+    for (int i = 0; i < count; ++i)
+      if (cls_of[i] == c) list.push_back(i);
+    std::stable_sort(list.begin(), list.end(), [&](int x, int y) { return cost[x] > cost[y]; });
+    class_order.insert(class_order.end(), list.begin(), list.end());
+    class_begin[c + 1] = static_cast<int>(class_order.size());
+  }
+  std::vector<int> lane_start(1, 0), lane_class;
+  for (int c = classes - 1; c >= 0; --c) {
+    for (int t = 0; t < teams[c]; ++t) {
+      lane_class.push_back(c);
+      lane_start.push_back(lane_start.back() + sizes[c]);
+    }
+  }
+  batch->lanes = static_cast<int>(lane_class.size());
+  batch->classes = classes;
+  std::vector<long long> particle_offset(batch->particle_offsets.begin(), batch->particle_offsets.end() - 1);
+  std::vector<long long> element_offset(batch->element_offsets.begin(), batch->element_offsets.end() - 1);
+  PD_CUDA(batch->d_forward_args.upload(forward));
+  PD_CUDA(batch->d_adjoint_args.upload(adjoint));
+  PD_CUDA(batch->d_lane_start.upload(lane_start));
+  PD_CUDA(batch->d_lane_class.upload(lane_class));
+  PD_CUDA(batch->d_class_begin.upload(class_begin));
+  PD_CUDA(batch->d_class_order.upload(class_order));
+  PD_CUDA(batch->d_particle_offset.upload(particle_offset));
+  PD_CUDA(batch->d_element_offset.upload(element_offset));
+  PD_CUDA(batch->d_class_head.allocate(static_cast<size_t>(classes) * sizeof(unsigned)));
+  PD_CUDA(batch->d_lane_slot.allocate(static_cast<size_t>(batch->lanes) * sizeof(int)));
+  PD_CUDA(batch->d_barriers.allocate(static_cast<size_t>(batch->lanes) * sizeof(pdb200::GridBarrier)));
+  PD_CUDA(batch->d_team_status.allocate(sizeof(int)));
+  PD_CUDA(batch->d_timeline.allocate(static_cast<size_t>(count) * 4 * sizeof(unsigned long long)));
+  PD_CUDA(pdb200::team_forward_max_blocks(batch->precision, smem, &per_sm_forward));
+  PD_CUDA(pdb200::team_adjoint_max_blocks(batch->precision, smem, &per_sm_adjoint));
+  batch->team_blocks = lane_start.back();
+  if (batch->team_blocks > std::max(1, std::min(per_sm_forward, per_sm_adjoint)) * sms)
+    return pd_set_error(PD_ERR_UNSUPPORTED, "the lanes do not fit the co-resident grid");
+  batch->team_smem = smem;
+  PD_CUDA(cudaStreamCreateWithFlags(&batch->capture, cudaStreamNonBlocking));
+  return PD_OK;
+}
+
+extern "C" int pd_batch_create(PdSolver* const* solvers, int32_t count, const PdBatchOptions* options,
+                               PdBatch** out) {
+  if (solvers == nullptr || out == nullptr || count < 1) return pd_set_error(PD_ERR_INVALID, "batch needs solvers");
+  *out = nullptr;
+  PdBatchOptions opts{};
+  opts.svd_warm_start = 1;
+  opts.task_nnz = 32768;
+  opts.run_gap = 2;
+  opts.local_cells = 64;
+  opts.schedule = PD_BATCH_TEAMS;
+  opts.team_nnz = 65536;
+  opts.team_samples = 512;
+  if (options != nullptr) opts = *options;
+  if (opts.task_nnz < 256 || opts.run_gap < 0 || opts.local_cells < 4 || opts.team_nnz < 1 || opts.team_samples < 1 ||
+      (opts.schedule != PD_BATCH_TEAMS && opts.schedule != PD_BATCH_PHASES))
+    return pd_set_error(PD_ERR_INVALID, "batch options out of range");
+  auto batch = std::make_unique<PdBatch>();
+  batch->count = count;
+  batch->solvers.assign(solvers, solvers + count);
+  for (int i = 0; i < count; ++i) {
+    const PdSolver* s = solvers[i];
+    if (s == nullptr) return pd_set_error(PD_ERR_INVALID, "null solver in batch");
+    if (!s->built || s->stale) return pd_set_error(PD_ERR_STATE, "every batched solver must be built (pd_build)");
+    if (s->device != solvers[0]->device || s->options.precision != solvers[0]->options.precision ||
+        s->options.state_precision != solvers[0]->options.state_precision || s->built_dt != solvers[0]->built_dt)
+      return pd_set_error(PD_ERR_INVALID, "batched solvers must share device, precision, state precision and dt");
+    if (s->activations != nullptr && !s->hex)
+      return pd_set_error(PD_ERR_UNSUPPORTED, "muscle activations are not supported by the batched path");
+  }
+  batch->device = solvers[0]->device;
+  batch->precision = solvers[0]->options.precision;
+  batch->state_f64 = solvers[0]->options.state_precision;
+  PD_CUDA(cudaSetDevice(batch->device));
+  int64_t particles = 0, elements = 0;
+  for (int i = 0; i < count; ++i) {
+    batch->particle_offsets.push_back(particles);
+    batch->element_offsets.push_back(elements);
+    particles += solvers[i]->n;
+    elements += solvers[i]->ne;
+  }
+  batch->particle_offsets.push_back(particles);
+  batch->element_offsets.push_back(elements);
+  batch->schedule = opts.schedule;
+  int max_iterations = 0;
+  for (int i = 0; i < count; ++i) max_iterations = std::max(max_iterations, solvers[i]->options.max_iterations);
+  batch->max_iterations = static_cast<unsigned>(max_iterations);
+  if (int status = opts.schedule == PD_BATCH_PHASES ? create_phases(batch.get(), opts) : create_teams(batch.get(), opts))
+    return status;
   *out = batch.release();
   return PD_OK;
 }
@@ -1097,6 +1281,63 @@ int build_graph(PdBatch* b, const GraphKey& key) {
 
 }  // namespace
 
+namespace {
+
+pdb200::TeamLaunch team_launch(const PdBatch* b, int steps, double dt, const double gravity[3]) {
+  pdb200::TeamLaunch launch{};
+  launch.forward = b->d_forward_args.as<pdb200::StepArgs>();
+  launch.adjoint = b->d_adjoint_args.as<pdb200::AdjointArgs>();
+  launch.lane_start = b->d_lane_start.as<int>();
+  launch.lane_class = b->d_lane_class.as<int>();
+  launch.class_begin = b->d_class_begin.as<int>();
+  launch.class_order = b->d_class_order.as<int>();
+  launch.particle_offset = b->d_particle_offset.as<long long>();
+  launch.element_offset = b->d_element_offset.as<long long>();
+  launch.count = b->count;
+  launch.lanes = b->lanes;
+  launch.steps = steps;
+  launch.dt = dt;
+  for (int c = 0; c < 3; ++c) launch.gravity[c] = gravity != nullptr ? gravity[c] : 0.0;
+  launch.state_f64 = b->state_f64;
+  launch.class_head = b->d_class_head.as<unsigned>();
+  launch.lane_slot = b->d_lane_slot.as<int>();
+  launch.lane_barrier = b->d_barriers.as<pdb200::GridBarrier>();
+  launch.status = b->d_team_status.as<int>();
+  launch.particles = b->particle_offsets.back();
+  return launch;
+}
+
+// Captures queue reset, the given clears and one team launch into a graph on
+// the batch's private stream (the caller's stream may be the legacy default
+// stream, which cannot capture).
+int capture_team_rollout(PdBatch* b, const pdb200::TeamLaunch& launch, bool adjoint,
+                         const std::vector<std::pair<void*, size_t>>& clears, cudaGraphExec_t* exec) {
+  if (*exec != nullptr) {
+    cudaGraphExecDestroy(*exec);
+    *exec = nullptr;
+  }
+  PD_CUDA(cudaStreamBeginCapture(b->capture, cudaStreamCaptureModeThreadLocal));
+  cudaError_t status = cudaMemsetAsync(b->d_barriers.ptr, 0, b->d_barriers.bytes, b->capture);
+  if (status == cudaSuccess) status = cudaMemsetAsync(b->d_class_head.ptr, 0, b->d_class_head.bytes, b->capture);
+  if (status == cudaSuccess) status = cudaMemsetAsync(b->d_team_status.ptr, 0, b->d_team_status.bytes, b->capture);
+  for (const auto& clear : clears) {
+    if (status == cudaSuccess && clear.first != nullptr) status = cudaMemsetAsync(clear.first, 0, clear.second, b->capture);
+  }
+  if (status == cudaSuccess) {
+    status = adjoint ? pdb200::launch_team_adjoint(launch, b->team_blocks, b->precision, b->team_smem, b->capture)
+                     : pdb200::launch_team_forward(launch, b->team_blocks, b->precision, b->team_smem, b->capture);
+  }
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ended = cudaStreamEndCapture(b->capture, &graph);
+  if (status == cudaSuccess) status = ended;
+  if (status == cudaSuccess) status = cudaGraphInstantiate(exec, graph, 0);
+  if (graph != nullptr) cudaGraphDestroy(graph);
+  PD_CUDA(status);
+  return PD_OK;
+}
+
+}  // namespace
+
 extern "C" int pd_batch_forward(PdBatch* batch, int32_t steps, double dt, const double gravity[3], const void* q0,
                                 const void* qd0, const void* forces, int64_t force_step_stride, void* q_traj,
                                 void* qd_traj, double* x_record, void* stream) {
@@ -1121,10 +1362,82 @@ extern "C" int pd_batch_forward(PdBatch* batch, int32_t steps, double dt, const 
   key.q_traj = q_traj;
   key.qd_traj = qd_traj;
   key.x_record = x_record;
+  if (batch->schedule == PD_BATCH_TEAMS) {
+    if (batch->exec == nullptr || !(batch->key == key)) {
+      PD_CUDA(batch->d_log.allocate(static_cast<size_t>(steps) * batch->count * sizeof(int)));
+      pdb200::TeamLaunch launch = team_launch(batch, steps, dt, gravity);
+      launch.q0 = q0;
+      launch.qd0 = qd0;
+      launch.forces = forces;
+      launch.force_stride = force_step_stride;
+      launch.q_traj = q_traj;
+      launch.qd_traj = qd_traj;
+      launch.x_record = x_record;
+      launch.iteration_log = batch->d_log.as<int>();
+      launch.timeline = batch->d_timeline.as<unsigned long long>();
+      if (int status = capture_team_rollout(batch, launch, false, {}, &batch->exec)) return status;
+      batch->key = key;
+    }
+    PD_CUDA(cudaGraphLaunch(batch->exec, static_cast<cudaStream_t>(stream)));
+    return PD_OK;
+  }
   if (batch->exec == nullptr || !(batch->key == key)) {
     if (int status = build_graph(batch, key)) return status;
   }
   PD_CUDA(cudaGraphLaunch(batch->exec, static_cast<cudaStream_t>(stream)));
+  return PD_OK;
+}
+
+extern "C" int pd_batch_backward(PdBatch* batch, int32_t steps, double dt, const double* x_record,
+                                 const void* grad_q_final, const void* grad_qd_final, void* grad_q, void* grad_qd,
+                                 void* grad_forces, double* grad_materials, int32_t* iterations, void* stream) {
+  if (batch == nullptr || x_record == nullptr || grad_q_final == nullptr || grad_qd_final == nullptr ||
+      grad_q == nullptr || grad_qd == nullptr || grad_forces == nullptr)
+    return pd_set_error(PD_ERR_INVALID, "null argument");
+  if (steps < 1) return pd_set_error(PD_ERR_INVALID, "steps must be positive");
+  if (batch->schedule != PD_BATCH_TEAMS)
+    return pd_set_error(PD_ERR_UNSUPPORTED, "the batched adjoint runs on the teams schedule");
+  for (const PdSolver* s : batch->solvers) {
+    if (!s->built || s->stale || s->built_dt != dt)
+      return pd_set_error(PD_ERR_STATE, "the batched adjoint needs the factors of its rollout (same dt)");
+  }
+  PD_CUDA(cudaSetDevice(batch->device));
+  GraphKey key;
+  key.steps = steps;
+  key.dt = dt;
+  key.q0 = x_record;
+  key.qd0 = grad_q_final;
+  key.forces = grad_qd_final;
+  key.q_traj = grad_q;
+  key.qd_traj = grad_qd;
+  key.x_record = const_cast<double*>(static_cast<const double*>(grad_forces));
+  key.force_stride = reinterpret_cast<long long>(grad_materials);
+  if (batch->adjoint_exec == nullptr || !(batch->adjoint_key == key)) {
+    PD_CUDA(batch->d_adjoint_log.allocate(static_cast<size_t>(steps) * batch->count * sizeof(int)));
+    pdb200::TeamLaunch launch = team_launch(batch, steps, dt, nullptr);
+    launch.x_record = const_cast<double*>(x_record);
+    launch.grad_q_final = grad_q_final;
+    launch.grad_qd_final = grad_qd_final;
+    launch.grad_q = grad_q;
+    launch.grad_qd = grad_qd;
+    launch.grad_forces = grad_forces;
+    launch.grad_materials = grad_materials;
+    launch.iteration_log = batch->d_adjoint_log.as<int>();
+    launch.timeline = batch->d_timeline.as<unsigned long long>() + 2 * batch->count;
+    const size_t elem = batch->state_f64 ? sizeof(double) : sizeof(float);
+    const size_t step_bytes = static_cast<size_t>(3) * batch->particle_offsets.back() * elem;
+    std::vector<std::pair<void*, size_t>> clears = {
+        {grad_forces, steps * step_bytes},
+        {grad_materials, static_cast<size_t>(2) * batch->element_offsets.back() * sizeof(double)}};
+    if (int status = capture_team_rollout(batch, launch, true, clears, &batch->adjoint_exec)) return status;
+    batch->adjoint_key = key;
+  }
+  PD_CUDA(cudaGraphLaunch(batch->adjoint_exec, static_cast<cudaStream_t>(stream)));
+  if (iterations != nullptr) {
+    PD_CUDA(cudaMemcpyAsync(iterations, batch->d_adjoint_log.ptr, static_cast<size_t>(steps) * batch->count * sizeof(int),
+                            cudaMemcpyDeviceToHost, static_cast<cudaStream_t>(stream)));
+    PD_CUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+  }
   return PD_OK;
 }
 
@@ -1157,6 +1470,8 @@ extern "C" int pd_batch_forward_stepwise(PdBatch* batch, int32_t steps, double d
     return pd_set_error(PD_ERR_INVALID, "null argument");
   if (steps < 1) return pd_set_error(PD_ERR_INVALID, "steps must be positive");
   if (force_step_stride < 0) return pd_set_error(PD_ERR_INVALID, "force step stride must be nonnegative");
+  if (batch->schedule != PD_BATCH_PHASES)
+    return pd_set_error(PD_ERR_UNSUPPORTED, "stepwise launches exist for the phases schedule");
   for (const PdSolver* s : batch->solvers) {
     if (!s->built || s->stale || s->built_dt != dt)
       return pd_set_error(PD_ERR_STATE, "every batched solver must be built (pd_build) for this dt");
@@ -1227,5 +1542,28 @@ extern "C" int pd_batch_forward_stepwise(PdBatch* batch, int32_t steps, double d
       if (active == 0) break;
     }
   }
+  return PD_OK;
+}
+
+extern "C" int pd_batch_team_sizes(const PdBatch* batch, int32_t* sizes, int32_t* grid) {
+  if (batch == nullptr) return pd_set_error(PD_ERR_INVALID, "null batch");
+  if (sizes != nullptr) {
+    for (int i = 0; i < batch->count; ++i) sizes[i] = batch->schedule == PD_BATCH_TEAMS ? batch->team_size[i] : 0;
+  }
+  if (grid != nullptr) *grid = batch->team_blocks;
+  return PD_OK;
+}
+
+extern "C" int pd_batch_timeline(PdBatch* batch, uint64_t* forward, uint64_t* adjoint, void* stream) {
+  if (batch == nullptr) return pd_set_error(PD_ERR_INVALID, "null batch");
+  if (batch->schedule != PD_BATCH_TEAMS || batch->d_timeline.ptr == nullptr)
+    return pd_set_error(PD_ERR_UNSUPPORTED, "timelines are recorded by the teams schedule");
+  PD_CUDA(cudaSetDevice(batch->device));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const size_t half = static_cast<size_t>(2) * batch->count * sizeof(uint64_t);
+  const char* base = static_cast<const char*>(batch->d_timeline.ptr);
+  if (forward != nullptr) PD_CUDA(cudaMemcpyAsync(forward, base, half, cudaMemcpyDeviceToHost, st));
+  if (adjoint != nullptr) PD_CUDA(cudaMemcpyAsync(adjoint, base + half, half, cudaMemcpyDeviceToHost, st));
+  PD_CUDA(cudaStreamSynchronize(st));
   return PD_OK;
 }

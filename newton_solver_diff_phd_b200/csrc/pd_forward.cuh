@@ -372,7 +372,9 @@ __device__ void spmv_block(const SpmvPlan& plan, const TV* global_values, bool r
     const int r = rowlist[w];
     const int begin = off[r], end = off[r + 1];
     double sx = 0.0, sy = 0.0, sz = 0.0;
-#pragma unroll 4
+    // Eight entries per lane in flight: enough independent loads to cover
+    // the latency of a factor streamed from L2 or HBM.
+#pragma unroll 8
     for (int k = begin + lane; k < end; k += 32) {
       const double value = static_cast<double>(val[k]);
       const int c = col[k];

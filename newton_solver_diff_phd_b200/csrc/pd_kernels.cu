@@ -3,6 +3,7 @@
 
 #include "pd_forward.cuh"
 #include "pd_kernels.h"
+#include "pd_team.cuh"
 
 // Phase timers of the persistent loop (block 0, thread 0), compiled in only
 // with -DPD_PHASE_TIMERS; the timing probe builds such a variant.
@@ -360,6 +361,60 @@ __global__ void __launch_bounds__(kBlock) forward_step_kernel(const StepArgs a) 
   forward_step_body<TL, TV>(a, Team{static_cast<int>(blockIdx.x), static_cast<int>(gridDim.x)}, dyn_smem);
 }
 
+// Whole forward rollouts of many instances, each by a team of blocks: the
+// single-instance step body with the team's rank and size, one step after
+// the other, a team barrier between steps (the next step reads the states
+// every member wrote).
+template <typename TL, typename TV>
+__global__ void __launch_bounds__(kBlock) team_forward_kernel(const TeamLaunch launch) {
+  extern __shared__ __align__(16) char dyn_smem[];
+  __shared__ StepArgs s_args;
+  Team team;
+  const int lane = lane_of_block(launch, team);
+  GridBarrier* barrier = &launch.lane_barrier[lane];
+  const int f64 = launch.state_f64;
+  const long long step_elements = 3 * launch.particles;
+  for (;;) {
+    const int instance = next_instance(launch, lane, team, launch.status);
+    if (instance < 0) return;
+    copy_arguments(launch.forward + instance, &s_args);
+    if (launch.timeline != nullptr && team.rank == 0 && threadIdx.x == 0) {
+      unsigned long long now;
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+      launch.timeline[2 * instance] = now;
+    }
+    const long long offset = 3 * launch.particle_offset[instance];
+    __syncthreads();
+    for (int t = 0; t < launch.steps; ++t) {
+      if (threadIdx.x == 0) {
+        s_args.barrier = barrier;
+        s_args.q_in = t == 0 ? state_offset(launch.q0, f64, offset)
+                             : state_offset(static_cast<const void*>(launch.q_traj), f64, (t - 1) * step_elements + offset);
+        s_args.qd_in = t == 0 ? state_offset(launch.qd0, f64, offset)
+                              : state_offset(static_cast<const void*>(launch.qd_traj), f64, (t - 1) * step_elements + offset);
+        s_args.f_in = state_offset(launch.forces, f64, t * launch.force_stride + offset);
+        s_args.dirichlet = nullptr;
+        s_args.q_out = state_offset(launch.q_traj, f64, t * step_elements + offset);
+        s_args.qd_out = state_offset(launch.qd_traj, f64, t * step_elements + offset);
+        s_args.x_record = launch.x_record != nullptr ? launch.x_record + t * step_elements + offset : nullptr;
+        s_args.dt = launch.dt;
+        for (int c = 0; c < 3; ++c) s_args.gravity[c] = launch.gravity[c];
+      }
+      __syncthreads();
+      if (!forward_step_body<TL, TV>(s_args, team, dyn_smem)) return;
+      if (team.rank == 0 && threadIdx.x == 0 && launch.iteration_log != nullptr)
+        launch.iteration_log[t * launch.count + instance] = *s_args.iteration;
+      // The next step reads the states every rank of the lane wrote.
+      if (!grid_sync(barrier, s_args.status, team.size, team.rank)) return;
+    }
+    if (launch.timeline != nullptr && team.rank == 0 && threadIdx.x == 0) {
+      unsigned long long now;
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+      launch.timeline[2 * instance + 1] = now;
+    }
+  }
+}
+
 // Plain out = S^T (S rhs) with separate launches (SparseInverse.apply).
 template <typename TV>
 __global__ void __launch_bounds__(kBlock) spmv_kernel(const int* off, const int* col, const TV* val, const double* vec,
@@ -411,6 +466,33 @@ static const void* forward_kernel(int precision) {
   if (precision == 0) return reinterpret_cast<const void*>(&forward_step_kernel<double, double>);
   if (precision == 1) return reinterpret_cast<const void*>(&forward_step_kernel<double, float>);
   return reinterpret_cast<const void*>(&forward_step_kernel<float, float>);
+}
+
+static const void* team_forward(int precision) {
+  if (precision == 0) return reinterpret_cast<const void*>(&team_forward_kernel<double, double>);
+  if (precision == 1) return reinterpret_cast<const void*>(&team_forward_kernel<double, float>);
+  return reinterpret_cast<const void*>(&team_forward_kernel<float, float>);
+}
+
+cudaError_t launch_team_forward(const TeamLaunch& launch, int blocks, int precision, size_t smem, cudaStream_t stream) {
+  void* params[] = {const_cast<TeamLaunch*>(&launch)};
+  return cudaLaunchCooperativeKernel(team_forward(precision), dim3(blocks), dim3(kBlock), params, smem, stream);
+}
+
+cudaError_t team_forward_max_blocks(int precision, size_t smem, int* blocks_per_sm) {
+  const void* kernel = team_forward(precision);
+  int device = 0, optin = 0;
+  cudaError_t status = cudaGetDevice(&device);
+  if (status != cudaSuccess) return status;
+  status = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+  if (status != cudaSuccess) return status;
+  cudaFuncAttributes attributes{};
+  status = cudaFuncGetAttributes(&attributes, kernel);
+  if (status != cudaSuccess) return status;
+  status = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                optin - static_cast<int>(attributes.sharedSizeBytes));
+  if (status != cudaSuccess) return status;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kernel, kBlock, smem);
 }
 
 cudaError_t launch_forward_step(const StepArgs& args, int blocks, int precision, size_t smem, cudaStream_t stream) {

@@ -91,6 +91,57 @@ struct AdjointArgs {
   double dt, inertia;
 };
 
+// One persistent launch that runs whole rollouts of many instances. The grid
+// is cut into lanes: fixed ranges of blocks that form one team each. Every
+// lane belongs to a size class and pulls instances of its class from the
+// class queue; a team runs all steps of its instance with the
+// single-instance step body and its lane's barrier, then pulls again.
+struct TeamLaunch {
+  const StepArgs* forward;          // [count] per-instance step arguments (class plans; per-step fields unset)
+  const AdjointArgs* adjoint;       // [count] per-instance adjoint arguments (per-call fields unset)
+  const int* lane_start;            // [lanes + 1] first block of each lane
+  const int* lane_class;            // [lanes]
+  const int* class_begin;           // [classes + 1] range of each class in class_order
+  const int* class_order;           // instance ids, grouped by class
+  const long long* particle_offset; // [count] first particle in the concatenated arrays
+  const long long* element_offset;  // [count] first element in the concatenated arrays
+  int count;
+  int lanes;
+  int steps;
+  double dt;
+  double gravity[3];
+  int state_f64;
+  unsigned* class_head;             // [classes] next position of each class queue
+  int* lane_slot;                   // [lanes] instance the lane works on (broadcast to its blocks)
+  GridBarrier* lane_barrier;        // [lanes]
+  int* status;                      // launch-wide status (a lane barrier that gave up)
+  int* iteration_log;               // [steps][count]
+  unsigned long long* timeline;     // [count][2] global-timer start and end of each instance's rollout, or nullptr
+  // Forward rollout: concatenated [P][3] states.
+  const void* q0;
+  const void* qd0;
+  const void* forces;               // step t at forces + t * force_stride elements
+  long long force_stride;
+  void* q_traj;                     // [steps][P][3]
+  void* qd_traj;
+  double* x_record;                 // [steps][P][3] float64 (required by the adjoint)
+  // Adjoint rollout: gradients of the loss w.r.t. the final state in, w.r.t.
+  // the initial state, every step's forces and the per-element Lame
+  // parameters out.
+  const void* grad_q_final;         // [P][3]
+  const void* grad_qd_final;
+  void* grad_q;                     // [2][P][3] ping-pong; the last written holds dL/dq0
+  void* grad_qd;
+  void* grad_forces;                // [steps][P][3], accumulated
+  double* grad_materials;           // [E][2] concatenated, accumulated
+  long long particles;              // P
+};
+
+cudaError_t launch_team_forward(const TeamLaunch& launch, int blocks, int precision, size_t smem, cudaStream_t stream);
+cudaError_t team_forward_max_blocks(int precision, size_t smem, int* blocks_per_sm);
+cudaError_t launch_team_adjoint(const TeamLaunch& launch, int blocks, int precision, size_t smem, cudaStream_t stream);
+cudaError_t team_adjoint_max_blocks(int precision, size_t smem, int* blocks_per_sm);
+
 cudaError_t launch_forward_step(const StepArgs& args, int blocks, int precision, size_t smem, cudaStream_t stream);
 cudaError_t forward_step_max_blocks(int precision, size_t smem, int* blocks_per_sm);
 cudaError_t launch_adjoint_step(const AdjointArgs& args, int blocks, int precision, size_t smem, cudaStream_t stream);

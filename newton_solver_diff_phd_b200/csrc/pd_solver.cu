@@ -91,6 +91,7 @@ int pd_set_error(int code, const std::string& message) {
 }
 
 
+
 namespace {
 
 int validate_options(const PdOptions& o) {
@@ -359,6 +360,61 @@ int pd_set_planar_energies(PdSolver* solver, int32_t count, const int32_t* verti
   return PD_OK;
 }
 
+// Splits both factor products into `blocks` nnz-balanced row ranges (the
+// blocks of one cooperative team), orders each range's rows for the SpMV, and
+// decides what stays in `budget` bytes of dynamic shared memory: the factor
+// slices for the whole launch when they fit, the SpMV input vector when it
+// fits as well. The factor arrays must be uploaded.
+int pd_plan_launch(PdSolver* s, int blocks, int budget) {
+  s->blocks = blocks;
+  const std::vector<int32_t> s_part = partition_rows(s->factor.s.offsets, blocks);
+  const std::vector<int32_t> st_part = partition_rows(s->factor.st.offsets, blocks);
+  PD_CUDA(s->d_s_part.upload(s_part));
+  PD_CUDA(s->d_st_part.upload(st_part));
+  {
+    std::vector<int32_t> rowlist, nshort;
+    int max_nnz = 0, max_rows = 0;
+    plan_rows(s->factor.s.offsets, s_part, rowlist, nshort, max_nnz, max_rows);
+    PD_CUDA(s->d_s_rowlist.upload(rowlist));
+    PD_CUDA(s->d_s_nshort.upload(nshort));
+    s->plan_s.max_nnz = max_nnz;
+    s->plan_s.max_rows = max_rows;
+    plan_rows(s->factor.st.offsets, st_part, rowlist, nshort, max_nnz, max_rows);
+    PD_CUDA(s->d_st_rowlist.upload(rowlist));
+    PD_CUDA(s->d_st_nshort.upload(nshort));
+    s->plan_st.max_nnz = max_nnz;
+    s->plan_st.max_rows = max_rows;
+  }
+  const int value_bytes = s->options.precision == PD_PRECISION_FP64 ? 8 : 4;
+  const int slice_s = pdb200::slice_bytes(s->plan_s.max_nnz, s->plan_s.max_rows, value_bytes);
+  const int slice_st = pdb200::slice_bytes(s->plan_st.max_nnz, s->plan_st.max_rows, value_bytes);
+  const int vector_bytes = pdb200::align16(3 * s->n * 8);
+  s->resident = s->options.resident != 0 && slice_s + slice_st <= budget ? 1 : 0;
+  const int slices = s->resident ? slice_s + slice_st : 0;
+  s->stage_vector = s->options.resident != 0 && slices + vector_bytes <= budget ? 1 : 0;
+  s->plan_s.smem_offset = 0;
+  s->plan_st.smem_offset = slice_s;
+  s->vector_smem_offset = slices;
+  s->smem = static_cast<size_t>(slices + (s->stage_vector ? vector_bytes : 0));
+  auto fill_plan = [&](pdb200::SpmvPlan& plan, const DeviceBuffer& off, const DeviceBuffer& col, const DeviceBuffer& val,
+                       const DeviceBuffer& val32, const DeviceBuffer& part, const DeviceBuffer& rowlist,
+                       const DeviceBuffer& nshort) {
+    plan.off = off.as<int>();
+    plan.col = col.as<int>();
+    plan.val64 = val.as<double>();
+    plan.val32 = val32.as<float>();
+    plan.part = part.as<int>();
+    plan.rowlist = rowlist.as<int>();
+    plan.nshort = nshort.as<int>();
+  };
+  fill_plan(s->plan_s, s->d_s_off, s->d_s_col, s->d_s_val, s->d_s_val32, s->d_s_part, s->d_s_rowlist, s->d_s_nshort);
+  fill_plan(s->plan_st, s->d_st_off, s->d_st_col, s->d_st_val, s->d_st_val32, s->d_st_part, s->d_st_rowlist,
+            s->d_st_nshort);
+  PD_CUDA(s->d_partials.allocate(static_cast<size_t>(blocks) * pdb200::kPartialStride * sizeof(double)));
+  PD_CUDA(s->b_partials.allocate(static_cast<size_t>(blocks) * pdb200::kPartialStride * sizeof(double)));
+  return PD_OK;
+}
+
 int pd_build(PdSolver* s, double dt) {
   if (s == nullptr) return fail(PD_ERR_INVALID, "null solver");
   if (!std::isfinite(dt) || dt <= 0.0) return fail(PD_ERR_INVALID, "dt must be finite and positive");
@@ -492,9 +548,6 @@ int pd_build(PdSolver* s, double dt) {
   }
   // Fixed-order reductions handle up to 256 blocks (8 chunks of 32).
   blocks = std::min(std::min(blocks, s->max_blocks), 256);
-  s->blocks = blocks;
-  const std::vector<int32_t> s_part = partition_rows(s->factor.s.offsets, blocks);
-  const std::vector<int32_t> st_part = partition_rows(s->factor.st.offsets, blocks);
   PD_CUDA(s->d_s_off.upload(s->factor.s.offsets));
   PD_CUDA(s->d_s_col.upload(s->factor.s.columns));
   PD_CUDA(s->d_s_val.upload(s->factor.s.values));
@@ -507,39 +560,10 @@ int pd_build(PdSolver* s, double dt) {
     PD_CUDA(s->d_s_val32.upload(s32));
     PD_CUDA(s->d_st_val32.upload(st32));
   }
-  PD_CUDA(s->d_s_part.upload(s_part));
-  PD_CUDA(s->d_st_part.upload(st_part));
-  {
-    std::vector<int32_t> rowlist, nshort;
-    int max_nnz = 0, max_rows = 0;
-    plan_rows(s->factor.s.offsets, s_part, rowlist, nshort, max_nnz, max_rows);
-    PD_CUDA(s->d_s_rowlist.upload(rowlist));
-    PD_CUDA(s->d_s_nshort.upload(nshort));
-    s->plan_s.max_nnz = max_nnz;
-    s->plan_s.max_rows = max_rows;
-    plan_rows(s->factor.st.offsets, st_part, rowlist, nshort, max_nnz, max_rows);
-    PD_CUDA(s->d_st_rowlist.upload(rowlist));
-    PD_CUDA(s->d_st_nshort.upload(nshort));
-    s->plan_st.max_nnz = max_nnz;
-    s->plan_st.max_rows = max_rows;
-  }
-  // Shared memory: keep the factor slices resident for the whole launch when
-  // they fit, and stage the SpMV input vector when it fits as well.
   {
     int optin = 0;
     PD_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, s->device));
-    const int budget = optin - 8 * 1024;  // static shared memory of the kernels
-    const int value_bytes = s->options.precision == PD_PRECISION_FP64 ? 8 : 4;
-    const int slice_s = pdb200::slice_bytes(s->plan_s.max_nnz, s->plan_s.max_rows, value_bytes);
-    const int slice_st = pdb200::slice_bytes(s->plan_st.max_nnz, s->plan_st.max_rows, value_bytes);
-    const int vector_bytes = pdb200::align16(3 * s->n * 8);
-    s->resident = s->options.resident != 0 && slice_s + slice_st <= budget ? 1 : 0;
-    const int slices = s->resident ? slice_s + slice_st : 0;
-    s->stage_vector = s->options.resident != 0 && slices + vector_bytes <= budget ? 1 : 0;
-    s->plan_s.smem_offset = 0;
-    s->plan_st.smem_offset = slice_s;
-    s->vector_smem_offset = slices;
-    s->smem = static_cast<size_t>(slices + (s->stage_vector ? vector_bytes : 0));
+    if (int status = pd_plan_launch(s, blocks, optin - 8 * 1024)) return status;  // 8 KB: static shared memory
     int per_sm_forward = 0, per_sm_adjoint = 0;
     PD_CUDA(pdb200::forward_step_max_blocks(s->options.precision, s->smem, &per_sm_forward));
     PD_CUDA(pdb200::adjoint_step_max_blocks(s->options.precision, s->smem, &per_sm_adjoint));
@@ -549,28 +573,12 @@ int pd_build(PdSolver* s, double dt) {
       return fail(PD_ERR_CUDA, "the persistent step kernels cannot keep the requested grid co-resident");
     }
   }
-  auto fill_plan = [&](pdb200::SpmvPlan& plan, const DeviceBuffer& off, const DeviceBuffer& col, const DeviceBuffer& val,
-                       const DeviceBuffer& val32, const DeviceBuffer& part, const DeviceBuffer& rowlist,
-                       const DeviceBuffer& nshort) {
-    plan.off = off.as<int>();
-    plan.col = col.as<int>();
-    plan.val64 = val.as<double>();
-    plan.val32 = val32.as<float>();
-    plan.part = part.as<int>();
-    plan.rowlist = rowlist.as<int>();
-    plan.nshort = nshort.as<int>();
-  };
-  fill_plan(s->plan_s, s->d_s_off, s->d_s_col, s->d_s_val, s->d_s_val32, s->d_s_part, s->d_s_rowlist, s->d_s_nshort);
-  fill_plan(s->plan_st, s->d_st_off, s->d_st_col, s->d_st_val, s->d_st_val32, s->d_st_part, s->d_st_rowlist,
-            s->d_st_nshort);
   PD_CUDA(s->d_a_off.upload(row_offsets));
   PD_CUDA(s->d_a_col.upload(row_columns));
   PD_CUDA(s->d_a_val.upload(row_values));
   PD_CUDA(s->d_wc.upload(wc));
   PD_CUDA(s->d_wv.upload(wv));
   PD_CUDA(s->d_wn.upload(wn));
-  PD_CUDA(s->d_partials.allocate(static_cast<size_t>(blocks) * pdb200::kPartialStride * sizeof(double)));
-  PD_CUDA(s->b_partials.allocate(static_cast<size_t>(blocks) * pdb200::kPartialStride * sizeof(double)));
   if (s->d_plane_weight.ptr == nullptr) {
     std::vector<double> none(s->n, 0.0);
     PD_CUDA(s->d_plane_weight.upload(none));
@@ -591,6 +599,87 @@ int pd_factor_stats(const PdSolver* s, int64_t* rows, int64_t* nnz_s, int64_t* n
   return PD_OK;
 }
 
+// Every field of the step arguments that does not change between steps.
+void fill_step_args(const PdSolver* s, StepArgs* a) {
+  a->n = s->n;
+  a->ne = s->ne;
+  a->corners = s->corners;
+  a->hex = s->hex;
+  a->indices = s->d_indices.as<int>();
+  a->gradients = s->d_gradients.as<double>();
+  a->free_ = s->d_free.as<int>();
+  a->inc_offsets = s->d_inc_offsets.as<int>();
+  a->inc_entries = s->d_inc_entries.as<int>();
+  a->plane_weight = s->plane_vertices.empty() ? nullptr : s->d_plane_weight.as<double>();
+  {
+    const double* p = s->plane;
+    for (int c = 0; c < 4; ++c) a->plane[c] = p[c];
+  }
+  a->wc = s->d_wc.as<double>();
+  a->wv = s->d_wv.as<double>();
+  a->wn = s->d_wn.as<double>();
+  a->wm = s->d_wm.as<double>();
+  a->mdir = s->d_mdir.as<double>();
+  a->mtarget = s->d_mtarget.as<double>();
+  a->activations = s->hex ? nullptr : s->activations;
+  a->has_muscles = s->has_muscles ? 1 : 0;
+  a->material = s->options.material;
+  a->nh_mu = s->nh_mu;
+  a->nh_lame = s->nh_lame;
+  a->nh_penalty = s->nh_penalty;
+  a->s_off = s->d_s_off.as<int>();
+  a->s_col = s->d_s_col.as<int>();
+  a->s_val = s->d_s_val.as<double>();
+  a->s_val32 = s->d_s_val32.as<float>();
+  a->st_off = s->d_st_off.as<int>();
+  a->st_col = s->d_st_col.as<int>();
+  a->st_val = s->d_st_val.as<double>();
+  a->st_val32 = s->d_st_val32.as<float>();
+  a->s_part = s->d_s_part.as<int>();
+  a->st_part = s->d_st_part.as<int>();
+  a->a_off = s->d_a_off.as<int>();
+  a->a_col = s->d_a_col.as<int>();
+  a->a_val = s->d_a_val.as<double>();
+  a->refine = s->options.precision != PD_PRECISION_FP64 ? 1 : 0;
+  a->position = s->d_position.as<double>();
+  a->velocity = s->d_velocity.as<double>();
+  a->target = s->d_target.as<double>();
+  a->boundary = s->d_boundary.as<double>();
+  a->x = s->d_x.as<double>();
+  a->prev = s->d_prev.as<double>();
+  a->proj = s->d_proj.as<double>();
+  a->prev_proj = s->d_prev_proj.as<double>();
+  a->rhs = s->d_rhs.as<double>();
+  a->y = s->d_y.as<double>();
+  a->contrib = s->d_contrib.as<double>();
+  a->window = s->options.anderson_window;
+  a->hist_x = s->d_hist_x.as<double>();
+  a->hist_g = s->d_hist_g.as<double>();
+  a->aa_state = s->d_aa_state.as<int>();
+  a->aa_gamma = s->d_aa_gamma.as<double>();
+  a->aa_accept = s->d_aa_accept.as<int>();
+  a->partials = s->d_partials.as<double>();
+  a->iteration = s->d_iteration.as<int>();
+  a->active = s->d_active.as<int>();
+  a->status = s->d_status.as<int>();
+  a->max_iterations = s->options.max_iterations;
+  a->abs_tol = s->options.abs_tol;
+  a->rel_tol = s->options.rel_tol;
+  a->barrier = s->d_barrier.as<pdb200::GridBarrier>();
+  a->mass = s->mass;
+  a->inertia = s->inertia;
+  a->integrate_pinned = s->options.integrate_pinned_velocities;
+  a->state_f64 = s->options.state_precision;
+  a->timers = s->timers;
+  a->plan_s = s->plan_s;
+  a->plan_st = s->plan_st;
+  a->resident = s->resident;
+  a->stage_vector = s->stage_vector;
+  a->vector_smem_offset = s->vector_smem_offset;
+  a->svd_u = s->options.svd_warm_start ? s->d_svd_u.as<double>() : nullptr;
+  a->svd_v = s->options.svd_warm_start ? s->d_svd_v.as<double>() : nullptr;
+}
+
 int pd_step(PdSolver* s, const void* q, const void* qd, const void* f, const void* dirichlet,
             const double gravity[3], double dt, void* q_out, void* qd_out, double* x_record, void* stream) {
   if (s == nullptr || q == nullptr || qd == nullptr || f == nullptr || gravity == nullptr || q_out == nullptr ||
@@ -606,71 +695,7 @@ int pd_step(PdSolver* s, const void* q, const void* qd, const void* f, const voi
   PD_CUDA(cudaSetDevice(s->device));
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   StepArgs a{};
-  a.n = s->n;
-  a.ne = s->ne;
-  a.corners = s->corners;
-  a.hex = s->hex;
-  a.indices = s->d_indices.as<int>();
-  a.gradients = s->d_gradients.as<double>();
-  a.free_ = s->d_free.as<int>();
-  a.inc_offsets = s->d_inc_offsets.as<int>();
-  a.inc_entries = s->d_inc_entries.as<int>();
-  a.plane_weight = s->plane_vertices.empty() ? nullptr : s->d_plane_weight.as<double>();
-  {
-    const double* p = s->plane;
-    for (int c = 0; c < 4; ++c) a.plane[c] = p[c];
-  }
-  a.wc = s->d_wc.as<double>();
-  a.wv = s->d_wv.as<double>();
-  a.wn = s->d_wn.as<double>();
-  a.wm = s->d_wm.as<double>();
-  a.mdir = s->d_mdir.as<double>();
-  a.mtarget = s->d_mtarget.as<double>();
-  a.activations = s->hex ? nullptr : s->activations;
-  a.has_muscles = s->has_muscles ? 1 : 0;
-  a.material = s->options.material;
-  a.nh_mu = s->nh_mu;
-  a.nh_lame = s->nh_lame;
-  a.nh_penalty = s->nh_penalty;
-  a.s_off = s->d_s_off.as<int>();
-  a.s_col = s->d_s_col.as<int>();
-  a.s_val = s->d_s_val.as<double>();
-  a.s_val32 = s->d_s_val32.as<float>();
-  a.st_off = s->d_st_off.as<int>();
-  a.st_col = s->d_st_col.as<int>();
-  a.st_val = s->d_st_val.as<double>();
-  a.st_val32 = s->d_st_val32.as<float>();
-  a.s_part = s->d_s_part.as<int>();
-  a.st_part = s->d_st_part.as<int>();
-  a.a_off = s->d_a_off.as<int>();
-  a.a_col = s->d_a_col.as<int>();
-  a.a_val = s->d_a_val.as<double>();
-  a.refine = s->options.precision != PD_PRECISION_FP64 ? 1 : 0;
-  a.position = s->d_position.as<double>();
-  a.velocity = s->d_velocity.as<double>();
-  a.target = s->d_target.as<double>();
-  a.boundary = s->d_boundary.as<double>();
-  a.x = s->d_x.as<double>();
-  a.prev = s->d_prev.as<double>();
-  a.proj = s->d_proj.as<double>();
-  a.prev_proj = s->d_prev_proj.as<double>();
-  a.rhs = s->d_rhs.as<double>();
-  a.y = s->d_y.as<double>();
-  a.contrib = s->d_contrib.as<double>();
-  a.window = s->options.anderson_window;
-  a.hist_x = s->d_hist_x.as<double>();
-  a.hist_g = s->d_hist_g.as<double>();
-  a.aa_state = s->d_aa_state.as<int>();
-  a.aa_gamma = s->d_aa_gamma.as<double>();
-  a.aa_accept = s->d_aa_accept.as<int>();
-  a.partials = s->d_partials.as<double>();
-  a.iteration = s->d_iteration.as<int>();
-  a.active = s->d_active.as<int>();
-  a.status = s->d_status.as<int>();
-  a.max_iterations = s->options.max_iterations;
-  a.abs_tol = s->options.abs_tol;
-  a.rel_tol = s->options.rel_tol;
-  a.barrier = s->d_barrier.as<pdb200::GridBarrier>();
+  fill_step_args(s, &a);
   a.q_in = q;
   a.qd_in = qd;
   a.f_in = f;
@@ -679,23 +704,99 @@ int pd_step(PdSolver* s, const void* q, const void* qd, const void* f, const voi
   a.qd_out = qd_out;
   a.x_record = x_record;
   a.dt = dt;
-  a.mass = s->mass;
-  a.inertia = s->inertia;
   for (int c = 0; c < 3; ++c) a.gravity[c] = gravity[c];
-  a.integrate_pinned = s->options.integrate_pinned_velocities;
-  a.state_f64 = s->options.state_precision;
-  a.timers = s->timers;
-  a.plan_s = s->plan_s;
-  a.plan_st = s->plan_st;
-  a.resident = s->resident;
-  a.stage_vector = s->stage_vector;
-  a.vector_smem_offset = s->vector_smem_offset;
-  a.svd_u = s->options.svd_warm_start ? s->d_svd_u.as<double>() : nullptr;
-  a.svd_v = s->options.svd_warm_start ? s->d_svd_v.as<double>() : nullptr;
   PD_CUDA(cudaMemsetAsync(s->d_barrier.ptr, 0, sizeof(pdb200::GridBarrier), st));
   PD_CUDA(pdb200::launch_forward_step(a, s->blocks, s->options.precision, s->smem, st));
   return PD_OK;
 }
+
+// Every field of the adjoint arguments that does not change between calls.
+void fill_adjoint_args(const PdSolver* s, AdjointArgs* b) {
+  b->n = s->n;
+  b->ne = s->ne;
+  b->corners = s->corners;
+  b->hex = s->hex;
+  b->indices = s->d_indices.as<int>();
+  b->gradients = s->d_gradients.as<double>();
+  b->free_ = s->d_free.as<int>();
+  b->inc_offsets = s->d_inc_offsets.as<int>();
+  b->inc_entries = s->d_inc_entries.as<int>();
+  b->wc = s->d_wc.as<double>();
+  b->wv = s->d_wv.as<double>();
+  b->wn = s->d_wn.as<double>();
+  b->wm = s->d_wm.as<double>();
+  b->mdir = s->d_mdir.as<double>();
+  b->mtarget = s->d_mtarget.as<double>();
+  b->has_muscles = s->has_muscles ? 1 : 0;
+  b->material = s->options.material;
+  b->exact = s->options.adjoint_mode == PD_ADJOINT_EXACT ? 1 : 0;
+  b->pcg = s->options.adjoint_solver == PD_ADJOINT_SOLVER_CG ||
+                  (s->options.adjoint_solver == PD_ADJOINT_SOLVER_AUTO && b->exact)
+              ? 1
+              : 0;
+  b->nh_mu = s->nh_mu;
+  b->nh_lame = s->nh_lame;
+  b->nh_penalty = s->nh_penalty;
+  const double volume = sample_volume_of(s);
+  // StepRecord.jacobian_weights (adjoint.py:828-832): the mean weight per energy.
+  b->jwc = s->options.material == PD_MATERIAL_PD ? 2.0 * s->nh_mu * volume : 0.0;
+  b->jwv = s->options.material == PD_MATERIAL_PD ? s->nh_lame * volume : 0.0;
+  b->jwn = s->options.material == PD_MATERIAL_NEO_HOOKEAN ? 2.0 * s->nh_mu * volume : 0.0;
+  b->sample_volume = volume;
+  b->s_off = s->d_s_off.as<int>();
+  b->s_col = s->d_s_col.as<int>();
+  b->s_val = s->d_s_val.as<double>();
+  b->s_val32 = s->d_s_val32.as<float>();
+  b->st_off = s->d_st_off.as<int>();
+  b->st_col = s->d_st_col.as<int>();
+  b->st_val = s->d_st_val.as<double>();
+  b->st_val32 = s->d_st_val32.as<float>();
+  b->s_part = s->d_s_part.as<int>();
+  b->st_part = s->d_st_part.as<int>();
+  b->a_off = s->d_a_off.as<int>();
+  b->a_col = s->d_a_col.as<int>();
+  b->a_val = s->d_a_val.as<double>();
+  b->refine = s->options.precision != PD_PRECISION_FP64 ? 1 : 0;
+  b->rhs = s->b_rhs.as<double>();
+  b->base = s->b_base.as<double>();
+  b->solution = s->b_solution.as<double>();
+  b->prev = s->b_prev.as<double>();
+  b->work = s->b_work.as<double>();
+  b->y = s->b_y.as<double>();
+  b->raw = s->b_raw.as<double>();
+  b->contrib = s->b_contrib.as<double>();
+  b->jac64 = s->b_jac.as<double>();
+  b->jac32 = s->b_jac.as<float>();
+  b->window = s->options.anderson_window;
+  b->hist_x = s->b_hist_x.as<double>();
+  b->hist_g = s->b_hist_g.as<double>();
+  b->aa_state = s->b_aa_state.as<int>();
+  b->aa_gamma = s->b_aa_gamma.as<double>();
+  b->aa_accept = s->b_aa_accept.as<int>();
+  b->partials = s->b_partials.as<double>();
+  b->iteration = s->b_iteration.as<int>();
+  b->active = s->b_active.as<int>();
+  b->status = s->d_status.as<int>();
+  b->max_iterations = s->options.max_iterations;
+  b->abs_tol = s->options.abs_tol;
+  b->rel_tol = s->options.rel_tol;
+  b->barrier = s->d_barrier.as<pdb200::GridBarrier>();
+  b->control_d = s->b_control_d.as<double>();
+  b->control_i = s->b_control_i.as<int>();
+  b->state_f64 = s->options.state_precision;
+  b->material_scratch = s->b_material_scratch.as<double>();
+  b->activation_scratch = s->b_activation_scratch.as<double>();
+  b->has_dirichlet = s->has_dirichlet ? 1 : 0;
+  b->integrate_pinned = s->options.integrate_pinned_velocities;
+  b->inertia = s->inertia;
+  b->plan_s = s->plan_s;
+  b->plan_st = s->plan_st;
+  b->resident = s->resident;
+  b->stage_vector = s->stage_vector;
+  b->vector_smem_offset = s->vector_smem_offset;
+}
+
+int pd_ensure_adjoint_buffers(PdSolver* s) { return ensure_adjoint_buffers(s); }
 
 int pd_backward(PdSolver* s, const double* x_record, const float* activations, double dt, const void* gq_out,
                 const void* gqd_out, void* gq, void* gqd, void* gf, void* gdirichlet, double* gmaterials,
@@ -713,102 +814,21 @@ int pd_backward(PdSolver* s, const double* x_record, const float* activations, d
     PD_CUDA(cudaMemsetAsync(s->b_zero_gqd.ptr, 0, fvec, st));
   }
   AdjointArgs b{};
-  b.n = s->n;
-  b.ne = s->ne;
-  b.corners = s->corners;
-  b.hex = s->hex;
-  b.indices = s->d_indices.as<int>();
-  b.gradients = s->d_gradients.as<double>();
-  b.free_ = s->d_free.as<int>();
-  b.inc_offsets = s->d_inc_offsets.as<int>();
-  b.inc_entries = s->d_inc_entries.as<int>();
-  b.wc = s->d_wc.as<double>();
-  b.wv = s->d_wv.as<double>();
-  b.wn = s->d_wn.as<double>();
-  b.wm = s->d_wm.as<double>();
-  b.mdir = s->d_mdir.as<double>();
-  b.mtarget = s->d_mtarget.as<double>();
-  b.has_muscles = s->has_muscles ? 1 : 0;
-  b.material = s->options.material;
-  b.exact = s->options.adjoint_mode == PD_ADJOINT_EXACT ? 1 : 0;
-  b.pcg = s->options.adjoint_solver == PD_ADJOINT_SOLVER_CG ||
-                  (s->options.adjoint_solver == PD_ADJOINT_SOLVER_AUTO && b.exact)
-              ? 1
-              : 0;
-  b.nh_mu = s->nh_mu;
-  b.nh_lame = s->nh_lame;
-  b.nh_penalty = s->nh_penalty;
-  const double volume = sample_volume_of(s);
-  // StepRecord.jacobian_weights (adjoint.py:828-832): the mean weight per energy.
-  b.jwc = s->options.material == PD_MATERIAL_PD ? 2.0 * s->nh_mu * volume : 0.0;
-  b.jwv = s->options.material == PD_MATERIAL_PD ? s->nh_lame * volume : 0.0;
-  b.jwn = s->options.material == PD_MATERIAL_NEO_HOOKEAN ? 2.0 * s->nh_mu * volume : 0.0;
-  b.sample_volume = volume;
-  b.s_off = s->d_s_off.as<int>();
-  b.s_col = s->d_s_col.as<int>();
-  b.s_val = s->d_s_val.as<double>();
-  b.s_val32 = s->d_s_val32.as<float>();
-  b.st_off = s->d_st_off.as<int>();
-  b.st_col = s->d_st_col.as<int>();
-  b.st_val = s->d_st_val.as<double>();
-  b.st_val32 = s->d_st_val32.as<float>();
-  b.s_part = s->d_s_part.as<int>();
-  b.st_part = s->d_st_part.as<int>();
-  b.a_off = s->d_a_off.as<int>();
-  b.a_col = s->d_a_col.as<int>();
-  b.a_val = s->d_a_val.as<double>();
-  b.refine = s->options.precision != PD_PRECISION_FP64 ? 1 : 0;
+  fill_adjoint_args(s, &b);
   b.x = x_record;
-  b.rhs = s->b_rhs.as<double>();
-  b.base = s->b_base.as<double>();
-  b.solution = s->b_solution.as<double>();
-  b.prev = s->b_prev.as<double>();
-  b.work = s->b_work.as<double>();
-  b.y = s->b_y.as<double>();
-  b.raw = s->b_raw.as<double>();
-  b.contrib = s->b_contrib.as<double>();
-  b.jac64 = s->b_jac.as<double>();
-  b.jac32 = s->b_jac.as<float>();
-  b.window = s->options.anderson_window;
-  b.hist_x = s->b_hist_x.as<double>();
-  b.hist_g = s->b_hist_g.as<double>();
-  b.aa_state = s->b_aa_state.as<int>();
-  b.aa_gamma = s->b_aa_gamma.as<double>();
-  b.aa_accept = s->b_aa_accept.as<int>();
-  b.partials = s->b_partials.as<double>();
-  b.iteration = s->b_iteration.as<int>();
-  b.active = s->b_active.as<int>();
-  b.status = s->d_status.as<int>();
-  b.max_iterations = s->options.max_iterations;
-  b.abs_tol = s->options.abs_tol;
-  b.rel_tol = s->options.rel_tol;
-  b.barrier = s->d_barrier.as<pdb200::GridBarrier>();
-  b.control_d = s->b_control_d.as<double>();
-  b.control_i = s->b_control_i.as<int>();
   b.gq_out = gq_out != nullptr ? gq_out : s->b_zero_gq.ptr;
   b.gqd_out = gqd_out != nullptr ? gqd_out : s->b_zero_gqd.ptr;
   b.gq = gq != nullptr ? gq : s->b_scratch_gq.ptr;
   b.gqd = gqd != nullptr ? gqd : s->b_scratch_gqd.ptr;
   b.gf = gf != nullptr ? gf : s->b_scratch_gf.ptr;
-  b.state_f64 = s->options.state_precision;
   b.gdirichlet = gdirichlet;
   b.gmaterials = gmaterials;
   b.gactivations = s->hex ? nullptr : gactivations;
-  b.material_scratch = s->b_material_scratch.as<double>();
-  b.activation_scratch = s->b_activation_scratch.as<double>();
-  b.has_dirichlet = s->has_dirichlet ? 1 : 0;
-  b.integrate_pinned = s->options.integrate_pinned_velocities;
   b.zero_energy_weight =
       (gmaterials != nullptr && s->options.material == PD_MATERIAL_PD && s->nh_lame == 0.0) ? 1 : 0;
   b.dt = dt;
-  b.inertia = s->inertia;
   // A Tet4 step's fibre targets are 1 - u of the activations it used.
   b.activations = (!s->hex && s->has_muscles) ? activations : nullptr;
-  b.plan_s = s->plan_s;
-  b.plan_st = s->plan_st;
-  b.resident = s->resident;
-  b.stage_vector = s->stage_vector;
-  b.vector_smem_offset = s->vector_smem_offset;
   PD_CUDA(cudaMemsetAsync(s->d_barrier.ptr, 0, sizeof(pdb200::GridBarrier), st));
   PD_CUDA(pdb200::launch_adjoint_step(b, s->blocks, s->options.precision, s->smem, st));
   return PD_OK;

@@ -17,6 +17,23 @@ using pdb200::InverseFactor;
 // Records the message returned by pd_last_error() and returns code.
 int pd_set_error(int code, const std::string& message);
 
+struct PdSolver;
+namespace pdb200 {
+struct StepArgs;
+struct AdjointArgs;
+}  // namespace pdb200
+
+extern "C" {
+// Launch plan of a built solver for a team of `blocks` blocks with `budget`
+// bytes of dynamic shared memory (pd_solver.cu).
+int pd_plan_launch(PdSolver* s, int blocks, int budget);
+// The fields of the step / adjoint arguments that do not change between
+// calls (pd_solver.cu); the adjoint buffers must exist (pd_ensure_adjoint_buffers).
+void fill_step_args(const PdSolver* s, pdb200::StepArgs* a);
+void fill_adjoint_args(const PdSolver* s, pdb200::AdjointArgs* b);
+int pd_ensure_adjoint_buffers(PdSolver* s);
+}
+
 #define PD_CUDA(call)                                                                                 \
   do {                                                                                                \
     cudaError_t pd_status_ = (call);                                                                  \

@@ -64,10 +64,14 @@ def _batched(instances, **options):
     return batch, q, qd, x, status, iterations
 
 
-def test_batched_fp64_matches_single_instance_steps():
+SCHEDULES = ["teams", "phases"]
+
+
+@pytest.mark.parametrize("schedule", SCHEDULES)
+def test_batched_fp64_matches_single_instance_steps(schedule):
     plain = [_plain(*inst) for inst in _instances("fp64", with_tet=True)]
     instances = _instances("fp64", with_tet=True)
-    batch, q, qd, x, status, iterations = _batched(instances)
+    batch, q, qd, x, status, iterations = _batched(instances, schedule=schedule)
     assert np.all(status == 0), status
     for i, (trajectory, its) in enumerate(plain):
         got = batch.split(q)[i]
@@ -109,26 +113,28 @@ def _relative(a, b):
     return float((a - b).abs().max()) / float(b.abs().max())
 
 
-def test_batched_fp32_refine_arithmetic_error_below_1e6():
+@pytest.mark.parametrize("schedule", SCHEDULES)
+def test_batched_fp32_refine_arithmetic_error_below_1e6(schedule):
     """Same iterations (no convergence stop): float32 factor products with
     float64 residual refinement stay within 1e-6 of the float64 iterates."""
     plain = [_plain64(*inst) for inst in _instances64("fp64", 0.0, 40, abs_tol=0.0)]
-    batch, q, qd, x, status, iterations = _batched(_instances64("fp32+refine", 0.0, 40, abs_tol=0.0))
+    batch, q, qd, x, status, iterations = _batched(_instances64("fp32+refine", 0.0, 40, abs_tol=0.0), schedule=schedule)
     assert np.all(iterations == 40), iterations
     for i, reference in enumerate(plain):
         assert _relative(batch.split(x)[i], reference) <= 1e-6, i
 
 
-def test_batched_fp32_refine_fixed_point_is_the_fp64_solution():
+@pytest.mark.parametrize("schedule", SCHEDULES)
+def test_batched_fp32_refine_fixed_point_is_the_fp64_solution(schedule):
     """Converged tightly, float32 factor products reach the float64 solution
     (within 1e-6); at the working tolerance they land as close to it as the
     float64 solver itself. Float32 local projections move the fixed point by
     about cond(A) * 6e-8, bounded here at 1e-4."""
     truth = [_plain64(*inst) for inst in _instances64("fp64", 1e-12, 50000, abs_tol=0.0)]
     fp64 = [_plain64(*inst) for inst in _instances64("fp64", 1e-6, 20000)]
-    tight = _batched(_instances64("fp32+refine", 1e-10, 50000, abs_tol=0.0))
-    loose = _batched(_instances64("fp32+refine", 1e-6, 20000))
-    fast = _batched(_instances64("fp32", 1e-8, 20000, abs_tol=0.0))
+    tight = _batched(_instances64("fp32+refine", 1e-10, 50000, abs_tol=0.0), schedule=schedule)
+    loose = _batched(_instances64("fp32+refine", 1e-6, 20000), schedule=schedule)
+    fast = _batched(_instances64("fp32", 1e-8, 20000, abs_tol=0.0), schedule=schedule)
     assert np.all(tight[4] == 0) and np.all(loose[4] == 0) and np.all(fast[4] == 0)
     for i, (t, r) in enumerate(zip(truth, fp64)):
         assert _relative(tight[0].split(tight[3])[i], t) <= 1e-6, i
@@ -138,9 +144,10 @@ def test_batched_fp32_refine_fixed_point_is_the_fp64_solution():
         assert _relative(fast[0].split(fast[3])[i], t) <= 1e-4, i
 
 
-def test_batched_rollout_is_bitwise_deterministic_and_graph_is_reused():
+@pytest.mark.parametrize("schedule", SCHEDULES)
+def test_batched_rollout_is_bitwise_deterministic_and_graph_is_reused(schedule):
     instances = _instances("fp32+refine", window=3)
-    batch = BatchedSolver([s for _, s, _ in instances], DT)
+    batch = BatchedSolver([s for _, s, _ in instances], DT, schedule=schedule)
     q0 = batch.concat([m.particle_q for m, _, _ in instances])
     qd0 = torch.zeros_like(q0)
     forces = batch.concat([f for _, _, f in instances])
@@ -151,9 +158,11 @@ def test_batched_rollout_is_bitwise_deterministic_and_graph_is_reused():
         assert torch.equal(a, b)
 
 
-def test_batched_per_step_forces_and_cold_svd():
+@pytest.mark.parametrize("schedule", SCHEDULES)
+def test_batched_per_step_forces_and_cold_svd(schedule):
     instances = _instances("fp64", window=0)
-    batch = BatchedSolver([s for _, s, _ in instances], DT, svd_warm_start=False, task_nnz=512)
+    batch = BatchedSolver([s for _, s, _ in instances], DT, schedule=schedule, svd_warm_start=False, task_nnz=512,
+                          team_nnz=2048, team_samples=64)
     q0 = batch.concat([m.particle_q for m, _, _ in instances])
     qd0 = torch.zeros_like(q0)
     forces = batch.concat([f for _, _, f in instances])
@@ -172,7 +181,7 @@ def test_batched_per_step_forces_and_cold_svd():
 
 def test_stepwise_launches_equal_the_graph():
     instances = _instances("fp32+refine")
-    batch = BatchedSolver([s for _, s, _ in instances], DT)
+    batch = BatchedSolver([s for _, s, _ in instances], DT, schedule="phases")
     q0 = batch.concat([m.particle_q for m, _, _ in instances])
     qd0 = torch.zeros_like(q0)
     forces = batch.concat([f for _, _, f in instances])
@@ -182,3 +191,56 @@ def test_stepwise_launches_equal_the_graph():
     assert np.array_equal(batch.read()[1], graph_iterations)
     for a, b in zip(graph, stepwise):
         assert torch.equal(a, b)
+
+
+def test_teams_form_from_factor_and_sample_counts():
+    instances = _instances("fp64")
+    batch = BatchedSolver([s for _, s, _ in instances], DT, team_nnz=2048, team_samples=64)
+    sizes, grid = batch.team_sizes()
+    assert grid >= 1 and np.all(sizes >= 1) and np.all(sizes <= grid)
+    assert sizes[2] > sizes[0]  # the 12x3x3 cantilever gets a larger team than the 4x2x2 one
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32+refine"])
+def test_batched_adjoint_matches_single_instance_rollouts(precision):
+    """Gradients of a loss on the final positions w.r.t. the initial state,
+    every step's forces and the per-element Lame parameters: the teams
+    adjoint against each instance's own Rollout backward."""
+    from newton_solver_diff_phd_b200.rollout import Rollout
+
+    def make():
+        out = []
+        for spec in _specs():
+            model, mesh, materials, forces = cantilever_model(spec)
+            solver = SolverDiffPhD(model, density=1000.0, hex_mesh=mesh, hex_materials=materials, precision=precision,
+                                   anderson_window=5, rel_tol=1e-8, abs_tol=1e-12, max_iterations=20000,
+                                   adjoint="exact", state_dtype=torch.float64)
+            out.append((model, solver, torch.as_tensor(forces, device="cuda", dtype=torch.float64)))
+        return out
+
+    rng = np.random.default_rng(11)
+    reference = []
+    for model, solver, forces in make():
+        driver = Rollout(solver, STEPS, DT)
+        q0 = model.particle_q.double()
+        final = driver.forward(q0, torch.zeros_like(q0), forces)
+        weights = torch.as_tensor(rng.standard_normal(final.particle_q.shape), device="cuda")
+        gq0, gqd0, gf, gm = driver.backward(weights, None)
+        reference.append((weights, final.particle_q.clone(), gq0.clone(), gqd0.clone(), gf.clone(), gm.clone()))
+    instances = make()
+    batch = BatchedSolver([s for _, s, _ in instances], DT)
+    q0 = batch.concat([m.particle_q for m, _, _ in instances])
+    qd0 = torch.zeros_like(q0)
+    forces = batch.concat([f for _, _, f in instances])
+    q, qd, x = batch.rollout(q0, qd0, forces, STEPS)
+    weights = batch.concat([r[0] for r in reference])
+    gq0, gqd0, gf, gm, iterations = batch.backward(x, weights)
+    assert np.all(iterations > 0)
+    status, _ = batch.read()
+    assert np.all((status & 8) == 0), status
+    eo = batch.element_offsets
+    for i, (w, final, rq, rqd, rf, rm) in enumerate(reference):
+        for got, want in ((batch.split(q)[i][-1], final), (batch.split(gq0)[i], rq), (batch.split(gqd0)[i], rqd),
+                          (batch.split(gf)[i], rf), (gm[eo[i]:eo[i + 1]], rm)):
+            scale = float(want.abs().max())
+            assert float((got - want).abs().max()) <= 1e-5 * scale + 1e-30, (i, float((got - want).abs().max()), scale)
