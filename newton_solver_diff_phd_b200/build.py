@@ -22,7 +22,8 @@ LIBRARY = BUILD / "libpdb200.so"
 
 CUDA_SOURCES = ("pd_kernels.cu", "pd_adjoint.cu", "pd_solver.cu", "pd_noalloc.cu", "pd_batch.cu")
 HOST_SOURCES = ("factor.cpp", "runs.cpp")
-HEADERS = ("factor.h", "pd_math.cuh", "pd_device.cuh", "pd_forward.cuh", "pd_kernels.h")
+HEADERS = ("factor.h", "runs.h", "pd_math.cuh", "pd_device.cuh", "pd_forward.cuh", "pd_kernels.h", "pd_batch.cuh",
+           "pd_team.cuh", "solver_state.h")
 ARCH = ("-gencode", "arch=compute_100a,code=sm_100a")
 
 

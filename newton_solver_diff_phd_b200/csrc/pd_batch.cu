@@ -683,7 +683,7 @@ struct PdBatch {
   DeviceBuffer d_forward_args, d_adjoint_args, d_lane_start, d_lane_class, d_class_begin, d_class_order,
       d_particle_offset, d_element_offset, d_class_head, d_lane_slot, d_barriers, d_team_status, d_adjoint_log,
       d_timeline;
-  int team_blocks = 0, lanes = 0, classes = 0;
+  int team_blocks = 0, lanes = 0, classes = 0, solo_class = -1;
   size_t team_smem = 0;
   cudaStream_t capture = nullptr;  // private stream the rollout graphs are captured on
   cudaGraphExec_t adjoint_exec = nullptr;
@@ -968,11 +968,17 @@ int create_teams(PdBatch* batch, const PdBatchOptions& opts) {
   int per_sm_forward = 0, per_sm_adjoint = 0;
   PD_CUDA(pdb200::team_forward_max_blocks(batch->precision, 0, &per_sm_forward));
   PD_CUDA(pdb200::team_adjoint_max_blocks(batch->precision, 0, &per_sm_adjoint));
-  const int grid_cap = std::max(1, std::min(per_sm_forward, per_sm_adjoint)) * sms;
+  // Blocks per SM the team kernels are built for: the shared-memory budget of
+  // an instance is the SM's share for one of them.
+  const int occupancy = std::max(1, std::min(per_sm_forward, per_sm_adjoint));
+  const int grid_cap = occupancy * sms;
   // Largest class: a power of two that leaves room for one lane of every smaller class.
   int largest = 1;
   while (largest * 4 <= grid_cap && largest < 64) largest *= 2;
-  const int budget = optin - 10 * 1024;  // static shared memory of the team kernels
+  int smem_per_sm = 0;
+  PD_CUDA(cudaDeviceGetAttribute(&smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, batch->device));
+  // 10 KB per block: static shared memory of the team kernels and the per-block reserve.
+  const int budget = std::min(optin, smem_per_sm / occupancy) - 10 * 1024;
   std::vector<double> cost(count);
   std::vector<int> cls_of(count);
   batch->team_size.assign(count, 1);
@@ -1023,6 +1029,9 @@ int create_teams(PdBatch* batch, const PdBatchOptions& opts) {
   double total_work = 0.0;
   for (double w : work) total_work += w;
   std::vector<int> teams(classes, 1);
+  // One-block teams are cheap and their instances often iterate longest:
+  // start with up to 16 of them.
+  if (sizes[0] == 1) teams[0] = std::max(1, std::min(members[0], 16));
   auto used = [&]() {
     int blocks = 0;
     for (int c = 0; c < classes; ++c) blocks += teams[c] * sizes[c];
@@ -1077,6 +1086,7 @@ int create_teams(PdBatch* batch, const PdBatchOptions& opts) {
   }
   batch->lanes = static_cast<int>(lane_class.size());
   batch->classes = classes;
+  batch->solo_class = sizes[0] == 1 ? 0 : -1;
   std::vector<long long> particle_offset(batch->particle_offsets.begin(), batch->particle_offsets.end() - 1);
   std::vector<long long> element_offset(batch->element_offsets.begin(), batch->element_offsets.end() - 1);
   PD_CUDA(batch->d_forward_args.upload(forward));
@@ -1295,6 +1305,7 @@ pdb200::TeamLaunch team_launch(const PdBatch* b, int steps, double dt, const dou
   launch.element_offset = b->d_element_offset.as<long long>();
   launch.count = b->count;
   launch.lanes = b->lanes;
+  launch.solo_class = b->solo_class;
   launch.steps = steps;
   launch.dt = dt;
   for (int c = 0; c < 3; ++c) launch.gravity[c] = gravity != nullptr ? gravity[c] : 0.0;

@@ -366,16 +366,18 @@ __global__ void __launch_bounds__(kBlock) forward_step_kernel(const StepArgs a) 
 // the other, a team barrier between steps (the next step reads the states
 // every member wrote).
 template <typename TL, typename TV>
-__global__ void __launch_bounds__(kBlock) team_forward_kernel(const TeamLaunch launch) {
+__global__ void __launch_bounds__(kBlock, 2) team_forward_kernel(const TeamLaunch launch) {
   extern __shared__ __align__(16) char dyn_smem[];
   __shared__ StepArgs s_args;
-  Team team;
-  const int lane = lane_of_block(launch, team);
+  Team lane_team;
+  const int lane = lane_of_block(launch, lane_team);
   GridBarrier* barrier = &launch.lane_barrier[lane];
   const int f64 = launch.state_f64;
   const long long step_elements = 3 * launch.particles;
+  bool solo = false;
   for (;;) {
-    const int instance = next_instance(launch, lane, team, launch.status);
+    Team team;
+    const int instance = next_work(launch, lane, lane_team, solo, team);
     if (instance < 0) return;
     copy_arguments(launch.forward + instance, &s_args);
     if (launch.timeline != nullptr && team.rank == 0 && threadIdx.x == 0) {

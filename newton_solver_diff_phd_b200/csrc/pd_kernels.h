@@ -107,6 +107,7 @@ struct TeamLaunch {
   const long long* element_offset;  // [count] first element in the concatenated arrays
   int count;
   int lanes;
+  int solo_class;                   // class of one-block teams (-1: none); idle lanes' blocks drain it
   int steps;
   double dt;
   double gravity[3];

@@ -45,6 +45,38 @@ __device__ __forceinline__ int next_instance(const TeamLaunch& launch, int lane,
   return s_instance;
 }
 
+// Every thread of the block: the next instance of the one-block class for a
+// block whose own lane has run out of work, or -1 when that queue is empty.
+__device__ __forceinline__ int claim_solo(const TeamLaunch& launch) {
+  __shared__ int s_instance;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int cls = launch.solo_class;
+    const unsigned position = atomicAdd(&launch.class_head[cls], 1u);
+    const int begin = launch.class_begin[cls];
+    const int end = launch.class_begin[cls + 1];
+    s_instance = static_cast<int>(position) < end - begin ? launch.class_order[begin + position] : -1;
+  }
+  __syncthreads();
+  return s_instance;
+}
+
+// The next instance of this block: its lane's queue first; when that is
+// empty, one-block instances on its own (a lane of one block needs no barrier).
+__device__ __forceinline__ int next_work(const TeamLaunch& launch, int lane, Team lane_team, bool& solo, Team& team) {
+  if (!solo) {
+    const int instance = next_instance(launch, lane, lane_team, launch.status);
+    if (instance >= 0) {
+      team = lane_team;
+      return instance;
+    }
+    if (launch.solo_class < 0 || launch.lane_class[lane] == launch.solo_class) return -1;
+    solo = true;
+  }
+  team = Team{0, 1};
+  return claim_solo(launch);
+}
+
 // Block-wide copy of an argument block (a multiple of 8 bytes) into shared memory.
 template <typename T>
 __device__ __forceinline__ void copy_arguments(const T* source, T* target) {
