@@ -15,6 +15,12 @@ state and forces). One bench step is one 50-step rollout forward and back.
 single instance does not shard (its inverse factor is dense-ish and every
 iteration would need an all-gather). ``value`` is the whole-job rate.
 
+A second leg (N=1, ``--no-batched`` skips it) times the batched path on the
+uneven Hex8 cantilever family (256 instances, nx uniform in [4, 40], ny =
+nz = max(2, nx // 4), 25 steps of dt 0.01 s, fp32+refine, forward + adjoint
+w.r.t. every instance's E) against the plain path stepping each instance on
+its own, and reports both under ``batched``.
+
 ``--impl reference`` times the CPU port of the reference's sparse algorithm
 (oracle/sparse_port.py; the reference's Warp CPU path needs warp-lang and
 newton, which are not installed) on this host's cores, on the same workload.
@@ -320,6 +326,8 @@ def run_b200(args):
     if rank == 0:
         result["e2e"] = run_e2e(args, solver, driver, q0, target, young, dmu_de, dlam_de, device)
         result["cpu_baseline"] = cpu_baseline(args, seconds=args.cpu_seconds)
+        if world == 1 and not args.no_batched:
+            result["batched"] = run_batched(args, device)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -369,6 +377,153 @@ def run_e2e(args, solver, driver, q0, target, young, dmu_de, dlam_de, device):
     d2h = 8 + out_grad.numel() * 8
     return {"value": STEPS_PER_ROLLOUT * steps / (ms / 1000.0), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(d2h), "grad_wrt": "per-tet Young's modulus (E), loss scalar"}
+
+
+BATCH_COUNT = 256
+BATCH_STEPS = 25
+BATCH_DT = 0.01
+BATCH_WORKLOAD = "hex8_cantilever_family_256_uneven_25steps_fwd_adjoint"
+
+
+def batch_family(device, precision, count=BATCH_COUNT, rel_tol=REL_TOL, abs_tol=ABS_TOL, max_iterations=5000):
+    """The uneven Hex8 cantilever family: solvers, per-instance forces and Poisson ratios."""
+    import torch
+
+    from newton_solver_diff_phd_b200 import SolverDiffPhD
+    from newton_solver_diff_phd_b200.scenes import cantilever_family, cantilever_model
+
+    out = []
+    for spec in cantilever_family(count, seed=0):
+        model, mesh, materials, forces = cantilever_model(spec, device=device)
+        solver = SolverDiffPhD(model, density=1000.0, hex_mesh=mesh, hex_materials=materials, precision=precision,
+                               anderson_window=5, rel_tol=rel_tol, abs_tol=abs_tol, max_iterations=max_iterations,
+                               adjoint="exact")
+        out.append((spec, model, solver, torch.as_tensor(forces, device=device)))
+    return out
+
+
+def build_all(solvers, dt):
+    from concurrent.futures import ThreadPoolExecutor
+
+    with ThreadPoolExecutor(os.cpu_count() or 4) as pool:  # the host factor builds release the GIL
+        list(pool.map(lambda s: s._build(dt), solvers))
+
+
+def run_batched(args, device):
+    """Batched vs plain on the uneven cantilever family (forward + adjoint w.r.t. every instance's E)."""
+    import torch
+
+    from newton_solver_diff_phd_b200 import meshes
+    from newton_solver_diff_phd_b200.batch import BatchedSolver
+    from newton_solver_diff_phd_b200.rollout import Rollout
+
+    precision = "fp32+refine"
+    family = batch_family(device, precision)
+    build_all([s for _, _, s, _ in family], BATCH_DT)
+    rng = np.random.default_rng(1)
+    weights = [torch.as_tensor(rng.standard_normal((m.particle_count, 3)), dtype=torch.float32, device=device)
+               for _, m, _, _ in family]
+    # Plain path: every instance on its own, one cooperative launch per step (untouched plans).
+    stream = torch.cuda.current_stream()
+    plain_ms, plain_final = 0.0, []
+    for (spec, model, solver, forces), w in zip(family, weights):
+        driver = Rollout(solver, BATCH_STEPS, BATCH_DT)
+        q0 = model.particle_q
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        final = driver.forward(q0, torch.zeros_like(q0), forces)
+        driver.backward(w, None)
+        end.record(stream)
+        torch.cuda.synchronize()
+        plain_ms += start.elapsed_time(end)
+        plain_final.append(final.particle_q.clone())
+    for _, _, solver, _ in family:
+        solver.read_status()
+    # Batched path.
+    batch = BatchedSolver([s for _, _, s, _ in family], BATCH_DT)
+    sizes, grid = batch.team_sizes()
+    q0 = batch.concat([m.particle_q for _, m, _, _ in family])
+    qd0 = torch.zeros_like(q0)
+    forces = batch.concat([f for _, _, _, f in family])
+    weight = batch.concat(weights)
+    eo = batch.element_offsets
+    nu = torch.tensor(np.repeat([spec.poisson for spec, _, _, _ in family], np.diff(eo)), device=device)
+    dmu_de = 1.0 / (2.0 * (1.0 + nu))
+    dlam_de = nu / ((1.0 + nu) * (1.0 - 2.0 * nu))
+    index = torch.tensor(np.repeat(np.arange(batch.count), np.diff(eo)), device=device)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+
+    def one(out=None):
+        traj = batch.rollout(q0, qd0, forces, BATCH_STEPS, out=out)
+        gq0, gqd0, gf, gm, its = batch.backward(traj[2], weight)
+        grad_e = torch.zeros(batch.count, dtype=torch.float64, device=device)
+        grad_e.index_add_(0, index, gm[:, 0] * dmu_de + gm[:, 1] * dlam_de)
+        return traj, grad_e, its
+
+    traj, grad_e, _ = one()
+    torch.cuda.synchronize()
+    flush.fill_(1.0)
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0.record(stream)
+    traj = batch.rollout(q0, qd0, forces, BATCH_STEPS, out=traj)
+    e1.record(stream)
+    gq0, gqd0, gf, gm, adjoint_its = batch.backward(traj[2], weight)
+    e2.record(stream)
+    torch.cuda.synchronize()
+    fwd_ms, adj_ms = e0.elapsed_time(e1), e1.elapsed_time(e2)
+    status, forward_its = batch.read()
+    batched_ms = fwd_ms + adj_ms
+    final = batch.split(traj[0][-1])
+    converged = (status & 1) == 0
+    errs = [float((a.double() - b.double()).abs().max() / b.double().abs().max()) for a, b in zip(final, plain_final)]
+    err = max(e for e, ok in zip(errs, converged) if ok)
+    # End to end through the public API with host buffers (pinned in, dL/dE out).
+    host = {k: v.cpu().pin_memory() for k, v in (("q0", q0), ("forces", forces), ("weight", weight))}
+    out_grad = torch.empty(batch.count, dtype=torch.float64).pin_memory()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    q0_d = host["q0"].to(device, non_blocking=True)
+    forces_d = host["forces"].to(device, non_blocking=True)
+    weight_d = host["weight"].to(device, non_blocking=True)
+    traj_e = batch.rollout(q0_d, torch.zeros_like(q0_d), forces_d, BATCH_STEPS, out=traj)
+    r = batch.backward(traj_e[2], weight_d)
+    grad_e = torch.zeros(batch.count, dtype=torch.float64, device=device)
+    grad_e.index_add_(0, index, r[3][:, 0] * dmu_de + r[3][:, 1] * dlam_de)
+    out_grad.copy_(grad_e, non_blocking=True)
+    end.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = start.elapsed_time(end)
+    steps_total = batch.count * BATCH_STEPS
+    return {
+        "workload": BATCH_WORKLOAD,
+        "metric": "instance PD steps/s (forward + adjoint w.r.t. every instance's E)",
+        "value": steps_total / (batched_ms / 1000.0),
+        "plain_value": steps_total / (plain_ms / 1000.0),
+        "batched_vs_plain": plain_ms / batched_ms,
+        "e2e": {"value": steps_total / (e2e_ms / 1000.0), "h2d_bytes_per_step": int(sum(v.numel() * v.element_size()
+                                                                                         for v in host.values())),
+                "d2h_bytes_per_step": int(out_grad.numel() * 8)},
+        "forward_ms": fwd_ms,
+        "adjoint_ms": adj_ms,
+        "plain_ms": plain_ms,
+        "precision": precision,
+        "schedule": "teams",
+        "instances": batch.count,
+        "particles": int(batch.particle_count),
+        "team_sizes": {str(int(k)): int(v) for k, v in zip(*np.unique(sizes, return_counts=True))},
+        "grid_blocks": int(grid),
+        "forward_iterations": int(forward_its.sum()),
+        "adjoint_iterations": int(adjoint_its.sum()),
+        "max_iterations_per_step": 5000,
+        "instances_hitting_max_iterations": int(np.count_nonzero(status & 1)),
+        "max_rel_position_err_vs_plain_same_precision": err,
+        "err_note": "final positions, instances that converged within the iteration limit in every step; both paths "
+                    "stop at rel 1e-6, so they differ by the stopping rule (the fixed point itself equals FP64's, "
+                    "tests/test_gpu_batch.py)",
+        "gpu_launches_per_rollout": 2,
+        "data": "synthetic (cantilever_family(256, seed=0): nx uniform [4,40], ny=nz=max(2,nx//4), E log-uniform "
+                "[1e5,1e7] Pa, nu uniform [0.3,0.45], tip +X forces uniform [0,50] N)",
+    }
 
 
 def cpu_sample(steps, threads):
@@ -452,6 +607,7 @@ def main():
     parser.add_argument("--adjoint", choices=["reference", "exact"], default="exact")
     parser.add_argument("--precision", choices=["fp64", "fp32+refine"], default="fp64")
     parser.add_argument("--cpu-seconds", type=float, default=20.0)
+    parser.add_argument("--no-batched", action="store_true", help="skip the batched-vs-plain cantilever family leg")
     parser.add_argument("--no-extras", action="store_true",
                         help="skip the e2e, CPU-baseline and per-launch timing legs (profiling runs)")
     args = parser.parse_args()
