@@ -262,6 +262,10 @@ int pd_batch_backward(PdBatch* batch, int32_t steps, double dt, const double* x_
    and adjoint rollout started and ended on its lane (teams schedule). Either
    pointer may be NULL. Synchronises. */
 int pd_batch_timeline(PdBatch* batch, uint64_t* forward, uint64_t* adjoint, void* stream);
+/* Phase timers of one instance's forward steps in the teams schedule: device
+   uint64 [8] accumulating global-timer nanoseconds per phase, written only by
+   builds compiled with -DPD_PHASE_TIMERS (as pd_set_phase_timers). */
+int pd_batch_set_phase_timers(PdBatch* batch, int32_t instance, unsigned long long* device_timers);
 /* Team size of every instance (0 under the phases schedule) and the grid of the team launch. */
 int pd_batch_team_sizes(const PdBatch* batch, int32_t* sizes, int32_t* grid);
 /* The same rollout without a graph: every kernel launched on its own, the

@@ -651,7 +651,7 @@ __device__ __forceinline__ bool adjoint_step_body(const AdjointArgs& b, const Te
         if (!clip && b.window > 0) {
           const int entries = count * (count + 1) / 2 + count;
           reduce_partials(b.partials, kSlotGram, entries, team.size, s_reduced, s_scratch);
-          if (threadIdx.x == 0) aa_solve(b.aa_state, b.aa_gamma, b.aa_accept, s_reduced, b.window);
+          if (threadIdx.x == 0) aa_solve(b.aa_state, b.aa_gamma, b.aa_accept, s_reduced, b.window, s_scratch);
         }
         barrier_release(b.barrier, generation, team.size);
         __syncthreads();
@@ -685,7 +685,7 @@ __device__ __forceinline__ bool adjoint_step_body(const AdjointArgs& b, const Te
         if (b.window > 0) {
           const int entries = count * (count + 1) / 2 + count;
           reduce_partials(b.partials, kSlotGram, entries, team.size, s_reduced, s_scratch);
-          if (threadIdx.x == 0) aa_solve(b.aa_state, b.aa_gamma, b.aa_accept, s_reduced, b.window);
+          if (threadIdx.x == 0) aa_solve(b.aa_state, b.aa_gamma, b.aa_accept, s_reduced, b.window, s_scratch);
           __syncthreads();
         }
         reduce_partials(b.partials, kSlotStep, 1, team.size, s_reduced, s_scratch);

@@ -518,7 +518,7 @@ __global__ void __launch_bounds__(kBlock) batch_anderson_kernel(const BatchInsta
           for (int i = 0; i < count; ++i) reduced[entry++] = s_out[kMaxWindow + i];
         }
         int accept = 0;
-        aa_solve(a.aa_state, s_gamma, &accept, reduced, window);
+        aa_solve(a.aa_state, s_gamma, &accept, reduced, window, s_scratch);
         s_ctl[0] = accept;
         s_ctl[1] = a.aa_state[2];
         s_ctl[2] = a.aa_state[3];
@@ -684,6 +684,8 @@ struct PdBatch {
       d_particle_offset, d_element_offset, d_class_head, d_lane_slot, d_barriers, d_team_status, d_adjoint_log,
       d_timeline;
   int team_blocks = 0, lanes = 0, classes = 0, solo_class = -1;
+  unsigned long long* timers = nullptr;  // phase timers of one instance (PD_PHASE_TIMERS builds)
+  int timer_instance = -1;
   size_t team_smem = 0;
   cudaStream_t capture = nullptr;  // private stream the rollout graphs are captured on
   cudaGraphExec_t adjoint_exec = nullptr;
@@ -1315,6 +1317,8 @@ pdb200::TeamLaunch team_launch(const PdBatch* b, int steps, double dt, const dou
   launch.lane_barrier = b->d_barriers.as<pdb200::GridBarrier>();
   launch.status = b->d_team_status.as<int>();
   launch.particles = b->particle_offsets.back();
+  launch.timers = b->timers;
+  launch.timer_instance = b->timer_instance;
   return launch;
 }
 
@@ -1576,5 +1580,16 @@ extern "C" int pd_batch_timeline(PdBatch* batch, uint64_t* forward, uint64_t* ad
   if (forward != nullptr) PD_CUDA(cudaMemcpyAsync(forward, base, half, cudaMemcpyDeviceToHost, st));
   if (adjoint != nullptr) PD_CUDA(cudaMemcpyAsync(adjoint, base + half, half, cudaMemcpyDeviceToHost, st));
   PD_CUDA(cudaStreamSynchronize(st));
+  return PD_OK;
+}
+
+extern "C" int pd_batch_set_phase_timers(PdBatch* batch, int32_t instance, unsigned long long* device_timers) {
+  if (batch == nullptr) return pd_set_error(PD_ERR_INVALID, "null batch");
+  batch->timers = device_timers;
+  batch->timer_instance = instance;
+  if (batch->exec != nullptr) {  // the captured launch holds the old setting
+    cudaGraphExecDestroy(batch->exec);
+    batch->exec = nullptr;
+  }
   return PD_OK;
 }

@@ -250,6 +250,12 @@ struct SpmvPlan {
   int smem_offset;      // byte offset of this product's slice in dynamic shared memory (resident plans)
   int max_nnz;          // largest per-block nnz (slice layout size)
   int max_rows;         // largest per-block row count
+  // Streaming layout for plans that are not resident: every row padded to a
+  // multiple of four entries (zero values), so a lane moves four entries per
+  // 16-byte load of columns and of values. Row r covers groups [off4[r], off4[r+1]).
+  const int* off4;      // [rows + 1]
+  const int4* col4;     // [groups]
+  const void* val4;     // [groups][4] values in the factor precision
 };
 
 // Shared-memory layout of one resident slice: values, columns, relative row

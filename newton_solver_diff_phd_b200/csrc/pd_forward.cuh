@@ -319,6 +319,87 @@ __device__ __forceinline__ void stage_vector(const double* vec, double* smem_vec
   __syncthreads();
 }
 
+// Four consecutive padded entries of a streamed row.
+template <typename TV>
+struct Group4;
+template <>
+struct Group4<float> {
+  float v[4];
+  __device__ __forceinline__ void load(const void* base, int g) {
+    const float4 q = __ldg(reinterpret_cast<const float4*>(base) + g);
+    v[0] = q.x;
+    v[1] = q.y;
+    v[2] = q.z;
+    v[3] = q.w;
+  }
+};
+template <>
+struct Group4<double> {
+  double v[4];
+  __device__ __forceinline__ void load(const void* base, int g) {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(base) + 2 * g);
+    const double2 b = __ldg(reinterpret_cast<const double2*>(base) + 2 * g + 1);
+    v[0] = a.x;
+    v[1] = a.y;
+    v[2] = b.x;
+    v[3] = b.y;
+  }
+};
+
+template <typename TV>
+__device__ __forceinline__ void group_fma(const Group4<TV>& values, const int4 cols, const double* vec, double& sx,
+                                          double& sy, double& sz) {
+  const int c[4] = {cols.x, cols.y, cols.z, cols.w};
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const double value = static_cast<double>(values.v[k]);
+    sx += value * vec[3 * c[k]];
+    sy += value * vec[3 * c[k] + 1];
+    sz += value * vec[3 * c[k] + 2];
+  }
+}
+
+// out = M vec over the padded streaming layout (plans that are not resident):
+// the same row-to-unit assignment as the resident path, four entries per
+// 16-byte load, eight groups in flight per lane of a long row.
+template <typename TV>
+__device__ void spmv_block_streamed(const SpmvPlan& plan, const double* vec, double* out, const int* rowlist, int nshort,
+                                    int rows) {
+  for (int t = threadIdx.x; t < nshort; t += blockDim.x) {
+    const int r = rowlist[t];
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    for (int g = plan.off4[r]; g < plan.off4[r + 1]; ++g) {
+      Group4<TV> values;
+      values.load(plan.val4, g);
+      group_fma<TV>(values, __ldg(plan.col4 + g), vec, sx, sy, sz);
+    }
+    out[3 * r] = sx;
+    out[3 * r + 1] = sy;
+    out[3 * r + 2] = sz;
+  }
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  for (int w = nshort + warp; w < rows; w += kWarps) {
+    const int r = rowlist[w];
+    const int begin = plan.off4[r], end = plan.off4[r + 1];
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+#pragma unroll 8
+    for (int g = begin + lane; g < end; g += 32) {
+      Group4<TV> values;
+      values.load(plan.val4, g);
+      group_fma<TV>(values, __ldg(plan.col4 + g), vec, sx, sy, sz);
+    }
+    sx = warp_sum(sx);
+    sy = warp_sum(sy);
+    sz = warp_sum(sz);
+    if (lane == 0) {
+      out[3 * r] = sx;
+      out[3 * r + 1] = sy;
+      out[3 * r + 2] = sz;
+    }
+  }
+}
+
 // out = M vec for this block's rows of one product. Short rows (<= 32 nnz)
 // are summed sequentially by one thread, long rows by one warp (lane-strided,
 // fixed shuffle tree); each row always by the same unit, so the result is
@@ -344,6 +425,10 @@ __device__ void spmv_block(const SpmvPlan& plan, const TV* global_values, bool r
     rowlist = off + align16((plan.max_rows + 1) * 4) / 4;
     row_shift = r0;
   } else {
+    if (plan.off4 != nullptr) {
+      spmv_block_streamed<TV>(plan, vec, out, plan.rowlist + r0, nshort, rows);
+      return;
+    }
     val = global_values;
     col = plan.col;
     off = plan.off;
@@ -459,8 +544,11 @@ inline __device__ void gram_partials(const StepArgs& a, int r0, int r1, int coun
 }
 
 // Eigen-style pivoted LDL^T solve of the leading n x n block (anderson.py:357-407).
-inline __device__ void aa_ldlt_solve(double m[kMaxWindow][kMaxWindow], const double* b, int n, double* x) {
-  int perm[kMaxWindow];
+// m, y and perm live in shared memory (work): dynamic indexing of local arrays
+// would put them in local memory, a global-latency round trip per access.
+inline __device__ void aa_ldlt_solve(double (*m)[kMaxWindow], const double* b, int n, double* x, double* work) {
+  double* y = work;
+  int* perm = reinterpret_cast<int*>(work + kMaxWindow);
   for (int i = 0; i < n; ++i) perm[i] = i;
   for (int k = 0; k < n; ++k) {
     int biggest = k;
@@ -487,7 +575,6 @@ inline __device__ void aa_ldlt_solve(double m[kMaxWindow][kMaxWindow], const dou
       if (m[k][k] != 0.0) m[i][k] = m[i][k] / m[k][k];
     }
   }
-  double y[kMaxWindow];
   for (int i = 0; i < n; ++i) y[i] = b[perm[i]];
   for (int i = 0; i < n; ++i)
     for (int j = 0; j < i; ++j) y[i] = y[i] - m[i][j] * y[j];
@@ -500,7 +587,9 @@ inline __device__ void aa_ldlt_solve(double m[kMaxWindow][kMaxWindow], const dou
 }
 
 // Serial Anderson step (one thread) from the reduced Gram entries (anderson.py:424-475).
-inline __device__ void aa_solve(int* state, double* gamma, int* accept, const double* reduced, int window) {
+// work: shared memory of at least 2 * kMaxWindow * kMaxWindow doubles.
+inline __device__ void aa_solve(int* state, double* gamma, int* accept, const double* reduced, int window,
+                                double* work) {
   int count = state[0];
   int start = state[1];
   const int capacity = window + 1;
@@ -508,8 +597,9 @@ inline __device__ void aa_solve(int* state, double* gamma, int* accept, const do
   state[3] = start;
   *accept = 0;
   if (count >= 1) {
-    double gram[kMaxWindow][kMaxWindow];
-    double rhs[kMaxWindow];
+    double (*gram)[kMaxWindow] = reinterpret_cast<double (*)[kMaxWindow]>(work);
+    double* rhs = work + kMaxWindow * kMaxWindow;
+    double* coefficients = rhs + kMaxWindow;
     const int pairs = count * (count + 1) / 2;
     int entry = 0;
     for (int i = 0; i < count; ++i)
@@ -522,8 +612,7 @@ inline __device__ void aa_solve(int* state, double* gamma, int* accept, const do
     }
     const double regularization = fmax(1.0e-6 * trace / static_cast<double>(count), 1.0e-12);
     for (int i = 0; i < count; ++i) gram[i][i] = gram[i][i] + regularization;
-    double coefficients[kMaxWindow];
-    aa_ldlt_solve(gram, rhs, count, coefficients);
+    aa_ldlt_solve(gram, rhs, count, coefficients, coefficients + kMaxWindow);
     double norm = 0.0;
     for (int i = 0; i < count; ++i) {
       gamma[i] = coefficients[i];

@@ -5,12 +5,12 @@
 #include "pd_kernels.h"
 #include "pd_team.cuh"
 
-// Phase timers of the persistent loop (block 0, thread 0), compiled in only
+// Phase timers of the persistent loop (rank 0 of the team, thread 0), compiled in only
 // with -DPD_PHASE_TIMERS; the timing probe builds such a variant.
 #ifdef PD_PHASE_TIMERS
 #define PD_TIMER(slot)                                                              \
   do {                                                                             \
-    if (blockIdx.x == 0 && threadIdx.x == 0 && a.timers != nullptr) {             \
+    if (team.rank == 0 && threadIdx.x == 0 && a.timers != nullptr) {              \
       unsigned long long now_;                                                     \
       asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now_));                     \
       a.timers[slot] += now_ - timer_last_;                                        \
@@ -19,7 +19,7 @@
   } while (0)
 #define PD_TIMER_START()                                                           \
   unsigned long long timer_last_ = 0;                                              \
-  if (blockIdx.x == 0 && threadIdx.x == 0) asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(timer_last_))
+  if (team.rank == 0 && threadIdx.x == 0) asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(timer_last_))
 #else
 #define PD_TIMER(slot) \
   do {                 \
@@ -287,7 +287,7 @@ __device__ __forceinline__ bool forward_step_body(const StepArgs& a, const Team 
       if (barrier_arrive(a.barrier, generation, team.size)) {
         const int entries = gram_entries(count);
         reduce_partials(a.partials, 0, entries, team.size, s_reduced, s_scratch);
-        if (threadIdx.x == 0) aa_solve(a.aa_state, a.aa_gamma, a.aa_accept, s_reduced, a.window);
+        if (threadIdx.x == 0) aa_solve(a.aa_state, a.aa_gamma, a.aa_accept, s_reduced, a.window, s_scratch);
         barrier_release(a.barrier, generation, team.size);
         __syncthreads();
       } else if (!barrier_wait(a.barrier, generation, a.status)) {
@@ -401,6 +401,7 @@ __global__ void __launch_bounds__(kBlock, 2) team_forward_kernel(const TeamLaunc
         s_args.x_record = launch.x_record != nullptr ? launch.x_record + t * step_elements + offset : nullptr;
         s_args.dt = launch.dt;
         for (int c = 0; c < 3; ++c) s_args.gravity[c] = launch.gravity[c];
+        s_args.timers = instance == launch.timer_instance ? launch.timers : nullptr;
       }
       __syncthreads();
       if (!forward_step_body<TL, TV>(s_args, team, dyn_smem)) return;

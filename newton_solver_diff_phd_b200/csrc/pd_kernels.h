@@ -118,6 +118,8 @@ struct TeamLaunch {
   int* status;                      // launch-wide status (a lane barrier that gave up)
   int* iteration_log;               // [steps][count]
   unsigned long long* timeline;     // [count][2] global-timer start and end of each instance's rollout, or nullptr
+  unsigned long long* timers;       // phase timers of one instance (builds with PD_PHASE_TIMERS), or nullptr
+  int timer_instance;
   // Forward rollout: concatenated [P][3] states.
   const void* q0;
   const void* qd0;

@@ -410,6 +410,49 @@ int pd_plan_launch(PdSolver* s, int blocks, int budget) {
   fill_plan(s->plan_s, s->d_s_off, s->d_s_col, s->d_s_val, s->d_s_val32, s->d_s_part, s->d_s_rowlist, s->d_s_nshort);
   fill_plan(s->plan_st, s->d_st_off, s->d_st_col, s->d_st_val, s->d_st_val32, s->d_st_part, s->d_st_rowlist,
             s->d_st_nshort);
+  // Streaming layouts for a factor that stays in global memory.
+  auto pad = [&](const pdb200::Csr& csr, pdb200::SpmvPlan& plan, DeviceBuffer& off4, DeviceBuffer& col4,
+                 DeviceBuffer& val4) -> int {
+    if (s->resident) {
+      off4.release();
+      col4.release();
+      val4.release();
+      plan.off4 = nullptr;
+      plan.col4 = nullptr;
+      plan.val4 = nullptr;
+      return PD_OK;
+    }
+    const int rows = static_cast<int>(csr.offsets.size()) - 1;
+    std::vector<int32_t> offsets(rows + 1, 0);
+    for (int r = 0; r < rows; ++r) offsets[r + 1] = offsets[r] + (csr.offsets[r + 1] - csr.offsets[r] + 3) / 4;
+    const size_t groups = static_cast<size_t>(offsets[rows]);
+    std::vector<int32_t> columns(4 * groups, 0);
+    std::vector<double> values(4 * groups, 0.0);
+    for (int r = 0; r < rows; ++r) {
+      size_t slot = 4 * static_cast<size_t>(offsets[r]);
+      for (int k = csr.offsets[r]; k < csr.offsets[r + 1]; ++k, ++slot) {
+        columns[slot] = csr.columns[k];
+        values[slot] = csr.values[k];
+      }
+      // Padding entries repeat the row's last column with a zero value.
+      const int32_t last = csr.offsets[r + 1] > csr.offsets[r] ? csr.columns[csr.offsets[r + 1] - 1] : 0;
+      for (; slot < 4 * static_cast<size_t>(offsets[r + 1]); ++slot) columns[slot] = last;
+    }
+    PD_CUDA(off4.upload(offsets));
+    PD_CUDA(col4.upload(columns));
+    if (s->options.precision == PD_PRECISION_FP64) {
+      PD_CUDA(val4.upload(values));
+    } else {
+      std::vector<float> narrow(values.begin(), values.end());
+      PD_CUDA(val4.upload(narrow));
+    }
+    plan.off4 = off4.as<int>();
+    plan.col4 = col4.as<int4>();
+    plan.val4 = val4.ptr;
+    return PD_OK;
+  };
+  if (int status = pad(s->factor.s, s->plan_s, s->d_s_off4, s->d_s_col4, s->d_s_val4)) return status;
+  if (int status = pad(s->factor.st, s->plan_st, s->d_st_off4, s->d_st_col4, s->d_st_val4)) return status;
   PD_CUDA(s->d_partials.allocate(static_cast<size_t>(blocks) * pdb200::kPartialStride * sizeof(double)));
   PD_CUDA(s->b_partials.allocate(static_cast<size_t>(blocks) * pdb200::kPartialStride * sizeof(double)));
   return PD_OK;

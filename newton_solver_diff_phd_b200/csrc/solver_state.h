@@ -118,6 +118,8 @@ struct PdSolver {
   DeviceBuffer d_wc, d_wv, d_wn, d_wm, d_mdir, d_mtarget;
   DeviceBuffer d_s_off, d_s_col, d_s_val, d_s_val32, d_st_off, d_st_col, d_st_val, d_st_val32, d_s_part, d_st_part;
   DeviceBuffer d_a_off, d_a_col, d_a_val;
+  // Padded streaming layouts of S and S^T (plans that are not resident).
+  DeviceBuffer d_s_off4, d_s_col4, d_s_val4, d_st_off4, d_st_col4, d_st_val4;
   // Step vectors.
   DeviceBuffer d_position, d_velocity, d_target, d_boundary, d_x, d_prev, d_proj, d_prev_proj, d_rhs, d_y, d_contrib;
   DeviceBuffer d_hist_x, d_hist_g, d_aa_state, d_aa_gamma, d_aa_accept, d_partials;

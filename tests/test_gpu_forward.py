@@ -235,3 +235,41 @@ def test_rollout_matches_oracle_with_anderson_on_a_larger_block():
         v = state_out.particle_qd.cpu().numpy().astype(np.float64)
         q = q_next
         state_in, state_out = state_out, state_in
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32+refine"])
+def test_streamed_factor_matches_the_resident_one(precision):
+    """A factor left in global memory (padded streaming layout) steps like the
+    one kept in shared memory; the adjoint as well."""
+    from newton_solver_diff_phd_b200 import ModelBuilder, meshes
+
+    results = []
+    for resident in (True, False):
+        builder = ModelBuilder(gravity=(0.0, 0.0, -9.81))
+        builder.add_soft_grid(pos=(0, 0, 0), rot=None, vel=(0, 0, 0), dim_x=8, dim_y=3, dim_z=3, cell_x=0.01,
+                              cell_y=0.01, cell_z=0.01, density=DENSITY, k_mu=1.0, k_lambda=1.0, k_damp=0.0,
+                              fix_left=True)
+        model = builder.finalize("cuda")
+        rng = np.random.default_rng(0)
+        young = np.exp(rng.uniform(np.log(1e5), np.log(1e7), model.tet_count))
+        mu, lam = meshes.lame_from_young(young, 0.4)
+        model.tet_materials.copy_(torch.tensor(np.column_stack((mu, lam, np.zeros_like(mu))), dtype=torch.float32))
+        solver = SolverDiffPhD(model, density=DENSITY, rel_tol=1e-8, abs_tol=1e-12, precision=precision,
+                               resident=resident, adjoint="exact", blocks=4)
+        state_in, state_out = model.state(), model.state()
+        record = torch.zeros((model.particle_count, 3), dtype=torch.float64, device="cuda")
+        iterations = []
+        for _ in range(3):
+            solver.step(state_in, state_out, None, None, 5e-3, record=record)
+            iterations.append(int(solver.iterations[0]))
+            state_in, state_out = state_out, state_in
+        solver.check_status()
+        state_in.requires_grad_(True)
+        state_out.requires_grad_(True)
+        state_in.particle_q.grad.normal_(generator=torch.Generator(device="cuda").manual_seed(3))
+        solver.backward_step(record, 5e-3, state_out, state_in)
+        results.append((solver._x.clone(), iterations, state_out.particle_q.grad.clone()))
+    (x_r, it_r, g_r), (x_s, it_s, g_s) = results
+    assert max(abs(a - b) for a, b in zip(it_r, it_s)) <= 1
+    assert float((x_r - x_s).abs().max()) <= 1e-7 * float(x_r.abs().max())
+    assert float((g_r - g_s).abs().max()) <= 1e-5 * float(g_r.abs().max())
