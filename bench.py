@@ -82,7 +82,9 @@ def build_model(device):
 
 
 def algorithmic_bytes_per_iteration(n, elements, nnz_s, corners=4, window=5, value_bytes=8):
-    """Bytes one local/global iteration must move (SURVEY 8(d) B_iter with b = value bytes)."""
+    """Bytes one local/global iteration must move: factor values and indices of S and S^T, the vectors
+    around the two products, element contributions, the Anderson history and the convergence norms
+    (b = value bytes)."""
     b = value_bytes
     return (2 * (nnz_s * (b + 4) + 4 * (n + 1)) + 2 * (3 * n * b) * 2 + elements * corners * 4 + 3 * elements * 8
             + 3 * n * b + 3 * n * b + (2 * window + 4) * 3 * n * b + 4 * 3 * n * b)

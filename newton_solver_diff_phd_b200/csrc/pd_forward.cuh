@@ -368,6 +368,7 @@ __device__ void spmv_block_streamed(const SpmvPlan& plan, const double* vec, dou
   for (int t = threadIdx.x; t < nshort; t += blockDim.x) {
     const int r = rowlist[t];
     double sx = 0.0, sy = 0.0, sz = 0.0;
+#pragma unroll 4
     for (int g = plan.off4[r]; g < plan.off4[r + 1]; ++g) {
       Group4<TV> values;
       values.load(plan.val4, g);
