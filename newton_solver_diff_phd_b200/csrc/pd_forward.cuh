@@ -378,22 +378,31 @@ __device__ void spmv_block_streamed(const SpmvPlan& plan, const double* vec, dou
     out[3 * r + 1] = sy;
     out[3 * r + 2] = sz;
   }
-  const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
-  for (int w = nshort + warp; w < rows; w += kWarps) {
-    const int r = rowlist[w];
-    const int begin = plan.off4[r], end = plan.off4[r + 1];
+  // Long rows: eight lanes per row, four rows per warp in flight, so a row of
+  // a few hundred entries keeps every lane busy with several loads at once.
+  const int lane = threadIdx.x & 7;
+  const int slot = threadIdx.x >> 3;  // 32 row slots per block
+  const int longs = rows - nshort;
+  for (int base = 0; base < longs; base += kBlock / 8) {
+    const int w = base + slot;
+    const bool valid = w < longs;
+    const int r = valid ? rowlist[nshort + w] : 0;
+    const int begin = valid ? plan.off4[r] : 0;
+    const int end = valid ? plan.off4[r + 1] : 0;
     double sx = 0.0, sy = 0.0, sz = 0.0;
 #pragma unroll 8
-    for (int g = begin + lane; g < end; g += 32) {
+    for (int g = begin + lane; g < end; g += 8) {
       Group4<TV> values;
       values.load(plan.val4, g);
       group_fma<TV>(values, __ldg(plan.col4 + g), vec, sx, sy, sz);
     }
-    sx = warp_sum(sx);
-    sy = warp_sum(sy);
-    sz = warp_sum(sz);
-    if (lane == 0) {
+#pragma unroll
+    for (int offset = 4; offset > 0; offset >>= 1) {
+      sx += __shfl_xor_sync(0xffffffffu, sx, offset);
+      sy += __shfl_xor_sync(0xffffffffu, sy, offset);
+      sz += __shfl_xor_sync(0xffffffffu, sz, offset);
+    }
+    if (valid && lane == 0) {
       out[3 * r] = sx;
       out[3 * r + 1] = sy;
       out[3 * r + 2] = sz;
