@@ -107,6 +107,11 @@ int pd_destroy(PdSolver* solver);
 /* Mutable convergence settings (solver.max_iterations / abs_tol / rel_tol). */
 int pd_set_tolerances(PdSolver* solver, int32_t max_iterations, double abs_tol, double rel_tol);
 
+/* Anderson window (0..8) of the following steps and backward passes; the
+   history grows when needed. The reference fixes it at construction
+   (anderson_window keyword); changing it lets a driver tune it. */
+int pd_set_anderson_window(PdSolver* solver, int32_t window);
+
 /* Lame parameters [mu, lambda] per element (model.tet_materials columns 0-1,
    or hex_materials), float64 host array [n_elements][2]. Marks the factor
    stale (notify_model_changed, solver.py:419-427). */

@@ -96,6 +96,7 @@ SIGNATURES = {
     "pd_create": ([ctypes.POINTER(PdMeshDesc), ctypes.POINTER(PdOptions), ctypes.c_int, ctypes.POINTER(_P)], ctypes.c_int),
     "pd_destroy": ([_P], ctypes.c_int),
     "pd_set_tolerances": ([_P, _I32, _D, _D], ctypes.c_int),
+    "pd_set_anderson_window": ([_P, _I32], ctypes.c_int),
     "pd_set_materials": ([_P, _P], ctypes.c_int),
     "pd_set_muscles": ([_P, _P, _P], ctypes.c_int),
     "pd_set_muscle_targets": ([_P, _P], ctypes.c_int),

@@ -35,7 +35,9 @@ class BatchedSolver:
     Every solver is built for ``dt`` here (as its first ``step`` would). The
     solvers must share device, precision and state dtype, must outlive the
     batch, and must not be stepped on their own while a batched rollout runs.
-    Dirichlet targets and Tet4 muscle activations are not supported.
+    A new batch over the same solvers re-plans them: only the newest batch of
+    a set of solvers may be used. Dirichlet targets and Tet4 muscle
+    activations are not supported.
 
     ``schedule="teams"`` (default) runs each instance's whole rollout on a
     team of blocks of one persistent launch, with the single-instance step
@@ -227,3 +229,52 @@ class BatchedSolver:
             except Exception:
                 pass
             self._handle = None
+
+
+def _time_forward(batch, q0, qd0, forces, steps):
+    out = batch.rollout(q0, qd0, forces, steps)
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    batch.rollout(q0, qd0, forces, steps, out=out)
+    end.record()
+    torch.cuda.synchronize()
+    return start.elapsed_time(end)
+
+
+def autotune(solvers, dt, q0, qd0, forces, *, steps: int = 2, windows=(3, 5, 8),
+             teams=((65536, 512), (32768, 256), (131072, 1024)), **options):
+    """Pick the Anderson window and the team sizing of a batch from short rollouts.
+
+    Times a ``steps``-step forward rollout of the batch for every window (with
+    the first team sizing), then for every other team sizing with the best
+    window, and returns ``(BatchedSolver, report)`` built with the fastest
+    setting (the solvers keep its window). ``q0``, ``qd0``, ``forces`` are the
+    concatenated rollout inputs; the probe runs the rollout's first steps.
+    """
+    report = []
+    best = None
+
+    def probe(window, team_nnz, team_samples):
+        nonlocal best
+        for solver in solvers:
+            if solver.anderson_window != window:
+                solver.set_anderson_window(window)
+        batch = BatchedSolver(solvers, dt, team_nnz=team_nnz, team_samples=team_samples, **options)
+        ms = _time_forward(batch, q0, qd0, forces, steps)
+        report.append({"window": window, "team_nnz": team_nnz, "team_samples": team_samples, "ms": ms})
+        if best is None or ms < best[0]:
+            best = (ms, window, team_nnz, team_samples)
+        del batch
+
+    for window in windows:
+        probe(window, *teams[0])
+    for team_nnz, team_samples in teams[1:]:
+        probe(best[1], team_nnz, team_samples)
+    _, window, team_nnz, team_samples = best
+    for solver in solvers:
+        if solver.anderson_window != window:
+            solver.set_anderson_window(window)
+    batch = BatchedSolver(solvers, dt, team_nnz=team_nnz, team_samples=team_samples, **options)
+    return batch, {"chosen": {"window": window, "team_nnz": team_nnz, "team_samples": team_samples},
+                   "probes": report, "probe_steps": steps}

@@ -411,7 +411,7 @@ __device__ void spmv_block_streamed(const SpmvPlan& plan, const double* vec, dou
 }
 
 // out = M vec for this block's rows of one product. Short rows (<= 32 nnz)
-// are summed sequentially by one thread, long rows by one warp (lane-strided,
+// are summed sequentially by one thread, long rows by eight lanes (lane-strided,
 // fixed shuffle tree); each row always by the same unit, so the result is
 // bitwise reproducible. Slice data comes from shared memory when resident.
 template <typename TV>
@@ -461,26 +461,33 @@ __device__ void spmv_block(const SpmvPlan& plan, const TV* global_values, bool r
     out[3 * row + 1] = sy;
     out[3 * row + 2] = sz;
   }
-  const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
-  for (int w = nshort + warp; w < rows; w += kWarps) {
-    const int r = rowlist[w];
-    const int begin = off[r], end = off[r + 1];
+  // Long rows: eight lanes per row, four rows per warp at once (lane-strided
+  // entries, fixed three-level shuffle tree).
+  const int lane = threadIdx.x & 7;
+  const int slot = threadIdx.x >> 3;
+  const int longs = rows - nshort;
+  for (int base = 0; base < longs; base += kBlock / 8) {
+    const int w = base + slot;
+    const bool valid = w < longs;
+    const int r = valid ? rowlist[nshort + w] : 0;
+    const int begin = valid ? off[r] : 0;
+    const int end = valid ? off[r + 1] : 0;
     double sx = 0.0, sy = 0.0, sz = 0.0;
-    // Eight entries per lane in flight: enough independent loads to cover
-    // the latency of a factor streamed from L2 or HBM.
 #pragma unroll 8
-    for (int k = begin + lane; k < end; k += 32) {
+    for (int k = begin + lane; k < end; k += 8) {
       const double value = static_cast<double>(val[k]);
       const int c = col[k];
       sx += value * vec[3 * c];
       sy += value * vec[3 * c + 1];
       sz += value * vec[3 * c + 2];
     }
-    sx = warp_sum(sx);
-    sy = warp_sum(sy);
-    sz = warp_sum(sz);
-    if (lane == 0) {
+#pragma unroll
+    for (int offset = 4; offset > 0; offset >>= 1) {
+      sx += __shfl_xor_sync(0xffffffffu, sx, offset);
+      sy += __shfl_xor_sync(0xffffffffu, sy, offset);
+      sz += __shfl_xor_sync(0xffffffffu, sz, offset);
+    }
+    if (valid && lane == 0) {
       const int row = r + row_shift;
       out[3 * row] = sx;
       out[3 * row + 1] = sy;

@@ -280,6 +280,26 @@ int pd_set_tolerances(PdSolver* solver, int32_t max_iterations, double abs_tol, 
   return PD_OK;
 }
 
+int pd_set_anderson_window(PdSolver* solver, int32_t window) {
+  if (solver == nullptr) return fail(PD_ERR_INVALID, "null solver");
+  PdOptions o = solver->options;
+  o.anderson_window = window;
+  if (int status = validate_options(o)) return status;
+  PD_CUDA(cudaSetDevice(solver->device));
+  const size_t vec = static_cast<size_t>(3) * solver->n * sizeof(double);
+  const size_t need = (static_cast<size_t>(window) + 1) * vec;
+  if (solver->d_hist_x.bytes < need) {
+    PD_CUDA(solver->d_hist_x.allocate(need));
+    PD_CUDA(solver->d_hist_g.allocate(need));
+  }
+  if (solver->b_hist_x.ptr != nullptr && solver->b_hist_x.bytes < need) {
+    PD_CUDA(solver->b_hist_x.allocate(need));
+    PD_CUDA(solver->b_hist_g.allocate(need));
+  }
+  solver->options = o;
+  return PD_OK;
+}
+
 int pd_set_materials(PdSolver* solver, const double* mu_lambda) {
   if (solver == nullptr || mu_lambda == nullptr) return fail(PD_ERR_INVALID, "null argument");
   solver->mu.resize(solver->ne);

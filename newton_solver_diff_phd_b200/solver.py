@@ -451,6 +451,13 @@ class SolverDiffPhD:
         self._factor_key = dt
         self._model_changed = False
 
+    def set_anderson_window(self, window: int) -> None:
+        """Change the Anderson window (0..8) of the following steps and backward passes (added)."""
+        if int(window) != window or not 0 <= window <= MAX_WINDOW:
+            raise ValueError(f"anderson_window must be an integer in [0, {MAX_WINDOW}]")
+        _lib.check(self._lib.pd_set_anderson_window(self._handle, int(window)))
+        self.anderson_window = int(window)
+
     def notify_model_changed(self, flags: int = 0) -> None:
         """Rebuild the material weights and inverse factor before the next step."""
         if torch.cuda.is_current_stream_capturing():

@@ -244,3 +244,42 @@ def test_batched_adjoint_matches_single_instance_rollouts(precision):
                           (batch.split(gf)[i], rf), (gm[eo[i]:eo[i + 1]], rm)):
             scale = float(want.abs().max())
             assert float((got - want).abs().max()) <= 1e-5 * scale + 1e-30, (i, float((got - want).abs().max()), scale)
+
+
+def test_anderson_window_can_change_after_construction():
+    """A solver switched to window 8 steps exactly like one built with it."""
+    results = []
+    for switch in (False, True):
+        spec = _specs()[2]
+        model, mesh, materials, forces = cantilever_model(spec)
+        solver = SolverDiffPhD(model, density=1000.0, hex_mesh=mesh, hex_materials=materials,
+                               anderson_window=3 if switch else 8, rel_tol=1e-6, abs_tol=1e-9)
+        if switch:
+            solver.set_anderson_window(8)
+        results.append(_plain(model, solver, torch.as_tensor(forces, device="cuda")))
+    assert torch.equal(results[0][0], results[1][0])
+    assert results[0][1] == results[1][1]
+    with pytest.raises(ValueError):
+        solver.set_anderson_window(9)
+
+
+def test_autotune_picks_a_probed_setting():
+    from newton_solver_diff_phd_b200.batch import autotune
+
+    instances = _instances("fp32+refine")
+    solvers = [s for _, s, _ in instances]
+    probe = BatchedSolver(solvers, DT)
+    q0 = probe.concat([m.particle_q for m, _, _ in instances])
+    forces = probe.concat([f for _, _, f in instances])
+    del probe
+    batch, report = autotune(solvers, DT, q0, torch.zeros_like(q0), forces, steps=1, windows=(3, 5),
+                             teams=((65536, 512), (2048, 64)))
+    assert len(report["probes"]) == 3
+    chosen = report["chosen"]
+    assert chosen["window"] in (3, 5) and all(s.anderson_window == chosen["window"] for s in solvers)
+    assert min(p["ms"] for p in report["probes"]) == [p["ms"] for p in report["probes"]
+                                                      if (p["window"], p["team_nnz"]) == (chosen["window"],
+                                                                                          chosen["team_nnz"])][0]
+    q, qd, x = batch.rollout(q0, torch.zeros_like(q0), forces, STEPS)
+    status, _ = batch.read()
+    assert np.all(status == 0)
