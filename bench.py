@@ -416,7 +416,7 @@ def run_batched(args, device):
     import torch
 
     from newton_solver_diff_phd_b200 import meshes
-    from newton_solver_diff_phd_b200.batch import BatchedSolver
+    from newton_solver_diff_phd_b200.batch import autotune
     from newton_solver_diff_phd_b200.rollout import Rollout
 
     precision = "fp32+refine"
@@ -425,7 +425,8 @@ def run_batched(args, device):
     rng = np.random.default_rng(1)
     weights = [torch.as_tensor(rng.standard_normal((m.particle_count, 3)), dtype=torch.float32, device=device)
                for _, m, _, _ in family]
-    # Plain path: every instance on its own, one cooperative launch per step (untouched plans).
+    # Plain path: every instance on its own, one cooperative launch per step
+    # (default plans, Anderson window 5).
     stream = torch.cuda.current_stream()
     plain_ms, plain_final = 0.0, []
     for (spec, model, solver, forces), w in zip(family, weights):
@@ -441,12 +442,13 @@ def run_batched(args, device):
         plain_final.append(final.particle_q.clone())
     for _, _, solver, _ in family:
         solver.read_status()
-    # Batched path.
-    batch = BatchedSolver([s for _, _, s, _ in family], BATCH_DT)
-    sizes, grid = batch.team_sizes()
-    q0 = batch.concat([m.particle_q for _, m, _, _ in family])
+    # Batched path: Anderson window and team sizing chosen by the autotuner
+    # from 6-step probe rollouts (untimed).
+    q0 = torch.cat([m.particle_q for _, m, _, _ in family]).contiguous()
     qd0 = torch.zeros_like(q0)
-    forces = batch.concat([f for _, _, _, f in family])
+    forces = torch.cat([f for _, _, _, f in family]).contiguous()
+    batch, tuning = autotune([s for _, _, s, _ in family], BATCH_DT, q0, qd0, forces, steps=6)
+    sizes, grid = batch.team_sizes()
     weight = batch.concat(weights)
     eo = batch.element_offsets
     nu = torch.tensor(np.repeat([spec.poisson for spec, _, _, _ in family], np.diff(eo)), device=device)
@@ -510,6 +512,8 @@ def run_batched(args, device):
         "plain_ms": plain_ms,
         "precision": precision,
         "schedule": "teams",
+        "autotune": tuning["chosen"],
+        "plain_anderson_window": 5,
         "instances": batch.count,
         "particles": int(batch.particle_count),
         "team_sizes": {str(int(k)): int(v) for k, v in zip(*np.unique(sizes, return_counts=True))},

@@ -411,8 +411,9 @@ __device__ void spmv_block_streamed(const SpmvPlan& plan, const double* vec, dou
 }
 
 // out = M vec for this block's rows of one product. Short rows (<= 32 nnz)
-// are summed sequentially by one thread, long rows by eight lanes (lane-strided,
-// fixed shuffle tree); each row always by the same unit, so the result is
+// are summed sequentially by one thread, long rows by one warp when a block has
+// few of them, else by eight lanes (lane-strided, fixed shuffle trees); each
+// row always by the same unit, so the result is
 // bitwise reproducible. Slice data comes from shared memory when resident.
 template <typename TV>
 __device__ void spmv_block(const SpmvPlan& plan, const TV* global_values, bool resident, const char* smem,
@@ -461,11 +462,37 @@ __device__ void spmv_block(const SpmvPlan& plan, const TV* global_values, bool r
     out[3 * row + 1] = sy;
     out[3 * row + 2] = sz;
   }
-  // Long rows: eight lanes per row, four rows per warp at once (lane-strided
-  // entries, fixed three-level shuffle tree).
+  const int longs = rows - nshort;
+  if (longs <= 4 * kWarps) {
+    // Few long rows: one warp each (lane-strided, fixed shuffle tree).
+    const int lane = threadIdx.x & 31;
+    for (int w = nshort + (threadIdx.x >> 5); w < rows; w += kWarps) {
+      const int r = rowlist[w];
+      double sx = 0.0, sy = 0.0, sz = 0.0;
+#pragma unroll 4
+      for (int k = off[r] + lane; k < off[r + 1]; k += 32) {
+        const double value = static_cast<double>(val[k]);
+        const int c = col[k];
+        sx += value * vec[3 * c];
+        sy += value * vec[3 * c + 1];
+        sz += value * vec[3 * c + 2];
+      }
+      sx = warp_sum(sx);
+      sy = warp_sum(sy);
+      sz = warp_sum(sz);
+      if (lane == 0) {
+        const int row = r + row_shift;
+        out[3 * row] = sx;
+        out[3 * row + 1] = sy;
+        out[3 * row + 2] = sz;
+      }
+    }
+    return;
+  }
+  // Many long rows: eight lanes per row, four rows per warp at once
+  // (lane-strided entries, fixed three-level shuffle tree).
   const int lane = threadIdx.x & 7;
   const int slot = threadIdx.x >> 3;
-  const int longs = rows - nshort;
   for (int base = 0; base < longs; base += kBlock / 8) {
     const int w = base + slot;
     const bool valid = w < longs;
