@@ -135,6 +135,24 @@ int pd_set_activations(PdSolver* solver, const float* device_contractions);
 int pd_set_planar_energies(PdSolver* solver, int32_t count, const int32_t* vertices, const double* stiffness,
                            const double plane[4]);
 
+/* The reference's mesh_contact state force between two bodies
+   (mesh_contact.py:185-272, wired in solver.py:321-325 and :762-770): radius
+   [m], normal stiffness of A's vertices against B's faces (kn_left) and of B's
+   against A's (kn_right) [N/m], friction bound kf [N s/m], Coulomb mu, and the
+   surface triangles [n][3] (particle indices, host arrays) of A and B. Every
+   following step evaluates it on its start-of-step state and adds h^2/m f to
+   the inertial target; it has no gradient, as in the reference. Tet4 only. */
+int pd_set_mesh_contact(PdSolver* solver, double radius, double kn_left, double kn_right, double kf, double mu,
+                        int32_t n_faces_a, const int32_t* faces_a, int32_t n_faces_b, const int32_t* faces_b);
+/* MeshContact.evaluate (mesh_contact.py:253-272) on given float64 device
+   positions and velocities [n][3]: force (device float64 [n][3], or NULL)
+   and the number of vertex-face pairs within the radius (host, or NULL;
+   synchronises). */
+int pd_mesh_contact_force(PdSolver* solver, const double* q, const double* v, double* force, int32_t* pairs,
+                          void* stream);
+/* Pairs within the radius at the last step (solver.mesh_contact_pairs, solver.py:351-353). Synchronises. */
+int pd_mesh_contact_pairs(PdSolver* solver, int32_t* pairs, void* stream);
+
 /* SolverDiffPhD._build (solver.py:491-552): assembles the constant matrix
    A = m/h^2 I + sum_e w_e Vbar G_e^T G_e (+ fibres, + plane diagonal) and builds
    the exact inverse factor A^{-1} = S^T S on the host (sparse.py:291-320),

@@ -102,6 +102,9 @@ SIGNATURES = {
     "pd_set_muscle_targets": ([_P, _P], ctypes.c_int),
     "pd_set_activations": ([_P, _P], ctypes.c_int),
     "pd_set_planar_energies": ([_P, _I32, _P, _P, _P], ctypes.c_int),
+    "pd_set_mesh_contact": ([_P, _D, _D, _D, _D, _D, _I32, _P, _I32, _P], ctypes.c_int),
+    "pd_mesh_contact_force": ([_P, _P, _P, _P, _P, _P], ctypes.c_int),
+    "pd_mesh_contact_pairs": ([_P, _P, _P], ctypes.c_int),
     "pd_build": ([_P, _D], ctypes.c_int),
     "pd_factor_stats": ([_P, ctypes.POINTER(_I64), ctypes.POINTER(_I64), ctypes.POINTER(_I64)], ctypes.c_int),
     "pd_step": ([_P, _P, _P, _P, _P, _P, _D, _P, _P, _P, _P], ctypes.c_int),

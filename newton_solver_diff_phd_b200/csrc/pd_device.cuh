@@ -286,6 +286,7 @@ struct StepArgs {
   const int* inc_offsets;  // [n+1]
   const int* inc_entries;  // element*corners + corner, element-major order
   const double* plane_weight;  // [n] stiffness of the vertex-plane energy (0: none), or nullptr
+  const double* extra_force;   // [n][3] state force added to the inertial target (mesh contact), or nullptr
   double plane[4];
   // Materials (per element; for Hex8 already multiplied by the sample volume)
   const double* wc;

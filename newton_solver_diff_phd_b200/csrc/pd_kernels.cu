@@ -98,6 +98,11 @@ __device__ __forceinline__ bool forward_step_body(const StepArgs& a, const Team 
     V3<double> target;
 #pragma unroll
     for (int c = 0; c < 3; ++c) target[c] = start[c] + dt * velocity[c] + dt * dt * acceleration[c];
+    if (a.extra_force != nullptr) {
+      // q~ += h^2/m f(q, v) of a state force (the reference's add_state_force).
+#pragma unroll
+      for (int c = 0; c < 3; ++c) target[c] = target[c] + dt * dt / a.mass * a.extra_force[3 * i + c];
+    }
     store3(a.target, i, target);
     V3<double> boundary = v3<double>(0.0, 0.0, 0.0);
     if (a.free_[i] == 0) {

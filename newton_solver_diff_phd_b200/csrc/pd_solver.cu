@@ -768,6 +768,11 @@ int pd_step(PdSolver* s, const void* q, const void* qd, const void* f, const voi
   a.x_record = x_record;
   a.dt = dt;
   for (int c = 0; c < 3; ++c) a.gravity[c] = gravity[c];
+  if (s->has_mesh_contact) {
+    // Evaluated once on the start-of-step state (mesh_contact.py, solver.py:762-770).
+    if (int status = pd_evaluate_mesh_contact(s, q, qd, s->options.state_precision, st)) return status;
+    a.extra_force = s->mc_force.as<double>();
+  }
   PD_CUDA(cudaMemsetAsync(s->d_barrier.ptr, 0, sizeof(pdb200::GridBarrier), st));
   PD_CUDA(pdb200::launch_forward_step(a, s->blocks, s->options.precision, s->smem, st));
   return PD_OK;

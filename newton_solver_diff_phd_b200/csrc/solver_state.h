@@ -32,6 +32,8 @@ int pd_plan_launch(PdSolver* s, int blocks, int budget);
 void fill_step_args(const PdSolver* s, pdb200::StepArgs* a);
 void fill_adjoint_args(const PdSolver* s, pdb200::AdjointArgs* b);
 int pd_ensure_adjoint_buffers(PdSolver* s);
+// The mesh contact force of the state (q, v) into s->mc_force (pd_contact.cu).
+int pd_evaluate_mesh_contact(PdSolver* s, const void* q, const void* v, int f64, cudaStream_t stream);
 }
 
 #define PD_CUDA(call)                                                                                 \
@@ -115,6 +117,15 @@ struct PdSolver {
   InverseFactor factor;
   // Device mesh data.
   DeviceBuffer d_indices, d_gradients, d_free, d_inc_offsets, d_inc_entries, d_plane_weight;
+  // Mesh contact state force between two bodies (mesh_contact.py): parameters
+  // (radius, kn_left, kn_right, kf, mu), surface vertices and faces of A and
+  // B, per-particle slots and (face, corner) incidence, pair buffers.
+  bool has_mesh_contact = false;
+  double mc_params[5] = {0, 0, 0, 0, 0};
+  int mc_va = 0, mc_vb = 0, mc_fa = 0, mc_fb = 0;
+  DeviceBuffer mc_vertices_a, mc_vertices_b, mc_faces_a, mc_faces_b, mc_slot_a, mc_slot_b;
+  DeviceBuffer mc_inc_a_off, mc_inc_a, mc_inc_b_off, mc_inc_b;
+  DeviceBuffer mc_force_ab, mc_bary_ab, mc_force_ba, mc_bary_ba, mc_force, mc_pairs;
   DeviceBuffer d_wc, d_wv, d_wn, d_wm, d_mdir, d_mtarget;
   DeviceBuffer d_s_off, d_s_col, d_s_val, d_s_val32, d_st_off, d_st_col, d_st_val, d_st_val32, d_s_part, d_st_part;
   DeviceBuffer d_a_off, d_a_col, d_a_val;

@@ -126,8 +126,21 @@ class ModelBuilder:
         self.particle_qd.extend([list(map(float, v)) for v in vel])
         self.particle_mass.extend([float(m) for m in mass])
 
+    def add_particle(self, pos, vel, mass, radius=None) -> int:
+        """Add one particle; returns its index."""
+        self.add_particles([pos], [vel], [mass])
+        return self.particle_count - 1
+
+    def add_tetrahedron(self, i, j, k, l, k_mu=1.0e3, k_lambda=1.0e3, k_damp=0.0) -> None:
+        """Add one tetrahedron over existing particles, its rest pose from their current positions."""
+        tet = np.array([[i, j, k, l]], dtype=np.int32)
+        vertices = np.asarray(self.particle_q, dtype=np.float64)
+        self.tet_indices.extend(tet.tolist())
+        self.tet_materials.append([float(k_mu), float(k_lambda), float(k_damp)])
+        self._poses.extend(meshes.tet_rest_poses(vertices, tet))
+
     def add_soft_grid(self, pos, rot, vel, dim_x, dim_y, dim_z, cell_x, cell_y, cell_z, density, k_mu, k_lambda,
-                      k_damp, fix_left=False, fix_right=False):
+                      k_damp, fix_left=False, fix_right=False, fix_bottom=False):
         """Add a Tet4 block of ``dim_x x dim_y x dim_z`` cubes split into five tetrahedra each.
 
         ``rot`` must be the identity; cells may have per-axis sizes.
@@ -146,6 +159,9 @@ class ModelBuilder:
             mass[x == x.min()] = 0.0
         if fix_right:
             mass[x == x.max()] = 0.0
+        if fix_bottom:
+            z = vertices[:, 2]
+            mass[z == z.min()] = 0.0
         self.add_particles(vertices, np.tile(np.asarray(vel, dtype=float), (len(vertices), 1)), mass)
         self.tet_indices.extend((tets + start).tolist())
         self.tet_materials.extend([[float(k_mu), float(k_lambda), float(k_damp)]] * len(tets))

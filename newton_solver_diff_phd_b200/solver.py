@@ -24,8 +24,8 @@ size, 0 = automatic), ``resident`` and ``svd_warm_start`` (kernel tuning).
 ``state_dtype=torch.float64`` (added) keeps particle states and their
 gradients in float64 between steps; the default float32 matches Newton.
 
-Differences from the reference: frictional boundaries and ``mesh_contact`` are
-not available in this build (``NotImplementedError``); gravity is taken from
+Differences from the reference: frictional boundaries are not available in
+this build (``NotImplementedError``; ``mesh_contact`` is); gravity is taken from
 one world; Hex8 steps can be recorded for the backward pass (the reference
 rejects them, ``solver.py:726-729``).
 """
@@ -214,8 +214,18 @@ class SolverDiffPhD:
             raise ValueError("Explicit muscle_targets and planar_energies currently require hex_mesh")
         if hex_mesh is not None and any(x is not None for x in (frictional_boundary, mesh_contact)):
             raise NotImplementedError("Hex8 currently supports planar_energies, not frictional or mesh contact")
-        if frictional_boundary is not None or mesh_contact is not None:
-            raise NotImplementedError("frictional_boundary and mesh_contact are not available in this build")
+        if frictional_boundary is not None:
+            raise NotImplementedError("frictional_boundary is not available in this build")
+        if mesh_contact is not None:
+            if len(mesh_contact) != 7:
+                raise ValueError("mesh_contact is (contact_radius, kn_left, kn_right, kf, mu, faces_a, faces_b)")
+            mesh_faces = []
+            for faces in mesh_contact[5:]:
+                faces = np.ascontiguousarray(np.asarray(faces).reshape(-1, 3), dtype=np.int32)
+                mesh_faces.append(faces)
+            self._mesh_contact_args = (tuple(float(value) for value in mesh_contact[:5]), mesh_faces)
+        else:
+            self._mesh_contact_args = None
         if frictional_vertices is not None or friction or restitution:
             raise ValueError("frictional_vertices, friction and restitution need a frictional_boundary")
         if not np.isfinite(density) or density <= 0:
@@ -351,6 +361,10 @@ class SolverDiffPhD:
             _lib.check(
                 lib.pd_set_planar_energies(handle, len(vertices), _lib.ptr(vertices), _lib.ptr(stiffness), _lib.ptr(plane))
             )
+        if self._mesh_contact_args is not None:
+            (radius, kn_left, kn_right, kf, mu), (faces_a, faces_b) = self._mesh_contact_args
+            _lib.check(lib.pd_set_mesh_contact(handle, radius, kn_left, kn_right, kf, mu, len(faces_a), _lib.ptr(faces_a),
+                                               len(faces_b), _lib.ptr(faces_b)))
         self._x = torch.zeros((self._n, 3), dtype=torch.float64, device=self.device)
         self._factor_key = None
         self._model_changed = True
@@ -450,6 +464,26 @@ class SolverDiffPhD:
         )
         self._factor_key = dt
         self._model_changed = False
+
+    @property
+    def mesh_contact_pairs(self) -> int | None:
+        """Vertex-face pairs within the contact radius in the last step, or None (one host synchronization)."""
+        if self._mesh_contact_args is None:
+            return None
+        pairs = ctypes.c_int32()
+        _lib.check(self._lib.pd_mesh_contact_pairs(self._handle, ctypes.byref(pairs), _stream()))
+        return pairs.value
+
+    def mesh_contact_force(self, positions: torch.Tensor, velocities: torch.Tensor) -> torch.Tensor:
+        """The mesh_contact force [N] of a float64 ``(N, 3)`` state (``MeshContact.evaluate``)."""
+        if self._mesh_contact_args is None:
+            raise RuntimeError("the solver has no mesh_contact")
+        q = positions.detach().to(self.device, torch.float64).contiguous()
+        v = velocities.detach().to(self.device, torch.float64).contiguous()
+        force = torch.empty_like(q)
+        _lib.check(self._lib.pd_mesh_contact_force(self._handle, _lib.ptr(q), _lib.ptr(v), _lib.ptr(force), None,
+                                                   _stream()))
+        return force
 
     def set_anderson_window(self, window: int) -> None:
         """Change the Anderson window (0..8) of the following steps and backward passes (added)."""

@@ -459,3 +459,85 @@ def rollout(body, q0, v0, forces, gravity, dt, steps, **options):
         positions.append(x)
         iterations.append(it)
     return positions, iterations
+
+
+# ---------------------------------------------------------------------------
+# The reference's mesh_contact state force (mesh_contact.py:34-210): penalty
+# plus velocity friction between the surface vertices of one body and the
+# faces of the other, evaluated once per step on the start-of-step state.
+
+
+def closest_point_on_triangle(p, a, b, c):
+    """Closest point of triangle abc to p and its barycentric weights (Voronoi regions, mesh_contact.py:34-76)."""
+    ab, ac, ap = b - a, c - a, p - a
+    d1, d2 = ab @ ap, ac @ ap
+    if d1 <= 0.0 and d2 <= 0.0:
+        return a, np.array((1.0, 0.0, 0.0))
+    bp = p - b
+    d3, d4 = ab @ bp, ac @ bp
+    if d3 >= 0.0 and d4 <= d3:
+        return b, np.array((0.0, 1.0, 0.0))
+    vc = d1 * d4 - d3 * d2
+    if vc <= 0.0 and d1 >= 0.0 and d3 <= 0.0:
+        t = d1 / (d1 - d3)
+        return a + t * ab, np.array((1.0 - t, t, 0.0))
+    cp = p - c
+    d5, d6 = ab @ cp, ac @ cp
+    if d6 >= 0.0 and d5 <= d6:
+        return c, np.array((0.0, 0.0, 1.0))
+    vb = d5 * d2 - d1 * d6
+    if vb <= 0.0 and d2 >= 0.0 and d6 <= 0.0:
+        t = d2 / (d2 - d6)
+        return a + t * ac, np.array((1.0 - t, 0.0, t))
+    va = d3 * d6 - d5 * d4
+    if va <= 0.0 and (d4 - d3) >= 0.0 and (d5 - d6) >= 0.0:
+        t = (d4 - d3) / ((d4 - d3) + (d5 - d6))
+        return b + t * (c - b), np.array((0.0, 1.0 - t, t))
+    scale = 1.0 / (va + vb + vc)
+    v, w = vb * scale, vc * scale
+    return a + ab * v + ac * w, np.array((1.0 - v - w, v, w))
+
+
+def _pair_force(p, face_points, vp, face_velocities, radius, kn, kf, mu):
+    """Force on the vertex from one face (zero outside the radius) and the closest point's weights."""
+    a, b, c = face_points
+    closest, weights = closest_point_on_triangle(p, a, b, c)
+    gap2 = (p - closest) @ (p - closest)
+    if gap2 >= radius * radius:
+        return None
+    gap = np.sqrt(gap2)
+    if gap > EPS:
+        normal = (p - closest) / gap
+    else:
+        normal = np.cross(b - a, c - a)
+        length = np.linalg.norm(normal)
+        if length <= EPS:
+            return None
+        normal = normal / length
+    if normal @ (p - closest) < 0.0:
+        normal = -normal
+    magnitude = kn * (radius - gap)
+    relative = vp - weights @ face_velocities
+    tangential = relative - normal * (relative @ normal)
+    speed = np.linalg.norm(tangential)
+    friction = np.zeros(3)
+    if speed > EPS:
+        friction = -min(kf, mu * magnitude / (speed + EPS)) * tangential
+    return magnitude * normal + friction, weights
+
+
+def mesh_contact_force(q, v, faces_a, faces_b, radius, kn_left, kn_right, kf, mu):
+    """Per-particle force [N]: A's surface vertices against B's faces with kn_left, B's against A's with kn_right."""
+    q, v = np.asarray(q, dtype=np.float64), np.asarray(v, dtype=np.float64)
+    faces_a, faces_b = np.asarray(faces_a), np.asarray(faces_b)
+    force = np.zeros_like(q)
+    for vertices, faces, kn in ((np.unique(faces_a), faces_b, kn_left), (np.unique(faces_b), faces_a, kn_right)):
+        for vid in vertices:
+            for face in faces:
+                hit = _pair_force(q[vid], q[face], v[vid], v[face], radius, kn, kf, mu)
+                if hit is None:
+                    continue
+                total, weights = hit
+                force[vid] += total
+                force[face] -= np.outer(weights, total)
+    return force

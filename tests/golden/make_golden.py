@@ -313,7 +313,43 @@ def main():
         for name, value in result.items():
             backward[f"{key}__out_{name}"] = value
     np.savez_compressed(HERE / "tet_backward.npz", **backward)
+    np.savez_compressed(HERE / "mesh_contact.npz", **mesh_contact_fixture(oracle))
     print("wrote", sorted(p.name for p in HERE.glob("*.npz")))
+
+
+_TET_FACES = np.array(((1, 2, 3), (0, 3, 2), (0, 1, 3), (0, 2, 1)))
+
+
+def two_bodies(gap):
+    """A 3x2x2 grid of 0.1 m cubes (bottom pinned) and one tetrahedron whose apex
+    reaches ``gap`` above the grid top (the reference test's two-body scene)."""
+    vertices, tets, _ = meshes.tet_grid(3, 2, 2, 0.1)
+    grid = len(vertices)
+    extra = np.array(((0.13, 0.11, 0.2 + gap), (0.33, 0.07, 0.5), (0.05, 0.18, 0.5), (0.17, 0.02, 0.55)))
+    vertices = np.vstack((vertices, extra))
+    tets = np.vstack((tets, np.arange(grid, grid + 4)[None]))
+    faces = tets[:, _TET_FACES].reshape(-1, 3)
+    _, first, counts = np.unique(np.sort(faces, axis=1), axis=0, return_index=True, return_counts=True)
+    faces = faces[first[counts == 1]]
+    faces_a = faces[np.all(faces < grid, axis=1)]
+    faces_b = faces[np.all(faces >= grid, axis=1)]
+    return vertices, tets, faces_a, faces_b
+
+
+def mesh_contact_fixture(oracle):
+    """``mesh_contact_force`` of the reference transcription on perturbed two-body states."""
+    out = {}
+    rng = np.random.default_rng(7)
+    vertices, tets, faces_a, faces_b = two_bodies(-0.004)
+    options = (0.02, 5.0e3, 5.0e4, 50.0, 0.5)
+    out["vertices"], out["tets"], out["faces_a"], out["faces_b"] = vertices, tets, faces_a, faces_b
+    out["options"] = np.array(options)
+    for trial in range(4):
+        q = vertices + 0.012 * rng.standard_normal(vertices.shape) * (trial > 0)
+        v = rng.standard_normal(vertices.shape)
+        out[f"t{trial}__q"], out[f"t{trial}__v"] = q, v
+        out[f"t{trial}__force"] = oracle.mesh_contact_force(q, v, faces_a, faces_b, *options)
+    return out
 
 
 if __name__ == "__main__":

@@ -96,3 +96,12 @@ def test_projections_follow_unsigned_svd_conventions():
     mats = np.eye(3) + 0.3 * rng.standard_normal((16, 3, 3))
     mats = mats[np.linalg.det(mats) > 0.1]
     np.testing.assert_allclose(np.linalg.det(pd_oracle.volume_projection(mats)), 1.0, atol=1e-9)
+
+
+def test_mesh_contact_force_matches_reference_transcription():
+    g = golden("mesh_contact.npz")
+    for trial in range(4):
+        expected = g[f"t{trial}__force"]
+        got = pd_oracle.mesh_contact_force(g[f"t{trial}__q"], g[f"t{trial}__v"], g["faces_a"], g["faces_b"],
+                                           *g["options"])
+        np.testing.assert_allclose(got, expected, rtol=0.0, atol=1e-12 * max(np.abs(expected).max(), 1.0))
