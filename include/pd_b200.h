@@ -153,6 +153,36 @@ int pd_mesh_contact_force(PdSolver* solver, const double* q, const double* v, do
 /* Pairs within the radius at the last step (solver.mesh_contact_pairs, solver.py:351-353). Synchronises. */
 int pd_mesh_contact_pairs(PdSolver* solver, int32_t* pairs, void* stream);
 
+#define PD_BOUNDARY_PLANAR 0    /* parameters (nx, ny, nz, offset): gap (n.x + offset) / |n| */
+#define PD_BOUNDARY_SPHERICAL 1 /* parameters (cx, cy, cz, radius): gap |x - c| - radius */
+#define PD_BOUNDARY_MESH 2      /* parameters[0] = contact radius; faces_left / faces_right, split index */
+/* The reference's frictional boundary (FrictionalContact, contact.py:684-1015;
+   SolverDiffPhD(frictional_boundary=..., frictional_vertices=..., friction=...,
+   restitution=...), solver.py:170-171 and :303-320): `count` registered
+   particles `nodes` (host, unique). Every local/global iteration of the
+   following steps takes one Fischer-Burmeister Newton step on their normal
+   multipliers and a Coulomb stick/slip update, and restitution acts after
+   convergence. The mesh kind tests vertices below `split` against faces_right
+   and the others against faces_left (host [n][3]); the other kinds ignore
+   split and faces. The multipliers start from zero at every factor build and
+   warm-start the following steps. Tet4 only; one boundary per solver. */
+int pd_set_frictional_boundary(PdSolver* solver, int32_t kind, const double parameters[4], int32_t count,
+                               const int32_t* nodes, double friction, double restitution, int32_t split,
+                               int32_t n_left, const int32_t* faces_left, int32_t n_right,
+                               const int32_t* faces_right);
+/* Device pointers of the boundary parameters (float64 [4]; planar and
+   spherical kinds read them at every step, so edits between steps and
+   between graph replays take effect: solver.boundary_parameters,
+   solver.py:340-343) and of the normal multipliers (float64 [count]; the
+   warm start: solver.contact_multipliers, solver.py:345-348). */
+int pd_frictional_buffers(PdSolver* solver, double** parameters, double** multipliers, int32_t* count);
+/* Copies of the last step's contact state (the StepRecord snapshot,
+   adjoint.py:834-841): multipliers [count], omega [count], normals [count][3]
+   and mesh candidate flags [count] into caller buffers (device or host,
+   NULL to skip), ordered on `stream`. */
+int pd_frictional_state(PdSolver* solver, double* multiplier, double* omega, double* normal, int32_t* candidate,
+                        void* stream);
+
 /* SolverDiffPhD._build (solver.py:491-552): assembles the constant matrix
    A = m/h^2 I + sum_e w_e Vbar G_e^T G_e (+ fibres, + plane diagonal) and builds
    the exact inverse factor A^{-1} = S^T S on the host (sparse.py:291-320),

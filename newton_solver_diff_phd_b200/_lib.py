@@ -105,6 +105,9 @@ SIGNATURES = {
     "pd_set_mesh_contact": ([_P, _D, _D, _D, _D, _D, _I32, _P, _I32, _P], ctypes.c_int),
     "pd_mesh_contact_force": ([_P, _P, _P, _P, _P, _P], ctypes.c_int),
     "pd_mesh_contact_pairs": ([_P, _P, _P], ctypes.c_int),
+    "pd_set_frictional_boundary": ([_P, _I32, _P, _I32, _P, _D, _D, _I32, _I32, _P, _I32, _P], ctypes.c_int),
+    "pd_frictional_buffers": ([_P, ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_I32)], ctypes.c_int),
+    "pd_frictional_state": ([_P, _P, _P, _P, _P, _P], ctypes.c_int),
     "pd_build": ([_P, _D], ctypes.c_int),
     "pd_factor_stats": ([_P, ctypes.POINTER(_I64), ctypes.POINTER(_I64), ctypes.POINTER(_I64)], ctypes.c_int),
     "pd_step": ([_P, _P, _P, _P, _P, _P, _D, _P, _P, _P, _P], ctypes.c_int),
@@ -250,3 +253,14 @@ def dense_to_csr(matrix):
         values.extend(row[nz].tolist())
         offsets.append(len(columns))
     return np.asarray(offsets), np.asarray(columns), np.asarray(values)
+
+
+class DeviceView:
+    """A library-owned device array as a ``__cuda_array_interface__`` object, so that
+    ``torch.as_tensor(view, device=...)`` aliases it without a copy."""
+
+    def __init__(self, pointer: int, shape: tuple, typestr: str, owner):
+        self._owner = owner  # keeps the solver (and its allocation) alive
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (int(pointer), False),
+                                         "version": 3, "strides": None}
+

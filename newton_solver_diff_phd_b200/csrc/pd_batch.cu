@@ -1144,6 +1144,8 @@ extern "C" int pd_batch_create(PdSolver* const* solvers, int32_t count, const Pd
       return pd_set_error(PD_ERR_UNSUPPORTED, "muscle activations are not supported by the batched path");
     if (s->has_mesh_contact)
       return pd_set_error(PD_ERR_UNSUPPORTED, "mesh_contact is not supported by the batched path");
+    if (s->has_friction)
+      return pd_set_error(PD_ERR_UNSUPPORTED, "frictional_boundary is not supported by the batched path");
   }
   batch->device = solvers[0]->device;
   batch->precision = solvers[0]->options.precision;

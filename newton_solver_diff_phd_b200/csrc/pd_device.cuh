@@ -273,6 +273,45 @@ struct Team {
   int size;
 };
 
+// A frictional boundary of the step (the reference's FrictionalContact):
+// registered vertices, boundary description, the factor's panel and the
+// per-step and per-iteration contact state. count == 0 disables it.
+struct FrictionArgs {
+  int count;              // registered vertices K
+  int kind;               // 0 planar, 1 spherical, 2 mesh
+  const double* params;   // [4] plane (n, offset) or sphere (center, radius); device memory, editable
+  const int* nodes;       // [K] particle of each contact
+  double friction;        // Coulomb coefficient
+  double restitution;     // normal restitution coefficient
+  const int* faces;       // mesh: [F][3], faces_left then faces_right
+  int face_count, left_count, split;
+  double radius;          // mesh contact radius
+  const double* panel;    // [n][K] A^{-1} e_nodes[j]
+  const double* block;    // [K][K] panel rows of the registered vertices
+  double* normal;         // [K][3] frames frozen at the step start
+  double* tangent1;
+  double* tangent2;
+  double* delassus;       // [K][K]
+  double* regularization; // [K]
+  int* candidate;         // [K] mesh pre-filter (1 for planar and spherical)
+  double* multiplier;     // [K] normal multipliers, warm start across steps
+  double* lambda_t;       // [K][2] tangential multipliers
+  double* omega;          // [K] per-iteration Fischer-Burmeister scalars
+  double* diagonal;
+  double* residual;
+  double* rhs;
+  double* force;          // [K][3]
+  double* response;       // [K][3]
+  int* order;             // [K] coupled candidates in candidate order
+  int* slot;              // [K] position in order or -1
+  int* active;            // [1] number of coupled candidates
+  double* matrix;         // [K][K] coupled Newton block and its factor
+  double* compact;        // [K]
+  int* permutation;       // [K]
+  double* work;           // [K]
+  double* surface;        // [n][3] mesh restitution: iterate of the last contact update
+};
+
 // Everything one persistent launch needs. Passed by value as kernel argument.
 struct StepArgs {
   // Mesh
@@ -361,6 +400,7 @@ struct StepArgs {
   double dt, mass, inertia;
   double gravity[3];
   int integrate_pinned;
+  FrictionArgs fc;
 };
 
 }  // namespace pdb200

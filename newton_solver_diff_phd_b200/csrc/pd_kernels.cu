@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include "pd_forward.cuh"
+#include "pd_friction.cuh"
 #include "pd_kernels.h"
 #include "pd_team.cuh"
 
@@ -146,6 +147,12 @@ __device__ __forceinline__ bool forward_step_body(const StepArgs& a, const Team 
   }
   double* vector_smem = reinterpret_cast<double*>(dyn_smem + a.vector_smem_offset);
   if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
+  if (a.fc.count > 0) {
+    // Frictional boundary: frames, candidates, Delassus matrix (FrictionalContact.begin_step).
+    fb_begin_frames(a, team);
+    if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
+    fb_begin_delassus(a, team);
+  }
 
   const int r0 = a.st_part[team.rank], r1 = a.st_part[team.rank + 1];
   // This block's partial-sum slots: my_partials[slot * team.size].
@@ -263,6 +270,18 @@ __device__ __forceinline__ bool forward_step_body(const StepArgs& a, const Team 
       }
       spmv_block<TV>(a.plan_st, st_values, a.resident != 0, dyn_smem, in, a.x, team.rank);
     }
+    int contact_active = 0;
+    if (a.fc.count > 0) {
+      // x = A^{-1} (b + J^T lambda): one Newton step on the multipliers by the
+      // first block, then the correction through the panel columns.
+      if (a.fc.kind == kBoundaryMesh && a.fc.restitution > 0.0) {
+        for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) store3(a.fc.surface, i, load3d(a.prev, i));
+      }
+      if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
+      if (team.rank == 0) fb_newton(a);
+      if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
+      contact_active = *reinterpret_cast<volatile int*>(a.fc.active);
+    }
     __syncthreads();
     const int count = a.window > 0 ? a.aa_state[0] : 0;
     const int start = a.window > 0 ? a.aa_state[1] : 0;
@@ -270,6 +289,7 @@ __device__ __forceinline__ bool forward_step_body(const StepArgs& a, const Team 
     for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
       V3<double> value = load3d(a.x, i);
       if (a.refine) value = value + load3d(a.prev, i);
+      if (contact_active > 0) value = value + fb_correction(a.fc, i, contact_active);
       if (a.free_[i] == 0) value = load3d(a.boundary, i);
       store3(a.x, i, value);
       if (a.window > 0) {
@@ -346,6 +366,11 @@ __device__ __forceinline__ bool forward_step_body(const StepArgs& a, const Team 
     }
   }
 
+  if (a.fc.count > 0 && a.fc.restitution > 0.0) {
+    // FrictionalContact.finish_step: restitution on the converged positions.
+    fb_restitution(a, team);
+    if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
+  }
   // ---- Epilogue: write_state (kernels.py:404-414) and the step record.
   for (int i = gtid; i < n; i += gthreads) {
 #pragma unroll

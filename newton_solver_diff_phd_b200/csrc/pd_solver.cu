@@ -649,6 +649,9 @@ int pd_build(PdSolver* s, double dt) {
   s->built = true;
   s->stale = false;
   s->built_dt = dt;
+  if (s->has_friction) {
+    if (int status = pd_build_frictional_panel(s)) return status;
+  }
   return PD_OK;
 }
 
@@ -741,6 +744,7 @@ void fill_step_args(const PdSolver* s, StepArgs* a) {
   a->vector_smem_offset = s->vector_smem_offset;
   a->svd_u = s->options.svd_warm_start ? s->d_svd_u.as<double>() : nullptr;
   a->svd_v = s->options.svd_warm_start ? s->d_svd_v.as<double>() : nullptr;
+  a->fc = s->fc;
 }
 
 int pd_step(PdSolver* s, const void* q, const void* qd, const void* f, const void* dirichlet,

@@ -34,6 +34,9 @@ void fill_adjoint_args(const PdSolver* s, pdb200::AdjointArgs* b);
 int pd_ensure_adjoint_buffers(PdSolver* s);
 // The mesh contact force of the state (q, v) into s->mc_force (pd_contact.cu).
 int pd_evaluate_mesh_contact(PdSolver* s, const void* q, const void* v, int f64, cudaStream_t stream);
+// Panel A^{-1}[:, nodes] and block of the frictional boundary from the built
+// factor; zeroes the multipliers (pd_friction.cu).
+int pd_build_frictional_panel(PdSolver* s);
 }
 
 #define PD_CUDA(call)                                                                                 \
@@ -126,6 +129,14 @@ struct PdSolver {
   DeviceBuffer mc_vertices_a, mc_vertices_b, mc_faces_a, mc_faces_b, mc_slot_a, mc_slot_b;
   DeviceBuffer mc_inc_a_off, mc_inc_a, mc_inc_b_off, mc_inc_b;
   DeviceBuffer mc_force_ab, mc_bary_ab, mc_force_ba, mc_bary_ba, mc_force, mc_pairs;
+  // Frictional boundary (contact.py FrictionalContact): the device argument
+  // block with pointers into the buffers below; fc.count == 0 when absent.
+  bool has_friction = false;
+  pdb200::FrictionArgs fc{};
+  DeviceBuffer fc_params, fc_nodes, fc_faces, fc_panel, fc_block, fc_normal, fc_tangent1, fc_tangent2, fc_delassus,
+      fc_regularization, fc_candidate, fc_multiplier, fc_lambda_t, fc_omega, fc_diagonal, fc_residual, fc_rhs,
+      fc_force, fc_response, fc_order, fc_slot, fc_active, fc_matrix, fc_compact, fc_permutation, fc_work,
+      fc_surface;
   DeviceBuffer d_wc, d_wv, d_wn, d_wm, d_mdir, d_mtarget;
   DeviceBuffer d_s_off, d_s_col, d_s_val, d_s_val32, d_st_off, d_st_col, d_st_val, d_st_val32, d_s_part, d_st_part;
   DeviceBuffer d_a_off, d_a_col, d_a_val;

@@ -42,6 +42,7 @@ from . import _lib
 from .meshes import Mesh
 
 MATERIALS = {"pd": 0, "neo_hookean": 1}
+BOUNDARY_KINDS = {"planar": 0, "spherical": 1, "mesh": 2}
 PRECISIONS = {"fp64": _lib.PRECISION_FP64, "fp32+refine": _lib.PRECISION_FP32_REFINE, "fp32": _lib.PRECISION_FP32}
 ADJOINTS = {"reference": _lib.ADJOINT_REFERENCE, "exact": _lib.ADJOINT_EXACT}
 ADJOINT_SOLVERS = {"auto": 0, "fixed_point": 1, "cg": 2}
@@ -214,8 +215,12 @@ class SolverDiffPhD:
             raise ValueError("Explicit muscle_targets and planar_energies currently require hex_mesh")
         if hex_mesh is not None and any(x is not None for x in (frictional_boundary, mesh_contact)):
             raise NotImplementedError("Hex8 currently supports planar_energies, not frictional or mesh contact")
+        self._frictional_args = None
         if frictional_boundary is not None:
-            raise NotImplementedError("frictional_boundary is not available in this build")
+            self._frictional_args = self._validate_frictional(model, frictional_boundary, frictional_vertices, friction,
+                                                              restitution, hex_mesh)
+        elif frictional_vertices is not None or friction or restitution:
+            raise ValueError("frictional_vertices, friction and restitution need a frictional_boundary")
         if mesh_contact is not None:
             if len(mesh_contact) != 7:
                 raise ValueError("mesh_contact is (contact_radius, kn_left, kn_right, kf, mu, faces_a, faces_b)")
@@ -226,8 +231,6 @@ class SolverDiffPhD:
             self._mesh_contact_args = (tuple(float(value) for value in mesh_contact[:5]), mesh_faces)
         else:
             self._mesh_contact_args = None
-        if frictional_vertices is not None or friction or restitution:
-            raise ValueError("frictional_vertices, friction and restitution need a frictional_boundary")
         if not np.isfinite(density) or density <= 0:
             raise ValueError("density must be finite and positive")
         for name, value in (("abs_tol", abs_tol), ("rel_tol", rel_tol)):
@@ -365,6 +368,22 @@ class SolverDiffPhD:
             (radius, kn_left, kn_right, kf, mu), (faces_a, faces_b) = self._mesh_contact_args
             _lib.check(lib.pd_set_mesh_contact(handle, radius, kn_left, kn_right, kf, mu, len(faces_a), _lib.ptr(faces_a),
                                                len(faces_b), _lib.ptr(faces_b)))
+        self.boundary_parameters = None
+        self.contact_multipliers = None
+        if self._frictional_args is not None:
+            kind, parameters, nodes, friction_value, restitution_value, split, left, right = self._frictional_args
+            _lib.check(lib.pd_set_frictional_boundary(
+                handle, kind, _lib.ptr(parameters), len(nodes), _lib.ptr(nodes), friction_value, restitution_value,
+                split, len(left), _lib.ptr(left), len(right), _lib.ptr(right)))
+            params_ptr, multipliers_ptr, count = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_int32()
+            _lib.check(lib.pd_frictional_buffers(handle, ctypes.byref(params_ptr), ctypes.byref(multipliers_ptr),
+                                                 ctypes.byref(count)))
+            # Views of the solver's own device arrays: edits take effect at the next step.
+            self.boundary_parameters = torch.as_tensor(
+                _lib.DeviceView(params_ptr.value, (1, 4), "<f8", self), device=self.device)
+            self.contact_multipliers = torch.as_tensor(
+                _lib.DeviceView(multipliers_ptr.value, (count.value,), "<f8", self), device=self.device)
+            self.frictional_vertices = nodes
         self._x = torch.zeros((self._n, 3), dtype=torch.float64, device=self.device)
         self._factor_key = None
         self._model_changed = True
@@ -372,6 +391,55 @@ class SolverDiffPhD:
         self._activation_source = None
 
     # ------------------------------------------------------------------ setup
+    def _validate_frictional(self, model, boundary, vertices, friction, restitution, hex_mesh):
+        """Host checks of ``frictional_boundary`` (contact.py:715-760) and the default
+        registered vertices (solver.py:303-309): the mesh's face vertices, else the
+        surface vertices of the tetrahedra."""
+        if len(boundary) != 2:
+            raise ValueError("frictional_boundary is (kind, parameters)")
+        kind, parameters = boundary
+        if kind not in BOUNDARY_KINDS:
+            raise ValueError("frictional boundary must be 'planar', 'spherical' or 'mesh'")
+        split, left, right = 0, np.zeros((0, 3), np.int32), np.zeros((0, 3), np.int32)
+        if kind == "mesh":
+            if len(parameters) != 4:
+                raise ValueError("mesh boundary parameters are (contact_radius, split_index, faces_left, faces_right)")
+            split = int(parameters[1])
+            left, right = (np.ascontiguousarray(np.asarray(f, dtype=np.int32).reshape(-1, 3)) for f in parameters[2:4])
+            values = np.array([float(parameters[0]), 0.0, 0.0, 0.0])
+        else:
+            values = np.asarray(parameters, dtype=np.float64)
+            if values.shape != (4,):
+                raise ValueError("frictional boundary parameters must be four finite values")
+        if vertices is None:
+            if kind == "mesh":
+                vertices = np.unique(np.concatenate([left.reshape(-1), right.reshape(-1)]))
+            else:
+                tets = model.tet_indices.cpu().numpy().reshape(-1, 4)
+                faces = np.sort(np.concatenate([tets[:, [0, 1, 2]], tets[:, [0, 1, 3]], tets[:, [0, 2, 3]],
+                                                tets[:, [1, 2, 3]]]), axis=1)
+                unique, counts = np.unique(faces, axis=0, return_counts=True)
+                vertices = np.unique(unique[counts == 1])
+        vertices = np.asarray(vertices.cpu().numpy() if isinstance(vertices, torch.Tensor) else vertices)
+        if vertices.ndim != 1:
+            raise ValueError("frictional vertices must be unique particle indices")
+        nodes = np.ascontiguousarray(vertices, dtype=np.int32)
+        return (BOUNDARY_KINDS[kind], np.ascontiguousarray(values, dtype=np.float64), nodes, float(friction),
+                float(restitution), split, left, right)
+
+    def frictional_state(self):
+        """``(multipliers, omega, normals, candidates)`` of the last step as device tensors, or None."""
+        if self._frictional_args is None:
+            return None
+        count = len(self._frictional_args[2])
+        multiplier = torch.empty(count, dtype=torch.float64, device=self.device)
+        omega = torch.empty_like(multiplier)
+        normal = torch.empty((count, 3), dtype=torch.float64, device=self.device)
+        candidate = torch.empty(count, dtype=torch.int32, device=self.device)
+        _lib.check(self._lib.pd_frictional_state(self._handle, _lib.ptr(multiplier), _lib.ptr(omega), _lib.ptr(normal),
+                                                 _lib.ptr(candidate), _stream()))
+        return multiplier, omega, normal, candidate
+
     def _initialize_muscles(self, directions, stiffness):
         count = self._element_count
         self._has_muscles = False

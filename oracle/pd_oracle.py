@@ -260,15 +260,22 @@ class Body:
 
 # --------------------------------------------------------------------------- forward
 def step(body, q, v, f_ext, gravity, dt, *, max_iterations, abs_tol, rel_tol, window=5, boundary=None,
-         targets=None, integrate_pinned=False):
-    """One reference step. Returns ``(x, iterations, converged)``."""
+         targets=None, integrate_pinned=False, contact=None):
+    """One reference step. Returns ``(x, iterations, converged)``.
+
+    ``contact`` is a :class:`FrictionalBoundary`; its multipliers carry over
+    from call to call like the solver's warm start.
+    """
     q = np.asarray(q, dtype=np.float64)
     v = np.asarray(v, dtype=np.float64)
     if boundary is None:
         boundary = np.where(body.free[:, None], 0.0, q + (dt * v if integrate_pinned else 0.0))
     q_tilde = q + dt * v + dt**2 * (np.asarray(f_ext, dtype=np.float64) / body.mass + np.asarray(gravity, float))
-    factor = scipy.linalg.cho_factor(body.matrix(dt))
+    matrix = body.matrix(dt)
+    factor = scipy.linalg.cho_factor(matrix)
     inertia = body.mass / dt**2
+    if contact is not None:
+        contact.begin_step(q, np.linalg.inv(matrix), dt)
     x = q.copy()
     previous_rhs = np.zeros_like(x)
     history_x, history_g = [], []
@@ -277,6 +284,8 @@ def step(body, q, v, f_ext, gravity, dt, *, max_iterations, abs_tol, rel_tol, wi
         p = body.projection_rhs(x, boundary, targets)
         x_previous = x
         x = scipy.linalg.cho_solve(factor, inertia * q_tilde + p)
+        if contact is not None and len(contact.nodes):
+            x = contact.iterate(x_previous, x, q)
         x[~body.free] = boundary[~body.free]
         if window > 0:
             g = x - x_previous
@@ -301,7 +310,11 @@ def step(body, q, v, f_ext, gravity, dt, *, max_iterations, abs_tol, rel_tol, wi
         rhs_small = np.linalg.norm(p - previous_rhs) <= rel_tol * np.linalg.norm(previous_rhs) + abs_tol
         previous_rhs = p
         if iteration > 0 and step_small and rhs_small:
+            if contact is not None:
+                x = contact.restitution(x, q, v, dt)
             return x, iteration + 1, True
+    if contact is not None:
+        x = contact.restitution(x, q, v, dt)
     return x, max_iterations, False
 
 
@@ -541,3 +554,242 @@ def mesh_contact_force(q, v, faces_a, faces_b, radius, kn_left, kn_right, kf, mu
                 force[vid] += total
                 force[face] -= np.outer(weights, total)
     return force
+
+
+# ---------------------------------------------------------------------------
+# The reference's frictional boundary (contact.py:77-1015): per local/global
+# iteration one semismooth Newton step on the Fischer-Burmeister function of
+# every registered vertex against a planar, spherical or mesh boundary, an
+# isotropic Coulomb stick/slip update, and the position correction through
+# the columns A^{-1} e_j of the registered vertices.
+
+
+def _boundary_gap(point, kind, parameters):
+    """``boundary_gap`` (contact.py:77-89): signed distance to the plane or sphere."""
+    if kind == "planar":
+        axis = parameters[:3]
+        norm = np.sqrt(axis @ axis)
+        unit = axis / norm
+        return point[0] * unit[0] + point[1] * unit[1] + point[2] * unit[2] + parameters[3] / norm
+    offset = point - parameters[:3]
+    return np.sqrt(offset @ offset) - parameters[3]
+
+
+def _boundary_normal(point, kind, parameters):
+    """``boundary_normal`` (contact.py:92-98)."""
+    if kind == "planar":
+        axis = parameters[:3]
+        return axis / np.sqrt(axis @ axis)
+    offset = point - parameters[:3]
+    return offset / np.sqrt(offset @ offset)
+
+
+def _plane_frame(normal):
+    """``GetLocalFrame`` (contact.py:182-193): t1 = normalize(n x e_i) of the axis maximising |n x e_i|."""
+    best = np.zeros(3)
+    for i in range(3):
+        candidate = np.cross(normal, np.eye(3)[i])
+        if candidate @ candidate > best @ best:
+            best = candidate
+    t1 = best / np.sqrt(best @ best)
+    t2 = np.cross(normal, t1)
+    return t1, t2 / np.sqrt(t2 @ t2)
+
+
+def _gram_schmidt_frame(normal):
+    """Tangents of a mesh contact (contact.py:225-236): from the axis least parallel to n, first on ties."""
+    axis = 0
+    for d in (1, 2):
+        if abs(normal[d]) < abs(normal[axis]):
+            axis = d
+    unit = np.eye(3)[axis]
+    t1 = unit - (normal @ unit) * normal
+    t1 = t1 / np.sqrt(t1 @ t1)
+    t2 = np.cross(normal, t1)
+    return t1, t2 / np.sqrt(t2 @ t2)
+
+
+class FrictionalBoundary:
+    """Frictional boundary of the reference step with the device's arithmetic layout.
+
+    ``kind`` is ``"planar"`` with ``parameters = (nx, ny, nz, offset)``,
+    ``"spherical"`` with ``(cx, cy, cz, radius)``, or ``"mesh"`` with
+    ``(contact_radius, split_index, faces_left, faces_right)``. The Delassus
+    matrix is ``W_ij = (n_i . n_j) B_ij`` with ``B = A^{-1}`` restricted to the
+    registered vertices (contact.py:242-256); only candidates with ``omega != 0``
+    enter the coupled Newton block (contact.py:450-528), the others take
+    ``d lambda = rhs / E`` (contact.py:531-546).
+    """
+
+    def __init__(self, kind, parameters, nodes, friction=0.0, restitution=0.0):
+        self.kind = kind
+        self.nodes = np.asarray(nodes, dtype=np.int64)
+        self.friction = float(friction)
+        self.restitution_coefficient = float(restitution)
+        k = len(self.nodes)
+        self.multiplier = np.zeros(k)
+        self.lambda_t = np.zeros((k, 2))
+        if kind == "mesh":
+            radius, split, left, right = parameters
+            self.radius, self.split = float(radius), int(split)
+            self.faces_left = np.asarray(left, dtype=np.int64).reshape(-1, 3)
+            self.faces_right = np.asarray(right, dtype=np.int64).reshape(-1, 3)
+            self.parameters = np.array([self.radius, 0.0, 0.0, 0.0])
+        else:
+            self.parameters = np.asarray(parameters, dtype=np.float64)
+        self.candidate = np.ones(k, dtype=bool)
+        self.omega = np.zeros(k)
+
+    # -- mesh geometry (contact.py:101-148)
+    def closest(self, p, node, x):
+        """Closest point, unit face normal and squared distance on the surface opposite ``node``."""
+        faces = self.faces_right if node < self.split else self.faces_left
+        best, closest, normal = np.inf, np.zeros(3), np.array([0.0, 0.0, 1.0])
+        for a, b, c in faces:
+            point, _ = closest_point_on_triangle(p, x[a], x[b], x[c])
+            dist2 = (p - point) @ (p - point)
+            if dist2 < best:
+                best, closest = dist2, point
+                n = np.cross(x[b] - x[a], x[c] - x[a])
+                length = np.sqrt(n @ n)
+                normal = n / length if length > EPS else np.array([0.0, 0.0, 1.0])
+        return closest, normal, best
+
+    @staticmethod
+    def direction(p, closest, face_normal):
+        offset = p - closest
+        length = np.sqrt(offset @ offset)
+        return offset / length if length > 1.0e-12 else face_normal
+
+    def begin_step(self, q, inverse, dt):
+        """Panel, frames, candidates, Delassus matrix and regularisation of the step (contact.py:775-836)."""
+        q = np.asarray(q, dtype=np.float64)
+        k = len(self.nodes)
+        self.panel = inverse[:, self.nodes]
+        self.block = self.panel[self.nodes]
+        self.normal = np.zeros((k, 3))
+        self.t1 = np.zeros((k, 3))
+        self.t2 = np.zeros((k, 3))
+        for c, node in enumerate(self.nodes):
+            if self.kind == "mesh":
+                closest, face_normal, dist2 = self.closest(q[node], node, q)
+                self.candidate[c] = np.sqrt(dist2) - self.radius <= 5.0 * self.radius
+                n = self.direction(q[node], closest, face_normal)
+                t1, t2 = _gram_schmidt_frame(n)
+                if not self.candidate[c]:
+                    self.multiplier[c] = 0.0
+            else:
+                n = _boundary_normal(q[node], self.kind, self.parameters)
+                t1, t2 = _plane_frame(n)
+            self.normal[c], self.t1[c], self.t2[c] = n, t1, t2
+        self.lambda_t[:] = 0.0
+        cosines = self.normal @ self.normal.T
+        self.delassus = cosines * np.tril(self.block) + (cosines * np.tril(self.block, -1)).T
+        self.regularization = np.maximum(dt * dt * np.diag(self.delassus), 1.0e-10)
+
+    def _scalars(self, x):
+        k = len(self.nodes)
+        delta = np.zeros(k)
+        omega = np.zeros(k)
+        diagonal = np.ones(k)
+        residual = np.zeros(k)
+        if self.kind == "mesh":
+            self.surface = x.copy()
+        for c, node in enumerate(self.nodes):
+            if not self.candidate[c]:
+                continue
+            if self.kind == "mesh":
+                closest, _, _ = self.closest(x[node], node, x)
+                delta[c] = (x[node] - closest) @ self.normal[c] - self.radius
+            else:
+                delta[c] = _boundary_gap(x[node], self.kind, self.parameters)
+            lam, r = self.multiplier[c], self.regularization[c]
+            s = max(np.sqrt(delta[c] * delta[c] + r * r * lam * lam), 1.0e-14)
+            omega[c] = 1.0 - delta[c] / s
+            diagonal[c] = (1.0 - r * lam / s) * r
+            residual[c] = delta[c] + r * lam - s
+        return delta, omega, diagonal, residual
+
+    def _forces(self, omega, tangential):
+        force = (omega * self.multiplier)[:, None] * self.normal
+        if tangential:
+            force = force + self.lambda_t[:, :1] * self.t1 + self.lambda_t[:, 1:] * self.t2
+        return force
+
+    def iterate(self, x, solved, q):
+        """One Newton step and friction update; returns ``A^{-1} (b + J^T lambda)`` (contact.py:909-984)."""
+        nodes = self.nodes
+        delta, omega, diagonal, residual = self._scalars(x)
+        self.omega = omega
+        active = np.flatnonzero(omega != 0.0)
+        force = self._forces(omega, True)
+        response = self.block[:, active] @ force[active]
+        rhs = -residual + omega * np.einsum("ij,ij->i", self.normal, x[nodes])
+        rhs -= omega * np.einsum("ij,ij->i", self.normal, solved[nodes] + response)
+        step = np.divide(rhs, diagonal, out=np.zeros_like(rhs), where=omega == 0.0)
+        if len(active):
+            system = omega[active, None] * self.delassus[np.ix_(active, active)] * omega[None, active]
+            system[np.diag_indices(len(active))] += diagonal[active]
+            step[active] = np.linalg.solve(system, rhs[active])
+        self.multiplier = np.clip(self.multiplier + step, 0.0, 1.0e8)
+        if self.friction > 0:
+            normal_response = self.block[:, active] @ self._forces(omega, False)[active]
+            for c, node in enumerate(nodes):
+                if self.multiplier[c] <= 0.0:
+                    self.lambda_t[c] = 0.0
+                    continue
+                move = solved[node] + normal_response[c] - q[node]
+                n = self.normal[c]
+                tangential = move - (move @ n) * n
+                u1, u2 = tangential @ self.t1[c], tangential @ self.t2[c]
+                diagonal_c = self.block[c, c]
+                w11 = (self.t1[c] @ self.t1[c]) * diagonal_c
+                w12 = (self.t1[c] @ self.t2[c]) * diagonal_c
+                w22 = (self.t2[c] @ self.t2[c]) * diagonal_c
+                determinant = w11 * w22 - w12 * w12
+                stick = np.zeros(2)
+                if abs(determinant) > 1.0e-20:
+                    stick = np.array((-(w22 * u1 - w12 * u2), -(-w12 * u1 + w11 * u2))) / determinant
+                radius = self.friction * self.multiplier[c]
+                if np.sqrt(stick @ stick) <= radius + 1.0e-14:
+                    self.lambda_t[c] = stick
+                else:
+                    magnitude = np.sqrt(u1 * u1 + u2 * u2)
+                    self.lambda_t[c] = (-radius * u1 / magnitude, -radius * u2 / magnitude) if magnitude > 1.0e-14 \
+                        else (0.0, 0.0)
+        force = self._forces(omega, True)
+        return solved + self.panel[:, active] @ force[active]
+
+    def restitution(self, x, q, v, dt):
+        """Post-solve restitution (contact.py:595-667)."""
+        if self.restitution_coefficient <= 0 or not len(self.nodes):
+            return x
+        x = x.copy()
+        for c, node in enumerate(self.nodes):
+            if self.multiplier[c] <= 0.0:
+                continue
+            point = x[node].copy()
+            if self.kind == "mesh":
+                reference = self.normal[c]
+                closest, face_normal, _ = self.closest(point, node, self.surface)
+                distance = (point - closest) @ reference - self.radius
+                n = self.direction(point, closest, face_normal)
+                if n @ reference < 0.0:
+                    n = -n
+                slop = 0.1 * self.radius
+            else:
+                distance = _boundary_gap(point, self.kind, self.parameters)
+                n = _boundary_normal(point, self.kind, self.parameters)
+                slop = 1.0e-8
+            norm = np.sqrt(n @ n)
+            if norm <= 1.0e-12:
+                continue
+            n = n / norm
+            if distance > slop:
+                continue
+            incoming = v[node] @ n
+            if incoming < 0.0:
+                change = -self.restitution_coefficient * incoming - ((point - q[node]) / dt) @ n
+                if change > 0.0:
+                    x[node] = point + dt * change * n
+        return x

@@ -161,8 +161,13 @@ def tet_matrix(oracle, vertices, tets, poses, mu, lame, free, material, dt, musc
 def main():
     parser = argparse.ArgumentParser()
     parser.add_argument("--reference", default="/root/reference")
+    parser.add_argument("--only", choices=("frictional_contact",), default=None,
+                        help="regenerate one fixture file and leave the others untouched")
     args = parser.parse_args()
     oracle, sparse, hex_oracle = load_reference(Path(args.reference))
+    if args.only == "frictional_contact":
+        np.savez_compressed(HERE / "frictional_contact.npz", **frictional_contact_fixture(oracle))
+        return
 
     # --- Sparse inverse factors (sparse.py host setup) ------------------------
     factors = {}
@@ -314,6 +319,7 @@ def main():
             backward[f"{key}__out_{name}"] = value
     np.savez_compressed(HERE / "tet_backward.npz", **backward)
     np.savez_compressed(HERE / "mesh_contact.npz", **mesh_contact_fixture(oracle))
+    np.savez_compressed(HERE / "frictional_contact.npz", **frictional_contact_fixture(oracle))
     print("wrote", sorted(p.name for p in HERE.glob("*.npz")))
 
 
@@ -349,6 +355,111 @@ def mesh_contact_fixture(oracle):
         v = rng.standard_normal(vertices.shape)
         out[f"t{trial}__q"], out[f"t{trial}__v"] = q, v
         out[f"t{trial}__force"] = oracle.mesh_contact_force(q, v, faces_a, faces_b, *options)
+    return out
+
+
+# Options of the reference contact tests (tests/test_diff_phd_contact.py:16-18).
+CONTACT_TIGHT = {"max_iterations": 2000, "abs_tol": 1.0e-12, "rel_tol": 1.0e-11}
+CONTACT_REFERENCE = {"max_iterations": 2000, "abs_tol": 1.0e-9, "rel_tol": 1.0e-6}
+
+
+def surface_faces(tets):
+    """Faces of exactly one tetrahedron, in first-occurrence orientation (tests/test_diff_phd_mesh_boundary.py:22-25)."""
+    faces = np.concatenate([tets[:, [0, 1, 2]], tets[:, [0, 1, 3]], tets[:, [0, 2, 3]], tets[:, [1, 2, 3]]])
+    _unique, index, counts = np.unique(np.sort(faces, axis=1), axis=0, return_index=True, return_counts=True)
+    return faces[np.sort(index[counts == 1])]
+
+
+def contact_rollout(oracle, step, contact, q, v, gravity, dt, steps, options, registered=None):
+    """Step the reference oracle with its contact and chain the float32 states as the solver writes them."""
+    out = {}
+    for t in range(steps):
+        x, iterations, converged = step.step(q, v, np.zeros_like(q), gravity, dt, contact=contact, **options)
+        out[f"s{t}__q"], out[f"s{t}__v"], out[f"s{t}__x"] = q, v, x
+        out[f"s{t}__iterations"] = np.int32(iterations)
+        out[f"s{t}__converged"] = np.int32(converged)
+        if registered is None:
+            out[f"s{t}__multiplier"] = contact.multiplier.copy()
+        else:
+            out[f"s{t}__multiplier"] = contact.registered_multiplier()
+            out[f"s{t}__candidate"] = np.isin(registered, contact.nodes).astype(np.int32)
+        # write_state: q+ = x, v+ = (x - q) / h, stored as float32.
+        q, v = x.astype(np.float32).astype(np.float64), ((x - q) / dt).astype(np.float32).astype(np.float64)
+    return out
+
+
+def frictional_contact_fixture(oracle):
+    """``ReferenceContact`` / ``ReferenceMeshContact`` rollouts of the reference contact tests
+    (tests/test_diff_phd_contact.py:40-142, tests/test_diff_phd_mesh_boundary.py:28-135)."""
+    out = {}
+    dt = 0.004
+    gravity = np.array([0.0, 0.0, -9.81], dtype=np.float32).astype(np.float64)
+    vertices, tets, _ = meshes.tet_grid(3, 2, 2, 0.1, origin=(0.0, 0.0, 1.0))
+    # Newton keeps rest poses in float32.
+    poses = meshes.tet_rest_poses(vertices, tets).astype(np.float32).astype(np.float64)
+    mu = np.full(len(tets), 2.0e4, dtype=np.float32).astype(np.float64)
+    lame = np.full(len(tets), 5.0e4, dtype=np.float32).astype(np.float64)
+    free = np.ones(len(vertices), dtype=bool)
+    nodes = np.unique(surface_faces(tets))
+    center = vertices.astype(np.float32).astype(np.float64).mean(axis=0)
+    sphere = ("spherical", (center[0], center[1], -0.25, 0.25))
+    plane = ("planar", (0.0, 0.0, 1.0, 0.0))
+    cases = {
+        "plane": (plane, 0.0, 0.0, 0.001, (0.0, 0.0, -1.0), 3, CONTACT_TIGHT),
+        "stick": (plane, 2.0, 0.0, 0.001, (0.05, 0.0, -1.0), 3, CONTACT_TIGHT),
+        "slide": (plane, 0.1, 0.0, 0.001, (2.0, 0.0, -1.0), 3, CONTACT_TIGHT),
+        "sphere": (sphere, 0.4, 0.0, 0.0005, (0.0, 0.0, -1.0), 3, CONTACT_REFERENCE),
+        "chatter": (sphere, 0.4, 0.0, 0.0005, (0.0, 0.0, -1.0), 2, CONTACT_TIGHT),
+        "restitution": (plane, 0.0, 0.5, 0.001, (0.0, 0.0, -1.0), 2, CONTACT_TIGHT),
+    }
+    out["grid__nodes"] = nodes
+    for name, (boundary, friction, restitution, height, velocity, steps, options) in cases.items():
+        q = vertices.astype(np.float32).astype(np.float64)
+        q[:, 2] += height - q[:, 2].min()
+        q = q.astype(np.float32).astype(np.float64)
+        v = np.tile(np.asarray(velocity, dtype=np.float32), (len(q), 1)).astype(np.float64)
+        step = oracle.ReferenceStep(tets, poses, mu, lame, 1000.0, free, "pd")
+        contact = oracle.ReferenceContact(*boundary, nodes, friction=friction, restitution=restitution)
+        out[f"{name}__parameters"] = np.asarray(boundary[1], dtype=np.float64)
+        out[f"{name}__options"] = np.array([options["max_iterations"], options["abs_tol"], options["rel_tol"],
+                                            friction, restitution])
+        for key, value in contact_rollout(oracle, step, contact, q, v, gravity, dt, steps, options).items():
+            out[f"{name}__{key}"] = value
+    # Two soft blocks (tests/test_diff_phd_mesh_boundary.py:28-40): a free 2x1x1 block
+    # above a 3x2x2 block with a pinned bottom, offset half a cell in x.
+    radius = 0.01
+    upper, upper_tets, _ = meshes.tet_grid(2, 1, 1, 0.1, origin=(0.05, 0.0, 0.2 + radius + 0.002))
+    lower, lower_tets, _ = meshes.tet_grid(3, 2, 2, 0.1)
+    split = len(upper)
+    vertices = np.vstack((upper, lower))
+    tets = np.vstack((upper_tets, lower_tets + split))
+    poses = meshes.tet_rest_poses(vertices, tets).astype(np.float32).astype(np.float64)
+    mu = np.full(len(tets), 2.0e4, dtype=np.float32).astype(np.float64)
+    lame = np.full(len(tets), 5.0e4, dtype=np.float32).astype(np.float64)
+    free = np.ones(len(vertices), dtype=bool)
+    free[split:] = lower[:, 2] > 0.0
+    faces_left, faces_right = surface_faces(upper_tets), surface_faces(lower_tets) + split
+    out.update({"blocks__vertices": vertices, "blocks__tets": tets, "blocks__split": np.int32(split),
+                "blocks__faces_left": faces_left, "blocks__faces_right": faces_right, "blocks__free": free})
+    registered = np.unique(np.concatenate([faces_left, faces_right]))
+    registered = registered[free[registered]]
+    mesh_cases = {
+        "mesh": (registered[registered < split], 0.0, 0.0, (0.0, 0.0, -1.0), 4, CONTACT_TIGHT),
+        "mesh_stick": (registered[registered < split], 2.0, 0.0, (0.5, 0.0, -1.0), 4, CONTACT_REFERENCE),
+        "mesh_restitution": (registered[registered < split], 0.0, 0.5, (0.0, 0.0, -1.0), 4, CONTACT_TIGHT),
+        "mesh_two_sided": (registered, 0.0, 0.0, (0.0, 0.0, -1.0), 3, CONTACT_REFERENCE),
+    }
+    for name, (nodes, friction, restitution, velocity, steps, options) in mesh_cases.items():
+        q = vertices.astype(np.float32).astype(np.float64)
+        v = np.zeros_like(q)
+        v[:split] = np.asarray(velocity, dtype=np.float32)
+        step = oracle.ReferenceStep(tets, poses, mu, lame, 1000.0, free, "pd")
+        contact = oracle.ReferenceMeshContact(radius, split, faces_left, faces_right, nodes, friction, restitution)
+        out[f"{name}__nodes"] = nodes
+        out[f"{name}__options"] = np.array([options["max_iterations"], options["abs_tol"], options["rel_tol"],
+                                            friction, restitution, radius])
+        for key, value in contact_rollout(oracle, step, contact, q, v, gravity, dt, steps, options, nodes).items():
+            out[f"{name}__{key}"] = value
     return out
 
 

@@ -105,3 +105,57 @@ def test_mesh_contact_force_matches_reference_transcription():
         got = pd_oracle.mesh_contact_force(g[f"t{trial}__q"], g[f"t{trial}__v"], g["faces_a"], g["faces_b"],
                                            *g["options"])
         np.testing.assert_allclose(got, expected, rtol=0.0, atol=1e-12 * max(np.abs(expected).max(), 1.0))
+
+
+CONTACT_CASES = ["plane", "stick", "slide", "sphere", "chatter", "restitution", "mesh", "mesh_stick",
+                 "mesh_restitution", "mesh_two_sided"]
+
+
+def contact_scene(g, name):
+    """Oracle body, boundary and per-step fixture inputs of one reference contact rollout."""
+    if name.startswith("mesh"):
+        vertices, tets = g["blocks__vertices"], g["blocks__tets"]
+        free = g["blocks__free"]
+        options = g[f"{name}__options"]
+        parameters = (float(options[5]), int(g["blocks__split"]), g["blocks__faces_left"], g["blocks__faces_right"])
+        boundary = pd_oracle.FrictionalBoundary("mesh", parameters, g[f"{name}__nodes"], friction=float(options[3]),
+                                                restitution=float(options[4]))
+    else:
+        vertices, tets, _ = meshes.tet_grid(3, 2, 2, 0.1, origin=(0.0, 0.0, 1.0))
+        free = np.ones(len(vertices), dtype=bool)
+        options = g[f"{name}__options"]
+        kind = "spherical" if name in ("sphere", "chatter") else "planar"
+        boundary = pd_oracle.FrictionalBoundary(kind, g[f"{name}__parameters"], g["grid__nodes"],
+                                                friction=float(options[3]), restitution=float(options[4]))
+    poses = meshes.tet_rest_poses(vertices, tets).astype(np.float32).astype(np.float64)
+    mu = np.full(len(tets), 2.0e4, dtype=np.float32).astype(np.float64)
+    lame = np.full(len(tets), 5.0e4, dtype=np.float32).astype(np.float64)
+    body = pd_oracle.Body.tet(tets, poses, free, mu, lame, 1000.0)
+    solve = {"max_iterations": int(options[0]), "abs_tol": float(options[1]), "rel_tol": float(options[2])}
+    steps = sum(1 for key in g.files if key.startswith(f"{name}__s") and key.endswith("__x"))
+    return body, boundary, solve, steps
+
+
+@pytest.mark.parametrize("name", CONTACT_CASES)
+def test_frictional_boundary_matches_reference_transcription(name):
+    """The restated frictional boundary against ``ReferenceContact`` / ``ReferenceMeshContact``
+    rollouts (tests/test_diff_phd_contact.py:40-142, tests/test_diff_phd_mesh_boundary.py:42-110)."""
+    g = golden("frictional_contact.npz")
+    body, boundary, solve, steps = contact_scene(g, name)
+    for t in range(steps):
+        key = f"{name}__s{t}"
+        q, v = g[key + "__q"], g[key + "__v"]
+        x, iterations, converged = pd_oracle.step(body, q, v, np.zeros_like(q), GRAVITY, 0.004, contact=boundary,
+                                                  **solve)
+        assert iterations == int(g[key + "__iterations"])
+        assert converged == bool(g[key + "__converged"])
+        if not converged:
+            # The stick/slip projection chatters to the iteration cap; the reference
+            # compares only the iteration count and the status there.
+            continue
+        np.testing.assert_allclose(x, g[key + "__x"], rtol=0.0, atol=1.0e-9)
+        if name.startswith("mesh"):
+            np.testing.assert_array_equal(boundary.candidate.astype(np.int32), g[key + "__candidate"])
+        if name != "mesh_two_sided":
+            tolerance = {"rtol": 1.0e-5, "atol": 1.0e-6} if name.startswith("mesh") else {"rtol": 1.0e-6, "atol": 1.0e-9}
+            np.testing.assert_allclose(boundary.multiplier, g[key + "__multiplier"], **tolerance)
