@@ -219,6 +219,19 @@ int pd_step(PdSolver* solver, const void* q, const void* qd, const void* f, cons
 int pd_backward(PdSolver* solver, const double* x_record, const float* activations, double dt, const void* gq_out,
                 const void* gqd_out, void* gq, void* gqd, void* gf, void* gdirichlet, double* gmaterials,
                 float* gactivations, void* stream);
+/* pd_backward of a step with a frictional boundary, given the contact state
+   that step recorded (pd_frictional_state right after it: device float64
+   multipliers [count], omega [count], normals [count][3]). When material or
+   activation gradients are requested, they use the reference's contact
+   projection z = mu - W_T G^{-1} (J mu) (Adjoint._woodbury, adjoint.py:1272-1354):
+   one adjoint fixed point per selected contact row, capped at
+   min(max_iterations, 120) iterations; the state gradients use mu as in the
+   reference. Reads the selected row count back to the host once (synchronises
+   `stream`). NULL snapshot pointers make it pd_backward. */
+int pd_backward_contact(PdSolver* solver, const double* x_record, const float* activations, double dt,
+                        const void* gq_out, const void* gqd_out, void* gq, void* gqd, void* gf, void* gdirichlet,
+                        double* gmaterials, float* gactivations, const double* multiplier, const double* omega,
+                        const double* normal, void* stream);
 
 /* Device buffer of 8 uint64 nanosecond accumulators for the per-phase timers
    of a library built with -DPD_PHASE_TIMERS (profiling); ignored otherwise.

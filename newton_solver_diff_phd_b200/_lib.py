@@ -112,6 +112,7 @@ SIGNATURES = {
     "pd_factor_stats": ([_P, ctypes.POINTER(_I64), ctypes.POINTER(_I64), ctypes.POINTER(_I64)], ctypes.c_int),
     "pd_step": ([_P, _P, _P, _P, _P, _P, _D, _P, _P, _P, _P], ctypes.c_int),
     "pd_backward": ([_P, _P, _P, _D, _P, _P, _P, _P, _P, _P, _P, _P, _P], ctypes.c_int),
+    "pd_backward_contact": ([_P, _P, _P, _D] + [_P] * 12, ctypes.c_int),
     "pd_set_phase_timers": ([_P, _P], ctypes.c_int),
     "pd_read_status": ([_P, ctypes.POINTER(_I32), _P], ctypes.c_int),
     "pd_iterations": ([_P, ctypes.POINTER(_I32), ctypes.POINTER(_I32), _P], ctypes.c_int),

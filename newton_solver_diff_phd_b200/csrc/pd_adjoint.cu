@@ -296,14 +296,18 @@ __device__ __forceinline__ bool adjoint_step_body(const AdjointArgs& b, const Te
   const double dt = b.dt;
 
   // ---- Prologue: seed (own rows), local Jacobians (elements).
-  {
+  if (b.mode != 2) {
     double rhs2 = 0.0;
     for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
       V3<double> g;
-      for (int c = 0; c < 3; ++c) {
-        const double velocity = state_load(b.gqd_out, b.state_f64, 3 * i + c) / dt;
-        g[c] = state_load(b.gq_out, b.state_f64, 3 * i + c) + velocity;
-        b.base[3 * i + c] = -velocity;
+      if (b.mode == 1) {
+        g = load3d(b.seed, i);
+      } else {
+        for (int c = 0; c < 3; ++c) {
+          const double velocity = state_load(b.gqd_out, b.state_f64, 3 * i + c) / dt;
+          g[c] = state_load(b.gq_out, b.state_f64, 3 * i + c) + velocity;
+          b.base[3 * i + c] = -velocity;
+        }
       }
       store3(b.rhs, i, g);
       store3(b.solution, i, v3<double>(0.0, 0.0, 0.0));
@@ -312,7 +316,7 @@ __device__ __forceinline__ bool adjoint_step_body(const AdjointArgs& b, const Te
     rhs2 = block_sum(rhs2, s_scratch);
     if (threadIdx.x == 0) my_partials[(kSlotRhs) * team.size] = rhs2;
   }
-  for (int t = gtid; t < b.ne * samples; t += gthreads) {
+  for (int t = b.reuse_jacobian ? b.ne * samples : gtid; t < b.ne * samples; t += gthreads) {
     const int e = t / samples;
     const int s = t % samples;
     double fm[3][3];
@@ -342,7 +346,9 @@ __device__ __forceinline__ bool adjoint_step_body(const AdjointArgs& b, const Te
   double* vector_smem = reinterpret_cast<double*>(dyn_smem + b.vector_smem_offset);
   if (!grid_sync(b.barrier, b.status, team.size, team.rank)) return false;
 
-  if (b.pcg) {
+  if (b.mode == 2) {
+    // Parameters only: the solution buffer already holds z.
+  } else if (b.pcg) {
     // ---- Preconditioned conjugate gradients on (A - K) mu = g over the free
     // rows, preconditioned by the factor A^{-1} = S^T S. The reference's
     // fixed-point step A^{-1}(g + K mu) - mu equals the preconditioned residual
@@ -412,7 +418,7 @@ __device__ __forceinline__ bool adjoint_step_body(const AdjointArgs& b, const Te
               active = 0;
             } else if (k + 1 >= b.max_iterations) {
               active = 0;
-              atomicOr(b.status, kStatusAdjointNotConverged);
+              if (b.mode == 0) atomicOr(b.status, kStatusAdjointNotConverged);
             } else if (!(rho > 0.0) || !isfinite(rho)) {
               // Zero residual (exact solve) or a non-positive preconditioned norm.
               active = 0;
@@ -744,7 +750,7 @@ __device__ __forceinline__ bool adjoint_step_body(const AdjointArgs& b, const Te
             active = 0;
           } else if (k + 1 >= b.max_iterations) {
             active = 0;
-            atomicOr(b.status, kStatusAdjointNotConverged);
+            if (b.mode == 0) atomicOr(b.status, kStatusAdjointNotConverged);
           }
           *b.active = active;
           b.control_d[3] = solution_norm;
@@ -767,8 +773,10 @@ __device__ __forceinline__ bool adjoint_step_body(const AdjointArgs& b, const Te
 
   }
 
+  if (b.mode == 1) return true;  // one Woodbury column in `solution`
+
   // ---- Routing guard (adjoint.py:1125-1138, :226-261), in one serial section.
-  {
+  if (b.mode == 0) {
     unsigned generation;
     if (barrier_arrive(b.barrier, generation, team.size)) {
       reduce_partials(b.partials, kSlotRhs, 1, team.size, s_reduced, s_scratch);
@@ -800,7 +808,7 @@ __device__ __forceinline__ bool adjoint_step_body(const AdjointArgs& b, const Te
   const int diverged = *reinterpret_cast<volatile int*>(b.control_i);
 
   // ---- State gradients (own rows, adjoint.py:474-490).
-  for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+  for (int i = b.mode == 0 ? r0 + threadIdx.x : r1; i < r1; i += blockDim.x) {
     for (int c = 0; c < 3; ++c) {
       const double mu = b.solution[3 * i + c];
       const double injection = routing * b.inertia * mu;
@@ -812,7 +820,7 @@ __device__ __forceinline__ bool adjoint_step_body(const AdjointArgs& b, const Te
 
   // ---- Element epilogue: Dirichlet coupling contributions, material and
   // activation gradients from z = mu (no contact rows).
-  if (b.has_dirichlet) {
+  if (b.has_dirichlet && b.mode == 0) {
     if (diverged) {
       for (int t = gtid; t < b.ne * corners * 3; t += gthreads) b.contrib[t] = 0.0;
     } else {
@@ -921,7 +929,7 @@ __device__ __forceinline__ bool adjoint_step_body(const AdjointArgs& b, const Te
     }
   }
   // Dirichlet gradients: dL/dx_D = g_D - (A - K)_DF mu_F (adjoint.py:524-553).
-  if (b.has_dirichlet) {
+  if (b.has_dirichlet && b.mode == 0) {
     for (int i = gtid; i < n; i += gthreads) {
       if (b.free_[i] != 0) continue;
       const V3<double> coupling = gather_row(b, i);

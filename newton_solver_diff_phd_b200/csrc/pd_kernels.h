@@ -89,6 +89,14 @@ struct AdjointArgs {
   int integrate_pinned;
   int zero_energy_weight;
   double dt, inertia;
+  // Passes of the contact (Woodbury) projection of the parameter gradients:
+  // 0 the whole step; 1 only the fixed point (A - K) w = seed from zero,
+  // capped at max_iterations without a status bit (one column of
+  // W_T = (A - K)^{-1} J^T); 2 only the parameter gradients of the solution
+  // already in `solution` (z), with the divergence flag of the last pass 0.
+  int mode;
+  const double* seed;   // [n][3] right-hand side of mode 1
+  int reuse_jacobian;   // the local Jacobians of x are already in jac64/jac32
 };
 
 // One persistent launch that runs whole rollouts of many instances. The grid

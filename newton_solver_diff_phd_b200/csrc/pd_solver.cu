@@ -873,7 +873,18 @@ int pd_ensure_adjoint_buffers(PdSolver* s) { return ensure_adjoint_buffers(s); }
 int pd_backward(PdSolver* s, const double* x_record, const float* activations, double dt, const void* gq_out,
                 const void* gqd_out, void* gq, void* gqd, void* gf, void* gdirichlet, double* gmaterials,
                 float* gactivations, void* stream) {
+  return pd_backward_contact(s, x_record, activations, dt, gq_out, gqd_out, gq, gqd, gf, gdirichlet, gmaterials,
+                             gactivations, nullptr, nullptr, nullptr, stream);
+}
+
+int pd_backward_contact(PdSolver* s, const double* x_record, const float* activations, double dt, const void* gq_out,
+                        const void* gqd_out, void* gq, void* gqd, void* gf, void* gdirichlet, double* gmaterials,
+                        float* gactivations, const double* multiplier, const double* omega, const double* normal,
+                        void* stream) {
   if (s == nullptr || x_record == nullptr) return fail(PD_ERR_INVALID, "null argument");
+  if ((multiplier != nullptr || omega != nullptr || normal != nullptr) &&
+      (multiplier == nullptr || omega == nullptr || normal == nullptr || !s->has_friction))
+    return fail(PD_ERR_INVALID, "a contact snapshot needs multipliers, omega and normals of a frictional boundary");
   if (!s->built || s->stale || s->built_dt != dt)
     return fail(PD_ERR_STATE, "the backward pass needs the factor of its recorded step (same dt and model)");
   PD_CUDA(cudaSetDevice(s->device));
@@ -901,8 +912,17 @@ int pd_backward(PdSolver* s, const double* x_record, const float* activations, d
   b.dt = dt;
   // A Tet4 step's fibre targets are 1 - u of the activations it used.
   b.activations = (!s->hex && s->has_muscles) ? activations : nullptr;
+  // Parameter gradients with recorded contact rows use z = mu - W_T G^{-1} J mu
+  // (adjoint.py:1141-1145): the full pass leaves them to the projection.
+  const bool woodbury = multiplier != nullptr && s->fc.count > 0 && (b.gmaterials != nullptr || b.gactivations != nullptr);
+  pdb200::AdjointArgs full = b;
+  if (woodbury) {
+    full.gmaterials = nullptr;
+    full.gactivations = nullptr;
+  }
   PD_CUDA(cudaMemsetAsync(s->d_barrier.ptr, 0, sizeof(pdb200::GridBarrier), st));
-  PD_CUDA(pdb200::launch_adjoint_step(b, s->blocks, s->options.precision, s->smem, st));
+  PD_CUDA(pdb200::launch_adjoint_step(full, s->blocks, s->options.precision, s->smem, st));
+  if (woodbury) return pd_woodbury_gradients(s, b, multiplier, omega, normal, st);
   return PD_OK;
 }
 

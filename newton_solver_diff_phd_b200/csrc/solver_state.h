@@ -38,6 +38,13 @@ int pd_evaluate_mesh_contact(PdSolver* s, const void* q, const void* v, int f64,
 // factor; zeroes the multipliers (pd_friction.cu).
 int pd_build_frictional_panel(PdSolver* s);
 }
+// After the full adjoint pass `full` (run without parameter gradients): the
+// Woodbury columns of the recorded contact state and the parameter gradients
+// of z (pd_woodbury.cu).
+int pd_woodbury_gradients(PdSolver* s, const pdb200::AdjointArgs& full, const double* multiplier, const double* omega,
+                          const double* normal, cudaStream_t st);
+extern "C" {
+}
 
 #define PD_CUDA(call)                                                                                 \
   do {                                                                                                \
@@ -137,6 +144,10 @@ struct PdSolver {
       fc_regularization, fc_candidate, fc_multiplier, fc_lambda_t, fc_omega, fc_diagonal, fc_residual, fc_rhs,
       fc_force, fc_response, fc_order, fc_slot, fc_active, fc_matrix, fc_compact, fc_permutation, fc_work,
       fc_surface;
+  // Contact projection of the parameter gradients (pd_woodbury.cu), sized for w_rows rows.
+  int w_rows = 0;
+  DeviceBuffer w_row_node, w_row_vector, w_value, w_selected, w_order, w_control, w_columns, w_gram, w_coefficients,
+      w_permutation, w_work, w_seed, w_mu;
   DeviceBuffer d_wc, d_wv, d_wn, d_wm, d_mdir, d_mtarget;
   DeviceBuffer d_s_off, d_s_col, d_s_val, d_s_val32, d_st_off, d_st_col, d_st_val, d_st_val32, d_s_part, d_st_part;
   DeviceBuffer d_a_off, d_a_col, d_a_val;

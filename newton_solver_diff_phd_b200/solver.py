@@ -734,6 +734,11 @@ class SolverDiffPhD:
         materials = self.model.tet_materials if self._hex is None else self.hex_materials
         # The control's (or model's) tensor is the one whose gradient the user reads.
         activation_source = self._activation_source if activations is not None else None
+        # StepRecord.contact (adjoint.py:834-841): the multipliers, omega and normals the step ended with.
+        contact = None
+        if self._frictional_args is not None and len(self._frictional_args[2]):
+            multiplier, omega, normal, _candidate = self.frictional_state()
+            contact = (multiplier, omega, normal)
 
         def backward():
             if self._factor_key != factor_key or self._model_changed:
@@ -747,17 +752,20 @@ class SolverDiffPhD:
                 activation_grad=_grad(activation_source) if activation_source is not None else None,
                 materials=materials,
                 dirichlet_positions=dirichlet_positions,
+                contact=contact,
             )
 
         tape.record_func(backward, [state_in.particle_q, state_out.particle_q])
 
     def backward_step(self, x_record, dt, state_in, state_out, *, activations=None, activation_grad=None,
-                      materials=None, dirichlet_positions=None):
+                      materials=None, dirichlet_positions=None, contact=None):
         """Backward pass of one recorded step (``adjoint.py:1088-1259``).
 
         Reads ``state_out`` gradients and accumulates into ``state_in`` gradients,
         ``materials.grad[:, :2]`` (float32, as the reference) and the activation
-        and Dirichlet-target gradients when present.
+        and Dirichlet-target gradients when present. ``contact`` is the step's
+        ``(multipliers, omega, normals)`` of the frictional boundary (float64
+        device tensors); parameter gradients then use the contact projection.
         """
         gq_out = _grad(state_out.particle_q)
         gqd_out = _grad(state_out.particle_qd)
@@ -773,8 +781,9 @@ class SolverDiffPhD:
                       and grad.is_contiguous())
             material_grad = grad if direct else torch.zeros((self._element_count, 2), dtype=torch.float64,
                                                             device=self.device)
+        snapshot = (None, None, None) if contact is None else tuple(t.contiguous() for t in contact)
         _lib.check(
-            self._lib.pd_backward(
+            self._lib.pd_backward_contact(
                 self._handle,
                 _lib.ptr(x_record),
                 _lib.ptr(activations),
@@ -787,6 +796,7 @@ class SolverDiffPhD:
                 _lib.ptr(gdirichlet),
                 _lib.ptr(material_grad),
                 _lib.ptr(activation_grad),
+                *(_lib.ptr(t) for t in snapshot),
                 _stream(),
             )
         )

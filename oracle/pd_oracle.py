@@ -389,8 +389,64 @@ def stiffness_matrix(body, x, targets=None, mode="reference"):
     return stiffness_matrix_blocks(body, x, targets, mode).toarray()
 
 
-def backward(body, x_next, dt, dl_dq_next, dl_dv_next, targets=None, mode="reference"):
-    """Dense adjoint of one step: ``mu`` and the gradients of the step inputs and materials."""
+def _backward_tangents(normal):
+    """``_backward_tangents`` (adjoint.py:322-344): Gram-Schmidt from the axis least parallel to n."""
+    axis = 0
+    for d in (1, 2):
+        if abs(normal[d]) < abs(normal[axis]):
+            axis = d
+    unit = np.eye(3)[axis]
+    t1 = unit - (normal @ unit) * normal
+    length = np.sqrt(t1 @ t1)
+    t1 = t1 / length if length > 1.0e-12 else np.array([1.0, 0.0, 0.0])
+    t2 = np.cross(normal, t1)
+    length = np.sqrt(t2 @ t2)
+    t2 = t2 / length if length > 1.0e-12 else np.array([0.0, 1.0, 0.0])
+    return t1, t2
+
+
+def woodbury_projection(operator, free, mu, contact):
+    """``z = mu - W_T G^{-1} (J mu)`` of the contact rows (adjoint.py:347-471, :1272-1354).
+
+    ``contact`` is ``(nodes, multipliers, omega, normals, friction)`` of the
+    forward step. Rows: ``omega n`` of every contact with ``lambda > 0`` and
+    ``omega >= 0.5``, then, with friction, the two tangents of those with
+    ``lambda > 1e-8``; rows with ``|J mu| < max(1e-12, 1e-3 max|J mu|)`` are
+    dropped; the columns ``(A - K)^{-1} J^T`` are solved directly here.
+    """
+    nodes, multiplier, omega, normal, friction = contact
+    n3 = len(mu)
+    rows = []
+    for c, node in enumerate(nodes):
+        if multiplier[c] > 0 and omega[c] >= 0.5:
+            rows.append((node, omega[c] * normal[c]))
+    if friction > 0:
+        for c, node in enumerate(nodes):
+            if multiplier[c] > 0 and omega[c] >= 0.5 and multiplier[c] > 1.0e-8:
+                rows.extend((node, t) for t in _backward_tangents(normal[c]))
+    if not rows:
+        return mu.copy()
+    values = np.array([vector @ mu[3 * node:3 * node + 3] for node, vector in rows])
+    gate = max(1.0e-12, 1.0e-3 * np.abs(values).max())
+    keep = np.abs(values) >= gate
+    rows = [row for row, selected in zip(rows, keep) if selected]
+    values = values[keep]
+    columns = []
+    for node, vector in rows:
+        j = np.zeros(n3)
+        j[3 * node:3 * node + 3] = vector
+        column = np.zeros(n3)
+        column[free] = np.linalg.solve(operator, j[free])
+        columns.append(column)
+    gram = np.array([[vector @ columns[k][3 * node:3 * node + 3] for k in range(len(rows))] for node, vector in rows])
+    gram = np.tril(gram) + np.tril(gram, -1).T
+    alpha = np.linalg.solve(gram, values)
+    return mu - sum(a * column for a, column in zip(alpha, columns))
+
+
+def backward(body, x_next, dt, dl_dq_next, dl_dv_next, targets=None, mode="reference", contact=None):
+    """Dense adjoint of one step: ``mu``, ``z`` and the gradients of the step inputs, materials and
+    (with fibres) the contractions; ``contact`` projects the parameter gradients (:func:`woodbury_projection`)."""
     n = body.n
     free = np.repeat(body.free, 3)
     k_matrix = stiffness_matrix(body, x_next, targets, mode)
@@ -413,7 +469,8 @@ def backward(body, x_next, dt, dl_dq_next, dl_dv_next, targets=None, mode="refer
         unassembled = element_matrix(body, dt) - k_matrix
         coupling[pinned] = (unassembled[np.ix_(pinned, free)] @ mu[free])
         out["dirichlet"] = np.where(pinned, rhs - coupling, 0.0).reshape(-1, 3)
-    z = mu.reshape(-1, 3)
+    z = (mu if contact is None else woodbury_projection(operator, free, mu, contact)).reshape(-1, 3)
+    out["z"] = z
     f = body.deformation(x_next)
     material = np.zeros((len(body.elements), 2))
     for name, weight in body.energies():
@@ -433,6 +490,15 @@ def backward(body, x_next, dt, dl_dq_next, dl_dv_next, targets=None, mode="refer
         else:
             material[:, 0] += 2.0 * value
     out["materials"] = material
+    if body.muscle_directions is not None:
+        # dL/du = sum_k z_k . (w_m / |F m| (m . g_k)) F m (adjoint.py:647-659).
+        m = body.muscle_directions
+        fibre = np.einsum("esij,ej->esi", f, m)
+        length = np.linalg.norm(fibre, axis=-1)
+        mw = body.muscle_stiffness[:, None] * body.sample_volume
+        scale = np.where(length > EPS, mw / np.where(length > EPS, length, 1.0), 0.0)
+        mg = np.einsum("ej,eskj->esk", m, body.gradients)
+        out["activations"] = -np.einsum("eki,esk,es,esi->e", z[body.elements], mg, scale, fibre)
     return out
 
 

@@ -161,12 +161,15 @@ def tet_matrix(oracle, vertices, tets, poses, mu, lame, free, material, dt, musc
 def main():
     parser = argparse.ArgumentParser()
     parser.add_argument("--reference", default="/root/reference")
-    parser.add_argument("--only", choices=("frictional_contact",), default=None,
+    parser.add_argument("--only", choices=("frictional_contact", "woodbury"), default=None,
                         help="regenerate one fixture file and leave the others untouched")
     args = parser.parse_args()
     oracle, sparse, hex_oracle = load_reference(Path(args.reference))
     if args.only == "frictional_contact":
         np.savez_compressed(HERE / "frictional_contact.npz", **frictional_contact_fixture(oracle))
+        return
+    if args.only == "woodbury":
+        np.savez_compressed(HERE / "woodbury.npz", **woodbury_fixture(oracle))
         return
 
     # --- Sparse inverse factors (sparse.py host setup) ------------------------
@@ -320,6 +323,7 @@ def main():
     np.savez_compressed(HERE / "tet_backward.npz", **backward)
     np.savez_compressed(HERE / "mesh_contact.npz", **mesh_contact_fixture(oracle))
     np.savez_compressed(HERE / "frictional_contact.npz", **frictional_contact_fixture(oracle))
+    np.savez_compressed(HERE / "woodbury.npz", **woodbury_fixture(oracle))
     print("wrote", sorted(p.name for p in HERE.glob("*.npz")))
 
 
@@ -460,6 +464,62 @@ def frictional_contact_fixture(oracle):
                                             friction, restitution, radius])
         for key, value in contact_rollout(oracle, step, contact, q, v, gravity, dt, steps, options, nodes).items():
             out[f"{name}__{key}"] = value
+    return out
+
+
+def woodbury_fixture(oracle):
+    """``reference_backward`` with the contact projection after a frictional rollout with fibres
+    (tests/test_diff_phd_adjoint.py:339-416): the grid on a plane, lifted 1 mm, moving at
+    (0.3, 0, -1) m/s; two steps, then the recorded third step and its backward pass."""
+
+    class RecordingContact(oracle.ReferenceContact):
+        """ReferenceContact that also keeps the last iteration's omega (the StepRecord snapshot)."""
+
+        def iterate(self, x, b_full, q):
+            delta = self.gaps(x)
+            s = np.maximum(np.sqrt(delta**2 + self.r**2 * self.multiplier**2), 1.0e-14)
+            self.omega = 1.0 - delta / s
+            return super().iterate(x, b_full, q)
+
+    out = {}
+    dt = 0.004
+    gravity = np.array([0.0, 0.0, -9.81], dtype=np.float32).astype(np.float64)
+    vertices, tets, _ = meshes.tet_grid(3, 2, 2, 0.1, origin=(0.0, 0.0, 1.0))
+    poses = meshes.tet_rest_poses(vertices, tets).astype(np.float32).astype(np.float64)
+    mu = np.full(len(tets), 2.0e4, dtype=np.float32).astype(np.float64)
+    lame = np.full(len(tets), 5.0e4, dtype=np.float32).astype(np.float64)
+    free = np.ones(len(vertices), dtype=bool)
+    nodes = np.unique(surface_faces(tets))
+    for friction in (0.0, 0.5):
+        key = f"f{int(10 * friction)}"
+        rng = np.random.default_rng(31)
+        directions = rng.standard_normal((len(tets), 3))
+        stiffness = np.full(len(tets), 4.0e4)
+        contraction = rng.uniform(0.0, 0.3, len(tets)).astype(np.float32)
+        targets = 1.0 - contraction.astype(np.float64)
+        step = oracle.ReferenceStep(tets, poses, mu, lame, 1000.0, free, "pd", muscle_directions=directions,
+                                    muscle_stiffness=stiffness)
+        contact = RecordingContact("planar", (0.0, 0.0, 1.0, 0.0), nodes, friction=friction)
+        q = vertices.astype(np.float32).astype(np.float64)
+        q[:, 2] += 0.001 - q[:, 2].min()
+        q = q.astype(np.float32).astype(np.float64)
+        v = np.tile(np.array([0.3, 0.0, -1.0], dtype=np.float32), (len(q), 1)).astype(np.float64)
+        for t in range(3):
+            x, _iterations, converged = step.step(q, v, np.zeros_like(q), gravity, dt, contact=contact,
+                                                   targets=targets, **CONTACT_TIGHT)
+            assert converged
+            if t < 2:
+                q, v = x.astype(np.float32).astype(np.float64), ((x - q) / dt).astype(np.float32).astype(np.float64)
+        q_weight = rng.standard_normal((len(q), 3)).astype(np.float32).astype(np.float64)
+        qd_weight = (0.01 * rng.standard_normal((len(q), 3))).astype(np.float32).astype(np.float64)
+        snapshot = (nodes, contact.multiplier.copy(), contact.omega.copy(), contact.normals.copy(), friction)
+        result = oracle.reference_backward(step, x, dt, q_weight, qd_weight, contact=snapshot, targets=targets)
+        out.update({f"{key}__q": q, f"{key}__v": v, f"{key}__x": x, f"{key}__gq": q_weight, f"{key}__gv": qd_weight,
+                    f"{key}__directions": directions, f"{key}__contraction": contraction,
+                    f"{key}__multiplier": snapshot[1], f"{key}__omega": snapshot[2], f"{key}__normal": snapshot[3]})
+        for name, value in result.items():
+            out[f"{key}__out_{name}"] = value
+    out["nodes"] = nodes
     return out
 
 

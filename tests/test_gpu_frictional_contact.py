@@ -190,3 +190,53 @@ def test_invalid_frictional_boundaries_are_rejected():
     ):
         with pytest.raises(ValueError):
             SolverDiffPhD(model, density=DENSITY, **kwargs)
+
+
+@pytest.mark.parametrize("key", ["f0", "f5"])
+def test_contact_woodbury_projection_matches_reference(key):
+    """Parameter gradients through the contact projection (tests/test_diff_phd_adjoint.py:339-416):
+    against the reference's reference_backward outputs and against the oracle on the
+    solver's own recorded contact state; state gradients use mu."""
+    from newton_solver_diff_phd_b200 import Tape
+
+    g = golden("woodbury.npz")
+    friction = 0.5 if key == "f5" else 0.0
+    model = tet_grid_model(fix_left=False, requires_grad=True)
+    directions = g[key + "__directions"]
+    solver = SolverDiffPhD(model, density=DENSITY, frictional_boundary=("planar", (0.0, 0.0, 1.0, 0.0)),
+                           frictional_vertices=g["nodes"], friction=friction, muscle_directions=directions,
+                           muscle_stiffness=4.0e4, max_iterations=2000, abs_tol=1.0e-12, rel_tol=1.0e-11)
+    control = model.control()
+    contraction = g[key + "__contraction"]
+    control.tet_activations = torch.tensor(contraction, device="cuda")
+    control.tet_activations.grad = torch.zeros_like(control.tet_activations)
+    q = model.particle_q.cpu().numpy().astype(np.float64)
+    q[:, 2] += 0.001 - q[:, 2].min()
+    states = [_state(model, q, np.tile([0.3, 0.0, -1.0], (model.particle_count, 1)))]
+    states += [model.state(requires_grad=True) for _ in range(3)]
+    for i in range(2):
+        solver.step(states[i], states[i + 1], control, None, 0.004)
+    state_in, state_out = states[2], states[3]
+    state_in.requires_grad_(True)
+    with Tape() as tape:
+        solver.step(state_in, state_out, control, None, 0.004)
+    np.testing.assert_allclose(solver._x.cpu().numpy(), g[key + "__x"], rtol=0.0, atol=1.0e-8)
+    tape.backward(grads={state_out.particle_q: torch.tensor(g[key + "__gq"], dtype=torch.float32, device="cuda"),
+                         state_out.particle_qd: torch.tensor(g[key + "__gv"], dtype=torch.float32, device="cuda")})
+    solver.check_status()
+    multiplier, omega, normal, _ = solver.frictional_state()
+    assert int((multiplier > 0).sum()) > 0
+    body = oracle_tet_body(model, muscle_directions=directions, muscle_stiffness=np.full(model.tet_count, 4.0e4))
+    oracle = pd_oracle.backward(body, solver._x.cpu().numpy(), 0.004, g[key + "__gq"], g[key + "__gv"],
+                                targets=1.0 - contraction.astype(np.float64),
+                                contact=(g["nodes"], multiplier.cpu().numpy(), omega.cpu().numpy(),
+                                         normal.cpu().numpy(), friction))
+    pairs = (
+        ("q", state_in.particle_q.grad), ("qd", state_in.particle_qd.grad), ("f", state_in.particle_f.grad),
+        ("materials", model.tet_materials.grad[:, :2]), ("activations", control.tet_activations.grad),
+    )
+    for name, tensor in pairs:
+        actual = tensor.detach().cpu().numpy()
+        for expected in (oracle[name], g[f"{key}__out_{name}"]):
+            scale = max(np.abs(expected).max(), 1.0e-30)
+            np.testing.assert_allclose(actual, expected, rtol=0.0, atol=1.0e-5 * scale, err_msg=name)

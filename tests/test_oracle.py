@@ -159,3 +159,24 @@ def test_frictional_boundary_matches_reference_transcription(name):
         if name != "mesh_two_sided":
             tolerance = {"rtol": 1.0e-5, "atol": 1.0e-6} if name.startswith("mesh") else {"rtol": 1.0e-6, "atol": 1.0e-9}
             np.testing.assert_allclose(boundary.multiplier, g[key + "__multiplier"], **tolerance)
+
+
+@pytest.mark.parametrize("key", ["f0", "f5"])
+def test_woodbury_projection_matches_reference_backward(key):
+    """The restated contact projection of the parameter gradients against ``reference_backward``
+    with contact (tests/reference_oracle.py:497-615) after a frictional rollout with fibres."""
+    g = golden("woodbury.npz")
+    vertices, tets, _ = meshes.tet_grid(3, 2, 2, 0.1, origin=(0.0, 0.0, 1.0))
+    poses = meshes.tet_rest_poses(vertices, tets).astype(np.float32).astype(np.float64)
+    mu = np.full(len(tets), 2.0e4, dtype=np.float32).astype(np.float64)
+    lame = np.full(len(tets), 5.0e4, dtype=np.float32).astype(np.float64)
+    body = pd_oracle.Body.tet(tets, poses, np.ones(len(vertices), dtype=bool), mu, lame, 1000.0,
+                              muscle_directions=g[key + "__directions"], muscle_stiffness=np.full(len(tets), 4.0e4))
+    friction = 0.5 if key == "f5" else 0.0
+    contact = (g["nodes"], g[key + "__multiplier"], g[key + "__omega"], g[key + "__normal"], friction)
+    targets = 1.0 - g[key + "__contraction"].astype(np.float64)
+    out = pd_oracle.backward(body, g[key + "__x"], 0.004, g[key + "__gq"], g[key + "__gv"], targets=targets,
+                             contact=contact)
+    for name in ("mu", "z", "q", "qd", "f", "materials", "activations"):
+        reference = g[f"{key}__out_{name}"]
+        np.testing.assert_allclose(out[name], reference, rtol=0.0, atol=1.0e-6 * np.abs(reference).max(), err_msg=name)
