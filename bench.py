@@ -443,11 +443,13 @@ def run_batched(args, device):
     for _, _, solver, _ in family:
         solver.read_status()
     # Batched path: Anderson window and team sizing chosen by the autotuner
-    # from 6-step probe rollouts (untimed).
+    # from 6-step probe rollouts, then team sizes and lanes re-planned from one
+    # measured 25-step rollout (all untimed).
     q0 = torch.cat([m.particle_q for _, m, _, _ in family]).contiguous()
     qd0 = torch.zeros_like(q0)
     forces = torch.cat([f for _, _, _, f in family]).contiguous()
-    batch, tuning = autotune([s for _, _, s, _ in family], BATCH_DT, q0, qd0, forces, steps=6)
+    batch, tuning = autotune([s for _, _, s, _ in family], BATCH_DT, q0, qd0, forces, steps=6,
+                             replan_steps=BATCH_STEPS)
     sizes, grid = batch.team_sizes()
     weight = batch.concat(weights)
     eo = batch.element_offsets
@@ -513,6 +515,7 @@ def run_batched(args, device):
         "precision": precision,
         "schedule": "teams",
         "autotune": tuning["chosen"],
+        "autotune_replan": [p for p in tuning["probes"] if "replan_steps" in p],
         "plain_anderson_window": 5,
         "instances": batch.count,
         "particles": int(batch.particle_count),

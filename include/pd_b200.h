@@ -294,6 +294,16 @@ typedef struct PdBatchOptions {
   int32_t schedule;       /* PD_BATCH_TEAMS (default) or PD_BATCH_PHASES */
   int32_t team_nnz;       /* teams: factor entries of S per block of a team (default 65536) */
   int32_t team_samples;   /* teams: element samples per block of a team (default 512) */
+  /* teams, optional (all three or none): a previous rollout of the same
+     instances measured per instance, [count] each: its duration on its lane
+     [us] (pd_batch_timeline), its total local/global iterations
+     (pd_batch_read) and the team size it ran with (pd_batch_team_sizes).
+     Team sizes and lanes are then planned from these costs: instances whose
+     estimated duration would set the makespan get larger teams, and lanes
+     go to the classes with the longest estimated completion. */
+  const double* measured_us;
+  const int32_t* measured_iterations;
+  const int32_t* measured_team;
 } PdBatchOptions;
 /* options may be NULL (defaults). */
 int pd_batch_create(PdSolver* const* solvers, int32_t count, const PdBatchOptions* options, PdBatch** out);

@@ -82,6 +82,9 @@ class PdBatchOptions(ctypes.Structure):
         ("schedule", ctypes.c_int32),
         ("team_nnz", ctypes.c_int32),
         ("team_samples", ctypes.c_int32),
+        ("measured_us", ctypes.c_void_p),
+        ("measured_iterations", ctypes.c_void_p),
+        ("measured_team", ctypes.c_void_p),
     ]
 
 

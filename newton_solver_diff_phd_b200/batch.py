@@ -47,7 +47,7 @@ class BatchedSolver:
 
     def __init__(self, solvers: list[SolverDiffPhD], dt: float, *, schedule: str = "teams",
                  team_nnz: int = 65536, team_samples: int = 512, svd_warm_start: bool = True,
-                 task_nnz: int = 32768, run_gap: int = 2, local_cells: int = 64):
+                 task_nnz: int = 32768, run_gap: int = 2, local_cells: int = 64, measured=None):
         if not solvers:
             raise ValueError("BatchedSolver needs at least one solver")
         if not np.isfinite(dt) or dt <= 0:
@@ -77,6 +77,16 @@ class BatchedSolver:
         handles = (ctypes.c_void_p * len(solvers))(*[ctypes.cast(s._handle, ctypes.c_void_p).value for s in solvers])
         options = _lib.PdBatchOptions(int(svd_warm_start), int(task_nnz), int(run_gap), int(local_cells),
                                       SCHEDULES[schedule], int(team_nnz), int(team_samples))
+        if measured is not None:
+            # (durations [us], iterations, team sizes) per instance of a previous rollout (measurement()).
+            us, iterations, teams = measured
+            self._measured = (np.ascontiguousarray(us, dtype=np.float64),
+                              np.ascontiguousarray(iterations, dtype=np.int32),
+                              np.ascontiguousarray(teams, dtype=np.int32))
+            if any(len(a) != len(solvers) for a in self._measured):
+                raise ValueError("measured costs need one entry per instance")
+            options.measured_us, options.measured_iterations, options.measured_team = (
+                _lib.ptr(a) for a in self._measured)
         handle = ctypes.c_void_p()
         _lib.check(self._lib.pd_batch_create(ctypes.cast(handles, ctypes.c_void_p), len(solvers), ctypes.byref(options), ctypes.byref(handle)))
         self._handle = handle
@@ -156,6 +166,19 @@ class BatchedSolver:
         adjoint = np.zeros((self.count, 2), np.uint64)
         _lib.check(self._lib.pd_batch_timeline(self._handle, _lib.ptr(forward), _lib.ptr(adjoint), _stream()))
         return forward, adjoint
+
+    def measurement(self):
+        """``(durations [us], iterations, team sizes)`` of every instance in the last forward
+        rollout (plus its last adjoint, when one ran): the ``measured`` costs a re-planned
+        batch of the same instances takes."""
+        forward, adjoint = self.timeline()
+        # The lanes serve both rollouts: the adjoint's time joins the forward's when it ran.
+        us = (forward[:, 1].astype(np.float64) - forward[:, 0].astype(np.float64)) / 1.0e3
+        if np.all(adjoint[:, 1] >= adjoint[:, 0]) and np.any(adjoint[:, 1] > 0):
+            us = us + (adjoint[:, 1].astype(np.float64) - adjoint[:, 0].astype(np.float64)) / 1.0e3
+        _, iterations = self.read()
+        sizes, _ = self.team_sizes()
+        return us, iterations.sum(axis=0).astype(np.int32), sizes
 
     def concat(self, tensors) -> torch.Tensor:
         """Concatenate per-instance ``(n_i, 3)`` tensors into one ``(P, 3)`` state array."""
@@ -243,7 +266,7 @@ def _time_forward(batch, q0, qd0, forces, steps):
 
 
 def autotune(solvers, dt, q0, qd0, forces, *, steps: int = 2, windows=(3, 5, 8),
-             teams=((65536, 512), (32768, 256), (131072, 1024)), **options):
+             teams=((65536, 512), (32768, 256), (131072, 1024)), replan_steps: int = 0, **options):
     """Pick the Anderson window and the team sizing of a batch from short rollouts.
 
     Times a ``steps``-step forward rollout of the batch for every window (with
@@ -251,6 +274,9 @@ def autotune(solvers, dt, q0, qd0, forces, *, steps: int = 2, windows=(3, 5, 8),
     window, and returns ``(BatchedSolver, report)`` built with the fastest
     setting (the solvers keep its window). ``q0``, ``qd0``, ``forces`` are the
     concatenated rollout inputs; the probe runs the rollout's first steps.
+    With ``replan_steps`` > 0 a rollout of that many steps then measures
+    every instance's cost and the batch is re-planned from it (larger teams
+    for the instances on the critical path) when that is faster.
     """
     report = []
     best = None
@@ -276,5 +302,18 @@ def autotune(solvers, dt, q0, qd0, forces, *, steps: int = 2, windows=(3, 5, 8),
         if solver.anderson_window != window:
             solver.set_anderson_window(window)
     batch = BatchedSolver(solvers, dt, team_nnz=team_nnz, team_samples=team_samples, **options)
-    return batch, {"chosen": {"window": window, "team_nnz": team_nnz, "team_samples": team_samples},
-                   "probes": report, "probe_steps": steps}
+    chosen = {"window": window, "team_nnz": team_nnz, "team_samples": team_samples}
+    if replan_steps:
+        # Second stage: one rollout of `replan_steps` steps with the chosen
+        # setting measures every instance's duration and iterations; the batch
+        # is re-planned from those costs when that rollout gets faster.
+        first = _time_forward(batch, q0, qd0, forces, replan_steps)
+        measured = batch.measurement()
+        replanned = BatchedSolver(solvers, dt, team_nnz=team_nnz, team_samples=team_samples, measured=measured,
+                                  **options)
+        second = _time_forward(replanned, q0, qd0, forces, replan_steps)
+        report.append({"replan_steps": replan_steps, "ms": first, "replanned_ms": second})
+        if second < first:
+            batch = replanned
+            chosen["replanned"] = True
+    return batch, {"chosen": chosen, "probes": report, "probe_steps": steps}

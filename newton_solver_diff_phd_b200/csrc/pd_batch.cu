@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <functional>
 #include <cmath>
 #include <memory>
 #include <string>
@@ -962,6 +963,62 @@ int create_phases(PdBatch* batch, const PdBatchOptions& opts) {
 // a share of blocks per class proportional to the class's work (factor
 // entries plus element samples); every solver is planned for its class's
 // team size, and the queues list each class's instances by decreasing work.
+// Completion time of instances with the given durations on `lanes` lanes,
+// longest first, each to the lane that frees first.
+static double lpt_completion(const std::vector<double>& durations, int lanes) {
+  std::vector<double> load(std::max(lanes, 1), 0.0);
+  for (double d : durations) *std::min_element(load.begin(), load.end()) += d;
+  return *std::max_element(load.begin(), load.end());
+}
+
+// Smallest makespan T for which every size class, given just enough lanes
+// that its members (longest first) finish by T, fits the grid; `lanes_out`
+// receives those lane counts in ascending class order.
+template <typename Estimate>
+static double plan_makespan(const std::vector<int>& team_size, Estimate estimate, int grid_cap,
+                            std::vector<int>* lanes_out) {
+  std::vector<int> sizes(team_size);
+  std::sort(sizes.begin(), sizes.end());
+  sizes.erase(std::unique(sizes.begin(), sizes.end()), sizes.end());
+  const int classes = static_cast<int>(sizes.size());
+  std::vector<std::vector<double>> durations(classes);
+  double low = 0.0, high = 0.0;
+  for (size_t i = 0; i < team_size.size(); ++i) {
+    const int c = static_cast<int>(std::lower_bound(sizes.begin(), sizes.end(), team_size[i]) - sizes.begin());
+    const double d = estimate(static_cast<int>(i), team_size[i]);
+    durations[c].push_back(d);
+    low = std::max(low, d);
+    high += d;
+  }
+  for (auto& d : durations) std::sort(d.begin(), d.end(), std::greater<double>());
+  auto lanes_for = [&](double t, std::vector<int>& lanes) {
+    int blocks = 0;
+    for (int c = 0; c < classes; ++c) {
+      const int members = static_cast<int>(durations[c].size());
+      int l = 1;
+      while (l < members && lpt_completion(durations[c], l) > t) ++l;
+      lanes[c] = l;
+      blocks += l * sizes[c];
+    }
+    return blocks;
+  };
+  std::vector<int> lanes(classes, 1);
+  if (lanes_for(low, lanes) <= grid_cap) high = low;
+  for (int it = 0; it < 48 && high > low * (1.0 + 1e-3); ++it) {
+    const double mid = 0.5 * (low + high);
+    if (lanes_for(mid, lanes) <= grid_cap) {
+      high = mid;
+    } else {
+      low = mid;
+    }
+  }
+  if (lanes_out != nullptr) {
+    lanes_out->assign(classes, 1);
+    lanes_for(high, *lanes_out);
+  }
+  return high;
+}
+
 int create_teams(PdBatch* batch, const PdBatchOptions& opts) {
   const int count = batch->count;
   int sms = 0, optin = 0;
@@ -994,6 +1051,47 @@ int create_teams(PdBatch* batch, const PdBatchOptions& opts) {
     batch->team_size[i] = size;
     cost[i] = nnz + 64.0 * samples;
   }
+  const bool measured = opts.measured_us != nullptr && opts.measured_iterations != nullptr &&
+                        opts.measured_team != nullptr;
+  // Measured plan: per-iteration time t(b) = c + (t0 - c) b0 / b on b blocks
+  // from the time t0 per iteration seen on b0 blocks, c the fixed latency of
+  // an iteration (barriers, serial sections); estimated duration = iterations
+  // x t(b), work = duration x b block-us.
+  std::vector<double> per_iteration(count, 0.0), iterations(count, 0.0), measured_team(count, 1.0);
+  auto estimate = [&](int i, int b) {
+    constexpr double kFixedUs = 40.0;
+    const double t0 = per_iteration[i];
+    const double scalable = std::max(t0 - kFixedUs, 0.0) * measured_team[i] / b;
+    return iterations[i] * (std::min(t0, kFixedUs) + scalable);
+  };
+  if (measured) {
+    for (int i = 0; i < count; ++i) {
+      iterations[i] = std::max(1, opts.measured_iterations[i]);
+      measured_team[i] = std::max(1, opts.measured_team[i]);
+      per_iteration[i] = std::max(opts.measured_us[i], 0.0) / iterations[i];
+      int size = 1;
+      while (size < std::min(largest, opts.measured_team[i])) size *= 2;
+      batch->team_size[i] = size;
+    }
+    // Team sizes by a greedy descent on the planned makespan: double the
+    // team of the instance with the longest estimated duration while that
+    // shortens the plan (plan_makespan below).
+    for (int guard = 0; guard < count; ++guard) {
+      const double current = plan_makespan(batch->team_size, estimate, grid_cap, nullptr);
+      int worst = -1;
+      for (int i = 0; i < count; ++i) {
+        if (batch->team_size[i] >= largest) continue;
+        if (worst < 0 || estimate(i, batch->team_size[i]) > estimate(worst, batch->team_size[worst])) worst = i;
+      }
+      if (worst < 0) break;
+      batch->team_size[worst] *= 2;
+      if (!(plan_makespan(batch->team_size, estimate, grid_cap, nullptr) < current)) {
+        batch->team_size[worst] /= 2;
+        break;
+      }
+    }
+    for (int i = 0; i < count; ++i) cost[i] = estimate(i, batch->team_size[i]);
+  }
   // Classes present, ascending size. A class whose share of the grid (by
   // work) is smaller than one of its teams moves down to half the size, so
   // that no class with much work is left with a single serial lane.
@@ -1017,7 +1115,7 @@ int create_teams(PdBatch* batch, const PdBatchOptions& opts) {
       total += cost[i];
     }
     int shrink = -1;
-    for (int c = classes - 1; c >= 0; --c) {
+    for (int c = measured ? -1 : classes - 1; c >= 0; --c) {
       const double share = grid_cap * work[c] / total;
       if (sizes[c] > 1 && share < 2.0 * sizes[c] && members[c] > 1) {
         shrink = sizes[c];
@@ -1040,6 +1138,12 @@ int create_teams(PdBatch* batch, const PdBatchOptions& opts) {
     return blocks;
   };
   if (used() > grid_cap) return pd_set_error(PD_ERR_UNSUPPORTED, "the team classes do not fit the co-resident grid");
+  if (measured) {
+    std::vector<int> planned;
+    plan_makespan(batch->team_size, estimate, grid_cap, &planned);
+    for (int c = 0; c < classes; ++c) teams[c] = planned[c];
+    if (used() > grid_cap) return pd_set_error(PD_ERR_UNSUPPORTED, "the measured plan does not fit the co-resident grid");
+  }
   // Add lanes where a class's share of the grid is furthest below its share of the work.
   for (;;) {
     int best = -1;

@@ -283,3 +283,24 @@ def test_autotune_picks_a_probed_setting():
     q, qd, x = batch.rollout(q0, torch.zeros_like(q0), forces, STEPS)
     status, _ = batch.read()
     assert np.all(status == 0)
+
+
+def test_measured_replan_keeps_the_results():
+    """A batch planned from a previous rollout's measured costs (team sizes and
+    lanes) solves the same problems: single-instance results within 1e-6."""
+    plain = [_plain(*inst) for inst in _instances("fp64")]
+    instances = _instances("fp64")
+    batch, q, _, _, status, _ = _batched(instances, team_nnz=2048, team_samples=64)
+    us, iterations, teams = batch.measurement()
+    assert us.shape == iterations.shape == teams.shape == (len(instances),)
+    assert np.all(us > 0) and np.all(iterations >= STEPS)
+    replanned, q2, _, _, status2, _ = _batched(instances, team_nnz=2048, team_samples=64,
+                                               measured=(us, iterations, teams))
+    sizes, grid = replanned.team_sizes()
+    assert np.all(status2 == 0) and grid >= 1
+    assert np.all((sizes & (sizes - 1)) == 0) and np.all(sizes <= 64)
+    for i, (trajectory, _) in enumerate(plain):
+        scale = float(trajectory.abs().max())
+        assert float((replanned.split(q2)[i] - trajectory).abs().max()) <= 1e-6 * scale
+    with pytest.raises(ValueError):
+        BatchedSolver([s for _, s, _ in instances], DT, measured=(us[:2], iterations, teams))
