@@ -411,6 +411,48 @@ def build_all(solvers, dt):
         list(pool.map(lambda s: s._build(dt), solvers))
 
 
+def precision_check(device, stride=16, steps=3):
+    """Batched fp32+refine against batched fp64 on every `stride`-th instance of the family, both
+    converged to rel 1e-11: the position and dL/dE error of the arithmetic alone (at the bench's
+    rel 1e-6 both paths stop wherever the slow instances' step rule lets them)."""
+    import torch
+
+    from newton_solver_diff_phd_b200 import SolverDiffPhD
+    from newton_solver_diff_phd_b200.batch import BatchedSolver
+    from newton_solver_diff_phd_b200.scenes import cantilever_family, cantilever_model
+
+    specs = cantilever_family(BATCH_COUNT, seed=0)[::stride]
+    results = {}
+    for precision in ("fp64", "fp32+refine"):
+        solvers, models, forces = [], [], []
+        for spec in specs:
+            model, mesh, materials, force = cantilever_model(spec, device=device)
+            solvers.append(SolverDiffPhD(model, density=1000.0, hex_mesh=mesh, hex_materials=materials,
+                                         precision=precision, anderson_window=5, rel_tol=1.0e-11, abs_tol=1.0e-14,
+                                         max_iterations=20000, adjoint="exact"))
+            models.append(model)
+            forces.append(torch.as_tensor(force, device=device))
+        build_all(solvers, BATCH_DT)
+        batch = BatchedSolver(solvers, BATCH_DT)
+        q0 = batch.concat([m.particle_q for m in models])
+        q, _, x = batch.rollout(q0, torch.zeros_like(q0), batch.concat(forces), steps)
+        rng = np.random.default_rng(2)
+        weight = torch.as_tensor(rng.standard_normal((batch.particle_count, 3)), dtype=torch.float32, device=device)
+        _, _, _, gm, _ = batch.backward(x, weight)
+        status, _ = batch.read()
+        eo = batch.element_offsets
+        grad = [gm[eo[i]:eo[i + 1]].double().cpu().numpy() for i in range(batch.count)]
+        results[precision] = ([t.double().cpu().numpy() for t in batch.split(x[-1])], grad, (status & 1) == 0)
+    x64, g64, ok64 = results["fp64"]
+    x32, g32, ok32 = results["fp32+refine"]
+    ok = ok64 & ok32
+    pos = [float(np.abs(a - b).max() / np.abs(b).max()) for a, b, k in zip(x32, x64, ok) if k]
+    grad = [float(np.abs(a - b).max() / np.abs(b).max()) for a, b, k in zip(g32, g64, ok) if k]
+    return {"instances": len(specs), "converged_both": int(ok.sum()), "steps": steps, "rel_tol": 1.0e-11,
+            "max_rel_position_err_fp32_refine_vs_fp64": max(pos) if pos else None,
+            "max_rel_grad_mu_lambda_err_fp32_refine_vs_fp64": max(grad) if grad else None}
+
+
 def run_batched(args, device):
     """Batched vs plain on the uneven cantilever family (forward + adjoint w.r.t. every instance's E)."""
     import torch
@@ -500,6 +542,9 @@ def run_batched(args, device):
     torch.cuda.synchronize()
     e2e_ms = start.elapsed_time(end)
     steps_total = batch.count * BATCH_STEPS
+    instances, particles = batch.count, int(batch.particle_count)
+    del batch
+    precision = precision_check(device)
     return {
         "workload": BATCH_WORKLOAD,
         "metric": "instance PD steps/s (forward + adjoint w.r.t. every instance's E)",
@@ -512,13 +557,14 @@ def run_batched(args, device):
         "forward_ms": fwd_ms,
         "adjoint_ms": adj_ms,
         "plain_ms": plain_ms,
-        "precision": precision,
+        "precision": "fp32+refine",
+        "precision_check": precision,
         "schedule": "teams",
         "autotune": tuning["chosen"],
         "autotune_replan": [p for p in tuning["probes"] if "replan_steps" in p],
         "plain_anderson_window": 5,
-        "instances": batch.count,
-        "particles": int(batch.particle_count),
+        "instances": instances,
+        "particles": particles,
         "team_sizes": {str(int(k)): int(v) for k, v in zip(*np.unique(sizes, return_counts=True))},
         "grid_blocks": int(grid),
         "forward_iterations": int(forward_its.sum()),
