@@ -453,6 +453,45 @@ def precision_check(device, stride=16, steps=3):
             "max_rel_grad_mu_lambda_err_fp32_refine_vs_fp64": max(grad) if grad else None}
 
 
+def family_cpu_baseline(instances=32, steps=1):
+    """The CPU port on the first `instances` instances of the cantilever family (first `steps` steps
+    forward then adjoint each), one process per core side by side (spawned, numpy single-threaded
+    each): instance PD steps per second of wall time."""
+    import multiprocessing
+
+    import scipy.sparse as sp
+
+    from newton_solver_diff_phd_b200 import _lib, meshes
+    from newton_solver_diff_phd_b200.scenes import cantilever_family
+    from oracle import pd_oracle
+    from oracle.sparse_port import time_hex_instance
+
+    jobs = []
+    for spec in cantilever_family(BATCH_COUNT, seed=0)[:instances]:
+        vertices, hexes, _ = meshes.hex_grid(spec.nx, spec.ny, spec.nz, 0.01)
+        free = vertices[:, 0] > 1.0e-12
+        mu, lame = meshes.lame_from_young(np.full(len(hexes), spec.young), spec.poisson)
+        body = pd_oracle.Body.hex(vertices, hexes, free, mu, lame, 1000.0)
+        csr = sp.csr_matrix(body.matrix(BATCH_DT))
+        factor = _lib.inverse_factor((csr.indptr, csr.indices, csr.data))
+        tip = np.flatnonzero(np.abs(vertices[:, 0] - spec.nx * 0.01) <= 1.0e-12)
+        forces = np.zeros_like(vertices)
+        forces[tip, 0] = np.asarray(spec.tip_forces)[: len(tip)]
+        jobs.append((vertices, hexes, free, mu, lame, forces, factor, BATCH_DT, steps))
+    workers = max(1, min(16, os.cpu_count() or 1, len(jobs)))
+    for name in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[name] = "1"
+    # Largest first, so that the pool's wall time is not one long job started last.
+    jobs.sort(key=lambda job: -len(job[0]))
+    start = time.perf_counter()
+    with multiprocessing.get_context("spawn").Pool(workers) as pool:
+        done = pool.map(time_hex_instance, jobs, chunksize=1)
+    wall = time.perf_counter() - start
+    return {"value": sum(n for _, n in done) / wall, "unit": "instance PD steps/s", "cores": workers, "kind": "port",
+            "sample": f"first {steps} step(s) forward then adjoint of the family's first {len(jobs)} instances, "
+                      f"oracle/sparse_port.py, {workers} processes side by side (wall {wall:.1f} s)"}
+
+
 def run_batched(args, device):
     """Batched vs plain on the uneven cantilever family (forward + adjoint w.r.t. every instance's E)."""
     import torch
@@ -545,12 +584,15 @@ def run_batched(args, device):
     instances, particles = batch.count, int(batch.particle_count)
     del batch
     precision = precision_check(device)
+    cpu = family_cpu_baseline()
     return {
         "workload": BATCH_WORKLOAD,
         "metric": "instance PD steps/s (forward + adjoint w.r.t. every instance's E)",
         "value": steps_total / (batched_ms / 1000.0),
         "plain_value": steps_total / (plain_ms / 1000.0),
         "batched_vs_plain": plain_ms / batched_ms,
+        "cpu_baseline": cpu,
+        "batched_vs_cpu": (steps_total / (batched_ms / 1000.0)) / cpu["value"],
         "e2e": {"value": steps_total / (e2e_ms / 1000.0), "h2d_bytes_per_step": int(sum(v.numel() * v.element_size()
                                                                                          for v in host.values())),
                 "d2h_bytes_per_step": int(out_grad.numel() * 8)},

@@ -120,3 +120,29 @@ class SparsePort:
             value = -np.einsum("eki,esij,eskj,es->e", solution[body.elements], stress, body.gradients, body.sample_volume)
             material[:, 1 if name == "volume" else 0] += value if name == "volume" else 2.0 * value
         return solution, material, iteration + 1
+
+
+def time_hex_instance(job):
+    """Forward steps then their exact-mode adjoints of one Hex8 instance with this port; returns
+    ``(seconds, steps)``. ``job`` is ``(vertices, hexes, free, mu, lame, forces, factor, dt, steps)``
+    (picklable, so a process pool can run instances side by side)."""
+    import time
+
+    vertices, hexes, free, mu, lame, forces, factor, dt, steps = job
+    body = pd_oracle.Body.hex(vertices, hexes, free, mu, lame, 1000.0)
+    port = SparsePort(body, factor, dt)
+    q = np.asarray(vertices, dtype=np.float64).copy()
+    v = np.zeros_like(q)
+    start = time.perf_counter()
+    records = []
+    for _ in range(steps):
+        x, _, _ = port.step(q, v, forces, np.zeros(3), max_iterations=5000, abs_tol=1.0e-9, rel_tol=1.0e-6)
+        records.append(x)
+        v = (x - q) / dt
+        q = x
+    seed = np.ones_like(q)
+    for x in reversed(records):
+        mu_adj, _, _ = port.backward(x, seed, np.zeros_like(seed), max_iterations=5000, abs_tol=1.0e-9,
+                                     rel_tol=1.0e-6, mode="exact")
+        seed = body.mass / dt**2 * mu_adj
+    return time.perf_counter() - start, steps
