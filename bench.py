@@ -330,6 +330,8 @@ def run_b200(args):
         result["cpu_baseline"] = cpu_baseline(args, seconds=args.cpu_seconds)
         if world == 1 and not args.no_batched:
             result["batched"] = run_batched(args, device)
+        if world == 1 and not args.no_contact:
+            result["contact"] = run_contact(args, device)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -623,6 +625,92 @@ def run_batched(args, device):
     }
 
 
+def run_contact(args, device):
+    """The Tet4 contact workload (a 20x20x10 block of 1 mm cubes, 20,000 Tet4, on a frictional
+    plane, poked by a meshed probe through the penalty mesh contact): the first `contact_steps`
+    of its 200-step rollout forward, their state adjoint, and the contact projection of dL/d(mu,
+    lambda) for the last step. The rollout is cut short so the leg stays within seconds."""
+    import torch
+
+    from newton_solver_diff_phd_b200 import SolverDiffPhD, Tape
+    from newton_solver_diff_phd_b200.scenes import Poke, poke_scene
+
+    spec = Poke(offset=(0.0, 0.0))
+    steps = min(args.contact_steps, spec.steps)
+    model, opt = poke_scene(spec, device=device)
+    solver = SolverDiffPhD(model, density=spec.density, frictional_boundary=opt["frictional_boundary"],
+                           frictional_vertices=opt["frictional_vertices"], mesh_contact=opt["mesh_contact"],
+                           max_iterations=5000, rel_tol=REL_TOL, abs_tol=ABS_TOL)
+    dirichlet = torch.as_tensor(opt["dirichlet"], device=device)
+    rng = np.random.default_rng(0)
+    chosen = rng.choice(np.unique(opt["surface"]), 64, replace=False)
+    seed = torch.zeros((model.particle_count, 3), dtype=torch.float32, device=device)
+    seed[chosen] = torch.as_tensor(rng.standard_normal((64, 3)), dtype=torch.float32, device=device)
+    stream = torch.cuda.current_stream()
+    # Warm-up: the factor build, the panel of the plane's vertices and one step.
+    warm_in, warm_out = model.state(), model.state()
+    solver.step(warm_in, warm_out, None, None, spec.dt, dirichlet_positions=dirichlet[0])
+    torch.cuda.synchronize()
+    solver.read_status()
+    states = [model.state(requires_grad=True) for _ in range(steps + 1)]
+    iterations, active, pairs = [], [], []
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    forward_ms = 0.0
+    with Tape() as tape:
+        for t in range(steps):
+            e0.record(stream)
+            solver.step(states[t], states[t + 1], None, None, spec.dt, dirichlet_positions=dirichlet[t])
+            e1.record(stream)
+            torch.cuda.synchronize()
+            forward_ms += e0.elapsed_time(e1)
+            iterations.append(int(solver.iterations[0]))
+            active.append(int((solver.contact_multipliers > 0).sum()))
+            pairs.append(solver.mesh_contact_pairs)
+    forward_status = solver.read_status()
+    e0.record(stream)
+    tape.backward(grads={states[-1].particle_q: seed})
+    e1.record(stream)
+    torch.cuda.synchronize()
+    adjoint_ms = e0.elapsed_time(e1)
+    adjoint_status = solver.read_status()
+    # Parameter gradients of the last step through the contact projection.
+    model.tet_materials.requires_grad_(True)
+    model.tet_materials.grad = torch.zeros_like(model.tet_materials)
+    last_in, last_out = model.state(requires_grad=True), model.state(requires_grad=True)
+    with torch.no_grad():
+        last_in.particle_q.copy_(states[-2].particle_q)
+        last_in.particle_qd.copy_(states[-2].particle_qd)
+    with Tape() as tape:
+        solver.step(last_in, last_out, None, None, spec.dt, dirichlet_positions=dirichlet[steps - 1])
+    rows = int((solver.contact_multipliers > 0).sum())
+    e1.record(stream)
+    tape.backward(grads={last_out.particle_q: seed})
+    e2.record(stream)
+    torch.cuda.synchronize()
+    woodbury_ms = e1.elapsed_time(e2)
+    total_iterations = int(sum(iterations))
+    return {
+        "workload": "tet4_poke_block_20x20x10_plane_probe",
+        "steps": steps,
+        "forward_ms_per_step": forward_ms / steps,
+        "forward_us_per_iteration": 1000.0 * forward_ms / max(total_iterations, 1),
+        "forward_iterations": iterations,
+        "steps_at_iteration_limit": int(sum(1 for i in iterations if i >= 5000)),
+        "plane_contacts_active": active,
+        "probe_pairs": pairs,
+        "state_adjoint_ms_per_step": adjoint_ms / steps,
+        "woodbury_last_step_ms": woodbury_ms,
+        "woodbury_contact_rows_active": rows,
+        "status_forward": forward_status,
+        "status_adjoint": adjoint_status,
+        "config": {"particles": model.particle_count, "tets": model.tet_count, "plane_vertices": 441,
+                   "probe": "icosphere r 3 mm (162 surface particles), prescribed 4 mm descent over 200 steps",
+                   "mesh_contact": "radius 0.55 mm, kn 5e3 N/m, kf 50 N s/m, mu 0.5", "dt": spec.dt,
+                   "rel_tol": REL_TOL, "precision": "fp64", "adjoint": "reference"},
+        "data": "synthetic (block and probe built in scenes.poke_scene)",
+    }
+
+
 def cpu_sample(steps, threads):
     """Time the CPU port on the first `steps` PD steps (forward then adjoint); returns (seconds, steps)."""
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
@@ -705,6 +793,8 @@ def main():
     parser.add_argument("--precision", choices=["fp64", "fp32+refine"], default="fp64")
     parser.add_argument("--cpu-seconds", type=float, default=20.0)
     parser.add_argument("--no-batched", action="store_true", help="skip the batched-vs-plain cantilever family leg")
+    parser.add_argument("--no-contact", action="store_true", help="skip the Tet4 contact (poke) leg")
+    parser.add_argument("--contact-steps", type=int, default=30, help="steps of the contact leg's rollout")
     parser.add_argument("--no-extras", action="store_true",
                         help="skip the e2e, CPU-baseline and per-launch timing legs (profiling runs)")
     args = parser.parse_args()

@@ -9,9 +9,10 @@
 // correction of particle i reads one contiguous row; B = P[nodes] is [K][K].
 // Frames, Delassus matrix W_ij = (n_i . n_j) B_ij and the regularisation are
 // frozen at the step start. The Newton section (compaction, response, right
-// hand side, coupled block, LDL^T, multiplier and friction updates) runs in
-// one block between two team barriers; K is the number of registered
-// vertices (the floor face of a block: hundreds).
+// hand side, coupled block and its factorisation, multiplier and friction
+// updates) runs in one block between two team barriers for up to
+// kTeamContacts registered vertices, and spread over the team with a blocked
+// Cholesky for more (the floor face of a block: hundreds).
 #pragma once
 
 #include <cfloat>
@@ -470,6 +471,337 @@ __device__ inline void fb_newton(const StepArgs& a) {
     __syncthreads();
   }
   fb_forces(f, true);
+}
+
+// ---------------------------------------------------------------------------
+// The same Newton step spread over the whole team, for large contact sets
+// (more than kTeamContacts registered vertices): every per-contact and
+// per-entry loop is distributed over the team's blocks, and the coupled
+// block, symmetric positive definite (contact.py:33-39), is factorised by a
+// right-looking Cholesky in 32-wide panels: one warp factors the diagonal
+// tile in shared memory, the team solves the panel below (a warp per row)
+// and updates the trailing lower triangle (a thread per entry), with a team
+// barrier between the three.
+
+constexpr int kTeamContacts = 32;
+constexpr int kPanel = 32;
+
+__device__ __forceinline__ int team_warp(const Team team) { return team.rank * kWarps + (threadIdx.x >> 5); }
+
+// Scalars at the iterate, one warp per contact over the team.
+__device__ inline void fb_scalars_team(const StepArgs& a, const Team team) {
+  const FrictionArgs& f = a.fc;
+  const int lane = threadIdx.x & 31;
+  for (int c = team_warp(team); c < f.count; c += team.size * kWarps) {
+    const int node = f.nodes[c];
+    double delta = 0.0, omega = 0.0, e = 1.0, phi = 0.0;
+    if (f.candidate[c] != 0) {
+      const V3<double> p = load3d(a.prev, node);
+      if (f.kind == kBoundaryMesh) {
+        V3<double> closest, face_normal;
+        double dist2;
+        fb_mesh_closest(f, p, node, a.prev, closest, face_normal, dist2);
+        delta = dot(p - closest, load3d(f.normal, c)) - f.radius;
+      } else {
+        delta = fb_gap(f, p);
+      }
+      fb_complementarity(delta, f.multiplier[c], f.regularization[c], omega, e, phi);
+    }
+    if (lane == 0) {
+      f.omega[c] = omega;
+      f.diagonal[c] = e;
+      f.residual[c] = phi;
+    }
+  }
+}
+
+// Ordered compaction of omega != 0 and the current forces, by one block.
+__device__ inline void fb_compact_block(const FrictionArgs& f) {
+  __shared__ int s_warp_count[kWarps];
+  __shared__ int s_base;
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) s_base = 0;
+  __syncthreads();
+  for (int start = 0; start < f.count; start += blockDim.x) {
+    const int c = start + threadIdx.x;
+    const bool flag = c < f.count && f.omega[c] != 0.0;
+    const unsigned ballot = __ballot_sync(0xffffffffu, flag);
+    if (lane == 0) s_warp_count[warp] = __popc(ballot);
+    __syncthreads();
+    int offset = s_base;
+    for (int w = 0; w < warp; ++w) offset += s_warp_count[w];
+    offset += __popc(ballot & ((1u << lane) - 1u));
+    if (c < f.count) {
+      f.slot[c] = flag ? offset : -1;
+      if (flag) f.order[offset] = c;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int total = 0;
+      for (int w = 0; w < kWarps; ++w) total += s_warp_count[w];
+      s_base += total;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *f.active = s_base;
+  fb_forces(f, true);
+}
+
+__device__ inline void fb_forces_team(const FrictionArgs& f, const Team team, bool tangential) {
+  for (int c = team.rank * blockDim.x + threadIdx.x; c < f.count; c += team.size * blockDim.x) {
+    const double scale = f.omega[c] * f.multiplier[c];
+    V3<double> value = scale * load3d(f.normal, c);
+    if (tangential)
+      value = value + f.lambda_t[2 * c] * load3d(f.tangent1, c) + f.lambda_t[2 * c + 1] * load3d(f.tangent2, c);
+    store3(f.force, c, value);
+  }
+}
+
+__device__ inline void fb_response_team(const FrictionArgs& f, const Team team, int active) {
+  const int lane = threadIdx.x & 31;
+  for (int c = team_warp(team); c < f.count; c += team.size * kWarps) {
+    const double* row = f.block + static_cast<long long>(c) * f.count;
+    double rx = 0.0, ry = 0.0, rz = 0.0;
+#pragma unroll 4
+    for (int k = lane; k < active; k += 32) {
+      const int j = f.order[k];
+      const double b = row[j];
+      rx += b * f.force[3 * j];
+      ry += b * f.force[3 * j + 1];
+      rz += b * f.force[3 * j + 2];
+    }
+    rx = warp_sum(rx);
+    ry = warp_sum(ry);
+    rz = warp_sum(rz);
+    if (lane == 0) store3(f.response, c, v3<double>(rx, ry, rz));
+  }
+}
+
+// Right-hand side per contact and the lower triangle of Omega W Omega + E.
+__device__ inline void fb_system_team(const StepArgs& a, const Team team, int active) {
+  const FrictionArgs& f = a.fc;
+  const int gtid = team.rank * blockDim.x + threadIdx.x;
+  const int gthreads = team.size * blockDim.x;
+  for (int c = gtid; c < f.count; c += gthreads) {
+    const int node = f.nodes[c];
+    const V3<double> n = load3d(f.normal, c);
+    const V3<double> point = load3d(a.prev, node);
+    const V3<double> solved = v3<double>(fb_solved(a, node, 0), fb_solved(a, node, 1), fb_solved(a, node, 2));
+    f.rhs[c] = -f.residual[c] + f.omega[c] * dot(n, point) - f.omega[c] * dot(n, solved + load3d(f.response, c));
+  }
+  const long long entries = static_cast<long long>(active) * active;
+  for (long long t = gtid; t < entries; t += gthreads) {
+    const int i = static_cast<int>(t / active), j = static_cast<int>(t % active);
+    if (j > i) continue;
+    const int p = f.order[i], q = f.order[j];
+    double value = f.omega[p] * f.delassus[static_cast<long long>(p) * f.count + q] * f.omega[q];
+    if (i == j) value += f.diagonal[p];
+    f.matrix[static_cast<long long>(i) * f.count + j] = value;
+  }
+}
+
+// In-place Cholesky of the lower triangle of m[:n, :n] (leading dimension
+// ld) by the team. Returns false when a team barrier gave up.
+__device__ inline bool fb_cholesky_team(const StepArgs& a, const Team team, double* m, int ld, int n,
+                                        double* tile /* shared [kPanel * (kPanel + 1)] */) {
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  auto at = [&](int i, int j) -> double& { return m[static_cast<long long>(i) * ld + j]; };
+  for (int c0 = 0; c0 < n; c0 += kPanel) {
+    const int w = min(kPanel, n - c0);
+    if (team.rank == 0 && warp == 0) {
+      // Diagonal tile: lane r owns row r.
+      for (int r = 0; r < w; ++r)
+        if (lane <= r) tile[r * (kPanel + 1) + lane] = at(c0 + r, c0 + lane);
+      __syncwarp();
+      for (int k = 0; k < w; ++k) {
+        double d = tile[k * (kPanel + 1) + k];
+        d = d > 0.0 ? sqrt(d) : sqrt(DBL_MIN);
+        __syncwarp();
+        if (lane == k) tile[k * (kPanel + 1) + k] = d;
+        if (lane > k && lane < w) tile[lane * (kPanel + 1) + k] /= d;
+        __syncwarp();
+        if (lane > k && lane < w) {
+          const double lk = tile[lane * (kPanel + 1) + k];
+          for (int c = k + 1; c <= lane; ++c) tile[lane * (kPanel + 1) + c] -= lk * tile[c * (kPanel + 1) + k];
+        }
+        __syncwarp();
+      }
+      for (int r = 0; r < w; ++r)
+        if (lane <= r) at(c0 + r, c0 + lane) = tile[r * (kPanel + 1) + lane];
+    }
+    if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
+    if (c0 + w >= n) break;
+    // Panel below: L_ip = M_ip L_pp^-T, a warp per row.
+    for (int r = threadIdx.x; r < w * w; r += blockDim.x) {
+      const int i = r / w, j = r % w;
+      if (j <= i) tile[i * (kPanel + 1) + j] = at(c0 + i, c0 + j);
+    }
+    __syncthreads();
+    for (int row = c0 + w + team_warp(team); row < n; row += team.size * kWarps) {
+      double v = lane < w ? at(row, c0 + lane) : 0.0;
+      for (int j = 0; j < w; ++j) {
+        const double x = __shfl_sync(0xffffffffu, v, j) / tile[j * (kPanel + 1) + j];
+        if (lane == j) v = x;
+        if (lane > j && lane < w) v -= x * tile[lane * (kPanel + 1) + j];
+      }
+      if (lane < w) at(row, c0 + lane) = v;
+    }
+    if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
+    // Trailing lower triangle: M_ij -= L_ip . L_jp.
+    const int t0 = c0 + w, rest = n - t0;
+    const long long entries = static_cast<long long>(rest) * rest;
+    for (long long t = static_cast<long long>(team.rank) * blockDim.x + threadIdx.x; t < entries;
+         t += static_cast<long long>(team.size) * blockDim.x) {
+      const int i = t0 + static_cast<int>(t / rest), j = t0 + static_cast<int>(t % rest);
+      if (j > i) continue;
+      const double* li = m + static_cast<long long>(i) * ld + c0;
+      const double* lj = m + static_cast<long long>(j) * ld + c0;
+      double sum = 0.0;
+#pragma unroll 8
+      for (int l = 0; l < w; ++l) sum += li[l] * lj[l];
+      at(i, j) -= sum;
+    }
+    if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
+  }
+  return true;
+}
+
+// L L^T x = rhs on the factor from fb_cholesky_team, by one block: panel by
+// panel, the off-panel part by a warp per row, the tile by warp 0.
+__device__ inline void fb_cholesky_solve_block(const double* m, int ld, int n, double* x,
+                                               double* tile /* shared [kPanel * (kPanel + 1)] */) {
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  auto at = [&](int i, int j) -> double { return m[static_cast<long long>(i) * ld + j]; };
+  auto load_tile = [&](int c0, int w) {
+    for (int r = threadIdx.x; r < w * w; r += blockDim.x) {
+      const int i = r / w, j = r % w;
+      if (j <= i) tile[i * (kPanel + 1) + j] = at(c0 + i, c0 + j);
+    }
+  };
+  for (int c0 = 0; c0 < n; c0 += kPanel) {
+    const int w = min(kPanel, n - c0);
+    load_tile(c0, w);
+    for (int r = c0 + warp; r < c0 + w; r += kWarps) {
+      double sum = 0.0;
+      for (int c = lane; c < c0; c += 32) sum += at(r, c) * x[c];
+      sum = warp_sum(sum);
+      if (lane == 0) x[r] -= sum;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      double v = lane < w ? x[c0 + lane] : 0.0;
+      for (int j = 0; j < w; ++j) {
+        const double y = __shfl_sync(0xffffffffu, v, j) / tile[j * (kPanel + 1) + j];
+        if (lane == j) v = y;
+        if (lane > j && lane < w) v -= y * tile[lane * (kPanel + 1) + j];
+      }
+      if (lane < w) x[c0 + lane] = v;
+    }
+    __syncthreads();
+  }
+  for (int c0 = ((n - 1) / kPanel) * kPanel; c0 >= 0; c0 -= kPanel) {
+    const int w = min(kPanel, n - c0);
+    load_tile(c0, w);
+    for (int r = c0 + warp; r < c0 + w; r += kWarps) {
+      double sum = 0.0;
+      for (int c = c0 + w + lane; c < n; c += 32) sum += at(c, r) * x[c];
+      sum = warp_sum(sum);
+      if (lane == 0) x[r] -= sum;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      double v = lane < w ? x[c0 + lane] : 0.0;
+      for (int j = w - 1; j >= 0; --j) {
+        const double y = __shfl_sync(0xffffffffu, v, j) / tile[j * (kPanel + 1) + j];
+        if (lane == j) v = y;
+        if (lane < j) v -= y * tile[j * (kPanel + 1) + lane];
+      }
+      if (lane < w) x[c0 + lane] = v;
+    }
+    __syncthreads();
+  }
+}
+
+__device__ inline void fb_update_team(const FrictionArgs& f, const Team team) {
+  for (int c = team.rank * blockDim.x + threadIdx.x; c < f.count; c += team.size * blockDim.x) {
+    const int slot = f.slot[c];
+    const double step = slot >= 0 ? f.compact[slot] : f.rhs[c] / f.diagonal[c];
+    f.multiplier[c] = fmin(fmax(f.multiplier[c] + step, 0.0), 1.0e8);
+  }
+}
+
+__device__ inline void fb_friction_team(const StepArgs& a, const Team team) {
+  const FrictionArgs& f = a.fc;
+  for (int c = team.rank * blockDim.x + threadIdx.x; c < f.count; c += team.size * blockDim.x) {
+    if (f.multiplier[c] <= 0.0) {
+      f.lambda_t[2 * c] = f.lambda_t[2 * c + 1] = 0.0;
+      continue;
+    }
+    const int node = f.nodes[c];
+    const V3<double> solved = v3<double>(fb_solved(a, node, 0), fb_solved(a, node, 1), fb_solved(a, node, 2));
+    const V3<double> step = solved + load3d(f.response, c) - load3d(a.position, node);
+    const V3<double> n = load3d(f.normal, c), t1 = load3d(f.tangent1, c), t2 = load3d(f.tangent2, c);
+    const V3<double> tangential = step - dot(step, n) * n;
+    const double u1 = dot(tangential, t1), u2 = dot(tangential, t2);
+    const double diagonal = f.block[static_cast<long long>(c) * f.count + c];
+    const double w11 = dot(t1, t1) * diagonal, w12 = dot(t1, t2) * diagonal, w22 = dot(t2, t2) * diagonal;
+    const double determinant = w11 * w22 - w12 * w12;
+    double s1 = 0.0, s2 = 0.0;
+    if (fabs(determinant) > 1.0e-20) {
+      s1 = -(w22 * u1 - w12 * u2) / determinant;
+      s2 = -(-w12 * u1 + w11 * u2) / determinant;
+    }
+    const double radius = f.friction * f.multiplier[c];
+    if (sqrt(s1 * s1 + s2 * s2) <= radius + 1.0e-14) {
+      f.lambda_t[2 * c] = s1;
+      f.lambda_t[2 * c + 1] = s2;
+    } else {
+      const double magnitude = sqrt(u1 * u1 + u2 * u2);
+      f.lambda_t[2 * c] = magnitude > 1.0e-14 ? -radius * u1 / magnitude : 0.0;
+      f.lambda_t[2 * c + 1] = magnitude > 1.0e-14 ? -radius * u2 / magnitude : 0.0;
+    }
+  }
+}
+
+// The whole contact section of one iteration for large contact sets; every
+// block of the team calls it after A^{-1} b is complete. Returns false when a
+// team barrier gave up.
+__device__ inline bool fb_newton_team(const StepArgs& a, const Team team) {
+  __shared__ double tile[kPanel * (kPanel + 1)];
+  const FrictionArgs& f = a.fc;
+  fb_scalars_team(a, team);
+  if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
+  if (team.rank == 0) fb_compact_block(f);
+  if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
+  const int active = *reinterpret_cast<volatile int*>(f.active);
+  fb_response_team(f, team, active);
+  if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
+  fb_system_team(a, team, active);
+  if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
+  if (active > 0) {
+    if (!fb_cholesky_team(a, team, f.matrix, f.count, active, tile)) return false;
+    if (team.rank == 0) {
+      for (int i = threadIdx.x; i < active; i += blockDim.x) f.compact[i] = f.rhs[f.order[i]];
+      __syncthreads();
+      fb_cholesky_solve_block(f.matrix, f.count, active, f.compact, tile);
+    }
+    if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
+  }
+  fb_update_team(f, team);
+  if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
+  if (f.friction > 0.0) {
+    fb_forces_team(f, team, false);
+    if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
+    fb_response_team(f, team, active);
+    if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
+    fb_friction_team(a, team);
+    if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
+  }
+  fb_forces_team(f, team, true);
+  return grid_sync(a.barrier, a.status, team.size, team.rank);
 }
 
 // x_i += sum_k P[i][order_k] f_order_k (contact_solution, contact.py:412-427).

@@ -69,8 +69,9 @@ __device__ void warp_convergence(const StepArgs& a, int blocks) {
 // One projective-dynamics step of one instance by one team of blocks:
 // prologue, every local/global iteration, epilogue. Returns false when a team
 // barrier gave up (the status word says why).
-// TL: precision of the local projections; TV: precision of the factor values.
-template <typename TL, typename TV>
+// TL: precision of the local projections; TV: precision of the factor values;
+// kContact: the frictional boundary is compiled in (single-instance launches).
+template <typename TL, typename TV, bool kContact>
 __device__ __forceinline__ bool forward_step_body(const StepArgs& a, const Team team, char* dyn_smem) {
   __shared__ double s_grad[8 * 8 * 3];
   __shared__ double s_scratch[kBlock];
@@ -147,11 +148,13 @@ __device__ __forceinline__ bool forward_step_body(const StepArgs& a, const Team 
   }
   double* vector_smem = reinterpret_cast<double*>(dyn_smem + a.vector_smem_offset);
   if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
-  if (a.fc.count > 0) {
-    // Frictional boundary: frames, candidates, Delassus matrix (FrictionalContact.begin_step).
-    fb_begin_frames(a, team);
-    if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
-    fb_begin_delassus(a, team);
+  if constexpr (kContact) {
+    if (a.fc.count > 0) {
+      // Frictional boundary: frames, candidates, Delassus matrix (FrictionalContact.begin_step).
+      fb_begin_frames(a, team);
+      if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
+      fb_begin_delassus(a, team);
+    }
   }
 
   const int r0 = a.st_part[team.rank], r1 = a.st_part[team.rank + 1];
@@ -271,16 +274,23 @@ __device__ __forceinline__ bool forward_step_body(const StepArgs& a, const Team 
       spmv_block<TV>(a.plan_st, st_values, a.resident != 0, dyn_smem, in, a.x, team.rank);
     }
     int contact_active = 0;
-    if (a.fc.count > 0) {
-      // x = A^{-1} (b + J^T lambda): one Newton step on the multipliers by the
-      // first block, then the correction through the panel columns.
-      if (a.fc.kind == kBoundaryMesh && a.fc.restitution > 0.0) {
-        for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) store3(a.fc.surface, i, load3d(a.prev, i));
+    if constexpr (kContact) {
+      if (a.fc.count > 0) {
+        // x = A^{-1} (b + J^T lambda): one Newton step on the multipliers (by
+        // the first block for small contact sets, by the team for large ones),
+        // then the correction through the panel columns.
+        if (a.fc.kind == kBoundaryMesh && a.fc.restitution > 0.0) {
+          for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) store3(a.fc.surface, i, load3d(a.prev, i));
+        }
+        if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
+        if (a.fc.count <= kTeamContacts) {
+          if (team.rank == 0) fb_newton(a);
+          if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
+        } else if (!fb_newton_team(a, team)) {
+          return false;
+        }
+        contact_active = *reinterpret_cast<volatile int*>(a.fc.active);
       }
-      if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
-      if (team.rank == 0) fb_newton(a);
-      if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
-      contact_active = *reinterpret_cast<volatile int*>(a.fc.active);
     }
     __syncthreads();
     const int count = a.window > 0 ? a.aa_state[0] : 0;
@@ -366,10 +376,12 @@ __device__ __forceinline__ bool forward_step_body(const StepArgs& a, const Team 
     }
   }
 
-  if (a.fc.count > 0 && a.fc.restitution > 0.0) {
-    // FrictionalContact.finish_step: restitution on the converged positions.
-    fb_restitution(a, team);
-    if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
+  if constexpr (kContact) {
+    if (a.fc.count > 0 && a.fc.restitution > 0.0) {
+      // FrictionalContact.finish_step: restitution on the converged positions.
+      fb_restitution(a, team);
+      if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
+    }
   }
   // ---- Epilogue: write_state (kernels.py:404-414) and the step record.
   for (int i = gtid; i < n; i += gthreads) {
@@ -388,7 +400,7 @@ __device__ __forceinline__ bool forward_step_body(const StepArgs& a, const Team 
 template <typename TL, typename TV>
 __global__ void __launch_bounds__(kBlock) forward_step_kernel(const StepArgs a) {
   extern __shared__ __align__(16) char dyn_smem[];
-  forward_step_body<TL, TV>(a, Team{static_cast<int>(blockIdx.x), static_cast<int>(gridDim.x)}, dyn_smem);
+  forward_step_body<TL, TV, true>(a, Team{static_cast<int>(blockIdx.x), static_cast<int>(gridDim.x)}, dyn_smem);
 }
 
 // Whole forward rollouts of many instances, each by a team of blocks: the
@@ -434,7 +446,7 @@ __global__ void __launch_bounds__(kBlock, 2) team_forward_kernel(const TeamLaunc
         s_args.timers = instance == launch.timer_instance ? launch.timers : nullptr;
       }
       __syncthreads();
-      if (!forward_step_body<TL, TV>(s_args, team, dyn_smem)) return;
+      if (!forward_step_body<TL, TV, false>(s_args, team, dyn_smem)) return;
       if (team.rank == 0 && threadIdx.x == 0 && launch.iteration_log != nullptr)
         launch.iteration_log[t * launch.count + instance] = *s_args.iteration;
       // The next step reads the states every rank of the lane wrote.

@@ -626,7 +626,9 @@ int pd_build(PdSolver* s, double dt) {
   {
     int optin = 0;
     PD_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, s->device));
-    if (int status = pd_plan_launch(s, blocks, optin - 8 * 1024)) return status;  // 8 KB: static shared memory
+    // 16 KB: static shared memory of the step kernels (the contact section's
+    // 32 x 33 Cholesky tile included).
+    if (int status = pd_plan_launch(s, blocks, optin - 16 * 1024)) return status;
     int per_sm_forward = 0, per_sm_adjoint = 0;
     PD_CUDA(pdb200::forward_step_max_blocks(s->options.precision, s->smem, &per_sm_forward));
     PD_CUDA(pdb200::adjoint_step_max_blocks(s->options.precision, s->smem, &per_sm_adjoint));

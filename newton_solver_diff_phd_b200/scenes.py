@@ -62,3 +62,113 @@ def cantilever_model(spec: Cantilever, edge: float = 0.01, device="cuda", gravit
     forces = np.zeros_like(vertices, dtype=np.float32)
     forces[tip, 0] = np.asarray(spec.tip_forces, dtype=np.float32)[: len(tip)]
     return model, meshes.Mesh(f"cantilever{spec.nx}x{spec.ny}x{spec.nz}", vertices, hexes), materials, forces
+
+
+# ---------------------------------------------------------------------------
+# The Tet4 contact workload: a soft block resting on a fixed plane, poked by a
+# rigid sphere probe. The block is 20 x 20 x 10 cubes of 1 mm split into five
+# tetrahedra each (20,000 Tet4, 4,851 particles; E = 1e5 Pa, nu = 0.45,
+# density 1100 kg/m^3); the plane is a frictional boundary z = 0 holding the
+# bottom-face particles; the probe is a meshed ball of radius 3 mm (an
+# icosphere of 162 surface particles around a centre, 320 tetrahedra) whose particles are
+# prescribed (Dirichlet) and move down 4 mm at constant speed over the
+# rollout; block and probe meet through the penalty mesh contact (radius
+# 0.55 mm, normal stiffness 5e3 N/m, tangential damping 50 N s/m, friction
+# 0.5).
+
+
+@dataclass
+class Poke:
+    offset: tuple          # probe offset (dx, dy) [m] from the block's top centre
+    nx: int = 20
+    ny: int = 20
+    nz: int = 10
+    edge: float = 1.0e-3
+    young: float = 1.0e5
+    poisson: float = 0.45
+    density: float = 1100.0
+    probe_radius: float = 3.0e-3
+    probe_level: int = 2      # icosphere subdivisions: 162 surface particles, 320 faces
+    probe_travel: float = 4.0e-3
+    start_gap: float = 0.25e-3
+    steps: int = 200
+    dt: float = 1.0e-3
+
+
+def _icosphere(level: int):
+    """Unit sphere triangulated from the icosahedron by ``level`` 4-to-1 subdivisions: ``(points, faces)``."""
+    phi = (1.0 + 5.0 ** 0.5) / 2.0
+    points = [np.array(p, dtype=np.float64) for p in
+              ([0, 1, phi], [0, -1, phi], [0, 1, -phi], [0, -1, -phi], [1, phi, 0], [-1, phi, 0],
+               [1, -phi, 0], [-1, -phi, 0], [phi, 0, 1], [-phi, 0, 1], [phi, 0, -1], [-phi, 0, -1])]
+    points = [p / np.linalg.norm(p) for p in points]
+    # The 20 faces: every triple of mutually adjacent vertices.
+    table = np.array(points)
+    distance = np.linalg.norm(table[:, None] - table[None], axis=2)
+    adjacent = np.abs(distance - distance[distance > 1e-9].min()) < 1e-9
+    faces = [(a, b, c) for a in range(12) for b in range(a + 1, 12) for c in range(b + 1, 12)
+             if adjacent[a, b] and adjacent[b, c] and adjacent[a, c]]
+    for _ in range(level):
+        midpoint = {}
+
+        def middle(i, j):
+            key = (min(i, j), max(i, j))
+            if key not in midpoint:
+                m = points[i] + points[j]
+                points.append(m / np.linalg.norm(m))
+                midpoint[key] = len(points) - 1
+            return midpoint[key]
+
+        refined = []
+        for a, b, c in faces:
+            ab, bc, ca = middle(a, b), middle(b, c), middle(c, a)
+            refined += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        faces = refined
+    return np.array(points), np.array(faces, dtype=np.int32)
+
+
+def poke_scene(spec: Poke, device="cuda"):
+    """``(model, options)`` of the poke workload.
+
+    ``options`` holds the solver keywords of the contact (``frictional_boundary``,
+    ``frictional_vertices``, ``mesh_contact``), the per-step prescribed probe
+    positions ``dirichlet`` (float32 ``(steps, N, 3)``), the block's surface
+    faces and the probe's particle range.
+    """
+    vertices, tets, _ = meshes.tet_grid(spec.nx, spec.ny, spec.nz, spec.edge)
+    mu, lam = meshes.lame_from_young(spec.young, spec.poisson)
+    builder = ModelBuilder(gravity=(0.0, 0.0, -9.81))
+    builder.add_soft_grid(pos=(0.0, 0.0, 0.0), rot=None, vel=(0.0, 0.0, 0.0), dim_x=spec.nx, dim_y=spec.ny,
+                          dim_z=spec.nz, cell_x=spec.edge, cell_y=spec.edge, cell_z=spec.edge,
+                          density=spec.density, k_mu=float(mu), k_lambda=float(lam), k_damp=0.0)
+    block = builder.particle_count
+    points, faces = _icosphere(spec.probe_level)
+    top = spec.nz * spec.edge
+    center = np.array([spec.nx * spec.edge / 2 + spec.offset[0], spec.ny * spec.edge / 2 + spec.offset[1],
+                       top + spec.probe_radius + spec.start_gap])
+    ball = np.vstack((points * spec.probe_radius + center, center[None]))
+    for p in ball:
+        builder.add_particle(p, (0.0, 0.0, 0.0), 0.0)
+    hub = block + len(points)
+    for a, b, c in faces:
+        tet = [hub, block + a, block + b, block + c]
+        edges = ball[[a, b, c]] - center
+        if np.linalg.det(edges) < 0.0:
+            tet[2], tet[3] = tet[3], tet[2]
+        builder.add_tetrahedron(*tet, k_mu=float(mu), k_lambda=float(lam))
+    model = builder.finalize(device)
+    surface = meshes.boundary_faces_tet(tets)
+    bottom = np.flatnonzero(np.abs(vertices[:, 2]) <= 1.0e-12).astype(np.int32)
+    q0 = model.particle_q.detach().cpu().numpy().astype(np.float64)
+    dirichlet = np.repeat(q0[None], spec.steps, axis=0)
+    for t in range(spec.steps):
+        dirichlet[t, block:, 2] -= spec.probe_travel * (t + 1) / spec.steps
+    options = {
+        "frictional_boundary": ("planar", (0.0, 0.0, 1.0, 0.0)),
+        "frictional_vertices": bottom,
+        "mesh_contact": (0.55e-3, 5.0e3, 5.0e3, 50.0, 0.5, surface, faces + block),
+        "dirichlet": dirichlet.astype(np.float32),
+        "surface": surface,
+        "probe": (block, model.particle_count),
+    }
+    return model, options

@@ -240,3 +240,38 @@ def test_contact_woodbury_projection_matches_reference(key):
         for expected in (oracle[name], g[f"{key}__out_{name}"]):
             scale = max(np.abs(expected).max(), 1.0e-30)
             np.testing.assert_allclose(actual, expected, rtol=0.0, atol=1.0e-5 * scale, err_msg=name)
+
+
+def test_large_contact_set_on_the_team_path_matches_the_oracle():
+    """A 8x6x2 block: 63 floor contacts plus 200 registered surface vertices, so
+    the Newton step runs across the team with the panelled Cholesky (two panels)."""
+    from newton_solver_diff_phd_b200 import ModelBuilder
+
+    builder = ModelBuilder(gravity=(0.0, 0.0, -9.81))
+    builder.add_soft_grid(pos=(0.0, 0.0, 0.0), rot=None, vel=(0.0, 0.0, 0.0), dim_x=8, dim_y=6, dim_z=2, cell_x=0.05,
+                          cell_y=0.05, cell_z=0.05, density=DENSITY, k_mu=2.0e4, k_lambda=5.0e4, k_damp=0.0)
+    model = builder.finalize("cuda")
+    options = {"max_iterations": 2000, "abs_tol": 1.0e-12, "rel_tol": 1.0e-11}
+    solver = SolverDiffPhD(model, density=DENSITY, frictional_boundary=("planar", (0.0, 0.0, 1.0, 0.0)),
+                           friction=0.5, **options)
+    nodes = solver.frictional_vertices
+    assert len(nodes) > 32
+    body = oracle_tet_body(model)
+    boundary = pd_oracle.FrictionalBoundary("planar", (0.0, 0.0, 1.0, 0.0), nodes, friction=0.5)
+    q = model.particle_q.cpu().numpy().astype(np.float64)
+    q[:, 2] += 0.0005
+    q = q.astype(np.float32).astype(np.float64)
+    v = np.tile(np.array([0.2, 0.0, -1.0], dtype=np.float32), (model.particle_count, 1)).astype(np.float64)
+    gravity = model.gravity[0].cpu().numpy().astype(np.float64)
+    for _ in range(2):
+        solver.step(_state(model, q, v), model.state(), None, None, 0.004)
+        solver.check_status()
+        expected, iterations, converged = pd_oracle.step(body, q, v, np.zeros_like(q), gravity, 0.004,
+                                                         contact=boundary, **options)
+        assert converged and int(solver.iterations[0]) == iterations
+        np.testing.assert_allclose(solver._x.cpu().numpy(), expected, rtol=0.0, atol=1.0e-9)
+        np.testing.assert_allclose(solver.contact_multipliers.cpu().numpy(), boundary.multiplier, rtol=1.0e-6,
+                                   atol=1.0e-9)
+        assert int((boundary.multiplier > 0).sum()) > 32
+        x = solver._x.cpu().numpy()
+        q, v = x.astype(np.float32).astype(np.float64), ((x - q) / 0.004).astype(np.float32).astype(np.float64)
