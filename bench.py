@@ -175,13 +175,10 @@ def run_b200(args):
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     device = torch.device("cuda", local)
-    dist = None
-    if world > 1:
-        import datetime
+    from newton_solver_diff_phd_b200 import distributed
 
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=device)
+    # One process per GPU; the group has a bounded collective timeout.
+    ranks = distributed.setup("nccl", timeout_s=600.0, device=device)
     model, young, poisson, target = build_model(device)
     solver = SolverDiffPhD(model, density=1000.0, rel_tol=REL_TOL, abs_tol=ABS_TOL, adjoint=args.adjoint,
                            precision=args.precision)
@@ -210,8 +207,7 @@ def run_b200(args):
     stream = torch.cuda.current_stream()
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    if dist is not None:
-        dist.barrier()
+    distributed.barrier(ranks)
     torch.cuda.synchronize()
     with ClockSampler(local) as sampler:
         for k in range(args.steps):
@@ -222,18 +218,14 @@ def run_b200(args):
         torch.cuda.synchronize()
     clocks = sampler.summary()
     elapsed_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
-    if dist is not None:
-        t = torch.tensor([elapsed_ms], dtype=torch.float64, device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
+    elapsed_ms = distributed.max_over_ranks(elapsed_ms, ranks)
     status |= solver.read_status()
     total_steps = STEPS_PER_ROLLOUT * args.steps * world
     value = total_steps / (elapsed_ms / 1000.0)
 
     if args.no_extras:
-        if dist is not None:
-            dist.barrier()
-            dist.destroy_process_group()
+        distributed.barrier(ranks)
+        distributed.teardown(ranks)
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                               "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "profiling_run": True}))
@@ -332,9 +324,8 @@ def run_b200(args):
             result["batched"] = run_batched(args, device)
         if world == 1 and not args.no_contact:
             result["contact"] = run_contact(args, device)
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    distributed.barrier(ranks)
+    distributed.teardown(ranks)
     if rank == 0:
         print(json.dumps(result), flush=True)
 
