@@ -360,6 +360,11 @@ int pd_batch_read(PdBatch* batch, int32_t* status, int32_t* iterations, void* st
    (SparseInverse.__init__, sparse.py:291-320). Arrays are host memory; the
    result is freed with pd_inverse_free. */
 typedef struct PdInverseFactor PdInverseFactor;
+/* Update work (entries of earlier rows a row combines) from which a row of
+   the inverse factor is computed by all host threads, each on a column range
+   (default 65536; 0: every row). The factor is bit-identical either way.
+   Process-wide setting. */
+int pd_inverse_parallel_work(int64_t work);
 int pd_inverse_build(int32_t size, const int32_t* row_offsets, const int32_t* columns, const double* values,
                      PdInverseFactor** out);
 int pd_inverse_sizes(const PdInverseFactor* factor, int32_t* size, int64_t* nnz, int64_t* factorization_nnz);

@@ -133,6 +133,7 @@ SIGNATURES = {
     "pd_batch_team_sizes": ([_P, _P, _P], ctypes.c_int),
     "pd_batch_timeline": ([_P, _P, _P, _P], ctypes.c_int),
     "pd_batch_set_phase_timers": ([_P, _I32, _P], ctypes.c_int),
+    "pd_inverse_parallel_work": ([_I64], ctypes.c_int),
     "pd_inverse_build": ([_I32, _P, _P, _P, ctypes.POINTER(_P)], ctypes.c_int),
     "pd_inverse_sizes": ([_P, ctypes.POINTER(_I32), ctypes.POINTER(_I64), ctypes.POINTER(_I64)], ctypes.c_int),
     "pd_inverse_export": ([_P, _P, _P, _P, _P, _P, _P, _P], ctypes.c_int),

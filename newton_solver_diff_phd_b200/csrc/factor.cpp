@@ -10,15 +10,86 @@
 #include "factor.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <condition_variable>
 #include <cstdint>
+#include <functional>
 #include <limits>
+#include <memory>
+#include <mutex>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace pdb200 {
+
+// Rows of L^{-1} whose update work (entries of the earlier rows they
+// combine) reaches this are split over host threads.
+std::atomic<int64_t> g_parallel_row_work{1 << 16};
+
 namespace {
+
+// A fixed set of worker threads that run one task per worker and wait for
+// all of them (one row of the inverse at a time).
+class RowPool {
+ public:
+  explicit RowPool(unsigned workers) {
+    for (unsigned w = 1; w < workers; ++w) threads_.emplace_back([this, w] { loop(w); });
+    count_ = workers;
+  }
+  ~RowPool() {
+    {
+      std::lock_guard<std::mutex> lock(mutex_);
+      stop_ = true;
+      ++generation_;
+    }
+    wake_.notify_all();
+    for (auto& t : threads_) t.join();
+  }
+  unsigned size() const { return count_; }
+  // Runs task(w) for w = 0 .. size()-1, worker 0 on the calling thread.
+  void run(const std::function<void(unsigned)>& task) {
+    {
+      std::lock_guard<std::mutex> lock(mutex_);
+      task_ = &task;
+      pending_ = count_ - 1;
+      ++generation_;
+    }
+    wake_.notify_all();
+    task(0);
+    std::unique_lock<std::mutex> lock(mutex_);
+    done_.wait(lock, [this] { return pending_ == 0; });
+  }
+
+ private:
+  void loop(unsigned w) {
+    uint64_t seen = 0;
+    for (;;) {
+      const std::function<void(unsigned)>* task;
+      {
+        std::unique_lock<std::mutex> lock(mutex_);
+        wake_.wait(lock, [&] { return generation_ != seen; });
+        seen = generation_;
+        if (stop_) return;
+        task = task_;
+      }
+      (*task)(w);
+      {
+        std::lock_guard<std::mutex> lock(mutex_);
+        if (--pending_ == 0) done_.notify_one();
+      }
+    }
+  }
+  std::vector<std::thread> threads_;
+  std::mutex mutex_;
+  std::condition_variable wake_, done_;
+  const std::function<void(unsigned)>* task_ = nullptr;
+  uint64_t generation_ = 0;
+  unsigned pending_ = 0, count_ = 1;
+  bool stop_ = false;
+};
 
 using Adjacency = std::vector<std::vector<int32_t>>;
 
@@ -348,14 +419,86 @@ std::string build_inverse_factor(int32_t size, const int32_t* row_offsets, const
   std::vector<std::vector<int32_t>>().swap(columns);
 
   // --- Inverse rows (sparse.py:159-177) ----------------------------------
-  // Unscaled rows of L^{-1} in elimination order, stored CSR.
+  // Unscaled rows of L^{-1} in elimination order, stored CSR. A row with much
+  // update work is split by column range over host threads: every thread
+  // walks the same earlier rows in the same order and applies only the
+  // updates of its columns, so each entry sees the same sequence of rounded
+  // operations as the sequential walk and the factor stays bit-identical.
   std::vector<int64_t> inv_start(1, 0);
   std::vector<int32_t> inv_columns;
   std::vector<double> inv_values;
   std::vector<double> current(size, 0.0);
   std::vector<int32_t> touched_mark(size, -1);
   std::vector<int32_t> touched;
+  const unsigned hardware = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  std::unique_ptr<RowPool> pool;
+  std::vector<std::vector<std::pair<int32_t, double>>> pieces;
+  const int64_t parallel_work = g_parallel_row_work.load();
   for (int32_t i = 0; i < size; ++i) {
+    int64_t work = 0;
+    for (int64_t p = row_start[i]; p < row_start[i + 1] - 1; ++p) work += inv_start[pattern[p] + 1] - inv_start[pattern[p]];
+    // Split only rows whose earlier rows are long: every range costs one
+    // binary search per earlier row.
+    const int64_t terms = row_start[i + 1] - 1 - row_start[i];
+    if (hardware > 1 && work >= parallel_work && work >= 512 * terms) {
+      if (!pool) {
+        pool.reset(new RowPool(hardware));
+        pieces.resize(2 * hardware);
+      }
+      // Column ranges handed out dynamically, several per thread, for balance.
+      const int chunks = static_cast<int>(pieces.size());
+      const int64_t span = static_cast<int64_t>(i) + 1;  // row i of L^{-1} has columns 0 .. i
+      std::atomic<int> next_chunk{0};
+      pool->run([&](unsigned) {
+        std::vector<int32_t> mine;
+        for (int chunk = next_chunk++; chunk < chunks; chunk = next_chunk++) {
+        const int32_t lo = static_cast<int32_t>(span * chunk / chunks);
+        const int32_t hi = static_cast<int32_t>(span * (chunk + 1) / chunks);
+        std::vector<std::pair<int32_t, double>>& piece = pieces[chunk];
+        piece.clear();
+        mine.clear();
+        if (i >= lo && i < hi) {
+          current[i] = 1.0;
+          touched_mark[i] = i;
+          mine.push_back(i);
+        }
+        for (int64_t p = row_start[i]; p < row_start[i + 1] - 1; ++p) {
+          const int32_t k = pattern[p];
+          const double coefficient = values[p];
+          if (coefficient == 0.0) continue;
+          const int32_t* first = inv_columns.data() + inv_start[k];
+          const int32_t* last = inv_columns.data() + inv_start[k + 1];
+          const int32_t* begin = std::lower_bound(first, last, lo);
+          const int32_t* end = std::lower_bound(begin, last, hi);
+          for (const int32_t* c_at = begin; c_at < end; ++c_at) {
+            const int32_t c = *c_at;
+            if (touched_mark[c] != i) {
+              touched_mark[c] = i;
+              mine.push_back(c);
+            }
+            const double product = coefficient * inv_values[c_at - inv_columns.data()];
+            current[c] = current[c] - product;
+          }
+        }
+        std::sort(mine.begin(), mine.end());
+        for (int32_t c : mine) {
+          if (current[c] != 0.0) piece.emplace_back(c, current[c]);
+          current[c] = 0.0;
+        }
+        }
+      });
+      for (int chunk = 0; chunk < chunks; ++chunk) {
+        for (const auto& entry : pieces[chunk]) {
+          inv_columns.push_back(entry.first);
+          inv_values.push_back(entry.second);
+        }
+      }
+      if (inv_columns.size() > static_cast<size_t>(std::numeric_limits<int32_t>::max())) {
+        return "inverse factor fill exceeds int32 sparse indexing";
+      }
+      inv_start.push_back(static_cast<int64_t>(inv_columns.size()));
+      continue;
+    }
     touched.clear();
     current[i] = 1.0;
     touched_mark[i] = i;

@@ -10,6 +10,7 @@
 // bit-identical to the reference's for the same input rows.
 #pragma once
 
+#include <atomic>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -31,6 +32,10 @@ struct InverseFactor {
   int64_t factorization_nnz = 0;     // size + strict lower nnz(L)
   int64_t matrix_nnz = 0;
 };
+
+// Update work (entries of earlier rows combined) from which one row of the
+// inverse is split over host threads; the result is bit-identical either way.
+extern std::atomic<int64_t> g_parallel_row_work;
 
 // Validates rows (finite, positive diagonal, exact symmetry) and builds the
 // factor. Returns an empty string on success, otherwise the reason.

@@ -1005,6 +1005,11 @@ struct PdInverseFactor {
   InverseFactor factor;
 };
 
+int pd_inverse_parallel_work(int64_t work) {
+  pdb200::g_parallel_row_work.store(std::max<int64_t>(work, 0));
+  return PD_OK;
+}
+
 int pd_inverse_build(int32_t size, const int32_t* row_offsets, const int32_t* columns, const double* values,
                      PdInverseFactor** out) {
   if (out == nullptr || row_offsets == nullptr || (size > 0 && (columns == nullptr || values == nullptr)))

@@ -117,3 +117,29 @@ def test_run_format_is_the_same_factor(name, gap):
     if gap >= 2 and name == "cantilever":
         # Postorder labels make every row of S a single contiguous run.
         assert np.all(np.diff(runs["s_row_runs"]) <= 1)
+
+
+def test_threaded_inverse_rows_are_bit_identical():
+    """Rows of the inverse split over host threads by column range give the same arrays."""
+    import scipy.sparse as sp
+
+    from newton_solver_diff_phd_b200 import _lib, meshes
+    from oracle import pd_oracle
+
+    vertices, hexes, _ = meshes.hex_grid(14, 5, 5, 0.01)
+    free = vertices[:, 0] > 1.0e-12
+    mu, lam = meshes.lame_from_young(np.full(len(hexes), 1.0e6), 0.45)
+    body = pd_oracle.Body.hex(vertices, hexes, free, mu, lam, 1000.0)
+    a = sp.csr_matrix(body.matrix(0.01))
+    a = ((a + a.T) * 0.5).tocsr()
+    a.sort_indices()
+    lib = _lib.library()
+    results = []
+    try:
+        for work in (1 << 62, 0):
+            _lib.check(lib.pd_inverse_parallel_work(work))
+            results.append(_lib.inverse_factor((a.indptr, a.indices, a.data)))
+    finally:
+        _lib.check(lib.pd_inverse_parallel_work(1 << 16))
+    for key in ("permutation", "s_offsets", "s_columns", "s_values", "st_offsets", "st_columns", "st_values"):
+        assert np.array_equal(results[0][key], results[1][key]), key
