@@ -172,3 +172,62 @@ def poke_scene(spec: Poke, device="cuda"):
         "probe": (block, model.particle_count),
     }
     return model, options
+
+
+# ---------------------------------------------------------------------------
+# The large Hex8 twist-release workload: an 80 x 20 x 20 cell cantilever
+# (32,000 Hex8, 35,721 particles) of 1 cm cells, the x = 0 face pinned, the
+# middle third of the x slabs ten times stiffer (the rule of the reference
+# cantilever, cells nx//3 < i <= 2 (nx//3)), nu = 0.45, density 1000 kg/m^3,
+# no gravity. The initial state rotates every cross-section about the beam
+# axis by an angle growing linearly from 0 at the root to 30 degrees at the
+# tip (the reference twisted_positions) and releases it at rest.
+
+
+@dataclass
+class Twist:
+    nx: int = 80
+    ny: int = 20
+    nz: int = 20
+    edge: float = 0.01
+    young: float = 1.0e6
+    stiff_ratio: float = 10.0
+    poisson: float = 0.45
+    density: float = 1000.0
+    angle_degrees: float = 30.0
+    steps: int = 100
+    dt: float = 1.0e-3
+
+
+def twisted_positions(rest: np.ndarray, angle: float) -> np.ndarray:
+    """Cross-sections rotated about the beam's centre line, 0 at the root to ``angle`` [rad] at the tip."""
+    rest = np.asarray(rest, dtype=np.float64)
+    low, high = rest.min(axis=0), rest.max(axis=0)
+    theta = angle * (rest[:, 0] - low[0]) / (high[0] - low[0])
+    center = 0.5 * (low[1:] + high[1:])
+    offset = rest[:, 1:] - center
+    q = rest.copy()
+    q[:, 1] = center[0] + np.cos(theta) * offset[:, 0] - np.sin(theta) * offset[:, 1]
+    q[:, 2] = center[1] + np.sin(theta) * offset[:, 0] + np.cos(theta) * offset[:, 1]
+    root = rest[:, 0] == low[0]
+    q[root] = rest[root]
+    return q
+
+
+def twist_cantilever(spec: Twist, device="cuda"):
+    """``(model, mesh, hex_materials, q0, tip)``: the twisted initial positions (float64) and the tip-face particles."""
+    vertices, hexes, cells = meshes.hex_grid(spec.nx, spec.ny, spec.nz, spec.edge)
+    pinned = vertices[:, 0] <= 1.0e-12
+    builder = ModelBuilder(gravity=(0.0, 0.0, 0.0))
+    builder.add_particles(pos=vertices.tolist(), vel=np.zeros_like(vertices).tolist(),
+                          mass=[0.0 if p else 1.0 for p in pinned])
+    model = builder.finalize(device)
+    slab = np.asarray(cells)  # x index of every cell
+    third = spec.nx // 3
+    stiff = (slab > third) & (slab <= 2 * third)
+    young = spec.young * np.where(stiff, spec.stiff_ratio, 1.0)
+    mu, lam = meshes.lame_from_young(young, spec.poisson)
+    q0 = twisted_positions(vertices, np.radians(spec.angle_degrees))
+    tip = np.flatnonzero(np.abs(vertices[:, 0] - spec.nx * spec.edge) <= 1.0e-12)
+    mesh = meshes.Mesh(f"twist{spec.nx}x{spec.ny}x{spec.nz}", vertices, hexes)
+    return model, mesh, np.stack([mu, lam], axis=1), q0, tip
