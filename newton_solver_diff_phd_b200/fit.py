@@ -67,7 +67,10 @@ class MaterialFit:
         with tape if tape is not None else nullcontext():
             for frame in range(4):
                 self.solver.step(states[frame], states[frame + 1], None, None, 0.035)
-        self.solver.check_status()
+        # The forward must have converged; the backward's safeguards act silently
+        # as in the reference demo, which reads no status.
+        if self.solver.read_status() & 7:
+            raise RuntimeError("the calibration rollout did not converge")
         outputs = [s.particle_q.detach().clone() for s in states[1:]]
         loss, grad = 0.0, None
         if self.target is not None:
