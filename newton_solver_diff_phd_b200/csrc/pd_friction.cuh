@@ -578,20 +578,42 @@ __device__ inline void fb_response_team(const FrictionArgs& f, const Team team, 
   }
 }
 
-// Right-hand side per contact and the lower triangle of Omega W Omega + E.
-__device__ inline void fb_system_team(const StepArgs& a, const Team team, int active) {
+// The response of every contact and, by the same warp, its right-hand side
+// (contact_newton_rhs, contact.py:430-447).
+__device__ inline void fb_response_rhs_team(const StepArgs& a, const Team team, int active) {
   const FrictionArgs& f = a.fc;
-  const int gtid = team.rank * blockDim.x + threadIdx.x;
-  const int gthreads = team.size * blockDim.x;
-  for (int c = gtid; c < f.count; c += gthreads) {
-    const int node = f.nodes[c];
-    const V3<double> n = load3d(f.normal, c);
-    const V3<double> point = load3d(a.prev, node);
-    const V3<double> solved = v3<double>(fb_solved(a, node, 0), fb_solved(a, node, 1), fb_solved(a, node, 2));
-    f.rhs[c] = -f.residual[c] + f.omega[c] * dot(n, point) - f.omega[c] * dot(n, solved + load3d(f.response, c));
+  const int lane = threadIdx.x & 31;
+  for (int c = team_warp(team); c < f.count; c += team.size * kWarps) {
+    const double* row = f.block + static_cast<long long>(c) * f.count;
+    double rx = 0.0, ry = 0.0, rz = 0.0;
+#pragma unroll 4
+    for (int k = lane; k < active; k += 32) {
+      const int j = f.order[k];
+      const double b = row[j];
+      rx += b * f.force[3 * j];
+      ry += b * f.force[3 * j + 1];
+      rz += b * f.force[3 * j + 2];
+    }
+    rx = warp_sum(rx);
+    ry = warp_sum(ry);
+    rz = warp_sum(rz);
+    if (lane == 0) {
+      const V3<double> response = v3<double>(rx, ry, rz);
+      store3(f.response, c, response);
+      const int node = f.nodes[c];
+      const V3<double> n = load3d(f.normal, c);
+      const V3<double> point = load3d(a.prev, node);
+      const V3<double> solved = v3<double>(fb_solved(a, node, 0), fb_solved(a, node, 1), fb_solved(a, node, 2));
+      f.rhs[c] = -f.residual[c] + f.omega[c] * dot(n, point) - f.omega[c] * dot(n, solved + response);
+    }
   }
+}
+
+// The lower triangle of the coupled block Omega W Omega + E (contact_system, contact.py:502-528).
+__device__ inline void fb_matrix_team(const FrictionArgs& f, const Team team, int active) {
   const long long entries = static_cast<long long>(active) * active;
-  for (long long t = gtid; t < entries; t += gthreads) {
+  for (long long t = static_cast<long long>(team.rank) * blockDim.x + threadIdx.x; t < entries;
+       t += static_cast<long long>(team.size) * blockDim.x) {
     const int i = static_cast<int>(t / active), j = static_cast<int>(t % active);
     if (j > i) continue;
     const int p = f.order[i], q = f.order[j];
@@ -602,44 +624,48 @@ __device__ inline void fb_system_team(const StepArgs& a, const Team team, int ac
 }
 
 // In-place Cholesky of the lower triangle of m[:n, :n] (leading dimension
-// ld) by the team. Returns false when a team barrier gave up.
+// ld) by the team. Returns false when a team barrier gave up. Two team
+// barriers per panel: the first block folds the next diagonal tile's
+// trailing update into its own share and factors that tile right away.
 __device__ inline bool fb_cholesky_team(const StepArgs& a, const Team team, double* m, int ld, int n,
                                         double* tile /* shared [kPanel * (kPanel + 1)] */) {
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   auto at = [&](int i, int j) -> double& { return m[static_cast<long long>(i) * ld + j]; };
-  for (int c0 = 0; c0 < n; c0 += kPanel) {
-    const int w = min(kPanel, n - c0);
-    if (team.rank == 0 && warp == 0) {
-      // Diagonal tile: lane r owns row r.
-      for (int r = 0; r < w; ++r)
-        if (lane <= r) tile[r * (kPanel + 1) + lane] = at(c0 + r, c0 + lane);
+  // Diagonal tile at c0 (w rows) by warp 0 of the calling block: lane r owns row r.
+  auto factor_tile = [&](int c0, int w) {
+    if (warp != 0) return;
+    for (int r = 0; r < w; ++r)
+      if (lane <= r) tile[r * (kPanel + 1) + lane] = at(c0 + r, c0 + lane);
+    __syncwarp();
+    for (int k = 0; k < w; ++k) {
+      double d = tile[k * (kPanel + 1) + k];
+      d = d > 0.0 ? sqrt(d) : sqrt(DBL_MIN);
       __syncwarp();
-      for (int k = 0; k < w; ++k) {
-        double d = tile[k * (kPanel + 1) + k];
-        d = d > 0.0 ? sqrt(d) : sqrt(DBL_MIN);
-        __syncwarp();
-        if (lane == k) tile[k * (kPanel + 1) + k] = d;
-        if (lane > k && lane < w) tile[lane * (kPanel + 1) + k] /= d;
-        __syncwarp();
-        if (lane > k && lane < w) {
-          const double lk = tile[lane * (kPanel + 1) + k];
-          for (int c = k + 1; c <= lane; ++c) tile[lane * (kPanel + 1) + c] -= lk * tile[c * (kPanel + 1) + k];
-        }
-        __syncwarp();
+      if (lane == k) tile[k * (kPanel + 1) + k] = d;
+      if (lane > k && lane < w) tile[lane * (kPanel + 1) + k] /= d;
+      __syncwarp();
+      if (lane > k && lane < w) {
+        const double lk = tile[lane * (kPanel + 1) + k];
+        for (int c = k + 1; c <= lane; ++c) tile[lane * (kPanel + 1) + c] -= lk * tile[c * (kPanel + 1) + k];
       }
-      for (int r = 0; r < w; ++r)
-        if (lane <= r) at(c0 + r, c0 + lane) = tile[r * (kPanel + 1) + lane];
+      __syncwarp();
     }
-    if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
-    if (c0 + w >= n) break;
+    for (int r = 0; r < w; ++r)
+      if (lane <= r) at(c0 + r, c0 + lane) = tile[r * (kPanel + 1) + lane];
+  };
+  if (team.rank == 0) factor_tile(0, min(kPanel, n));
+  if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
+  for (int c0 = 0; c0 + kPanel < n; c0 += kPanel) {
+    const int w = kPanel;
+    const int t0 = c0 + w, w2 = min(kPanel, n - t0);
     // Panel below: L_ip = M_ip L_pp^-T, a warp per row.
     for (int r = threadIdx.x; r < w * w; r += blockDim.x) {
       const int i = r / w, j = r % w;
       if (j <= i) tile[i * (kPanel + 1) + j] = at(c0 + i, c0 + j);
     }
     __syncthreads();
-    for (int row = c0 + w + team_warp(team); row < n; row += team.size * kWarps) {
+    for (int row = t0 + team_warp(team); row < n; row += team.size * kWarps) {
       double v = lane < w ? at(row, c0 + lane) : 0.0;
       for (int j = 0; j < w; ++j) {
         const double x = __shfl_sync(0xffffffffu, v, j) / tile[j * (kPanel + 1) + j];
@@ -649,19 +675,31 @@ __device__ inline bool fb_cholesky_team(const StepArgs& a, const Team team, doub
       if (lane < w) at(row, c0 + lane) = v;
     }
     if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
-    // Trailing lower triangle: M_ij -= L_ip . L_jp.
-    const int t0 = c0 + w, rest = n - t0;
-    const long long entries = static_cast<long long>(rest) * rest;
-    for (long long t = static_cast<long long>(team.rank) * blockDim.x + threadIdx.x; t < entries;
-         t += static_cast<long long>(team.size) * blockDim.x) {
-      const int i = t0 + static_cast<int>(t / rest), j = t0 + static_cast<int>(t % rest);
-      if (j > i) continue;
+    // Trailing lower triangle M_ij -= L_ip . L_jp; the next diagonal tile
+    // (rows below t0 + w2) by the first block, which then factors it.
+    auto update = [&](int i, int j) {
       const double* li = m + static_cast<long long>(i) * ld + c0;
       const double* lj = m + static_cast<long long>(j) * ld + c0;
       double sum = 0.0;
 #pragma unroll 8
       for (int l = 0; l < w; ++l) sum += li[l] * lj[l];
       at(i, j) -= sum;
+    };
+    const int rest = n - t0;
+    const long long entries = static_cast<long long>(rest) * rest;
+    for (long long t = static_cast<long long>(team.rank) * blockDim.x + threadIdx.x; t < entries;
+         t += static_cast<long long>(team.size) * blockDim.x) {
+      const int i = t0 + static_cast<int>(t / rest), j = t0 + static_cast<int>(t % rest);
+      if (j > i || i < t0 + w2) continue;
+      update(i, j);
+    }
+    if (team.rank == 0) {
+      for (int t = threadIdx.x; t < w2 * w2; t += blockDim.x) {
+        const int i = t0 + t / w2, j = t0 + t % w2;
+        if (j <= i) update(i, j);
+      }
+      __syncthreads();
+      factor_tile(t0, w2);
     }
     if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
   }
@@ -725,11 +763,19 @@ __device__ inline void fb_cholesky_solve_block(const double* m, int ld, int n, d
   }
 }
 
+// Multiplier update (contact_update, contact.py:531-546) and the contact's
+// force right after it: normal only when friction follows, else final.
 __device__ inline void fb_update_team(const FrictionArgs& f, const Team team) {
+  const bool tangential = !(f.friction > 0.0);
   for (int c = team.rank * blockDim.x + threadIdx.x; c < f.count; c += team.size * blockDim.x) {
     const int slot = f.slot[c];
     const double step = slot >= 0 ? f.compact[slot] : f.rhs[c] / f.diagonal[c];
-    f.multiplier[c] = fmin(fmax(f.multiplier[c] + step, 0.0), 1.0e8);
+    const double lambda = fmin(fmax(f.multiplier[c] + step, 0.0), 1.0e8);
+    f.multiplier[c] = lambda;
+    V3<double> value = (f.omega[c] * lambda) * load3d(f.normal, c);
+    if (tangential)
+      value = value + f.lambda_t[2 * c] * load3d(f.tangent1, c) + f.lambda_t[2 * c + 1] * load3d(f.tangent2, c);
+    store3(f.force, c, value);
   }
 }
 
@@ -777,9 +823,8 @@ __device__ inline bool fb_newton_team(const StepArgs& a, const Team team) {
   if (team.rank == 0) fb_compact_block(f);
   if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
   const int active = *reinterpret_cast<volatile int*>(f.active);
-  fb_response_team(f, team, active);
-  if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
-  fb_system_team(a, team, active);
+  fb_response_rhs_team(a, team, active);
+  fb_matrix_team(f, team, active);
   if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
   if (active > 0) {
     if (!fb_cholesky_team(a, team, f.matrix, f.count, active, tile)) return false;
@@ -793,15 +838,13 @@ __device__ inline bool fb_newton_team(const StepArgs& a, const Team team) {
   fb_update_team(f, team);
   if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
   if (f.friction > 0.0) {
-    fb_forces_team(f, team, false);
-    if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
     fb_response_team(f, team, active);
     if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
     fb_friction_team(a, team);
+    fb_forces_team(f, team, true);
     if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
   }
-  fb_forces_team(f, team, true);
-  return grid_sync(a.barrier, a.status, team.size, team.rank);
+  return true;
 }
 
 // x_i += sum_k P[i][order_k] f_order_k (contact_solution, contact.py:412-427).
