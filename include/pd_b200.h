@@ -304,6 +304,10 @@ typedef struct PdBatchOptions {
   const double* measured_us;
   const int32_t* measured_iterations;
   const int32_t* measured_team;
+  /* teams, optional with the three above: each instance's last adjoint
+     rollout duration [us]; the adjoint launch then gets its own lane counts
+     and queue order (same team sizes). NULL: the adjoint uses the forward's lanes. */
+  const double* measured_adjoint_us;
 } PdBatchOptions;
 /* options may be NULL (defaults). */
 int pd_batch_create(PdSolver* const* solvers, int32_t count, const PdBatchOptions* options, PdBatch** out);

@@ -85,6 +85,7 @@ class PdBatchOptions(ctypes.Structure):
         ("measured_us", ctypes.c_void_p),
         ("measured_iterations", ctypes.c_void_p),
         ("measured_team", ctypes.c_void_p),
+        ("measured_adjoint_us", ctypes.c_void_p),
     ]
 
 

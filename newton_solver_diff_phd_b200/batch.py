@@ -78,15 +78,21 @@ class BatchedSolver:
         options = _lib.PdBatchOptions(int(svd_warm_start), int(task_nnz), int(run_gap), int(local_cells),
                                       SCHEDULES[schedule], int(team_nnz), int(team_samples))
         if measured is not None:
-            # (durations [us], iterations, team sizes) per instance of a previous rollout (measurement()).
-            us, iterations, teams = measured
-            self._measured = (np.ascontiguousarray(us, dtype=np.float64),
-                              np.ascontiguousarray(iterations, dtype=np.int32),
-                              np.ascontiguousarray(teams, dtype=np.int32))
+            # (forward durations [us], iterations, team sizes[, adjoint durations [us]]) per instance
+            # of a previous rollout (measurement()).
+            if len(measured) not in (3, 4):
+                raise ValueError("measured is (durations, iterations, team sizes[, adjoint durations])")
+            self._measured = (np.ascontiguousarray(measured[0], dtype=np.float64),
+                              np.ascontiguousarray(measured[1], dtype=np.int32),
+                              np.ascontiguousarray(measured[2], dtype=np.int32))
+            if len(measured) == 4 and measured[3] is not None:
+                self._measured += (np.ascontiguousarray(measured[3], dtype=np.float64),)
             if any(len(a) != len(solvers) for a in self._measured):
                 raise ValueError("measured costs need one entry per instance")
             options.measured_us, options.measured_iterations, options.measured_team = (
-                _lib.ptr(a) for a in self._measured)
+                _lib.ptr(a) for a in self._measured[:3])
+            if len(self._measured) == 4:
+                options.measured_adjoint_us = _lib.ptr(self._measured[3])
         handle = ctypes.c_void_p()
         _lib.check(self._lib.pd_batch_create(ctypes.cast(handles, ctypes.c_void_p), len(solvers), ctypes.byref(options), ctypes.byref(handle)))
         self._handle = handle
@@ -168,17 +174,17 @@ class BatchedSolver:
         return forward, adjoint
 
     def measurement(self):
-        """``(durations [us], iterations, team sizes)`` of every instance in the last forward
-        rollout (plus its last adjoint, when one ran): the ``measured`` costs a re-planned
-        batch of the same instances takes."""
+        """``(forward durations [us], iterations, team sizes, adjoint durations [us] or None)``
+        of every instance in the last forward rollout and the last adjoint (when one ran):
+        the ``measured`` costs a re-planned batch of the same instances takes."""
         forward, adjoint = self.timeline()
-        # The lanes serve both rollouts: the adjoint's time joins the forward's when it ran.
         us = (forward[:, 1].astype(np.float64) - forward[:, 0].astype(np.float64)) / 1.0e3
-        if np.all(adjoint[:, 1] >= adjoint[:, 0]) and np.any(adjoint[:, 1] > 0):
-            us = us + (adjoint[:, 1].astype(np.float64) - adjoint[:, 0].astype(np.float64)) / 1.0e3
+        adjoint_us = None
+        if np.all(adjoint[:, 1] >= adjoint[:, 0]) and np.all(adjoint[:, 1] > 0):
+            adjoint_us = (adjoint[:, 1].astype(np.float64) - adjoint[:, 0].astype(np.float64)) / 1.0e3
         _, iterations = self.read()
         sizes, _ = self.team_sizes()
-        return us, iterations.sum(axis=0).astype(np.int32), sizes
+        return us, iterations.sum(axis=0).astype(np.int32), sizes, adjoint_us
 
     def concat(self, tensors) -> torch.Tensor:
         """Concatenate per-instance ``(n_i, 3)`` tensors into one ``(P, 3)`` state array."""

@@ -681,6 +681,9 @@ struct PdBatch {
   GraphKey key;
   // Teams schedule: per-instance team sizes and argument blocks, the queue.
   std::vector<int> team_size;
+  // Adjoint lanes planned from measured adjoint durations (adj_lanes > 0), else the forward's.
+  DeviceBuffer d_adj_lane_start, d_adj_lane_class, d_adj_class_begin, d_adj_class_order;
+  int adj_lanes = 0, adj_team_blocks = 0;
   DeviceBuffer d_forward_args, d_adjoint_args, d_lane_start, d_lane_class, d_class_begin, d_class_order,
       d_particle_offset, d_element_offset, d_class_head, d_lane_slot, d_barriers, d_team_status, d_adjoint_log,
       d_timeline;
@@ -1193,6 +1196,66 @@ int create_teams(PdBatch* batch, const PdBatchOptions& opts) {
   batch->lanes = static_cast<int>(lane_class.size());
   batch->classes = classes;
   batch->solo_class = sizes[0] == 1 ? 0 : -1;
+  // The adjoint's own lane counts and queue order from its measured durations
+  // (same team sizes and classes, so the same plans serve both launches).
+  batch->adj_lanes = 0;
+  if (measured && opts.measured_adjoint_us != nullptr) {
+    auto adjoint_estimate = [&](int i, int b) {
+      return std::max(opts.measured_adjoint_us[i], 0.0) * measured_team[i] / b;
+    };
+    std::vector<int> adj_teams;
+    plan_makespan(batch->team_size, adjoint_estimate, grid_cap, &adj_teams);
+    int blocks = 0;
+    for (int c = 0; c < classes; ++c) blocks += adj_teams[c] * sizes[c];
+    if (blocks <= grid_cap) {
+      std::vector<double> adj_cost(count), adj_work(classes, 0.0);
+      double adj_total = 0.0;
+      for (int i = 0; i < count; ++i) {
+        adj_cost[i] = adjoint_estimate(i, batch->team_size[i]);
+        adj_work[cls_of[i]] += adj_cost[i];
+        adj_total += adj_cost[i];
+      }
+      for (;;) {
+        int best = -1;
+        double best_gap = 0.0;
+        for (int c = 0; c < classes; ++c) {
+          if (adj_teams[c] >= members[c] || blocks + sizes[c] > grid_cap) continue;
+          const double gap = adj_work[c] / std::max(adj_total, 1e-30) -
+                             static_cast<double>(adj_teams[c] * sizes[c]) / grid_cap;
+          if (best < 0 || gap > best_gap) {
+            best = c;
+            best_gap = gap;
+          }
+        }
+        if (best < 0) break;
+        adj_teams[best] += 1;
+        blocks += sizes[best];
+      }
+      std::vector<int> adj_begin(classes + 1, 0), adj_order;
+      for (int c = 0; c < classes; ++c) {
+        std::vector<int> list;
+        for (int i = 0; i < count; ++i)
+          if (cls_of[i] == c) list.push_back(i);
+        std::stable_sort(list.begin(), list.end(), [&](int x, int y) { return adj_cost[x] > adj_cost[y]; });
+        adj_order.insert(adj_order.end(), list.begin(), list.end());
+        adj_begin[c + 1] = static_cast<int>(adj_order.size());
+      }
+      std::vector<int> adj_start(1, 0), adj_class;
+      for (int c = classes - 1; c >= 0; --c) {
+        for (int t = 0; t < adj_teams[c]; ++t) {
+          adj_class.push_back(c);
+          adj_start.push_back(adj_start.back() + sizes[c]);
+        }
+      }
+      PD_CUDA(batch->d_adj_lane_start.upload(adj_start));
+      PD_CUDA(batch->d_adj_lane_class.upload(adj_class));
+      PD_CUDA(batch->d_adj_class_begin.upload(adj_begin));
+      PD_CUDA(batch->d_adj_class_order.upload(adj_order));
+      batch->adj_lanes = static_cast<int>(adj_class.size());
+      batch->adj_team_blocks = adj_start.back();
+    }
+  }
+  const int lane_slots = std::max(batch->lanes, batch->adj_lanes);
   std::vector<long long> particle_offset(batch->particle_offsets.begin(), batch->particle_offsets.end() - 1);
   std::vector<long long> element_offset(batch->element_offsets.begin(), batch->element_offsets.end() - 1);
   PD_CUDA(batch->d_forward_args.upload(forward));
@@ -1204,14 +1267,14 @@ int create_teams(PdBatch* batch, const PdBatchOptions& opts) {
   PD_CUDA(batch->d_particle_offset.upload(particle_offset));
   PD_CUDA(batch->d_element_offset.upload(element_offset));
   PD_CUDA(batch->d_class_head.allocate(static_cast<size_t>(classes) * sizeof(unsigned)));
-  PD_CUDA(batch->d_lane_slot.allocate(static_cast<size_t>(batch->lanes) * sizeof(int)));
-  PD_CUDA(batch->d_barriers.allocate(static_cast<size_t>(batch->lanes) * sizeof(pdb200::GridBarrier)));
+  PD_CUDA(batch->d_lane_slot.allocate(static_cast<size_t>(lane_slots) * sizeof(int)));
+  PD_CUDA(batch->d_barriers.allocate(static_cast<size_t>(lane_slots) * sizeof(pdb200::GridBarrier)));
   PD_CUDA(batch->d_team_status.allocate(sizeof(int)));
   PD_CUDA(batch->d_timeline.allocate(static_cast<size_t>(count) * 4 * sizeof(unsigned long long)));
   PD_CUDA(pdb200::team_forward_max_blocks(batch->precision, smem, &per_sm_forward));
   PD_CUDA(pdb200::team_adjoint_max_blocks(batch->precision, smem, &per_sm_adjoint));
   batch->team_blocks = lane_start.back();
-  if (batch->team_blocks > std::max(1, std::min(per_sm_forward, per_sm_adjoint)) * sms)
+  if (std::max(batch->team_blocks, batch->adj_team_blocks) > std::max(1, std::min(per_sm_forward, per_sm_adjoint)) * sms)
     return pd_set_error(PD_ERR_UNSUPPORTED, "the lanes do not fit the co-resident grid");
   batch->team_smem = smem;
   PD_CUDA(cudaStreamCreateWithFlags(&batch->capture, cudaStreamNonBlocking));
@@ -1403,18 +1466,19 @@ int build_graph(PdBatch* b, const GraphKey& key) {
 
 namespace {
 
-pdb200::TeamLaunch team_launch(const PdBatch* b, int steps, double dt, const double gravity[3]) {
+pdb200::TeamLaunch team_launch(const PdBatch* b, int steps, double dt, const double gravity[3], bool adjoint = false) {
   pdb200::TeamLaunch launch{};
+  const bool own = adjoint && b->adj_lanes > 0;
   launch.forward = b->d_forward_args.as<pdb200::StepArgs>();
   launch.adjoint = b->d_adjoint_args.as<pdb200::AdjointArgs>();
-  launch.lane_start = b->d_lane_start.as<int>();
-  launch.lane_class = b->d_lane_class.as<int>();
-  launch.class_begin = b->d_class_begin.as<int>();
-  launch.class_order = b->d_class_order.as<int>();
+  launch.lane_start = own ? b->d_adj_lane_start.as<int>() : b->d_lane_start.as<int>();
+  launch.lane_class = own ? b->d_adj_lane_class.as<int>() : b->d_lane_class.as<int>();
+  launch.class_begin = own ? b->d_adj_class_begin.as<int>() : b->d_class_begin.as<int>();
+  launch.class_order = own ? b->d_adj_class_order.as<int>() : b->d_class_order.as<int>();
   launch.particle_offset = b->d_particle_offset.as<long long>();
   launch.element_offset = b->d_element_offset.as<long long>();
   launch.count = b->count;
-  launch.lanes = b->lanes;
+  launch.lanes = own ? b->adj_lanes : b->lanes;
   launch.solo_class = b->solo_class;
   launch.steps = steps;
   launch.dt = dt;
@@ -1447,7 +1511,8 @@ int capture_team_rollout(PdBatch* b, const pdb200::TeamLaunch& launch, bool adjo
     if (status == cudaSuccess && clear.first != nullptr) status = cudaMemsetAsync(clear.first, 0, clear.second, b->capture);
   }
   if (status == cudaSuccess) {
-    status = adjoint ? pdb200::launch_team_adjoint(launch, b->team_blocks, b->precision, b->team_smem, b->capture)
+    status = adjoint ? pdb200::launch_team_adjoint(launch, b->adj_lanes > 0 ? b->adj_team_blocks : b->team_blocks,
+                                                   b->precision, b->team_smem, b->capture)
                      : pdb200::launch_team_forward(launch, b->team_blocks, b->precision, b->team_smem, b->capture);
   }
   cudaGraph_t graph = nullptr;
@@ -1537,7 +1602,7 @@ extern "C" int pd_batch_backward(PdBatch* batch, int32_t steps, double dt, const
   key.force_stride = reinterpret_cast<long long>(grad_materials);
   if (batch->adjoint_exec == nullptr || !(batch->adjoint_key == key)) {
     PD_CUDA(batch->d_adjoint_log.allocate(static_cast<size_t>(steps) * batch->count * sizeof(int)));
-    pdb200::TeamLaunch launch = team_launch(batch, steps, dt, nullptr);
+    pdb200::TeamLaunch launch = team_launch(batch, steps, dt, nullptr, true);
     launch.x_record = const_cast<double*>(x_record);
     launch.grad_q_final = grad_q_final;
     launch.grad_qd_final = grad_qd_final;

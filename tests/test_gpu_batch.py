@@ -291,8 +291,8 @@ def test_measured_replan_keeps_the_results():
     plain = [_plain(*inst) for inst in _instances("fp64")]
     instances = _instances("fp64")
     batch, q, _, _, status, _ = _batched(instances, team_nnz=2048, team_samples=64)
-    us, iterations, teams = batch.measurement()
-    assert us.shape == iterations.shape == teams.shape == (len(instances),)
+    us, iterations, teams, adjoint_us = batch.measurement()
+    assert us.shape == iterations.shape == teams.shape == (len(instances),) and adjoint_us is None
     assert np.all(us > 0) and np.all(iterations >= STEPS)
     replanned, q2, _, _, status2, _ = _batched(instances, team_nnz=2048, team_samples=64,
                                                measured=(us, iterations, teams))
@@ -304,3 +304,28 @@ def test_measured_replan_keeps_the_results():
         assert float((replanned.split(q2)[i] - trajectory).abs().max()) <= 1e-6 * scale
     with pytest.raises(ValueError):
         BatchedSolver([s for _, s, _ in instances], DT, measured=(us[:2], iterations, teams))
+
+
+def test_adjoint_lanes_from_measured_adjoint_durations_keep_the_gradients():
+    """A batch re-planned with the adjoint's own measured durations (its own lanes) returns
+    the adjoint of the first plan: same team sizes, so the same arithmetic."""
+    instances = _instances("fp64")
+    batch, q, qd, x, status, _ = _batched(instances, team_nnz=2048, team_samples=64)
+    weight = torch.as_tensor(np.random.default_rng(8).standard_normal(tuple(q.shape[1:])), dtype=torch.float32,
+                             device="cuda")
+    first = [t.clone() for t in batch.backward(x, weight)[:4]]
+    us, iterations, teams, adjoint_us = batch.measurement()
+    assert adjoint_us is not None and adjoint_us.shape == (len(instances),) and np.all(adjoint_us > 0)
+    replanned, q2, _, x2, status2, _ = _batched(instances, team_nnz=2048, team_samples=64,
+                                                measured=(us, iterations, teams, adjoint_us))
+    sizes, _ = replanned.team_sizes()
+    second = replanned.backward(x2, weight)[:4]
+    assert np.all(status2 == 0)
+    if np.array_equal(sizes, teams):
+        for a, b in zip(first, second):
+            assert torch.equal(a, b)
+    else:
+        for a, b in zip(first, second):
+            scale = float(a.abs().max())
+            assert float((a - b).abs().max()) <= 1e-6 * max(scale, 1e-30)
+
