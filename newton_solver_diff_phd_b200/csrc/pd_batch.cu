@@ -659,6 +659,30 @@ struct GraphKey {
 
 }  // namespace
 
+// Launch-plan buffers of one instance planned for its team: the batch owns
+// them, so a later batch over the same solvers cannot invalidate this one.
+struct TeamPlanBuffers {
+  DeviceBuffer s_part, st_part, s_rowlist, s_nshort, st_rowlist, st_nshort, s_off4, s_col4, s_val4, st_off4, st_col4,
+      st_val4, partials, b_partials;
+  void take(PdSolver* s) {
+    s_part.swap(s->d_s_part);
+    st_part.swap(s->d_st_part);
+    s_rowlist.swap(s->d_s_rowlist);
+    s_nshort.swap(s->d_s_nshort);
+    st_rowlist.swap(s->d_st_rowlist);
+    st_nshort.swap(s->d_st_nshort);
+    s_off4.swap(s->d_s_off4);
+    s_col4.swap(s->d_s_col4);
+    s_val4.swap(s->d_s_val4);
+    st_off4.swap(s->d_st_off4);
+    st_col4.swap(s->d_st_col4);
+    st_val4.swap(s->d_st_val4);
+    partials.swap(s->d_partials);
+    b_partials.swap(s->b_partials);
+    s->plan_valid = false;
+  }
+};
+
 struct PdBatch {
   int schedule = PD_BATCH_TEAMS;
   int device = 0;
@@ -668,6 +692,8 @@ struct PdBatch {
   std::vector<PdSolver*> solvers;
   std::vector<int64_t> particle_offsets, element_offsets;
   std::vector<std::unique_ptr<InstanceBuffers>> buffers;
+  std::vector<std::unique_ptr<TeamPlanBuffers>> team_plans;
+  std::vector<uint64_t> generations;  // of every solver when the batch was created
   DeviceBuffer d_instances, d_local_tasks, d_gather_tasks, d_s_tasks, d_st_tasks, d_control, d_io, d_log;
   DeviceBuffer d_task_begin, d_n_active, d_active, d_prefix;
   int grid[pdb200::kTaskKinds] = {1, 1, 1, 1};
@@ -1162,20 +1188,24 @@ int create_teams(PdBatch* batch, const PdBatchOptions& opts) {
     if (best < 0) break;
     teams[best] += 1;
   }
-  // Plans, argument blocks and queues.
+  // Plans, argument blocks and queues. Each instance is planned for its team,
+  // its argument blocks take the plan's pointers, and the batch takes the
+  // plan's buffers (the solver plans its single-instance launch again when it
+  // next steps on its own).
   size_t smem = 0;
+  std::vector<pdb200::StepArgs> forward(count);
+  std::vector<pdb200::AdjointArgs> adjoint(count);
+  batch->team_plans.clear();
   for (int i = 0; i < count; ++i) {
     PdSolver* s = batch->solvers[i];
     if (int status = pd_plan_launch(s, batch->team_size[i], budget)) return status;
     if (int status = pd_ensure_adjoint_buffers(s)) return status;
     smem = std::max(smem, s->smem);
-  }
-  std::vector<pdb200::StepArgs> forward(count);
-  std::vector<pdb200::AdjointArgs> adjoint(count);
-  for (int i = 0; i < count; ++i) {
-    fill_step_args(batch->solvers[i], &forward[i]);
-    fill_adjoint_args(batch->solvers[i], &adjoint[i]);
+    fill_step_args(s, &forward[i]);
+    fill_adjoint_args(s, &adjoint[i]);
     forward[i].timers = nullptr;
+    batch->team_plans.emplace_back(new TeamPlanBuffers());
+    batch->team_plans.back()->take(s);
   }
   std::vector<int> class_begin(classes + 1, 0), class_order;
   for (int c = 0; c < classes; ++c) {
@@ -1327,6 +1357,7 @@ extern "C" int pd_batch_create(PdSolver* const* solvers, int32_t count, const Pd
   }
   batch->particle_offsets.push_back(particles);
   batch->element_offsets.push_back(elements);
+  for (int i = 0; i < count; ++i) batch->generations.push_back(solvers[i]->generation);
   batch->schedule = opts.schedule;
   int max_iterations = 0;
   for (int i = 0; i < count; ++i) max_iterations = std::max(max_iterations, solvers[i]->options.max_iterations);
@@ -1526,6 +1557,17 @@ int capture_team_rollout(PdBatch* b, const pdb200::TeamLaunch& launch, bool adjo
 
 }  // namespace
 
+// A batch holds pointers into its solvers' buffers: after a rebuild or a
+// window change reallocated them, it must be created again.
+static int check_generations(const PdBatch* batch) {
+  for (size_t i = 0; i < batch->solvers.size(); ++i) {
+    if (batch->solvers[i]->generation != batch->generations[i])
+      return pd_set_error(PD_ERR_STATE, "a batched solver was rebuilt or resized after the batch was created; "
+                                        "create the batch again");
+  }
+  return PD_OK;
+}
+
 extern "C" int pd_batch_forward(PdBatch* batch, int32_t steps, double dt, const double gravity[3], const void* q0,
                                 const void* qd0, const void* forces, int64_t force_step_stride, void* q_traj,
                                 void* qd_traj, double* x_record, void* stream) {
@@ -1538,6 +1580,7 @@ extern "C" int pd_batch_forward(PdBatch* batch, int32_t steps, double dt, const 
     if (!s->built || s->stale || s->built_dt != dt)
       return pd_set_error(PD_ERR_STATE, "every batched solver must be built (pd_build) for this dt");
   }
+  if (int status = check_generations(batch)) return status;
   PD_CUDA(cudaSetDevice(batch->device));
   GraphKey key;
   key.steps = steps;
@@ -1589,6 +1632,7 @@ extern "C" int pd_batch_backward(PdBatch* batch, int32_t steps, double dt, const
     if (!s->built || s->stale || s->built_dt != dt)
       return pd_set_error(PD_ERR_STATE, "the batched adjoint needs the factors of its rollout (same dt)");
   }
+  if (int status = check_generations(batch)) return status;
   PD_CUDA(cudaSetDevice(batch->device));
   GraphKey key;
   key.steps = steps;
@@ -1664,6 +1708,7 @@ extern "C" int pd_batch_forward_stepwise(PdBatch* batch, int32_t steps, double d
     if (!s->built || s->stale || s->built_dt != dt)
       return pd_set_error(PD_ERR_STATE, "every batched solver must be built (pd_build) for this dt");
   }
+  if (int status = check_generations(batch)) return status;
   PD_CUDA(cudaSetDevice(batch->device));
   GraphKey key;
   key.steps = steps;

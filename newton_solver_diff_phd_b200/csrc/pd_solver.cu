@@ -291,10 +291,12 @@ int pd_set_anderson_window(PdSolver* solver, int32_t window) {
   if (solver->d_hist_x.bytes < need) {
     PD_CUDA(solver->d_hist_x.allocate(need));
     PD_CUDA(solver->d_hist_g.allocate(need));
+    solver->generation += 1;
   }
   if (solver->b_hist_x.ptr != nullptr && solver->b_hist_x.bytes < need) {
     PD_CUDA(solver->b_hist_x.allocate(need));
     PD_CUDA(solver->b_hist_g.allocate(need));
+    solver->generation += 1;
   }
   solver->options = o;
   return PD_OK;
@@ -478,6 +480,13 @@ int pd_plan_launch(PdSolver* s, int blocks, int budget) {
   return PD_OK;
 }
 
+int pd_ensure_plan(PdSolver* s) {
+  if (s->plan_valid) return PD_OK;
+  if (int status = pd_plan_launch(s, s->default_blocks, s->default_budget)) return status;
+  s->plan_valid = true;
+  return PD_OK;
+}
+
 int pd_build(PdSolver* s, double dt) {
   if (s == nullptr) return fail(PD_ERR_INVALID, "null solver");
   if (!std::isfinite(dt) || dt <= 0.0) return fail(PD_ERR_INVALID, "dt must be finite and positive");
@@ -629,6 +638,9 @@ int pd_build(PdSolver* s, double dt) {
     // 16 KB: static shared memory of the step kernels (the contact section's
     // 32 x 33 Cholesky tile included).
     if (int status = pd_plan_launch(s, blocks, optin - 16 * 1024)) return status;
+    s->default_blocks = blocks;
+    s->default_budget = optin - 16 * 1024;
+    s->plan_valid = true;
     int per_sm_forward = 0, per_sm_adjoint = 0;
     PD_CUDA(pdb200::forward_step_max_blocks(s->options.precision, s->smem, &per_sm_forward));
     PD_CUDA(pdb200::adjoint_step_max_blocks(s->options.precision, s->smem, &per_sm_adjoint));
@@ -651,6 +663,7 @@ int pd_build(PdSolver* s, double dt) {
   s->built = true;
   s->stale = false;
   s->built_dt = dt;
+  s->generation += 1;
   if (s->has_friction) {
     if (int status = pd_build_frictional_panel(s)) return status;
   }
@@ -762,6 +775,7 @@ int pd_step(PdSolver* s, const void* q, const void* qd, const void* f, const voi
   if (!s->built || s->stale || s->built_dt != dt)
     return fail(PD_ERR_STATE, "SolverDiffPhD must rebuild its factor (pd_build) for this dt and model");
   PD_CUDA(cudaSetDevice(s->device));
+  if (int status = pd_ensure_plan(s)) return status;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   StepArgs a{};
   fill_step_args(s, &a);
@@ -890,6 +904,7 @@ int pd_backward_contact(PdSolver* s, const double* x_record, const float* activa
   if (!s->built || s->stale || s->built_dt != dt)
     return fail(PD_ERR_STATE, "the backward pass needs the factor of its recorded step (same dt and model)");
   PD_CUDA(cudaSetDevice(s->device));
+  if (int status = pd_ensure_plan(s)) return status;
   if (int status = ensure_adjoint_buffers(s)) return status;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const size_t fvec = static_cast<size_t>(3) * s->n * (s->options.state_precision ? sizeof(double) : sizeof(float));

@@ -6,6 +6,7 @@
 
 #include <cstdint>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/pd_b200.h"
@@ -27,6 +28,8 @@ extern "C" {
 // Launch plan of a built solver for a team of `blocks` blocks with `budget`
 // bytes of dynamic shared memory (pd_solver.cu).
 int pd_plan_launch(PdSolver* s, int blocks, int budget);
+// The single-instance plan of the last build, planned again if a batch took it.
+int pd_ensure_plan(PdSolver* s);
 // The fields of the step / adjoint arguments that do not change between
 // calls (pd_solver.cu); the adjoint buffers must exist (pd_ensure_adjoint_buffers).
 void fill_step_args(const PdSolver* s, pdb200::StepArgs* a);
@@ -89,6 +92,11 @@ struct DeviceBuffer {
   T* as() const {
     return static_cast<T*>(ptr);
   }
+  // Exchanges the allocations of two buffers (ownership moves, pointers stay valid).
+  void swap(DeviceBuffer& other) {
+    std::swap(ptr, other.ptr);
+    std::swap(bytes, other.bytes);
+  }
 };
 
 struct PdSolver {
@@ -118,6 +126,14 @@ struct PdSolver {
   double nh_mu = 0.0, nh_lame = 0.0, nh_penalty = 0.0;
   int blocks = 0;
   int max_blocks = 0;
+  // The single-instance launch plan of the last build; a batch that plans the
+  // solver for a team takes that plan's buffers and leaves plan_valid false,
+  // so the next single-instance call plans again.
+  int default_blocks = 0, default_budget = 0;
+  bool plan_valid = false;
+  // Bumped whenever a build or a window change reallocates buffers that a
+  // batch's argument blocks point to; a batch refuses to run after a change.
+  uint64_t generation = 0;
   // Launch plan of the sparse products.
   pdb200::SpmvPlan plan_s{}, plan_st{};
   int resident = 0, stage_vector = 0, vector_smem_offset = 0;

@@ -329,3 +329,26 @@ def test_adjoint_lanes_from_measured_adjoint_durations_keep_the_gradients():
             scale = float(a.abs().max())
             assert float((a - b).abs().max()) <= 1e-6 * max(scale, 1e-30)
 
+
+
+def test_a_second_batch_over_the_same_solvers_leaves_the_first_valid():
+    """Each batch owns its instances' team plans: building another batch (other team
+    sizes) over the same solvers, or stepping a solver alone, does not disturb it."""
+    instances = _instances("fp64")
+    first, q, _, _, status, _ = _batched(instances, team_nnz=2048, team_samples=64)
+    second, q2, _, _, _, _ = _batched(instances, team_nnz=1 << 20, team_samples=1 << 20)
+    assert not np.array_equal(first.team_sizes()[0], second.team_sizes()[0])
+    _plain(*instances[0])  # the solver plans its single-instance launch again
+    q0 = first.concat([m.particle_q for m, _, _ in instances])
+    forces = first.concat([f for _, _, f in instances])
+    again, _, _ = first.rollout(q0, torch.zeros_like(q0), forces, STEPS)
+    assert torch.equal(again, q)
+
+
+def test_a_batch_refuses_to_run_after_its_solvers_were_resized():
+    instances = _instances("fp64", window=3)
+    batch, *_ = _batched(instances)
+    instances[0][1].set_anderson_window(8)  # grows (reallocates) the history
+    q0 = batch.concat([m.particle_q for m, _, _ in instances])
+    with pytest.raises(RuntimeError):
+        batch.rollout(q0, torch.zeros_like(q0), batch.concat([f for _, _, f in instances]), STEPS)
