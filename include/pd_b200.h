@@ -232,6 +232,12 @@ int pd_backward_contact(PdSolver* solver, const double* x_record, const float* a
                         const void* gq_out, const void* gqd_out, void* gq, void* gqd, void* gf, void* gdirichlet,
                         double* gmaterials, float* gactivations, const double* multiplier, const double* omega,
                         const double* normal, void* stream);
+/* How pd_backward_contact solves two or more selected columns. 1: side by
+   side, up to 64 per launch, each on its own lane of blocks with its own
+   vectors (the reference's batches of columns, adjoint.py:666-806); 0: one
+   launch per column, one after the other. Both give the same gradients to
+   rounding. */
+int pd_set_woodbury_lanes(PdSolver* solver, int32_t enabled);
 
 /* Device buffer of 8 uint64 nanosecond accumulators for the per-phase timers
    of a library built with -DPD_PHASE_TIMERS (profiling); ignored otherwise.

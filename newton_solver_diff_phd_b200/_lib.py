@@ -112,6 +112,7 @@ SIGNATURES = {
     "pd_set_frictional_boundary": ([_P, _I32, _P, _I32, _P, _D, _D, _I32, _I32, _P, _I32, _P], ctypes.c_int),
     "pd_frictional_buffers": ([_P, ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_I32)], ctypes.c_int),
     "pd_frictional_state": ([_P, _P, _P, _P, _P, _P], ctypes.c_int),
+    "pd_set_woodbury_lanes": ([_P, _I32], ctypes.c_int),
     "pd_build": ([_P, _D], ctypes.c_int),
     "pd_factor_stats": ([_P, ctypes.POINTER(_I64), ctypes.POINTER(_I64), ctypes.POINTER(_I64)], ctypes.c_int),
     "pd_step": ([_P, _P, _P, _P, _P, _P, _D, _P, _P, _P, _P], ctypes.c_int),

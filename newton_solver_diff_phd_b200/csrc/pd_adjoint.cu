@@ -1050,6 +1050,58 @@ cudaError_t team_adjoint_max_blocks(int precision, size_t smem, int* blocks_per_
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kernel, kBlock, smem);
 }
 
+// Columns of the contact projection (W_T = (A - K)^{-1} J^T), one work item
+// per column: the single-instance adjoint fixed point (mode 1) with the
+// column's own vectors, by the lane's team, as many columns at once as there
+// are lanes (the reference solves them in batches, adjoint.py:666-806).
+template <typename TL, typename TV>
+__global__ void __launch_bounds__(kBlock, 2) team_column_kernel(const TeamLaunch launch) {
+  extern __shared__ __align__(16) char dyn_smem[];
+  __shared__ AdjointArgs s_args;
+  Team lane_team;
+  const int lane = lane_of_block(launch, lane_team);
+  GridBarrier* barrier = &launch.lane_barrier[lane];
+  bool solo = false;
+  for (;;) {
+    Team team;
+    const int instance = next_work(launch, lane, lane_team, solo, team);
+    if (instance < 0) return;
+    copy_arguments(launch.adjoint + instance, &s_args);
+    __syncthreads();
+    if (threadIdx.x == 0) s_args.barrier = barrier;
+    __syncthreads();
+    if (!adjoint_step_body<TL, TV>(s_args, team, dyn_smem)) return;
+    if (!grid_sync(barrier, s_args.status, team.size, team.rank)) return;
+  }
+}
+
+static const void* team_columns(int precision) {
+  if (precision == 0) return reinterpret_cast<const void*>(&team_column_kernel<double, double>);
+  if (precision == 1) return reinterpret_cast<const void*>(&team_column_kernel<double, float>);
+  return reinterpret_cast<const void*>(&team_column_kernel<float, float>);
+}
+
+cudaError_t launch_team_columns(const TeamLaunch& launch, int blocks, int precision, size_t smem, cudaStream_t stream) {
+  void* params[] = {const_cast<TeamLaunch*>(&launch)};
+  return cudaLaunchCooperativeKernel(team_columns(precision), dim3(blocks), dim3(kBlock), params, smem, stream);
+}
+
+cudaError_t team_columns_max_blocks(int precision, size_t smem, int* blocks_per_sm) {
+  const void* kernel = team_columns(precision);
+  int device = 0, optin = 0;
+  cudaError_t status = cudaGetDevice(&device);
+  if (status != cudaSuccess) return status;
+  status = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+  if (status != cudaSuccess) return status;
+  cudaFuncAttributes attributes{};
+  status = cudaFuncGetAttributes(&attributes, kernel);
+  if (status != cudaSuccess) return status;
+  status = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                optin - static_cast<int>(attributes.sharedSizeBytes));
+  if (status != cudaSuccess) return status;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kernel, kBlock, smem);
+}
+
 // precision 0: FP64; 1: FP64 Jacobians, FP32 factor products; 2: FP32 Jacobians and factor.
 static const void* adjoint_kernel(int precision) {
   if (precision == 0) return reinterpret_cast<const void*>(&adjoint_step_kernel<double, double>);

@@ -659,30 +659,6 @@ struct GraphKey {
 
 }  // namespace
 
-// Launch-plan buffers of one instance planned for its team: the batch owns
-// them, so a later batch over the same solvers cannot invalidate this one.
-struct TeamPlanBuffers {
-  DeviceBuffer s_part, st_part, s_rowlist, s_nshort, st_rowlist, st_nshort, s_off4, s_col4, s_val4, st_off4, st_col4,
-      st_val4, partials, b_partials;
-  void take(PdSolver* s) {
-    s_part.swap(s->d_s_part);
-    st_part.swap(s->d_st_part);
-    s_rowlist.swap(s->d_s_rowlist);
-    s_nshort.swap(s->d_s_nshort);
-    st_rowlist.swap(s->d_st_rowlist);
-    st_nshort.swap(s->d_st_nshort);
-    s_off4.swap(s->d_s_off4);
-    s_col4.swap(s->d_s_col4);
-    s_val4.swap(s->d_s_val4);
-    st_off4.swap(s->d_st_off4);
-    st_col4.swap(s->d_st_col4);
-    st_val4.swap(s->d_st_val4);
-    partials.swap(s->d_partials);
-    b_partials.swap(s->b_partials);
-    s->plan_valid = false;
-  }
-};
-
 struct PdBatch {
   int schedule = PD_BATCH_TEAMS;
   int device = 0;
@@ -692,6 +668,8 @@ struct PdBatch {
   std::vector<PdSolver*> solvers;
   std::vector<int64_t> particle_offsets, element_offsets;
   std::vector<std::unique_ptr<InstanceBuffers>> buffers;
+  // Launch-plan buffers of every instance planned for its team: the batch owns
+  // them, so a later batch over the same solvers cannot invalidate this one.
   std::vector<std::unique_ptr<TeamPlanBuffers>> team_plans;
   std::vector<uint64_t> generations;  // of every solver when the batch was created
   DeviceBuffer d_instances, d_local_tasks, d_gather_tasks, d_s_tasks, d_st_tasks, d_control, d_io, d_log;

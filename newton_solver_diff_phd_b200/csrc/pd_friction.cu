@@ -212,4 +212,10 @@ int pd_frictional_state(PdSolver* s, double* multiplier, double* omega, double* 
   return PD_OK;
 }
 
+int pd_set_woodbury_lanes(PdSolver* s, int32_t enabled) {
+  if (s == nullptr) return pd_set_error(PD_ERR_INVALID, "null solver");
+  s->woodbury_lanes = enabled != 0;
+  return PD_OK;
+}
+
 }  // extern "C"

@@ -152,6 +152,9 @@ cudaError_t launch_team_forward(const TeamLaunch& launch, int blocks, int precis
 cudaError_t team_forward_max_blocks(int precision, size_t smem, int* blocks_per_sm);
 cudaError_t launch_team_adjoint(const TeamLaunch& launch, int blocks, int precision, size_t smem, cudaStream_t stream);
 cudaError_t team_adjoint_max_blocks(int precision, size_t smem, int* blocks_per_sm);
+// Woodbury columns on lanes: one mode-1 adjoint fixed point per work item.
+cudaError_t launch_team_columns(const TeamLaunch& launch, int blocks, int precision, size_t smem, cudaStream_t stream);
+cudaError_t team_columns_max_blocks(int precision, size_t smem, int* blocks_per_sm);
 
 cudaError_t launch_forward_step(const StepArgs& args, int blocks, int precision, size_t smem, cudaStream_t stream);
 cudaError_t forward_step_max_blocks(int precision, size_t smem, int* blocks_per_sm);

@@ -98,6 +98,17 @@ __global__ void woodbury_rows_kernel(const int* nodes, const double* multiplier,
   }
 }
 
+// Right-hand sides of columns first .. first + count - 1, one [n][3] vector each.
+__global__ void woodbury_seeds_kernel(int n, const int* order, int first, int count, const int* row_node,
+                                      const double* row_vector, double* seeds) {
+  const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= static_cast<long long>(count) * n) return;
+  const int k = static_cast<int>(t / n), i = static_cast<int>(t % n);
+  const int row = order[first + k];
+  const V3<double> value = i == row_node[row] ? load3d(row_vector, row) : v3<double>(0.0, 0.0, 0.0);
+  store3(seeds + static_cast<size_t>(k) * 3 * n, i, value);
+}
+
 // Right-hand side of column k: the row vector at its particle (_batch_setup, adjoint.py:667-689).
 __global__ void woodbury_seed_kernel(int n, const int* order, int k, const int* row_node, const double* row_vector,
                                      double* seed) {
@@ -185,6 +196,153 @@ static int ensure_woodbury_buffers(PdSolver* s, int rows) {
   return PD_OK;
 }
 
+// The selected columns side by side: the solver is planned for a team of T
+// blocks (T from the factor's nnz and the element samples, as a batch sizes
+// its teams; the solver's own plan is set aside and put back), and every lane
+// of one launch solves one column with its own vectors, up to 64 columns per
+// launch. Each column keeps its own stop rule, as in the sequential path.
+static int woodbury_columns_team(PdSolver* s, const pdb200::AdjointArgs& column, int selected, cudaStream_t st) {
+  const int n = s->n;
+  int sms = 0, optin = 0, smem_per_sm = 0, per_sm = 0;
+  PD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device));
+  PD_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, s->device));
+  PD_CUDA(cudaDeviceGetAttribute(&smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, s->device));
+  PD_CUDA(pdb200::team_columns_max_blocks(s->options.precision, 0, &per_sm));
+  const int occupancy = std::max(1, std::min(per_sm, 2));
+  const int grid_cap = occupancy * sms;
+  const int budget = std::min(optin, smem_per_sm / occupancy) - 10 * 1024;
+  const double nnz = static_cast<double>(s->factor.s.columns.size());
+  const double samples = static_cast<double>(s->ne) * (s->hex ? 8 : 1);
+  const double want = std::max(1.0, std::max(nnz / 65536.0, samples / 512.0));
+  int team = 1;
+  while (team < 64 && team * 2 <= grid_cap && team * 1.5 < want) team *= 2;
+  const int capacity = std::max(1, std::min(64, grid_cap / team));
+  // Plan for the team, keep that plan's buffers for the launches, put the
+  // solver's own plan back (the mode-2 pass after the columns uses it).
+  SavedPlan saved;
+  saved.save(s);
+  TeamPlanBuffers team_plan;
+  pdb200::AdjointArgs planned{};
+  size_t smem = 0;
+  {
+    const int status = pd_plan_launch(s, team, budget);
+    if (status == PD_OK) {
+      fill_adjoint_args(s, &planned);
+      smem = s->smem;
+      team_plan.take(s);
+    }
+    saved.restore(s);
+    if (status != PD_OK) return status;
+  }
+  int blocks_per_sm = 0;
+  PD_CUDA(pdb200::team_columns_max_blocks(s->options.precision, smem, &blocks_per_sm));
+  if (blocks_per_sm < 1 || capacity * team > blocks_per_sm * sms)
+    return pd_set_error(PD_ERR_CUDA, "the column lanes do not fit the co-resident grid");
+  // The column's arguments with the team plan's product layout.
+  pdb200::AdjointArgs base = column;
+  base.s_part = planned.s_part;
+  base.st_part = planned.st_part;
+  base.plan_s = planned.plan_s;
+  base.plan_st = planned.plan_st;
+  base.resident = planned.resident;
+  base.stage_vector = planned.stage_vector;
+  base.vector_smem_offset = planned.vector_smem_offset;
+  // Per-column buffers for `capacity` columns.
+  const size_t vec = static_cast<size_t>(3) * n;
+  const size_t window = static_cast<size_t>(s->options.anderson_window) + 1;
+  const size_t contrib = static_cast<size_t>(s->ne) * s->corners * 3;
+  const size_t partials = static_cast<size_t>(team) * pdb200::kPartialStride;
+  const auto ensure = [](DeviceBuffer& buffer, size_t bytes) -> cudaError_t {
+    return buffer.bytes >= bytes ? cudaSuccess : buffer.allocate(bytes);
+  };
+  const size_t slots = static_cast<size_t>(capacity);
+  PD_CUDA(ensure(s->w_team_args, slots * sizeof(pdb200::AdjointArgs)));
+  PD_CUDA(ensure(s->w_team_lane_start, (slots + 1) * sizeof(int)));
+  PD_CUDA(ensure(s->w_team_lane_class, slots * sizeof(int)));
+  PD_CUDA(ensure(s->w_team_class_begin, 2 * sizeof(int)));
+  PD_CUDA(ensure(s->w_team_class_order, slots * sizeof(int)));
+  PD_CUDA(ensure(s->w_team_class_head, sizeof(unsigned)));
+  PD_CUDA(ensure(s->w_team_lane_slot, slots * sizeof(int)));
+  PD_CUDA(ensure(s->w_team_barriers, slots * sizeof(pdb200::GridBarrier)));
+  PD_CUDA(ensure(s->w_team_vectors, slots * 6 * vec * sizeof(double)));
+  PD_CUDA(ensure(s->w_team_hist, slots * 2 * window * vec * sizeof(double)));
+  PD_CUDA(ensure(s->w_team_contrib, slots * contrib * sizeof(double)));
+  PD_CUDA(ensure(s->w_team_ints, slots * 32 * sizeof(int)));
+  PD_CUDA(ensure(s->w_team_doubles, slots * 16 * sizeof(double)));
+  PD_CUDA(ensure(s->w_team_partials, slots * partials * sizeof(double)));
+  PD_CUDA(ensure(s->w_team_seeds, slots * vec * sizeof(double)));
+  std::vector<int> lane_start(capacity + 1), lane_class(capacity, 0), order(capacity);
+  for (int k = 0; k <= capacity; ++k) lane_start[k] = k * team;
+  for (int k = 0; k < capacity; ++k) order[k] = k;
+  PD_CUDA(cudaMemcpy(s->w_team_lane_start.ptr, lane_start.data(), lane_start.size() * sizeof(int),
+                     cudaMemcpyHostToDevice));
+  PD_CUDA(cudaMemcpy(s->w_team_lane_class.ptr, lane_class.data(), lane_class.size() * sizeof(int),
+                     cudaMemcpyHostToDevice));
+  PD_CUDA(cudaMemcpy(s->w_team_class_order.ptr, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice));
+  double* vectors = s->w_team_vectors.as<double>();
+  double* hist = s->w_team_hist.as<double>();
+  int* ints = s->w_team_ints.as<int>();
+  double* doubles = s->w_team_doubles.as<double>();
+  std::vector<pdb200::AdjointArgs> args(capacity);
+  for (int first = 0; first < selected; first += capacity) {
+    const int count = std::min(capacity, selected - first);
+    const long long entries = static_cast<long long>(count) * n;
+    pdb200::woodbury_seeds_kernel<<<static_cast<unsigned>((entries + 255) / 256), 256, 0, st>>>(
+        n, s->w_order.as<int>(), first, count, s->w_row_node.as<int>(), s->w_row_vector.as<double>(),
+        s->w_team_seeds.as<double>());
+    PD_CUDA(cudaGetLastError());
+    for (int k = 0; k < count; ++k) {
+      pdb200::AdjointArgs& a = args[k];
+      a = base;
+      double* v = vectors + static_cast<size_t>(k) * 6 * vec;
+      a.rhs = v;
+      a.base = v + vec;
+      a.prev = v + 2 * vec;
+      a.work = v + 3 * vec;
+      a.y = v + 4 * vec;
+      a.raw = v + 5 * vec;
+      a.solution = s->w_columns.as<double>() + static_cast<size_t>(first + k) * vec;
+      a.seed = s->w_team_seeds.as<double>() + static_cast<size_t>(k) * vec;
+      a.hist_x = hist + static_cast<size_t>(k) * 2 * window * vec;
+      a.hist_g = a.hist_x + window * vec;
+      a.contrib = s->w_team_contrib.as<double>() + static_cast<size_t>(k) * contrib;
+      // 32 ints a column: Anderson state [8], accept, iteration, active, control [8] at 16.
+      a.aa_state = ints + 32 * k;
+      a.aa_accept = ints + 32 * k + 8;
+      a.iteration = ints + 32 * k + 9;
+      a.active = ints + 32 * k + 10;
+      a.control_i = ints + 32 * k + 16;
+      // 16 doubles a column: Anderson coefficients [kMaxWindow = 8], control [8].
+      a.aa_gamma = doubles + 16 * k;
+      a.control_d = doubles + 16 * k + pdb200::kMaxWindow;
+      a.partials = s->w_team_partials.as<double>() + static_cast<size_t>(k) * partials;
+    }
+    const int class_begin[2] = {0, count};
+    PD_CUDA(cudaMemcpyAsync(s->w_team_args.ptr, args.data(), count * sizeof(pdb200::AdjointArgs),
+                            cudaMemcpyHostToDevice, st));
+    PD_CUDA(cudaMemcpyAsync(s->w_team_class_begin.ptr, class_begin, sizeof(class_begin), cudaMemcpyHostToDevice, st));
+    PD_CUDA(cudaMemsetAsync(s->w_team_class_head.ptr, 0, sizeof(unsigned), st));
+    PD_CUDA(cudaMemsetAsync(s->w_team_barriers.ptr, 0, count * sizeof(pdb200::GridBarrier), st));
+    pdb200::TeamLaunch launch{};
+    launch.adjoint = s->w_team_args.as<pdb200::AdjointArgs>();
+    launch.lane_start = s->w_team_lane_start.as<int>();
+    launch.lane_class = s->w_team_lane_class.as<int>();
+    launch.class_begin = s->w_team_class_begin.as<int>();
+    launch.class_order = s->w_team_class_order.as<int>();
+    launch.count = count;
+    launch.lanes = count;
+    launch.solo_class = -1;
+    launch.class_head = s->w_team_class_head.as<unsigned>();
+    launch.lane_slot = s->w_team_lane_slot.as<int>();
+    launch.lane_barrier = s->w_team_barriers.as<pdb200::GridBarrier>();
+    launch.status = s->d_status.as<int>();
+    PD_CUDA(pdb200::launch_team_columns(launch, count * team, s->options.precision, smem, st));
+    // The host argument blocks and class range are reused by the next chunk.
+    PD_CUDA(cudaStreamSynchronize(st));
+  }
+  return PD_OK;
+}
+
 int pd_woodbury_gradients(PdSolver* s, const pdb200::AdjointArgs& full, const double* multiplier, const double* omega,
                           const double* normal, cudaStream_t st) {
   const int count = s->fc.count;
@@ -211,13 +369,20 @@ int pd_woodbury_gradients(PdSolver* s, const pdb200::AdjointArgs& full, const do
   column.max_iterations = std::min(s->options.max_iterations, pdb200::kWoodburyMaxIterations);
   column.iteration = control + 1;
   column.active = control + 2;
-  for (int k = 0; k < selected; ++k) {
-    pdb200::woodbury_seed_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, s->w_order.as<int>(), k, s->w_row_node.as<int>(),
-                                                                  s->w_row_vector.as<double>(), s->w_seed.as<double>());
-    PD_CUDA(cudaMemsetAsync(s->d_barrier.ptr, 0, sizeof(pdb200::GridBarrier), st));
-    PD_CUDA(pdb200::launch_adjoint_step(column, s->blocks, s->options.precision, s->smem, st));
-    PD_CUDA(cudaMemcpyAsync(s->w_columns.as<double>() + static_cast<size_t>(k) * 3 * n, s->b_solution.ptr, vec,
-                            cudaMemcpyDeviceToDevice, st));
+  if (selected >= 2 && s->woodbury_lanes) {
+    // Side by side on lanes of one launch, as the reference's column batches.
+    if (int status = woodbury_columns_team(s, column, selected, st)) return status;
+  } else {
+    for (int k = 0; k < selected; ++k) {
+      pdb200::woodbury_seed_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, s->w_order.as<int>(), k,
+                                                                    s->w_row_node.as<int>(),
+                                                                    s->w_row_vector.as<double>(),
+                                                                    s->w_seed.as<double>());
+      PD_CUDA(cudaMemsetAsync(s->d_barrier.ptr, 0, sizeof(pdb200::GridBarrier), st));
+      PD_CUDA(pdb200::launch_adjoint_step(column, s->blocks, s->options.precision, s->smem, st));
+      PD_CUDA(cudaMemcpyAsync(s->w_columns.as<double>() + static_cast<size_t>(k) * 3 * n, s->b_solution.ptr, vec,
+                              cudaMemcpyDeviceToDevice, st));
+    }
   }
   pdb200::woodbury_project_kernel<<<1, pdb200::kBlock, 0, st>>>(
       n, s->d_free.as<int>(), s->w_mu.as<double>(), s->w_columns.as<double>(), s->w_order.as<int>(), control,

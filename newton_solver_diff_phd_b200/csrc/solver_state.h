@@ -162,8 +162,14 @@ struct PdSolver {
       fc_surface;
   // Contact projection of the parameter gradients (pd_woodbury.cu), sized for w_rows rows.
   int w_rows = 0;
+  bool woodbury_lanes = false;  // columns side by side on lanes (false: one launch per column)
   DeviceBuffer w_row_node, w_row_vector, w_value, w_selected, w_order, w_control, w_columns, w_gram, w_coefficients,
       w_permutation, w_work, w_seed, w_mu;
+  // Columns solved side by side on lanes of one launch: argument blocks,
+  // lanes and each column's own vectors.
+  DeviceBuffer w_team_args, w_team_lane_start, w_team_lane_class, w_team_class_begin, w_team_class_order,
+      w_team_class_head, w_team_lane_slot, w_team_barriers, w_team_vectors, w_team_hist, w_team_contrib,
+      w_team_ints, w_team_doubles, w_team_partials, w_team_seeds;
   DeviceBuffer d_wc, d_wv, d_wn, d_wm, d_mdir, d_mtarget;
   DeviceBuffer d_s_off, d_s_col, d_s_val, d_s_val32, d_st_off, d_st_col, d_st_val, d_st_val32, d_s_part, d_st_part;
   DeviceBuffer d_a_off, d_a_col, d_a_val;
@@ -177,4 +183,65 @@ struct PdSolver {
   DeviceBuffer b_rhs, b_base, b_solution, b_prev, b_work, b_y, b_raw, b_contrib, b_jac, b_hist_x, b_hist_g, b_aa_state,
       b_aa_gamma, b_aa_accept, b_partials, b_iteration, b_active, b_control_d, b_control_i, b_material_scratch,
       b_activation_scratch, b_zero_gq, b_zero_gqd, b_scratch_gq, b_scratch_gqd, b_scratch_gf;
+};
+
+// Buffers of a launch plan planned for a team size (row partitions, row
+// lists, streaming layouts, partial sums), taken out of the solver: the
+// argument blocks filled from that plan stay valid while this object lives,
+// whatever the solver plans next.
+struct TeamPlanBuffers {
+  DeviceBuffer s_part, st_part, s_rowlist, s_nshort, st_rowlist, st_nshort, s_off4, s_col4, s_val4, st_off4, st_col4,
+      st_val4, partials, b_partials;
+  void take(PdSolver* s) {
+    s_part.swap(s->d_s_part);
+    st_part.swap(s->d_st_part);
+    s_rowlist.swap(s->d_s_rowlist);
+    s_nshort.swap(s->d_s_nshort);
+    st_rowlist.swap(s->d_st_rowlist);
+    st_nshort.swap(s->d_st_nshort);
+    s_off4.swap(s->d_s_off4);
+    s_col4.swap(s->d_s_col4);
+    s_val4.swap(s->d_s_val4);
+    st_off4.swap(s->d_st_off4);
+    st_col4.swap(s->d_st_col4);
+    st_val4.swap(s->d_st_val4);
+    partials.swap(s->d_partials);
+    b_partials.swap(s->b_partials);
+    s->plan_valid = false;
+  }
+};
+
+// The whole single-instance launch plan of a solver, set aside while the
+// solver is planned for another team size and put back afterwards (pointers
+// taken from the saved plan stay valid throughout).
+struct SavedPlan {
+  TeamPlanBuffers buffers;
+  int blocks = 0, resident = 0, stage_vector = 0, vector_smem_offset = 0;
+  size_t smem = 0;
+  pdb200::SpmvPlan plan_s{}, plan_st{};
+  bool valid = false;
+  void save(PdSolver* s) {
+    blocks = s->blocks;
+    resident = s->resident;
+    stage_vector = s->stage_vector;
+    vector_smem_offset = s->vector_smem_offset;
+    smem = s->smem;
+    plan_s = s->plan_s;
+    plan_st = s->plan_st;
+    valid = s->plan_valid;
+    buffers.take(s);
+  }
+  void restore(PdSolver* s) {
+    TeamPlanBuffers other;
+    other.take(s);    // releases whatever plan the solver holds now when `other` goes out of scope
+    buffers.take(s);  // swaps the saved buffers back in
+    s->blocks = blocks;
+    s->resident = resident;
+    s->stage_vector = stage_vector;
+    s->vector_smem_offset = vector_smem_offset;
+    s->smem = smem;
+    s->plan_s = plan_s;
+    s->plan_st = plan_st;
+    s->plan_valid = valid;
+  }
 };

@@ -275,3 +275,54 @@ def test_large_contact_set_on_the_team_path_matches_the_oracle():
         assert int((boundary.multiplier > 0).sum()) > 32
         x = solver._x.cpu().numpy()
         q, v = x.astype(np.float32).astype(np.float64), ((x - q) / 0.004).astype(np.float32).astype(np.float64)
+
+
+@pytest.mark.parametrize("friction", [0.0, 0.5])
+def test_woodbury_columns_on_lanes_match_one_launch_per_column(friction):
+    """The contact projection of a 8x6x2 block resting on the floor (63 contacts,
+    up to 189 rows with friction, so more than one launch of 64 lanes): the
+    parameter and state gradients with the columns side by side on lanes equal
+    those of one launch per column, and the lanes' material gradients agree
+    with the oracle's Woodbury projection."""
+    from newton_solver_diff_phd_b200 import Tape
+    from newton_solver_diff_phd_b200 import _lib
+
+    builder = ModelBuilder(gravity=(0.0, 0.0, -9.81))
+    builder.add_soft_grid(pos=(0.0, 0.0, 0.0), rot=None, vel=(0.0, 0.0, 0.0), dim_x=8, dim_y=6, dim_z=2, cell_x=0.05,
+                          cell_y=0.05, cell_z=0.05, density=DENSITY, k_mu=2.0e4, k_lambda=5.0e4, k_damp=0.0)
+    model = builder.finalize("cuda", requires_grad=True)
+    solver = SolverDiffPhD(model, density=DENSITY, frictional_boundary=("planar", (0.0, 0.0, 1.0, 0.0)),
+                           friction=friction, max_iterations=2000, abs_tol=1.0e-12, rel_tol=1.0e-11)
+    q = model.particle_q.cpu().numpy().astype(np.float64)
+    q[:, 2] += 0.0002
+    v = np.tile([0.1, 0.0, -0.5], (model.particle_count, 1))
+    rng = np.random.default_rng(7)
+    gq = rng.standard_normal((model.particle_count, 3)).astype(np.float32)
+    gv = rng.standard_normal((model.particle_count, 3)).astype(np.float32)
+    results = []
+    for lanes in (1, 0):
+        _lib.check(solver._lib.pd_set_woodbury_lanes(solver._handle, lanes))
+        model.tet_materials.grad = torch.zeros_like(model.tet_materials)
+        state_in = _state(model, q, v)
+        state_in.requires_grad_(True)
+        state_out = model.state(requires_grad=True)
+        with Tape() as tape:
+            solver.step(state_in, state_out, None, None, 0.004)
+        solver.check_status()
+        tape.backward(grads={state_out.particle_q: torch.tensor(gq, device="cuda"),
+                             state_out.particle_qd: torch.tensor(gv, device="cuda")})
+        results.append({"materials": model.tet_materials.grad[:, :2].double().cpu().numpy(),
+                        "q": state_in.particle_q.grad.double().cpu().numpy(),
+                        "qd": state_in.particle_qd.grad.double().cpu().numpy()})
+    multiplier, omega, normal, _ = solver.frictional_state()
+    assert int(((multiplier > 0) & (omega >= 0.5)).sum()) > 32
+    for name in results[0]:
+        scale = max(np.abs(results[1][name]).max(), 1.0e-30)
+        np.testing.assert_allclose(results[0][name], results[1][name], rtol=0.0, atol=1.0e-9 * scale, err_msg=name)
+    body = oracle_tet_body(model)
+    oracle = pd_oracle.backward(body, solver._x.cpu().numpy(), 0.004, gq.astype(np.float64), gv.astype(np.float64),
+                                contact=(solver.frictional_vertices, multiplier.cpu().numpy(), omega.cpu().numpy(),
+                                         normal.cpu().numpy(), friction))
+    # The columns are fixed points capped at 120 iterations, the oracle's are direct solves.
+    scale = max(np.abs(oracle["materials"]).max(), 1.0e-30)
+    np.testing.assert_allclose(results[0]["materials"], oracle["materials"], rtol=0.0, atol=1.0e-4 * scale)
