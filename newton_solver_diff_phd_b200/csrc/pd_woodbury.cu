@@ -98,15 +98,16 @@ __global__ void woodbury_rows_kernel(const int* nodes, const double* multiplier,
   }
 }
 
-// Right-hand sides of columns first .. first + count - 1, one [n][3] vector each.
+// Right-hand sides of columns first .. first + count - 1, one [n][3] vector
+// each, `pitch` doubles apart.
 __global__ void woodbury_seeds_kernel(int n, const int* order, int first, int count, const int* row_node,
-                                      const double* row_vector, double* seeds) {
+                                      const double* row_vector, size_t pitch, double* seeds) {
   const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (t >= static_cast<long long>(count) * n) return;
   const int k = static_cast<int>(t / n), i = static_cast<int>(t % n);
   const int row = order[first + k];
   const V3<double> value = i == row_node[row] ? load3d(row_vector, row) : v3<double>(0.0, 0.0, 0.0);
-  store3(seeds + static_cast<size_t>(k) * 3 * n, i, value);
+  store3(seeds + static_cast<size_t>(k) * pitch, i, value);
 }
 
 // Right-hand side of column k: the row vector at its particle (_batch_setup, adjoint.py:667-689).
@@ -247,10 +248,14 @@ static int woodbury_columns_team(PdSolver* s, const pdb200::AdjointArgs& column,
   base.resident = planned.resident;
   base.stage_vector = planned.stage_vector;
   base.vector_smem_offset = planned.vector_smem_offset;
-  // Per-column buffers for `capacity` columns.
+  // Per-column buffers for `capacity` columns. Every vector starts on a
+  // 256-byte boundary (pitch: 3n rounded up to 32 doubles), as a vector of its
+  // own allocation does: the products stage their input vector into shared
+  // memory with 16-byte loads.
   const size_t vec = static_cast<size_t>(3) * n;
+  const size_t pitch = (vec + 31) & ~static_cast<size_t>(31);
   const size_t window = static_cast<size_t>(s->options.anderson_window) + 1;
-  const size_t contrib = static_cast<size_t>(s->ne) * s->corners * 3;
+  const size_t contrib = (static_cast<size_t>(s->ne) * s->corners * 3 + 31) & ~static_cast<size_t>(31);
   const size_t partials = static_cast<size_t>(team) * pdb200::kPartialStride;
   const auto ensure = [](DeviceBuffer& buffer, size_t bytes) -> cudaError_t {
     return buffer.bytes >= bytes ? cudaSuccess : buffer.allocate(bytes);
@@ -264,13 +269,13 @@ static int woodbury_columns_team(PdSolver* s, const pdb200::AdjointArgs& column,
   PD_CUDA(ensure(s->w_team_class_head, sizeof(unsigned)));
   PD_CUDA(ensure(s->w_team_lane_slot, slots * sizeof(int)));
   PD_CUDA(ensure(s->w_team_barriers, slots * sizeof(pdb200::GridBarrier)));
-  PD_CUDA(ensure(s->w_team_vectors, slots * 6 * vec * sizeof(double)));
-  PD_CUDA(ensure(s->w_team_hist, slots * 2 * window * vec * sizeof(double)));
+  PD_CUDA(ensure(s->w_team_vectors, slots * 7 * pitch * sizeof(double)));
+  PD_CUDA(ensure(s->w_team_hist, slots * 2 * window * pitch * sizeof(double)));
   PD_CUDA(ensure(s->w_team_contrib, slots * contrib * sizeof(double)));
   PD_CUDA(ensure(s->w_team_ints, slots * 32 * sizeof(int)));
   PD_CUDA(ensure(s->w_team_doubles, slots * 16 * sizeof(double)));
   PD_CUDA(ensure(s->w_team_partials, slots * partials * sizeof(double)));
-  PD_CUDA(ensure(s->w_team_seeds, slots * vec * sizeof(double)));
+  PD_CUDA(ensure(s->w_team_seeds, slots * pitch * sizeof(double)));
   std::vector<int> lane_start(capacity + 1), lane_class(capacity, 0), order(capacity);
   for (int k = 0; k <= capacity; ++k) lane_start[k] = k * team;
   for (int k = 0; k < capacity; ++k) order[k] = k;
@@ -288,23 +293,23 @@ static int woodbury_columns_team(PdSolver* s, const pdb200::AdjointArgs& column,
     const int count = std::min(capacity, selected - first);
     const long long entries = static_cast<long long>(count) * n;
     pdb200::woodbury_seeds_kernel<<<static_cast<unsigned>((entries + 255) / 256), 256, 0, st>>>(
-        n, s->w_order.as<int>(), first, count, s->w_row_node.as<int>(), s->w_row_vector.as<double>(),
+        n, s->w_order.as<int>(), first, count, s->w_row_node.as<int>(), s->w_row_vector.as<double>(), pitch,
         s->w_team_seeds.as<double>());
     PD_CUDA(cudaGetLastError());
     for (int k = 0; k < count; ++k) {
       pdb200::AdjointArgs& a = args[k];
       a = base;
-      double* v = vectors + static_cast<size_t>(k) * 6 * vec;
+      double* v = vectors + static_cast<size_t>(k) * 7 * pitch;
       a.rhs = v;
-      a.base = v + vec;
-      a.prev = v + 2 * vec;
-      a.work = v + 3 * vec;
-      a.y = v + 4 * vec;
-      a.raw = v + 5 * vec;
-      a.solution = s->w_columns.as<double>() + static_cast<size_t>(first + k) * vec;
-      a.seed = s->w_team_seeds.as<double>() + static_cast<size_t>(k) * vec;
-      a.hist_x = hist + static_cast<size_t>(k) * 2 * window * vec;
-      a.hist_g = a.hist_x + window * vec;
+      a.base = v + pitch;
+      a.prev = v + 2 * pitch;
+      a.work = v + 3 * pitch;
+      a.y = v + 4 * pitch;
+      a.raw = v + 5 * pitch;
+      a.solution = v + 6 * pitch;
+      a.seed = s->w_team_seeds.as<double>() + static_cast<size_t>(k) * pitch;
+      a.hist_x = hist + static_cast<size_t>(k) * 2 * window * pitch;
+      a.hist_g = a.hist_x + window * pitch;
       a.contrib = s->w_team_contrib.as<double>() + static_cast<size_t>(k) * contrib;
       // 32 ints a column: Anderson state [8], accept, iteration, active, control [8] at 16.
       a.aa_state = ints + 32 * k;
@@ -337,6 +342,10 @@ static int woodbury_columns_team(PdSolver* s, const pdb200::AdjointArgs& column,
     launch.lane_barrier = s->w_team_barriers.as<pdb200::GridBarrier>();
     launch.status = s->d_status.as<int>();
     PD_CUDA(pdb200::launch_team_columns(launch, count * team, s->options.precision, smem, st));
+    // The solutions into the [selected][n][3] columns the projection reads.
+    PD_CUDA(cudaMemcpy2DAsync(s->w_columns.as<double>() + static_cast<size_t>(first) * vec, vec * sizeof(double),
+                              vectors + 6 * pitch, 7 * pitch * sizeof(double), vec * sizeof(double), count,
+                              cudaMemcpyDeviceToDevice, st));
     // The host argument blocks and class range are reused by the next chunk.
     PD_CUDA(cudaStreamSynchronize(st));
   }
