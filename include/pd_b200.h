@@ -232,8 +232,8 @@ int pd_backward_contact(PdSolver* solver, const double* x_record, const float* a
                         const void* gq_out, const void* gqd_out, void* gq, void* gqd, void* gf, void* gdirichlet,
                         double* gmaterials, float* gactivations, const double* multiplier, const double* omega,
                         const double* normal, void* stream);
-/* How pd_backward_contact solves two or more selected columns. 1: side by
-   side, up to 64 per launch, each on its own lane of blocks with its own
+/* How pd_backward_contact solves two or more selected columns. 1 (default):
+   side by side, up to 64 per launch, each on its own lane of blocks with its own
    vectors (the reference's batches of columns, adjoint.py:666-806); 0: one
    launch per column, one after the other. Both give the same gradients to
    rounding. */
