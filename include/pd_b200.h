@@ -233,11 +233,15 @@ int pd_backward_contact(PdSolver* solver, const double* x_record, const float* a
                         double* gmaterials, float* gactivations, const double* multiplier, const double* omega,
                         const double* normal, void* stream);
 /* How pd_backward_contact solves two or more selected columns. 1 (default):
-   side by side, up to 64 per launch, each on its own lane of blocks with its own
-   vectors (the reference's batches of columns, adjoint.py:666-806); 0: one
-   launch per column, one after the other. Both give the same gradients to
-   rounding. */
+   side by side, as many per launch as the grid holds, each on its own lane
+   of blocks with its own vectors (the reference solves its columns in
+   batches, adjoint.py:666-806); 0: one launch per column, one after the
+   other. Both give the same gradients to rounding. */
 int pd_set_woodbury_lanes(PdSolver* solver, int32_t enabled);
+/* Blocks per lane of those columns: 0 (default) picks it from nnz(S) and the
+   element samples; 1, 2, 4, ..., 64 fixes it (a tuning knob; the reference
+   has none). Fewer blocks per lane give more lanes per launch. */
+int pd_set_woodbury_team(PdSolver* solver, int32_t blocks);
 
 /* Device buffer of 8 uint64 nanosecond accumulators for the per-phase timers
    of a library built with -DPD_PHASE_TIMERS (profiling); ignored otherwise.

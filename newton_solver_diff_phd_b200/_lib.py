@@ -113,6 +113,7 @@ SIGNATURES = {
     "pd_frictional_buffers": ([_P, ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_I32)], ctypes.c_int),
     "pd_frictional_state": ([_P, _P, _P, _P, _P, _P], ctypes.c_int),
     "pd_set_woodbury_lanes": ([_P, _I32], ctypes.c_int),
+    "pd_set_woodbury_team": ([_P, _I32], ctypes.c_int),
     "pd_build": ([_P, _D], ctypes.c_int),
     "pd_factor_stats": ([_P, ctypes.POINTER(_I64), ctypes.POINTER(_I64), ctypes.POINTER(_I64)], ctypes.c_int),
     "pd_step": ([_P, _P, _P, _P, _P, _P, _D, _P, _P, _P, _P], ctypes.c_int),

@@ -218,4 +218,12 @@ int pd_set_woodbury_lanes(PdSolver* s, int32_t enabled) {
   return PD_OK;
 }
 
+int pd_set_woodbury_team(PdSolver* s, int32_t blocks) {
+  if (s == nullptr) return pd_set_error(PD_ERR_INVALID, "null solver");
+  if (blocks < 0 || blocks > 64 || (blocks & (blocks - 1)) != 0)
+    return pd_set_error(PD_ERR_INVALID, "the Woodbury team must be 0 (automatic) or a power of two up to 64");
+  s->woodbury_team = blocks;
+  return PD_OK;
+}
+
 }  // extern "C"

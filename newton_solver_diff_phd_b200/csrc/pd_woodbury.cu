@@ -198,10 +198,12 @@ static int ensure_woodbury_buffers(PdSolver* s, int rows) {
 }
 
 // The selected columns side by side: the solver is planned for a team of T
-// blocks (T from the factor's nnz and the element samples, as a batch sizes
-// its teams; the solver's own plan is set aside and put back), and every lane
-// of one launch solves one column with its own vectors, up to 64 columns per
-// launch. Each column keeps its own stop rule, as in the sequential path.
+// blocks (T set by pd_set_woodbury_team, else from the factor's nnz and the
+// element samples, as a batch sizes its teams; the solver's own plan is set
+// aside and put back), and every lane of one launch solves one column with
+// its own vectors: as many lanes as the co-resident grid holds (and 8 GB of
+// per-column vectors), the columns split evenly over the launches. Each
+// column keeps its own stop rule, as in the sequential path.
 static int woodbury_columns_team(PdSolver* s, const pdb200::AdjointArgs& column, int selected, cudaStream_t st) {
   const int n = s->n;
   int sms = 0, optin = 0, smem_per_sm = 0, per_sm = 0;
@@ -216,8 +218,24 @@ static int woodbury_columns_team(PdSolver* s, const pdb200::AdjointArgs& column,
   const double samples = static_cast<double>(s->ne) * (s->hex ? 8 : 1);
   const double want = std::max(1.0, std::max(nnz / 65536.0, samples / 512.0));
   int team = 1;
-  while (team < 64 && team * 2 <= grid_cap && team * 1.5 < want) team *= 2;
-  const int capacity = std::max(1, std::min(64, grid_cap / team));
+  if (s->woodbury_team > 0) {
+    team = std::min(s->woodbury_team, grid_cap);
+  } else {
+    while (team < 64 && team * 2 <= grid_cap && team * 1.5 < want) team *= 2;
+  }
+  // Per-column buffers. Every vector starts on a 256-byte boundary (pitch: 3n
+  // rounded up to 32 doubles), as a vector of its own allocation does: the
+  // products stage their input vector into shared memory with 16-byte loads.
+  const size_t vec = static_cast<size_t>(3) * n;
+  const size_t pitch = (vec + 31) & ~static_cast<size_t>(31);
+  const size_t window = static_cast<size_t>(s->options.anderson_window) + 1;
+  const size_t contrib = (static_cast<size_t>(s->ne) * s->corners * 3 + 31) & ~static_cast<size_t>(31);
+  const size_t partials = static_cast<size_t>(team) * pdb200::kPartialStride;
+  const size_t column_bytes = (8 * pitch + 2 * window * pitch + contrib + partials + 48) * sizeof(double);
+  const size_t memory_lanes = std::max<size_t>(1, (static_cast<size_t>(8) << 30) / column_bytes);
+  const int lanes_cap = static_cast<int>(std::min<size_t>(std::max(1, grid_cap / team), memory_lanes));
+  const int launches = (selected + lanes_cap - 1) / lanes_cap;
+  const int capacity = (selected + launches - 1) / launches;
   // Plan for the team, keep that plan's buffers for the launches, put the
   // solver's own plan back (the mode-2 pass after the columns uses it).
   SavedPlan saved;
@@ -248,15 +266,7 @@ static int woodbury_columns_team(PdSolver* s, const pdb200::AdjointArgs& column,
   base.resident = planned.resident;
   base.stage_vector = planned.stage_vector;
   base.vector_smem_offset = planned.vector_smem_offset;
-  // Per-column buffers for `capacity` columns. Every vector starts on a
-  // 256-byte boundary (pitch: 3n rounded up to 32 doubles), as a vector of its
-  // own allocation does: the products stage their input vector into shared
-  // memory with 16-byte loads.
-  const size_t vec = static_cast<size_t>(3) * n;
-  const size_t pitch = (vec + 31) & ~static_cast<size_t>(31);
-  const size_t window = static_cast<size_t>(s->options.anderson_window) + 1;
-  const size_t contrib = (static_cast<size_t>(s->ne) * s->corners * 3 + 31) & ~static_cast<size_t>(31);
-  const size_t partials = static_cast<size_t>(team) * pdb200::kPartialStride;
+  // Per-column buffers for `capacity` columns.
   const auto ensure = [](DeviceBuffer& buffer, size_t bytes) -> cudaError_t {
     return buffer.bytes >= bytes ? cudaSuccess : buffer.allocate(bytes);
   };

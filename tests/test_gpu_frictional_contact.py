@@ -280,10 +280,11 @@ def test_large_contact_set_on_the_team_path_matches_the_oracle():
 @pytest.mark.parametrize("friction", [0.0, 0.5])
 def test_woodbury_columns_on_lanes_match_one_launch_per_column(friction):
     """The contact projection of a 8x6x2 block resting on the floor (63 contacts,
-    up to 189 rows with friction, so more than one launch of 64 lanes): the
-    parameter and state gradients with the columns side by side on lanes equal
-    those of one launch per column, and the lanes' material gradients agree
-    with the oracle's Woodbury projection."""
+    189 rows with friction): the parameter and state gradients with the columns
+    side by side on lanes (automatic team: one launch; teams of 4 blocks: 74
+    lanes, so three launches with friction) equal those of one launch per
+    column, and the lanes' material gradients agree with the oracle's Woodbury
+    projection."""
     from newton_solver_diff_phd_b200 import Tape
     from newton_solver_diff_phd_b200 import _lib
 
@@ -299,9 +300,12 @@ def test_woodbury_columns_on_lanes_match_one_launch_per_column(friction):
     rng = np.random.default_rng(7)
     gq = rng.standard_normal((model.particle_count, 3)).astype(np.float32)
     gv = rng.standard_normal((model.particle_count, 3)).astype(np.float32)
+    for invalid in (-1, 3, 128):
+        assert solver._lib.pd_set_woodbury_team(solver._handle, invalid) != 0
     results = []
-    for lanes in (1, 0):
+    for lanes, team in ((1, 0), (1, 4), (0, 0)):
         _lib.check(solver._lib.pd_set_woodbury_lanes(solver._handle, lanes))
+        _lib.check(solver._lib.pd_set_woodbury_team(solver._handle, team))
         model.tet_materials.grad = torch.zeros_like(model.tet_materials)
         state_in = _state(model, q, v)
         state_in.requires_grad_(True)
@@ -316,9 +320,10 @@ def test_woodbury_columns_on_lanes_match_one_launch_per_column(friction):
                         "qd": state_in.particle_qd.grad.double().cpu().numpy()})
     multiplier, omega, normal, _ = solver.frictional_state()
     assert int(((multiplier > 0) & (omega >= 0.5)).sum()) > 32
-    for name in results[0]:
-        scale = max(np.abs(results[1][name]).max(), 1.0e-30)
-        np.testing.assert_allclose(results[0][name], results[1][name], rtol=0.0, atol=1.0e-9 * scale, err_msg=name)
+    for result in results[:2]:
+        for name in result:
+            scale = max(np.abs(results[2][name]).max(), 1.0e-30)
+            np.testing.assert_allclose(result[name], results[2][name], rtol=0.0, atol=1.0e-9 * scale, err_msg=name)
     body = oracle_tet_body(model)
     oracle = pd_oracle.backward(body, solver._x.cpu().numpy(), 0.004, gq.astype(np.float64), gv.astype(np.float64),
                                 contact=(solver.frictional_vertices, multiplier.cpu().numpy(), omega.cpu().numpy(),
