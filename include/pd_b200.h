@@ -248,6 +248,22 @@ int pd_set_woodbury_team(PdSolver* solver, int32_t blocks);
    NULL disables. */
 int pd_set_phase_timers(PdSolver* solver, unsigned long long* device_timers);
 
+/* Failure detection of the device barriers (the reference's status contract,
+   kernels.py:28-31, has no barrier of its own: Warp launches are separate).
+   Every wait of a persistent launch polls a bounded number of times, then
+   sets PD_STATUS_BARRIER_TIMEOUT, raises the team's abort flag and returns.
+   pd_set_spin_limit lowers that poll budget for the solver's following step
+   and backward launches (0 restores the built-in budget of 2^26 polls), so a
+   test can make the waits run out. pd_barrier_probe launches `blocks`
+   cooperative blocks (at most one per SM) on a barrier that expects
+   `missing` more arrivals than are launched, with a budget of `polls`
+   (mode 0: the plain grid barrier; mode 1: the serial-section barrier), and
+   returns the status bits and how many blocks gave up and returned.
+   Synchronises the device. */
+int pd_set_spin_limit(PdSolver* solver, uint32_t polls);
+int pd_barrier_probe(int device, int32_t blocks, int32_t missing, int32_t mode, uint32_t polls, int32_t* status,
+                     int32_t* returned);
+
 /* Reads and clears the status word (read_status, solver.py:380-390). Synchronises the stream. */
 int pd_read_status(PdSolver* solver, int32_t* bits, void* stream);
 /* Iteration count of the last step and of the last backward fixed point. Synchronises the stream. */
@@ -266,22 +282,23 @@ int pd_apply_inverse(PdSolver* solver, const double* rhs, double* out, void* str
    stream capture, under a host-owned allocator, in a real-time loop): the
    intermediate vector lives in a file-scope device array of at most 65536
    particles (1.5 MiB, resident on each GPU that loads the library until
-   exit). Rejects larger solvers with PD_ERR_INVALID. The first call on a
-   device resolves the array's address and must come before any stream
-   capture. All calls share the array: calls that overlap on the GPU race. */
+   exit). Rejects larger solvers with PD_ERR_INVALID, built or not. The
+   first call on a device resolves the array's address and must come before
+   any stream capture. All calls share the array: calls that overlap on the
+   GPU race. The caller's current device is the same after the call. */
 int pd_apply_inverse_static(PdSolver* solver, const double* rhs, double* out, void* stream);
 
 /* ---- Batched rollouts.
-   Many independent built solvers (uneven sizes allowed) advanced together:
-   one CUDA graph per rollout, every PD step a WHILE loop of per-phase kernels
-   over all instances that still iterate. Each instance follows the same
+   Many independent built solvers (uneven sizes allowed) advanced together in
+   one CUDA graph per rollout. Under the default TEAMS schedule the graph is
+   one persistent cooperative launch: every instance runs all its steps on a
+   team of blocks with the single-instance step body (PHASES, kept for
+   comparison: per-phase kernels over all iterating instances in a graph WHILE
+   loop, the factor in postorder run format). Each instance follows the same
    algorithm as pd_step (solver.py:582-687: local step, gather, S^T S solve,
    Anderson, dual convergence gate) with its own tolerances and iteration
-   limit; the factor is the instance's own, stored in postorder run format.
-   The reference steps one model at a time; batching has no counterpart there.
-   Instances do not wait for each other between steps: an instance whose
-   step has converged writes it out and starts its next step while others
-   are still iterating.
+   limit. The reference steps one model at a time; batching has no
+   counterpart there. Instances do not wait for each other between steps.
    Every solver must be built for the same dt, on one device, with one
    precision and one state precision, without Dirichlet targets or Tet4
    activations. The solvers must outlive the batch and must not step on

@@ -120,6 +120,8 @@ SIGNATURES = {
     "pd_backward": ([_P, _P, _P, _D, _P, _P, _P, _P, _P, _P, _P, _P, _P], ctypes.c_int),
     "pd_backward_contact": ([_P, _P, _P, _D] + [_P] * 12, ctypes.c_int),
     "pd_set_phase_timers": ([_P, _P], ctypes.c_int),
+    "pd_set_spin_limit": ([_P, ctypes.c_uint32], ctypes.c_int),
+    "pd_barrier_probe": ([ctypes.c_int, _I32, _I32, _I32, ctypes.c_uint32, _P, _P], ctypes.c_int),
     "pd_read_status": ([_P, ctypes.POINTER(_I32), _P], ctypes.c_int),
     "pd_iterations": ([_P, ctypes.POINTER(_I32), ctypes.POINTER(_I32), _P], ctypes.c_int),
     "pd_deformation_determinants": ([_P, _P, _P, _P], ctypes.c_int),

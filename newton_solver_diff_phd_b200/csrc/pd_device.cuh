@@ -20,7 +20,8 @@ constexpr int kWarps = kBlock / 32;
 constexpr int kPartialStride = 64;  // partial-sum slots per block
 constexpr int kMaxWindow = 8;
 // Poll budget of one barrier wait (~2^26 polls of >= 32 ns: seconds, far
-// beyond any legitimate phase).
+// beyond any legitimate phase). A nonzero GridBarrier::spin_limit replaces it
+// (a test knob: the host writes it after clearing the barrier).
 constexpr unsigned kSpinLimit = 1u << 26;
 
 constexpr int kStatusNotConverged = 1;
@@ -37,8 +38,13 @@ struct GridBarrier {
   unsigned int state;  // serial-section barriers
   unsigned int abort;
   unsigned int flip;   // plain barriers: arrival count with a flipping high bit
-  unsigned int pad;
+  unsigned int spin_limit;  // polls before a wait gives up; 0: kSpinLimit
 };
+
+__device__ __forceinline__ unsigned spin_limit_of(const GridBarrier* bar) {
+  const unsigned limit = *reinterpret_cast<const volatile unsigned*>(&bar->spin_limit);
+  return limit != 0u ? limit : kSpinLimit;
+}
 
 constexpr unsigned kCountBits = 16;
 constexpr unsigned kCountMask = (1u << kCountBits) - 1u;
@@ -95,12 +101,13 @@ __device__ __forceinline__ bool barrier_wait(GridBarrier* bar, unsigned generati
   if (threadIdx.x == 0) {
     int ok = 1;
     unsigned spins = 0;
+    const unsigned limit = spin_limit_of(bar);
     while ((load_acquire(&bar->state) >> kCountBits) == (generation & (kCountMask))) {
       if (load_volatile(&bar->abort) != 0u) {
         ok = 0;
         break;
       }
-      if (++spins > kSpinLimit) {
+      if (++spins > limit) {
         atomicOr(status, kStatusBarrierTimeout);
         atomicExch(&bar->abort, 1u);
         ok = 0;
@@ -127,12 +134,13 @@ __device__ __forceinline__ bool grid_sync(GridBarrier* bar, int* status, int blo
     const unsigned old = add_acq_rel(&bar->flip, increment);
     int ok = 1;
     unsigned spins = 0;
+    const unsigned limit = spin_limit_of(bar);
     while (((old ^ load_acquire(&bar->flip)) & 0x80000000u) == 0u) {
       if (load_volatile(&bar->abort) != 0u) {
         ok = 0;
         break;
       }
-      if (++spins > kSpinLimit) {
+      if (++spins > limit) {
         atomicOr(status, kStatusBarrierTimeout);
         atomicExch(&bar->abort, 1u);
         ok = 0;

@@ -487,6 +487,30 @@ __global__ void __launch_bounds__(kBlock) spmv_kernel(const int* off, const int*
   }
 }
 
+__global__ void set_spin_limit_kernel(GridBarrier* barrier, unsigned limit) { barrier->spin_limit = limit; }
+
+// Waits at a barrier that never completes: the team is `blocks + missing`
+// blocks, only `blocks` are launched. The wait gives up after the barrier's
+// poll budget (or when another block raised the abort flag) and the block
+// counts itself out.
+__global__ void __launch_bounds__(kBlock) barrier_probe_kernel(GridBarrier* barrier, int* status, int* returned,
+                                                               int missing, int mode) {
+  const int team = static_cast<int>(gridDim.x) + missing;
+  bool ok;
+  if (mode == 0) {
+    ok = grid_sync(barrier, status, team, static_cast<int>(blockIdx.x));
+  } else {
+    unsigned generation;
+    if (barrier_arrive(barrier, generation, team)) {
+      barrier_release(barrier, generation, team);  // not reached while missing > 0
+      ok = true;
+    } else {
+      ok = barrier_wait(barrier, generation, status);
+    }
+  }
+  if (!ok && threadIdx.x == 0) atomicAdd(returned, 1);
+}
+
 __global__ void hex_determinants_kernel(const float* q, const int* indices, const double* gradients, int ne,
                                         double* out) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -571,6 +595,18 @@ cudaError_t launch_apply_inverse(const int* s_off, const int* s_col, const doubl
   spmv_kernel<double><<<blocks, kBlock, 0, stream>>>(s_off, s_col, s_val, rhs, work, rows);
   spmv_kernel<double><<<blocks, kBlock, 0, stream>>>(st_off, st_col, st_val, work, out, rows);
   return cudaGetLastError();
+}
+
+cudaError_t launch_set_spin_limit(GridBarrier* barrier, unsigned limit, cudaStream_t stream) {
+  set_spin_limit_kernel<<<1, 1, 0, stream>>>(barrier, limit);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_barrier_probe(GridBarrier* barrier, int* status, int* returned, int blocks, int missing, int mode,
+                                 cudaStream_t stream) {
+  void* params[] = {&barrier, &status, &returned, &missing, &mode};
+  return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(&barrier_probe_kernel), dim3(blocks), dim3(kBlock),
+                                     params, 0, stream);
 }
 
 cudaError_t launch_hex_determinants(const float* q, const int* indices, const double* gradients, int ne, double* out,

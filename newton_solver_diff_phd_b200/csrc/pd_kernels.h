@@ -163,6 +163,14 @@ cudaError_t adjoint_step_max_blocks(int precision, size_t smem, int* blocks_per_
 cudaError_t launch_apply_inverse(const int* s_off, const int* s_col, const double* s_val, const int* st_off,
                                  const int* st_col, const double* st_val, int rows, const double* rhs, double* work,
                                  double* out, cudaStream_t stream);
+// Writes a barrier's poll budget (after the launch's barrier was cleared).
+cudaError_t launch_set_spin_limit(GridBarrier* barrier, unsigned limit, cudaStream_t stream);
+// Cooperative probe of the bounded waits: `blocks` blocks wait at a barrier
+// that expects blocks + missing arrivals (mode 0: grid_sync; mode 1: the
+// serial-section barrier). Every block counts itself in `returned` once its
+// wait has given up.
+cudaError_t launch_barrier_probe(GridBarrier* barrier, int* status, int* returned, int blocks, int missing, int mode,
+                                 cudaStream_t stream);
 cudaError_t launch_hex_determinants(const float* q, const int* indices, const double* gradients, int ne, double* out,
                                     cudaStream_t stream);
 

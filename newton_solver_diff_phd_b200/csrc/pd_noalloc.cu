@@ -62,27 +62,58 @@ __global__ void static_spmv_kernel(const int* __restrict__ off, const int* __res
 
 }  // namespace
 
-// Defined in pd_solver.cu: the factor arrays of a built solver (device pointers).
+// Defined in pd_solver.cu: the factor arrays of a built solver (device
+// pointers) and the particle count of any solver.
 int pd_internal_factor(PdSolver* solver, int* device, int* rows, const int** s_off, const int** s_col,
                        const double** s_val, const int** st_off, const int** st_col, const double** st_val);
+int pd_internal_particles(const PdSolver* solver);
 int pd_internal_fail(int code, const char* message);
+
+namespace {
+
+// Makes the solver's device current for the call and puts the caller's
+// device back on every return path: callers that own their allocator also
+// own the current-device setting of their thread.
+class DeviceScope {
+ public:
+  cudaError_t enter(int device) {
+    cudaError_t status = cudaGetDevice(&previous_);
+    if (status != cudaSuccess) return status;
+    entered_ = true;
+    return previous_ == device ? cudaSuccess : cudaSetDevice(device);
+  }
+  ~DeviceScope() {
+    if (entered_) cudaSetDevice(previous_);
+  }
+
+ private:
+  int previous_ = 0;
+  bool entered_ = false;
+};
+
+}  // namespace
 
 extern "C" int pd_apply_inverse_static(PdSolver* solver, const double* rhs, double* out, void* stream) {
   if (solver == nullptr || rhs == nullptr || out == nullptr) return pd_internal_fail(PD_ERR_INVALID, "null argument");
+  // The size limit is checked first, so that an oversized solver is refused
+  // whether or not its factor has been built.
+  const int particles = pd_internal_particles(solver);
+  if (particles > kStaticScratchParticles) {
+    return pd_internal_fail(PD_ERR_INVALID,
+                            ("pd_apply_inverse_static handles at most " + std::to_string(kStaticScratchParticles) +
+                             " particles; this solver has " + std::to_string(particles))
+                                .c_str());
+  }
   int device = 0, rows = 0;
   const int *s_off = nullptr, *s_col = nullptr, *st_off = nullptr, *st_col = nullptr;
   const double *s_val = nullptr, *st_val = nullptr;
   if (int status = pd_internal_factor(solver, &device, &rows, &s_off, &s_col, &s_val, &st_off, &st_col, &st_val)) {
     return status;
   }
-  if (rows > kStaticScratchParticles) {
-    return pd_internal_fail(PD_ERR_INVALID,
-                            ("pd_apply_inverse_static handles at most " + std::to_string(kStaticScratchParticles) +
-                             " particles; this solver has " + std::to_string(rows))
-                                .c_str());
-  }
+  if (rows == 0) return PD_OK;  // nothing to apply; a zero-block launch would be an error
   if (device < 0 || device >= kMaxDevices) return pd_internal_fail(PD_ERR_INVALID, "device ordinal out of range");
-  cudaError_t status = cudaSetDevice(device);
+  DeviceScope scope;
+  cudaError_t status = scope.enter(device);
   if (status != cudaSuccess) return pd_internal_fail(PD_ERR_CUDA, cudaGetErrorString(status));
   void* scratch = nullptr;
   {

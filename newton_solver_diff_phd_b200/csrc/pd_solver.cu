@@ -794,6 +794,7 @@ int pd_step(PdSolver* s, const void* q, const void* qd, const void* f, const voi
     a.extra_force = s->mc_force.as<double>();
   }
   PD_CUDA(cudaMemsetAsync(s->d_barrier.ptr, 0, sizeof(pdb200::GridBarrier), st));
+  if (s->spin_limit != 0u) PD_CUDA(pdb200::launch_set_spin_limit(a.barrier, s->spin_limit, st));
   PD_CUDA(pdb200::launch_forward_step(a, s->blocks, s->options.precision, s->smem, st));
   return PD_OK;
 }
@@ -938,8 +939,45 @@ int pd_backward_contact(PdSolver* s, const double* x_record, const float* activa
     full.gactivations = nullptr;
   }
   PD_CUDA(cudaMemsetAsync(s->d_barrier.ptr, 0, sizeof(pdb200::GridBarrier), st));
+  if (s->spin_limit != 0u) PD_CUDA(pdb200::launch_set_spin_limit(full.barrier, s->spin_limit, st));
   PD_CUDA(pdb200::launch_adjoint_step(full, s->blocks, s->options.precision, s->smem, st));
   if (woodbury) return pd_woodbury_gradients(s, b, multiplier, omega, normal, st);
+  return PD_OK;
+}
+
+int pd_set_spin_limit(PdSolver* s, uint32_t polls) {
+  if (s == nullptr) return fail(PD_ERR_INVALID, "null solver");
+  s->spin_limit = polls;
+  return PD_OK;
+}
+
+int pd_barrier_probe(int device, int32_t blocks, int32_t missing, int32_t mode, uint32_t polls, int32_t* status,
+                     int32_t* returned) {
+  if (status == nullptr || returned == nullptr) return fail(PD_ERR_INVALID, "null argument");
+  if (blocks < 1 || missing < 1 || (mode != 0 && mode != 1) || polls == 0u || polls > (1u << 20) ||
+      blocks + missing > static_cast<int>(pdb200::kCountMask))
+    return fail(PD_ERR_INVALID, "blocks and missing must be positive, mode 0 or 1, polls in [1, 2^20]");
+  int previous = 0;
+  PD_CUDA(cudaGetDevice(&previous));
+  PD_CUDA(cudaSetDevice(device));
+  int sms = 0;
+  cudaError_t error = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  void* memory = nullptr;
+  if (error == cudaSuccess && blocks > sms) error = cudaErrorInvalidValue;  // one block per SM is co-resident
+  if (error == cudaSuccess) error = cudaMalloc(&memory, sizeof(pdb200::GridBarrier) + 2 * sizeof(int));
+  if (error == cudaSuccess) error = cudaMemset(memory, 0, sizeof(pdb200::GridBarrier) + 2 * sizeof(int));
+  auto* barrier = static_cast<pdb200::GridBarrier*>(memory);
+  int* words = reinterpret_cast<int*>(barrier + 1);
+  if (error == cudaSuccess) error = pdb200::launch_set_spin_limit(barrier, polls, nullptr);
+  if (error == cudaSuccess) error = pdb200::launch_barrier_probe(barrier, words, words + 1, blocks, missing, mode, nullptr);
+  if (error == cudaSuccess) error = cudaDeviceSynchronize();
+  int host[2] = {0, 0};
+  if (error == cudaSuccess) error = cudaMemcpy(host, words, sizeof(host), cudaMemcpyDeviceToHost);
+  if (memory != nullptr) cudaFree(memory);
+  cudaSetDevice(previous);
+  if (error != cudaSuccess) return fail(PD_ERR_CUDA, cudaGetErrorString(error));
+  *status = host[0];
+  *returned = host[1];
   return PD_OK;
 }
 
@@ -999,6 +1037,8 @@ int pd_apply_inverse(PdSolver* s, const double* rhs, double* out, void* stream) 
 
 // Internal hooks for pd_noalloc.cu (C++ linkage, not part of the ABI).
 int pd_internal_fail(int code, const char* message) { return fail(code, message); }
+
+int pd_internal_particles(const PdSolver* s) { return s->n; }
 
 int pd_internal_factor(PdSolver* s, int* device, int* rows, const int** s_off, const int** s_col, const double** s_val,
                        const int** st_off, const int** st_col, const double** st_val) {

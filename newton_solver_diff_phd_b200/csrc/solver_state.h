@@ -163,6 +163,7 @@ struct PdSolver {
   // Contact projection of the parameter gradients (pd_woodbury.cu), sized for w_rows rows.
   int w_rows = 0;
   bool woodbury_lanes = true;  // columns side by side on lanes (false: one launch per column)
+  unsigned spin_limit = 0;     // poll budget of the step and backward barriers (0: the built-in budget)
   int woodbury_team = 0;       // blocks per lane (0: from nnz(S) and the element samples)
   DeviceBuffer w_row_node, w_row_vector, w_value, w_selected, w_order, w_control, w_columns, w_gram, w_coefficients,
       w_permutation, w_work, w_seed, w_mu;

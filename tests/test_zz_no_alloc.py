@@ -38,3 +38,27 @@ def test_static_scratch_apply_matches_solver_scratch_apply_on_consecutive_calls(
         actual = _apply(solver, "pd_apply_inverse_static", rhs)
         np.testing.assert_allclose(actual.cpu().numpy(), expected.cpu().numpy(), rtol=1e-14, atol=1e-16,
                                    err_msg=f"call {call}")
+
+
+def test_static_scratch_apply_refuses_more_particles_than_its_array_holds_and_keeps_the_device():
+    from newton_solver_diff_phd_b200 import ModelBuilder
+
+    # 41 x 41 x 40 vertices = 67,240 particles: one more layer than the
+    # 65,536-particle array holds. The factor is never built: the size check
+    # comes first.
+    builder = ModelBuilder(gravity=(0.0, 0.0, 0.0))
+    builder.add_soft_grid(pos=(0.0, 0.0, 0.0), rot=None, vel=(0.0, 0.0, 0.0), dim_x=40, dim_y=40, dim_z=39,
+                          cell_x=0.01, cell_y=0.01, cell_z=0.01, density=DENSITY, k_mu=1.0e4, k_lambda=1.0e4,
+                          k_damp=0.0, fix_left=True)
+    model = builder.finalize("cuda")
+    assert model.particle_count > 65536
+    solver = SolverDiffPhD(model, density=DENSITY)
+    rhs = torch.zeros((model.particle_count, 3), dtype=torch.float64, device="cuda")
+    out = torch.empty_like(rhs)
+    device = torch.cuda.current_device()
+    lib = _lib.library()
+    code = lib.pd_apply_inverse_static(solver._handle, _lib.ptr(rhs), _lib.ptr(out),
+                                       torch.cuda.current_stream().cuda_stream)
+    assert code == _lib.PD_ERR_INVALID
+    assert b"65536" in lib.pd_last_error()
+    assert torch.cuda.current_device() == device
