@@ -12,6 +12,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PACKAGE = Path(__file__).resolve().parent
@@ -53,24 +54,27 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     BUILD.mkdir(exist_ok=True)
     headers = [CSRC / h for h in HEADERS] + [INCLUDE / "pd_b200.h"]
     objects = []
+    commands = []
     nvcc = _nvcc()
     for source in CUDA_SOURCES:
         obj = BUILD / (source + ".o")
         if force or _stale(obj, [CSRC / source, *headers]):
-            command = [
+            commands.append([
                 nvcc, *ARCH, "-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xptxas", "-v",
                 "-I", str(INCLUDE), "-c", str(CSRC / source), "-o", str(obj),
-            ]
-            result = _run(command)
-            if verbose:
-                print(result.stderr)
+            ])
         objects.append(obj)
     for source in HOST_SOURCES:
         obj = BUILD / (source + ".o")
         if force or _stale(obj, [CSRC / source, *headers]):
-            _run(["g++", "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math",
-                  "-c", str(CSRC / source), "-o", str(obj)])
+            commands.append(["g++", "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math",
+                             "-c", str(CSRC / source), "-o", str(obj)])
         objects.append(obj)
+    # Translation units compile side by side (the slowest one bounds the build).
+    with ThreadPoolExecutor(max(1, min(len(commands), os.cpu_count() or 1))) as pool:
+        for result in pool.map(_run, commands):
+            if verbose:
+                print(result.stderr)
     if force or _stale(LIBRARY, objects):
         _run([nvcc, *ARCH, "-shared", "-o", str(LIBRARY), *map(str, objects), "-lcudart"])
     return LIBRARY

@@ -231,3 +231,92 @@ def twist_cantilever(spec: Twist, device="cuda"):
     tip = np.flatnonzero(np.abs(vertices[:, 0] - spec.nx * spec.edge) <= 1.0e-12)
     mesh = meshes.Mesh(f"twist{spec.nx}x{spec.ny}x{spec.nz}", vertices, hexes)
     return model, mesh, np.stack([mu, lam], axis=1), q0, tip
+
+
+# ---------------------------------------------------------------------------
+# The reference's own Hex8 cantilever (src/newton_solver_diff_phd/examples/
+# _diff_phd_cantilever.py:82-185, geometry of tools/bake_cantilever.py:22-49):
+# 20 x 5 x 5 cubic cells in binary corner order, vertex (i, j, k) at index
+# i*36 + j*6 + k, the x = 0 face pinned; x slabs 7..12 (cells 20//3 < i <=
+# 2*(20//3)) at E = 1e7 Pa, the rest 1e6 Pa, nu = 0.45, density 1000 kg/m^3,
+# no gravity; a +x fibre of stiffness 1e5 and target length 0 in cells i*25
+# (the bottom-edge cells (i, 0, 0)); vertex-plane energies of stiffness 100 on
+# vertices 720 and 750 against the half-space z + 0.1 >= 0. The axial motion
+# pulls every tip vertex with +x force 80 t / 25 N at step t = 0..24 (dt 0.01,
+# rel 1e-4); the twist motion releases the cross-sections rotated linearly
+# along x up to 30 degrees at the tip (dt 0.001, 100 steps, rel 1e-6). The
+# reference bakes 0.016 m cells; BASELINE's variant uses 0.01 m.
+
+
+@dataclass
+class ReferenceCantilever:
+    edge: float = 0.016
+    motion: str = "axial"     # "axial" or "twist"
+    nx: int = 20
+    ny: int = 5
+    nz: int = 5
+    young: float = 1.0e6
+    stiff_ratio: float = 10.0
+    poisson: float = 0.45
+    density: float = 1000.0
+    muscle_stiffness: float = 1.0e5
+    plane_vertices: tuple = (720, 750)
+    plane_stiffness: float = 100.0
+    plane: tuple = (0.0, 0.0, 1.0, 0.1)
+    twist_degrees: float = 30.0
+
+    @property
+    def dt(self) -> float:
+        return 0.01 if self.motion == "axial" else 0.001
+
+    @property
+    def steps(self) -> int:
+        return 25 if self.motion == "axial" else 100
+
+    @property
+    def rel_tol(self) -> float:
+        return 1.0e-4 if self.motion == "axial" else 1.0e-6
+
+    def tip_force(self, step: int) -> float:
+        """+x force on every tip vertex at ``step`` [N] (zero for the twist release)."""
+        return 80.0 * step / 25.0 if self.motion == "axial" else 0.0
+
+
+def reference_cantilever(spec: ReferenceCantilever, device="cuda"):
+    """``(model, solver_options, q0, tip)`` of the reference cantilever.
+
+    ``solver_options`` are the ``SolverDiffPhD`` keywords of the reference
+    example (hex mesh and materials, fibres, targets, planar energies and the
+    convergence settings); ``q0`` is the float64 initial position (the rest
+    pose, or the twisted pose); ``tip`` the tip-face particles.
+    """
+    if spec.motion not in ("axial", "twist"):
+        raise ValueError("motion must be 'axial' or 'twist'")
+    vertices, hexes, cells = meshes.hex_grid(spec.nx, spec.ny, spec.nz, spec.edge)
+    pinned = vertices[:, 0] == 0.0
+    builder = ModelBuilder(gravity=(0.0, 0.0, 0.0))
+    builder.add_particles(pos=vertices.tolist(), vel=np.zeros_like(vertices).tolist(),
+                          mass=[0.0 if p else spec.density * spec.edge**3 for p in pinned])
+    model = builder.finalize(device)
+    third = spec.nx // 3
+    stiff = (cells > third) & (cells <= 2 * third)
+    mu, lam = meshes.lame_from_young(spec.young * np.where(stiff, spec.stiff_ratio, 1.0), spec.poisson)
+    muscle = np.zeros(len(hexes))
+    muscle[np.arange(spec.nx) * spec.ny * spec.nz] = spec.muscle_stiffness
+    options = {
+        "hex_mesh": meshes.Mesh(f"cantilever{spec.nx}x{spec.ny}x{spec.nz}", vertices, hexes),
+        "hex_materials": np.column_stack([mu, lam]),
+        "density": spec.density,
+        "material": "pd",
+        "muscle_directions": np.tile([1.0, 0.0, 0.0], (len(hexes), 1)),
+        "muscle_stiffness": muscle,
+        "muscle_targets": np.zeros(len(hexes)),
+        "planar_energies": (np.asarray(spec.plane_vertices, dtype=np.int32), spec.plane_stiffness, spec.plane),
+        "max_iterations": 5000,
+        "abs_tol": 1.0e-9,
+        "rel_tol": spec.rel_tol,
+        "anderson_window": 5,
+    }
+    q0 = vertices.copy() if spec.motion == "axial" else twisted_positions(vertices, np.radians(spec.twist_degrees))
+    tip = np.flatnonzero(vertices[:, 0] == vertices[:, 0].max())
+    return model, options, q0, tip

@@ -180,3 +180,54 @@ def test_woodbury_projection_matches_reference_backward(key):
     for name in ("mu", "z", "q", "qd", "f", "materials", "activations"):
         reference = g[f"{key}__out_{name}"]
         np.testing.assert_allclose(out[name], reference, rtol=0.0, atol=1.0e-6 * np.abs(reference).max(), err_msg=name)
+
+
+@pytest.mark.parametrize("name", ["cancel", "grid2d", "tet322", "hex632"])
+def test_factor_port_is_bit_identical_to_the_reference_setup(name):
+    from oracle import factor_port
+
+    g = golden("sparse_factors.npz")
+    out = factor_port.inverse_factor(g[name + "__matrix"])
+    for key in ("permutation", "s_offsets", "s_columns", "s_values", "st_offsets", "st_columns", "st_values"):
+        np.testing.assert_array_equal(out[key], g[f"{name}__{key}"], err_msg=key)
+
+
+def test_factor_port_rejects_what_the_reference_rejects():
+    from oracle import factor_port
+
+    with pytest.raises(ValueError, match="symmetric"):
+        factor_port.inverse_factor(np.array([[2.0, 1.0], [0.5, 2.0]]))
+    with pytest.raises(ValueError, match="positive"):
+        factor_port.inverse_factor(np.array([[1.0, 2.0], [2.0, 1.0]]))
+
+
+# The reference publishes its port's results on its own Hex8 cantilever
+# (docs/validation/cantilever-reference-2026-11-02.json:264-265): min Gauss
+# det(F) 0.9661699048673299 over the 25 axial steps, at most 16 iterations,
+# and 192 iterations over steps 3..24 (cantilever-performance-2026-11-02.json:142).
+def test_oracle_reproduces_the_published_axial_cantilever():
+    from newton_solver_diff_phd_b200.scenes import ReferenceCantilever, reference_cantilever
+
+    spec = ReferenceCantilever(edge=0.016, motion="axial")
+    _, options, q0, tip = reference_cantilever(spec, device="cpu")
+    mesh = options["hex_mesh"]
+    mu, lam = options["hex_materials"].T
+    body = pd_oracle.Body.hex(mesh.vertices, mesh.indices, mesh.vertices[:, 0] != 0.0, mu, lam, spec.density,
+                              muscle_directions=options["muscle_directions"],
+                              muscle_stiffness=options["muscle_stiffness"], planes=options["planar_energies"])
+    q = q0.astype(np.float32).astype(np.float64)
+    v = np.zeros_like(q)
+    iterations, determinants = [], []
+    for t in range(spec.steps):
+        f = np.zeros_like(q)
+        f[tip, 0] = np.float32(spec.tip_force(t))
+        x, count, converged = pd_oracle.step(body, q, v, f, np.zeros(3), spec.dt, max_iterations=5000, abs_tol=1e-9,
+                                             rel_tol=spec.rel_tol, window=5, targets=options["muscle_targets"])
+        assert converged
+        v = ((x - q) / spec.dt).astype(np.float32).astype(np.float64)
+        q = x.astype(np.float32).astype(np.float64)
+        iterations.append(count)
+        determinants.append(np.linalg.det(body.deformation(q)).min())
+    assert max(iterations) == 16
+    assert sum(iterations[3:]) == 192
+    assert abs(min(determinants) - 0.9661699048673299) < 1e-12
