@@ -81,6 +81,24 @@ def build_model(device):
     return model, young, poisson, target
 
 
+def workload_config(args, nnz_s, world):
+    """The workload both arms run (identical in both lines; measured values go elsewhere)."""
+    return {
+        "workload": WORKLOAD,
+        "particles": (NX + 1) * (NY + 1) * (NZ + 1),
+        "tets": 5 * NX * NY * NZ,
+        "rollout_steps": STEPS_PER_ROLLOUT,
+        "dt": DT,
+        "rel_tol": REL_TOL,
+        "abs_tol": ABS_TOL,
+        "anderson_window": 5,
+        "adjoint": f"{args.adjoint} (dL/dE of every tet; CG preconditioned by the factor)",
+        "nnz_S": int(nnz_s),
+        "l2": "GPU arm: 256 MiB write between timed rollouts (flush); the factor re-enters L2 within a rollout",
+        "parallelism": f"replicas x{world}",
+    }
+
+
 def algorithmic_bytes_per_iteration(n, elements, nnz_s, corners=4, window=5, value_bytes=8):
     """Bytes one local/global iteration must move: factor values and indices of S and S^T, the vectors
     around the two products, element contributions, the Anderson history and the convergence norms
@@ -220,6 +238,7 @@ def run_b200(args):
     elapsed_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
     elapsed_ms = distributed.max_over_ranks(elapsed_ms, ranks)
     status |= solver.read_status()
+    errors = rollout_errors(driver, grad_e)
     total_steps = STEPS_PER_ROLLOUT * args.steps * world
     value = total_steps / (elapsed_ms / 1000.0)
 
@@ -283,22 +302,13 @@ def run_b200(args):
         "vs_baseline": None,
         "dtype": "f64" if args.precision == "fp64" else "f32+f64-refine",
         "data": "synthetic (seeded Tet4 block; materials log-uniform from default_rng(0))",
-        "config": {
-            "workload": WORKLOAD,
-            "particles": int(solver._n),
-            "tets": int(solver._element_count),
-            "pd_steps_per_bench_step": STEPS_PER_ROLLOUT,
-            "dt": DT,
-            "rel_tol": REL_TOL,
-            "abs_tol": ABS_TOL,
-            "anderson_window": 5,
-            "adjoint": args.adjoint,
-            "precision": args.precision,
-            "nnz_S": int(nnz_s),
-            "l2": "256 MiB write between timed rollouts (flush); the factor re-enters L2 within a rollout",
-            "parallelism": f"replicas x{world}",
-            "forward_iterations_mean": float(np.mean(fwd_iters)),
-            "backward_iterations_mean": float(np.mean(bwd_iters)),
+        "config": workload_config(args, nnz_s, world),
+        "bench_step": f"one {STEPS_PER_ROLLOUT}-step rollout forward and its adjoint ({STEPS_PER_ROLLOUT} PD steps)",
+        "precision": args.precision,
+        "errors": errors,
+        "measured": {
+            "sample_forward_iterations_mean": float(np.mean(fwd_iters)),
+            "sample_backward_iterations_mean": float(np.mean(bwd_iters)),
             "status_bits": int(status),
         },
         "gpu_launches": 2 * STEPS_PER_ROLLOUT * args.steps,
@@ -319,17 +329,34 @@ def run_b200(args):
     }
     if rank == 0:
         result["e2e"] = run_e2e(args, solver, driver, q0, target, young, dmu_de, dlam_de, device)
-        result["cpu_baseline"] = cpu_baseline(args, seconds=args.cpu_seconds)
+        result["cpu_baseline"] = cpu_baseline(args)
         if world == 1 and not args.no_batched:
             result["batched"] = run_batched(args, device)
         if world == 1 and not args.no_contact:
             result["contact"] = run_contact(args, device)
         if world == 1 and args.twist:
             result["twist"] = run_twist(args, device)
+        if world == 1 and not args.no_cantilever:
+            result["cantilever"] = run_cantilever(args, device)
     distributed.barrier(ranks)
     distributed.teardown(ranks)
     if rank == 0:
         print(json.dumps(result), flush=True)
+
+
+def rollout_errors(driver, grad_e):
+    """Errors of the last timed rollout against the CPU oracle's rollout of the same workload
+    (tests/golden/tet_block_rollout.npz): final positions and dL/dE, relative in the 2-norm."""
+    g = np.load(FIXTURE)
+    final = driver.checkpoints[-1].particle_q.double().cpu().numpy()
+    grad = grad_e.double().cpu().numpy()
+    return {
+        "position_rel_vs_fp64_oracle": float(np.linalg.norm(final - g["q_final"]) / np.linalg.norm(g["q_final"])),
+        "position_max_abs_m": float(np.abs(final - g["q_final"]).max()),
+        "grad_E_rel_vs_fp64_oracle": float(np.linalg.norm(grad - g["grad_young"]) / np.linalg.norm(g["grad_young"])),
+        "oracle": "the reference algorithm in float64 on the CPU (oracle/sparse_port.py, exact inverse factor of "
+                  "oracle/factor_port.py), same inputs; both stop at rel 1e-6",
+    }
 
 
 def run_e2e(args, solver, driver, q0, target, young, dmu_de, dlam_de, device):
@@ -737,6 +764,73 @@ def run_contact(args, device):
     }
 
 
+# The reference's own Hex8 cantilever (examples/_diff_phd_cantilever.py), whose
+# port numbers the reference publishes for 0.016 m cells on a GB10:
+# docs/validation/cantilever-performance-2026-11-02.json:43-46 (22 replayed
+# steps in 41.9 ms of GPU graph time, 1.905 ms/step) and
+# cantilever-reference-2026-11-02.json:264-265 (min Gauss det(F)
+# 0.9661699048673299, at most 16 iterations).
+PUBLISHED_CANTILEVER = {"gb10_graph_ms_per_step_replay": 1.905, "min_gauss_j": 0.9661699048673299,
+                        "max_iterations": 16, "replay_iterations": 192}
+
+
+def run_cantilever(args, device):
+    """Forward steps of the reference cantilever (axial pull, 25 steps of dt 0.01 s, rel 1e-4) at the
+    published 0.016 m cells and at BASELINE's 0.01 m cells, timed per step with CUDA events."""
+    import torch
+
+    from newton_solver_diff_phd_b200 import SolverDiffPhD
+    from newton_solver_diff_phd_b200.scenes import ReferenceCantilever, reference_cantilever
+
+    stream = torch.cuda.current_stream()
+    out = {"workload": "reference Hex8 cantilever 20x5x5 (756 particles, 500 Hex8 x 8 samples), axial pull",
+           "published_gb10": PUBLISHED_CANTILEVER}
+    for edge in (0.016, 0.01):
+        spec = ReferenceCantilever(edge=edge, motion="axial")
+        model, options, q0, tip = reference_cantilever(spec, device=device)
+        solver = SolverDiffPhD(model, **options)
+        forces = torch.zeros((spec.steps, model.particle_count, 3), dtype=torch.float32, device=device)
+        tip_index = torch.as_tensor(tip, device=device)
+        for t in range(spec.steps):
+            forces[t, tip_index, 0] = spec.tip_force(t)
+        runs = []
+        for _ in range(2):  # the first run builds the factor; the second is reported
+            states = [model.state(), model.state()]
+            states[0].particle_q.copy_(torch.as_tensor(q0, dtype=torch.float32, device=device))
+            times, iterations, determinants = [], [], []
+            for t in range(spec.steps):
+                states[0].particle_f.copy_(forces[t])
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                solver.step(states[0], states[1], None, None, spec.dt)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                times.append(e0.elapsed_time(e1))
+                iterations.append(int(solver.iterations[0]))
+                determinants.append(float(solver.deformation_determinants(states[1]).min()))
+                states.reverse()
+            runs.append((times, iterations, determinants, solver.read_status()))
+        times, iterations, determinants, status = runs[-1]
+        out[f"edge_{edge}"] = {
+            "forward_ms_per_step": float(np.mean(times)),
+            "forward_ms_per_step_steps_3_24": float(np.mean(times[3:])),
+            "forward_us_per_iteration": 1000.0 * float(np.sum(times)) / max(1, sum(iterations)),
+            "iterations": iterations,
+            "min_gauss_det_F": min(determinants),
+            "status": int(status),
+        }
+    published = PUBLISHED_CANTILEVER
+    mine = out["edge_0.016"]
+    out["vs_published_0.016"] = {
+        "min_gauss_det_F_abs_diff": abs(mine["min_gauss_det_F"] - published["min_gauss_j"]),
+        "max_iterations_equal": max(mine["iterations"]) == published["max_iterations"],
+        "replay_iterations_equal": sum(mine["iterations"][3:]) == published["replay_iterations"],
+        "replay_speedup_vs_gb10_graph_time": published["gb10_graph_ms_per_step_replay"]
+        / mine["forward_ms_per_step_steps_3_24"],
+    }
+    return out
+
+
 def run_twist(args, device):
     """The large Hex8 twist-release workload (80x20x20 cells, 35,721 particles): `twist_steps` steps
     of dt 1e-3 at rel 1e-6 forward, then the adjoint of the final tip rotation angle w.r.t. the
@@ -803,50 +897,93 @@ def run_twist(args, device):
     return out
 
 
-def cpu_sample(steps, threads):
-    """Time the CPU port on the first `steps` PD steps (forward then adjoint); returns (seconds, steps)."""
-    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
-    from newton_solver_diff_phd_b200 import _lib, meshes
-    from oracle import pd_oracle
-    from oracle.sparse_port import SparsePort
+# ---------------------------------------------------------------------------
+# The CPU side: the reference's algorithm for this path on the host cores.
+# The reference's own CPU path (Warp CPU kernels) needs warp-lang and newton,
+# which are not installed; oracle/sparse_port.py runs the same algorithm with
+# NumPy/SciPy on a thread pool, with the inverse factor of
+# oracle/factor_port.py (bit-identical to the reference's sparse.py setup).
+# Nothing here loads this package's CUDA library.
+#
+# A PD step of the rollout costs between 4 and 900 local/global iterations
+# (bursts where the pinned beam swings back), so a few consecutive steps are
+# not a fair sample. tests/golden/tet_block_rollout.npz holds the oracle's own
+# rollout of this workload: the input state of every second step and the loss
+# gradient its adjoint receives. A CPU sample point is one of those 25 steps,
+# forward then adjoint (conjugate gradients preconditioned by the factor, the
+# same solver as the GPU arm's exact adjoint), from the recorded inputs.
 
-    vertices, tets, young, poisson, target = workload_arrays()
-    poses = meshes.tet_rest_poses(vertices.astype(np.float32).astype(np.float64), tets).astype(np.float32)
-    mu, lam = meshes.lame_from_young(young, poisson)
-    mu = mu.astype(np.float32).astype(np.float64)
-    lam = lam.astype(np.float32).astype(np.float64)
-    free = vertices[:, 0] > 0
-    body = pd_oracle.Body.tet(tets, poses, free, mu, lam, 1000.0)
-    a = body.matrix(DT)
-    import scipy.sparse as sp
-
-    csr = sp.csr_matrix(a)
-    factor = _lib.inverse_factor((csr.indptr, csr.indices, csr.data))
-    port = SparsePort(body, factor, DT)
-    q = vertices.astype(np.float32).astype(np.float64)
-    v = np.zeros_like(q)
-    gravity = np.array([0.0, 0.0, -9.81], dtype=np.float32).astype(np.float64)
-    start = time.perf_counter()
-    records = []
-    for _ in range(steps):
-        x, _, _ = port.step(q, v, np.zeros_like(q), gravity, max_iterations=10000, abs_tol=ABS_TOL, rel_tol=REL_TOL)
-        records.append(x)
-        v = (x - q) / DT
-        q = x
-    seed = 2.0 * (q - target)
-    for x in reversed(records):
-        mu_adj, _, _ = port.backward(x, seed, np.zeros_like(seed), max_iterations=10000, abs_tol=ABS_TOL,
-                                     rel_tol=REL_TOL, mode="exact")
-        seed = body.mass / DT**2 * mu_adj
-    return time.perf_counter() - start, steps
+FIXTURE = ROOT / "tests" / "golden" / "tet_block_rollout.npz"
 
 
-def cpu_baseline(args, seconds=20.0):
+class CpuWorkload:
+    """The port on the bench's Tet4 block (built from the same arrays the solver gets)."""
+
+    def __init__(self, threads):
+        import scipy.sparse as sp
+
+        from newton_solver_diff_phd_b200 import ModelBuilder, meshes
+        from oracle import factor_port, pd_oracle
+        from oracle.sparse_port import SparsePort
+
+        vertices, tets, young, poisson, _ = workload_arrays()
+        builder = ModelBuilder(gravity=(0.0, 0.0, -9.81))
+        builder.add_soft_grid(pos=(0.0, 0.0, 0.0), rot=None, vel=(0.0, 0.0, 0.0), dim_x=NX, dim_y=NY, dim_z=NZ,
+                              cell_x=EDGE, cell_y=EDGE, cell_z=EDGE, density=1000.0, k_mu=1.0, k_lambda=1.0,
+                              k_damp=0.0, fix_left=True)
+        model = builder.finalize("cpu")
+        mu, lam = meshes.lame_from_young(young, poisson)
+        free = model.particle_inv_mass.numpy() > 0
+        self.body = pd_oracle.Body.tet(model.tet_indices.numpy().reshape(-1, 4), model.tet_poses.numpy(), free,
+                                       mu.astype(np.float32).astype(np.float64),
+                                       lam.astype(np.float32).astype(np.float64), 1000.0)
+        start = time.perf_counter()
+        self.factor = factor_port.inverse_factor(sp.csr_matrix(self.body.matrix(DT)))
+        self.setup_s = time.perf_counter() - start
+        self.port = SparsePort(self.body, self.factor, DT, threads=threads)
+        self.gravity = model.gravity.numpy()[0].astype(np.float64)
+        self.fixture = np.load(FIXTURE)
+        self.points = len(self.fixture["steps"])
+
+    def run_point(self, k):
+        """Forward then adjoint of sample point ``k``; returns ``(seconds, forward iterations, adjoint iterations)``."""
+        g = self.fixture
+        q = g["q_in"][k].astype(np.float64)
+        v = g["qd_in"][k].astype(np.float64)
+        start = time.perf_counter()
+        x, forward, _ = self.port.step(q, v, np.zeros_like(q), self.gravity, max_iterations=10000, abs_tol=ABS_TOL,
+                                       rel_tol=REL_TOL)
+        _, _, backward = self.port.backward_cg(x, g["grad_q_out"][k].astype(np.float64),
+                                               g["grad_qd_out"][k].astype(np.float64), max_iterations=10000,
+                                               abs_tol=ABS_TOL, rel_tol=REL_TOL, mode="exact")
+        return time.perf_counter() - start, forward, backward
+
+    def stratified_points(self, count):
+        """``count`` points that follow the rollout's iteration distribution: the points sorted by
+        the oracle's forward iterations, the median of each of ``count`` equal strata."""
+        iterations = self.fixture["iterations"][self.fixture["steps"]]
+        order = np.argsort(iterations, kind="stable")
+        bounds = np.linspace(0, len(order), count + 1)
+        return [int(order[int((lo + hi) // 2)]) for lo, hi in zip(bounds[:-1], bounds[1:])]
+
+
+def cpu_baseline(args, points=5):
     threads = os.cpu_count() or 1
-    elapsed, steps = cpu_sample(2, threads)
-    return {"value": steps / elapsed, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"first {steps} PD steps of the rollout forward then their adjoints, oracle/sparse_port.py "
-                      "(SciPy CSR S^T S, NumPy projections; SpMV single-threaded)"}
+    work = CpuWorkload(threads)
+    chosen = work.stratified_points(points)
+    total, forward, backward = 0.0, 0, 0
+    for k in chosen:
+        seconds, f, b = work.run_point(k)
+        total += seconds
+        forward += f
+        backward += b
+    steps = [int(work.fixture["steps"][k]) for k in chosen]
+    return {"value": len(chosen) / total, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"PD steps {steps} of the 50-step rollout (the medians of {points} strata of the oracle's "
+                      f"per-step iteration counts), each forward ({forward} iterations in all) then its exact adjoint "
+                      f"by CG ({backward} iterations), from the oracle rollout's recorded inputs; "
+                      "oracle/sparse_port.py on a thread pool, factor from oracle/factor_port.py "
+                      f"({work.setup_s:.1f} s, untimed)"}
 
 
 def run_reference(args):
@@ -854,25 +991,59 @@ def run_reference(args):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
+    work = CpuWorkload(threads)
+    # Warm-up: the first step of the rollout (the cheapest, 40 iterations).
     for _ in range(args.warmup):
-        cpu_sample(1, threads)
-    total, steps = 0.0, 0
-    for _ in range(args.steps):
-        elapsed, n = cpu_sample(1, threads)
-        total += elapsed
-        steps += n
-    value = steps / total
+        work.run_point(0)
+    # Timed step k: sample point (k * 25) // K, so the K steps spread evenly
+    # over the rollout (all 25 points when K >= 25, cycling beyond).
+    total, forward, backward, used = 0.0, 0, 0, []
+    for k in range(args.steps):
+        point = (k * work.points) // args.steps if args.steps <= work.points else k % work.points
+        seconds, f, b = work.run_point(point)
+        total += seconds
+        forward += f
+        backward += b
+        used.append(int(work.fixture["steps"][point]))
+    value = args.steps / total
+    sample = (f"one PD step forward + exact adjoint per bench step, at rollout steps {used} "
+              f"({forward} forward and {backward} adjoint CG iterations in all), from the oracle rollout's recorded "
+              "inputs (tests/golden/tet_block_rollout.npz); oracle/sparse_port.py on a thread pool, the reference "
+              "algorithm on the host cores (warp-lang and newton are not installed)")
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded Tet4 block)", "impl": "reference",
-        "config": {"workload": WORKLOAD, "sample": "first PD step forward + adjoint per bench step"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": "first PD step of the Tet4 block rollout, forward then adjoint, per bench step"},
+        "data": "synthetic (seeded Tet4 block; materials log-uniform from default_rng(0))", "impl": "reference",
+        "config": workload_config(args, nnz_s=len(work.factor["s_values"]), world=1),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(result), flush=True)
+
+
+def run_batch_profile(args):
+    """A small batched rollout for profilers: the instances ``--profile-batch`` lists (indices into
+    cantilever_family(256, seed=0)), ``--profile-steps`` steps, fp32+refine, teams schedule, run
+    twice (the first rollout captures the graph)."""
+    import torch
+
+    from newton_solver_diff_phd_b200.batch import BatchedSolver
+
+    device = torch.device("cuda", 0)
+    chosen = [int(k) for k in args.profile_batch.split(",")]
+    family = batch_family(device, "fp32+refine")
+    family = [family[k] for k in chosen]
+    build_all([s for _, _, s, _ in family], BATCH_DT)
+    batch = BatchedSolver([s for _, _, s, _ in family], BATCH_DT)
+    q0 = torch.cat([m.particle_q for _, m, _, _ in family]).contiguous()
+    forces = torch.cat([f for _, _, _, f in family]).contiguous()
+    traj = batch.rollout(q0, torch.zeros_like(q0), forces, args.profile_steps)
+    traj = batch.rollout(q0, torch.zeros_like(q0), forces, args.profile_steps, out=traj)
+    torch.cuda.synchronize()
+    status, iterations = batch.read()
+    print(json.dumps({"instances": chosen, "steps": args.profile_steps, "status": status.tolist(),
+                      "iterations": iterations.sum(axis=0).tolist()}))
 
 
 def main():
@@ -883,16 +1054,22 @@ def main():
     parser.add_argument("--impl", choices=["b200", "reference"], default="b200")
     parser.add_argument("--adjoint", choices=["reference", "exact"], default="exact")
     parser.add_argument("--precision", choices=["fp64", "fp32+refine"], default="fp64")
-    parser.add_argument("--cpu-seconds", type=float, default=20.0)
     parser.add_argument("--no-batched", action="store_true", help="skip the batched-vs-plain cantilever family leg")
     parser.add_argument("--no-contact", action="store_true", help="skip the Tet4 contact (poke) leg")
+    parser.add_argument("--no-cantilever", action="store_true", help="skip the reference Hex8 cantilever leg")
     parser.add_argument("--contact-steps", type=int, default=30, help="steps of the contact leg's rollout")
     parser.add_argument("--twist", action="store_true",
                         help="add the 35,721-particle Hex8 twist-release leg (minutes: its host factor build)")
     parser.add_argument("--twist-steps", type=int, default=100, help="steps of the twist-release leg")
     parser.add_argument("--no-extras", action="store_true",
                         help="skip the e2e, CPU-baseline and per-launch timing legs (profiling runs)")
+    parser.add_argument("--profile-batch", default=None,
+                        help="comma-separated family instances: run only a small batched rollout (for profilers)")
+    parser.add_argument("--profile-steps", type=int, default=2, help="steps of the --profile-batch rollout")
     args = parser.parse_args()
+    if args.profile_batch:
+        run_batch_profile(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:
