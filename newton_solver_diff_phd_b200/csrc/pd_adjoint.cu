@@ -368,7 +368,7 @@ __device__ __forceinline__ bool adjoint_step_body(const AdjointArgs& b, const Te
       {
         const double* in = b.work;
         if (b.stage_vector) {
-          stage_vector(b.work, vector_smem, n);
+          stage_for(b.plan_s, team.rank, b.work, vector_smem, n);
           in = vector_smem;
         }
         spmv_block<TV>(b.plan_s, s_values, b.resident != 0, dyn_smem, in, b.y, team.rank);
@@ -377,7 +377,7 @@ __device__ __forceinline__ bool adjoint_step_body(const AdjointArgs& b, const Te
       {
         const double* in = b.y;
         if (b.stage_vector) {
-          stage_vector(b.y, vector_smem, n);
+          stage_for(b.plan_st, team.rank, b.y, vector_smem, n);
           in = vector_smem;
         }
         spmv_block<TV>(b.plan_st, st_values, b.resident != 0, dyn_smem, in, b.raw, team.rank);
@@ -583,7 +583,7 @@ __device__ __forceinline__ bool adjoint_step_body(const AdjointArgs& b, const Te
     {
       const double* in = b.work;
       if (b.stage_vector) {
-        stage_vector(b.work, vector_smem, n);
+        stage_for(b.plan_s, team.rank, b.work, vector_smem, n);
         in = vector_smem;
       }
       spmv_block<TV>(b.plan_s, s_values, b.resident != 0, dyn_smem, in, b.y, team.rank);
@@ -594,7 +594,7 @@ __device__ __forceinline__ bool adjoint_step_body(const AdjointArgs& b, const Te
     {
       const double* in = b.y;
       if (b.stage_vector) {
-        stage_vector(b.y, vector_smem, n);
+        stage_for(b.plan_st, team.rank, b.y, vector_smem, n);
         in = vector_smem;
       }
       spmv_block<TV>(b.plan_st, st_values, b.resident != 0, dyn_smem, in, b.raw, team.rank);

@@ -264,6 +264,13 @@ struct SpmvPlan {
   const int* off4;      // [rows + 1]
   const int4* col4;     // [groups]
   const void* val4;     // [groups][4] values in the factor precision
+  // Subset staging (resident plans whose vector is staged): block b stages
+  // only the vector entries stage_cols[stage_off[b] .. stage_off[b+1]) and its
+  // resident slice holds columns renumbered into that list (col_local).
+  // nullptr: the whole vector is staged and the slice keeps global columns.
+  const int* stage_off;
+  const int* stage_cols;
+  const int* col_local;
 };
 
 // Shared-memory layout of one resident slice: values, columns, relative row
@@ -362,6 +369,7 @@ struct StepArgs {
   int resident;        // 1: factor slices live in dynamic shared memory for the launch
   int stage_vector;    // 1: the SpMV input vector is staged in shared memory
   int vector_smem_offset;
+  int f32_vectors;     // 1: refinement products on float4 vectors with float32 sums (resident, staged)
   double* svd_u;       // warm-start singular vectors per element sample [E*S][9] (or nullptr)
   double* svd_v;
   const int* a_off;    // constant matrix A (refinement residual)
@@ -384,6 +392,10 @@ struct StepArgs {
   int window;
   double* hist_x;   // [(window+1)][3n]
   double* hist_g;
+  // History of the block's own particle rows in dynamic shared memory: byte
+  // offset of [window+1][hist_rows][3] x then g, or -1 to use hist_x/hist_g.
+  int hist_smem_offset;
+  int hist_rows;
   int* aa_state;    // count, start, count_used, start_used
   double* aa_gamma; // [kMaxWindow]
   int* aa_accept;

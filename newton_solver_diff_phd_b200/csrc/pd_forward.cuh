@@ -6,9 +6,9 @@
 //   P3 y = S b          S rows, nnz-balanced block ranges    (sparse.py:209-227)
 //   P4 x = S^T y        S^T rows + Dirichlet values + Anderson history and Gram partials
 //                       (sparse.py:341-348, kernels.py:287-291, anderson.py:306-354)
-//   serial              Anderson least squares in the last-arriving block (anderson.py:410-475)
+//   every block         Anderson least squares on the reduced partials (anderson.py:410-475)
 //   P5 Anderson apply + convergence partials                 (anderson.py:478-503, kernels.py:354-401)
-//   serial              dual convergence gate, loop decision
+//   one warp, next P1   dual convergence gate, loop decision
 // Only P1->P2, P2->P3, P3->P4, P4->P5 and P5->P1 cross blocks; particle rows
 // of P4/P5 are owned by one block, so history, previous iterate and previous
 // projection of a particle are only ever touched by that block.
@@ -139,13 +139,22 @@ __device__ __forceinline__ void tet_element(const Args& a, int e, bool warm, TS*
   }
 }
 
-// P1 for Tet4: one thread per element. Element e belongs to block
-// e % blocks: the local step is spread over every SM instead of filling the
-// first ones.
+// Contiguous range [first, last) of `count` work items of this block: the
+// items are split evenly (sizes differ by at most one) over the team.
+__device__ __forceinline__ void team_range(int count, Team team, int& first, int& last) {
+  const int share = count / team.size, extra = count % team.size;
+  first = team.rank * share + min(team.rank, extra);
+  last = first + share + (team.rank < extra ? 1 : 0);
+}
+
+// P1 for Tet4: one thread per element, each block a contiguous range of
+// elements, so the loads of indices, gradients and warm-start vectors of a
+// warp are contiguous.
 template <typename TL>
 __device__ void local_step_tet(const StepArgs& a, bool warm, Team team) {
-  const int gthreads = team.size * blockDim.x;
-  for (int e = threadIdx.x * team.size + team.rank; e < a.ne; e += gthreads) tet_element<TL>(a, e, warm, a.svd_u, a.svd_v);
+  int first, last;
+  team_range(a.ne, team, first, last);
+  for (int e = first + threadIdx.x; e < last; e += blockDim.x) tet_element<TL>(a, e, warm, a.svd_u, a.svd_v);
 }
 
 // Local step of Hex8 cell e by the eight lanes (lane & 7 = Gauss sample) of
@@ -245,16 +254,18 @@ __device__ __forceinline__ void hex_cell(const Args& a, const double* grad_smem,
   }
 }
 
-// P1 for Hex8: eight lanes per cell, four cells per warp. Cell groups are
-// interleaved over the team's blocks (group g lives in block g % blocks).
+// P1 for Hex8: eight lanes per cell, four cells per warp, each block a
+// contiguous range of cells. Every lane of a warp takes part in each pass
+// (the sample reduction shuffles span the warp); lanes past the range work
+// on a clamped cell and store nothing.
 template <typename TL>
 __device__ void local_step_hex(const StepArgs& a, const double* grad_smem, bool warm, Team team) {
-  const int lane = threadIdx.x & 31;
-  const int group_in_warp = lane >> 3;
-  const int warps_total = (team.size * blockDim.x) >> 5;
-  const int warp_in_block = threadIdx.x >> 5;
-  for (int base = (warp_in_block * team.size + team.rank) * 4; base < a.ne; base += warps_total * 4) {
-    hex_cell<TL>(a, grad_smem, base + group_in_warp, warm, a.svd_u, a.svd_v);
+  int first, last;
+  team_range(a.ne, team, first, last);
+  const int group = threadIdx.x >> 3;  // cell slot of this lane group in the block, 0..31
+  for (int base = first; base < last; base += kBlock / 8) {
+    const int e = base + group;
+    hex_cell<TL>(a, grad_smem, e < last ? e : a.ne, warm, a.svd_u, a.svd_v);
   }
 }
 
@@ -299,9 +310,10 @@ __device__ void load_slice(const SpmvPlan& plan, const TV* global_values, char* 
   int* col = reinterpret_cast<int*>(base + align16(plan.max_nnz * static_cast<int>(sizeof(TV))));
   int* off = col + align16(plan.max_nnz * 4) / 4;
   int* rowlist = off + align16((plan.max_rows + 1) * 4) / 4;
+  const int* columns = plan.col_local != nullptr ? plan.col_local : plan.col;
   for (int k = threadIdx.x; k < nnz; k += blockDim.x) {
     val[k] = global_values[k0 + k];
-    col[k] = plan.col[k0 + k];
+    col[k] = columns[k0 + k];
   }
   for (int r = threadIdx.x; r <= rows; r += blockDim.x) off[r] = plan.off[r0 + r] - k0;
   for (int r = threadIdx.x; r < rows; r += blockDim.x) rowlist[r] = plan.rowlist[r0 + r] - r0;
@@ -316,6 +328,23 @@ __device__ __forceinline__ void stage_vector(const double* vec, double* smem_vec
 #pragma unroll 4
   for (int k = threadIdx.x; k < pairs; k += blockDim.x) dst[k] = src[k];
   if ((count & 1) && threadIdx.x == 0) smem_vec[count - 1] = vec[count - 1];
+  __syncthreads();
+}
+
+// Stages the vector a product's slice reads into shared memory: the block's
+// subset of entries (renumbered, when the plan has one) or the whole [n][3]
+// vector. Ends with __syncthreads.
+__device__ __forceinline__ void stage_for(const SpmvPlan& plan, int rank, const double* vec, double* smem_vec, int n) {
+  if (plan.stage_cols == nullptr) {
+    stage_vector(vec, smem_vec, n);
+    return;
+  }
+  const int first = plan.stage_off[rank], count = plan.stage_off[rank + 1] - first;
+  const int* cols = plan.stage_cols + first;
+  for (int t = threadIdx.x; t < 3 * count; t += blockDim.x) {
+    const int j = t / 3, c = t - 3 * j;
+    smem_vec[t] = vec[3 * cols[j] + c];
+  }
   __syncthreads();
 }
 
@@ -410,14 +439,79 @@ __device__ void spmv_block_streamed(const SpmvPlan& plan, const double* vec, dou
   }
 }
 
-// out = M vec for this block's rows of one product. Short rows (<= 32 nnz)
-// are summed sequentially by one thread, long rows by one warp when a block has
-// few of them, else by eight lanes (lane-strided, fixed shuffle trees); each
-// row always by the same unit, so the result is
+// Readers of the product's input vector and writers of its output. The
+// float64 pair keeps xyz triples of doubles and accumulates in double; the
+// float32 pair (the refinement modes' residual products) keeps one float4
+// (x, y, z, 0) per particle, a single 16-byte shared-memory load per entry,
+// and accumulates in float: the residual form corrects the rounding.
+struct VecF64 {
+  const double* v;
+  using Acc = double;
+  template <typename TV>
+  __device__ __forceinline__ void fma(TV value, int c, double& sx, double& sy, double& sz) const {
+    const double w = static_cast<double>(value);
+    sx += w * v[3 * c];
+    sy += w * v[3 * c + 1];
+    sz += w * v[3 * c + 2];
+  }
+};
+struct VecF32 {
+  const float4* v;
+  using Acc = float;
+  __device__ __forceinline__ void fma(float value, int c, float& sx, float& sy, float& sz) const {
+    const float4 q = v[c];
+    sx = fmaf(value, q.x, sx);
+    sy = fmaf(value, q.y, sy);
+    sz = fmaf(value, q.z, sz);
+  }
+};
+struct OutF64 {
+  double* o;
+  template <typename A>
+  __device__ __forceinline__ void store(int row, A x, A y, A z) const {
+    o[3 * row] = static_cast<double>(x);
+    o[3 * row + 1] = static_cast<double>(y);
+    o[3 * row + 2] = static_cast<double>(z);
+  }
+};
+struct OutF32 {
+  float4* o;
+  __device__ __forceinline__ void store(int row, float x, float y, float z) const { o[row] = make_float4(x, y, z, 0.0f); }
+};
+
+// Stages a float64 [n][3] vector into shared memory as float4 per particle
+// (the block's subset when the plan has one).
+__device__ __forceinline__ void stage_vector_f32(const SpmvPlan& plan, int rank, const double* vec, float4* smem_vec,
+                                                 int n) {
+  const int first = plan.stage_cols != nullptr ? plan.stage_off[rank] : 0;
+  const int count = plan.stage_cols != nullptr ? plan.stage_off[rank + 1] - first : n;
+  for (int j = threadIdx.x; j < count; j += blockDim.x) {
+    const int i = plan.stage_cols != nullptr ? plan.stage_cols[first + j] : j;
+    smem_vec[j] = make_float4(static_cast<float>(vec[3 * i]), static_cast<float>(vec[3 * i + 1]),
+                              static_cast<float>(vec[3 * i + 2]), 0.0f);
+  }
+  __syncthreads();
+}
+// Copies a float4-per-particle vector into shared memory (the block's subset
+// when the plan has one).
+__device__ __forceinline__ void stage_float4(const SpmvPlan& plan, int rank, const float4* vec, float4* smem_vec, int n) {
+  const int first = plan.stage_cols != nullptr ? plan.stage_off[rank] : 0;
+  const int count = plan.stage_cols != nullptr ? plan.stage_off[rank + 1] - first : n;
+#pragma unroll 4
+  for (int j = threadIdx.x; j < count; j += blockDim.x)
+    smem_vec[j] = vec[plan.stage_cols != nullptr ? plan.stage_cols[first + j] : j];
+  __syncthreads();
+}
+
+// out = M vec for this block's rows of one resident or global CSR slice.
+// Short rows (<= 32 nnz) are summed sequentially by one thread, long rows by
+// one warp when a block has few of them, else by eight lanes (lane-strided,
+// fixed shuffle trees); each row always by the same unit, so the result is
 // bitwise reproducible. Slice data comes from shared memory when resident.
-template <typename TV>
-__device__ void spmv_block(const SpmvPlan& plan, const TV* global_values, bool resident, const char* smem,
-                           const double* vec, double* out, int rank) {
+template <typename TV, typename Vec, typename Out>
+__device__ void spmv_block_rows(const SpmvPlan& plan, const TV* global_values, bool resident, const char* smem,
+                                const Vec vec, const Out out, int rank) {
+  using Acc = typename Vec::Acc;
   const int r0 = plan.part[rank], r1 = plan.part[rank + 1];
   const int rows = r1 - r0;
   const int nshort = plan.nshort[rank];
@@ -436,10 +530,6 @@ __device__ void spmv_block(const SpmvPlan& plan, const TV* global_values, bool r
     rowlist = off + align16((plan.max_rows + 1) * 4) / 4;
     row_shift = r0;
   } else {
-    if (plan.off4 != nullptr) {
-      spmv_block_streamed<TV>(plan, vec, out, plan.rowlist + r0, nshort, rows);
-      return;
-    }
     val = global_values;
     col = plan.col;
     off = plan.off;
@@ -449,18 +539,9 @@ __device__ void spmv_block(const SpmvPlan& plan, const TV* global_values, bool r
   for (int t = threadIdx.x; t < nshort; t += blockDim.x) {
     const int r = rowlist[t];
     const int begin = off[r], end = off[r + 1];
-    double sx = 0.0, sy = 0.0, sz = 0.0;
-    for (int k = begin; k < end; ++k) {
-      const double value = static_cast<double>(val[k]);
-      const int c = col[k];
-      sx += value * vec[3 * c];
-      sy += value * vec[3 * c + 1];
-      sz += value * vec[3 * c + 2];
-    }
-    const int row = r + row_shift;
-    out[3 * row] = sx;
-    out[3 * row + 1] = sy;
-    out[3 * row + 2] = sz;
+    Acc sx = Acc(0), sy = Acc(0), sz = Acc(0);
+    for (int k = begin; k < end; ++k) vec.fma(val[k], col[k], sx, sy, sz);
+    out.store(r + row_shift, sx, sy, sz);
   }
   const int longs = rows - nshort;
   if (longs <= 4 * kWarps) {
@@ -468,24 +549,16 @@ __device__ void spmv_block(const SpmvPlan& plan, const TV* global_values, bool r
     const int lane = threadIdx.x & 31;
     for (int w = nshort + (threadIdx.x >> 5); w < rows; w += kWarps) {
       const int r = rowlist[w];
-      double sx = 0.0, sy = 0.0, sz = 0.0;
+      Acc sx = Acc(0), sy = Acc(0), sz = Acc(0);
 #pragma unroll 4
-      for (int k = off[r] + lane; k < off[r + 1]; k += 32) {
-        const double value = static_cast<double>(val[k]);
-        const int c = col[k];
-        sx += value * vec[3 * c];
-        sy += value * vec[3 * c + 1];
-        sz += value * vec[3 * c + 2];
+      for (int k = off[r] + lane; k < off[r + 1]; k += 32) vec.fma(val[k], col[k], sx, sy, sz);
+#pragma unroll
+      for (int offset = 16; offset > 0; offset >>= 1) {
+        sx += __shfl_xor_sync(0xffffffffu, sx, offset);
+        sy += __shfl_xor_sync(0xffffffffu, sy, offset);
+        sz += __shfl_xor_sync(0xffffffffu, sz, offset);
       }
-      sx = warp_sum(sx);
-      sy = warp_sum(sy);
-      sz = warp_sum(sz);
-      if (lane == 0) {
-        const int row = r + row_shift;
-        out[3 * row] = sx;
-        out[3 * row + 1] = sy;
-        out[3 * row + 2] = sz;
-      }
+      if (lane == 0) out.store(r + row_shift, sx, sy, sz);
     }
     return;
   }
@@ -499,28 +572,30 @@ __device__ void spmv_block(const SpmvPlan& plan, const TV* global_values, bool r
     const int r = valid ? rowlist[nshort + w] : 0;
     const int begin = valid ? off[r] : 0;
     const int end = valid ? off[r + 1] : 0;
-    double sx = 0.0, sy = 0.0, sz = 0.0;
+    Acc sx = Acc(0), sy = Acc(0), sz = Acc(0);
 #pragma unroll 8
-    for (int k = begin + lane; k < end; k += 8) {
-      const double value = static_cast<double>(val[k]);
-      const int c = col[k];
-      sx += value * vec[3 * c];
-      sy += value * vec[3 * c + 1];
-      sz += value * vec[3 * c + 2];
-    }
+    for (int k = begin + lane; k < end; k += 8) vec.fma(val[k], col[k], sx, sy, sz);
 #pragma unroll
     for (int offset = 4; offset > 0; offset >>= 1) {
       sx += __shfl_xor_sync(0xffffffffu, sx, offset);
       sy += __shfl_xor_sync(0xffffffffu, sy, offset);
       sz += __shfl_xor_sync(0xffffffffu, sz, offset);
     }
-    if (valid && lane == 0) {
-      const int row = r + row_shift;
-      out[3 * row] = sx;
-      out[3 * row + 1] = sy;
-      out[3 * row + 2] = sz;
-    }
+    if (valid && lane == 0) out.store(r + row_shift, sx, sy, sz);
   }
+}
+
+// out = M vec (float64 vectors) for this block's rows of one product; plans
+// that are not resident stream the padded layout.
+template <typename TV>
+__device__ void spmv_block(const SpmvPlan& plan, const TV* global_values, bool resident, const char* smem,
+                           const double* vec, double* out, int rank) {
+  if (!resident && plan.off4 != nullptr) {
+    const int r0 = plan.part[rank], r1 = plan.part[rank + 1];
+    spmv_block_streamed<TV>(plan, vec, out, plan.rowlist + r0, plan.nshort[rank], r1 - r0);
+    return;
+  }
+  spmv_block_rows<TV>(plan, global_values, resident, smem, VecF64{vec}, OutF64{out}, rank);
 }
 
 // Anderson Gram entries for history state (count, start): entries
@@ -538,11 +613,24 @@ __device__ __forceinline__ void gram_entry_pair(int entry, int count, int& a, in
   b = a + k;
 }
 
+// Anderson history of the particle rows a block owns: slot k of row i is at
+// x + k * slot_stride + 3 * (i - base) (and likewise g). Either the whole
+// history in global memory (base 0, slot stride 3n) or the block's own rows in
+// shared memory (base = first own row).
+struct History {
+  double* x;
+  double* g;
+  size_t slot_stride;
+  int base;
+  __device__ __forceinline__ double* xs(int slot, int i) const { return x + slot * slot_stride + 3 * (i - base); }
+  __device__ __forceinline__ double* gs(int slot, int i) const { return g + slot * slot_stride + 3 * (i - base); }
+};
+
 // Block partial of the Gram entries over this block's particle rows [r0, r1).
-inline __device__ void gram_partials(const StepArgs& a, int r0, int r1, int count, int start, double* block_out,
-                              double* scratch, int blocks) {
+inline __device__ void gram_partials(const History& h, int window, int r0, int r1, int count, int start,
+                                     double* block_out, double* scratch, int blocks) {
   const int entries = gram_entries(count);
-  const int capacity = a.window + 1;
+  const int capacity = window + 1;
   const int groups = entries > 0 ? kBlock / entries : 0;
   const int t = threadIdx.x;
   double sum = 0.0;
@@ -550,30 +638,32 @@ inline __device__ void gram_partials(const StepArgs& a, int r0, int r1, int coun
     const int entry = t % entries;
     const int group = t / entries;
     const int pairs = count * (count + 1) / 2;
-    const size_t stride = static_cast<size_t>(3) * a.n;
     if (entry < pairs) {
       int ea, eb;
       gram_entry_pair(entry, count, ea, eb);
-      const double* ga1 = a.hist_g + ((start + ea + 1) % capacity) * stride;
-      const double* ga0 = a.hist_g + ((start + ea) % capacity) * stride;
-      const double* gb1 = a.hist_g + ((start + eb + 1) % capacity) * stride;
-      const double* gb0 = a.hist_g + ((start + eb) % capacity) * stride;
+      const int a1 = (start + ea + 1) % capacity, a0 = (start + ea) % capacity;
+      const int b1 = (start + eb + 1) % capacity, b0 = (start + eb) % capacity;
       for (int i = r0 + group; i < r1; i += groups) {
+        const double* ga1 = h.gs(a1, i);
+        const double* ga0 = h.gs(a0, i);
+        const double* gb1 = h.gs(b1, i);
+        const double* gb0 = h.gs(b0, i);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          const double da = ga1[3 * i + c] - ga0[3 * i + c];
-          const double db = gb1[3 * i + c] - gb0[3 * i + c];
+          const double da = ga1[c] - ga0[c];
+          const double db = gb1[c] - gb0[c];
           sum += da * db;
         }
       }
     } else {
       const int ea = entry - pairs;
-      const double* ga1 = a.hist_g + ((start + ea + 1) % capacity) * stride;
-      const double* ga0 = a.hist_g + ((start + ea) % capacity) * stride;
-      const double* gn = a.hist_g + ((start + count) % capacity) * stride;
+      const int a1 = (start + ea + 1) % capacity, a0 = (start + ea) % capacity, top = (start + count) % capacity;
       for (int i = r0 + group; i < r1; i += groups) {
+        const double* ga1 = h.gs(a1, i);
+        const double* ga0 = h.gs(a0, i);
+        const double* gn = h.gs(top, i);
 #pragma unroll
-        for (int c = 0; c < 3; ++c) sum += (ga1[3 * i + c] - ga0[3 * i + c]) * gn[3 * i + c];
+        for (int c = 0; c < 3; ++c) sum += (ga1[c] - ga0[c]) * gn[c];
       }
     }
   }
@@ -587,53 +677,116 @@ inline __device__ void gram_partials(const StepArgs& a, int r0, int r1, int coun
   __syncthreads();
 }
 
-// Eigen-style pivoted LDL^T solve of the leading n x n block (anderson.py:357-407).
-// m, y and perm live in shared memory (work): dynamic indexing of local arrays
-// would put them in local memory, a global-latency round trip per access.
-inline __device__ void aa_ldlt_solve(double (*m)[kMaxWindow], const double* b, int n, double* x, double* work) {
-  double* y = work;
-  int* perm = reinterpret_cast<int*>(work + kMaxWindow);
-  for (int i = 0; i < n; ++i) perm[i] = i;
-  for (int k = 0; k < n; ++k) {
+// Anderson coefficients for a history of exactly M columns: the regularised
+// Gram system (anderson.py:424-447) solved by Eigen's pivoted LDL^T
+// (anderson.py:357-407: largest remaining diagonal as pivot, full row and
+// column swaps, pseudo-inverse of D), with every index fixed at compile time
+// so the matrix lives in registers on this serial path. Returns |gamma|^2.
+template <int M>
+__device__ __noinline__ double aa_coefficients(const double* reduced, double* gamma) {
+  double g[M][M], b[M];
+  {
+    int entry = 0;
+#pragma unroll
+    for (int i = 0; i < M; ++i)
+#pragma unroll
+      for (int j = i; j < M; ++j) g[i][j] = reduced[entry++];
+  }
+  constexpr int pairs = M * (M + 1) / 2;
+#pragma unroll
+  for (int i = 0; i < M; ++i) b[i] = reduced[pairs + i];
+  double trace = 0.0;
+#pragma unroll
+  for (int i = 0; i < M; ++i) {
+    trace += g[i][i];
+#pragma unroll
+    for (int j = i + 1; j < M; ++j) g[j][i] = g[i][j];
+  }
+  const double regularization = fmax(1.0e-6 * trace / static_cast<double>(M), 1.0e-12);
+#pragma unroll
+  for (int i = 0; i < M; ++i) g[i][i] = g[i][i] + regularization;
+  int perm[M];
+#pragma unroll
+  for (int i = 0; i < M; ++i) perm[i] = i;
+#pragma unroll
+  for (int k = 0; k < M; ++k) {
     int biggest = k;
-    for (int i = k + 1; i < n; ++i)
-      if (fabs(m[i][i]) > fabs(m[biggest][biggest])) biggest = i;
-    if (biggest != k) {
-      for (int j = 0; j < n; ++j) {
-        const double t = m[k][j];
-        m[k][j] = m[biggest][j];
-        m[biggest][j] = t;
+    double largest = fabs(g[k][k]);
+#pragma unroll
+    for (int i = k + 1; i < M; ++i) {
+      const double value = fabs(g[i][i]);
+      if (value > largest) {
+        biggest = i;
+        largest = value;
       }
-      for (int i = 0; i < n; ++i) {
-        const double t = m[i][k];
-        m[i][k] = m[i][biggest];
-        m[i][biggest] = t;
-      }
-      const int t = perm[k];
-      perm[k] = perm[biggest];
-      perm[biggest] = t;
     }
-    for (int j = 0; j < k; ++j) m[k][k] = m[k][k] - m[k][j] * m[k][j] * m[j][j];
-    for (int i = k + 1; i < n; ++i) {
-      for (int j = 0; j < k; ++j) m[i][k] = m[i][k] - m[i][j] * m[j][j] * m[k][j];
-      if (m[k][k] != 0.0) m[i][k] = m[i][k] / m[k][k];
+#pragma unroll
+    for (int i = k + 1; i < M; ++i) {
+      if (biggest == i) {
+#pragma unroll
+        for (int j = 0; j < M; ++j) {
+          const double t = g[k][j];
+          g[k][j] = g[i][j];
+          g[i][j] = t;
+        }
+#pragma unroll
+        for (int r = 0; r < M; ++r) {
+          const double t = g[r][k];
+          g[r][k] = g[r][i];
+          g[r][i] = t;
+        }
+        const int t = perm[k];
+        perm[k] = perm[i];
+        perm[i] = t;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < k; ++j) g[k][k] = g[k][k] - g[k][j] * g[k][j] * g[j][j];
+#pragma unroll
+    for (int i = k + 1; i < M; ++i) {
+#pragma unroll
+      for (int j = 0; j < k; ++j) g[i][k] = g[i][k] - g[i][j] * g[j][j] * g[k][j];
+      if (g[k][k] != 0.0) g[i][k] = g[i][k] / g[k][k];
     }
   }
-  for (int i = 0; i < n; ++i) y[i] = b[perm[i]];
-  for (int i = 0; i < n; ++i)
-    for (int j = 0; j < i; ++j) y[i] = y[i] - m[i][j] * y[j];
-  for (int i = 0; i < n; ++i) y[i] = fabs(m[i][i]) > DBL_MIN ? y[i] / m[i][i] : 0.0;
-  for (int r = 0; r < n; ++r) {
-    const int i = n - 1 - r;
-    for (int j = i + 1; j < n; ++j) y[i] = y[i] - m[j][i] * y[j];
+  double y[M];
+#pragma unroll
+  for (int i = 0; i < M; ++i) {
+    y[i] = 0.0;
+#pragma unroll
+    for (int r = 0; r < M; ++r)
+      if (perm[i] == r) y[i] = b[r];
   }
-  for (int i = 0; i < n; ++i) x[perm[i]] = y[i];
+#pragma unroll
+  for (int i = 0; i < M; ++i)
+#pragma unroll
+    for (int j = 0; j < i; ++j) y[i] = y[i] - g[i][j] * y[j];
+#pragma unroll
+  for (int i = 0; i < M; ++i) y[i] = fabs(g[i][i]) > DBL_MIN ? y[i] / g[i][i] : 0.0;
+#pragma unroll
+  for (int r = 0; r < M; ++r) {
+    const int i = M - 1 - r;
+#pragma unroll
+    for (int j = i + 1; j < M; ++j) y[i] = y[i] - g[j][i] * y[j];
+  }
+  double norm = 0.0;
+#pragma unroll
+  for (int r = 0; r < M; ++r) {
+    double x = 0.0;
+#pragma unroll
+    for (int i = 0; i < M; ++i)
+      if (perm[i] == r) x = y[i];
+    gamma[r] = x;
+    norm += x * x;
+  }
+  return norm;
 }
 
 // Serial Anderson step (one thread) from the reduced Gram entries (anderson.py:424-475).
-// work: shared memory of at least 2 * kMaxWindow * kMaxWindow doubles.
+// work: unused scratch kept for the callers' signature.
 inline __device__ void aa_solve(int* state, double* gamma, int* accept, const double* reduced, int window,
                                 double* work) {
+  (void)work;
   int count = state[0];
   int start = state[1];
   const int capacity = window + 1;
@@ -641,26 +794,16 @@ inline __device__ void aa_solve(int* state, double* gamma, int* accept, const do
   state[3] = start;
   *accept = 0;
   if (count >= 1) {
-    double (*gram)[kMaxWindow] = reinterpret_cast<double (*)[kMaxWindow]>(work);
-    double* rhs = work + kMaxWindow * kMaxWindow;
-    double* coefficients = rhs + kMaxWindow;
-    const int pairs = count * (count + 1) / 2;
-    int entry = 0;
-    for (int i = 0; i < count; ++i)
-      for (int j = i; j < count; ++j) gram[i][j] = reduced[entry++];
-    for (int i = 0; i < count; ++i) rhs[i] = reduced[pairs + i];
-    double trace = 0.0;
-    for (int i = 0; i < count; ++i) {
-      trace += gram[i][i];
-      for (int j = i + 1; j < count; ++j) gram[j][i] = gram[i][j];
-    }
-    const double regularization = fmax(1.0e-6 * trace / static_cast<double>(count), 1.0e-12);
-    for (int i = 0; i < count; ++i) gram[i][i] = gram[i][i] + regularization;
-    aa_ldlt_solve(gram, rhs, count, coefficients, coefficients + kMaxWindow);
     double norm = 0.0;
-    for (int i = 0; i < count; ++i) {
-      gamma[i] = coefficients[i];
-      norm += coefficients[i] * coefficients[i];
+    switch (count) {
+      case 1: norm = aa_coefficients<1>(reduced, gamma); break;
+      case 2: norm = aa_coefficients<2>(reduced, gamma); break;
+      case 3: norm = aa_coefficients<3>(reduced, gamma); break;
+      case 4: norm = aa_coefficients<4>(reduced, gamma); break;
+      case 5: norm = aa_coefficients<5>(reduced, gamma); break;
+      case 6: norm = aa_coefficients<6>(reduced, gamma); break;
+      case 7: norm = aa_coefficients<7>(reduced, gamma); break;
+      default: norm = aa_coefficients<8>(reduced, gamma); break;
     }
     if (sqrt(norm) >= 10.0) {
       count = 0;
@@ -682,28 +825,29 @@ inline __device__ void aa_solve(int* state, double* gamma, int* accept, const do
 
 // Anderson-mixed value of particle i (anderson.py:478-503), given the history
 // before trimming (count_used, start_used) and the coefficients.
-__device__ __forceinline__ V3<double> aa_apply_row(const StepArgs& a, int i, int count, int start,
+__device__ __forceinline__ V3<double> aa_apply_row(const History& h, int window, int i, int count, int start,
                                                    const double* gamma) {
-  const int capacity = a.window + 1;
-  const size_t stride = static_cast<size_t>(3) * a.n;
+  const int capacity = window + 1;
   const int slot = (start + count) % capacity;
-  const double* hx = a.hist_x + 3 * static_cast<size_t>(i);
-  const double* hg = a.hist_g + 3 * static_cast<size_t>(i);
   V3<double> value;
+  {
+    const double* hx = h.xs(slot, i);
+    const double* hg = h.gs(slot, i);
 #pragma unroll
-  for (int c = 0; c < 3; ++c) value[c] = hx[slot * stride + c] + hg[slot * stride + c];
+    for (int c = 0; c < 3; ++c) value[c] = hx[c] + hg[c];
+  }
   // Fully unrolled and predicated so every history load is issued up front.
 #pragma unroll
   for (int k = 0; k < kMaxWindow; ++k) {
     if (k < count) {
       const int low = (start + k) % capacity;
       const int high = (start + k + 1) % capacity;
+      const double* xh = h.xs(high, i);
+      const double* xl = h.xs(low, i);
+      const double* gh = h.gs(high, i);
+      const double* gl = h.gs(low, i);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const size_t h = high * stride + c;
-        const size_t l = low * stride + c;
-        value[c] -= (hx[h] - hx[l] + hg[h] - hg[l]) * gamma[k];
-      }
+      for (int c = 0; c < 3; ++c) value[c] -= (xh[c] - xl[c] + gh[c] - gl[c]) * gamma[k];
     }
   }
   return value;

@@ -76,6 +76,10 @@ __device__ __forceinline__ bool forward_step_body(const StepArgs& a, const Team 
   __shared__ double s_grad[8 * 8 * 3];
   __shared__ double s_scratch[kBlock];
   __shared__ double s_reduced[64];
+  __shared__ double s_gamma[kMaxWindow];
+  // Anderson state of the step, kept by every block: history count and start,
+  // the count and start the last coefficients were solved for, acceptance.
+  __shared__ int s_aa[5];
   __shared__ int s_control[8];
   const int gtid = team.rank * blockDim.x + threadIdx.x;
   const int gthreads = team.size * blockDim.x;
@@ -132,11 +136,10 @@ __device__ __forceinline__ bool forward_step_body(const StepArgs& a, const Team 
     }
   }
   if (gtid == 0) {
-    a.aa_state[0] = a.aa_state[1] = a.aa_state[2] = a.aa_state[3] = 0;
-    *a.aa_accept = 0;
     *a.iteration = 0;
     *a.active = 1;
   }
+  if (threadIdx.x < 5) s_aa[threadIdx.x] = 0;
   // Factor slices of this block stay in shared memory for the whole step.
   const TV* s_values = sizeof(TV) == sizeof(double) ? reinterpret_cast<const TV*>(a.s_val)
                                                     : reinterpret_cast<const TV*>(a.s_val32);
@@ -160,7 +163,19 @@ __device__ __forceinline__ bool forward_step_body(const StepArgs& a, const Team 
   const int r0 = a.st_part[team.rank], r1 = a.st_part[team.rank + 1];
   // This block's partial-sum slots: my_partials[slot * team.size].
   double* my_partials = a.partials + team.rank;
-  const size_t hstride = static_cast<size_t>(3) * n;
+  // Anderson history of the own rows: in shared memory when the plan made room.
+  History history;
+  if (a.hist_smem_offset >= 0) {
+    history.x = reinterpret_cast<double*>(dyn_smem + a.hist_smem_offset);
+    history.slot_stride = static_cast<size_t>(3) * a.hist_rows;
+    history.g = history.x + (a.window + 1) * history.slot_stride;
+    history.base = r0;
+  } else {
+    history.x = a.hist_x;
+    history.g = a.hist_g;
+    history.slot_stride = static_cast<size_t>(3) * n;
+    history.base = 0;
+  }
 
   PD_TIMER_START();
   for (int iter = 0;; ++iter) {
@@ -251,11 +266,22 @@ __device__ __forceinline__ bool forward_step_body(const StepArgs& a, const Team 
     PD_TIMER(1);
     if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
     PD_TIMER(5);
-    // ---- P3: y = S b.
-    {
+    // ---- P3: y = S b (the residual in the refinement modes, in float32
+    // when the slices and the float4 vector are resident).
+    bool f32_vectors = false;
+    if constexpr (sizeof(TV) == sizeof(float)) {
+      f32_vectors = a.f32_vectors != 0;
+      if (f32_vectors) {
+        float4* staged = reinterpret_cast<float4*>(vector_smem);
+        stage_vector_f32(a.plan_s, team.rank, a.rhs, staged, n);
+        spmv_block_rows<TV>(a.plan_s, s_values, true, dyn_smem, VecF32{staged},
+                            OutF32{reinterpret_cast<float4*>(a.y)}, team.rank);
+      }
+    }
+    if (!f32_vectors) {
       const double* in = a.rhs;
       if (a.stage_vector) {
-        stage_vector(a.rhs, vector_smem, n);
+        stage_for(a.plan_s, team.rank, a.rhs, vector_smem, n);
         in = vector_smem;
       }
       spmv_block<TV>(a.plan_s, s_values, a.resident != 0, dyn_smem, in, a.y, team.rank);
@@ -265,10 +291,17 @@ __device__ __forceinline__ bool forward_step_body(const StepArgs& a, const Team 
     PD_TIMER(5);
 
     // ---- P4: x = S^T y, Dirichlet values, Anderson history and Gram partials.
-    {
+    if constexpr (sizeof(TV) == sizeof(float)) {
+      if (f32_vectors) {
+        float4* staged = reinterpret_cast<float4*>(vector_smem);
+        stage_float4(a.plan_st, team.rank, reinterpret_cast<const float4*>(a.y), staged, n);
+        spmv_block_rows<TV>(a.plan_st, st_values, true, dyn_smem, VecF32{staged}, OutF64{a.x}, team.rank);
+      }
+    }
+    if (!f32_vectors) {
       const double* in = a.y;
       if (a.stage_vector) {
-        stage_vector(a.y, vector_smem, n);
+        stage_for(a.plan_st, team.rank, a.y, vector_smem, n);
         in = vector_smem;
       }
       spmv_block<TV>(a.plan_st, st_values, a.resident != 0, dyn_smem, in, a.x, team.rank);
@@ -293,8 +326,8 @@ __device__ __forceinline__ bool forward_step_body(const StepArgs& a, const Team 
       }
     }
     __syncthreads();
-    const int count = a.window > 0 ? a.aa_state[0] : 0;
-    const int start = a.window > 0 ? a.aa_state[1] : 0;
+    const int count = a.window > 0 ? s_aa[0] : 0;
+    const int start = a.window > 0 ? s_aa[1] : 0;
     const int capacity = a.window + 1;
     for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
       V3<double> value = load3d(a.x, i);
@@ -305,8 +338,8 @@ __device__ __forceinline__ bool forward_step_body(const StepArgs& a, const Team 
       if (a.window > 0) {
         const int slot = (start + count) % capacity;
         const V3<double> previous = load3d(a.prev, i);
-        double* hx = a.hist_x + slot * hstride + 3 * i;
-        double* hg = a.hist_g + slot * hstride + 3 * i;
+        double* hx = history.xs(slot, i);
+        double* hg = history.gs(slot, i);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           hx[c] = previous[c];
@@ -316,18 +349,15 @@ __device__ __forceinline__ bool forward_step_body(const StepArgs& a, const Team 
     }
     if (a.window > 0) {
       __syncthreads();
-      gram_partials(a, r0, r1, count, start, my_partials, s_scratch, team.size);
+      gram_partials(history, a.window, r0, r1, count, start, my_partials, s_scratch, team.size);
       PD_TIMER(3);
-      unsigned generation;
-      if (barrier_arrive(a.barrier, generation, team.size)) {
-        const int entries = gram_entries(count);
-        reduce_partials(a.partials, 0, entries, team.size, s_reduced, s_scratch);
-        if (threadIdx.x == 0) aa_solve(a.aa_state, a.aa_gamma, a.aa_accept, s_reduced, a.window, s_scratch);
-        barrier_release(a.barrier, generation, team.size);
-        __syncthreads();
-      } else if (!barrier_wait(a.barrier, generation, a.status)) {
-        return false;
-      }
+      // Every block reduces the partials in the same fixed order and solves
+      // the same small least-squares problem, so every block holds the same
+      // coefficients and history state: no serial section, no release wait.
+      if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
+      reduce_partials(a.partials, 0, gram_entries(count), team.size, s_reduced, s_scratch);
+      if (threadIdx.x == 0) aa_solve(s_aa, s_gamma, s_aa + 4, s_reduced, a.window, s_scratch);
+      __syncthreads();
       PD_TIMER(6);
     }
 
@@ -335,16 +365,14 @@ __device__ __forceinline__ bool forward_step_body(const StepArgs& a, const Team 
     {
       int accept = 0, used_count = 0, used_start = 0;
       if (a.window > 0) {
-        accept = *reinterpret_cast<volatile int*>(a.aa_accept);
-        used_count = a.aa_state[2];
-        used_start = a.aa_state[3];
-        if (threadIdx.x < kMaxWindow) s_reduced[32 + threadIdx.x] = a.aa_gamma[threadIdx.x];
-        __syncthreads();
+        accept = s_aa[4];
+        used_count = s_aa[2];
+        used_start = s_aa[3];
       }
       double step2 = 0.0, prev2 = 0.0, change2 = 0.0, proj2 = 0.0;
       for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
         V3<double> value = load3d(a.x, i);
-        if (accept) value = aa_apply_row(a, i, used_count, used_start, s_reduced + 32);
+        if (accept) value = aa_apply_row(history, a.window, i, used_count, used_start, s_gamma);
         if (a.free_[i] == 0) value = load3d(a.boundary, i);
         store3(a.x, i, value);
         const V3<double> previous = load3d(a.prev, i);

@@ -418,6 +418,21 @@ int pd_plan_launch(PdSolver* s, int blocks, int budget) {
   s->plan_st.smem_offset = slice_s;
   s->vector_smem_offset = slices;
   s->smem = static_cast<size_t>(slices + (s->stage_vector ? vector_bytes : 0));
+  // The Anderson history of a block's own particle rows, x and g, for the
+  // current window, when it fits beside the slices.
+  {
+    const int slots = s->options.anderson_window + 1;
+    const size_t history_bytes = 2 * static_cast<size_t>(slots) * s->plan_st.max_rows * 3 * sizeof(double);
+    const size_t offset = static_cast<size_t>(pdb200::align16(static_cast<int>(s->smem)));
+    if (s->options.resident != 0 && s->options.anderson_window > 0 && offset + history_bytes <= static_cast<size_t>(budget)) {
+      s->hist_smem_offset = static_cast<int>(offset);
+      s->hist_slots = slots;
+      s->smem = offset + history_bytes;
+    } else {
+      s->hist_smem_offset = -1;
+      s->hist_slots = 0;
+    }
+  }
   auto fill_plan = [&](pdb200::SpmvPlan& plan, const DeviceBuffer& off, const DeviceBuffer& col, const DeviceBuffer& val,
                        const DeviceBuffer& val32, const DeviceBuffer& part, const DeviceBuffer& rowlist,
                        const DeviceBuffer& nshort) {
@@ -432,6 +447,46 @@ int pd_plan_launch(PdSolver* s, int blocks, int budget) {
   fill_plan(s->plan_s, s->d_s_off, s->d_s_col, s->d_s_val, s->d_s_val32, s->d_s_part, s->d_s_rowlist, s->d_s_nshort);
   fill_plan(s->plan_st, s->d_st_off, s->d_st_col, s->d_st_val, s->d_st_val32, s->d_st_part, s->d_st_rowlist,
             s->d_st_nshort);
+  // Subset staging: with resident slices and a staged vector, each block
+  // stages only the vector entries its rows read (a block of S^T rows reads
+  // the elimination rows above its particles, a fraction of the vector), and
+  // its slice columns are renumbered into that list.
+  auto subset = [&](const pdb200::Csr& csr, const std::vector<int32_t>& part, pdb200::SpmvPlan& plan,
+                    DeviceBuffer& stage_off, DeviceBuffer& stage_cols, DeviceBuffer& col_local) -> int {
+    if (!(s->resident && s->stage_vector)) {
+      stage_off.release();
+      stage_cols.release();
+      col_local.release();
+      plan.stage_off = nullptr;
+      plan.stage_cols = nullptr;
+      plan.col_local = nullptr;
+      return PD_OK;
+    }
+    std::vector<int32_t> offsets(blocks + 1, 0), columns, local(csr.columns.size());
+    std::vector<int32_t> position(s->n, -1);
+    for (int b = 0; b < blocks; ++b) {
+      const int k0 = csr.offsets[part[b]], k1 = csr.offsets[part[b + 1]];
+      std::vector<int32_t> used(csr.columns.begin() + k0, csr.columns.begin() + k1);
+      std::sort(used.begin(), used.end());
+      used.erase(std::unique(used.begin(), used.end()), used.end());
+      for (size_t j = 0; j < used.size(); ++j) position[used[j]] = static_cast<int32_t>(j);
+      for (int k = k0; k < k1; ++k) local[k] = position[csr.columns[k]];
+      columns.insert(columns.end(), used.begin(), used.end());
+      offsets[b + 1] = static_cast<int32_t>(columns.size());
+    }
+    if (columns.empty()) columns.push_back(0);
+    PD_CUDA(stage_off.upload(offsets));
+    PD_CUDA(stage_cols.upload(columns));
+    PD_CUDA(col_local.upload(local));
+    plan.stage_off = stage_off.as<int>();
+    plan.stage_cols = stage_cols.as<int>();
+    plan.col_local = col_local.as<int>();
+    return PD_OK;
+  };
+  if (int status = subset(s->factor.s, s_part, s->plan_s, s->d_s_stage_off, s->d_s_stage_cols, s->d_s_col_local))
+    return status;
+  if (int status = subset(s->factor.st, st_part, s->plan_st, s->d_st_stage_off, s->d_st_stage_cols, s->d_st_col_local))
+    return status;
   // Streaming layouts for a factor that stays in global memory.
   auto pad = [&](const pdb200::Csr& csr, pdb200::SpmvPlan& plan, DeviceBuffer& off4, DeviceBuffer& col4,
                  DeviceBuffer& val4) -> int {
@@ -736,6 +791,9 @@ void fill_step_args(const PdSolver* s, StepArgs* a) {
   a->window = s->options.anderson_window;
   a->hist_x = s->d_hist_x.as<double>();
   a->hist_g = s->d_hist_g.as<double>();
+  a->hist_smem_offset =
+      (s->hist_smem_offset >= 0 && s->options.anderson_window + 1 <= s->hist_slots) ? s->hist_smem_offset : -1;
+  a->hist_rows = s->plan_st.max_rows;
   a->aa_state = s->d_aa_state.as<int>();
   a->aa_gamma = s->d_aa_gamma.as<double>();
   a->aa_accept = s->d_aa_accept.as<int>();
@@ -757,6 +815,7 @@ void fill_step_args(const PdSolver* s, StepArgs* a) {
   a->resident = s->resident;
   a->stage_vector = s->stage_vector;
   a->vector_smem_offset = s->vector_smem_offset;
+  a->f32_vectors = (s->options.precision != PD_PRECISION_FP64 && s->resident && s->stage_vector) ? 1 : 0;
   a->svd_u = s->options.svd_warm_start ? s->d_svd_u.as<double>() : nullptr;
   a->svd_v = s->options.svd_warm_start ? s->d_svd_v.as<double>() : nullptr;
   a->fc = s->fc;

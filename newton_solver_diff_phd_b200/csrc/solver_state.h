@@ -137,8 +137,14 @@ struct PdSolver {
   // Launch plan of the sparse products.
   pdb200::SpmvPlan plan_s{}, plan_st{};
   int resident = 0, stage_vector = 0, vector_smem_offset = 0;
+  // Own-row Anderson history in dynamic shared memory (offset -1: global),
+  // planned for hist_slots history slots.
+  int hist_smem_offset = -1, hist_slots = 0;
   size_t smem = 0;
   DeviceBuffer d_s_rowlist, d_s_nshort, d_st_rowlist, d_st_nshort, d_svd_u, d_svd_v;
+  // Subset staging of the product vectors (resident, staged plans): per block
+  // the columns its slice reads, and the slice columns renumbered into them.
+  DeviceBuffer d_s_stage_off, d_s_stage_cols, d_s_col_local, d_st_stage_off, d_st_stage_cols, d_st_col_local;
   unsigned long long* timers = nullptr;  // phase timers of PD_PHASE_TIMERS builds
   InverseFactor factor;
   // Device mesh data.
@@ -193,7 +199,7 @@ struct PdSolver {
 // whatever the solver plans next.
 struct TeamPlanBuffers {
   DeviceBuffer s_part, st_part, s_rowlist, s_nshort, st_rowlist, st_nshort, s_off4, s_col4, s_val4, st_off4, st_col4,
-      st_val4, partials, b_partials;
+      st_val4, partials, b_partials, s_stage_off, s_stage_cols, s_col_local, st_stage_off, st_stage_cols, st_col_local;
   void take(PdSolver* s) {
     s_part.swap(s->d_s_part);
     st_part.swap(s->d_st_part);
@@ -209,6 +215,12 @@ struct TeamPlanBuffers {
     st_val4.swap(s->d_st_val4);
     partials.swap(s->d_partials);
     b_partials.swap(s->b_partials);
+    s_stage_off.swap(s->d_s_stage_off);
+    s_stage_cols.swap(s->d_s_stage_cols);
+    s_col_local.swap(s->d_s_col_local);
+    st_stage_off.swap(s->d_st_stage_off);
+    st_stage_cols.swap(s->d_st_stage_cols);
+    st_col_local.swap(s->d_st_col_local);
     s->plan_valid = false;
   }
 };
@@ -218,7 +230,7 @@ struct TeamPlanBuffers {
 // taken from the saved plan stay valid throughout).
 struct SavedPlan {
   TeamPlanBuffers buffers;
-  int blocks = 0, resident = 0, stage_vector = 0, vector_smem_offset = 0;
+  int blocks = 0, resident = 0, stage_vector = 0, vector_smem_offset = 0, hist_smem_offset = -1, hist_slots = 0;
   size_t smem = 0;
   pdb200::SpmvPlan plan_s{}, plan_st{};
   bool valid = false;
@@ -227,6 +239,8 @@ struct SavedPlan {
     resident = s->resident;
     stage_vector = s->stage_vector;
     vector_smem_offset = s->vector_smem_offset;
+    hist_smem_offset = s->hist_smem_offset;
+    hist_slots = s->hist_slots;
     smem = s->smem;
     plan_s = s->plan_s;
     plan_st = s->plan_st;
@@ -241,6 +255,8 @@ struct SavedPlan {
     s->resident = resident;
     s->stage_vector = stage_vector;
     s->vector_smem_offset = vector_smem_offset;
+    s->hist_smem_offset = hist_smem_offset;
+    s->hist_slots = hist_slots;
     s->smem = smem;
     s->plan_s = plan_s;
     s->plan_st = plan_st;
