@@ -683,7 +683,7 @@ inline __device__ void gram_partials(const History& h, int window, int r0, int r
 // column swaps, pseudo-inverse of D), with every index fixed at compile time
 // so the matrix lives in registers on this serial path. Returns |gamma|^2.
 template <int M>
-__device__ __noinline__ double aa_coefficients(const double* reduced, double* gamma) {
+__device__ __forceinline__ double aa_coefficients(const double* reduced, double* gamma) {
   double g[M][M], b[M];
   {
     int entry = 0;
@@ -784,7 +784,7 @@ __device__ __noinline__ double aa_coefficients(const double* reduced, double* ga
 
 // Serial Anderson step (one thread) from the reduced Gram entries (anderson.py:424-475).
 // work: unused scratch kept for the callers' signature.
-inline __device__ void aa_solve(int* state, double* gamma, int* accept, const double* reduced, int window,
+__device__ __forceinline__ void aa_solve(int* state, double* gamma, int* accept, const double* reduced, int window,
                                 double* work) {
   (void)work;
   int count = state[0];
