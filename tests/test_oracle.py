@@ -231,3 +231,29 @@ def test_oracle_reproduces_the_published_axial_cantilever():
     assert max(iterations) == 16
     assert sum(iterations[3:]) == 192
     assert abs(min(determinants) - 0.9661699048673299) < 1e-12
+
+
+DIFF_PD_SCENES = ["free_fall", "pinned", "planar", "arc", "history", "external"]
+DIFF_PD_FORCES = {
+    "planar": [("planar_contact", [0.0, 0.0, 2.0, 0.0, 3, 1.0e6, 1.0, 0.1])],
+    "arc": [("arc_contact", [0.0, 0.0, 1.0, 0.0, 2.0, 0.0, np.sin(np.radians(30.0)), 0.0, -np.cos(np.radians(30.0)),
+                             1.0, np.radians(32.0), 3, 1.0e6, 1.0, 0.1])],
+}
+
+
+@pytest.mark.parametrize("scene", DIFF_PD_SCENES)
+def test_diff_pd_oracle_matches_the_reference_oracle(scene):
+    from oracle.diff_pd_oracle import DiffPdStep
+
+    g = golden("diff_pd.npz")
+    key = scene + "__"
+    step = DiffPdStep(g[key + "rest"], g[key + "tets"], 1000.0, 4.0e4, 5.0e4, g[key + "free"], (0.0, 0.0, -9.81),
+                      DIFF_PD_FORCES.get(scene, []))
+    dt = float(g[key + "dt"])
+    for t in range(len(g[key + "iterations"])):
+        x, v, iterations = step.step(g[key + "q_in"][t], g[key + "v_in"][t], g[key + "f"][t], dt)
+        assert iterations == int(g[key + "iterations"][t])
+        assert step.halvings == int(g[key + "halvings"][t])
+        assert step.fallbacks == int(g[key + "fallbacks"][t])
+        np.testing.assert_allclose(x, g[key + "q_out"][t], rtol=0.0, atol=1e-12)
+        np.testing.assert_allclose(v, g[key + "v_out"][t], rtol=0.0, atol=1e-10)
