@@ -288,6 +288,43 @@ int pd_apply_inverse(PdSolver* solver, const double* rhs, double* out, void* str
    GPU race. The caller's current device is the same after the call. */
 int pd_apply_inverse_static(PdSolver* solver, const double* rhs, double* out, void* stream);
 
+/* ---- The DiffPD pd_eigen forward step (SolverDiffPD, reference
+   src/newton_solver_diff_phd/_src/solvers/diff_pd/solver.py:65-591). It runs on a
+   Tet4 solver created and built as usual, whose materials are mu = w_c / 2
+   and lambda = w_v for every element (so its constant matrix and inverse
+   factor are DiffPD's A = m/h^2 I + (w_c + w_v) Vbar sum_e G_e G_e^T). Each
+   step minimises 1/2 m/h^2 |x - rhs|^2 + E_pd(x) by L-BFGS with A^{-1} as
+   initial inverse Hessian and a backtracking Armijo line search, in one
+   persistent launch. Status bits (pd_read_status): 1 not converged within
+   max_pd_iter, 2 a singular deformation gradient met the volume projection,
+   4 a line search used all max_ls_iter halvings (informational). */
+typedef struct PdDiffPdOptions {
+  int32_t max_pd_iter;     /* >= 1 */
+  int32_t max_ls_iter;     /* >= 1 */
+  int32_t history;         /* L-BFGS pairs, 2..32 */
+  int32_t use_corotated;   /* 1: the corotated energy w_c/2 |F - R|^2 is on */
+  int32_t use_volume;      /* 1: the volume energy w_v/2 |F - P_v(F)|^2 is on */
+  double corotated_weight; /* w_c [Pa] */
+  double volume_weight;    /* w_v [Pa] */
+  double abs_tol;          /* [N] */
+  double rel_tol;          /* relative to |m/h^2 rhs| over the free rows */
+} PdDiffPdOptions;
+/* The explicit contact state forces after gravity (SolverDiffPD(state_forces=...),
+   solver.py:23-55): kinds[count] (0 planar_contact, 1 arc_contact) and packed
+   rows parameters[count][18] (planar: unit normal, offset / |n|, p, kn, kf, mu;
+   arc: center, unit axis, unit start, axis x start, radius, angle, p, kn, kf,
+   mu). Host arrays, copied. count 0 removes them. */
+int pd_diffpd_set_state_forces(PdSolver* solver, int32_t count, const int32_t* kinds, const double* parameters);
+/* SolverDiffPD.step (solver.py:549-591): q, qd, f device [n][3] in the state
+   precision; gravity host [3] (the gravity state force); q_out, qd_out device
+   outputs (distinct from the inputs). dt must equal the last pd_build's dt. */
+int pd_diffpd_step(PdSolver* solver, const PdDiffPdOptions* options, const void* q, const void* qd, const void* f,
+                   const double gravity[3], double dt, void* q_out, void* qd_out, void* stream);
+/* Device float64 [n][3] positions and velocities of the last DiffPD step
+   (solver.positions / solver.velocities, solver.py:365-375) and its L-BFGS
+   iteration count (host; synchronises `stream` when requested). */
+int pd_diffpd_results(PdSolver* solver, double** positions, double** velocities, int32_t* iterations, void* stream);
+
 /* ---- Batched rollouts.
    Many independent built solvers (uneven sizes allowed) advanced together in
    one CUDA graph per rollout. Under the default TEAMS schedule the graph is

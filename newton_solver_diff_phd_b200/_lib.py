@@ -73,6 +73,20 @@ class PdOptions(ctypes.Structure):
     ]
 
 
+class PdDiffPdOptions(ctypes.Structure):
+    _fields_ = [
+        ("max_pd_iter", ctypes.c_int32),
+        ("max_ls_iter", ctypes.c_int32),
+        ("history", ctypes.c_int32),
+        ("use_corotated", ctypes.c_int32),
+        ("use_volume", ctypes.c_int32),
+        ("corotated_weight", ctypes.c_double),
+        ("volume_weight", ctypes.c_double),
+        ("abs_tol", ctypes.c_double),
+        ("rel_tol", ctypes.c_double),
+    ]
+
+
 class PdBatchOptions(ctypes.Structure):
     _fields_ = [
         ("svd_warm_start", ctypes.c_int32),
@@ -121,6 +135,9 @@ SIGNATURES = {
     "pd_backward_contact": ([_P, _P, _P, _D] + [_P] * 12, ctypes.c_int),
     "pd_set_phase_timers": ([_P, _P], ctypes.c_int),
     "pd_set_spin_limit": ([_P, ctypes.c_uint32], ctypes.c_int),
+    "pd_diffpd_set_state_forces": ([_P, _I32, _P, _P], ctypes.c_int),
+    "pd_diffpd_step": ([_P, ctypes.POINTER(PdDiffPdOptions), _P, _P, _P, _P, _D, _P, _P, _P], ctypes.c_int),
+    "pd_diffpd_results": ([_P, ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_I32), _P], ctypes.c_int),
     "pd_barrier_probe": ([ctypes.c_int, _I32, _I32, _I32, ctypes.c_uint32, _P, _P], ctypes.c_int),
     "pd_read_status": ([_P, ctypes.POINTER(_I32), _P], ctypes.c_int),
     "pd_iterations": ([_P, ctypes.POINTER(_I32), ctypes.POINTER(_I32), _P], ctypes.c_int),

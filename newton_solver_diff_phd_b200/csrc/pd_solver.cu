@@ -815,7 +815,11 @@ void fill_step_args(const PdSolver* s, StepArgs* a) {
   a->resident = s->resident;
   a->stage_vector = s->stage_vector;
   a->vector_smem_offset = s->vector_smem_offset;
-  a->f32_vectors = (s->options.precision != PD_PRECISION_FP64 && s->resident && s->stage_vector) ? 1 : 0;
+  // Float32 residual products, except with a frictional boundary: its Newton
+  // step on the multipliers combines the product with the float64 panel,
+  // and the float32 sums keep the coupled iteration from its tight tolerances.
+  a->f32_vectors =
+      (s->options.precision != PD_PRECISION_FP64 && s->resident && s->stage_vector && !s->has_friction) ? 1 : 0;
   a->svd_u = s->options.svd_warm_start ? s->d_svd_u.as<double>() : nullptr;
   a->svd_v = s->options.svd_warm_start ? s->d_svd_v.as<double>() : nullptr;
   a->fc = s->fc;

@@ -170,6 +170,11 @@ struct PdSolver {
   int w_rows = 0;
   bool woodbury_lanes = true;  // columns side by side on lanes (false: one launch per column)
   unsigned spin_limit = 0;     // poll budget of the step and backward barriers (0: the built-in budget)
+  // DiffPD forward (pd_diffpd.cu): vectors, L-BFGS history for dp_history
+  // pairs, element energies, packed state forces and counters.
+  DeviceBuffer dp_vectors, dp_hist, dp_energy, dp_kinds, dp_params, dp_counters;
+  int dp_history = 0;
+  int dp_force_count = 0;
   int woodbury_team = 0;       // blocks per lane (0: from nnz(S) and the element samples)
   DeviceBuffer w_row_node, w_row_vector, w_value, w_selected, w_order, w_control, w_columns, w_gram, w_coefficients,
       w_permutation, w_work, w_seed, w_mu;
