@@ -272,6 +272,10 @@ __device__ bool diffpd_step_body(const DiffPdArgs& a, const Team team, char* dyn
     a.counters[0] = 0;
     a.counters[1] = 0;
   }
+  // rhs and the first trial were written by particle index across the team;
+  // the threshold reads rhs by owned row and the first evaluation reads every
+  // corner of its elements.
+  if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
   if (a.resident) {
     load_slice<double>(a.plan_s, a.s_val, dyn_smem, team.rank);
     load_slice<double>(a.plan_st, a.st_val, dyn_smem, team.rank);

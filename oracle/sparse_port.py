@@ -223,27 +223,24 @@ class SparsePort:
         return mu, material, iterations
 
 
-def time_hex_instance(job):
-    """Forward steps then their exact-mode adjoints of one Hex8 instance with this port; returns
-    ``(seconds, steps)``. ``job`` is ``(vertices, hexes, free, mu, lame, forces, factor, dt, steps)``
-    (picklable, so a process pool can run instances side by side)."""
+def time_hex_iterations(job):
+    """Cost of one forward local/global iteration and of one adjoint CG iteration of one Hex8
+    instance with this port, from a given state: ``(particles, forward s/iteration, adjoint
+    s/iteration)``. ``job`` is ``(vertices, hexes, free, mu, lame, forces, factor, q, v, dt,
+    iterations)`` with ``factor`` the inverse factor of ``body.matrix(dt)`` (picklable: a process
+    pool measures instances side by side)."""
     import time
 
-    vertices, hexes, free, mu, lame, forces, factor, dt, steps = job
+    vertices, hexes, free, mu, lame, forces, factor, q, v, dt, iterations = job
     body = pd_oracle.Body.hex(vertices, hexes, free, mu, lame, 1000.0)
     port = SparsePort(body, factor, dt)
-    q = np.asarray(vertices, dtype=np.float64).copy()
-    v = np.zeros_like(q)
+    q = np.asarray(q, dtype=np.float64)
+    v = np.asarray(v, dtype=np.float64)
     start = time.perf_counter()
-    records = []
-    for _ in range(steps):
-        x, _, _ = port.step(q, v, forces, np.zeros(3), max_iterations=5000, abs_tol=1.0e-9, rel_tol=1.0e-6)
-        records.append(x)
-        v = (x - q) / dt
-        q = x
+    x, _, _ = port.step(q, v, forces, np.zeros(3), max_iterations=iterations, abs_tol=0.0, rel_tol=0.0)
+    forward = (time.perf_counter() - start) / iterations
     seed = np.ones_like(q)
-    for x in reversed(records):
-        mu_adj, _, _ = port.backward(x, seed, np.zeros_like(seed), max_iterations=5000, abs_tol=1.0e-9,
-                                     rel_tol=1.0e-6, mode="exact")
-        seed = body.mass / dt**2 * mu_adj
-    return time.perf_counter() - start, steps
+    start = time.perf_counter()
+    _, _, count = port.backward_cg(x, seed, np.zeros_like(seed), max_iterations=iterations, abs_tol=0.0, rel_tol=0.0)
+    adjoint = (time.perf_counter() - start) / max(count, 1)
+    return len(vertices), forward, adjoint

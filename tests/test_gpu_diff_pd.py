@@ -6,7 +6,9 @@ deformed block, a pinned cantilever, planar and arc penalty contacts, a long
 step whose L-BFGS history wraps and whose line search halves, external
 forces). As in the reference test, every step starts from the same float32
 state on both sides, so the iteration counts must be equal and the float64
-positions agree to rounding.
+positions agree to rounding: within 1e-10 m, since the device sums in a
+different order and the long step's 160 L-BFGS iterations carry those
+roundings along (1.1e-11 m measured).
 """
 
 import numpy as np
@@ -19,7 +21,7 @@ from tests.helpers import golden
 
 DENSITY, COROTATED, VOLUME, DT = 1000.0, 4.0e4, 5.0e4, 1.0e-2
 GRAVITY = (0.0, 0.0, -9.81)
-POSITION_TOL = 1.0e-12
+POSITION_TOL = 1.0e-10
 ARC_START = (np.sin(np.radians(30.0)), 0.0, -np.cos(np.radians(30.0)))
 SCENES = {
     "free_fall": ((0.0, 0.0, 1.0), False, []),
