@@ -88,7 +88,7 @@ __device__ __forceinline__ V3<double> dp_friction(V3<double> v, V3<double> norma
   return (-fmin(kf, mu * fn / (length(us) + DBL_EPSILON))) * us;
 }
 
-// One packed contact state force at (q, v) (kernels.py:119-150).
+// One packed contact state force at (q, v) (diff_pd/kernels.py:118-152).
 __device__ __forceinline__ V3<double> dp_state_force(int kind, const double* c, V3<double> q, V3<double> v) {
   V3<double> force = v3<double>(0.0, 0.0, 0.0);
   if (kind == kPlanarContact) {
@@ -113,7 +113,7 @@ __device__ __forceinline__ V3<double> dp_state_force(int kind, const double* c, 
 }
 
 // Energy and corner forces of element e at the positions `vec`
-// (kernels.py:238-280): -Vbar sum_E w_E (F - P_E) g_k, energies in order.
+// (diff_pd/kernels.py:231-271): -Vbar sum_E w_E (F - P_E) g_k, energies in order.
 __device__ __forceinline__ void dp_element(const DiffPdArgs& a, int e, const double* vec) {
   double m[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
 #pragma unroll

@@ -560,6 +560,21 @@ class SolverDiffPhD:
         _lib.check(self._lib.pd_set_anderson_window(self._handle, int(window)))
         self.anderson_window = int(window)
 
+    def set_tolerances(self, *, rel_tol: float | None = None, abs_tol: float | None = None,
+                       max_iterations: int | None = None) -> None:
+        """Change the stopping rule of later steps (and of batches created afterwards) without
+        rebuilding the factor; arguments left as ``None`` keep their values."""
+        rel = self.rel_tol if rel_tol is None else rel_tol
+        absolute = self.abs_tol if abs_tol is None else abs_tol
+        limit = self.max_iterations if max_iterations is None else max_iterations
+        for name, value in (("abs_tol", absolute), ("rel_tol", rel)):
+            if not np.isfinite(value) or value < 0:
+                raise ValueError(f"{name} must be finite and nonnegative")
+        if not np.isfinite(limit) or limit < 1 or int(limit) != limit:
+            raise ValueError("max_iterations must be a positive integer")
+        _lib.check(self._lib.pd_set_tolerances(self._handle, int(limit), float(absolute), float(rel)))
+        self.rel_tol, self.abs_tol, self.max_iterations = float(rel), float(absolute), int(limit)
+
     def notify_model_changed(self, flags: int = 0) -> None:
         """Rebuild the material weights and inverse factor before the next step."""
         if torch.cuda.is_current_stream_capturing():
