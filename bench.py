@@ -570,6 +570,33 @@ def family_cpu_baseline(q_traj, qd_traj, offsets, forward_iterations, adjoint_it
             "estimated_single_core_seconds": seconds}
 
 
+def batched_roofline(family, iterations, forward_ms, window):
+    """HBM roofline of the batched forward launch: the algorithmic bytes of every local/global
+    iteration of every instance, summed over the run's recorded iteration counts, per second of
+    the launch. Per iteration of an instance (fp32+refine: float32 factor values and product
+    vectors, float64 elsewhere): the two factor products 2 (nnz(S) (4 + 4) + 4 (N + 1)) and
+    their vectors 2 (3N 4) 2, the element indices and contributions E 8 4 + 3E 8, the iterate
+    and projection 2 (3N 8), the Anderson history (2m + 4) 3N 8, the convergence vectors
+    4 (3N 8), and the float64 refinement residual nnz(A) (8 + 4) + 2 (3N 8)."""
+    total = 0.0
+    for i, (spec, _, solver, _) in enumerate(family):
+        n = (spec.nx + 1) * (spec.ny + 1) * (spec.nz + 1)
+        e = spec.nx * spec.ny * spec.nz
+        nnz_s = solver.factor_stats()[1]
+        counts = [np.array([1 + (k > 0) + (k < d) for k in range(d + 1)]) for d in (spec.nx, spec.ny, spec.nz)]
+        nnz_a = int(np.einsum("i,j,k->", *counts))
+        per_iteration = (2 * (nnz_s * 8 + 4 * (n + 1)) + 2 * (3 * n * 4) * 2 + e * 8 * 4 + 3 * e * 8 + 2 * 3 * n * 8
+                         + (2 * window + 4) * 3 * n * 8 + 4 * 3 * n * 8 + nnz_a * 12 + 2 * 3 * n * 8)
+        total += float(iterations[:, i].sum()) * per_iteration
+    peak, peak_kind = measured_peak()
+    achieved = total / (forward_ms / 1000.0) / 1.0e9
+    return {"bound": "hbm", "kernel": "team_forward_kernel<double,float> (one launch = the whole 25-step rollout)",
+            "achieved": achieved, "peak": peak, "peak_kind": f"{peak_kind} burst copy GB/s", "unit": "GB/s",
+            "frac": achieved / peak, "traffic": None, "algorithmic_bytes_per_launch": total,
+            "traffic_note": "the 8-second launch is beyond the capture size rule; a small batch's DRAM traffic is "
+                            "in profiles/team_forward_kernel_cantilever_batch.md"}
+
+
 def stalled_instances(family, status):
     """The instances that hit the iteration limit in some step, with their nominal tip strain
     F / (E A) (total tip force over Young's modulus times the cross-section)."""
@@ -739,6 +766,7 @@ def run_batched(args, device):
     measurement = batch.measurement()
     del batch
     stalled = stalled_instances(family, status)
+    roofline = batched_roofline(family, forward_its, fwd_ms, int(chosen["window"]))
     accurate = accurate_batched(family, chosen, measurement, q0, qd0, forces, weight, steps_total)
     precision = precision_check(device)
     cpu = family_cpu_baseline(traj[0], traj[1], batch_offsets, forward_its, adjoint_its)
@@ -760,7 +788,7 @@ def run_batched(args, device):
         "precision_check": precision,
         "schedule": "teams",
         "autotune": tuning["chosen"],
-        "autotune_replan": [p for p in tuning["probes"] if "replan_steps" in p or "adjoint_replan" in p],
+        "autotune_probes": tuning["probes"],
         "plain_anderson_window": 5,
         "instances": instances,
         "particles": particles,
@@ -771,6 +799,7 @@ def run_batched(args, device):
         "max_iterations_per_step": 5000,
         "instances_hitting_max_iterations": int(np.count_nonzero(status & 1)),
         "stalled_instances": stalled,
+        "roofline": roofline,
         "at_rel_tol_1e-9": accurate,
         "max_rel_position_err_vs_plain_same_precision": err,
         "err_note": "final positions, instances that converged within the iteration limit in every step; both paths "
@@ -784,16 +813,37 @@ def run_batched(args, device):
 
 def run_contact(args, device):
     """The Tet4 contact workload (a 20x20x10 block of 1 mm cubes, 20,000 Tet4, on a frictional
-    plane, poked by a meshed probe through the penalty mesh contact): the first `contact_steps`
-    of its 200-step rollout forward, their state adjoint, and the contact projection of dL/d(mu,
-    lambda) for the last step. The rollout is cut short so the leg stays within seconds."""
+    plane, poked by a meshed probe through the penalty mesh contact), twice:
+
+    * as configured (dt 1 ms, probe 4 mm down over 200 steps): the first `contact_steps` steps
+      forward, their state adjoint, and the contact projection of dL/d(mu, lambda) of the
+      busiest converged step. At dt 1 ms the explicit penalty (kn 5e3 N/m on a 1.1 mg vertex)
+      is outside its stability limit (dt < 2 / sqrt(kn / m) = 30 us), so this measures the
+      contact machinery under chatter, not a physical poke;
+    * a stable variant, all 200 steps: dt 20 us (omega dt = 1.35 < 2 for the penalty), the probe
+      starting 0.6 mm above the block (outside the contact radius) and 1 mm down over the rollout
+      (0.25 m/s), everything else the same.
+    """
+    from newton_solver_diff_phd_b200.scenes import Poke
+
+    out = _contact_leg(Poke(offset=(0.0, 0.0)), args.contact_steps, device)
+    if not args.no_contact_stable:
+        stable = Poke(offset=(0.0, 0.0), dt=2.0e-5, probe_travel=1.0e-3, start_gap=0.6e-3)
+        out["stable"] = _contact_leg(stable, stable.steps, device)
+        out["stable"]["variant"] = ("dt 20 us (explicit penalty stable: omega dt = 1.35 < 2), the probe starting "
+                                    "0.6 mm above the block (outside the 0.55 mm contact radius) and 1 mm down over "
+                                    "200 steps; block, plane, probe and contact parameters as configured")
+    return out
+
+
+def _contact_leg(spec, steps, device):
+    """One contact rollout of `steps` steps of `spec` (see `run_contact`)."""
     import torch
 
     from newton_solver_diff_phd_b200 import SolverDiffPhD, Tape
-    from newton_solver_diff_phd_b200.scenes import Poke, poke_scene
+    from newton_solver_diff_phd_b200.scenes import poke_scene
 
-    spec = Poke(offset=(0.0, 0.0))
-    steps = min(args.contact_steps, spec.steps)
+    steps = min(steps, spec.steps)
     model, opt = poke_scene(spec, device=device)
     solver = SolverDiffPhD(model, density=spec.density, frictional_boundary=opt["frictional_boundary"],
                            frictional_vertices=opt["frictional_vertices"], mesh_contact=opt["mesh_contact"],
@@ -870,7 +920,8 @@ def run_contact(args, device):
         "status_forward": forward_status,
         "status_adjoint": adjoint_status,
         "config": {"particles": model.particle_count, "tets": model.tet_count, "plane_vertices": 441,
-                   "probe": "icosphere r 3 mm (162 surface particles), prescribed 4 mm descent over 200 steps",
+                   "probe": f"icosphere r 3 mm (162 surface particles), prescribed {spec.probe_travel * 1e3:g} mm "
+                            f"descent over {spec.steps} steps",
                    "mesh_contact": "radius 0.55 mm, kn 5e3 N/m, kf 50 N s/m, mu 0.5", "dt": spec.dt,
                    "rel_tol": REL_TOL, "precision": "fp64", "adjoint": "reference"},
         "data": "synthetic (block and probe built in scenes.poke_scene)",
@@ -1171,6 +1222,8 @@ def main():
     parser.add_argument("--no-contact", action="store_true", help="skip the Tet4 contact (poke) leg")
     parser.add_argument("--no-cantilever", action="store_true", help="skip the reference Hex8 cantilever leg")
     parser.add_argument("--contact-steps", type=int, default=30, help="steps of the contact leg's rollout")
+    parser.add_argument("--no-contact-stable", action="store_true",
+                        help="skip the contact leg's stable 200-step variant (dt 20 us)")
     parser.add_argument("--twist", action="store_true",
                         help="add the 35,721-particle Hex8 twist-release leg (minutes: its host factor build)")
     parser.add_argument("--twist-steps", type=int, default=100, help="steps of the twist-release leg")

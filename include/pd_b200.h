@@ -310,18 +310,18 @@ typedef struct PdDiffPdOptions {
   double rel_tol;          /* relative to |m/h^2 rhs| over the free rows */
 } PdDiffPdOptions;
 /* The explicit contact state forces after gravity (SolverDiffPD(state_forces=...),
-   solver.py:23-55): kinds[count] (0 planar_contact, 1 arc_contact) and packed
+   solver.py:24-56): kinds[count] (0 planar_contact, 1 arc_contact) and packed
    rows parameters[count][18] (planar: unit normal, offset / |n|, p, kn, kf, mu;
    arc: center, unit axis, unit start, axis x start, radius, angle, p, kn, kf,
    mu). Host arrays, copied. count 0 removes them. */
 int pd_diffpd_set_state_forces(PdSolver* solver, int32_t count, const int32_t* kinds, const double* parameters);
-/* SolverDiffPD.step (solver.py:549-591): q, qd, f device [n][3] in the state
+/* SolverDiffPD.step (solver.py:539-591): q, qd, f device [n][3] in the state
    precision; gravity host [3] (the gravity state force); q_out, qd_out device
    outputs (distinct from the inputs). dt must equal the last pd_build's dt. */
 int pd_diffpd_step(PdSolver* solver, const PdDiffPdOptions* options, const void* q, const void* qd, const void* f,
                    const double gravity[3], double dt, void* q_out, void* qd_out, void* stream);
 /* Device float64 [n][3] positions and velocities of the last DiffPD step
-   (solver.positions / solver.velocities, solver.py:365-375) and its L-BFGS
+   (solver.positions / solver.velocities, solver.py:260-268) and its L-BFGS
    iteration count (host; synchronises `stream` when requested). */
 int pd_diffpd_results(PdSolver* solver, double** positions, double** velocities, int32_t* iterations, void* stream);
 

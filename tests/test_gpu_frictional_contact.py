@@ -331,3 +331,68 @@ def test_woodbury_columns_on_lanes_match_one_launch_per_column(friction):
     # The columns are fixed points capped at 120 iterations, the oracle's are direct solves.
     scale = max(np.abs(oracle["materials"]).max(), 1.0e-30)
     np.testing.assert_allclose(results[0]["materials"], oracle["materials"], rtol=0.0, atol=1.0e-4 * scale)
+
+
+def test_young_and_poisson_gradients_through_the_contact_projection_match_central_differences():
+    """dL/dE and dL/dnu of one contact step (an 8x6x2 block pressed onto the frictionless floor,
+    63 active contacts) through the Woodbury projection, against central differences of the
+    float64 step result. E and nu are global; the tape's per-tet dL/d(mu, lambda) is contracted
+    with the float32 Lame parameters each perturbed model actually holds. Both perturbed steps
+    keep the base step's active contact set (checked), inside which the contact solution is
+    smooth. With friction the reference's projection holds both tangent directions of every
+    active contact fixed (adjoint.py:21-25), which is not the derivative of a sliding contact
+    (measured 11 % off on this block), so the finite-difference check is frictionless."""
+    friction = 0.0
+    from newton_solver_diff_phd_b200 import Tape, meshes
+
+    young, poisson, dt = 5.0e4, 0.35, 0.004
+    rng = np.random.default_rng(11)
+
+    def step(young_value, poisson_value, taped):
+        mu, lam = meshes.lame_from_young(young_value, poisson_value)
+        builder = ModelBuilder(gravity=(0.0, 0.0, -9.81))
+        builder.add_soft_grid(pos=(0.0, 0.0, 0.0), rot=None, vel=(0.0, 0.0, 0.0), dim_x=8, dim_y=6, dim_z=2,
+                              cell_x=0.05, cell_y=0.05, cell_z=0.05, density=DENSITY, k_mu=float(mu),
+                              k_lambda=float(lam), k_damp=0.0)
+        model = builder.finalize("cuda", requires_grad=taped)
+        solver = SolverDiffPhD(model, density=DENSITY, frictional_boundary=("planar", (0.0, 0.0, 1.0, 0.0)),
+                               friction=friction, max_iterations=4000, abs_tol=1.0e-13, rel_tol=1.0e-12)
+        q = model.particle_q.cpu().numpy().astype(np.float64)
+        q[:, 2] += 0.0002
+        v = np.tile([0.1, 0.0, -0.5], (model.particle_count, 1))
+        state_in, state_out = _state(model, q, v), model.state(requires_grad=taped)
+        if taped:
+            model.tet_materials.grad = torch.zeros_like(model.tet_materials)
+            state_in.requires_grad_(True)
+            with Tape() as tape:
+                solver.step(state_in, state_out, None, None, dt)
+            tape.backward(grads={state_out.particle_q: torch.tensor(gq, dtype=torch.float32, device="cuda"),
+                                 state_out.particle_qd: torch.tensor(gv, dtype=torch.float32, device="cuda")})
+        else:
+            solver.step(state_in, state_out, None, None, dt)
+        solver.check_status()
+        x = solver._x.cpu().numpy()
+        q_in = state_in.particle_q.detach().double().cpu().numpy()
+        loss = float(np.sum(gq * x) + np.sum(gv * (x - q_in) / dt))
+        active = (solver.contact_multipliers.cpu().numpy() > 0).copy()
+        lame = model.tet_materials[:, :2].detach().double().cpu().numpy()
+        grad = model.tet_materials.grad[:, :2].double().cpu().numpy() if taped else None
+        return loss, active, lame, grad
+
+    builder_count = 9 * 7 * 3
+    gq = rng.standard_normal((builder_count, 3))
+    gv = rng.standard_normal((builder_count, 3))
+    _, base_active, _, grad = step(young, poisson, True)
+    assert base_active.sum() > 32
+    for name, eps in (("young", 1.0e-4 * young), ("poisson", 1.0e-4)):
+        results = []
+        for sign in (1.0, -1.0):
+            e = young + sign * eps if name == "young" else young
+            nu = poisson + sign * eps if name == "poisson" else poisson
+            results.append(step(e, nu, False))
+        (loss_p, active_p, lame_p, _), (loss_m, active_m, lame_m, _) = results
+        np.testing.assert_array_equal(active_p, base_active)
+        np.testing.assert_array_equal(active_m, base_active)
+        measured = loss_p - loss_m
+        predicted = float(np.sum(grad * (lame_p - lame_m)))
+        assert abs(predicted - measured) <= 1.0e-3 * abs(measured), (name, predicted, measured)
