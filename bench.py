@@ -433,13 +433,14 @@ def build_all(solvers, dt):
         list(pool.map(lambda s: s._build(dt), solvers))
 
 
-def precision_check(device, stride=32, steps=BATCH_STEPS):
+def precision_check(device, windows=None, stride=32, steps=BATCH_STEPS):
     """Errors of the batched leg on every `stride`-th instance of the family over the whole
     rollout, against batched fp64 converged to rel 1e-11: (1) fp32+refine converged to rel 1e-11
     as well, the error of the arithmetic alone; (2) fp32+refine at the bench's own stopping rule
     (rel 1e-6, abs 1e-9), the error the timed leg's results carry, instance by instance; (3)
     fp32+refine at rel 1e-9, the tightened rule of `accurate_batched`. Every run stops at 5,000
-    iterations per step; instances that reach it in any run are left out of the maxima."""
+    iterations per step; instances that reach it in any run are left out of the maxima. `windows`
+    gives every family instance's Anderson window (those of the timed batch; default 5)."""
     import torch
 
     from newton_solver_diff_phd_b200 import SolverDiffPhD
@@ -447,16 +448,17 @@ def precision_check(device, stride=32, steps=BATCH_STEPS):
     from newton_solver_diff_phd_b200.scenes import cantilever_family, cantilever_model
 
     specs = cantilever_family(BATCH_COUNT, seed=0)[::stride]
+    sample_windows = [5] * len(specs) if windows is None else list(windows)[::stride]
     runs = {"fp64": ("fp64", 1.0e-11, 1.0e-14, 5000), "fp32+refine": ("fp32+refine", 1.0e-11, 1.0e-14, 5000),
             "bench": ("fp32+refine", REL_TOL, ABS_TOL, 5000), "tight": ("fp32+refine", 1.0e-9, 1.0e-12, 5000)}
     results = {}
     for name, (precision, rel_tol, abs_tol, limit) in runs.items():
         solvers, models, forces = [], [], []
-        for spec in specs:
+        for spec, window in zip(specs, sample_windows):
             model, mesh, materials, force = cantilever_model(spec, device=device)
             solvers.append(SolverDiffPhD(model, density=1000.0, hex_mesh=mesh, hex_materials=materials,
-                                         precision=precision, anderson_window=5, rel_tol=rel_tol, abs_tol=abs_tol,
-                                         max_iterations=limit, adjoint="exact"))
+                                         precision=precision, anderson_window=window, rel_tol=rel_tol,
+                                         abs_tol=abs_tol, max_iterations=limit, adjoint="exact"))
             models.append(model)
             forces.append(torch.as_tensor(force, device=device))
         build_all(solvers, BATCH_DT)
@@ -492,7 +494,7 @@ def precision_check(device, stride=32, steps=BATCH_STEPS):
                 "max_rel_grad_err": float(g[k].max()) if k.any() else None,
                 "instances_within_1e-6_position": int(np.count_nonzero(p[k] <= 1.0e-6))}
 
-    return {"instances": [int(i) for i in range(0, BATCH_COUNT, stride)],
+    return {"instances": [int(i) for i in range(0, BATCH_COUNT, stride)], "anderson_windows": sample_windows,
             "sample": f"every {stride}th instance of the family, all {steps} steps, final positions",
             "converged_both": int(keep.sum()), "steps": steps, "rel_tol": 1.0e-11,
             "max_rel_position_err_fp32_refine_vs_fp64": float(pos[keep].max()) if keep.any() else None,
@@ -662,31 +664,35 @@ def run_batched(args, device):
     rng = np.random.default_rng(1)
     weights = [torch.as_tensor(rng.standard_normal((m.particle_count, 3)), dtype=torch.float32, device=device)
                for _, m, _, _ in family]
+    # Autotuner (untimed): the Anderson window of every instance from 6-step
+    # probe rollouts (windows 0, 3, 5, 8 for all, then each instance's best),
+    # the team sizing, a stall fallback to window 0 and a re-plan of team sizes
+    # and lanes from one measured 25-step rollout.
+    q0 = torch.cat([m.particle_q for _, m, _, _ in family]).contiguous()
+    qd0 = torch.zeros_like(q0)
+    forces = torch.cat([f for _, _, _, f in family]).contiguous()
+    batch, tuning = autotune([s for _, _, s, _ in family], BATCH_DT, q0, qd0, forces, steps=6, windows=(0, 3, 5, 8),
+                             replan_steps=BATCH_STEPS, instance_windows=True)
+    tuned = tuning["chosen"]
+    tuned_plan = batch.measurement() if tuned.get("replanned") else None
+    del batch
     # Plain path: every instance on its own, one cooperative launch per step
-    # (default plans, Anderson window 5).
+    # (default plans), with the same per-instance Anderson windows.
     stream = torch.cuda.current_stream()
     plain_ms, plain_final = 0.0, []
-    for (spec, model, solver, forces), w in zip(family, weights):
+    for (spec, model, solver, instance_forces), w in zip(family, weights):
         driver = Rollout(solver, BATCH_STEPS, BATCH_DT)
-        q0 = model.particle_q
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         start.record(stream)
-        final = driver.forward(q0, torch.zeros_like(q0), forces)
+        final = driver.forward(model.particle_q, torch.zeros_like(model.particle_q), instance_forces)
         driver.backward(w, None)
         end.record(stream)
         torch.cuda.synchronize()
         plain_ms += start.elapsed_time(end)
         plain_final.append(final.particle_q.clone())
-    for _, _, solver, _ in family:
-        solver.read_status()
-    # Batched path: Anderson window and team sizing chosen by the autotuner
-    # from 6-step probe rollouts, then team sizes and lanes re-planned from one
-    # measured 25-step rollout (all untimed).
-    q0 = torch.cat([m.particle_q for _, m, _, _ in family]).contiguous()
-    qd0 = torch.zeros_like(q0)
-    forces = torch.cat([f for _, _, _, f in family]).contiguous()
-    batch, tuning = autotune([s for _, _, s, _ in family], BATCH_DT, q0, qd0, forces, steps=6,
-                             replan_steps=BATCH_STEPS)
+    plain_status = np.array([solver.read_status() for _, _, solver, _ in family])
+    batch = BatchedSolver([s for _, _, s, _ in family], BATCH_DT, team_nnz=tuned["team_nnz"],
+                          team_samples=tuned["team_samples"], measured=tuned_plan)
     sizes, grid = batch.team_sizes()
     weight = batch.concat(weights)
     eo = batch.element_offsets
@@ -768,7 +774,7 @@ def run_batched(args, device):
     stalled = stalled_instances(family, status)
     roofline = batched_roofline(family, forward_its, fwd_ms, int(chosen["window"]))
     accurate = accurate_batched(family, chosen, measurement, q0, qd0, forces, weight, steps_total)
-    precision = precision_check(device)
+    precision = precision_check(device, windows=[s.anderson_window for _, _, s, _ in family])
     cpu = family_cpu_baseline(traj[0], traj[1], batch_offsets, forward_its, adjoint_its)
     return {
         "workload": BATCH_WORKLOAD,
@@ -789,7 +795,8 @@ def run_batched(args, device):
         "schedule": "teams",
         "autotune": tuning["chosen"],
         "autotune_probes": tuning["probes"],
-        "plain_anderson_window": 5,
+        "plain_anderson_windows": "the batch's per-instance windows",
+        "plain_instances_with_status": int(np.count_nonzero(plain_status)),
         "instances": instances,
         "particles": particles,
         "team_sizes": {str(int(k)): int(v) for k, v in zip(*np.unique(sizes, return_counts=True))},

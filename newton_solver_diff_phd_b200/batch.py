@@ -272,7 +272,8 @@ def _time_forward(batch, q0, qd0, forces, steps):
 
 
 def autotune(solvers, dt, q0, qd0, forces, *, steps: int = 2, windows=(3, 5, 8),
-             teams=((65536, 512), (32768, 256), (131072, 1024)), replan_steps: int = 0, **options):
+             teams=((65536, 512), (32768, 256), (131072, 1024)), replan_steps: int = 0,
+             instance_windows: bool = False, **options):
     """Pick the Anderson window and the team sizing of a batch from short rollouts.
 
     Times a ``steps``-step forward rollout of the batch for every window (with
@@ -280,40 +281,73 @@ def autotune(solvers, dt, q0, qd0, forces, *, steps: int = 2, windows=(3, 5, 8),
     window, and returns ``(BatchedSolver, report)`` built with the fastest
     setting (the solvers keep its window). ``q0``, ``qd0``, ``forces`` are the
     concatenated rollout inputs; the probe runs the rollout's first steps.
-    With ``replan_steps`` > 0 a rollout of that many steps then measures
-    every instance's cost and the batch is re-planned from it (larger teams
-    for the instances on the critical path) when that is faster.
+
+    With ``instance_windows`` every instance also gets its own window: the one
+    of the probed windows with which it needed the fewest iterations without
+    reaching its iteration limit (Anderson mixing stalls on some strongly
+    nonlinear instances that plain local/global iterations solve); that
+    mixed setting is timed like the others and kept when it is the fastest.
+    With ``replan_steps`` > 0 a rollout of that many steps then measures every
+    instance's cost; with ``instance_windows``, instances that reached their
+    iteration limit there fall back to window 0 (no mixing) and the rollout is
+    measured again; the batch is then re-planned from those costs (larger
+    teams for the instances on the critical path) when that is faster.
     """
     report = []
     best = None
+    per_window = {}
 
-    def probe(window, team_nnz, team_samples):
-        nonlocal best
-        for solver in solvers:
+    def apply(assignment):
+        for solver, window in zip(solvers, assignment):
             if solver.anderson_window != window:
                 solver.set_anderson_window(window)
+
+    def probe(assignment, label, team_nnz, team_samples):
+        nonlocal best
+        apply(assignment)
         batch = BatchedSolver(solvers, dt, team_nnz=team_nnz, team_samples=team_samples, **options)
         ms = _time_forward(batch, q0, qd0, forces, steps)
-        report.append({"window": window, "team_nnz": team_nnz, "team_samples": team_samples, "ms": ms})
+        status, iterations = batch.read()
+        report.append({"window": label, "team_nnz": team_nnz, "team_samples": team_samples, "ms": ms,
+                       "iterations": int(iterations.sum()), "instances_at_limit": int(np.count_nonzero(status & 1))})
         if best is None or ms < best[0]:
-            best = (ms, window, team_nnz, team_samples)
+            best = (ms, list(assignment), label, team_nnz, team_samples)
         del batch
+        return status, iterations
 
     for window in windows:
-        probe(window, *teams[0])
+        status, iterations = probe([window] * len(solvers), window, *teams[0])
+        per_window[window] = (iterations.sum(axis=0), (status & 1) != 0)
+    if instance_windows and len(windows) > 1:
+        order = list(windows)
+        cost = np.stack([per_window[w][0] + np.where(per_window[w][1], np.iinfo(np.int32).max // 4, 0)
+                         for w in order])
+        mixed = [order[k] for k in np.argmin(cost, axis=0)]
+        if len(set(mixed)) > 1:
+            probe(mixed, "per-instance", *teams[0])
     for team_nnz, team_samples in teams[1:]:
-        probe(best[1], team_nnz, team_samples)
-    _, window, team_nnz, team_samples = best
-    for solver in solvers:
-        if solver.anderson_window != window:
-            solver.set_anderson_window(window)
+        probe(best[1], best[2], team_nnz, team_samples)
+    _, assignment, label, team_nnz, team_samples = best
+    apply(assignment)
     batch = BatchedSolver(solvers, dt, team_nnz=team_nnz, team_samples=team_samples, **options)
-    chosen = {"window": window, "team_nnz": team_nnz, "team_samples": team_samples}
+    chosen = {"window": label, "team_nnz": team_nnz, "team_samples": team_samples}
     if replan_steps:
         # Second stage: one rollout of `replan_steps` steps with the chosen
         # setting measures every instance's duration and iterations; the batch
         # is re-planned from those costs when that rollout gets faster.
         first = _time_forward(batch, q0, qd0, forces, replan_steps)
+        if instance_windows:
+            status, _ = batch.read()
+            stalled = [i for i in np.flatnonzero(status & 1) if assignment[i] != 0]
+            if stalled:
+                for i in stalled:
+                    assignment[i] = 0
+                apply(assignment)
+                del batch
+                batch = BatchedSolver(solvers, dt, team_nnz=team_nnz, team_samples=team_samples, **options)
+                report.append({"stall_fallback": [int(i) for i in stalled], "ms_before": first})
+                first = _time_forward(batch, q0, qd0, forces, replan_steps)
+                chosen["window"] = "per-instance"
         measured = batch.measurement()
         replanned = BatchedSolver(solvers, dt, team_nnz=team_nnz, team_samples=team_samples, measured=measured,
                                   **options)
@@ -322,4 +356,7 @@ def autotune(solvers, dt, q0, qd0, forces, *, steps: int = 2, windows=(3, 5, 8),
         if second < first:
             batch = replanned
             chosen["replanned"] = True
+    if chosen["window"] == "per-instance":
+        counts = np.unique([s.anderson_window for s in solvers], return_counts=True)
+        chosen["windows"] = {str(int(w)): int(c) for w, c in zip(*counts)}
     return batch, {"chosen": chosen, "probes": report, "probe_steps": steps}

@@ -285,6 +285,38 @@ def test_autotune_picks_a_probed_setting():
     assert np.all(status == 0)
 
 
+def test_autotune_gives_a_stalling_instance_its_own_window():
+    """Instance 203 of the family (6x2x2 cells, E 1.96e5 Pa, 219 N at the tip, nominal strain
+    2.8) reaches the iteration limit with Anderson window 5 already in its second step, while
+    plain local/global iterations (window 0) converge in under 1,000; instance 0 converges
+    with either. The per-instance autotuner keeps mixing for the instance it helps and gives
+    the stalling one window 0, and the tuned batch converges in every step."""
+    from newton_solver_diff_phd_b200.batch import autotune
+    from newton_solver_diff_phd_b200.scenes import cantilever_family
+
+    family = cantilever_family(256, seed=0)
+    instances = []
+    for spec in (family[0], family[203]):
+        model, mesh, materials, forces = cantilever_model(spec)
+        solver = SolverDiffPhD(model, density=1000.0, hex_mesh=mesh, hex_materials=materials,
+                               precision="fp32+refine", anderson_window=5, rel_tol=1e-6, abs_tol=1e-9,
+                               max_iterations=5000)
+        instances.append((model, solver, torch.as_tensor(forces, device="cuda")))
+    solvers = [s for _, s, _ in instances]
+    probe = BatchedSolver(solvers, DT)
+    q0 = probe.concat([m.particle_q for m, _, _ in instances])
+    forces = probe.concat([f for _, _, f in instances])
+    del probe
+    batch, report = autotune(solvers, DT, q0, torch.zeros_like(q0), forces, steps=2, windows=(0, 5),
+                             teams=((65536, 512),), replan_steps=6, instance_windows=True)
+    stalled_probe = [p for p in report["probes"] if p.get("window") == 5]
+    assert stalled_probe and stalled_probe[0]["instances_at_limit"] == 1
+    assert solvers[1].anderson_window == 0
+    batch.rollout(q0, torch.zeros_like(q0), forces, 6)
+    status, iterations = batch.read()
+    assert np.all(status == 0) and iterations[:, 1].max() < 5000
+
+
 def test_measured_replan_keeps_the_results():
     """A batch planned from a previous rollout's measured costs (team sizes and
     lanes) solves the same problems: single-instance results within 1e-6."""
