@@ -338,6 +338,8 @@ def run_b200(args):
             result["twist"] = run_twist(args, device)
         if world == 1 and not args.no_cantilever:
             result["cantilever"] = run_cantilever(args, device)
+        if world == 1:
+            result["factor_build"] = run_factor_build(device)
     distributed.barrier(ranks)
     distributed.teardown(ranks)
     if rank == 0:
@@ -572,14 +574,15 @@ def family_cpu_baseline(q_traj, qd_traj, offsets, forward_iterations, adjoint_it
             "estimated_single_core_seconds": seconds}
 
 
-def batched_roofline(family, iterations, forward_ms, window):
+def batched_roofline(family, iterations, forward_ms):
     """HBM roofline of the batched forward launch: the algorithmic bytes of every local/global
     iteration of every instance, summed over the run's recorded iteration counts, per second of
     the launch. Per iteration of an instance (fp32+refine: float32 factor values and product
     vectors, float64 elsewhere): the two factor products 2 (nnz(S) (4 + 4) + 4 (N + 1)) and
     their vectors 2 (3N 4) 2, the element indices and contributions E 8 4 + 3E 8, the iterate
     and projection 2 (3N 8), the Anderson history (2m + 4) 3N 8, the convergence vectors
-    4 (3N 8), and the float64 refinement residual nnz(A) (8 + 4) + 2 (3N 8)."""
+    4 (3N 8), and the float64 refinement residual nnz(A) (8 + 4) + 2 (3N 8); m is the instance's own
+    Anderson window."""
     total = 0.0
     for i, (spec, _, solver, _) in enumerate(family):
         n = (spec.nx + 1) * (spec.ny + 1) * (spec.nz + 1)
@@ -588,7 +591,7 @@ def batched_roofline(family, iterations, forward_ms, window):
         counts = [np.array([1 + (k > 0) + (k < d) for k in range(d + 1)]) for d in (spec.nx, spec.ny, spec.nz)]
         nnz_a = int(np.einsum("i,j,k->", *counts))
         per_iteration = (2 * (nnz_s * 8 + 4 * (n + 1)) + 2 * (3 * n * 4) * 2 + e * 8 * 4 + 3 * e * 8 + 2 * 3 * n * 8
-                         + (2 * window + 4) * 3 * n * 8 + 4 * 3 * n * 8 + nnz_a * 12 + 2 * 3 * n * 8)
+                         + (2 * solver.anderson_window + 4) * 3 * n * 8 + 4 * 3 * n * 8 + nnz_a * 12 + 2 * 3 * n * 8)
         total += float(iterations[:, i].sum()) * per_iteration
     peak, peak_kind = measured_peak()
     achieved = total / (forward_ms / 1000.0) / 1.0e9
@@ -629,6 +632,7 @@ def accurate_batched(family, chosen, measurement, q0, qd0, forces, weight, steps
     try:
         batch = BatchedSolver(solvers, BATCH_DT, team_nnz=chosen["team_nnz"], team_samples=chosen["team_samples"],
                               measured=measurement)
+        batch.read()  # clears the status bits of the earlier runs
         stream = torch.cuda.current_stream()
         e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
         e0.record(stream)
@@ -664,20 +668,22 @@ def run_batched(args, device):
     rng = np.random.default_rng(1)
     weights = [torch.as_tensor(rng.standard_normal((m.particle_count, 3)), dtype=torch.float32, device=device)
                for _, m, _, _ in family]
-    # Autotuner (untimed): the Anderson window of every instance from 6-step
-    # probe rollouts (windows 0, 3, 5, 8 for all, then each instance's best),
-    # the team sizing, a stall fallback to window 0 and a re-plan of team sizes
-    # and lanes from one measured 25-step rollout.
+    # Autotuner (untimed): the Anderson window from 6-step probe rollouts
+    # (3, 5, 8), the team sizing, and a re-plan of team sizes and lanes from
+    # one measured 25-step rollout. (Per-instance windows with a window-0
+    # fallback for stalled instances, `instance_windows=True`, converge more
+    # of them but slow the batch by a third on this family and leave the
+    # window-0 instances farther from the fixed point at rel 1e-6.)
     q0 = torch.cat([m.particle_q for _, m, _, _ in family]).contiguous()
     qd0 = torch.zeros_like(q0)
     forces = torch.cat([f for _, _, _, f in family]).contiguous()
-    batch, tuning = autotune([s for _, _, s, _ in family], BATCH_DT, q0, qd0, forces, steps=6, windows=(0, 3, 5, 8),
-                             replan_steps=BATCH_STEPS, instance_windows=True)
+    batch, tuning = autotune([s for _, _, s, _ in family], BATCH_DT, q0, qd0, forces, steps=6, windows=(3, 5, 8),
+                             replan_steps=BATCH_STEPS)
     tuned = tuning["chosen"]
     tuned_plan = batch.measurement() if tuned.get("replanned") else None
     del batch
     # Plain path: every instance on its own, one cooperative launch per step
-    # (default plans), with the same per-instance Anderson windows.
+    # (default plans), with the tuned Anderson window.
     stream = torch.cuda.current_stream()
     plain_ms, plain_final = 0.0, []
     for (spec, model, solver, instance_forces), w in zip(family, weights):
@@ -735,6 +741,7 @@ def run_batched(args, device):
     tuning["probes"].append({"adjoint_replan": True, "ms": first_ms, "replanned_ms": second_ms})
     del replanned, one_batch
     torch.cuda.synchronize()
+    batch.read()  # clears the status bits of the untimed rollouts
     flush.fill_(1.0)
     e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
     e0.record(stream)
@@ -772,7 +779,7 @@ def run_batched(args, device):
     measurement = batch.measurement()
     del batch
     stalled = stalled_instances(family, status)
-    roofline = batched_roofline(family, forward_its, fwd_ms, int(chosen["window"]))
+    roofline = batched_roofline(family, forward_its, fwd_ms)
     accurate = accurate_batched(family, chosen, measurement, q0, qd0, forces, weight, steps_total)
     precision = precision_check(device, windows=[s.anderson_window for _, _, s, _ in family])
     cpu = family_cpu_baseline(traj[0], traj[1], batch_offsets, forward_its, adjoint_its)
@@ -795,7 +802,7 @@ def run_batched(args, device):
         "schedule": "teams",
         "autotune": tuning["chosen"],
         "autotune_probes": tuning["probes"],
-        "plain_anderson_windows": "the batch's per-instance windows",
+        "plain_anderson_window": "the batch's",
         "plain_instances_with_status": int(np.count_nonzero(plain_status)),
         "instances": instances,
         "particles": particles,
@@ -1002,11 +1009,43 @@ def run_cantilever(args, device):
     return out
 
 
+def run_factor_build(device):
+    """The exact inverse factor of the largest family instance's PD matrix (Hex8 40x10x10 cells,
+    4,961 rows), built on the host threads and with the rows of L^{-1} on the device: wall time
+    of each build and whether every array is bit-identical."""
+    import scipy.sparse as sp
+
+    from newton_solver_diff_phd_b200 import _lib, meshes
+    from oracle import pd_oracle
+
+    vertices, hexes, _ = meshes.hex_grid(40, 10, 10, 0.01)
+    free = vertices[:, 0] > 1.0e-12
+    young = np.exp(np.random.default_rng(3).uniform(np.log(1.0e5), np.log(1.0e7), len(hexes)))
+    mu, lam = meshes.lame_from_young(young, 0.45)
+    matrix = sp.csr_matrix(pd_oracle.Body.hex(vertices, hexes, free, mu, lam, 1000.0).matrix(BATCH_DT))
+    matrix.sort_indices()
+    csr = (matrix.indptr, matrix.indices, matrix.data)
+    _lib.inverse_factor(csr, device=device.index or 0)  # context and module load, untimed
+    start = time.perf_counter()
+    host = _lib.inverse_factor(csr)
+    host_s = time.perf_counter() - start
+    start = time.perf_counter()
+    on_device = _lib.inverse_factor(csr, device=device.index or 0)
+    device_s = time.perf_counter() - start
+    same = all(np.array_equal(host[k], on_device[k]) for k in host)
+    return {"matrix": "Hex8 cantilever 40x10x10 cells, 4,961 rows", "nnz_S": int(len(host["s_values"])),
+            "host_threads_s": host_s, "device_rows_s": device_s, "bit_identical": bool(same),
+            "host_threads": os.cpu_count(),
+            "note": "ordering, symbolic fill, numeric LDL^T and the CSR assembly run on the host in both builds"}
+
+
 def run_twist(args, device):
     """The large Hex8 twist-release workload (80x20x20 cells, 35,721 particles): `twist_steps` steps
     of dt 1e-3 at rel 1e-6 forward, then the adjoint of the final tip rotation angle w.r.t. the
     initial positions and every cell's Young's modulus with a checkpoint every 10 steps (exact
-    adjoint), in fp64 and in fp32+refine; the factor build (host, threaded) is timed apart."""
+    adjoint), in fp64 and in fp32+refine; the factor build is timed apart, on the host threads for
+    the fp64 solver and with the rows of L^{-1} on the device for the fp32+refine solver (the two
+    factors are bit-identical; tests/test_gpu_factor_device.py)."""
     import torch
 
     from newton_solver_diff_phd_b200 import SolverDiffPhD
@@ -1029,6 +1068,7 @@ def run_twist(args, device):
         solver = SolverDiffPhD(model, density=spec.density, hex_mesh=mesh, hex_materials=materials,
                                precision=precision, rel_tol=REL_TOL, abs_tol=ABS_TOL, max_iterations=5000,
                                adjoint="exact")
+        solver.set_factor_device(precision != "fp64")
         start = time.perf_counter()
         solver._build(spec.dt)
         build_s = time.perf_counter() - start
@@ -1050,7 +1090,8 @@ def run_twist(args, device):
         _, nnz_s, _ = solver.factor_stats()
         grad_e = (gm[:, 0] * dmu_de + gm[:, 1] * dlam_de).cpu().numpy()
         results[precision] = (final.particle_q.double().cpu().numpy(), grad_e, float(angle.detach()))
-        out[precision] = {"factor_build_s": build_s, "nnz_S": int(nnz_s), "forward_ms": e0.elapsed_time(e1),
+        out[precision] = {"factor_build_s": build_s, "factor_rows_of_inverse_on": "host threads" if precision == "fp64"
+                          else "device", "nnz_S": int(nnz_s), "forward_ms": e0.elapsed_time(e1),
                           "adjoint_ms": e1.elapsed_time(e2),
                           "fwd_adjoint_steps_per_s": steps / (e0.elapsed_time(e2) / 1000.0),
                           "final_tip_angle_deg": float(np.degrees(float(angle.detach()))), "status": int(status),

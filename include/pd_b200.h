@@ -188,6 +188,10 @@ int pd_frictional_state(PdSolver* solver, double* multiplier, double* omega, dou
    the exact inverse factor A^{-1} = S^T S on the host (sparse.py:291-320),
    then uploads it. Synchronous; not capturable. */
 int pd_build(PdSolver* solver, double dt);
+/* Where pd_build computes the rows of L^{-1}: 1 on the solver's device (see
+   pd_inverse_build_on), 0 on the host threads (default). Bit-identical either
+   way; takes effect at the next build. Added (no reference counterpart). */
+int pd_set_factor_device(PdSolver* solver, int32_t enabled);
 
 /* Factor statistics of the last build: rows, nnz(S), nnz(L) incl. diagonal. */
 int pd_factor_stats(const PdSolver* solver, int64_t* rows, int64_t* nnz_s, int64_t* nnz_l);
@@ -419,9 +423,10 @@ int pd_batch_team_sizes(const PdBatch* batch, int32_t* sizes, int32_t* grid);
 int pd_batch_forward_stepwise(PdBatch* batch, int32_t steps, double dt, const double gravity[3], const void* q0,
                               const void* qd0, const void* forces, int64_t force_step_stride, void* q_traj,
                               void* qd_traj, double* x_record, void* stream);
-/* Status bits per instance (accumulated, not cleared), [count], and the
-   iteration count of every step of the last rollout, [steps][count]. Either
-   pointer may be NULL. Synchronises the stream. */
+/* Status bits per instance accumulated since the last read, [count] (the read
+   clears them, like pd_read_status), and the iteration count of every step
+   of the last rollout, [steps][count]. Either pointer may be NULL.
+   Synchronises the stream. */
 int pd_batch_read(PdBatch* batch, int32_t* status, int32_t* iterations, void* stream);
 
 /* Host factor build for an arbitrary SPD matrix given as full symmetric CSR
@@ -435,6 +440,12 @@ typedef struct PdInverseFactor PdInverseFactor;
 int pd_inverse_parallel_work(int64_t work);
 int pd_inverse_build(int32_t size, const int32_t* row_offsets, const int32_t* columns, const double* values,
                      PdInverseFactor** out);
+/* pd_inverse_build with the rows of L^{-1} (sparse.py:159-177, the dominant
+   part of the build) computed on CUDA device `device`, level by level of the
+   elimination tree; the factor is bit-identical to the host build. device < 0
+   builds on the host. Added: the reference builds on the host only. */
+int pd_inverse_build_on(int32_t device, int32_t size, const int32_t* row_offsets, const int32_t* columns,
+                        const double* values, PdInverseFactor** out);
 int pd_inverse_sizes(const PdInverseFactor* factor, int32_t* size, int64_t* nnz, int64_t* factorization_nnz);
 /* Copies the arrays: permutation[size], s_offsets[size+1], s_columns[nnz], s_values[nnz],
    st_offsets[size+1], st_columns[nnz], st_values[nnz]. Any pointer may be NULL. */

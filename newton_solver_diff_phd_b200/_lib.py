@@ -157,6 +157,8 @@ SIGNATURES = {
     "pd_batch_set_phase_timers": ([_P, _I32, _P], ctypes.c_int),
     "pd_inverse_parallel_work": ([_I64], ctypes.c_int),
     "pd_inverse_build": ([_I32, _P, _P, _P, ctypes.POINTER(_P)], ctypes.c_int),
+    "pd_inverse_build_on": ([_I32, _I32, _P, _P, _P, ctypes.POINTER(_P)], ctypes.c_int),
+    "pd_set_factor_device": ([_P, _I32], ctypes.c_int),
     "pd_inverse_sizes": ([_P, ctypes.POINTER(_I32), ctypes.POINTER(_I64), ctypes.POINTER(_I64)], ctypes.c_int),
     "pd_inverse_export": ([_P, _P, _P, _P, _P, _P, _P, _P], ctypes.c_int),
     "pd_inverse_free": ([_P], ctypes.c_int),
@@ -214,12 +216,13 @@ def ptr(array) -> int | None:
     return array.data_ptr()
 
 
-def inverse_factor(matrix_csr, run_gap=None):
-    """Build the exact inverse factor of an SPD CSR matrix with the C++ host builder.
+def inverse_factor(matrix_csr, run_gap=None, device=None):
+    """Build the exact inverse factor of an SPD CSR matrix with the C++ builder.
 
     ``matrix_csr`` is ``(offsets, columns, values)`` of the full symmetric matrix.
     Returns a dict with ``permutation`` and the CSR arrays of S and S^T; with
-    ``run_gap`` also ``runs``, the postorder run format of both.
+    ``run_gap`` also ``runs``, the postorder run format of both. ``device``: a
+    CUDA device index computes the rows of L^{-1} there (bit-identical).
     """
     offsets, columns, values = (
         np.ascontiguousarray(matrix_csr[0], dtype=np.int32),
@@ -228,7 +231,11 @@ def inverse_factor(matrix_csr, run_gap=None):
     )
     lib = library()
     handle = _P()
-    check(lib.pd_inverse_build(len(offsets) - 1, ptr(offsets), ptr(columns), ptr(values), ctypes.byref(handle)))
+    if device is None:
+        check(lib.pd_inverse_build(len(offsets) - 1, ptr(offsets), ptr(columns), ptr(values), ctypes.byref(handle)))
+    else:
+        check(lib.pd_inverse_build_on(int(device), len(offsets) - 1, ptr(offsets), ptr(columns), ptr(values),
+                                      ctypes.byref(handle)))
     try:
         size, nnz, factorization = _I32(), _I64(), _I64()
         check(lib.pd_inverse_sizes(handle, ctypes.byref(size), ctypes.byref(nnz), ctypes.byref(factorization)))

@@ -243,7 +243,8 @@ class BatchedSolver:
         return q, qd, x_record
 
     def read(self):
-        """``(status bits per instance, iterations (steps, count) of the last rollout)``; synchronises."""
+        """``(status bits per instance since the last read, iterations (steps, count) of the last
+        rollout)``; the read clears the status bits (like ``SolverDiffPhD.read_status``); synchronises."""
         status = np.zeros(self.count, np.int32)
         iterations = np.zeros((max(self._steps, 0), self.count), np.int32)
         _lib.check(self._lib.pd_batch_read(self._handle, _lib.ptr(status), _lib.ptr(iterations) if self._steps else None,

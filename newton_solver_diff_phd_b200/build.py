@@ -22,7 +22,7 @@ BUILD = PACKAGE / "_build"
 LIBRARY = BUILD / "libpdb200.so"
 
 CUDA_SOURCES = ("pd_kernels.cu", "pd_adjoint.cu", "pd_solver.cu", "pd_noalloc.cu", "pd_batch.cu", "pd_contact.cu",
-                "pd_friction.cu", "pd_woodbury.cu", "pd_diffpd.cu")
+                "pd_friction.cu", "pd_woodbury.cu", "pd_diffpd.cu", "pd_factor_device.cu")
 HOST_SOURCES = ("factor.cpp", "runs.cpp")
 HEADERS = ("factor.h", "runs.h", "pd_math.cuh", "pd_device.cuh", "pd_forward.cuh", "pd_kernels.h", "pd_batch.cuh",
            "pd_team.cuh", "solver_state.h", "pd_geometry.cuh", "pd_friction.cuh")

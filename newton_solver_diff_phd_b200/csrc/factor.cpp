@@ -265,7 +265,7 @@ std::vector<int32_t> nested_dissection(const Adjacency& adjacency) {
 }
 
 std::string build_inverse_factor(int32_t size, const int32_t* row_offsets, const int32_t* row_columns,
-                                 const double* row_values, InverseFactor* out) {
+                                 const double* row_values, InverseFactor* out, const InverseRowsProvider& provider) {
   if (size < 0) return "matrix size must be nonnegative";
   // --- _validate_rows (sparse.py:73-95) ---------------------------------
   std::vector<std::vector<std::pair<int32_t, double>>> rows(size);
@@ -427,14 +427,35 @@ std::string build_inverse_factor(int32_t size, const int32_t* row_offsets, const
   std::vector<int64_t> inv_start(1, 0);
   std::vector<int32_t> inv_columns;
   std::vector<double> inv_values;
-  std::vector<double> current(size, 0.0);
-  std::vector<int32_t> touched_mark(size, -1);
+  if (provider) {
+    LowerFactorView view;
+    view.size = size;
+    view.row_start = row_start.data();
+    view.pattern = pattern.data();
+    view.values = values.data();
+    InverseRows rows_out;
+    const std::string error = provider(view, &rows_out);
+    if (!error.empty()) return error;
+    if (rows_out.start.size() != static_cast<size_t>(size) + 1 ||
+        rows_out.columns.size() != static_cast<size_t>(rows_out.start.back()) ||
+        rows_out.values.size() != rows_out.columns.size()) {
+      return "inverse rows provider returned inconsistent arrays";
+    }
+    if (rows_out.columns.size() > static_cast<size_t>(std::numeric_limits<int32_t>::max())) {
+      return "inverse factor fill exceeds int32 sparse indexing";
+    }
+    inv_start = std::move(rows_out.start);
+    inv_columns = std::move(rows_out.columns);
+    inv_values = std::move(rows_out.values);
+  }
+  std::vector<double> current(provider ? 0 : size, 0.0);
+  std::vector<int32_t> touched_mark(provider ? 0 : size, -1);
   std::vector<int32_t> touched;
   const unsigned hardware = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
   std::unique_ptr<RowPool> pool;
   std::vector<std::vector<std::pair<int32_t, double>>> pieces;
   const int64_t parallel_work = g_parallel_row_work.load();
-  for (int32_t i = 0; i < size; ++i) {
+  for (int32_t i = provider ? size : 0; i < size; ++i) {
     int64_t work = 0;
     for (int64_t p = row_start[i]; p < row_start[i + 1] - 1; ++p) work += inv_start[pattern[p] + 1] - inv_start[pattern[p]];
     // Split only rows whose earlier rows are long: every range costs one
@@ -533,6 +554,8 @@ std::string build_inverse_factor(int32_t size, const int32_t* row_offsets, const
   const int64_t nnz = static_cast<int64_t>(inv_columns.size());
 
   // --- CSR of S (rows: elimination order, columns: original, sorted) ------
+  // Rows are independent: host threads take ranges of rows. Every value is
+  // the same product inv_value * (1 / sqrt(pivot)) as in a sequential pass.
   out->size = size;
   out->permutation = permutation;
   out->diagonal = diagonal;
@@ -542,39 +565,93 @@ std::string build_inverse_factor(int32_t size, const int32_t* row_offsets, const
   s.offsets.assign(size + 1, 0);
   s.columns.resize(nnz);
   s.values.resize(nnz);
-  std::vector<std::pair<int32_t, double>> row;
-  for (int32_t i = 0; i < size; ++i) {
-    const double scale = 1.0 / std::sqrt(diagonal[i]);
-    row.clear();
-    for (int64_t q = inv_start[i]; q < inv_start[i + 1]; ++q) {
-      row.emplace_back(permutation[inv_columns[q]], inv_values[q] * scale);
+  for (int32_t i = 0; i < size; ++i) s.offsets[i + 1] = static_cast<int32_t>(inv_start[i + 1]);
+  const unsigned workers = (nnz >= (1 << 20) && hardware > 1) ? hardware : 1;
+  std::unique_ptr<RowPool> csr_pool(workers > 1 ? new RowPool(workers) : nullptr);
+  auto parallel_rows = [&](const std::function<void(int32_t, int32_t)>& body) {
+    if (!csr_pool) {
+      body(0, size);
+      return;
     }
-    std::sort(row.begin(), row.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
-    const int64_t base = inv_start[i];
-    for (size_t q = 0; q < row.size(); ++q) {
-      s.columns[base + q] = row[q].first;
-      s.values[base + q] = row[q].second;
-      if (!std::isfinite(row[q].second)) return "inverse factor overflowed float64";
+    const int32_t chunk = std::max<int32_t>(1, size / static_cast<int32_t>(8 * workers));
+    std::atomic<int32_t> next{0};
+    csr_pool->run([&](unsigned) {
+      for (int32_t lo = next.fetch_add(chunk); lo < size; lo = next.fetch_add(chunk)) body(lo, std::min(size, lo + chunk));
+    });
+  };
+  std::atomic<bool> overflow{false};
+  parallel_rows([&](int32_t lo, int32_t hi) {
+    std::vector<std::pair<int32_t, double>> row;
+    for (int32_t i = lo; i < hi; ++i) {
+      const double scale = 1.0 / std::sqrt(diagonal[i]);
+      row.clear();
+      for (int64_t q = inv_start[i]; q < inv_start[i + 1]; ++q) {
+        row.emplace_back(permutation[inv_columns[q]], inv_values[q] * scale);
+      }
+      std::sort(row.begin(), row.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+      const int64_t base = inv_start[i];
+      for (size_t q = 0; q < row.size(); ++q) {
+        s.columns[base + q] = row[q].first;
+        s.values[base + q] = row[q].second;
+        if (!std::isfinite(row[q].second)) overflow = true;
+      }
     }
-    s.offsets[i + 1] = static_cast<int32_t>(inv_start[i + 1]);
-  }
+  });
+  if (overflow) return "inverse factor overflowed float64";
+  std::vector<int32_t>().swap(inv_columns);
+  std::vector<double>().swap(inv_values);
   // --- CSR of S^T -----------------------------------------------------------
+  // Within a column, entries keep ascending row order: each worker counts the
+  // columns of a contiguous range of rows, and the ranges' cursors start
+  // where the previous ranges' entries end.
   Csr& st = out->st;
   st.offsets.assign(size + 1, 0);
   st.columns.resize(nnz);
   st.values.resize(nnz);
-  for (int64_t q = 0; q < nnz; ++q) st.offsets[s.columns[q] + 1] += 1;
-  for (int32_t i = 0; i < size; ++i) st.offsets[i + 1] += st.offsets[i];
-  {
-    std::vector<int32_t> cursor(st.offsets.begin(), st.offsets.end() - 1);
-    for (int32_t r = 0; r < size; ++r) {
-      for (int32_t q = s.offsets[r]; q < s.offsets[r + 1]; ++q) {
+  const int32_t ranges = csr_pool ? static_cast<int32_t>(workers) : 1;
+  std::vector<std::vector<int32_t>> counts(ranges, std::vector<int32_t>(size, 0));
+  auto range_rows = [&](int32_t r, int32_t& lo, int32_t& hi) {
+    lo = static_cast<int32_t>(static_cast<int64_t>(size) * r / ranges);
+    hi = static_cast<int32_t>(static_cast<int64_t>(size) * (r + 1) / ranges);
+  };
+  auto each_range = [&](const std::function<void(int32_t)>& body) {
+    if (!csr_pool) {
+      body(0);
+      return;
+    }
+    csr_pool->run([&](unsigned w) { body(static_cast<int32_t>(w)); });
+  };
+  each_range([&](int32_t r) {
+    int32_t lo, hi;
+    range_rows(r, lo, hi);
+    std::vector<int32_t>& count = counts[r];
+    for (int64_t q = s.offsets[lo]; q < s.offsets[hi]; ++q) count[s.columns[q]] += 1;
+  });
+  for (int32_t c = 0; c < size; ++c) {
+    int32_t total = 0;
+    for (int32_t r = 0; r < ranges; ++r) total += counts[r][c];
+    st.offsets[c + 1] = st.offsets[c] + total;
+  }
+  for (int32_t c = 0; c < size; ++c) {
+    int32_t cursor = st.offsets[c];
+    for (int32_t r = 0; r < ranges; ++r) {
+      const int32_t count = counts[r][c];
+      counts[r][c] = cursor;
+      cursor += count;
+    }
+  }
+  each_range([&](int32_t r) {
+    int32_t lo, hi;
+    range_rows(r, lo, hi);
+    std::vector<int32_t>& cursor = counts[r];
+    for (int32_t row = lo; row < hi; ++row) {
+      for (int32_t q = s.offsets[row]; q < s.offsets[row + 1]; ++q) {
         const int32_t at = cursor[s.columns[q]]++;
-        st.columns[at] = r;
+        st.columns[at] = row;
         st.values[at] = s.values[q];
       }
     }
-  }
+  });
   return std::string();
 }
 

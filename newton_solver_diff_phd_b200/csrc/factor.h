@@ -12,6 +12,7 @@
 
 #include <atomic>
 #include <cstdint>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -37,10 +38,39 @@ struct InverseFactor {
 // inverse is split over host threads; the result is bit-identical either way.
 extern std::atomic<int64_t> g_parallel_row_work;
 
+// The rows of the unit lower factor L in elimination order after the numeric
+// LDL^T: row i holds its columns k < i in ascending order with the
+// multipliers L(i, k), then its diagonal entry (position row_start[i+1] - 1,
+// not used by the inverse rows).
+struct LowerFactorView {
+  int32_t size = 0;
+  const int64_t* row_start = nullptr;  // [size + 1]
+  const int32_t* pattern = nullptr;
+  const double* values = nullptr;
+};
+
+// Unscaled rows of L^{-1} in elimination order, columns ascending, entries
+// that are exactly zero omitted (sparse.py:159-177).
+struct InverseRows {
+  std::vector<int64_t> start;  // [size + 1]
+  std::vector<int32_t> columns;
+  std::vector<double> values;
+};
+
+// Computes the inverse rows somewhere else (the device); returns an empty
+// string on success. Must produce exactly the rows of the host walk.
+using InverseRowsProvider = std::function<std::string(const LowerFactorView&, InverseRows*)>;
+
+// The inverse rows on the current CUDA device, level by level of the
+// elimination tree (pd_factor_device.cu); bit-identical to the host walk.
+std::string device_inverse_rows(const LowerFactorView& factor, InverseRows* out);
+
 // Validates rows (finite, positive diagonal, exact symmetry) and builds the
-// factor. Returns an empty string on success, otherwise the reason.
+// factor. Returns an empty string on success, otherwise the reason. With a
+// provider, the inverse rows come from it instead of the host walk.
 std::string build_inverse_factor(int32_t size, const int32_t* row_offsets, const int32_t* row_columns,
-                                 const double* row_values, InverseFactor* out);
+                                 const double* row_values, InverseFactor* out,
+                                 const InverseRowsProvider& provider = InverseRowsProvider());
 
 // Nested-dissection order of an undirected graph given as sorted adjacency
 // lists without self loops (the reference _nested_dissection).

@@ -1656,8 +1656,12 @@ extern "C" int pd_batch_read(PdBatch* batch, int32_t* status, int32_t* iteration
   PD_CUDA(cudaSetDevice(batch->device));
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (status) {
-    for (int i = 0; i < batch->count; ++i)
+    // Read and clear, like pd_read_status: the bits of the next read start
+    // from this one.
+    for (int i = 0; i < batch->count; ++i) {
       PD_CUDA(cudaMemcpyAsync(status + i, batch->solvers[i]->d_status.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
+      PD_CUDA(cudaMemsetAsync(batch->solvers[i]->d_status.ptr, 0, sizeof(int), st));
+    }
   }
   if (iterations && batch->d_log.ptr != nullptr && batch->key.steps > 0) {
     PD_CUDA(cudaMemcpyAsync(iterations, batch->d_log.ptr, static_cast<size_t>(batch->key.steps) * batch->count * sizeof(int),

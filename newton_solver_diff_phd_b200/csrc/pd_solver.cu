@@ -662,8 +662,15 @@ int pd_build(PdSolver* s, double dt) {
     if (s->free_[i]) add(i, i, s->plane_stiffness[p]);
   }
   InverseFactor factor;
+  pdb200::InverseRowsProvider provider;
+  if (s->factor_device) {
+    PD_CUDA(cudaSetDevice(s->device));
+    provider = [](const pdb200::LowerFactorView& lower, pdb200::InverseRows* rows) {
+      return pdb200::device_inverse_rows(lower, rows);
+    };
+  }
   const std::string error =
-      pdb200::build_inverse_factor(s->n, row_offsets.data(), row_columns.data(), row_values.data(), &factor);
+      pdb200::build_inverse_factor(s->n, row_offsets.data(), row_columns.data(), row_values.data(), &factor, provider);
   if (!error.empty()) return fail(error.find("positive definite") != std::string::npos ? PD_ERR_NOT_SPD : PD_ERR_INVALID, error);
   s->factor = std::move(factor);
   // Grid size: all SMs for large factors, fewer blocks for small meshes.
@@ -1008,6 +1015,13 @@ int pd_backward_contact(PdSolver* s, const double* x_record, const float* activa
   return PD_OK;
 }
 
+int pd_set_factor_device(PdSolver* s, int32_t enabled) {
+  if (s == nullptr) return fail(PD_ERR_INVALID, "null solver");
+  if (enabled != 0 && enabled != 1) return fail(PD_ERR_INVALID, "enabled must be 0 or 1");
+  s->factor_device = enabled;
+  return PD_OK;
+}
+
 int pd_set_spin_limit(PdSolver* s, uint32_t polls) {
   if (s == nullptr) return fail(PD_ERR_INVALID, "null solver");
   s->spin_limit = polls;
@@ -1130,10 +1144,28 @@ int pd_inverse_parallel_work(int64_t work) {
 
 int pd_inverse_build(int32_t size, const int32_t* row_offsets, const int32_t* columns, const double* values,
                      PdInverseFactor** out) {
+  return pd_inverse_build_on(-1, size, row_offsets, columns, values, out);
+}
+
+int pd_inverse_build_on(int32_t device, int32_t size, const int32_t* row_offsets, const int32_t* columns,
+                        const double* values, PdInverseFactor** out) {
   if (out == nullptr || row_offsets == nullptr || (size > 0 && (columns == nullptr || values == nullptr)))
     return fail(PD_ERR_INVALID, "null argument");
+  pdb200::InverseRowsProvider provider;
+  int previous = -1;
+  if (device >= 0) {
+    int count = 0;
+    PD_CUDA(cudaGetDeviceCount(&count));
+    if (device >= count) return fail(PD_ERR_INVALID, "no such CUDA device");
+    PD_CUDA(cudaGetDevice(&previous));
+    PD_CUDA(cudaSetDevice(device));
+    provider = [](const pdb200::LowerFactorView& lower, pdb200::InverseRows* rows) {
+      return pdb200::device_inverse_rows(lower, rows);
+    };
+  }
   auto result = new PdInverseFactor();
-  const std::string error = pdb200::build_inverse_factor(size, row_offsets, columns, values, &result->factor);
+  const std::string error = pdb200::build_inverse_factor(size, row_offsets, columns, values, &result->factor, provider);
+  if (previous >= 0) cudaSetDevice(previous);
   if (!error.empty()) {
     delete result;
     *out = nullptr;

@@ -170,6 +170,7 @@ struct PdSolver {
   int w_rows = 0;
   bool woodbury_lanes = true;  // columns side by side on lanes (false: one launch per column)
   unsigned spin_limit = 0;     // poll budget of the step and backward barriers (0: the built-in budget)
+  int factor_device = 0;       // 1: the inverse rows of the factor build run on the device
   // DiffPD forward (pd_diffpd.cu): vectors, L-BFGS history for dp_history
   // pairs, element energies, packed state forces and counters.
   DeviceBuffer dp_vectors, dp_hist, dp_energy, dp_kinds, dp_params, dp_counters;

@@ -575,6 +575,11 @@ class SolverDiffPhD:
         _lib.check(self._lib.pd_set_tolerances(self._handle, int(limit), float(absolute), float(rel)))
         self.rel_tol, self.abs_tol, self.max_iterations = float(rel), float(absolute), int(limit)
 
+    def set_factor_device(self, enabled: bool = True) -> None:
+        """Compute the rows of L^{-1} of later factor builds on the solver's device instead of the
+        host threads (added); the factor is bit-identical either way."""
+        _lib.check(self._lib.pd_set_factor_device(self._handle, 1 if enabled else 0))
+
     def notify_model_changed(self, flags: int = 0) -> None:
         """Rebuild the material weights and inverse factor before the next step."""
         if torch.cuda.is_current_stream_capturing():
