@@ -340,6 +340,8 @@ def run_b200(args):
             result["cantilever"] = run_cantilever(args, device)
         if world == 1:
             result["factor_build"] = run_factor_build(device)
+            if args.factor_twist:
+                result["factor_build_twist"] = run_factor_build(device, twist=True)
     distributed.barrier(ranks)
     distributed.teardown(ranks)
     if rank == 0:
@@ -1009,20 +1011,32 @@ def run_cantilever(args, device):
     return out
 
 
-def run_factor_build(device):
-    """The exact inverse factor of the largest family instance's PD matrix (Hex8 40x10x10 cells,
-    4,961 rows), built on the host threads and with the rows of L^{-1} on the device: wall time
-    of each build and whether every array is bit-identical."""
+def run_factor_build(device, twist=False):
+    """The exact inverse factor built on the host and with the numeric LDL^T and the rows of
+    L^{-1} on the device: wall time of each build and whether every array is bit-identical. The
+    matrix is the largest family instance's (Hex8 40x10x10 cells, 4,961 rows), or with `twist`
+    the twist-release workload's (80x20x20 cells, 35,721 rows; the host build takes about a
+    minute)."""
     import scipy.sparse as sp
 
     from newton_solver_diff_phd_b200 import _lib, meshes
+    from newton_solver_diff_phd_b200.scenes import Twist
     from oracle import pd_oracle
 
-    vertices, hexes, _ = meshes.hex_grid(40, 10, 10, 0.01)
+    if twist:
+        spec = Twist()
+        vertices, hexes, cells = meshes.hex_grid(spec.nx, spec.ny, spec.nz, spec.edge)
+        slab = np.asarray(cells)
+        third = spec.nx // 3
+        young = spec.young * np.where((slab > third) & (slab <= 2 * third), spec.stiff_ratio, 1.0)
+        poisson, density, dt, name = spec.poisson, spec.density, spec.dt, "Hex8 twist release 80x20x20 cells, 35,721 rows"
+    else:
+        vertices, hexes, _ = meshes.hex_grid(40, 10, 10, 0.01)
+        young = np.exp(np.random.default_rng(3).uniform(np.log(1.0e5), np.log(1.0e7), len(hexes)))
+        poisson, density, dt, name = 0.45, 1000.0, BATCH_DT, "Hex8 cantilever 40x10x10 cells, 4,961 rows"
     free = vertices[:, 0] > 1.0e-12
-    young = np.exp(np.random.default_rng(3).uniform(np.log(1.0e5), np.log(1.0e7), len(hexes)))
-    mu, lam = meshes.lame_from_young(young, 0.45)
-    matrix = sp.csr_matrix(pd_oracle.Body.hex(vertices, hexes, free, mu, lam, 1000.0).matrix(BATCH_DT))
+    mu, lam = meshes.lame_from_young(young, poisson)
+    matrix = sp.csr_matrix(pd_oracle.Body.hex(vertices, hexes, free, mu, lam, density).matrix(dt))
     matrix.sort_indices()
     csr = (matrix.indptr, matrix.indices, matrix.data)
     _lib.inverse_factor(csr, device=device.index or 0)  # context and module load, untimed
@@ -1033,19 +1047,19 @@ def run_factor_build(device):
     on_device = _lib.inverse_factor(csr, device=device.index or 0)
     device_s = time.perf_counter() - start
     same = all(np.array_equal(host[k], on_device[k]) for k in host)
-    return {"matrix": "Hex8 cantilever 40x10x10 cells, 4,961 rows", "nnz_S": int(len(host["s_values"])),
-            "host_threads_s": host_s, "device_rows_s": device_s, "bit_identical": bool(same),
-            "host_threads": os.cpu_count(),
-            "note": "ordering, symbolic fill, numeric LDL^T and the CSR assembly run on the host in both builds"}
+    return {"matrix": name, "nnz_S": int(len(host["s_values"])), "host_s": host_s, "device_s": device_s,
+            "bit_identical": bool(same), "host_threads": os.cpu_count(),
+            "note": "device build: numeric LDL^T and rows of L^{-1} on the GPU; ordering, symbolic fill and the "
+                    "CSR assembly on the host threads in both builds"}
 
 
 def run_twist(args, device):
     """The large Hex8 twist-release workload (80x20x20 cells, 35,721 particles): `twist_steps` steps
     of dt 1e-3 at rel 1e-6 forward, then the adjoint of the final tip rotation angle w.r.t. the
     initial positions and every cell's Young's modulus with a checkpoint every 10 steps (exact
-    adjoint), in fp64 and in fp32+refine; the factor build is timed apart, on the host threads for
-    the fp64 solver and with the rows of L^{-1} on the device for the fp32+refine solver (the two
-    factors are bit-identical; tests/test_gpu_factor_device.py)."""
+    adjoint), in fp64 and in fp32+refine; the factor build is timed apart, on the host for the
+    fp64 solver and with the numeric LDL^T and the rows of L^{-1} on the device for the fp32+refine
+    solver (the two factors are bit-identical; tests/test_gpu_factor_device.py)."""
     import torch
 
     from newton_solver_diff_phd_b200 import SolverDiffPhD
@@ -1090,7 +1104,7 @@ def run_twist(args, device):
         _, nnz_s, _ = solver.factor_stats()
         grad_e = (gm[:, 0] * dmu_de + gm[:, 1] * dlam_de).cpu().numpy()
         results[precision] = (final.particle_q.double().cpu().numpy(), grad_e, float(angle.detach()))
-        out[precision] = {"factor_build_s": build_s, "factor_rows_of_inverse_on": "host threads" if precision == "fp64"
+        out[precision] = {"factor_build_s": build_s, "factor_ldlt_and_inverse_rows_on": "host" if precision == "fp64"
                           else "device", "nnz_S": int(nnz_s), "forward_ms": e0.elapsed_time(e1),
                           "adjoint_ms": e1.elapsed_time(e2),
                           "fwd_adjoint_steps_per_s": steps / (e0.elapsed_time(e2) / 1000.0),
@@ -1275,6 +1289,8 @@ def main():
     parser.add_argument("--twist", action="store_true",
                         help="add the 35,721-particle Hex8 twist-release leg (minutes: its host factor build)")
     parser.add_argument("--twist-steps", type=int, default=100, help="steps of the twist-release leg")
+    parser.add_argument("--factor-twist", action="store_true",
+                        help="also time the twist-release matrix's factor build on the host and the device")
     parser.add_argument("--no-extras", action="store_true",
                         help="skip the e2e, CPU-baseline and per-launch timing legs (profiling runs)")
     parser.add_argument("--profile-batch", default=None,

@@ -188,9 +188,10 @@ int pd_frictional_state(PdSolver* solver, double* multiplier, double* omega, dou
    the exact inverse factor A^{-1} = S^T S on the host (sparse.py:291-320),
    then uploads it. Synchronous; not capturable. */
 int pd_build(PdSolver* solver, double dt);
-/* Where pd_build computes the rows of L^{-1}: 1 on the solver's device (see
-   pd_inverse_build_on), 0 on the host threads (default). Bit-identical either
-   way; takes effect at the next build. Added (no reference counterpart). */
+/* Where pd_build runs the numeric LDL^T and the rows of L^{-1}: 1 on the
+   solver's device (see pd_inverse_build_on), 0 on the host (default).
+   Bit-identical either way; takes effect at the next build. Added (no
+   reference counterpart). */
 int pd_set_factor_device(PdSolver* solver, int32_t enabled);
 
 /* Factor statistics of the last build: rows, nnz(S), nnz(L) incl. diagonal. */
@@ -440,10 +441,13 @@ typedef struct PdInverseFactor PdInverseFactor;
 int pd_inverse_parallel_work(int64_t work);
 int pd_inverse_build(int32_t size, const int32_t* row_offsets, const int32_t* columns, const double* values,
                      PdInverseFactor** out);
-/* pd_inverse_build with the rows of L^{-1} (sparse.py:159-177, the dominant
-   part of the build) computed on CUDA device `device`, level by level of the
-   elimination tree; the factor is bit-identical to the host build. device < 0
-   builds on the host. Added: the reference builds on the host only. */
+/* pd_inverse_build with the numeric LDL^T (sparse.py:136-151) and the rows of
+   L^{-1} (sparse.py:159-177), the two costly stages, computed on CUDA device
+   `device`, level by level of the elimination tree; ordering, symbolic fill
+   and the CSR assembly stay on the host. The factor is bit-identical to the
+   host build (rows of L longer than the device stages take run on the
+   host). device < 0 builds on the host. Added: the reference builds on the
+   host only. */
 int pd_inverse_build_on(int32_t device, int32_t size, const int32_t* row_offsets, const int32_t* columns,
                         const double* values, PdInverseFactor** out);
 int pd_inverse_sizes(const PdInverseFactor* factor, int32_t* size, int64_t* nnz, int64_t* factorization_nnz);

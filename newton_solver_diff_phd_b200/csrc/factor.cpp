@@ -265,7 +265,8 @@ std::vector<int32_t> nested_dissection(const Adjacency& adjacency) {
 }
 
 std::string build_inverse_factor(int32_t size, const int32_t* row_offsets, const int32_t* row_columns,
-                                 const double* row_values, InverseFactor* out, const InverseRowsProvider& provider) {
+                                 const double* row_values, InverseFactor* out, const InverseRowsProvider& provider,
+                                 const LdltProvider& ldlt_provider) {
   if (size < 0) return "matrix size must be nonnegative";
   // --- _validate_rows (sparse.py:73-95) ---------------------------------
   std::vector<std::vector<std::pair<int32_t, double>>> rows(size);
@@ -390,7 +391,32 @@ std::string build_inverse_factor(int32_t size, const int32_t* row_offsets, const
   std::vector<double> diagonal(size);
   std::vector<double> entries;
   std::vector<int64_t> locations;
-  for (int32_t k = 0; k < size; ++k) {
+  bool factored = false;
+  if (ldlt_provider) {
+    std::vector<int64_t> col_start(static_cast<size_t>(size) + 1, 0);
+    for (int32_t k = 0; k < size; ++k) col_start[k + 1] = col_start[k] + static_cast<int64_t>(columns[k].size());
+    std::vector<int32_t> col_rows(static_cast<size_t>(col_start[size]));
+    std::vector<int32_t> column_index(static_cast<size_t>(pattern_nnz), -1);
+    for (int32_t k = 0; k < size; ++k) {
+      for (size_t o = 0; o < columns[k].size(); ++o) {
+        col_rows[col_start[k] + o] = columns[k][o];
+        column_index[column_positions[k][o]] = static_cast<int32_t>(o);
+      }
+    }
+    SymbolicView view;
+    view.size = size;
+    view.row_start = row_start.data();
+    view.pattern = pattern.data();
+    view.col_start = col_start.data();
+    view.col_rows = col_rows.data();
+    view.column_index = column_index.data();
+    const std::string error = ldlt_provider(view, values.data(), diagonal.data());
+    if (error.rfind("device LDLT:", 0) != 0) {
+      if (!error.empty()) return error;
+      factored = true;
+    }
+  }
+  for (int32_t k = factored ? size : 0; k < size; ++k) {
     const double pivot = values[row_start[k + 1] - 1];
     if (!std::isfinite(pivot) || pivot <= 0.0) {
       return "matrix is not positive definite: LDLT pivot " + std::to_string(k) + " is " + std::to_string(pivot);

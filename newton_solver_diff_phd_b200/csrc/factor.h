@@ -61,6 +61,32 @@ struct InverseRows {
 // string on success. Must produce exactly the rows of the host walk.
 using InverseRowsProvider = std::function<std::string(const LowerFactorView&, InverseRows*)>;
 
+// The structure of the numeric LDL^T: the rows of L (columns k < i ascending,
+// then the diagonal) and, for every column k, the rows i > k it holds in
+// ascending order (col_start / col_rows) with, for every strict entry p of
+// the row arrays, the index of its row within its column (column_index).
+struct SymbolicView {
+  int32_t size = 0;
+  const int64_t* row_start = nullptr;  // [size + 1]
+  const int32_t* pattern = nullptr;
+  const int64_t* col_start = nullptr;  // [size + 1]
+  const int32_t* col_rows = nullptr;
+  const int32_t* column_index = nullptr;  // per row-array position; -1 at the diagonal
+};
+
+// The numeric LDL^T somewhere else: `values` holds the permuted lower
+// triangle of A at the row-array positions on entry; on success the strict
+// positions hold the multipliers L(i, k), the diagonal positions and
+// `diagonal` the pivots, exactly as the host's right-looking factorisation
+// leaves them (every entry updated by ascending pivots, one rounded multiply
+// then one rounded subtract each). Errors use the host's messages.
+using LdltProvider = std::function<std::string(const SymbolicView&, double* values, double* diagonal)>;
+
+// The numeric LDL^T on the current CUDA device, row by row within levels of
+// the elimination tree (pd_factor_device.cu). Rows longer than the shared
+// memory staging allows return an error starting with "device LDLT:".
+std::string device_ldlt(const SymbolicView& symbolic, double* values, double* diagonal);
+
 // The inverse rows on the current CUDA device, level by level of the
 // elimination tree (pd_factor_device.cu); bit-identical to the host walk.
 std::string device_inverse_rows(const LowerFactorView& factor, InverseRows* out);
@@ -70,7 +96,8 @@ std::string device_inverse_rows(const LowerFactorView& factor, InverseRows* out)
 // provider, the inverse rows come from it instead of the host walk.
 std::string build_inverse_factor(int32_t size, const int32_t* row_offsets, const int32_t* row_columns,
                                  const double* row_values, InverseFactor* out,
-                                 const InverseRowsProvider& provider = InverseRowsProvider());
+                                 const InverseRowsProvider& provider = InverseRowsProvider(),
+                                 const LdltProvider& ldlt_provider = LdltProvider());
 
 // Nested-dissection order of an undirected graph given as sorted adjacency
 // lists without self loops (the reference _nested_dissection).

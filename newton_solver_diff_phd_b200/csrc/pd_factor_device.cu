@@ -1,5 +1,6 @@
-// Rows of L^{-1} on the device: the inverse-rows stage of the factor build
-// (sparse.py:159-177), bit-identical to the host walk in factor.cpp.
+// The two costly stages of the factor build on the device, bit-identical to
+// the host's in factor.cpp: the numeric LDL^T (sparse.py:136-151; see
+// ldlt_rows_kernel) and the rows of L^{-1} (sparse.py:159-177, below).
 //
 // Row i of the unscaled inverse starts as e_i and, for every column k of row
 // i of L in ascending order (k < i, multiplier L(i, k) != 0), subtracts
@@ -166,6 +167,66 @@ __global__ void __launch_bounds__(kThreads) inverse_rows_copy_kernel(
     if (item.chunk == j0) row_off[i] = row_base;
     cb[cb_base[i] + (item.chunk - j0)] = static_cast<int32_t>(out - row_base);
     if (item.chunk == j1) cb[cb_base[i] + (j1 - j0) + 1] = static_cast<int32_t>(out + count - row_base);
+  }
+}
+
+constexpr int kLdltMaxPattern = 3072;  // strict entries of a row staged in shared memory
+
+// Row i of the numeric LDL^T, one block per row of a level. The row's entries
+// start as the permuted lower triangle of A; for every column k of the row in
+// ascending order the unscaled entry u = (i, k) is final, the multiplier is
+// u / d_k, and the block subtracts m * e(j, k) from entry (i, j) for every
+// row j of column k with k < j < i (all of them lie in row i's pattern) and
+// m * u from the diagonal, the same products and order as the host's
+// right-looking update. The unscaled entry is also stored in column k's slot
+// for the rows above i.
+__global__ void __launch_bounds__(kThreads) ldlt_rows_kernel(
+    const int32_t* __restrict__ rows, const int64_t* __restrict__ row_start, const int32_t* __restrict__ pattern,
+    const int64_t* __restrict__ col_start, const int32_t* __restrict__ col_rows,
+    const int32_t* __restrict__ column_index, double* __restrict__ values, double* __restrict__ col_values,
+    double* __restrict__ diagonal, int* __restrict__ fail_row, int* __restrict__ error) {
+  __shared__ int32_t pat[kLdltMaxPattern];
+  __shared__ double acc[kLdltMaxPattern + 1];
+  const int i = rows[blockIdx.x];
+  const int64_t start = row_start[i];
+  const int len = static_cast<int>(row_start[i + 1] - start - 1);
+  for (int t = threadIdx.x; t < len; t += blockDim.x) pat[t] = pattern[start + t];
+  for (int t = threadIdx.x; t <= len; t += blockDim.x) acc[t] = values[start + t];
+  __syncthreads();
+  for (int p = 0; p < len; ++p) {
+    const int k = pat[p];
+    const double u = acc[p];
+    const double m = u / diagonal[k];
+    const int64_t own = col_start[k] + column_index[start + p];
+    if (threadIdx.x == 0) {
+      values[start + p] = m;
+      col_values[own] = u;
+    }
+    for (int64_t q = col_start[k] + threadIdx.x; q < own; q += blockDim.x) {
+      const int j = col_rows[q];
+      int lo = p + 1, hi = len;
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (pat[mid] < j) {
+          lo = mid + 1;
+        } else {
+          hi = mid;
+        }
+      }
+      if (lo >= len || pat[lo] != j) {
+        atomicOr(error, 1);
+        continue;
+      }
+      acc[lo] = __dsub_rn(acc[lo], __dmul_rn(m, col_values[q]));
+    }
+    if (threadIdx.x == 0) acc[len] = __dsub_rn(acc[len], __dmul_rn(m, u));
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double pivot = acc[len];
+    values[start + len] = pivot;
+    diagonal[i] = pivot;
+    if (!isfinite(pivot) || pivot <= 0.0) atomicMin(fail_row, i);
   }
 }
 
@@ -391,6 +452,87 @@ std::string device_inverse_rows(const LowerFactorView& factor, InverseRows* out)
     std::copy(pool_c.begin() + row_off[i], pool_c.begin() + row_off[i] + length, out->columns.begin() + out->start[i]);
     std::copy(pool_v.begin() + row_off[i], pool_v.begin() + row_off[i] + length, out->values.begin() + out->start[i]);
   }
+  return std::string();
+}
+
+std::string device_ldlt(const SymbolicView& symbolic, double* values, double* diagonal) {
+  const int32_t n = symbolic.size;
+  if (n == 0) return std::string();
+  const int64_t nnz = symbolic.row_start[n];
+  const int64_t col_nnz = symbolic.col_start[n];
+  std::vector<int32_t> level(n, 0);
+  int32_t levels = 0;
+  for (int32_t i = 0; i < n; ++i) {
+    const int64_t strict = symbolic.row_start[i + 1] - 1 - symbolic.row_start[i];
+    if (strict > kLdltMaxPattern) {
+      return "device LDLT: a row of L has " + std::to_string(strict) + " entries (at most " +
+             std::to_string(kLdltMaxPattern) + " are staged)";
+    }
+    int32_t l = 0;
+    for (int64_t p = symbolic.row_start[i]; p < symbolic.row_start[i + 1] - 1; ++p)
+      l = std::max(l, level[symbolic.pattern[p]] + 1);
+    level[i] = l;
+    levels = std::max(levels, l + 1);
+  }
+  std::vector<int32_t> level_count(static_cast<size_t>(levels) + 1, 0);
+  for (int32_t i = 0; i < n; ++i) level_count[level[i] + 1] += 1;
+  for (int32_t l = 0; l < levels; ++l) level_count[l + 1] += level_count[l];
+  std::vector<int32_t> by_level(n);
+  {
+    std::vector<int32_t> cursor(level_count.begin(), level_count.end() - 1);
+    for (int32_t i = 0; i < n; ++i) by_level[cursor[level[i]]++] = i;
+  }
+  StreamGuard guard;
+  PD_FD_CHECK(cudaStreamCreateWithFlags(&guard.stream, cudaStreamNonBlocking), "stream");
+  cudaStream_t stream = guard.stream;
+  DeviceArray<int64_t> d_row_start, d_col_start;
+  DeviceArray<int32_t> d_pattern, d_col_rows, d_column_index, d_rows;
+  DeviceArray<double> d_values, d_col_values, d_diagonal;
+  DeviceArray<int> d_flags;
+  auto upload = [&](auto& array, const auto* host, size_t count) {
+    cudaError_t e = array.allocate(count);
+    if (e == cudaSuccess && count > 0)
+      e = cudaMemcpyAsync(array.ptr, host, count * sizeof(*host), cudaMemcpyHostToDevice, stream);
+    return e;
+  };
+  PD_FD_CHECK(upload(d_row_start, symbolic.row_start, static_cast<size_t>(n) + 1), "upload");
+  PD_FD_CHECK(upload(d_pattern, symbolic.pattern, static_cast<size_t>(nnz)), "upload");
+  PD_FD_CHECK(upload(d_col_start, symbolic.col_start, static_cast<size_t>(n) + 1), "upload");
+  PD_FD_CHECK(upload(d_col_rows, symbolic.col_rows, static_cast<size_t>(col_nnz)), "upload");
+  PD_FD_CHECK(upload(d_column_index, symbolic.column_index, static_cast<size_t>(nnz)), "upload");
+  PD_FD_CHECK(upload(d_values, values, static_cast<size_t>(nnz)), "upload");
+  PD_FD_CHECK(upload(d_rows, by_level.data(), by_level.size()), "upload");
+  PD_FD_CHECK(d_col_values.allocate(static_cast<size_t>(col_nnz)), "allocate");
+  PD_FD_CHECK(d_diagonal.allocate(n), "allocate");
+  PD_FD_CHECK(d_flags.allocate(2), "allocate");
+  const int flags_init[2] = {n, 0};  // first failing pivot (n: none), structure error
+  PD_FD_CHECK(cudaMemcpyAsync(d_flags.ptr, flags_init, sizeof(flags_init), cudaMemcpyHostToDevice, stream), "upload");
+  // Levels in order on one stream: a level's rows read only rows of lower levels.
+  for (int32_t l = 0; l < levels; ++l) {
+    const int32_t count = level_count[l + 1] - level_count[l];
+    ldlt_rows_kernel<<<count, kThreads, 0, stream>>>(d_rows.ptr + level_count[l], d_row_start.ptr, d_pattern.ptr,
+                                                      d_col_start.ptr, d_col_rows.ptr, d_column_index.ptr,
+                                                      d_values.ptr, d_col_values.ptr, d_diagonal.ptr, d_flags.ptr,
+                                                      d_flags.ptr + 1);
+    PD_FD_CHECK(cudaGetLastError(), "launch");
+  }
+  int flags[2] = {0, 0};
+  std::vector<double> out_values(static_cast<size_t>(nnz)), out_diagonal(n);
+  PD_FD_CHECK(cudaMemcpyAsync(flags, d_flags.ptr, sizeof(flags), cudaMemcpyDeviceToHost, stream), "read back");
+  PD_FD_CHECK(cudaMemcpyAsync(out_values.data(), d_values.ptr, out_values.size() * sizeof(double),
+                              cudaMemcpyDeviceToHost, stream),
+              "read back");
+  PD_FD_CHECK(cudaMemcpyAsync(out_diagonal.data(), d_diagonal.ptr, out_diagonal.size() * sizeof(double),
+                              cudaMemcpyDeviceToHost, stream),
+              "read back");
+  PD_FD_CHECK(cudaStreamSynchronize(stream), "read back");
+  if (flags[1] != 0) return "device LDLT: a column entry fell outside its row pattern";
+  if (flags[0] < n) {
+    return "matrix is not positive definite: LDLT pivot " + std::to_string(flags[0]) + " is " +
+           std::to_string(out_diagonal[flags[0]]);
+  }
+  std::copy(out_values.begin(), out_values.end(), values);
+  std::copy(out_diagonal.begin(), out_diagonal.end(), diagonal);
   return std::string();
 }
 

@@ -663,14 +663,18 @@ int pd_build(PdSolver* s, double dt) {
   }
   InverseFactor factor;
   pdb200::InverseRowsProvider provider;
+  pdb200::LdltProvider ldlt_provider;
   if (s->factor_device) {
     PD_CUDA(cudaSetDevice(s->device));
     provider = [](const pdb200::LowerFactorView& lower, pdb200::InverseRows* rows) {
       return pdb200::device_inverse_rows(lower, rows);
     };
+    ldlt_provider = [](const pdb200::SymbolicView& symbolic, double* values, double* diagonal) {
+      return pdb200::device_ldlt(symbolic, values, diagonal);
+    };
   }
-  const std::string error =
-      pdb200::build_inverse_factor(s->n, row_offsets.data(), row_columns.data(), row_values.data(), &factor, provider);
+  const std::string error = pdb200::build_inverse_factor(s->n, row_offsets.data(), row_columns.data(),
+                                                         row_values.data(), &factor, provider, ldlt_provider);
   if (!error.empty()) return fail(error.find("positive definite") != std::string::npos ? PD_ERR_NOT_SPD : PD_ERR_INVALID, error);
   s->factor = std::move(factor);
   // Grid size: all SMs for large factors, fewer blocks for small meshes.
@@ -1152,6 +1156,7 @@ int pd_inverse_build_on(int32_t device, int32_t size, const int32_t* row_offsets
   if (out == nullptr || row_offsets == nullptr || (size > 0 && (columns == nullptr || values == nullptr)))
     return fail(PD_ERR_INVALID, "null argument");
   pdb200::InverseRowsProvider provider;
+  pdb200::LdltProvider ldlt_provider;
   int previous = -1;
   if (device >= 0) {
     int count = 0;
@@ -1162,9 +1167,13 @@ int pd_inverse_build_on(int32_t device, int32_t size, const int32_t* row_offsets
     provider = [](const pdb200::LowerFactorView& lower, pdb200::InverseRows* rows) {
       return pdb200::device_inverse_rows(lower, rows);
     };
+    ldlt_provider = [](const pdb200::SymbolicView& symbolic, double* values, double* diagonal) {
+      return pdb200::device_ldlt(symbolic, values, diagonal);
+    };
   }
   auto result = new PdInverseFactor();
-  const std::string error = pdb200::build_inverse_factor(size, row_offsets, columns, values, &result->factor, provider);
+  const std::string error =
+      pdb200::build_inverse_factor(size, row_offsets, columns, values, &result->factor, provider, ldlt_provider);
   if (previous >= 0) cudaSetDevice(previous);
   if (!error.empty()) {
     delete result;

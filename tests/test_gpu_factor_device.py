@@ -1,5 +1,6 @@
-"""The factor build with the rows of L^{-1} computed on the device (pd_inverse_build_on,
-SolverDiffPhD.set_factor_device) against the host build: every array bit-identical.
+"""The factor build with the numeric LDL^T and the rows of L^{-1} computed on the device
+(pd_inverse_build_on, SolverDiffPhD.set_factor_device) against the host build: every array
+bit-identical, and the same error for a matrix that is not positive definite.
 
 The host build is itself bit-identical to the reference's sparse.py setup
 (tests/test_factor.py); the device build must therefore reproduce it exactly,
@@ -40,6 +41,16 @@ def test_golden_matrices(name):
 def test_exact_cancellation_and_identity_rows():
     matrix = np.asarray(((2.0, 2.0, 2.0, 0.0), (2.0, 5.0, 5.0, 0.0), (2.0, 5.0, 10.0, 0.0), (0.0, 0.0, 0.0, 1.0)))
     assert_same(_lib.dense_to_csr(matrix))
+
+
+def test_indefinite_matrix_fails_like_the_host():
+    matrix = np.asarray(((4.0, 1.0, 0.0), (1.0, 3.0, 5.0), (0.0, 5.0, 2.0)))
+    messages = []
+    for device in (None, torch.cuda.current_device()):
+        with pytest.raises(ValueError) as info:
+            _lib.inverse_factor(_lib.dense_to_csr(matrix), device=device)
+        messages.append(str(info.value))
+    assert "positive definite" in messages[0] and messages[0] == messages[1]
 
 
 def _csr(matrix):
