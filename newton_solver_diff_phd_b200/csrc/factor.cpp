@@ -396,10 +396,12 @@ std::string build_inverse_factor(int32_t size, const int32_t* row_offsets, const
     std::vector<int64_t> col_start(static_cast<size_t>(size) + 1, 0);
     for (int32_t k = 0; k < size; ++k) col_start[k + 1] = col_start[k] + static_cast<int64_t>(columns[k].size());
     std::vector<int32_t> col_rows(static_cast<size_t>(col_start[size]));
+    std::vector<int64_t> col_pos(static_cast<size_t>(col_start[size]));
     std::vector<int32_t> column_index(static_cast<size_t>(pattern_nnz), -1);
     for (int32_t k = 0; k < size; ++k) {
       for (size_t o = 0; o < columns[k].size(); ++o) {
         col_rows[col_start[k] + o] = columns[k][o];
+        col_pos[col_start[k] + o] = column_positions[k][o];
         column_index[column_positions[k][o]] = static_cast<int32_t>(o);
       }
     }
@@ -410,6 +412,7 @@ std::string build_inverse_factor(int32_t size, const int32_t* row_offsets, const
     view.col_start = col_start.data();
     view.col_rows = col_rows.data();
     view.column_index = column_index.data();
+    view.col_pos = col_pos.data();
     const std::string error = ldlt_provider(view, values.data(), diagonal.data());
     if (error.rfind("device LDLT:", 0) != 0) {
       if (!error.empty()) return error;

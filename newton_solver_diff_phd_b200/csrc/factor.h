@@ -72,6 +72,7 @@ struct SymbolicView {
   const int64_t* col_start = nullptr;  // [size + 1]
   const int32_t* col_rows = nullptr;
   const int32_t* column_index = nullptr;  // per row-array position; -1 at the diagonal
+  const int64_t* col_pos = nullptr;       // per column entry: its position in the row arrays
 };
 
 // The numeric LDL^T somewhere else: `values` holds the permuted lower
@@ -82,9 +83,9 @@ struct SymbolicView {
 // then one rounded subtract each). Errors use the host's messages.
 using LdltProvider = std::function<std::string(const SymbolicView&, double* values, double* diagonal)>;
 
-// The numeric LDL^T on the current CUDA device, row by row within levels of
-// the elimination tree (pd_factor_device.cu). Rows longer than the shared
-// memory staging allows return an error starting with "device LDLT:".
+// The numeric LDL^T on the current CUDA device, column by column within
+// levels of the elimination tree (pd_factor_device.cu). Rows longer than the
+// shared memory staging allows return an error starting with "device LDLT:".
 std::string device_ldlt(const SymbolicView& symbolic, double* values, double* diagonal);
 
 // The inverse rows on the current CUDA device, level by level of the

@@ -28,11 +28,27 @@
 
 #include "factor.h"
 
+// Stage timings on stderr in builds with -DPD_FACTOR_TIMING (the timing probe).
+#ifdef PD_FACTOR_TIMING
+#include <chrono>
+#include <cstdio>
+#define PD_FT_NOW() std::chrono::steady_clock::now()
+#define PD_FT_REPORT(name, t0, extra)                                                                          \
+  std::fprintf(stderr, "[factor] %s %.3f s %s\n", name,                                                      \
+               std::chrono::duration<double>(std::chrono::steady_clock::now() - (t0)).count(), (extra).c_str())
+#else
+#define PD_FT_NOW() 0
+#define PD_FT_REPORT(name, t0, extra) (void)(t0)
+#endif
+
 namespace pdb200 {
 
 namespace {
 
-constexpr int kChunk = 4096;   // labels per chunk: a 32 KB accumulator per block
+#ifndef PD_FACTOR_CHUNK
+#define PD_FACTOR_CHUNK 256
+#endif
+constexpr int kChunk = PD_FACTOR_CHUNK;  // labels per chunk (256: a 2 KB accumulator per block)
 constexpr int kThreads = 256;
 constexpr int kMetaBatch = 32;  // columns of row i whose metadata one warp loads at once
 
@@ -170,64 +186,87 @@ __global__ void __launch_bounds__(kThreads) inverse_rows_copy_kernel(
   }
 }
 
-constexpr int kLdltMaxPattern = 3072;  // strict entries of a row staged in shared memory
+constexpr int kLdltMaxPattern = 16384;  // strict entries of a row staged in (dynamic) shared memory
 
-// Row i of the numeric LDL^T, one block per row of a level. The row's entries
-// start as the permuted lower triangle of A; for every column k of the row in
-// ascending order the unscaled entry u = (i, k) is final, the multiplier is
-// u / d_k, and the block subtracts m * e(j, k) from entry (i, j) for every
-// row j of column k with k < j < i (all of them lie in row i's pattern) and
-// m * u from the diagonal, the same products and order as the host's
-// right-looking update. The unscaled entry is also stored in column k's slot
-// for the rows above i.
-__global__ void __launch_bounds__(kThreads) ldlt_rows_kernel(
-    const int32_t* __restrict__ rows, const int64_t* __restrict__ row_start, const int32_t* __restrict__ pattern,
-    const int64_t* __restrict__ col_start, const int32_t* __restrict__ col_rows,
-    const int32_t* __restrict__ column_index, double* __restrict__ values, double* __restrict__ col_values,
-    double* __restrict__ diagonal, int* __restrict__ fail_row, int* __restrict__ error) {
-  __shared__ int32_t pat[kLdltMaxPattern];
-  __shared__ double acc[kLdltMaxPattern + 1];
-  const int i = rows[blockIdx.x];
-  const int64_t start = row_start[i];
-  const int len = static_cast<int>(row_start[i + 1] - start - 1);
-  for (int t = threadIdx.x; t < len; t += blockDim.x) pat[t] = pattern[start + t];
-  for (int t = threadIdx.x; t <= len; t += blockDim.x) acc[t] = values[start + t];
+// Up to kThreads entries of one column j of L: entry 0 is the diagonal (row
+// j), entry e >= 1 is row col_rows[col_start[j] + e - 1].
+struct ColumnItem {
+  int32_t column;
+  int32_t first;
+};
+
+// Left-looking columns: every entry (i, j) of a column is the permuted A value
+// minus m(i, k) e(j, k) over the columns k < j that rows i and j share, in
+// ascending k, which is the sequence of rounded products and subtractions the
+// host's right-looking update applies to it (pivot k updates (i, j) exactly
+// when both rows hold column k). One thread per entry, merging row i's pattern
+// with row j's, staged in shared memory with row j's unscaled entries; all the
+// multipliers and unscaled entries read belong to columns of lower levels.
+// The entries are stored unscaled; the diagonal entry is the pivot.
+__global__ void __launch_bounds__(kThreads) ldlt_columns_kernel(
+    const ColumnItem* __restrict__ items, const int64_t* __restrict__ row_start, const int32_t* __restrict__ pattern,
+    const int64_t* __restrict__ col_start, const int32_t* __restrict__ col_rows, const int64_t* __restrict__ col_pos,
+    const double* __restrict__ initial, const double* __restrict__ multipliers, double* __restrict__ unscaled,
+    double* __restrict__ diagonal, int* __restrict__ fail_row) {
+  extern __shared__ __align__(16) unsigned char ldlt_smem[];
+  const ColumnItem item = items[blockIdx.x];
+  const int j = item.column;
+  const int64_t start_j = row_start[j];
+  const int len_j = static_cast<int>(row_start[j + 1] - start_j - 1);
+  double* e_j = reinterpret_cast<double*>(ldlt_smem);
+  int32_t* pat_j = reinterpret_cast<int32_t*>(e_j + len_j);
+  for (int t = threadIdx.x; t < len_j; t += blockDim.x) {
+    pat_j[t] = pattern[start_j + t];
+    e_j[t] = unscaled[start_j + t];
+  }
   __syncthreads();
-  for (int p = 0; p < len; ++p) {
-    const int k = pat[p];
-    const double u = acc[p];
-    const double m = u / diagonal[k];
-    const int64_t own = col_start[k] + column_index[start + p];
-    if (threadIdx.x == 0) {
-      values[start + p] = m;
-      col_values[own] = u;
-    }
-    for (int64_t q = col_start[k] + threadIdx.x; q < own; q += blockDim.x) {
-      const int j = col_rows[q];
-      int lo = p + 1, hi = len;
-      while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (pat[mid] < j) {
-          lo = mid + 1;
-        } else {
-          hi = mid;
-        }
-      }
-      if (lo >= len || pat[lo] != j) {
-        atomicOr(error, 1);
-        continue;
-      }
-      acc[lo] = __dsub_rn(acc[lo], __dmul_rn(m, col_values[q]));
-    }
-    if (threadIdx.x == 0) acc[len] = __dsub_rn(acc[len], __dmul_rn(m, u));
-    __syncthreads();
+  const int count = static_cast<int>(col_start[j + 1] - col_start[j]) + 1;
+  const int e = item.first + static_cast<int>(threadIdx.x);
+  if (e >= count) return;
+  if (e == 0) {
+    const int64_t pos = start_j + len_j;
+    double acc = initial[pos];
+    for (int q = 0; q < len_j; ++q) acc = __dsub_rn(acc, __dmul_rn(multipliers[start_j + q], e_j[q]));
+    unscaled[pos] = acc;
+    diagonal[j] = acc;
+    if (!isfinite(acc) || acc <= 0.0) atomicMin(fail_row, j);
+    return;
   }
-  if (threadIdx.x == 0) {
-    const double pivot = acc[len];
-    values[start + len] = pivot;
-    diagonal[i] = pivot;
-    if (!isfinite(pivot) || pivot <= 0.0) atomicMin(fail_row, i);
+  const int i = col_rows[col_start[j] + e - 1];
+  const int64_t pos = col_pos[col_start[j] + e - 1];  // entry (i, j): row i's columns before it are < j
+  double acc = initial[pos];
+  int64_t p = row_start[i];
+  int q = 0;
+  while (p < pos && q < len_j) {
+    const int a = pattern[p];
+    const int b = pat_j[q];
+    if (a < b) {
+      ++p;
+    } else if (b < a) {
+      ++q;
+    } else {
+      acc = __dsub_rn(acc, __dmul_rn(multipliers[p], e_j[q]));
+      ++p;
+      ++q;
+    }
   }
+  unscaled[pos] = acc;
+}
+
+// Multipliers of a level's columns: m(i, j) = e(i, j) / d_j (IEEE division).
+__global__ void __launch_bounds__(kThreads) ldlt_divide_kernel(const ColumnItem* __restrict__ items,
+                                                               const int64_t* __restrict__ col_start,
+                                                               const int64_t* __restrict__ col_pos,
+                                                               const double* __restrict__ unscaled,
+                                                               const double* __restrict__ diagonal,
+                                                               double* __restrict__ multipliers) {
+  const ColumnItem item = items[blockIdx.x];
+  const int j = item.column;
+  const int count = static_cast<int>(col_start[j + 1] - col_start[j]) + 1;
+  const int e = item.first + static_cast<int>(threadIdx.x);
+  if (e == 0 || e >= count) return;
+  const int64_t pos = col_pos[col_start[j] + e - 1];
+  multipliers[pos] = unscaled[pos] / diagonal[j];
 }
 
 // Device allocation released on scope exit.
@@ -274,6 +313,7 @@ std::string cuda_error(const char* what, cudaError_t e) {
 }  // namespace
 
 std::string device_inverse_rows(const LowerFactorView& factor, InverseRows* out) {
+  const auto timer = PD_FT_NOW();
   const int32_t n = factor.size;
   out->start.assign(static_cast<size_t>(n) + 1, 0);
   out->columns.clear();
@@ -452,19 +492,25 @@ std::string device_inverse_rows(const LowerFactorView& factor, InverseRows* out)
     std::copy(pool_c.begin() + row_off[i], pool_c.begin() + row_off[i] + length, out->columns.begin() + out->start[i]);
     std::copy(pool_v.begin() + row_off[i], pool_v.begin() + row_off[i] + length, out->values.begin() + out->start[i]);
   }
+  PD_FT_REPORT("inverse rows", timer, std::string("levels ") + std::to_string(levels) + " items " +
+                                         std::to_string(items.size()) + " nnz " + std::to_string(out->start[n]));
   return std::string();
 }
 
 std::string device_ldlt(const SymbolicView& symbolic, double* values, double* diagonal) {
+  const auto timer = PD_FT_NOW();
   const int32_t n = symbolic.size;
   if (n == 0) return std::string();
   const int64_t nnz = symbolic.row_start[n];
   const int64_t col_nnz = symbolic.col_start[n];
   std::vector<int32_t> level(n, 0);
   int32_t levels = 0;
+  int64_t longest = 0;
   for (int32_t i = 0; i < n; ++i) {
     const int64_t strict = symbolic.row_start[i + 1] - 1 - symbolic.row_start[i];
+    longest = std::max(longest, strict);
     if (strict > kLdltMaxPattern) {
+      PD_FT_REPORT("ldlt fallback", timer, std::string("row length ") + std::to_string(strict));
       return "device LDLT: a row of L has " + std::to_string(strict) + " entries (at most " +
              std::to_string(kLdltMaxPattern) + " are staged)";
     }
@@ -474,21 +520,28 @@ std::string device_ldlt(const SymbolicView& symbolic, double* values, double* di
     level[i] = l;
     levels = std::max(levels, l + 1);
   }
-  std::vector<int32_t> level_count(static_cast<size_t>(levels) + 1, 0);
-  for (int32_t i = 0; i < n; ++i) level_count[level[i] + 1] += 1;
-  for (int32_t l = 0; l < levels; ++l) level_count[l + 1] += level_count[l];
-  std::vector<int32_t> by_level(n);
-  {
-    std::vector<int32_t> cursor(level_count.begin(), level_count.end() - 1);
-    for (int32_t i = 0; i < n; ++i) by_level[cursor[level[i]]++] = i;
+  // Work items level by level: every column split into groups of kThreads entries.
+  std::vector<std::vector<int32_t>> columns_of(levels);
+  for (int32_t j = 0; j < n; ++j) columns_of[level[j]].push_back(j);
+  std::vector<ColumnItem> items;
+  std::vector<int64_t> level_items(static_cast<size_t>(levels) + 1, 0);
+  std::vector<int64_t> level_longest(levels, 0);
+  for (int32_t l = 0; l < levels; ++l) {
+    for (int32_t j : columns_of[l]) {
+      const int32_t count = static_cast<int32_t>(symbolic.col_start[j + 1] - symbolic.col_start[j]) + 1;
+      for (int32_t first = 0; first < count; first += kThreads) items.push_back(ColumnItem{j, first});
+      level_longest[l] = std::max(level_longest[l], symbolic.row_start[j + 1] - 1 - symbolic.row_start[j]);
+    }
+    level_items[l + 1] = static_cast<int64_t>(items.size());
   }
   StreamGuard guard;
   PD_FD_CHECK(cudaStreamCreateWithFlags(&guard.stream, cudaStreamNonBlocking), "stream");
   cudaStream_t stream = guard.stream;
-  DeviceArray<int64_t> d_row_start, d_col_start;
-  DeviceArray<int32_t> d_pattern, d_col_rows, d_column_index, d_rows;
-  DeviceArray<double> d_values, d_col_values, d_diagonal;
-  DeviceArray<int> d_flags;
+  DeviceArray<int64_t> d_row_start, d_col_start, d_col_pos;
+  DeviceArray<int32_t> d_pattern, d_col_rows;
+  DeviceArray<double> d_initial, d_multipliers, d_unscaled, d_diagonal;
+  DeviceArray<ColumnItem> d_items;
+  DeviceArray<int> d_fail;
   auto upload = [&](auto& array, const auto* host, size_t count) {
     cudaError_t e = array.allocate(count);
     if (e == cudaSuccess && count > 0)
@@ -499,40 +552,54 @@ std::string device_ldlt(const SymbolicView& symbolic, double* values, double* di
   PD_FD_CHECK(upload(d_pattern, symbolic.pattern, static_cast<size_t>(nnz)), "upload");
   PD_FD_CHECK(upload(d_col_start, symbolic.col_start, static_cast<size_t>(n) + 1), "upload");
   PD_FD_CHECK(upload(d_col_rows, symbolic.col_rows, static_cast<size_t>(col_nnz)), "upload");
-  PD_FD_CHECK(upload(d_column_index, symbolic.column_index, static_cast<size_t>(nnz)), "upload");
-  PD_FD_CHECK(upload(d_values, values, static_cast<size_t>(nnz)), "upload");
-  PD_FD_CHECK(upload(d_rows, by_level.data(), by_level.size()), "upload");
-  PD_FD_CHECK(d_col_values.allocate(static_cast<size_t>(col_nnz)), "allocate");
+  PD_FD_CHECK(upload(d_col_pos, symbolic.col_pos, static_cast<size_t>(col_nnz)), "upload");
+  PD_FD_CHECK(upload(d_initial, values, static_cast<size_t>(nnz)), "upload");
+  PD_FD_CHECK(upload(d_items, items.data(), items.size()), "upload");
+  PD_FD_CHECK(d_multipliers.allocate(static_cast<size_t>(nnz)), "allocate");
+  PD_FD_CHECK(d_unscaled.allocate(static_cast<size_t>(nnz)), "allocate");
   PD_FD_CHECK(d_diagonal.allocate(n), "allocate");
-  PD_FD_CHECK(d_flags.allocate(2), "allocate");
-  const int flags_init[2] = {n, 0};  // first failing pivot (n: none), structure error
-  PD_FD_CHECK(cudaMemcpyAsync(d_flags.ptr, flags_init, sizeof(flags_init), cudaMemcpyHostToDevice, stream), "upload");
-  // Levels in order on one stream: a level's rows read only rows of lower levels.
+  PD_FD_CHECK(d_fail.allocate(1), "allocate");
+  PD_FD_CHECK(cudaMemcpyAsync(d_fail.ptr, &n, sizeof(int), cudaMemcpyHostToDevice, stream), "upload");
+  const size_t smem_max = static_cast<size_t>(longest) * (sizeof(double) + sizeof(int32_t));
+  PD_FD_CHECK(cudaFuncSetAttribute(reinterpret_cast<const void*>(&ldlt_columns_kernel),
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(std::max<size_t>(smem_max, 1))),
+              "shared memory");
+  // Levels in order on one stream: a level's columns read only columns of lower levels.
   for (int32_t l = 0; l < levels; ++l) {
-    const int32_t count = level_count[l + 1] - level_count[l];
-    ldlt_rows_kernel<<<count, kThreads, 0, stream>>>(d_rows.ptr + level_count[l], d_row_start.ptr, d_pattern.ptr,
-                                                      d_col_start.ptr, d_col_rows.ptr, d_column_index.ptr,
-                                                      d_values.ptr, d_col_values.ptr, d_diagonal.ptr, d_flags.ptr,
-                                                      d_flags.ptr + 1);
+    const int64_t first = level_items[l];
+    const int32_t count = static_cast<int32_t>(level_items[l + 1] - first);
+    const size_t smem = static_cast<size_t>(level_longest[l]) * (sizeof(double) + sizeof(int32_t));
+    ldlt_columns_kernel<<<count, kThreads, smem, stream>>>(d_items.ptr + first, d_row_start.ptr, d_pattern.ptr,
+                                                           d_col_start.ptr, d_col_rows.ptr, d_col_pos.ptr,
+                                                           d_initial.ptr, d_multipliers.ptr, d_unscaled.ptr,
+                                                           d_diagonal.ptr, d_fail.ptr);
+    PD_FD_CHECK(cudaGetLastError(), "launch");
+    ldlt_divide_kernel<<<count, kThreads, 0, stream>>>(d_items.ptr + first, d_col_start.ptr, d_col_pos.ptr,
+                                                       d_unscaled.ptr, d_diagonal.ptr, d_multipliers.ptr);
     PD_FD_CHECK(cudaGetLastError(), "launch");
   }
-  int flags[2] = {0, 0};
-  std::vector<double> out_values(static_cast<size_t>(nnz)), out_diagonal(n);
-  PD_FD_CHECK(cudaMemcpyAsync(flags, d_flags.ptr, sizeof(flags), cudaMemcpyDeviceToHost, stream), "read back");
-  PD_FD_CHECK(cudaMemcpyAsync(out_values.data(), d_values.ptr, out_values.size() * sizeof(double),
+  int fail = n;
+  std::vector<double> multipliers(static_cast<size_t>(nnz)), pivots(n);
+  PD_FD_CHECK(cudaMemcpyAsync(&fail, d_fail.ptr, sizeof(int), cudaMemcpyDeviceToHost, stream), "read back");
+  PD_FD_CHECK(cudaMemcpyAsync(multipliers.data(), d_multipliers.ptr, multipliers.size() * sizeof(double),
                               cudaMemcpyDeviceToHost, stream),
               "read back");
-  PD_FD_CHECK(cudaMemcpyAsync(out_diagonal.data(), d_diagonal.ptr, out_diagonal.size() * sizeof(double),
-                              cudaMemcpyDeviceToHost, stream),
+  PD_FD_CHECK(cudaMemcpyAsync(pivots.data(), d_diagonal.ptr, pivots.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                              stream),
               "read back");
   PD_FD_CHECK(cudaStreamSynchronize(stream), "read back");
-  if (flags[1] != 0) return "device LDLT: a column entry fell outside its row pattern";
-  if (flags[0] < n) {
-    return "matrix is not positive definite: LDLT pivot " + std::to_string(flags[0]) + " is " +
-           std::to_string(out_diagonal[flags[0]]);
+  if (fail < n) {
+    return "matrix is not positive definite: LDLT pivot " + std::to_string(fail) + " is " +
+           std::to_string(pivots[fail]);
   }
-  std::copy(out_values.begin(), out_values.end(), values);
-  std::copy(out_diagonal.begin(), out_diagonal.end(), diagonal);
+  for (int32_t i = 0; i < n; ++i) {
+    for (int64_t p = symbolic.row_start[i]; p < symbolic.row_start[i + 1] - 1; ++p) values[p] = multipliers[p];
+    values[symbolic.row_start[i + 1] - 1] = pivots[i];
+    diagonal[i] = pivots[i];
+  }
+  PD_FT_REPORT("ldlt", timer, std::string("levels ") + std::to_string(levels) + " items " +
+                                  std::to_string(items.size()));
   return std::string();
 }
 

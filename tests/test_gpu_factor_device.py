@@ -5,7 +5,7 @@ bit-identical, and the same error for a matrix that is not positive definite.
 The host build is itself bit-identical to the reference's sparse.py setup
 (tests/test_factor.py); the device build must therefore reproduce it exactly,
 including the reference's exact-zero omission (the "cancel" matrix has entries
-of L^{-1} that cancel to zero) and rows that span several 4,096-label chunks
+of L^{-1} that cancel to zero) and rows that span many 256-label chunks
 (the 32x8x8 Tet4 block and a 40x10x10 Hex8 cantilever).
 """
 
