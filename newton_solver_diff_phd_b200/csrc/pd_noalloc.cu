@@ -93,6 +93,32 @@ class DeviceScope {
 
 }  // namespace
 
+// Device address of the scratch array on `device` (the current device),
+// resolved on the first request and cached.
+cudaError_t static_scratch_address(int device, void** address) {
+  std::lock_guard<std::mutex> lock(g_scratch_mutex);
+  if (g_scratch_address[device] == nullptr) {
+    const cudaError_t status = cudaGetSymbolAddress(&g_scratch_address[device], g_static_scratch);
+    if (status != cudaSuccess) {
+      g_scratch_address[device] = nullptr;
+      return status;
+    }
+  }
+  *address = g_scratch_address[device];
+  return cudaSuccess;
+}
+
+// Called by pd_build (never inside stream capture) so that a first
+// pd_apply_inverse_static inside a capture finds the address resolved.
+int pd_internal_resolve_static_scratch(int device) {
+  if (device < 0 || device >= kMaxDevices) return pd_internal_fail(PD_ERR_INVALID, "device ordinal out of range");
+  void* address = nullptr;
+  const cudaError_t status = static_scratch_address(device, &address);
+  if (status != cudaSuccess)
+    return pd_internal_fail(PD_ERR_CUDA, (std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(status)).c_str());
+  return PD_OK;
+}
+
 extern "C" int pd_apply_inverse_static(PdSolver* solver, const double* rhs, double* out, void* stream) {
   if (solver == nullptr || rhs == nullptr || out == nullptr) return pd_internal_fail(PD_ERR_INVALID, "null argument");
   // The size limit is checked first, so that an oversized solver is refused
@@ -116,19 +142,9 @@ extern "C" int pd_apply_inverse_static(PdSolver* solver, const double* rhs, doub
   cudaError_t status = scope.enter(device);
   if (status != cudaSuccess) return pd_internal_fail(PD_ERR_CUDA, cudaGetErrorString(status));
   void* scratch = nullptr;
-  {
-    std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (g_scratch_address[device] == nullptr) {
-      // First call on this device: resolve the array's device address with
-      // the device current. Make this first call outside stream capture.
-      status = cudaGetSymbolAddress(&g_scratch_address[device], g_static_scratch);
-      if (status != cudaSuccess) {
-        g_scratch_address[device] = nullptr;
-        return pd_internal_fail(PD_ERR_CUDA, (std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(status)).c_str());
-      }
-    }
-    scratch = g_scratch_address[device];
-  }
+  status = static_scratch_address(device, &scratch);  // resolved by pd_build already
+  if (status != cudaSuccess)
+    return pd_internal_fail(PD_ERR_CUDA, (std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(status)).c_str());
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const int blocks = (rows * 32 + pdb200::kBlock - 1) / pdb200::kBlock;
   double* y = static_cast<double*>(scratch);

@@ -24,6 +24,10 @@
 using pdb200::AdjointArgs;
 using pdb200::StepArgs;
 
+// pd_noalloc.cu: resolves the device address of pd_apply_inverse_static's
+// scratch array on `device` (the current device).
+int pd_internal_resolve_static_scratch(int device);
+
 namespace {
 
 thread_local std::string g_last_error;
@@ -686,6 +690,7 @@ int pd_build(PdSolver* s, double dt) {
   }
   // Fixed-order reductions handle up to 256 blocks (8 chunks of 32).
   blocks = std::min(std::min(blocks, s->max_blocks), 256);
+  if (int status = pd_internal_resolve_static_scratch(s->device)) return status;
   PD_CUDA(s->d_s_off.upload(s->factor.s.offsets));
   PD_CUDA(s->d_s_col.upload(s->factor.s.columns));
   PD_CUDA(s->d_s_val.upload(s->factor.s.values));
