@@ -338,6 +338,8 @@ def run_b200(args):
             result["twist"] = run_twist(args, device)
         if world == 1 and not args.no_cantilever:
             result["cantilever"] = run_cantilever(args, device)
+        if world == 1 and not args.no_diffpd:
+            result["diffpd"] = run_diffpd(args, device)
         if world == 1:
             result["factor_build"] = run_factor_build(device)
             if args.factor_twist:
@@ -1011,6 +1013,73 @@ def run_cantilever(args, device):
     return out
 
 
+def run_diffpd(args, device):
+    """The SolverDiffPD (L-BFGS) forward step on the Tet4 32x8x8 block of 1 cm cubes (the x = 0 face
+    pinned, gravity, corotated 4e4 Pa and volume 5e4 Pa weights, density 1000 kg/m^3, a planar
+    penalty contact 2 cm below the block with friction), `diffpd_steps` steps of dt 1e-2 at the
+    reference's default tolerances (rel 1e-4, abs 1e-9, 10 history pairs): per-step device time
+    and L-BFGS iterations, the first two steps checked against the NumPy restatement of the
+    reference step (oracle/diff_pd_oracle.py, dense Cholesky of A), which is also timed on the host
+    as the leg's CPU baseline."""
+    import torch
+
+    from newton_solver_diff_phd_b200 import ModelBuilder, SolverDiffPD
+    from oracle.diff_pd_oracle import DiffPdStep
+
+    builder = ModelBuilder(gravity=(0.0, 0.0, -9.81))
+    builder.add_soft_grid(pos=(0.0, 0.0, 0.0), rot=None, vel=(0.0, 0.0, 0.0), dim_x=NX, dim_y=NY, dim_z=NZ,
+                          cell_x=EDGE, cell_y=EDGE, cell_z=EDGE, density=1000.0, k_mu=2.0e4, k_lambda=5.0e4,
+                          k_damp=0.0, fix_left=True)
+    model = builder.finalize(device)
+    forces = [("planar_contact", [0.0, 0.0, 1.0, 0.02, 3, 1.0e6, 1.0, 0.1])]
+    solver = SolverDiffPD(model, density=1000.0, corotated_stiffness=4.0e4, volume_stiffness=5.0e4,
+                          state_forces=forces, gravity=(0.0, 0.0, -9.81))
+    dt, steps = 1.0e-2, args.diffpd_steps
+    states = [model.state(), model.state()]
+    solver.step(states[0], states[1], None, None, dt)  # factor build and warm-up
+    torch.cuda.synchronize()
+    solver.check_status()
+    states = [model.state(), model.state()]
+    stream = torch.cuda.current_stream()
+    ms, iterations, inputs, outputs = [], [], [], []
+    for t in range(steps):
+        if t < 2:
+            inputs.append((states[0].particle_q.double().cpu().numpy(), states[0].particle_qd.double().cpu().numpy()))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        solver.step(states[0], states[1], None, None, dt)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+        iterations.append(int(solver.iterations[0]))
+        if t < 2:
+            outputs.append(solver.positions.cpu().numpy())
+        states.reverse()
+    status = solver.read_status()
+    oracle = DiffPdStep(model.particle_q.cpu().numpy().astype(np.float64),
+                        model.tet_indices.cpu().numpy().reshape(-1, 4), 1000.0, 4.0e4, 5.0e4,
+                        model.particle_inv_mass.cpu().numpy() > 0, (0.0, 0.0, -9.81), forces)
+    errors, oracle_iterations, cpu_s = [], [], 0.0
+    for (q, v), x in zip(inputs, outputs):
+        start = time.perf_counter()
+        x_ref, _, count = oracle.step(q, v, np.zeros_like(q), dt)
+        cpu_s += time.perf_counter() - start
+        errors.append(float(np.abs(x - x_ref).max()))
+        oracle_iterations.append(int(count))
+    return {"workload": "tet4_block_32x8x8_diffpd_lbfgs", "steps": steps, "ms_per_step": float(np.mean(ms)),
+            "steps_per_s": 1000.0 * steps / float(np.sum(ms)),
+            "us_per_iteration": 1000.0 * float(np.sum(ms)) / max(sum(iterations), 1), "iterations": iterations,
+            "status": int(status), "first_steps_vs_oracle": {"max_abs_position_err_m": max(errors),
+                                                             "iterations": iterations[:2],
+                                                             "oracle_iterations": oracle_iterations},
+            "cpu_baseline": {"value": len(inputs) / cpu_s, "unit": "DiffPD steps/s", "cores": os.cpu_count(),
+                             "kind": "port", "sample": "the first two steps with oracle/diff_pd_oracle.py (NumPy, "
+                                                       "dense Cholesky of A, threaded BLAS)"},
+            "config": {"particles": model.particle_count, "tets": model.tet_count, "dt": dt, "rel_tol": 1.0e-4,
+                       "abs_tol": 1.0e-9, "history": 10, "max_ls_iter": 10,
+                       "state_forces": "gravity, planar_contact z = -0.02 m (p 3, kn 1e6, kf 1, mu 0.1)"}}
+
+
 def run_factor_build(device, twist=False):
     """The exact inverse factor built on the host and with the numeric LDL^T and the rows of
     L^{-1} on the device: wall time of each build and whether every array is bit-identical. The
@@ -1289,6 +1358,8 @@ def main():
     parser.add_argument("--twist", action="store_true",
                         help="add the 35,721-particle Hex8 twist-release leg (minutes: its host factor build)")
     parser.add_argument("--twist-steps", type=int, default=100, help="steps of the twist-release leg")
+    parser.add_argument("--no-diffpd", action="store_true", help="skip the SolverDiffPD (L-BFGS) leg")
+    parser.add_argument("--diffpd-steps", type=int, default=20, help="steps of the SolverDiffPD leg")
     parser.add_argument("--factor-twist", action="store_true",
                         help="also time the twist-release matrix's factor build on the host and the device")
     parser.add_argument("--no-extras", action="store_true",
