@@ -1360,6 +1360,8 @@ def main():
     parser.add_argument("--twist-steps", type=int, default=100, help="steps of the twist-release leg")
     parser.add_argument("--no-diffpd", action="store_true", help="skip the SolverDiffPD (L-BFGS) leg")
     parser.add_argument("--diffpd-steps", type=int, default=20, help="steps of the SolverDiffPD leg")
+    parser.add_argument("--profile-diffpd", action="store_true",
+                        help="run only the SolverDiffPD leg (for profilers; --diffpd-steps sets its length)")
     parser.add_argument("--factor-twist", action="store_true",
                         help="also time the twist-release matrix's factor build on the host and the device")
     parser.add_argument("--no-extras", action="store_true",
@@ -1370,6 +1372,11 @@ def main():
     args = parser.parse_args()
     if args.profile_batch:
         run_batch_profile(args)
+        return
+    if args.profile_diffpd:
+        import torch
+
+        print(json.dumps(run_diffpd(args, torch.device("cuda", 0))))
         return
     if args.impl == "reference":
         run_reference(args)
