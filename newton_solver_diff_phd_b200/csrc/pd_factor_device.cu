@@ -301,7 +301,7 @@ struct StreamGuard {
 };
 
 std::string cuda_error(const char* what, cudaError_t e) {
-  return std::string("device inverse rows: ") + what + ": " + cudaGetErrorString(e);
+  return std::string("device factor build: ") + what + ": " + cudaGetErrorString(e);
 }
 
 #define PD_FD_CHECK(call, what)                   \
