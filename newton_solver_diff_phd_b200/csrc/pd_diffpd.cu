@@ -464,6 +464,9 @@ namespace {
 
 int dp_fail(int code, const std::string& message) { return pd_set_error(code, message); }
 
+// Doubles between consecutive DiffPD vectors: 3n rounded up to 32 (256 bytes).
+size_t dp_vector_stride(int n) { return (static_cast<size_t>(3) * n + 31) / 32 * 32; }
+
 }  // namespace
 
 extern "C" {
@@ -506,7 +509,10 @@ int pd_diffpd_step(PdSolver* s, const PdDiffPdOptions* o, const void* q, const v
     return dp_fail(PD_ERR_STATE, "SolverDiffPD must rebuild its factor (pd_build) for this dt and model");
   PD_CUDA(cudaSetDevice(s->device));
   if (int status = pd_ensure_plan(s)) return status;
-  const size_t vec = static_cast<size_t>(3) * s->n;
+  // Every [n][3] vector starts on a 256-byte boundary: the products stage
+  // their input vector into shared memory with 16-byte loads, and a stride of
+  // 3n doubles would leave odd slots only 8-byte aligned.
+  const size_t vec = dp_vector_stride(s->n);
   constexpr int kVectors = 13;
   if (s->dp_vectors.ptr == nullptr) {
     PD_CUDA(s->dp_vectors.allocate(kVectors * vec * sizeof(double)));
@@ -593,7 +599,7 @@ int pd_diffpd_step(PdSolver* s, const PdDiffPdOptions* o, const void* q, const v
 int pd_diffpd_results(PdSolver* s, double** positions, double** velocities, int32_t* iterations, void* stream) {
   if (s == nullptr) return dp_fail(PD_ERR_INVALID, "null solver");
   if (s->dp_vectors.ptr == nullptr) return dp_fail(PD_ERR_STATE, "no DiffPD step has run");
-  const size_t vec = static_cast<size_t>(3) * s->n;
+  const size_t vec = dp_vector_stride(s->n);
   if (positions) *positions = s->dp_vectors.as<double>() + 3 * vec;
   if (velocities) *velocities = s->dp_vectors.as<double>() + 12 * vec;
   if (iterations) {

@@ -152,3 +152,31 @@ def test_invalid_configurations_are_rejected():
         arguments = {"density": DENSITY, **options}
         with pytest.raises(ValueError):
             SolverDiffPD(model, **arguments)
+
+
+@pytest.mark.gpu
+def test_a_streamed_factor_with_a_staged_vector_gives_the_same_steps():
+    """96 blocks instead of 148 on the 32x8x8 block: the larger slices of S and S^T no longer fit
+    in shared memory, so the products stream the factor and stage their input vector with
+    16-byte loads (every DiffPD vector starts on a 256-byte boundary for that; with the vectors
+    packed 3n doubles apart this launch stopped on a misaligned address); the steps follow the
+    default launch's within rounding."""
+    results = []
+    for blocks in (0, 96):
+        builder = ModelBuilder(gravity=GRAVITY)
+        builder.add_soft_grid(pos=(0.0, 0.0, 0.0), rot=None, vel=(0.0, 0.0, 0.0), dim_x=32, dim_y=8, dim_z=8,
+                              cell_x=0.01, cell_y=0.01, cell_z=0.01, density=DENSITY, k_mu=2.0e4, k_lambda=5.0e4,
+                              k_damp=0.0, fix_left=True)
+        model = builder.finalize("cuda")
+        solver = SolverDiffPD(model, density=DENSITY, corotated_stiffness=COROTATED, volume_stiffness=VOLUME,
+                              gravity=GRAVITY, blocks=blocks)
+        states = [model.state(), model.state()]
+        iterations = []
+        for _ in range(3):
+            solver.step(states[0], states[1], None, None, DT)
+            solver.check_status()
+            iterations.append(int(solver.iterations[0]))
+            states.reverse()
+        results.append((solver.positions.cpu().numpy().copy(), iterations))
+    assert all(abs(a - b) <= 1 for a, b in zip(results[0][1], results[1][1]))
+    np.testing.assert_allclose(results[1][0], results[0][0], rtol=0.0, atol=1.0e-8)
