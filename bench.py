@@ -1362,6 +1362,8 @@ def main():
     parser.add_argument("--twist-steps", type=int, default=100, help="steps of the twist-release leg")
     parser.add_argument("--no-diffpd", action="store_true", help="skip the SolverDiffPD (L-BFGS) leg")
     parser.add_argument("--diffpd-steps", type=int, default=20, help="steps of the SolverDiffPD leg")
+    parser.add_argument("--profile-factor", action="store_true",
+                        help="run only the factor-build leg (4,961 rows, host then device; for profilers)")
     parser.add_argument("--profile-diffpd", action="store_true",
                         help="run only the SolverDiffPD leg (for profilers; --diffpd-steps sets its length)")
     parser.add_argument("--factor-twist", action="store_true",
@@ -1379,6 +1381,11 @@ def main():
         import torch
 
         print(json.dumps(run_diffpd(args, torch.device("cuda", 0))))
+        return
+    if args.profile_factor:
+        import torch
+
+        print(json.dumps(run_factor_build(torch.device("cuda", 0))))
         return
     if args.impl == "reference":
         run_reference(args)
