@@ -29,6 +29,10 @@ namespace pdb200 {
 // combine) reaches this are split over host threads.
 std::atomic<int64_t> g_parallel_row_work{1 << 16};
 
+// Factors with at least this many entries of L take the numeric LDL^T over
+// host threads (left-looking columns, bit-identical).
+std::atomic<int64_t> g_parallel_ldlt_entries{int64_t{1} << 21};
+
 namespace {
 
 // A fixed set of worker threads that run one task per worker and wait for
@@ -264,6 +268,112 @@ std::vector<int32_t> nested_dissection(const Adjacency& adjacency) {
   return order;
 }
 
+// The numeric LDL^T as left-looking columns over host threads, for large
+// factors. Entry (i, j) is the permuted A value minus m(i, k) e(j, k) over the
+// columns k < j that rows i and j share, in ascending k: the sequence of
+// rounded products and subtractions the right-looking update applies to it,
+// so the factor is bit-identical. Columns are processed level by level of the
+// elimination tree (a column reads only columns of lower levels); within a
+// level every entry is independent, so the top of the tree, one column per
+// level, is split over the threads entry by entry. `values` holds the lower
+// triangle of A at the row positions on entry and the multipliers (strict
+// positions) and pivots (diagonal positions) on return; the caller checks the
+// pivots in elimination order.
+void ldlt_left_looking(int32_t size, const std::vector<int64_t>& row_start, const std::vector<int32_t>& pattern,
+                       const std::vector<std::vector<int32_t>>& columns,
+                       const std::vector<std::vector<int64_t>>& column_positions, std::vector<double>& values,
+                       std::vector<double>& diagonal, RowPool& pool) {
+  std::vector<int32_t> level(size, 0);
+  int32_t levels = 0;
+  for (int32_t i = 0; i < size; ++i) {
+    int32_t l = 0;
+    for (int64_t p = row_start[i]; p < row_start[i + 1] - 1; ++p) l = std::max(l, level[pattern[p]] + 1);
+    level[i] = l;
+    levels = std::max(levels, l + 1);
+  }
+  std::vector<int32_t> level_count(static_cast<size_t>(levels) + 1, 0);
+  for (int32_t j = 0; j < size; ++j) level_count[level[j] + 1] += 1;
+  for (int32_t l = 0; l < levels; ++l) level_count[l + 1] += level_count[l];
+  std::vector<int32_t> by_level(size);
+  {
+    std::vector<int32_t> cursor(level_count.begin(), level_count.end() - 1);
+    for (int32_t j = 0; j < size; ++j) by_level[cursor[level[j]]++] = j;
+  }
+  std::vector<double> unscaled(values.size(), 0.0);
+  std::vector<int64_t> first_entry;  // per column of the level: its first flat entry
+  const unsigned workers = pool.size();
+  for (int32_t l = 0; l < levels; ++l) {
+    const int32_t c0 = level_count[l], c1 = level_count[l + 1];
+    first_entry.assign(1, 0);
+    for (int32_t c = c0; c < c1; ++c)
+      first_entry.push_back(first_entry.back() + static_cast<int64_t>(columns[by_level[c]].size()) + 1);
+    const int64_t total = first_entry.back();
+    const int64_t chunk = std::max<int64_t>(16, total / (4 * static_cast<int64_t>(workers)) + 1);
+    // Entry e of the level's c-th column: 0 is the diagonal, e >= 1 row columns[j][e - 1].
+    auto for_entries = [&](const std::function<void(int32_t, int64_t)>& body) {
+      std::atomic<int64_t> next{0};
+      auto run = [&](unsigned) {
+        for (int64_t lo = next.fetch_add(chunk); lo < total; lo = next.fetch_add(chunk)) {
+          const int64_t hi = std::min(total, lo + chunk);
+          int64_t c = std::upper_bound(first_entry.begin(), first_entry.end(), lo) - first_entry.begin() - 1;
+          for (int64_t f = lo; f < hi; ++f) {
+            while (f >= first_entry[c + 1]) ++c;
+            body(by_level[c0 + c], f - first_entry[c]);
+          }
+        }
+      };
+      if (total <= chunk) {
+        run(0);
+      } else {
+        pool.run(run);
+      }
+    };
+    for_entries([&](int32_t j, int64_t e) {
+      const int64_t start_j = row_start[j];
+      const int64_t end_j = row_start[j + 1] - 1;  // the diagonal position of row j
+      if (e == 0) {
+        double acc = values[end_j];
+        for (int64_t q = start_j; q < end_j; ++q) {
+          const double product = values[q] * unscaled[q];
+          acc = acc - product;
+        }
+        unscaled[end_j] = acc;
+        return;
+      }
+      const int32_t i = columns[j][e - 1];
+      const int64_t pos = column_positions[j][e - 1];
+      double acc = values[pos];
+      int64_t p = row_start[i];
+      int64_t q = start_j;
+      while (p < pos && q < end_j) {
+        const int32_t a = pattern[p];
+        const int32_t b = pattern[q];
+        if (a < b) {
+          ++p;
+        } else if (b < a) {
+          ++q;
+        } else {
+          const double product = values[p] * unscaled[q];
+          acc = acc - product;
+          ++p;
+          ++q;
+        }
+      }
+      unscaled[pos] = acc;
+    });
+    for_entries([&](int32_t j, int64_t e) {
+      const int64_t end_j = row_start[j + 1] - 1;
+      if (e == 0) {
+        diagonal[j] = unscaled[end_j];
+        values[end_j] = unscaled[end_j];
+        return;
+      }
+      const int64_t pos = column_positions[j][e - 1];
+      values[pos] = unscaled[pos] / unscaled[end_j];
+    });
+  }
+}
+
 std::string build_inverse_factor(int32_t size, const int32_t* row_offsets, const int32_t* row_columns,
                                  const double* row_values, InverseFactor* out, const InverseRowsProvider& provider,
                                  const LdltProvider& ldlt_provider) {
@@ -416,6 +526,21 @@ std::string build_inverse_factor(int32_t size, const int32_t* row_offsets, const
     const std::string error = ldlt_provider(view, values.data(), diagonal.data());
     if (error.rfind("device LDLT:", 0) != 0) {
       if (!error.empty()) return error;
+      factored = true;
+    }
+  }
+  // Large factors: left-looking columns over the host threads (bit-identical).
+  if (!factored && pattern_nnz >= g_parallel_ldlt_entries.load()) {
+    const unsigned hardware = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    if (hardware > 1) {
+      RowPool pool(hardware);
+      ldlt_left_looking(size, row_start, pattern, columns, column_positions, values, diagonal, pool);
+      for (int32_t k = 0; k < size; ++k) {
+        const double pivot = diagonal[k];
+        if (!std::isfinite(pivot) || pivot <= 0.0) {
+          return "matrix is not positive definite: LDLT pivot " + std::to_string(k) + " is " + std::to_string(pivot);
+        }
+      }
       factored = true;
     }
   }

@@ -38,6 +38,10 @@ struct InverseFactor {
 // inverse is split over host threads; the result is bit-identical either way.
 extern std::atomic<int64_t> g_parallel_row_work;
 
+// Entries of L from which the numeric LDL^T runs as left-looking columns over
+// host threads instead of the sequential right-looking loop (bit-identical).
+extern std::atomic<int64_t> g_parallel_ldlt_entries;
+
 // The rows of the unit lower factor L in elimination order after the numeric
 // LDL^T: row i holds its columns k < i in ascending order with the
 // multipliers L(i, k), then its diagonal entry (position row_start[i+1] - 1,

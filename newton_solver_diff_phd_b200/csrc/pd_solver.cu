@@ -1154,6 +1154,11 @@ int pd_inverse_parallel_work(int64_t work) {
   return PD_OK;
 }
 
+int pd_inverse_parallel_ldlt(int64_t entries) {
+  pdb200::g_parallel_ldlt_entries.store(std::max<int64_t>(entries, 0));
+  return PD_OK;
+}
+
 int pd_inverse_build(int32_t size, const int32_t* row_offsets, const int32_t* columns, const double* values,
                      PdInverseFactor** out) {
   return pd_inverse_build_on(-1, size, row_offsets, columns, values, out);

@@ -143,3 +143,50 @@ def test_threaded_inverse_rows_are_bit_identical():
         _lib.check(lib.pd_inverse_parallel_work(1 << 16))
     for key in ("permutation", "s_offsets", "s_columns", "s_values", "st_offsets", "st_columns", "st_values"):
         assert np.array_equal(results[0][key], results[1][key]), key
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_threaded_ldlt_is_bit_identical_to_reference(name):
+    """The numeric LDL^T as left-looking columns over host threads (forced on every factor)
+    reproduces the reference's setup exactly on the golden matrices."""
+    g = golden("sparse_factors.npz")
+    lib = _lib.library()
+    try:
+        _lib.check(lib.pd_inverse_parallel_ldlt(0))
+        out = _lib.inverse_factor(_lib.dense_to_csr(g[name + "__matrix"]))
+    finally:
+        _lib.check(lib.pd_inverse_parallel_ldlt(1 << 21))
+    for key in ARRAYS:
+        np.testing.assert_array_equal(out[key], g[f"{name}__{key}"], err_msg=key)
+
+
+def test_threaded_ldlt_matches_the_sequential_loop_and_its_errors():
+    """A 2,541-row Hex8 beam (hundreds of elimination-tree levels, separator chains at the top):
+    the threaded LDL^T gives the sequential loop's arrays bit for bit; an indefinite matrix
+    fails with the same message both ways."""
+    import scipy.sparse as sp
+
+    from newton_solver_diff_phd_b200 import meshes
+    from oracle import pd_oracle
+
+    vertices, hexes, _ = meshes.hex_grid(20, 10, 10, 0.01)
+    free = vertices[:, 0] > 1.0e-12
+    young = np.exp(np.random.default_rng(5).uniform(np.log(1.0e5), np.log(1.0e7), len(hexes)))
+    mu, lam = meshes.lame_from_young(young, 0.45)
+    a = sp.csr_matrix(pd_oracle.Body.hex(vertices, hexes, free, mu, lam, 1000.0).matrix(0.01))
+    a.sort_indices()
+    indefinite = np.asarray(((4.0, 1.0, 0.0), (1.0, 3.0, 5.0), (0.0, 5.0, 2.0)))
+    lib = _lib.library()
+    results, messages = [], []
+    try:
+        for entries in (1 << 62, 0):
+            _lib.check(lib.pd_inverse_parallel_ldlt(entries))
+            results.append(_lib.inverse_factor((a.indptr, a.indices, a.data)))
+            with pytest.raises(ValueError) as info:
+                _lib.inverse_factor(_lib.dense_to_csr(indefinite))
+            messages.append(str(info.value))
+    finally:
+        _lib.check(lib.pd_inverse_parallel_ldlt(1 << 21))
+    for key in ARRAYS:
+        assert np.array_equal(results[0][key], results[1][key]), key
+    assert "positive definite" in messages[0] and messages[0] == messages[1]
