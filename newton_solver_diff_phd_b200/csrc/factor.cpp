@@ -29,9 +29,9 @@ namespace pdb200 {
 // combine) reaches this are split over host threads.
 std::atomic<int64_t> g_parallel_row_work{1 << 16};
 
-// Factors with at least this many entries of L take the numeric LDL^T over
-// host threads (left-looking columns, bit-identical).
-std::atomic<int64_t> g_parallel_ldlt_entries{int64_t{1} << 21};
+// Factors with at least this many entries of L take the numeric LDL^T and the
+// rows of L^{-1} over host threads level by level (bit-identical).
+std::atomic<int64_t> g_parallel_level_entries{int64_t{1} << 21};
 
 namespace {
 
@@ -374,6 +374,129 @@ void ldlt_left_looking(int32_t size, const std::vector<int64_t>& row_start, cons
   }
 }
 
+// Rows of L^{-1} over host threads, level by level of the elimination tree
+// (rows of a level are independent; row i reads rows k < i of lower levels).
+// Each row's label range is cut into kLevelChunk-label chunks aligned to
+// multiples of kLevelChunk, and every (row, chunk) item is one task: it walks
+// row i's columns k in ascending order and subtracts L(i, k) times row k's
+// entries inside the chunk, located through the chunk bounds stored with
+// row k. Every entry therefore sees the host walk's sequence of rounded
+// operations (one multiply, then one subtract, per k in ascending order) and
+// exact zeros are omitted the same way: the rows are bit-identical. The top
+// of the tree, one long row per level, is spread over the threads chunk by
+// chunk instead of column range by column range.
+void inverse_rows_by_levels(const LowerFactorView& f, InverseRows* out, RowPool& pool) {
+  constexpr int32_t kLevelChunk = 1024;
+  const int32_t n = f.size;
+  std::vector<int32_t> level(n, 0), lo(n);
+  int32_t levels = 0;
+  for (int32_t i = 0; i < n; ++i) {
+    int32_t l = 0, low = i;
+    for (int64_t p = f.row_start[i]; p < f.row_start[i + 1] - 1; ++p) {
+      const int32_t k = f.pattern[p];
+      l = std::max(l, level[k] + 1);
+      low = std::min(low, lo[k]);
+    }
+    level[i] = l;
+    lo[i] = low;
+    levels = std::max(levels, l + 1);
+  }
+  std::vector<int32_t> level_count(static_cast<size_t>(levels) + 1, 0);
+  for (int32_t i = 0; i < n; ++i) level_count[level[i] + 1] += 1;
+  for (int32_t l = 0; l < levels; ++l) level_count[l + 1] += level_count[l];
+  std::vector<int32_t> by_level(n);
+  {
+    std::vector<int32_t> cursor(level_count.begin(), level_count.end() - 1);
+    for (int32_t i = 0; i < n; ++i) by_level[cursor[level[i]]++] = i;
+  }
+  // Rows already computed, with the offsets of their chunks (relative).
+  std::vector<std::vector<int32_t>> row_cols(n), row_bounds(n);
+  std::vector<std::vector<double>> row_vals(n);
+  struct Item {
+    int32_t row, chunk;
+  };
+  std::vector<Item> items;
+  std::vector<std::vector<int32_t>> item_cols;
+  std::vector<std::vector<double>> item_vals;
+  for (int32_t l = 0; l < levels; ++l) {
+    items.clear();
+    for (int32_t r = level_count[l]; r < level_count[l + 1]; ++r) {
+      const int32_t i = by_level[r];
+      for (int32_t j = lo[i] / kLevelChunk; j <= i / kLevelChunk; ++j) items.push_back(Item{i, j});
+    }
+    const int64_t count = static_cast<int64_t>(items.size());
+    item_cols.assign(count, std::vector<int32_t>());
+    item_vals.assign(count, std::vector<double>());
+    std::atomic<int64_t> next{0};
+    auto work = [&](unsigned) {
+      std::vector<double> acc(kLevelChunk);
+      for (int64_t t = next.fetch_add(1); t < count; t = next.fetch_add(1)) {
+        const int32_t i = items[t].row;
+        const int32_t j = items[t].chunk;
+        const int32_t c_begin = std::max(lo[i], j * kLevelChunk);
+        const int32_t c_end = std::min(i, (j + 1) * kLevelChunk - 1) + 1;
+        const int32_t width = c_end - c_begin;
+        std::fill(acc.begin(), acc.begin() + width, 0.0);
+        if (i >= c_begin && i < c_end) acc[i - c_begin] = 1.0;
+        for (int64_t p = f.row_start[i]; p < f.row_start[i + 1] - 1; ++p) {
+          const int32_t k = f.pattern[p];
+          const double coefficient = f.values[p];
+          if (coefficient == 0.0) continue;
+          const int32_t j0 = lo[k] / kLevelChunk;
+          if (j < j0 || j > k / kLevelChunk) continue;
+          const int32_t b = row_bounds[k][j - j0];
+          const int32_t e = row_bounds[k][j - j0 + 1];
+          const int32_t* cols = row_cols[k].data();
+          const double* vals = row_vals[k].data();
+          for (int32_t q = b; q < e; ++q) {
+            const int32_t c = cols[q] - c_begin;
+            const double product = coefficient * vals[q];
+            acc[c] = acc[c] - product;
+          }
+        }
+        std::vector<int32_t>& oc = item_cols[t];
+        std::vector<double>& ov = item_vals[t];
+        for (int32_t u = 0; u < width; ++u) {
+          if (acc[u] != 0.0) {
+            oc.push_back(c_begin + u);
+            ov.push_back(acc[u]);
+          }
+        }
+      }
+    };
+    if (count > 1) {
+      pool.run(work);
+    } else {
+      work(0);
+    }
+    // Assemble the level's rows from their items (consecutive, ascending chunks).
+    for (int64_t t = 0; t < count;) {
+      const int32_t i = items[t].row;
+      std::vector<int32_t>& cols = row_cols[i];
+      std::vector<double>& vals = row_vals[i];
+      std::vector<int32_t>& bounds = row_bounds[i];
+      bounds.assign(1, 0);
+      for (; t < count && items[t].row == i; ++t) {
+        cols.insert(cols.end(), item_cols[t].begin(), item_cols[t].end());
+        vals.insert(vals.end(), item_vals[t].begin(), item_vals[t].end());
+        bounds.push_back(static_cast<int32_t>(cols.size()));
+        std::vector<int32_t>().swap(item_cols[t]);
+        std::vector<double>().swap(item_vals[t]);
+      }
+    }
+  }
+  out->start.assign(static_cast<size_t>(n) + 1, 0);
+  for (int32_t i = 0; i < n; ++i) out->start[i + 1] = out->start[i] + static_cast<int64_t>(row_cols[i].size());
+  out->columns.resize(static_cast<size_t>(out->start[n]));
+  out->values.resize(static_cast<size_t>(out->start[n]));
+  for (int32_t i = 0; i < n; ++i) {
+    std::copy(row_cols[i].begin(), row_cols[i].end(), out->columns.begin() + out->start[i]);
+    std::copy(row_vals[i].begin(), row_vals[i].end(), out->values.begin() + out->start[i]);
+    std::vector<int32_t>().swap(row_cols[i]);
+    std::vector<double>().swap(row_vals[i]);
+  }
+}
+
 std::string build_inverse_factor(int32_t size, const int32_t* row_offsets, const int32_t* row_columns,
                                  const double* row_values, InverseFactor* out, const InverseRowsProvider& provider,
                                  const LdltProvider& ldlt_provider) {
@@ -530,7 +653,7 @@ std::string build_inverse_factor(int32_t size, const int32_t* row_offsets, const
     }
   }
   // Large factors: left-looking columns over the host threads (bit-identical).
-  if (!factored && pattern_nnz >= g_parallel_ldlt_entries.load()) {
+  if (!factored && pattern_nnz >= g_parallel_level_entries.load()) {
     const unsigned hardware = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
     if (hardware > 1) {
       RowPool pool(hardware);
@@ -602,14 +725,32 @@ std::string build_inverse_factor(int32_t size, const int32_t* row_offsets, const
     inv_columns = std::move(rows_out.columns);
     inv_values = std::move(rows_out.values);
   }
-  std::vector<double> current(provider ? 0 : size, 0.0);
-  std::vector<int32_t> touched_mark(provider ? 0 : size, -1);
-  std::vector<int32_t> touched;
   const unsigned hardware = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  bool rows_done = static_cast<bool>(provider);
+  if (!rows_done && hardware > 1 && pattern_nnz >= g_parallel_level_entries.load()) {
+    LowerFactorView view;
+    view.size = size;
+    view.row_start = row_start.data();
+    view.pattern = pattern.data();
+    view.values = values.data();
+    InverseRows rows_out;
+    RowPool level_pool(hardware);
+    inverse_rows_by_levels(view, &rows_out, level_pool);
+    if (rows_out.columns.size() > static_cast<size_t>(std::numeric_limits<int32_t>::max())) {
+      return "inverse factor fill exceeds int32 sparse indexing";
+    }
+    inv_start = std::move(rows_out.start);
+    inv_columns = std::move(rows_out.columns);
+    inv_values = std::move(rows_out.values);
+    rows_done = true;
+  }
+  std::vector<double> current(rows_done ? 0 : size, 0.0);
+  std::vector<int32_t> touched_mark(rows_done ? 0 : size, -1);
+  std::vector<int32_t> touched;
   std::unique_ptr<RowPool> pool;
   std::vector<std::vector<std::pair<int32_t, double>>> pieces;
   const int64_t parallel_work = g_parallel_row_work.load();
-  for (int32_t i = provider ? size : 0; i < size; ++i) {
+  for (int32_t i = rows_done ? size : 0; i < size; ++i) {
     int64_t work = 0;
     for (int64_t p = row_start[i]; p < row_start[i + 1] - 1; ++p) work += inv_start[pattern[p] + 1] - inv_start[pattern[p]];
     // Split only rows whose earlier rows are long: every range costs one

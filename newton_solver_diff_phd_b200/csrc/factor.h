@@ -38,9 +38,10 @@ struct InverseFactor {
 // inverse is split over host threads; the result is bit-identical either way.
 extern std::atomic<int64_t> g_parallel_row_work;
 
-// Entries of L from which the numeric LDL^T runs as left-looking columns over
-// host threads instead of the sequential right-looking loop (bit-identical).
-extern std::atomic<int64_t> g_parallel_ldlt_entries;
+// Entries of L from which the numeric LDL^T (left-looking columns) and the
+// rows of L^{-1} (chunked rows) run over host threads level by level of the
+// elimination tree instead of sequentially (bit-identical).
+extern std::atomic<int64_t> g_parallel_level_entries;
 
 // The rows of the unit lower factor L in elimination order after the numeric
 // LDL^T: row i holds its columns k < i in ascending order with the

@@ -1154,8 +1154,8 @@ int pd_inverse_parallel_work(int64_t work) {
   return PD_OK;
 }
 
-int pd_inverse_parallel_ldlt(int64_t entries) {
-  pdb200::g_parallel_ldlt_entries.store(std::max<int64_t>(entries, 0));
+int pd_inverse_parallel_levels(int64_t entries) {
+  pdb200::g_parallel_level_entries.store(std::max<int64_t>(entries, 0));
   return PD_OK;
 }
 

@@ -147,23 +147,25 @@ def test_threaded_inverse_rows_are_bit_identical():
 
 @pytest.mark.parametrize("name", NAMES)
 def test_threaded_ldlt_is_bit_identical_to_reference(name):
-    """The numeric LDL^T as left-looking columns over host threads (forced on every factor)
-    reproduces the reference's setup exactly on the golden matrices."""
+    """The numeric LDL^T (left-looking columns) and the rows of L^{-1} (chunked rows) level by
+    level over host threads, forced on every factor, reproduce the reference's setup exactly on
+    the golden matrices."""
     g = golden("sparse_factors.npz")
     lib = _lib.library()
     try:
-        _lib.check(lib.pd_inverse_parallel_ldlt(0))
+        _lib.check(lib.pd_inverse_parallel_levels(0))
         out = _lib.inverse_factor(_lib.dense_to_csr(g[name + "__matrix"]))
     finally:
-        _lib.check(lib.pd_inverse_parallel_ldlt(1 << 21))
+        _lib.check(lib.pd_inverse_parallel_levels(1 << 21))
     for key in ARRAYS:
         np.testing.assert_array_equal(out[key], g[f"{name}__{key}"], err_msg=key)
 
 
 def test_threaded_ldlt_matches_the_sequential_loop_and_its_errors():
-    """A 2,541-row Hex8 beam (hundreds of elimination-tree levels, separator chains at the top):
-    the threaded LDL^T gives the sequential loop's arrays bit for bit; an indefinite matrix
-    fails with the same message both ways."""
+    """A 2,541-row Hex8 beam (hundreds of elimination-tree levels, separator chains at the top,
+    rows spanning several 1,024-label chunks): the level-parallel LDL^T and inverse rows give the
+    sequential loops' arrays bit for bit; an indefinite matrix fails with the same message both
+    ways."""
     import scipy.sparse as sp
 
     from newton_solver_diff_phd_b200 import meshes
@@ -180,13 +182,13 @@ def test_threaded_ldlt_matches_the_sequential_loop_and_its_errors():
     results, messages = [], []
     try:
         for entries in (1 << 62, 0):
-            _lib.check(lib.pd_inverse_parallel_ldlt(entries))
+            _lib.check(lib.pd_inverse_parallel_levels(entries))
             results.append(_lib.inverse_factor((a.indptr, a.indices, a.data)))
             with pytest.raises(ValueError) as info:
                 _lib.inverse_factor(_lib.dense_to_csr(indefinite))
             messages.append(str(info.value))
     finally:
-        _lib.check(lib.pd_inverse_parallel_ldlt(1 << 21))
+        _lib.check(lib.pd_inverse_parallel_levels(1 << 21))
     for key in ARRAYS:
         assert np.array_equal(results[0][key], results[1][key]), key
     assert "positive definite" in messages[0] and messages[0] == messages[1]
