@@ -409,34 +409,56 @@ void inverse_rows_by_levels(const LowerFactorView& f, InverseRows* out, RowPool&
     std::vector<int32_t> cursor(level_count.begin(), level_count.end() - 1);
     for (int32_t i = 0; i < n; ++i) by_level[cursor[level[i]]++] = i;
   }
-  // Rows already computed, with the offsets of their chunks (relative).
-  std::vector<std::vector<int32_t>> row_cols(n), row_bounds(n);
-  std::vector<std::vector<double>> row_vals(n);
+  // Computed rows live in one pool (in level order): row i starts at
+  // row_off[i]; its chunk bounds, relative to that start, at
+  // bounds[bounds_base[i] + (chunk - lo[i] / kLevelChunk)].
+  std::vector<int64_t> bounds_base(n);
+  int64_t bounds_total = 0;
+  for (int32_t i = 0; i < n; ++i) {
+    bounds_base[i] = bounds_total;
+    bounds_total += (i / kLevelChunk - lo[i] / kLevelChunk) + 2;
+  }
+  std::vector<int32_t> bounds(static_cast<size_t>(bounds_total), 0);
+  std::vector<int64_t> row_off(n, 0), row_len(n, 0);
+  std::vector<int32_t> pool_cols;
+  std::vector<double> pool_vals;
   struct Item {
     int32_t row, chunk;
+    int64_t slot;  // offset of the item's scratch slot
   };
   std::vector<Item> items;
-  std::vector<std::vector<int32_t>> item_cols;
-  std::vector<std::vector<double>> item_vals;
+  std::vector<int32_t> item_count, scratch_cols;
+  std::vector<double> scratch_vals;
   for (int32_t l = 0; l < levels; ++l) {
     items.clear();
+    int64_t slots = 0;
     for (int32_t r = level_count[l]; r < level_count[l + 1]; ++r) {
       const int32_t i = by_level[r];
-      for (int32_t j = lo[i] / kLevelChunk; j <= i / kLevelChunk; ++j) items.push_back(Item{i, j});
+      for (int32_t j = lo[i] / kLevelChunk; j <= i / kLevelChunk; ++j) {
+        const int32_t c_begin = std::max(lo[i], j * kLevelChunk);
+        const int32_t c_end = std::min(i, (j + 1) * kLevelChunk - 1) + 1;
+        items.push_back(Item{i, j, slots});
+        slots += c_end - c_begin;
+      }
     }
     const int64_t count = static_cast<int64_t>(items.size());
-    item_cols.assign(count, std::vector<int32_t>());
-    item_vals.assign(count, std::vector<double>());
+    item_count.assign(static_cast<size_t>(count), 0);
+    if (static_cast<int64_t>(scratch_cols.size()) < slots) {
+      scratch_cols.resize(static_cast<size_t>(slots));
+      scratch_vals.resize(static_cast<size_t>(slots));
+    }
     std::atomic<int64_t> next{0};
+    const int32_t* pcols = pool_cols.data();
+    const double* pvals = pool_vals.data();
     auto work = [&](unsigned) {
-      std::vector<double> acc(kLevelChunk);
+      double acc[kLevelChunk];
       for (int64_t t = next.fetch_add(1); t < count; t = next.fetch_add(1)) {
         const int32_t i = items[t].row;
         const int32_t j = items[t].chunk;
         const int32_t c_begin = std::max(lo[i], j * kLevelChunk);
         const int32_t c_end = std::min(i, (j + 1) * kLevelChunk - 1) + 1;
         const int32_t width = c_end - c_begin;
-        std::fill(acc.begin(), acc.begin() + width, 0.0);
+        std::fill(acc, acc + width, 0.0);
         if (i >= c_begin && i < c_end) acc[i - c_begin] = 1.0;
         for (int64_t p = f.row_start[i]; p < f.row_start[i + 1] - 1; ++p) {
           const int32_t k = f.pattern[p];
@@ -444,24 +466,26 @@ void inverse_rows_by_levels(const LowerFactorView& f, InverseRows* out, RowPool&
           if (coefficient == 0.0) continue;
           const int32_t j0 = lo[k] / kLevelChunk;
           if (j < j0 || j > k / kLevelChunk) continue;
-          const int32_t b = row_bounds[k][j - j0];
-          const int32_t e = row_bounds[k][j - j0 + 1];
-          const int32_t* cols = row_cols[k].data();
-          const double* vals = row_vals[k].data();
-          for (int32_t q = b; q < e; ++q) {
-            const int32_t c = cols[q] - c_begin;
-            const double product = coefficient * vals[q];
+          const int32_t* b = bounds.data() + bounds_base[k] + (j - j0);
+          const int64_t first = row_off[k] + b[0];
+          const int64_t last = row_off[k] + b[1];
+          for (int64_t q = first; q < last; ++q) {
+            const int32_t c = pcols[q] - c_begin;
+            const double product = coefficient * pvals[q];
             acc[c] = acc[c] - product;
           }
         }
-        std::vector<int32_t>& oc = item_cols[t];
-        std::vector<double>& ov = item_vals[t];
+        int32_t* oc = scratch_cols.data() + items[t].slot;
+        double* ov = scratch_vals.data() + items[t].slot;
+        int32_t kept = 0;
         for (int32_t u = 0; u < width; ++u) {
           if (acc[u] != 0.0) {
-            oc.push_back(c_begin + u);
-            ov.push_back(acc[u]);
+            oc[kept] = c_begin + u;
+            ov[kept] = acc[u];
+            ++kept;
           }
         }
+        item_count[t] = kept;
       }
     };
     if (count > 1) {
@@ -469,31 +493,42 @@ void inverse_rows_by_levels(const LowerFactorView& f, InverseRows* out, RowPool&
     } else {
       work(0);
     }
-    // Assemble the level's rows from their items (consecutive, ascending chunks).
+    // Append the level's rows to the pool (items of a row are consecutive, in
+    // ascending chunks) and record their offsets and chunk bounds.
+    int64_t added = 0;
+    for (int64_t t = 0; t < count; ++t) added += item_count[t];
+    const int64_t base = static_cast<int64_t>(pool_cols.size());
+    pool_cols.resize(static_cast<size_t>(base + added));
+    pool_vals.resize(static_cast<size_t>(base + added));
+    int64_t at = base;
     for (int64_t t = 0; t < count;) {
       const int32_t i = items[t].row;
-      std::vector<int32_t>& cols = row_cols[i];
-      std::vector<double>& vals = row_vals[i];
-      std::vector<int32_t>& bounds = row_bounds[i];
-      bounds.assign(1, 0);
-      for (; t < count && items[t].row == i; ++t) {
-        cols.insert(cols.end(), item_cols[t].begin(), item_cols[t].end());
-        vals.insert(vals.end(), item_vals[t].begin(), item_vals[t].end());
-        bounds.push_back(static_cast<int32_t>(cols.size()));
-        std::vector<int32_t>().swap(item_cols[t]);
-        std::vector<double>().swap(item_vals[t]);
+      row_off[i] = at;
+      int32_t* b = bounds.data() + bounds_base[i];
+      int32_t within = 0;
+      int32_t slot = 0;
+      for (; t < count && items[t].row == i; ++t, ++slot) {
+        b[slot] = within;
+        std::copy(scratch_cols.begin() + items[t].slot, scratch_cols.begin() + items[t].slot + item_count[t],
+                  pool_cols.begin() + at);
+        std::copy(scratch_vals.begin() + items[t].slot, scratch_vals.begin() + items[t].slot + item_count[t],
+                  pool_vals.begin() + at);
+        at += item_count[t];
+        within += item_count[t];
       }
+      b[slot] = within;
+      row_len[i] = within;
     }
   }
   out->start.assign(static_cast<size_t>(n) + 1, 0);
-  for (int32_t i = 0; i < n; ++i) out->start[i + 1] = out->start[i] + static_cast<int64_t>(row_cols[i].size());
+  for (int32_t i = 0; i < n; ++i) out->start[i + 1] = out->start[i] + row_len[i];
   out->columns.resize(static_cast<size_t>(out->start[n]));
   out->values.resize(static_cast<size_t>(out->start[n]));
   for (int32_t i = 0; i < n; ++i) {
-    std::copy(row_cols[i].begin(), row_cols[i].end(), out->columns.begin() + out->start[i]);
-    std::copy(row_vals[i].begin(), row_vals[i].end(), out->values.begin() + out->start[i]);
-    std::vector<int32_t>().swap(row_cols[i]);
-    std::vector<double>().swap(row_vals[i]);
+    std::copy(pool_cols.begin() + row_off[i], pool_cols.begin() + row_off[i] + row_len[i],
+              out->columns.begin() + out->start[i]);
+    std::copy(pool_vals.begin() + row_off[i], pool_vals.begin() + row_off[i] + row_len[i],
+              out->values.begin() + out->start[i]);
   }
 }
 
