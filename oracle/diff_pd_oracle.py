@@ -1,9 +1,10 @@
 """Dense NumPy restatement of the reference's DiffPD ``pd_eigen`` forward step.
 
-TEST INFRASTRUCTURE ONLY (imported by tests/). It restates
+TEST INFRASTRUCTURE ONLY (imported by tests/, by __graft_entry__.smoke() and by
+bench.py's DiffPD leg, as the checker and the timed CPU baseline). It restates
 ``src/newton_solver_diff_phd/_src/solvers/diff_pd/solver.py:65-591`` and
 ``kernels.py``: the explicit state forces (gravity first, then planar and arc
-penalty contacts with velocity friction, ``kernels.py:119-150``) give
+penalty contacts with velocity friction, ``kernels.py:118-152``) give
 ``rhs = q + h v + h^2/m (f_ext + f_state(q, v))``; L-BFGS minimises
 ``Phi(x) = 1/2 m/h^2 |x - rhs|^2 + E_pd(x)`` from ``x = q`` with the
 projective-dynamics matrix ``A`` as initial Hessian (two-loop recursion over
