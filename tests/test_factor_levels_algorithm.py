@@ -1,0 +1,132 @@
+"""The level-by-level algorithms of the factor build, restated in Python on the CPU.
+
+``csrc/pd_factor_device.cu`` (and the threaded host path of ``csrc/factor.cpp``)
+compute the numeric LDL^T as left-looking columns and the rows of L^{-1} in
+label chunks, level by level of the elimination tree. These tests restate the
+two schedules step for step (levels, label ranges, chunk bounds recorded per
+stored row, merge order) and check that they reproduce the sequential
+right-looking factorisation and row walk of ``oracle/factor_port.py`` bit for
+bit, for chunk widths from one label (every row split everywhere) to wider
+than the matrix. The CUDA kernels themselves are checked against the host
+build on the GPU (``tests/test_gpu_factor_device.py``).
+"""
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from newton_solver_diff_phd_b200 import meshes
+from oracle import factor_port, pd_oracle
+
+
+def beam(nx, ny, nz):
+    vertices, hexes, _ = meshes.hex_grid(nx, ny, nz, 0.01)
+    free = vertices[:, 0] > 1.0e-12
+    young = np.exp(np.random.default_rng(3).uniform(np.log(1.0e5), np.log(1.0e7), len(hexes)))
+    mu, lam = meshes.lame_from_young(young, 0.45)
+    matrix = sp.csr_matrix(pd_oracle.Body.hex(vertices, hexes, free, mu, lam, 1000.0).matrix(0.01))
+    csr = factor_port._validate(matrix)
+    permutation = factor_port.nested_dissection(factor_port._adjacency(csr))
+    lower, diagonal = factor_port.ldlt(csr, permutation)
+    return csr, permutation, lower, diagonal
+
+
+def row_walk(lower):
+    """The sequential walk: row i = e_i - sum_k L(i, k) row k, ascending k, exact zeros omitted."""
+    rows = []
+    for i in range(len(lower)):
+        current = {i: 1.0}
+        for k in sorted(lower[i]):
+            coefficient = lower[i][k]
+            if coefficient == 0.0:
+                continue
+            for c, value in zip(*rows[k]):
+                current[c] = current.get(c, 0.0) - coefficient * value
+        kept = sorted(c for c in current if current[c] != 0.0)
+        rows.append((kept, [current[c] for c in kept]))
+    return rows
+
+
+def levels_of(lower):
+    level, lo = [0] * len(lower), [0] * len(lower)
+    for i in range(len(lower)):
+        level[i] = max((level[k] + 1 for k in lower[i]), default=0)
+        lo[i] = min([i] + [lo[k] for k in lower[i]])
+    return level, lo
+
+
+def chunked_rows(lower, width):
+    """Rows in (row, chunk) items per level; each row keeps its chunk bounds for later rows."""
+    level, lo = levels_of(lower)
+    stored, bounds = {}, {}
+    for current_level in range(max(level) + 1):
+        for i in [r for r in range(len(lower)) if level[r] == current_level]:
+            cols, vals, offsets = [], [], [0]
+            for j in range(lo[i] // width, i // width + 1):
+                c_begin, c_end = max(lo[i], j * width), min(i, (j + 1) * width - 1) + 1
+                acc = [1.0 if c_begin + t == i else 0.0 for t in range(c_end - c_begin)]
+                for k in sorted(lower[i]):
+                    coefficient = lower[i][k]
+                    j0 = lo[k] // width
+                    if coefficient == 0.0 or not j0 <= j <= k // width:
+                        continue
+                    b, e = bounds[k][j - j0], bounds[k][j - j0 + 1]
+                    for c, value in zip(stored[k][0][b:e], stored[k][1][b:e]):
+                        assert c_begin <= c < c_end
+                        acc[c - c_begin] = acc[c - c_begin] - coefficient * value
+                for t, value in enumerate(acc):
+                    if value != 0.0:
+                        cols.append(c_begin + t)
+                        vals.append(value)
+                offsets.append(len(cols))
+            stored[i], bounds[i] = (cols, vals), offsets
+    return [stored[i] for i in range(len(lower))]
+
+
+def left_looking(csr, permutation, lower):
+    """Columns level by level: entry (i, j) = A(i, j) - sum m(i, k) e(j, k) over shared k, ascending."""
+    n = len(lower)
+    permuted = sp.csr_matrix(csr[permutation][:, permutation])
+    initial = {(i, int(k)): permuted[i, int(k)] for i in range(n) for k in list(lower[i]) + [i]}
+    pattern = [sorted(lower[i]) for i in range(n)]
+    rows_of = [[] for _ in range(n)]
+    for i in range(n):
+        for k in pattern[i]:
+            rows_of[k].append(i)
+    level, _ = levels_of(lower)
+    unscaled, multiplier, pivot = {}, {}, [0.0] * n
+    for current_level in range(max(level) + 1):
+        columns = [j for j in range(n) if level[j] == current_level]
+        for j in columns:
+            acc = initial[(j, j)]
+            for k in pattern[j]:
+                acc = acc - multiplier[(j, k)] * unscaled[(j, k)]
+            pivot[j] = acc
+            for i in rows_of[j]:
+                acc = initial[(i, j)]
+                shared = [k for k in pattern[i] if k < j and k in lower[j]]
+                for k in shared:  # ascending: the merge of two sorted patterns
+                    acc = acc - multiplier[(i, k)] * unscaled[(j, k)]
+                unscaled[(i, j)] = acc
+        for j in columns:
+            for i in rows_of[j]:
+                multiplier[(i, j)] = unscaled[(i, j)] / pivot[j]
+    return multiplier, pivot
+
+
+@pytest.mark.parametrize("width", [1, 3, 16, 64, 4096])
+def test_chunked_rows_reproduce_the_row_walk(width):
+    _, _, lower, _ = beam(6, 3, 3)
+    walk = row_walk(lower)
+    for (cols, vals), (ref_cols, ref_vals) in zip(chunked_rows(lower, width), walk):
+        assert cols == ref_cols
+        assert np.array_equal(np.asarray(vals), np.asarray(ref_vals))
+
+
+def test_left_looking_columns_reproduce_the_right_looking_factor():
+    csr, permutation, lower, diagonal = beam(8, 3, 3)
+    multiplier, pivot = left_looking(csr, permutation, lower)
+    assert np.array_equal(np.asarray(pivot), diagonal)
+    for i, row in enumerate(lower):
+        for k, value in row.items():
+            assert multiplier[(i, k)] == value
