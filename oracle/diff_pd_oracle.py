@@ -153,19 +153,7 @@ class DiffPdStep:
                 if len(pairs) > self.history:
                     pairs.pop(0)
             x_last, g_last = x, grad
-            r = grad.copy()
-            rhos = [1.0 / np.sum(y * s) for s, y in pairs]
-            alphas = [0.0] * len(pairs)
-            for k in reversed(range(len(pairs))):
-                s, y = pairs[k]
-                alphas[k] = rhos[k] * np.sum(s * r)
-                r = r - alphas[k] * y
-            direction = scipy.linalg.cho_solve(self.factor, r)
-            for k in range(len(pairs)):
-                s, y = pairs[k]
-                beta = rhos[k] * np.sum(y * direction)
-                direction = direction + s * (alphas[k] - beta)
-            slope = np.sum(direction * grad)
+            direction, slope = self.two_loop(grad, pairs)
             if slope <= 0:
                 direction = grad * mask
                 slope = np.sum(grad * grad)
@@ -193,3 +181,20 @@ class DiffPdStep:
                 return x, (x - q) / dt, iteration + 1
         self.status |= 1
         return x, (x - q) / dt, self.max_pd_iter
+
+    def two_loop(self, grad, pairs):
+        """The L-BFGS direction ``H grad`` with ``A^{-1}`` as initial inverse Hessian over ``pairs``
+        (oldest first) and its slope ``direction . grad``."""
+        r = grad.copy()
+        rhos = [1.0 / np.sum(y * s) for s, y in pairs]
+        alphas = [0.0] * len(pairs)
+        for k in reversed(range(len(pairs))):
+            s, y = pairs[k]
+            alphas[k] = rhos[k] * np.sum(s * r)
+            r = r - alphas[k] * y
+        direction = scipy.linalg.cho_solve(self.factor, r)
+        for k in range(len(pairs)):
+            s, y = pairs[k]
+            beta = rhos[k] * np.sum(y * direction)
+            direction = direction + s * (alphas[k] - beta)
+        return direction, np.sum(direction * grad)
