@@ -313,7 +313,14 @@ typedef struct PdDiffPdOptions {
   double volume_weight;    /* w_v [Pa] */
   double abs_tol;          /* [N] */
   double rel_tol;          /* relative to |m/h^2 rhs| over the free rows */
+  int32_t recursion;       /* PD_DIFFPD_TWO_LOOP or PD_DIFFPD_GRAM */
 } PdDiffPdOptions;
+/* The L-BFGS direction. TWO_LOOP: the reference's two loops, one team sum per
+   pair and loop. GRAM: the same recursion from the Gram matrix s_i . y_j of
+   the stored pairs and the products s_i . g, two batched team sums per
+   iteration; the dot products are rounded in another order. */
+#define PD_DIFFPD_TWO_LOOP 0
+#define PD_DIFFPD_GRAM 1
 /* The explicit contact state forces after gravity (SolverDiffPD(state_forces=...),
    solver.py:24-56): kinds[count] (0 planar_contact, 1 arc_contact) and packed
    rows parameters[count][18] (planar: unit normal, offset / |n|, p, kn, kf, mu;

@@ -84,7 +84,11 @@ class PdDiffPdOptions(ctypes.Structure):
         ("volume_weight", ctypes.c_double),
         ("abs_tol", ctypes.c_double),
         ("rel_tol", ctypes.c_double),
+        ("recursion", ctypes.c_int32),
     ]
+
+
+DIFFPD_TWO_LOOP, DIFFPD_GRAM = 0, 1
 
 
 class PdBatchOptions(ctypes.Structure):

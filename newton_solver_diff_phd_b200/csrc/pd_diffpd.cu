@@ -36,6 +36,11 @@ constexpr int kArcContact = 1;
 constexpr int kDpNotConverged = 1;
 constexpr int kDpSingular = 2;
 constexpr int kDpLineSearch = 4;
+// Slots of one group of the Gram recursion's batched team sums: g.g, s_j.g,
+// the new row and column of the Gram matrix and y.s of the newest pair.
+constexpr int kDpWideGroup = 3 * kDiffPdMaxHistory + 4;
+// Blocks a DiffPD launch may use (the fixed-order reductions' limit).
+constexpr int kDpMaxBlocks = 256;
 
 struct DiffPdArgs {
   int n, ne;
@@ -61,6 +66,7 @@ struct DiffPdArgs {
   double* energy;    // [ne]
   double* contrib;   // [ne][4][3]
   double* partials;  // [kPartialStride][blocks]
+  double* wide;      // [2 kDpWideGroup][blocks]: the Gram recursion's batched sums
   int* status;
   int* counters;     // [0] iterations of the last step, [1] singular flag
   GridBarrier* barrier;
@@ -239,18 +245,24 @@ __device__ __forceinline__ bool dp_apply_inverse(const DiffPdArgs& a, Team team,
   return true;
 }
 
-// One DiffPD step by one team (solver.py:689-786 with the device loop of
-// kernels.py). Returns false when a team barrier gave up.
-__device__ bool diffpd_step_body(const DiffPdArgs& a, const Team team, char* dyn_smem) {
-  __shared__ double s_scratch[kBlock];
-  __shared__ double s_out[64];
-  __shared__ double s_rho[kDiffPdMaxHistory];
-  __shared__ double s_alpha[kDiffPdMaxHistory];
+// What the start of a step leaves for the L-BFGS loop: this block's rows and
+// elements, the stop threshold, Phi(q) and whether q met a singular F.
+struct DpStart {
+  int r0, r1, e0, e1;
+  double threshold, objective;
+  bool singular;
+};
+
+// begin_step (solver.py:689-720): the state forces of the start-of-step state
+// and rhs, the stop threshold rel |(m/h^2 rhs) on the free rows| + abs, Phi at
+// x = q, and x and the masked gradient on the own rows. Returns false when a
+// team barrier gave up.
+__device__ __forceinline__ bool dp_begin_step(const DiffPdArgs& a, const Team team, char* dyn_smem, int& sequence,
+                                              double* s_out, double* s_scratch, DpStart* start) {
   const int n = a.n;
   const int gtid = team.rank * blockDim.x + threadIdx.x;
   const int gthreads = team.size * blockDim.x;
   const double dt = a.dt;
-  // ---- begin_step: the state forces of the start-of-step state and rhs.
   for (int i = gtid; i < n; i += gthreads) {
     const int f64 = a.state_f64;
     V3<double> q, v, f;
@@ -280,13 +292,10 @@ __device__ bool diffpd_step_body(const DiffPdArgs& a, const Team team, char* dyn
     load_slice<double>(a.plan_s, a.s_val, dyn_smem, team.rank);
     load_slice<double>(a.plan_st, a.st_val, dyn_smem, team.rank);
   }
-  double* vector_smem = reinterpret_cast<double*>(dyn_smem + a.vector_smem_offset);
   const int r0 = a.st_part[team.rank], r1 = a.st_part[team.rank + 1];
-  int e0, e1;
-  team_range(a.ne, team, e0, e1);
-  int sequence = 0;
-  // ---- Stop threshold rel |(m/h^2 rhs) on the free rows| + abs.
-  double threshold;
+  start->r0 = r0;
+  start->r1 = r1;
+  team_range(a.ne, team, start->e0, start->e1);
   {
     double partial = 0.0;
     for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
@@ -297,14 +306,11 @@ __device__ bool diffpd_step_body(const DiffPdArgs& a, const Team team, char* dyn
     }
     const double values[1] = {block_sum(partial, s_scratch)};
     if (!dp_team_sum(a, team, sequence, values, 1, s_out, s_scratch)) return false;
-    threshold = a.rel_tol * sqrt(s_out[0]) + a.abs_tol;
+    start->threshold = a.rel_tol * sqrt(s_out[0]) + a.abs_tol;
   }
-  // ---- Objective and gradient at x = q.
-  double objective;
-  if (!dp_evaluate(a, team, e0, e1, r0, r1, sequence, &objective, s_out, s_scratch)) return false;
-  int iterations = 0;
-  bool singular = *reinterpret_cast<volatile int*>(a.counters + 1) != 0;
-  if (singular) atomicOr(a.status, kDpSingular);
+  if (!dp_evaluate(a, team, start->e0, start->e1, r0, r1, sequence, &start->objective, s_out, s_scratch)) return false;
+  start->singular = *reinterpret_cast<volatile int*>(a.counters + 1) != 0;
+  if (start->singular) atomicOr(a.status, kDpSingular);
   for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
     const V3<double> x = load3d(a.trial, i);
     store3(a.x, i, x);
@@ -312,6 +318,72 @@ __device__ bool diffpd_step_body(const DiffPdArgs& a, const Team team, char* dyn
     if (!a.free_[i]) g = v3<double>(0.0, 0.0, 0.0);
     store3(a.gradient, i, g);
   }
+  return true;
+}
+
+// Backtracking Armijo line search along -direction from x (the last trial is
+// accepted untested): trial = x - step d, halved until
+// Phi(trial) < Phi(x) - 1e-4 step slope + eps or a singular F stops it.
+__device__ __forceinline__ bool dp_line_search(const DiffPdArgs& a, const Team team, const DpStart& start,
+                                               int& sequence, double objective, double slope,
+                                               double* trial_objective, bool* singular, bool* failed, double* s_out,
+                                               double* s_scratch) {
+  double step = 1.0;
+  *failed = false;
+  for (int evaluations = 1;; ++evaluations) {
+    for (int i = start.r0 + threadIdx.x; i < start.r1; i += blockDim.x)
+      store3(a.trial, i, load3d(a.x, i) - step * load3d(a.direction, i));
+    if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
+    if (!dp_evaluate(a, team, start.e0, start.e1, start.r0, start.r1, sequence, trial_objective, s_out, s_scratch))
+      return false;
+    *singular = *reinterpret_cast<volatile int*>(a.counters + 1) != 0;
+    if (*singular) break;
+    if (evaluations > a.max_ls_iter) {
+      *failed = true;
+      break;
+    }
+    const double bound = objective - 1.0e-4 * step * slope;
+    if (!isnan(*trial_objective) && *trial_objective < bound + DBL_EPSILON) break;
+    step *= 0.5;
+  }
+  return true;
+}
+
+// write_state: the float64 results and the rounded state on the own rows.
+__device__ __forceinline__ void dp_write_state(const DiffPdArgs& a, const Team team, const DpStart& start,
+                                               int iterations) {
+  const double dt = a.dt;
+  for (int i = start.r0 + threadIdx.x; i < start.r1; i += blockDim.x) {
+    const V3<double> x = load3d(a.x, i);
+    const V3<double> v = (1.0 / dt) * (x - load3d(a.position, i));
+    store3(a.next_velocity, i, v);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      state_store(a.q_out, a.state_f64, 3 * i + c, x[c]);
+      state_store(a.qd_out, a.state_f64, 3 * i + c, (x[c] - a.position[3 * i + c]) / dt);
+    }
+  }
+  if (team.rank == 0 && threadIdx.x == 0) a.counters[0] = iterations;
+}
+
+// One DiffPD step by one team (solver.py:689-786 with the device loop of
+// kernels.py), the two-loop recursion as the reference writes it: one team
+// sum per pair in each loop. Returns false when a team barrier gave up.
+__device__ bool diffpd_step_body(const DiffPdArgs& a, const Team team, char* dyn_smem) {
+  __shared__ double s_scratch[kBlock];
+  __shared__ double s_out[64];
+  __shared__ double s_rho[kDiffPdMaxHistory];
+  __shared__ double s_alpha[kDiffPdMaxHistory];
+  const int n = a.n;
+  const int gtid = team.rank * blockDim.x + threadIdx.x;
+  int sequence = 0;
+  DpStart start;
+  if (!dp_begin_step(a, team, dyn_smem, sequence, s_out, s_scratch, &start)) return false;
+  double* vector_smem = reinterpret_cast<double*>(dyn_smem + a.vector_smem_offset);
+  const int r0 = start.r0, r1 = start.r1;
+  double objective = start.objective;
+  bool singular = start.singular;
+  int iterations = 0;
   const int m = a.history;
   int pairs = 0, newest = m - 1;
   while (!singular) {
@@ -390,24 +462,11 @@ __device__ bool diffpd_step_body(const DiffPdArgs& a, const Team team, char* dyn
           store3(a.direction, i, a.free_[i] ? load3d(a.gradient, i) : v3<double>(0.0, 0.0, 0.0));
       }
     }
-    // ---- Backtracking Armijo line search (the last trial is accepted untested).
-    double step = 1.0, trial_objective = objective;
+    double trial_objective = objective;
     bool failed = false;
-    for (int evaluations = 1;; ++evaluations) {
-      for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x)
-        store3(a.trial, i, load3d(a.x, i) - step * load3d(a.direction, i));
-      if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
-      if (!dp_evaluate(a, team, e0, e1, r0, r1, sequence, &trial_objective, s_out, s_scratch)) return false;
-      singular = *reinterpret_cast<volatile int*>(a.counters + 1) != 0;
-      if (singular) break;
-      if (evaluations > a.max_ls_iter) {
-        failed = true;
-        break;
-      }
-      const double bound = objective - 1.0e-4 * step * slope;
-      if (!isnan(trial_objective) && trial_objective < bound + DBL_EPSILON) break;
-      step *= 0.5;
-    }
+    if (!dp_line_search(a, team, start, sequence, objective, slope, &trial_objective, &singular, &failed, s_out,
+                        s_scratch))
+      return false;
     // ---- Accept the trial; gradient and its norm.
     objective = trial_objective;
     double gg = 0.0;
@@ -427,30 +486,230 @@ __device__ bool diffpd_step_body(const DiffPdArgs& a, const Team team, char* dyn
       if (gtid == 0) atomicOr(a.status, kDpSingular);
       break;
     }
-    if (sqrt(s_out[0]) <= threshold) break;
+    if (sqrt(s_out[0]) <= start.threshold) break;
     if (iterations >= a.max_pd_iter) {
       if (gtid == 0) atomicOr(a.status, kDpNotConverged);
       break;
     }
   }
-  // ---- write_state: the float64 results and the rounded state.
-  for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-    const V3<double> x = load3d(a.x, i);
-    const V3<double> v = (1.0 / dt) * (x - load3d(a.position, i));
-    store3(a.next_velocity, i, v);
+  dp_write_state(a, team, start, iterations);
+  return true;
+}
+
+// Team-wide sums of `count` (<= kDpWideGroup) dot products over the owned
+// rows, dot_of(k, i) being product k's term of row i: warp w of every block
+// takes products w, w + 8, ..., its lanes the rows in a fixed stride and a
+// fixed shuffle tree, lane 0 writes the block's partial into the wide slots;
+// then a team barrier and every block sums the slots of all blocks in the
+// same fixed order into `out`. Groups alternate as in dp_team_sum.
+template <typename DotOf>
+__device__ __forceinline__ bool dp_wide_sums(const DiffPdArgs& a, Team team, int& sequence, int count, int r0, int r1,
+                                             DotOf dot_of, double* out, double* scratch) {
+  const int base = (sequence & 1) * kDpWideGroup;
+  ++sequence;
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  for (int k = warp; k < count; k += kBlock / 32) {
+    double sum = 0.0;
+    for (int i = r0 + lane; i < r1; i += 32) sum += dot_of(k, i);
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      state_store(a.q_out, a.state_f64, 3 * i + c, x[c]);
-      state_store(a.qd_out, a.state_f64, 3 * i + c, (x[c] - a.position[3 * i + c]) / dt);
+    for (int offset = 16; offset > 0; offset >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, offset);
+    if (lane == 0) a.wide[(base + k) * team.size + team.rank] = sum;
+  }
+  if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
+  reduce_partials(a.wide, base, count, team.size, out, scratch);
+  return true;
+}
+
+// One DiffPD step by one team with the two-loop recursion in Gram form. The
+// block keeps G[i][j] = s_i . y_j of the stored pairs and sg_i = s_i . g in
+// shared memory; the first loop's s_i . r_i = sg_i - sum_{j newer} alpha_j
+// G[i][j] and the second loop's y_i . d_i = y_i . d_0 + sum_{j older} c_j
+// G[j][i] are scalar recurrences every block runs in the same order, r and the
+// direction are formed on the own rows in the reference's order (newest
+// first for r, oldest first for d), and the slope d . g is d_0 . g +
+// sum_j c_j sg_j. An iteration takes two batched team sums around the
+// inverse product (y_j . d_0, d_0 . g, g . g before the line search; g . g,
+// sg_j and the new Gram row and column after it) instead of one per pair and
+// loop. Same status bits, history and line search as diffpd_step_body; the
+// dot products are rounded in another order.
+__device__ bool diffpd_gram_body(const DiffPdArgs& a, const Team team, char* dyn_smem) {
+  __shared__ double s_scratch[kBlock];
+  __shared__ double s_out[kDpWideGroup];
+  __shared__ double s_gram[kDiffPdMaxHistory * kDiffPdMaxHistory];
+  __shared__ double s_rho[kDiffPdMaxHistory];
+  __shared__ double s_alpha[kDiffPdMaxHistory];
+  __shared__ double s_coef[kDiffPdMaxHistory];
+  __shared__ double s_sg[kDiffPdMaxHistory];
+  __shared__ double s_scalars[2];  // slope, g . g
+  const int n = a.n;
+  const int gtid = team.rank * blockDim.x + threadIdx.x;
+  int sequence = 0;
+  DpStart start;
+  if (!dp_begin_step(a, team, dyn_smem, sequence, s_out, s_scratch, &start)) return false;
+  double* vector_smem = reinterpret_cast<double*>(dyn_smem + a.vector_smem_offset);
+  const int r0 = start.r0, r1 = start.r1;
+  double objective = start.objective;
+  bool singular = start.singular;
+  int iterations = 0;
+  const int m = a.history;
+  int pairs = 0, newest = m - 1;
+  // Ring slot of the pair of a given age (0 = newest).
+  auto slot_of = [&](int age) { return (newest - age + m) % m; };
+  for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+    store3(a.x_last, i, load3d(a.x, i));
+    store3(a.g_last, i, load3d(a.gradient, i));
+  }
+  while (!singular) {
+    // ---- First loop: alpha_i = rho_i (sg_i - sum_{j newer} alpha_j G[i][j]), newest first.
+    if (threadIdx.x == 0) {
+      for (int age = 0; age < pairs; ++age) {
+        const int i = slot_of(age);
+        double sr = s_sg[i];
+        for (int newer = 0; newer < age; ++newer) {
+          const int j = slot_of(newer);
+          sr = sr - s_alpha[j] * s_gram[i * kDiffPdMaxHistory + j];
+        }
+        s_alpha[i] = s_rho[i] * sr;
+      }
+    }
+    __syncthreads();
+    // ---- r = g - alpha_j y_j, newest first, then d_0 = A^{-1} r.
+    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+      V3<double> r = load3d(a.gradient, i);
+      for (int age = 0; age < pairs; ++age) {
+        const int j = slot_of(age);
+        r = r - s_alpha[j] * load3d(a.y_hist + static_cast<size_t>(j) * 3 * n, i);
+      }
+      store3(a.r, i, r);
+    }
+    if (!grid_sync(a.barrier, a.status, team.size, team.rank)) return false;
+    if (!dp_apply_inverse<double>(a, team, dyn_smem, vector_smem)) return false;
+    // ---- y_j . d_0 by age, d_0 . g and g . g in one team sum.
+    {
+      auto dot_of = [&](int k, int i) {
+        const V3<double> d0 = load3d(a.direction, i);
+        if (k < pairs) return dot(load3d(a.y_hist + static_cast<size_t>(slot_of(k)) * 3 * n, i), d0);
+        const V3<double> g = load3d(a.gradient, i);
+        return k == pairs ? dot(d0, g) : dot(g, g);
+      };
+      if (!dp_wide_sums(a, team, sequence, pairs + 2, r0, r1, dot_of, s_out, s_scratch)) return false;
+    }
+    // ---- Second loop: c_i = alpha_i - rho_i (y_i . d_0 + sum_{j older} c_j G[j][i]), oldest first;
+    // slope = d_0 . g + sum_j c_j sg_j, oldest first.
+    if (threadIdx.x == 0) {
+      for (int age = pairs - 1; age >= 0; --age) {
+        const int i = slot_of(age);
+        double yd = s_out[age];
+        for (int older = pairs - 1; older > age; --older) {
+          const int j = slot_of(older);
+          yd = yd + s_coef[j] * s_gram[j * kDiffPdMaxHistory + i];
+        }
+        s_coef[i] = s_alpha[i] - s_rho[i] * yd;
+      }
+      double slope = s_out[pairs];
+      for (int age = pairs - 1; age >= 0; --age) slope = slope + s_coef[slot_of(age)] * s_sg[slot_of(age)];
+      s_scalars[0] = slope;
+      s_scalars[1] = s_out[pairs + 1];
+    }
+    __syncthreads();
+    // ---- Direction d_0 + c_j s_j (oldest first), or the masked gradient when it does not descend.
+    double slope = s_scalars[0];
+    const bool descends = slope > 0.0;
+    if (!descends) slope = s_scalars[1];
+    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+      V3<double> d;
+      if (descends) {
+        d = load3d(a.direction, i);
+        for (int age = pairs - 1; age >= 0; --age) {
+          const int j = slot_of(age);
+          d = d + s_coef[j] * load3d(a.s_hist + static_cast<size_t>(j) * 3 * n, i);
+        }
+      } else {
+        d = a.free_[i] ? load3d(a.gradient, i) : v3<double>(0.0, 0.0, 0.0);
+      }
+      store3(a.direction, i, d);
+    }
+    double trial_objective = objective;
+    bool failed = false;
+    if (!dp_line_search(a, team, start, sequence, objective, slope, &trial_objective, &singular, &failed, s_out,
+                        s_scratch))
+      return false;
+    // ---- Accept the trial; gradient, history push (s, y) = (x - x_last, g - g_last).
+    objective = trial_objective;
+    newest = (newest + 1) % m;
+    pairs = min(pairs + 1, m);
+    {
+      double* s_new = a.s_hist + static_cast<size_t>(newest) * 3 * n;
+      double* y_new = a.y_hist + static_cast<size_t>(newest) * 3 * n;
+      for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+        const V3<double> x = load3d(a.trial, i);
+        store3(a.x, i, x);
+        V3<double> g = a.inertia * (x - load3d(a.rhs, i)) - load3d(a.force, i);
+        if (!a.free_[i]) g = v3<double>(0.0, 0.0, 0.0);
+        store3(a.gradient, i, g);
+        store3(s_new, i, x - load3d(a.x_last, i));
+        store3(y_new, i, g - load3d(a.g_last, i));
+        store3(a.x_last, i, x);
+        store3(a.g_last, i, g);
+      }
+      // The products read rows that other threads of this block wrote.
+      __syncthreads();
+      // Products: 0 g . g; 1 + age: s_age . g; then for every older age the new Gram row
+      // s_new . y_age and column s_age . y_new; last y_new . s_new.
+      const int older = pairs - 1;
+      auto dot_of = [&](int k, int i) {
+        const V3<double> g = load3d(a.gradient, i);
+        if (k == 0) return dot(g, g);
+        if (k <= pairs) return dot(load3d(a.s_hist + static_cast<size_t>(slot_of(k - 1)) * 3 * n, i), g);
+        if (k <= pairs + older) {
+          const int j = slot_of(k - pairs);
+          return dot(load3d(s_new, i), load3d(a.y_hist + static_cast<size_t>(j) * 3 * n, i));
+        }
+        if (k <= pairs + 2 * older) {
+          const int j = slot_of(k - pairs - older);
+          return dot(load3d(a.s_hist + static_cast<size_t>(j) * 3 * n, i), load3d(y_new, i));
+        }
+        return dot(load3d(y_new, i), load3d(s_new, i));
+      };
+      if (!dp_wide_sums(a, team, sequence, 3 * pairs, r0, r1, dot_of, s_out, s_scratch)) return false;
+      if (threadIdx.x == 0) {
+        for (int age = 0; age < pairs; ++age) s_sg[slot_of(age)] = s_out[1 + age];
+        for (int age = 1; age <= older; ++age) {
+          const int j = slot_of(age);
+          s_gram[newest * kDiffPdMaxHistory + j] = s_out[pairs + age];
+          s_gram[j * kDiffPdMaxHistory + newest] = s_out[pairs + older + age];
+        }
+        const double ys = s_out[3 * pairs - 1];
+        s_gram[newest * kDiffPdMaxHistory + newest] = ys;
+        s_rho[newest] = 1.0 / ys;
+      }
+    }
+    const double gg = s_out[0];
+    __syncthreads();
+    if (failed && gtid == 0) atomicOr(a.status, kDpLineSearch);
+    iterations += 1;
+    if (singular) {
+      if (gtid == 0) atomicOr(a.status, kDpSingular);
+      break;
+    }
+    if (sqrt(gg) <= start.threshold) break;
+    if (iterations >= a.max_pd_iter) {
+      if (gtid == 0) atomicOr(a.status, kDpNotConverged);
+      break;
     }
   }
-  if (gtid == 0) a.counters[0] = iterations;
+  dp_write_state(a, team, start, iterations);
   return true;
 }
 
 __global__ void __launch_bounds__(kBlock) diffpd_step_kernel(const DiffPdArgs a) {
   extern __shared__ __align__(16) char dyn_smem[];
   diffpd_step_body(a, Team{static_cast<int>(blockIdx.x), static_cast<int>(gridDim.x)}, dyn_smem);
+}
+
+__global__ void __launch_bounds__(kBlock) diffpd_gram_kernel(const DiffPdArgs a) {
+  extern __shared__ __align__(16) char dyn_smem[];
+  diffpd_gram_body(a, Team{static_cast<int>(blockIdx.x), static_cast<int>(gridDim.x)}, dyn_smem);
 }
 
 }  // namespace pdb200
@@ -505,17 +764,22 @@ int pd_diffpd_step(PdSolver* s, const PdDiffPdOptions* o, const void* q, const v
     return dp_fail(PD_ERR_INVALID, "max_pd_iter >= 1, max_ls_iter >= 1 and bfgs_history_size in [2, 32] are required");
   if (!(o->abs_tol >= 0.0) || !(o->rel_tol >= 0.0) || !std::isfinite(o->abs_tol) || !std::isfinite(o->rel_tol))
     return dp_fail(PD_ERR_INVALID, "abs_tol and rel_tol must be finite and nonnegative");
+  if (o->recursion != PD_DIFFPD_TWO_LOOP && o->recursion != PD_DIFFPD_GRAM)
+    return dp_fail(PD_ERR_INVALID, "recursion must be PD_DIFFPD_TWO_LOOP or PD_DIFFPD_GRAM");
   if (!s->built || s->stale || s->built_dt != dt)
     return dp_fail(PD_ERR_STATE, "SolverDiffPD must rebuild its factor (pd_build) for this dt and model");
   PD_CUDA(cudaSetDevice(s->device));
   if (int status = pd_ensure_plan(s)) return status;
+  if (s->blocks > pdb200::kDpMaxBlocks) return dp_fail(PD_ERR_INVALID, "SolverDiffPD launches at most 256 blocks");
   // Every [n][3] vector starts on a 256-byte boundary: the products stage
   // their input vector into shared memory with 16-byte loads, and a stride of
   // 3n doubles would leave odd slots only 8-byte aligned.
   const size_t vec = dp_vector_stride(s->n);
   constexpr int kVectors = 13;
+  // After the vectors: the wide partial slots of the Gram recursion.
+  const size_t wide = static_cast<size_t>(2) * pdb200::kDpWideGroup * pdb200::kDpMaxBlocks;
   if (s->dp_vectors.ptr == nullptr) {
-    PD_CUDA(s->dp_vectors.allocate(kVectors * vec * sizeof(double)));
+    PD_CUDA(s->dp_vectors.allocate((kVectors * vec + wide) * sizeof(double)));
     PD_CUDA(s->dp_energy.allocate(static_cast<size_t>(s->ne) * sizeof(double)));
     PD_CUDA(s->dp_counters.allocate(4 * sizeof(int)));
   }
@@ -551,6 +815,7 @@ int pd_diffpd_step(PdSolver* s, const PdDiffPdOptions* o, const void* q, const v
   double** slots[kVectors] = {&a.position, &a.velocity, &a.rhs,    &a.x,      &a.trial,  &a.force,        &a.gradient,
                               &a.direction, &a.r,       &a.x_last, &a.g_last, &a.product, &a.next_velocity};
   for (int k = 0; k < kVectors; ++k) *slots[k] = v + k * vec;
+  a.wide = v + kVectors * vec;
   a.s_hist = s->dp_hist.as<double>();
   a.y_hist = a.s_hist + static_cast<size_t>(o->history) * vec;
   a.energy = s->dp_energy.as<double>();
@@ -581,18 +846,18 @@ int pd_diffpd_step(PdSolver* s, const PdDiffPdOptions* o, const void* q, const v
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   PD_CUDA(cudaMemsetAsync(s->d_barrier.ptr, 0, sizeof(pdb200::GridBarrier), st));
   if (s->spin_limit != 0u) PD_CUDA(pdb200::launch_set_spin_limit(a.barrier, s->spin_limit, st));
+  const void* kernel = o->recursion == PD_DIFFPD_GRAM ? reinterpret_cast<const void*>(&pdb200::diffpd_gram_kernel)
+                                                      : reinterpret_cast<const void*>(&pdb200::diffpd_step_kernel);
   {
     int optin = 0;
     PD_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, s->device));
     cudaFuncAttributes attributes{};
-    PD_CUDA(cudaFuncGetAttributes(&attributes, reinterpret_cast<const void*>(&pdb200::diffpd_step_kernel)));
-    PD_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(&pdb200::diffpd_step_kernel),
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+    PD_CUDA(cudaFuncGetAttributes(&attributes, kernel));
+    PD_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  optin - static_cast<int>(attributes.sharedSizeBytes)));
   }
   void* params[] = {&a};
-  PD_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(&pdb200::diffpd_step_kernel), dim3(s->blocks),
-                                      dim3(pdb200::kBlock), params, s->smem, st));
+  PD_CUDA(cudaLaunchCooperativeKernel(kernel, dim3(s->blocks), dim3(pdb200::kBlock), params, s->smem, st));
   return PD_OK;
 }
 

@@ -78,6 +78,13 @@ class SolverDiffPD:
     rest volume ``Vbar``, the energy weights are global scalars, gravity and
     the contacts are explicit state forces of the start-of-step state, and
     particles with zero inverse mass are held at their start positions.
+
+    Added keywords: ``blocks`` (persistent grid size, 0 = automatic) and
+    ``recursion``: ``"two_loop"`` runs the reference's two loops (one team
+    sum per stored pair and loop); ``"gram"`` runs the same recursion from
+    the Gram matrix ``s_i . y_j`` of the stored pairs and the products
+    ``s_i . g`` (two batched team sums per iteration), with its dot products
+    rounded in another order.
     """
 
     ConvergenceError = ConvergenceError
@@ -85,7 +92,7 @@ class SolverDiffPD:
     def __init__(self, model, *, density: float, corotated_stiffness: float | None = None,
                  volume_stiffness: float | None = None, state_forces=(), gravity=None, rest_positions=None,
                  max_pd_iter: int = 4000, max_ls_iter: int = 10, abs_tol: float = 1.0e-9, rel_tol: float = 1.0e-4,
-                 bfgs_history_size: int = 10, blocks: int = 0):
+                 bfgs_history_size: int = 10, blocks: int = 0, recursion: str = "two_loop"):
         if model.tet_count == 0 or model.particle_count == 0:
             raise ValueError("SolverDiffPD requires tetrahedral soft bodies")
         if getattr(model, "body_count", 0) or getattr(model, "hex_count", 0):
@@ -103,6 +110,9 @@ class SolverDiffPD:
         self.bfgs_history_size = _positive_integer("bfgs_history_size", bfgs_history_size, 2)
         if self.bfgs_history_size > 32:
             raise ValueError("bfgs_history_size must be at most 32")
+        if recursion not in ("two_loop", "gram"):
+            raise ValueError("recursion must be 'two_loop' or 'gram'")
+        self.recursion = recursion
         self.abs_tol = float(abs_tol)
         self.rel_tol = float(rel_tol)
         self.corotated_stiffness = None if corotated_stiffness is None else float(corotated_stiffness)
@@ -262,7 +272,8 @@ class SolverDiffPD:
         return _lib.PdDiffPdOptions(self.max_pd_iter, self.max_ls_iter, self.bfgs_history_size,
                                     int(self.corotated_stiffness is not None), int(self.volume_stiffness is not None),
                                     self.corotated_stiffness or 0.0, self.volume_stiffness or 0.0, self.abs_tol,
-                                    self.rel_tol)
+                                    self.rel_tol,
+                                    _lib.DIFFPD_GRAM if self.recursion == "gram" else _lib.DIFFPD_TWO_LOOP)
 
     def step(self, state_in, state_out, control, contacts, dt: float) -> None:
         """Advance one step of length ``dt`` [s] on the current CUDA stream."""
