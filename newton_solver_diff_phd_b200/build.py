@@ -67,7 +67,7 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     for source in HOST_SOURCES:
         obj = BUILD / (source + ".o")
         if force or _stale(obj, [CSRC / source, *headers]):
-            commands.append(["g++", "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math",
+            commands.append(["g++", "-std=c++17", "-O3", "-fPIC", "-ffp-contract=off", "-fno-fast-math",
                              "-c", str(CSRC / source), "-o", str(obj)])
         objects.append(obj)
     # Translation units compile side by side (the slowest one bounds the build).

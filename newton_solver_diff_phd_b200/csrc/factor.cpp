@@ -13,6 +13,7 @@
 #include <atomic>
 #include <cmath>
 #include <condition_variable>
+#include <cstddef>
 #include <cstdint>
 #include <functional>
 #include <limits>
@@ -374,118 +375,206 @@ void ldlt_left_looking(int32_t size, const std::vector<int64_t>& row_start, cons
   }
 }
 
-// Rows of L^{-1} over host threads, level by level of the elimination tree
-// (rows of a level are independent; row i reads rows k < i of lower levels).
-// Each row's label range is cut into kLevelChunk-label chunks aligned to
-// multiples of kLevelChunk, and every (row, chunk) item is one task: it walks
-// row i's columns k in ascending order and subtracts L(i, k) times row k's
-// entries inside the chunk, located through the chunk bounds stored with
-// row k. Every entry therefore sees the host walk's sequence of rounded
-// operations (one multiply, then one subtract, per k in ascending order) and
-// exact zeros are omitted the same way: the rows are bit-identical. The top
-// of the tree, one long row per level, is spread over the threads chunk by
-// chunk instead of column range by column range.
-void inverse_rows_by_levels(const LowerFactorView& f, InverseRows* out, RowPool& pool) {
-  constexpr int32_t kLevelChunk = 1024;
+// dst[u] = dst[u] - coefficient * src[u] over `count` entries: one rounded
+// multiply, then one rounded subtract per entry (no contraction), so every
+// entry sees the host walk's operations; lanes are independent, so vector
+// code gives the same bits. Compiled for AVX2 and the baseline, chosen at
+// load time.
+__attribute__((target_clones("avx2", "default"))) static void subtract_scaled(double* __restrict dst,
+                                                                       const double* __restrict src,
+                                                                       double coefficient, int32_t count) {
+  for (int32_t u = 0; u < count; ++u) {
+    const double product = coefficient * src[u];
+    dst[u] = dst[u] - product;
+  }
+}
+
+// Rows of L^{-1} over host threads in groups of consecutive rows. Row i of
+// L^{-1} is nonzero only on the labels [lo_i, i] of its elimination subtree
+// (lo_i = min(i, lo_k over its columns k)); with the nested-dissection order
+// that range is almost fully dense, so rows are stored as dense segments and
+// row i's update by row k is a contiguous subtract over row k's range, which
+// lies inside row i's. Rows that share most of their columns form a group
+// (up to kGroupRows consecutive rows): per column chunk of kGroupChunk labels
+// the group applies each outside column k (k below the group's first row, in
+// ascending order) to all its rows that hold it, so row k's chunk is read
+// once for the group, then its own rows in ascending order. Each entry of a
+// row therefore sees its columns k in ascending order, one multiply and one
+// subtract each, and zero multipliers are skipped as in the walk; updates by
+// row k's exact zeros subtract signed zeros, which leave every nonzero value
+// unchanged, and exact zeros are omitted at the end: the rows are
+// bit-identical to the walk's. Groups are scheduled level by level (a group
+// reads only groups of lower levels) as (group, chunk) tasks. Returns false
+// without computing when the dense segments would hold more than twice the
+// rows' structural entries (an order far from a postorder).
+bool inverse_rows_by_groups(const LowerFactorView& f, InverseRows* out, RowPool& pool) {
+  constexpr int32_t kGroupChunk = 256;
+  constexpr int32_t kGroupRows = 32;
+  constexpr double kShare = 0.5;  // a row joins when half its outside columns are the group's
   const int32_t n = f.size;
-  std::vector<int32_t> level(n, 0), lo(n);
-  int32_t levels = 0;
+  std::vector<int32_t> lo(n), parent(n, -1);
+  std::vector<int64_t> subtree(n, 1);
   for (int32_t i = 0; i < n; ++i) {
-    int32_t l = 0, low = i;
+    int32_t low = i;
     for (int64_t p = f.row_start[i]; p < f.row_start[i + 1] - 1; ++p) {
       const int32_t k = f.pattern[p];
-      l = std::max(l, level[k] + 1);
       low = std::min(low, lo[k]);
+      if (parent[k] < 0) parent[k] = i;
     }
-    level[i] = l;
     lo[i] = low;
-    levels = std::max(levels, l + 1);
+  }
+  int64_t structural = 0;
+  for (int32_t k = 0; k < n; ++k) {
+    structural += subtree[k];
+    if (parent[k] >= 0) subtree[parent[k]] += subtree[k];
+  }
+  std::vector<int64_t> base(static_cast<size_t>(n) + 1, 0);
+  for (int32_t i = 0; i < n; ++i) base[i + 1] = base[i] + (i - lo[i] + 1);
+  if (base[n] > 2 * structural) return false;
+  std::vector<double> dense(static_cast<size_t>(base[n]));
+
+  // Groups of consecutive rows.
+  std::vector<int32_t> group_start(1, 0), group_of(n);
+  {
+    std::vector<int32_t> mark(n, -1);
+    int32_t a = 0;
+    for (int32_t r = 0; r < n; ++r) {
+      if (r > a) {
+        int32_t outside = 0, shared = 0;
+        for (int64_t p = f.row_start[r]; p < f.row_start[r + 1] - 1; ++p) {
+          const int32_t k = f.pattern[p];
+          if (k < a) {
+            ++outside;
+            shared += mark[k] == a;
+          }
+        }
+        if (r - a >= kGroupRows || shared < kShare * outside) {
+          a = r;
+          group_start.push_back(r);
+        }
+      }
+      for (int64_t p = f.row_start[r]; p < f.row_start[r + 1] - 1; ++p) {
+        const int32_t k = f.pattern[p];
+        if (k < a) mark[k] = a;
+      }
+      group_of[r] = static_cast<int32_t>(group_start.size()) - 1;
+    }
+    group_start.push_back(n);
+  }
+  const int32_t groups = static_cast<int32_t>(group_start.size()) - 1;
+  // Per group: its outside columns U ascending, multipliers outer[u][r] and
+  // inner[r][kk] (row a + r, column u or a + kk; zero where the row lacks it),
+  // the lowest label of its rows and its level.
+  std::vector<int64_t> u_start(static_cast<size_t>(groups) + 1, 0), outer_start(static_cast<size_t>(groups) + 1, 0),
+      inner_start(static_cast<size_t>(groups) + 1, 0);
+  std::vector<int32_t> u_cols, group_lo(groups), level(groups, 0);
+  std::vector<double> outer, inner;
+  int32_t levels = 0;
+  {
+    std::vector<int32_t> seen(n, -1);
+    for (int32_t g = 0; g < groups; ++g) {
+      const int32_t a = group_start[g], b = group_start[g + 1], rows = b - a;
+      const size_t u0 = u_cols.size();
+      int32_t low = a;
+      for (int32_t r = a; r < b; ++r) {
+        low = std::min(low, lo[r]);
+        for (int64_t p = f.row_start[r]; p < f.row_start[r + 1] - 1; ++p) {
+          const int32_t k = f.pattern[p];
+          if (k < a && seen[k] != g) {
+            seen[k] = g;
+            u_cols.push_back(k);
+          }
+        }
+      }
+      std::sort(u_cols.begin() + static_cast<std::ptrdiff_t>(u0), u_cols.end());
+      group_lo[g] = low;
+      int32_t l = 0;
+      for (size_t u = u0; u < u_cols.size(); ++u) l = std::max(l, level[group_of[u_cols[u]]] + 1);
+      level[g] = l;
+      levels = std::max(levels, l + 1);
+      u_start[g + 1] = static_cast<int64_t>(u_cols.size());
+      const size_t o0 = outer.size(), i0 = inner.size();
+      outer.resize(o0 + (u_cols.size() - u0) * rows, 0.0);
+      inner.resize(i0 + static_cast<size_t>(rows) * rows, 0.0);
+      for (int32_t r = a; r < b; ++r) {
+        for (int64_t p = f.row_start[r]; p < f.row_start[r + 1] - 1; ++p) {
+          const int32_t k = f.pattern[p];
+          if (k < a) {
+            const size_t u = std::lower_bound(u_cols.begin() + static_cast<std::ptrdiff_t>(u0), u_cols.end(), k) -
+                             (u_cols.begin() + static_cast<std::ptrdiff_t>(u0));
+            outer[o0 + u * rows + (r - a)] = f.values[p];
+          } else {
+            inner[i0 + static_cast<size_t>(r - a) * rows + (k - a)] = f.values[p];
+          }
+        }
+      }
+      outer_start[g + 1] = static_cast<int64_t>(outer.size());
+      inner_start[g + 1] = static_cast<int64_t>(inner.size());
+    }
   }
   std::vector<int32_t> level_count(static_cast<size_t>(levels) + 1, 0);
-  for (int32_t i = 0; i < n; ++i) level_count[level[i] + 1] += 1;
+  for (int32_t g = 0; g < groups; ++g) level_count[level[g] + 1] += 1;
   for (int32_t l = 0; l < levels; ++l) level_count[l + 1] += level_count[l];
-  std::vector<int32_t> by_level(n);
+  std::vector<int32_t> by_level(groups);
   {
     std::vector<int32_t> cursor(level_count.begin(), level_count.end() - 1);
-    for (int32_t i = 0; i < n; ++i) by_level[cursor[level[i]]++] = i;
+    for (int32_t g = 0; g < groups; ++g) by_level[cursor[level[g]]++] = g;
   }
-  // Computed rows live in one pool (in level order): row i starts at
-  // row_off[i]; its chunk bounds, relative to that start, at
-  // bounds[bounds_base[i] + (chunk - lo[i] / kLevelChunk)].
-  std::vector<int64_t> bounds_base(n);
-  int64_t bounds_total = 0;
-  for (int32_t i = 0; i < n; ++i) {
-    bounds_base[i] = bounds_total;
-    bounds_total += (i / kLevelChunk - lo[i] / kLevelChunk) + 2;
-  }
-  std::vector<int32_t> bounds(static_cast<size_t>(bounds_total), 0);
-  std::vector<int64_t> row_off(n, 0), row_len(n, 0);
-  std::vector<int32_t> pool_cols;
-  std::vector<double> pool_vals;
+
   struct Item {
-    int32_t row, chunk;
-    int64_t slot;  // offset of the item's scratch slot
+    int32_t group, chunk;
   };
   std::vector<Item> items;
-  std::vector<int32_t> item_count, scratch_cols;
-  std::vector<double> scratch_vals;
+  std::vector<std::vector<double>> tiles(pool.size(), std::vector<double>(static_cast<size_t>(kGroupRows) * kGroupChunk));
+  double* d = dense.data();
   for (int32_t l = 0; l < levels; ++l) {
     items.clear();
-    int64_t slots = 0;
-    for (int32_t r = level_count[l]; r < level_count[l + 1]; ++r) {
-      const int32_t i = by_level[r];
-      for (int32_t j = lo[i] / kLevelChunk; j <= i / kLevelChunk; ++j) {
-        const int32_t c_begin = std::max(lo[i], j * kLevelChunk);
-        const int32_t c_end = std::min(i, (j + 1) * kLevelChunk - 1) + 1;
-        items.push_back(Item{i, j, slots});
-        slots += c_end - c_begin;
-      }
+    for (int32_t q = level_count[l]; q < level_count[l + 1]; ++q) {
+      const int32_t g = by_level[q];
+      for (int32_t j = group_lo[g] / kGroupChunk; j <= (group_start[g + 1] - 1) / kGroupChunk; ++j)
+        items.push_back(Item{g, j});
     }
     const int64_t count = static_cast<int64_t>(items.size());
-    item_count.assign(static_cast<size_t>(count), 0);
-    if (static_cast<int64_t>(scratch_cols.size()) < slots) {
-      scratch_cols.resize(static_cast<size_t>(slots));
-      scratch_vals.resize(static_cast<size_t>(slots));
-    }
     std::atomic<int64_t> next{0};
-    const int32_t* pcols = pool_cols.data();
-    const double* pvals = pool_vals.data();
-    auto work = [&](unsigned) {
-      double acc[kLevelChunk];
+    auto work = [&](unsigned w) {
+      double* tile = tiles[w].data();
       for (int64_t t = next.fetch_add(1); t < count; t = next.fetch_add(1)) {
-        const int32_t i = items[t].row;
-        const int32_t j = items[t].chunk;
-        const int32_t c_begin = std::max(lo[i], j * kLevelChunk);
-        const int32_t c_end = std::min(i, (j + 1) * kLevelChunk - 1) + 1;
-        const int32_t width = c_end - c_begin;
-        std::fill(acc, acc + width, 0.0);
-        if (i >= c_begin && i < c_end) acc[i - c_begin] = 1.0;
-        for (int64_t p = f.row_start[i]; p < f.row_start[i + 1] - 1; ++p) {
-          const int32_t k = f.pattern[p];
-          const double coefficient = f.values[p];
-          if (coefficient == 0.0) continue;
-          const int32_t j0 = lo[k] / kLevelChunk;
-          if (j < j0 || j > k / kLevelChunk) continue;
-          const int32_t* b = bounds.data() + bounds_base[k] + (j - j0);
-          const int64_t first = row_off[k] + b[0];
-          const int64_t last = row_off[k] + b[1];
-          for (int64_t q = first; q < last; ++q) {
-            const int32_t c = pcols[q] - c_begin;
-            const double product = coefficient * pvals[q];
-            acc[c] = acc[c] - product;
+        const int32_t g = items[t].group;
+        const int32_t a = group_start[g], rows = group_start[g + 1] - a;
+        const int32_t c0 = items[t].chunk * kGroupChunk, c1 = c0 + kGroupChunk;
+        auto row_of = [&](int32_t r) { return tile + static_cast<size_t>(r) * kGroupChunk; };
+        for (int32_t r = 0; r < rows; ++r) {
+          std::fill(row_of(r), row_of(r) + kGroupChunk, 0.0);
+          if (a + r >= c0 && a + r < c1) row_of(r)[a + r - c0] = 1.0;
+        }
+        const double* multipliers = outer.data() + outer_start[g];
+        for (int64_t u = u_start[g]; u < u_start[g + 1]; ++u) {
+          const int32_t k = u_cols[u];
+          const int32_t from = std::max(lo[k], c0), to = std::min(k + 1, c1);
+          if (from >= to) continue;
+          const double* source = d + base[k] + (from - lo[k]);
+          const double* column = multipliers + (u - u_start[g]) * rows;
+          for (int32_t r = 0; r < rows; ++r) {
+            if (column[r] == 0.0) continue;
+            subtract_scaled(row_of(r) + (from - c0), source, column[r], to - from);
           }
         }
-        int32_t* oc = scratch_cols.data() + items[t].slot;
-        double* ov = scratch_vals.data() + items[t].slot;
-        int32_t kept = 0;
-        for (int32_t u = 0; u < width; ++u) {
-          if (acc[u] != 0.0) {
-            oc[kept] = c_begin + u;
-            ov[kept] = acc[u];
-            ++kept;
+        const double* own = inner.data() + inner_start[g];
+        for (int32_t kk = 0; kk + 1 < rows; ++kk) {
+          const int32_t k = a + kk;
+          const int32_t from = std::max(lo[k], c0), to = std::min(k + 1, c1);
+          if (from >= to) continue;
+          for (int32_t r = kk + 1; r < rows; ++r) {
+            const double coefficient = own[static_cast<size_t>(r) * rows + kk];
+            if (coefficient == 0.0) continue;
+            subtract_scaled(row_of(r) + (from - c0), row_of(kk) + (from - c0), coefficient, to - from);
           }
         }
-        item_count[t] = kept;
+        for (int32_t r = 0; r < rows; ++r) {
+          const int32_t i = a + r;
+          const int32_t from = std::max(lo[i], c0), to = std::min(i + 1, c1);
+          if (from < to) std::copy(row_of(r) + (from - c0), row_of(r) + (to - c0), d + base[i] + (from - lo[i]));
+        }
       }
     };
     if (count > 1) {
@@ -493,43 +582,40 @@ void inverse_rows_by_levels(const LowerFactorView& f, InverseRows* out, RowPool&
     } else {
       work(0);
     }
-    // Append the level's rows to the pool (items of a row are consecutive, in
-    // ascending chunks) and record their offsets and chunk bounds.
-    int64_t added = 0;
-    for (int64_t t = 0; t < count; ++t) added += item_count[t];
-    const int64_t base = static_cast<int64_t>(pool_cols.size());
-    pool_cols.resize(static_cast<size_t>(base + added));
-    pool_vals.resize(static_cast<size_t>(base + added));
-    int64_t at = base;
-    for (int64_t t = 0; t < count;) {
-      const int32_t i = items[t].row;
-      row_off[i] = at;
-      int32_t* b = bounds.data() + bounds_base[i];
-      int32_t within = 0;
-      int32_t slot = 0;
-      for (; t < count && items[t].row == i; ++t, ++slot) {
-        b[slot] = within;
-        std::copy(scratch_cols.begin() + items[t].slot, scratch_cols.begin() + items[t].slot + item_count[t],
-                  pool_cols.begin() + at);
-        std::copy(scratch_vals.begin() + items[t].slot, scratch_vals.begin() + items[t].slot + item_count[t],
-                  pool_vals.begin() + at);
-        at += item_count[t];
-        within += item_count[t];
-      }
-      b[slot] = within;
-      row_len[i] = within;
-    }
   }
+
+  // Compaction over row ranges: exact zeros omitted, columns ascending.
   out->start.assign(static_cast<size_t>(n) + 1, 0);
-  for (int32_t i = 0; i < n; ++i) out->start[i + 1] = out->start[i] + row_len[i];
+  const unsigned workers = pool.size();
+  auto ranges = [&](const std::function<void(int32_t, int32_t)>& body) {
+    pool.run([&](unsigned w) {
+      body(static_cast<int32_t>(static_cast<int64_t>(n) * w / workers),
+           static_cast<int32_t>(static_cast<int64_t>(n) * (w + 1) / workers));
+    });
+  };
+  ranges([&](int32_t r0, int32_t r1) {
+    for (int32_t i = r0; i < r1; ++i) {
+      int64_t kept = 0;
+      for (int64_t q = base[i]; q < base[i + 1]; ++q) kept += d[q] != 0.0;
+      out->start[i + 1] = kept;
+    }
+  });
+  for (int32_t i = 0; i < n; ++i) out->start[i + 1] += out->start[i];
   out->columns.resize(static_cast<size_t>(out->start[n]));
   out->values.resize(static_cast<size_t>(out->start[n]));
-  for (int32_t i = 0; i < n; ++i) {
-    std::copy(pool_cols.begin() + row_off[i], pool_cols.begin() + row_off[i] + row_len[i],
-              out->columns.begin() + out->start[i]);
-    std::copy(pool_vals.begin() + row_off[i], pool_vals.begin() + row_off[i] + row_len[i],
-              out->values.begin() + out->start[i]);
-  }
+  ranges([&](int32_t r0, int32_t r1) {
+    for (int32_t i = r0; i < r1; ++i) {
+      int64_t at = out->start[i];
+      for (int64_t q = base[i]; q < base[i + 1]; ++q) {
+        if (d[q] != 0.0) {
+          out->columns[at] = lo[i] + static_cast<int32_t>(q - base[i]);
+          out->values[at] = d[q];
+          ++at;
+        }
+      }
+    }
+  });
+  return true;
 }
 
 std::string build_inverse_factor(int32_t size, const int32_t* row_offsets, const int32_t* row_columns,
@@ -770,14 +856,15 @@ std::string build_inverse_factor(int32_t size, const int32_t* row_offsets, const
     view.values = values.data();
     InverseRows rows_out;
     RowPool level_pool(hardware);
-    inverse_rows_by_levels(view, &rows_out, level_pool);
-    if (rows_out.columns.size() > static_cast<size_t>(std::numeric_limits<int32_t>::max())) {
-      return "inverse factor fill exceeds int32 sparse indexing";
+    if (inverse_rows_by_groups(view, &rows_out, level_pool)) {
+      if (rows_out.columns.size() > static_cast<size_t>(std::numeric_limits<int32_t>::max())) {
+        return "inverse factor fill exceeds int32 sparse indexing";
+      }
+      inv_start = std::move(rows_out.start);
+      inv_columns = std::move(rows_out.columns);
+      inv_values = std::move(rows_out.values);
+      rows_done = true;
     }
-    inv_start = std::move(rows_out.start);
-    inv_columns = std::move(rows_out.columns);
-    inv_values = std::move(rows_out.values);
-    rows_done = true;
   }
   std::vector<double> current(rows_done ? 0 : size, 0.0);
   std::vector<int32_t> touched_mark(rows_done ? 0 : size, -1);

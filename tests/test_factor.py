@@ -163,9 +163,9 @@ def test_threaded_ldlt_is_bit_identical_to_reference(name):
 
 def test_threaded_ldlt_matches_the_sequential_loop_and_its_errors():
     """A 2,541-row Hex8 beam (hundreds of elimination-tree levels, separator chains at the top,
-    rows spanning several 1,024-label chunks): the level-parallel LDL^T and inverse rows give the
-    sequential loops' arrays bit for bit; an indefinite matrix fails with the same message both
-    ways."""
+    rows spanning several 256-label chunks, groups of up to 32 rows): the level-parallel LDL^T and
+    the grouped inverse rows give the sequential loops' arrays bit for bit; an indefinite matrix
+    fails with the same message both ways."""
     import scipy.sparse as sp
 
     from newton_solver_diff_phd_b200 import meshes

@@ -1,10 +1,13 @@
 """The level-by-level algorithms of the factor build, restated in Python on the CPU.
 
-``csrc/pd_factor_device.cu`` (and the threaded host path of ``csrc/factor.cpp``)
-compute the numeric LDL^T as left-looking columns and the rows of L^{-1} in
-label chunks, level by level of the elimination tree. These tests restate the
-two schedules step for step (levels, label ranges, chunk bounds recorded per
-stored row, merge order) and check that they reproduce the sequential
+``csrc/pd_factor_device.cu`` computes the numeric LDL^T as left-looking columns
+(as the threaded host path of ``csrc/factor.cpp`` does) and the rows of L^{-1}
+in label chunks, level by level of the elimination tree; the host computes
+the rows of L^{-1} as dense segments in groups of consecutive rows. These
+tests restate the three schedules step for step (levels, label ranges, chunk
+bounds recorded per stored row, merge order; group formation, outside
+columns before the group's own rows, zero multipliers skipped, updates by
+exact zeros, compaction) and check that they reproduce the sequential
 right-looking factorisation and row walk of ``oracle/factor_port.py`` bit for
 bit, for chunk widths from one label (every row split everywhere) to wider
 than the matrix. The CUDA kernels themselves are checked against the host
@@ -83,6 +86,48 @@ def chunked_rows(lower, width):
     return [stored[i] for i in range(len(lower))]
 
 
+def grouped_rows(lower, width, group_rows, share):
+    """Dense segments [lo_i, i] per row; groups of consecutive rows; per (group, chunk): the
+    outside columns ascending over every row holding them, then the group's own rows."""
+    n = len(lower)
+    _, lo = levels_of(lower)
+    starts, a, mark = [0], 0, {}
+    for r in range(1, n):
+        outside = [k for k in lower[r] if k < a]
+        shared = sum(mark.get(k) == a for k in outside)
+        if r - a >= group_rows or shared < share * len(outside):
+            a = r
+            starts.append(r)
+        for k in lower[r]:
+            if k < a:
+                mark[k] = a
+    starts.append(n)
+    dense = {}
+    for a, b in zip(starts[:-1], starts[1:]):  # consecutive groups: every outside row is done
+        union = sorted({k for r in range(a, b) for k in lower[r] if k < a})
+        for j in range(min(lo[a:b]) // width, (b - 1) // width + 1):
+            c0, c1 = j * width, (j + 1) * width
+            tile = {r: [1.0 if c0 + t == r else 0.0 for t in range(width)] for r in range(a, b)}
+            for k in union + list(range(a, b - 1)):
+                source = dense[k] if k < a else None
+                for r in range(max(a, k + 1), b):
+                    coefficient = lower[r].get(k, 0.0)
+                    if coefficient == 0.0:
+                        continue
+                    for c in range(max(lo[k], c0), min(k + 1, c1)):
+                        value = source[c - lo[k]] if k < a else tile[k][c - c0]
+                        tile[r][c - c0] = tile[r][c - c0] - coefficient * value
+            for r in range(a, b):
+                segment = dense.setdefault(r, [0.0] * (r - lo[r] + 1))
+                for c in range(max(lo[r], c0), min(r + 1, c1)):
+                    segment[c - lo[r]] = tile[r][c - c0]
+    rows = []
+    for i in range(n):
+        kept = [(lo[i] + u, value) for u, value in enumerate(dense[i]) if value != 0.0]
+        rows.append(([c for c, _ in kept], [value for _, value in kept]))
+    return rows
+
+
 def left_looking(csr, permutation, lower):
     """Columns level by level: entry (i, j) = A(i, j) - sum m(i, k) e(j, k) over shared k, ascending."""
     n = len(lower)
@@ -130,3 +175,12 @@ def test_left_looking_columns_reproduce_the_right_looking_factor():
     for i, row in enumerate(lower):
         for k, value in row.items():
             assert multiplier[(i, k)] == value
+
+
+@pytest.mark.parametrize("width, group_rows, share", [(1, 32, 0.5), (7, 4, 0.5), (64, 32, 0.0), (4096, 2, 1.0)])
+def test_grouped_dense_rows_reproduce_the_row_walk(width, group_rows, share):
+    _, _, lower, _ = beam(6, 3, 3)
+    walk = row_walk(lower)
+    for (cols, vals), (ref_cols, ref_vals) in zip(grouped_rows(lower, width, group_rows, share), walk):
+        assert cols == ref_cols
+        assert np.array_equal(np.asarray(vals), np.asarray(ref_vals))
