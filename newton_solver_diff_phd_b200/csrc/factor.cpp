@@ -303,12 +303,37 @@ void ldlt_left_looking(int32_t size, const std::vector<int64_t>& row_start, cons
   std::vector<double> unscaled(values.size(), 0.0);
   std::vector<int64_t> first_entry;  // per column of the level: its first flat entry
   const unsigned workers = pool.size();
+  // Levels of at most kDenseColumns columns with at least kDenseEntries
+  // entries (the top of the tree) scatter each column's row j into a dense
+  // array over the labels, so an entry (i, j) walks row i alone: its columns
+  // k < j that row j lacks read a zero, and subtracting a signed zero leaves
+  // every nonzero value unchanged (an entry that is exactly zero may change
+  // the sign of its zero; zero multipliers are skipped by the rows of L^{-1}).
+  // The dense arrays take at most 2^24 doubles.
+  const int32_t kDenseColumns =
+      static_cast<int32_t>(std::min<int64_t>(64, std::max<int64_t>(1, (int64_t{1} << 24) / std::max(size, 1))));
+  constexpr int64_t kDenseEntries = 256;
+  std::vector<double> dense_rows;
+  std::vector<int32_t> dense_slot(size, -1);
   for (int32_t l = 0; l < levels; ++l) {
     const int32_t c0 = level_count[l], c1 = level_count[l + 1];
     first_entry.assign(1, 0);
     for (int32_t c = c0; c < c1; ++c)
       first_entry.push_back(first_entry.back() + static_cast<int64_t>(columns[by_level[c]].size()) + 1);
     const int64_t total = first_entry.back();
+    const bool dense = c1 - c0 <= kDenseColumns && total >= kDenseEntries;
+    auto scatter_rows = [&](bool clear) {
+      for (int32_t c = c0; c < c1; ++c) {
+        const int32_t j = by_level[c];
+        double* row = dense_rows.data() + static_cast<size_t>(c - c0) * size;
+        dense_slot[j] = c - c0;
+        for (int64_t q = row_start[j]; q < row_start[j + 1] - 1; ++q) row[pattern[q]] = clear ? 0.0 : unscaled[q];
+      }
+    };
+    if (dense) {
+      if (dense_rows.empty()) dense_rows.assign(static_cast<size_t>(kDenseColumns) * size, 0.0);
+      scatter_rows(false);
+    }
     const int64_t chunk = std::max<int64_t>(16, total / (4 * static_cast<int64_t>(workers)) + 1);
     // Entry e of the level's c-th column: 0 is the diagonal, e >= 1 row columns[j][e - 1].
     auto for_entries = [&](const std::function<void(int32_t, int64_t)>& body) {
@@ -344,6 +369,15 @@ void ldlt_left_looking(int32_t size, const std::vector<int64_t>& row_start, cons
       const int32_t i = columns[j][e - 1];
       const int64_t pos = column_positions[j][e - 1];
       double acc = values[pos];
+      if (dense) {
+        const double* row_j = dense_rows.data() + static_cast<size_t>(dense_slot[j]) * size;
+        for (int64_t p = row_start[i]; p < pos; ++p) {
+          const double product = values[p] * row_j[pattern[p]];
+          acc = acc - product;
+        }
+        unscaled[pos] = acc;
+        return;
+      }
       int64_t p = row_start[i];
       int64_t q = start_j;
       while (p < pos && q < end_j) {
@@ -372,6 +406,7 @@ void ldlt_left_looking(int32_t size, const std::vector<int64_t>& row_start, cons
       const int64_t pos = column_positions[j][e - 1];
       values[pos] = unscaled[pos] / unscaled[end_j];
     });
+    if (dense) scatter_rows(true);
   }
 }
 
