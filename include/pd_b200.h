@@ -449,10 +449,11 @@ int pd_inverse_parallel_work(int64_t work);
 /* Entries of L (its nonzeros, diagonal included) from which the numeric LDL^T
    (sparse.py:136-151) and the rows of L^{-1} (sparse.py:159-177) run over all
    host threads level by level of the elimination tree (left-looking columns;
-   rows in 1,024-label chunks) instead of the sequential right-looking loop
-   and the row-by-row walk (default 2,097,152; 0: every factor). Every entry
-   sees the same sequence of rounded operations either way: the factor is
-   bit-identical. Process-wide setting. */
+   rows as dense segments in groups of consecutive rows and 256-label chunks)
+   instead of the sequential right-looking loop and the row-by-row walk
+   (default 32,768; 0: every factor). Every entry sees the same sequence of
+   rounded operations either way: the factor is bit-identical. Process-wide
+   setting. */
 int pd_inverse_parallel_levels(int64_t entries);
 int pd_inverse_build(int32_t size, const int32_t* row_offsets, const int32_t* columns, const double* values,
                      PdInverseFactor** out);

@@ -32,7 +32,7 @@ std::atomic<int64_t> g_parallel_row_work{1 << 16};
 
 // Factors with at least this many entries of L take the numeric LDL^T and the
 // rows of L^{-1} over host threads level by level (bit-identical).
-std::atomic<int64_t> g_parallel_level_entries{int64_t{1} << 21};
+std::atomic<int64_t> g_parallel_level_entries{int64_t{1} << 15};
 
 namespace {
 

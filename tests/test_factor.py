@@ -156,7 +156,7 @@ def test_threaded_ldlt_is_bit_identical_to_reference(name):
         _lib.check(lib.pd_inverse_parallel_levels(0))
         out = _lib.inverse_factor(_lib.dense_to_csr(g[name + "__matrix"]))
     finally:
-        _lib.check(lib.pd_inverse_parallel_levels(1 << 21))
+        _lib.check(lib.pd_inverse_parallel_levels(1 << 15))
     for key in ARRAYS:
         np.testing.assert_array_equal(out[key], g[f"{name}__{key}"], err_msg=key)
 
@@ -188,7 +188,7 @@ def test_threaded_ldlt_matches_the_sequential_loop_and_its_errors():
                 _lib.inverse_factor(_lib.dense_to_csr(indefinite))
             messages.append(str(info.value))
     finally:
-        _lib.check(lib.pd_inverse_parallel_levels(1 << 21))
+        _lib.check(lib.pd_inverse_parallel_levels(1 << 15))
     for key in ARRAYS:
         assert np.array_equal(results[0][key], results[1][key]), key
     assert "positive definite" in messages[0] and messages[0] == messages[1]
