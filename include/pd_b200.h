@@ -455,6 +455,15 @@ int pd_inverse_parallel_work(int64_t work);
    rounded operations either way: the factor is bit-identical. Process-wide
    setting. */
 int pd_inverse_parallel_levels(int64_t entries);
+/* How the device computes the rows of L^{-1} when the factor build runs on
+   the device (pd_set_factor_device, pd_inverse_build_on): 0 (default) rows in
+   256-label chunks, one block per (row, chunk), a block barrier per column k;
+   1 the host's grouped dense segments (groups of up to 32 consecutive rows),
+   one block per (group, chunk) and one thread per label holding the group's
+   entries in registers, no barriers, levels launched back to back. Both are
+   bit-identical to the host walk by construction; mode 1 has not yet run on
+   a GPU. Process-wide setting. */
+int pd_factor_device_rows(int32_t mode);
 int pd_inverse_build(int32_t size, const int32_t* row_offsets, const int32_t* columns, const double* values,
                      PdInverseFactor** out);
 /* pd_inverse_build with the numeric LDL^T (sparse.py:136-151) and the rows of

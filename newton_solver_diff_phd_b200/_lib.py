@@ -161,6 +161,7 @@ SIGNATURES = {
     "pd_batch_set_phase_timers": ([_P, _I32, _P], ctypes.c_int),
     "pd_inverse_parallel_work": ([_I64], ctypes.c_int),
     "pd_inverse_parallel_levels": ([_I64], ctypes.c_int),
+    "pd_factor_device_rows": ([_I32], ctypes.c_int),
     "pd_inverse_build": ([_I32, _P, _P, _P, ctypes.POINTER(_P)], ctypes.c_int),
     "pd_inverse_build_on": ([_I32, _I32, _P, _P, _P, ctypes.POINTER(_P)], ctypes.c_int),
     "pd_set_factor_device": ([_P, _I32], ctypes.c_int),

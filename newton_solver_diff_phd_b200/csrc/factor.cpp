@@ -33,6 +33,7 @@ std::atomic<int64_t> g_parallel_row_work{1 << 16};
 // Factors with at least this many entries of L take the numeric LDL^T and the
 // rows of L^{-1} over host threads level by level (bit-identical).
 std::atomic<int64_t> g_parallel_level_entries{int64_t{1} << 15};
+std::atomic<int32_t> g_device_rows_grouped{0};
 
 namespace {
 
@@ -430,24 +431,22 @@ __attribute__((target_clones("avx2", "default"))) static void subtract_scaled(do
 // that range is almost fully dense, so rows are stored as dense segments and
 // row i's update by row k is a contiguous subtract over row k's range, which
 // lies inside row i's. Rows that share most of their columns form a group
-// (up to kGroupRows consecutive rows): per column chunk of kGroupChunk labels
-// the group applies each outside column k (k below the group's first row, in
-// ascending order) to all its rows that hold it, so row k's chunk is read
-// once for the group, then its own rows in ascending order. Each entry of a
-// row therefore sees its columns k in ascending order, one multiply and one
-// subtract each, and zero multipliers are skipped as in the walk; updates by
-// row k's exact zeros subtract signed zeros, which leave every nonzero value
-// unchanged, and exact zeros are omitted at the end: the rows are
+// (up to kRowGroupRows consecutive rows): per column chunk of kRowGroupChunk
+// labels the group applies each outside column k (k below the group's first
+// row, in ascending order) to all its rows that hold it, so row k's chunk is
+// read once for the group, then its own rows in ascending order. Each entry
+// of a row therefore sees its columns k in ascending order, one multiply and
+// one subtract each, and zero multipliers are skipped as in the walk; updates
+// by row k's exact zeros subtract signed zeros, which leave every nonzero
+// value unchanged, and exact zeros are omitted at the end: the rows are
 // bit-identical to the walk's. Groups are scheduled level by level (a group
-// reads only groups of lower levels) as (group, chunk) tasks. Returns false
-// without computing when the dense segments would hold more than twice the
-// rows' structural entries (an order far from a postorder).
-bool inverse_rows_by_groups(const LowerFactorView& f, InverseRows* out, RowPool& pool) {
-  constexpr int32_t kGroupChunk = 256;
-  constexpr int32_t kGroupRows = 32;
+// reads only groups of lower levels) as (group, chunk) tasks.
+bool plan_row_groups(const LowerFactorView& f, RowGroups* plan) {
   constexpr double kShare = 0.5;  // a row joins when half its outside columns are the group's
   const int32_t n = f.size;
-  std::vector<int32_t> lo(n), parent(n, -1);
+  std::vector<int32_t>& lo = plan->lo;
+  lo.assign(n, 0);
+  std::vector<int32_t> parent(n, -1);
   std::vector<int64_t> subtree(n, 1);
   for (int32_t i = 0; i < n; ++i) {
     int32_t low = i;
@@ -463,13 +462,15 @@ bool inverse_rows_by_groups(const LowerFactorView& f, InverseRows* out, RowPool&
     structural += subtree[k];
     if (parent[k] >= 0) subtree[parent[k]] += subtree[k];
   }
-  std::vector<int64_t> base(static_cast<size_t>(n) + 1, 0);
+  std::vector<int64_t>& base = plan->base;
+  base.assign(static_cast<size_t>(n) + 1, 0);
   for (int32_t i = 0; i < n; ++i) base[i + 1] = base[i] + (i - lo[i] + 1);
   if (base[n] > 2 * structural) return false;
-  std::vector<double> dense(static_cast<size_t>(base[n]));
 
   // Groups of consecutive rows.
-  std::vector<int32_t> group_start(1, 0), group_of(n);
+  std::vector<int32_t>& group_start = plan->group_start;
+  std::vector<int32_t> group_of(n);
+  group_start.assign(1, 0);
   {
     std::vector<int32_t> mark(n, -1);
     int32_t a = 0;
@@ -483,7 +484,7 @@ bool inverse_rows_by_groups(const LowerFactorView& f, InverseRows* out, RowPool&
             shared += mark[k] == a;
           }
         }
-        if (r - a >= kGroupRows || shared < kShare * outside) {
+        if (r - a >= kRowGroupRows || shared < kShare * outside) {
           a = r;
           group_start.push_back(r);
         }
@@ -497,13 +498,17 @@ bool inverse_rows_by_groups(const LowerFactorView& f, InverseRows* out, RowPool&
     group_start.push_back(n);
   }
   const int32_t groups = static_cast<int32_t>(group_start.size()) - 1;
-  // Per group: its outside columns U ascending, multipliers outer[u][r] and
-  // inner[r][kk] (row a + r, column u or a + kk; zero where the row lacks it),
-  // the lowest label of its rows and its level.
-  std::vector<int64_t> u_start(static_cast<size_t>(groups) + 1, 0), outer_start(static_cast<size_t>(groups) + 1, 0),
-      inner_start(static_cast<size_t>(groups) + 1, 0);
-  std::vector<int32_t> u_cols, group_lo(groups), level(groups, 0);
-  std::vector<double> outer, inner;
+  plan->u_start.assign(static_cast<size_t>(groups) + 1, 0);
+  plan->outer_start.assign(static_cast<size_t>(groups) + 1, 0);
+  plan->inner_start.assign(static_cast<size_t>(groups) + 1, 0);
+  plan->group_lo.assign(groups, 0);
+  plan->u_cols.clear();
+  plan->outer.clear();
+  plan->inner.clear();
+  std::vector<int32_t>& u_cols = plan->u_cols;
+  std::vector<double>& outer = plan->outer;
+  std::vector<double>& inner = plan->inner;
+  std::vector<int32_t> level(groups, 0);
   int32_t levels = 0;
   {
     std::vector<int32_t> seen(n, -1);
@@ -522,12 +527,12 @@ bool inverse_rows_by_groups(const LowerFactorView& f, InverseRows* out, RowPool&
         }
       }
       std::sort(u_cols.begin() + static_cast<std::ptrdiff_t>(u0), u_cols.end());
-      group_lo[g] = low;
+      plan->group_lo[g] = low;
       int32_t l = 0;
       for (size_t u = u0; u < u_cols.size(); ++u) l = std::max(l, level[group_of[u_cols[u]]] + 1);
       level[g] = l;
       levels = std::max(levels, l + 1);
-      u_start[g + 1] = static_cast<int64_t>(u_cols.size());
+      plan->u_start[g + 1] = static_cast<int64_t>(u_cols.size());
       const size_t o0 = outer.size(), i0 = inner.size();
       outer.resize(o0 + (u_cols.size() - u0) * rows, 0.0);
       inner.resize(i0 + static_cast<size_t>(rows) * rows, 0.0);
@@ -543,30 +548,76 @@ bool inverse_rows_by_groups(const LowerFactorView& f, InverseRows* out, RowPool&
           }
         }
       }
-      outer_start[g + 1] = static_cast<int64_t>(outer.size());
-      inner_start[g + 1] = static_cast<int64_t>(inner.size());
+      plan->outer_start[g + 1] = static_cast<int64_t>(outer.size());
+      plan->inner_start[g + 1] = static_cast<int64_t>(inner.size());
     }
   }
-  std::vector<int32_t> level_count(static_cast<size_t>(levels) + 1, 0);
-  for (int32_t g = 0; g < groups; ++g) level_count[level[g] + 1] += 1;
-  for (int32_t l = 0; l < levels; ++l) level_count[l + 1] += level_count[l];
-  std::vector<int32_t> by_level(groups);
+  std::vector<int32_t>& level_start = plan->level_start;
+  level_start.assign(static_cast<size_t>(levels) + 1, 0);
+  for (int32_t g = 0; g < groups; ++g) level_start[level[g] + 1] += 1;
+  for (int32_t l = 0; l < levels; ++l) level_start[l + 1] += level_start[l];
+  plan->groups_by_level.assign(groups, 0);
   {
-    std::vector<int32_t> cursor(level_count.begin(), level_count.end() - 1);
-    for (int32_t g = 0; g < groups; ++g) by_level[cursor[level[g]]++] = g;
+    std::vector<int32_t> cursor(level_start.begin(), level_start.end() - 1);
+    for (int32_t g = 0; g < groups; ++g) plan->groups_by_level[cursor[level[g]]++] = g;
   }
+  return true;
+}
 
+void compact_dense_rows(const RowGroups& plan, const double* dense, InverseRows* out) {
+  const int32_t n = static_cast<int32_t>(plan.lo.size());
+  out->start.assign(static_cast<size_t>(n) + 1, 0);
+  const unsigned workers = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  RowPool pool(workers);
+  auto ranges = [&](const std::function<void(int32_t, int32_t)>& body) {
+    pool.run([&](unsigned w) {
+      body(static_cast<int32_t>(static_cast<int64_t>(n) * w / workers),
+           static_cast<int32_t>(static_cast<int64_t>(n) * (w + 1) / workers));
+    });
+  };
+  ranges([&](int32_t r0, int32_t r1) {
+    for (int32_t i = r0; i < r1; ++i) {
+      int64_t kept = 0;
+      for (int64_t q = plan.base[i]; q < plan.base[i + 1]; ++q) kept += dense[q] != 0.0;
+      out->start[i + 1] = kept;
+    }
+  });
+  for (int32_t i = 0; i < n; ++i) out->start[i + 1] += out->start[i];
+  out->columns.resize(static_cast<size_t>(out->start[n]));
+  out->values.resize(static_cast<size_t>(out->start[n]));
+  ranges([&](int32_t r0, int32_t r1) {
+    for (int32_t i = r0; i < r1; ++i) {
+      int64_t at = out->start[i];
+      for (int64_t q = plan.base[i]; q < plan.base[i + 1]; ++q) {
+        if (dense[q] != 0.0) {
+          out->columns[at] = plan.lo[i] + static_cast<int32_t>(q - plan.base[i]);
+          out->values[at] = dense[q];
+          ++at;
+        }
+      }
+    }
+  });
+}
+
+bool inverse_rows_by_groups(const LowerFactorView& f, InverseRows* out, RowPool& pool) {
+  RowGroups plan;
+  if (!plan_row_groups(f, &plan)) return false;
+  const std::vector<int32_t>& lo = plan.lo;
+  const std::vector<int64_t>& base = plan.base;
+  std::vector<double> dense(static_cast<size_t>(base[f.size]));
   struct Item {
     int32_t group, chunk;
   };
   std::vector<Item> items;
-  std::vector<std::vector<double>> tiles(pool.size(), std::vector<double>(static_cast<size_t>(kGroupRows) * kGroupChunk));
+  std::vector<std::vector<double>> tiles(pool.size(),
+                                         std::vector<double>(static_cast<size_t>(kRowGroupRows) * kRowGroupChunk));
   double* d = dense.data();
+  const int32_t levels = static_cast<int32_t>(plan.level_start.size()) - 1;
   for (int32_t l = 0; l < levels; ++l) {
     items.clear();
-    for (int32_t q = level_count[l]; q < level_count[l + 1]; ++q) {
-      const int32_t g = by_level[q];
-      for (int32_t j = group_lo[g] / kGroupChunk; j <= (group_start[g + 1] - 1) / kGroupChunk; ++j)
+    for (int32_t q = plan.level_start[l]; q < plan.level_start[l + 1]; ++q) {
+      const int32_t g = plan.groups_by_level[q];
+      for (int32_t j = plan.group_lo[g] / kRowGroupChunk; j <= (plan.group_start[g + 1] - 1) / kRowGroupChunk; ++j)
         items.push_back(Item{g, j});
     }
     const int64_t count = static_cast<int64_t>(items.size());
@@ -575,26 +626,26 @@ bool inverse_rows_by_groups(const LowerFactorView& f, InverseRows* out, RowPool&
       double* tile = tiles[w].data();
       for (int64_t t = next.fetch_add(1); t < count; t = next.fetch_add(1)) {
         const int32_t g = items[t].group;
-        const int32_t a = group_start[g], rows = group_start[g + 1] - a;
-        const int32_t c0 = items[t].chunk * kGroupChunk, c1 = c0 + kGroupChunk;
-        auto row_of = [&](int32_t r) { return tile + static_cast<size_t>(r) * kGroupChunk; };
+        const int32_t a = plan.group_start[g], rows = plan.group_start[g + 1] - a;
+        const int32_t c0 = items[t].chunk * kRowGroupChunk, c1 = c0 + kRowGroupChunk;
+        auto row_of = [&](int32_t r) { return tile + static_cast<size_t>(r) * kRowGroupChunk; };
         for (int32_t r = 0; r < rows; ++r) {
-          std::fill(row_of(r), row_of(r) + kGroupChunk, 0.0);
+          std::fill(row_of(r), row_of(r) + kRowGroupChunk, 0.0);
           if (a + r >= c0 && a + r < c1) row_of(r)[a + r - c0] = 1.0;
         }
-        const double* multipliers = outer.data() + outer_start[g];
-        for (int64_t u = u_start[g]; u < u_start[g + 1]; ++u) {
-          const int32_t k = u_cols[u];
+        const double* multipliers = plan.outer.data() + plan.outer_start[g];
+        for (int64_t u = plan.u_start[g]; u < plan.u_start[g + 1]; ++u) {
+          const int32_t k = plan.u_cols[u];
           const int32_t from = std::max(lo[k], c0), to = std::min(k + 1, c1);
           if (from >= to) continue;
           const double* source = d + base[k] + (from - lo[k]);
-          const double* column = multipliers + (u - u_start[g]) * rows;
+          const double* column = multipliers + (u - plan.u_start[g]) * rows;
           for (int32_t r = 0; r < rows; ++r) {
             if (column[r] == 0.0) continue;
             subtract_scaled(row_of(r) + (from - c0), source, column[r], to - from);
           }
         }
-        const double* own = inner.data() + inner_start[g];
+        const double* own = plan.inner.data() + plan.inner_start[g];
         for (int32_t kk = 0; kk + 1 < rows; ++kk) {
           const int32_t k = a + kk;
           const int32_t from = std::max(lo[k], c0), to = std::min(k + 1, c1);
@@ -618,38 +669,7 @@ bool inverse_rows_by_groups(const LowerFactorView& f, InverseRows* out, RowPool&
       work(0);
     }
   }
-
-  // Compaction over row ranges: exact zeros omitted, columns ascending.
-  out->start.assign(static_cast<size_t>(n) + 1, 0);
-  const unsigned workers = pool.size();
-  auto ranges = [&](const std::function<void(int32_t, int32_t)>& body) {
-    pool.run([&](unsigned w) {
-      body(static_cast<int32_t>(static_cast<int64_t>(n) * w / workers),
-           static_cast<int32_t>(static_cast<int64_t>(n) * (w + 1) / workers));
-    });
-  };
-  ranges([&](int32_t r0, int32_t r1) {
-    for (int32_t i = r0; i < r1; ++i) {
-      int64_t kept = 0;
-      for (int64_t q = base[i]; q < base[i + 1]; ++q) kept += d[q] != 0.0;
-      out->start[i + 1] = kept;
-    }
-  });
-  for (int32_t i = 0; i < n; ++i) out->start[i + 1] += out->start[i];
-  out->columns.resize(static_cast<size_t>(out->start[n]));
-  out->values.resize(static_cast<size_t>(out->start[n]));
-  ranges([&](int32_t r0, int32_t r1) {
-    for (int32_t i = r0; i < r1; ++i) {
-      int64_t at = out->start[i];
-      for (int64_t q = base[i]; q < base[i + 1]; ++q) {
-        if (d[q] != 0.0) {
-          out->columns[at] = lo[i] + static_cast<int32_t>(q - base[i]);
-          out->values[at] = d[q];
-          ++at;
-        }
-      }
-    }
-  });
+  compact_dense_rows(plan, d, out);
   return true;
 }
 

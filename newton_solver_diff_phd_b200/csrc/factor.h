@@ -88,6 +88,38 @@ struct SymbolicView {
 // then one rounded subtract each). Errors use the host's messages.
 using LdltProvider = std::function<std::string(const SymbolicView&, double* values, double* diagonal)>;
 
+// Rows of L^{-1} as dense segments in groups of consecutive rows (the host's
+// level path and, on request, the device's): row i is stored over the labels
+// [lo[i], i] of its elimination subtree at dense[base[i] + c - lo[i]]; group g
+// holds rows group_start[g] .. group_start[g+1]-1 (at most kRowGroupRows),
+// its outside columns u_cols[u_start[g] .. u_start[g+1]) ascending, the
+// multipliers outer[outer_start[g] + u * rows + r] of row a + r at outside
+// column u and inner[inner_start[g] + r * rows + kk] at the group's own row
+// a + kk (zero where the row lacks the column), and the lowest label of its
+// rows; groups_by_level lists the groups level by level (a group reads only
+// groups of lower levels), level_start indexing it.
+constexpr int32_t kRowGroupChunk = 256;
+constexpr int32_t kRowGroupRows = 32;
+struct RowGroups {
+  std::vector<int32_t> lo;
+  std::vector<int64_t> base;  // [size + 1]
+  std::vector<int32_t> group_start, group_lo;
+  std::vector<int64_t> u_start, outer_start, inner_start;
+  std::vector<int32_t> u_cols;
+  std::vector<double> outer, inner;
+  std::vector<int32_t> level_start, groups_by_level;
+};
+// Plans the groups; false when the dense segments would hold more than twice
+// the rows' structural entries (an order far from a postorder).
+bool plan_row_groups(const LowerFactorView& factor, RowGroups* plan);
+// The rows of L^{-1} from their dense segments: exact zeros omitted, columns
+// ascending (over host threads).
+void compact_dense_rows(const RowGroups& plan, const double* dense, InverseRows* out);
+// Which device computes the rows of L^{-1} when the build runs on the device:
+// 0 the chunked rows (default), 1 the grouped dense segments.
+extern std::atomic<int32_t> g_device_rows_grouped;
+std::string device_inverse_rows_grouped(const LowerFactorView& factor, InverseRows* out);
+std::string device_inverse_rows_chunked(const LowerFactorView& factor, InverseRows* out);
 // The numeric LDL^T on the current CUDA device, column by column within
 // levels of the elimination tree (pd_factor_device.cu). Rows longer than the
 // shared memory staging allows return an error starting with "device LDLT:".

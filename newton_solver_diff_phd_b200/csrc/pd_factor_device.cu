@@ -269,6 +269,73 @@ __global__ void __launch_bounds__(kThreads) ldlt_divide_kernel(const ColumnItem*
   multipliers[pos] = unscaled[pos] / diagonal[j];
 }
 
+// Rows of L^{-1} as dense segments in groups of consecutive rows (the
+// schedule of the host's inverse_rows_by_groups, planned by plan_row_groups):
+// one block per (group, chunk) item of a level, one thread per label c of the
+// chunk, which holds the entries (a + r, c) of the group's rows in registers.
+// The thread applies every outside column k of the group in ascending order
+// (row k's entry at c, read once for all the group's rows), then the group's
+// own rows in ascending order from its registers, skipping zero multipliers:
+// every entry sees the host walk's columns in ascending order, one
+// __dmul_rn then one __dsub_rn each, and no thread reads another's entries,
+// so the block has no barrier. Entries outside a row's labels [lo_i, i] are
+// never read or written.
+template <int kRows>
+__global__ void __launch_bounds__(kRowGroupChunk)
+    inverse_rows_group_kernel(const int2* items, const int32_t* group_start, const int64_t* u_start,
+                              const int32_t* u_cols, const int64_t* outer_start, const double* outer,
+                              const int64_t* inner_start, const double* inner, const int32_t* lo,
+                              const int64_t* base, double* dense) {
+  const int2 item = items[blockIdx.x];
+  const int32_t g = item.x;
+  const int32_t a = group_start[g];
+  const int32_t rows = group_start[g + 1] - a;
+  const int32_t c = item.y * kRowGroupChunk + static_cast<int32_t>(threadIdx.x);
+  double acc[kRows];
+#pragma unroll
+  for (int r = 0; r < kRows; ++r) acc[r] = a + r == c ? 1.0 : 0.0;
+  const double* multipliers = outer + outer_start[g];
+  const int64_t u0 = u_start[g], u1 = u_start[g + 1];
+  for (int64_t u = u0; u < u1; ++u) {
+    const int32_t k = u_cols[u];
+    const int32_t low = lo[k];
+    if (c < low || c > k) continue;
+    const double x = dense[base[k] + (c - low)];
+    const double* column = multipliers + (u - u0) * rows;
+#pragma unroll
+    for (int r = 0; r < kRows; ++r) {
+      if (r < rows) {
+        const double m = column[r];
+        if (m != 0.0) acc[r] = __dsub_rn(acc[r], __dmul_rn(m, x));
+      }
+    }
+  }
+  const double* own = inner + inner_start[g];
+#pragma unroll
+  for (int kk = 0; kk + 1 < kRows; ++kk) {
+    if (kk + 1 < rows) {
+      const int32_t k = a + kk;
+      if (c >= lo[k] && c <= k) {
+        const double x = acc[kk];
+#pragma unroll
+        for (int r = kk + 1; r < kRows; ++r) {
+          if (r < rows) {
+            const double m = own[r * rows + kk];
+            if (m != 0.0) acc[r] = __dsub_rn(acc[r], __dmul_rn(m, x));
+          }
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < kRows; ++r) {
+    if (r < rows) {
+      const int32_t i = a + r;
+      if (c >= lo[i] && c <= i) dense[base[i] + (c - lo[i])] = acc[r];
+    }
+  }
+}
+
 // Device allocation released on scope exit.
 template <typename T>
 struct DeviceArray {
@@ -313,6 +380,11 @@ std::string cuda_error(const char* what, cudaError_t e) {
 }  // namespace
 
 std::string device_inverse_rows(const LowerFactorView& factor, InverseRows* out) {
+  return g_device_rows_grouped.load() != 0 ? device_inverse_rows_grouped(factor, out)
+                                           : device_inverse_rows_chunked(factor, out);
+}
+
+std::string device_inverse_rows_chunked(const LowerFactorView& factor, InverseRows* out) {
   const auto timer = PD_FT_NOW();
   const int32_t n = factor.size;
   out->start.assign(static_cast<size_t>(n) + 1, 0);
@@ -600,6 +672,65 @@ std::string device_ldlt(const SymbolicView& symbolic, double* values, double* di
   }
   PD_FT_REPORT("ldlt", timer, std::string("levels ") + std::to_string(levels) + " items " +
                                   std::to_string(items.size()));
+  return std::string();
+}
+
+
+// The grouped dense rows of L^{-1} on the current device: the host plans the
+// groups (plan_row_groups), every level's items launch back to back on one
+// stream (no host round trip between levels: every row has its place in the
+// dense array from the start), and the host compacts the dense rows. An
+// order whose dense rows would be too large uses the chunked rows instead.
+std::string device_inverse_rows_grouped(const LowerFactorView& factor, InverseRows* out) {
+  RowGroups plan;
+  if (!plan_row_groups(factor, &plan)) return device_inverse_rows_chunked(factor, out);
+  const int32_t n = factor.size;
+  const int32_t levels = static_cast<int32_t>(plan.level_start.size()) - 1;
+  std::vector<int2> items;
+  std::vector<int64_t> level_items(static_cast<size_t>(levels) + 1, 0);
+  for (int32_t l = 0; l < levels; ++l) {
+    for (int32_t q = plan.level_start[l]; q < plan.level_start[l + 1]; ++q) {
+      const int32_t g = plan.groups_by_level[q];
+      for (int32_t j = plan.group_lo[g] / kRowGroupChunk; j <= (plan.group_start[g + 1] - 1) / kRowGroupChunk; ++j)
+        items.push_back(make_int2(g, j));
+    }
+    level_items[l + 1] = static_cast<int64_t>(items.size());
+  }
+  StreamGuard guard;
+  PD_FD_CHECK(cudaStreamCreateWithFlags(&guard.stream, cudaStreamNonBlocking), "stream");
+  cudaStream_t stream = guard.stream;
+  DeviceArray<int2> d_items;
+  DeviceArray<int32_t> d_group_start, d_u_cols, d_lo;
+  DeviceArray<int64_t> d_u_start, d_outer_start, d_inner_start, d_base;
+  DeviceArray<double> d_outer, d_inner, d_dense;
+  PD_FD_CHECK(d_items.upload(items, stream), "upload");
+  PD_FD_CHECK(d_group_start.upload(plan.group_start, stream), "upload");
+  PD_FD_CHECK(d_u_cols.upload(plan.u_cols, stream), "upload");
+  PD_FD_CHECK(d_lo.upload(plan.lo, stream), "upload");
+  PD_FD_CHECK(d_u_start.upload(plan.u_start, stream), "upload");
+  PD_FD_CHECK(d_outer_start.upload(plan.outer_start, stream), "upload");
+  PD_FD_CHECK(d_inner_start.upload(plan.inner_start, stream), "upload");
+  PD_FD_CHECK(d_base.upload(plan.base, stream), "upload");
+  PD_FD_CHECK(d_outer.upload(plan.outer, stream), "upload");
+  PD_FD_CHECK(d_inner.upload(plan.inner, stream), "upload");
+  const size_t slots = static_cast<size_t>(plan.base[n]);
+  PD_FD_CHECK(d_dense.allocate(slots), "allocate dense rows");
+  for (int32_t l = 0; l < levels; ++l) {
+    const int64_t first = level_items[l];
+    const int64_t count = level_items[l + 1] - first;
+    if (count == 0) continue;
+    inverse_rows_group_kernel<kRowGroupRows><<<static_cast<unsigned>(count), kRowGroupChunk, 0, stream>>>(
+        d_items.ptr + first, d_group_start.ptr, d_u_start.ptr, d_u_cols.ptr, d_outer_start.ptr, d_outer.ptr,
+        d_inner_start.ptr, d_inner.ptr, d_lo.ptr, d_base.ptr, d_dense.ptr);
+    PD_FD_CHECK(cudaGetLastError(), "launch");
+  }
+  std::vector<double> dense(slots);
+  if (slots > 0) {
+    PD_FD_CHECK(cudaMemcpyAsync(dense.data(), d_dense.ptr, slots * sizeof(double), cudaMemcpyDeviceToHost, stream),
+                "read back");
+  }
+  PD_FD_CHECK(cudaStreamSynchronize(stream), "rows of L^-1");
+  compact_dense_rows(plan, dense.data(), out);
   return std::string();
 }
 

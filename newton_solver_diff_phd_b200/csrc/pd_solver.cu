@@ -1159,6 +1159,12 @@ int pd_inverse_parallel_levels(int64_t entries) {
   return PD_OK;
 }
 
+int pd_factor_device_rows(int32_t mode) {
+  if (mode != 0 && mode != 1) return fail(PD_ERR_INVALID, "mode must be 0 (chunked rows) or 1 (grouped dense rows)");
+  pdb200::g_device_rows_grouped.store(mode);
+  return PD_OK;
+}
+
 int pd_inverse_build(int32_t size, const int32_t* row_offsets, const int32_t* columns, const double* values,
                      PdInverseFactor** out) {
   return pd_inverse_build_on(-1, size, row_offsets, columns, values, out);

@@ -7,7 +7,8 @@ the rows of L^{-1} as dense segments in groups of consecutive rows. These
 tests restate the three schedules step for step (levels, label ranges, chunk
 bounds recorded per stored row, merge order; group formation, outside
 columns before the group's own rows, zero multipliers skipped, updates by
-exact zeros, compaction) and check that they reproduce the sequential
+exact zeros, compaction; and the device's one-thread-per-label form of the
+grouped schedule) and check that they reproduce the sequential
 right-looking factorisation and row walk of ``oracle/factor_port.py`` bit for
 bit, for chunk widths from one label (every row split everywhere) to wider
 than the matrix. The CUDA kernels themselves are checked against the host
@@ -128,6 +129,57 @@ def grouped_rows(lower, width, group_rows, share):
     return rows
 
 
+def grouped_rows_by_label(lower, width, group_rows, share):
+    """``inverse_rows_group_kernel``'s view of the grouped schedule: one thread per label c of a
+    (group, chunk) item holds the entries (a + r, c) of the group's rows, applies the outside
+    columns k with lo_k <= c <= k in ascending order, then its own rows, and writes the entries
+    inside each row's labels; groups in elimination order, levels replaced by that order."""
+    n = len(lower)
+    _, lo = levels_of(lower)
+    starts, a, mark = [0], 0, {}
+    for r in range(1, n):
+        outside = [k for k in lower[r] if k < a]
+        shared = sum(mark.get(k) == a for k in outside)
+        if r - a >= group_rows or shared < share * len(outside):
+            a = r
+            starts.append(r)
+        for k in lower[r]:
+            if k < a:
+                mark[k] = a
+    starts.append(n)
+    dense = [[None] * (i - lo[i] + 1) for i in range(n)]
+    for a, b in zip(starts[:-1], starts[1:]):
+        rows = b - a
+        union = sorted({k for r in range(a, b) for k in lower[r] if k < a})
+        outer = [[lower[a + r].get(k, 0.0) for r in range(rows)] for k in union]
+        inner = [[lower[a + r].get(a + kk, 0.0) if kk < r else 0.0 for kk in range(rows)] for r in range(rows)]
+        for j in range(min(lo[a:b]) // width, (b - 1) // width + 1):
+            for t in range(width):
+                c = j * width + t
+                acc = [1.0 if a + r == c else 0.0 for r in range(rows)]
+                for u, k in enumerate(union):
+                    if c < lo[k] or c > k:
+                        continue
+                    x = dense[k][c - lo[k]]
+                    for r in range(rows):
+                        if outer[u][r] != 0.0:
+                            acc[r] = acc[r] - outer[u][r] * x
+                for kk in range(rows - 1):
+                    k = a + kk
+                    if lo[k] <= c <= k:
+                        for r in range(kk + 1, rows):
+                            if inner[r][kk] != 0.0:
+                                acc[r] = acc[r] - inner[r][kk] * acc[kk]
+                for r in range(rows):
+                    if lo[a + r] <= c <= a + r:
+                        dense[a + r][c - lo[a + r]] = acc[r]
+    rows_out = []
+    for i in range(n):
+        kept = [(lo[i] + u, value) for u, value in enumerate(dense[i]) if value != 0.0]
+        rows_out.append(([c for c, _ in kept], [value for _, value in kept]))
+    return rows_out
+
+
 def left_looking(csr, permutation, lower):
     """Columns level by level: entry (i, j) = A(i, j) - sum m(i, k) e(j, k) over shared k, ascending."""
     n = len(lower)
@@ -182,5 +234,14 @@ def test_grouped_dense_rows_reproduce_the_row_walk(width, group_rows, share):
     _, _, lower, _ = beam(6, 3, 3)
     walk = row_walk(lower)
     for (cols, vals), (ref_cols, ref_vals) in zip(grouped_rows(lower, width, group_rows, share), walk):
+        assert cols == ref_cols
+        assert np.array_equal(np.asarray(vals), np.asarray(ref_vals))
+
+
+@pytest.mark.parametrize("width, group_rows", [(16, 32), (256, 4)])
+def test_grouped_rows_by_label_reproduce_the_row_walk(width, group_rows):
+    _, _, lower, _ = beam(6, 3, 3)
+    walk = row_walk(lower)
+    for (cols, vals), (ref_cols, ref_vals) in zip(grouped_rows_by_label(lower, width, group_rows, 0.5), walk):
         assert cols == ref_cols
         assert np.array_equal(np.asarray(vals), np.asarray(ref_vals))
