@@ -855,7 +855,6 @@ std::string build_inverse_factor(int32_t size, const int32_t* row_offsets, const
     entries.resize(count);
     for (size_t o = 0; o < count; ++o) entries[o] = values[positions[o]];
     for (size_t o = 0; o < count; ++o) {
-      const int32_t i = neighbors[o];
       const double multiplier = entries[o] / pivot;
       values[positions[o]] = multiplier;
       // Walk row i for columns neighbors[0..o]; all lie after column k.
