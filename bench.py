@@ -1035,7 +1035,7 @@ def run_diffpd(args, device):
     model = builder.finalize(device)
     forces = [("planar_contact", [0.0, 0.0, 1.0, 0.5, 3, 1.0e6, 1.0, 0.1])]
     solver = SolverDiffPD(model, density=1000.0, corotated_stiffness=4.0e4, volume_stiffness=5.0e4,
-                          state_forces=forces, gravity=(0.0, 0.0, -9.81))
+                          state_forces=forces, gravity=(0.0, 0.0, -9.81), recursion=args.diffpd_recursion)
     dt, steps = 1.0e-2, args.diffpd_steps
     states = [model.state(), model.state()]
     solver.step(states[0], states[1], None, None, dt)  # factor build and warm-up
@@ -1068,7 +1068,8 @@ def run_diffpd(args, device):
         cpu_s += time.perf_counter() - start
         errors.append(float(np.abs(x - x_ref).max()))
         oracle_iterations.append(int(count))
-    return {"workload": "tet4_block_32x8x8_diffpd_lbfgs", "steps": steps, "ms_per_step": float(np.mean(ms)),
+    return {"workload": "tet4_block_32x8x8_diffpd_lbfgs", "recursion": args.diffpd_recursion, "steps": steps,
+            "ms_per_step": float(np.mean(ms)),
             "steps_per_s": 1000.0 * steps / float(np.sum(ms)),
             "us_per_iteration": 1000.0 * float(np.sum(ms)) / max(sum(iterations), 1), "iterations": iterations,
             "status": int(status), "first_steps_vs_oracle": {"max_abs_position_err_m": max(errors),
@@ -1362,6 +1363,10 @@ def main():
     parser.add_argument("--twist-steps", type=int, default=100, help="steps of the twist-release leg")
     parser.add_argument("--no-diffpd", action="store_true", help="skip the SolverDiffPD (L-BFGS) leg")
     parser.add_argument("--diffpd-steps", type=int, default=20, help="steps of the SolverDiffPD leg")
+    parser.add_argument("--diffpd-recursion", choices=("two_loop", "gram"), default="two_loop",
+                        help="L-BFGS recursion of the SolverDiffPD leg (the reference's two loops or the Gram form)")
+    parser.add_argument("--factor-device-rows", type=int, choices=(0, 1), default=0,
+                        help="device rows of L^-1 in the factor-build legs: 0 chunked, 1 grouped dense segments")
     parser.add_argument("--profile-factor", action="store_true",
                         help="run only the factor-build leg (4,961 rows, host then device; for profilers)")
     parser.add_argument("--profile-diffpd", action="store_true",
@@ -1374,6 +1379,10 @@ def main():
                         help="comma-separated family instances: run only a small batched rollout (for profilers)")
     parser.add_argument("--profile-steps", type=int, default=2, help="steps of the --profile-batch rollout")
     args = parser.parse_args()
+    if args.factor_device_rows:
+        from newton_solver_diff_phd_b200 import _lib
+
+        _lib.check(_lib.library().pd_factor_device_rows(args.factor_device_rows))
     if args.profile_batch:
         run_batch_profile(args)
         return
