@@ -367,18 +367,43 @@ void ldlt_left_looking(int32_t size, const std::vector<int64_t>& row_start, cons
         unscaled[end_j] = acc;
         return;
       }
+      if (dense) {
+        // Entries 1 + 4 m .. 4 + 4 m of the column are computed together by
+        // the task of the first: four independent chains side by side, each
+        // in its own order.
+        if ((e - 1) % 4 != 0) return;
+        const double* row_j = dense_rows.data() + static_cast<size_t>(dense_slot[j]) * size;
+        const int64_t count = std::min<int64_t>(4, static_cast<int64_t>(columns[j].size()) - (e - 1));
+        int64_t p[4] = {0, 0, 0, 0}, end[4] = {0, 0, 0, 0};
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        int64_t common = std::numeric_limits<int64_t>::max();
+        for (int64_t t = 0; t < count; ++t) {
+          end[t] = column_positions[j][e - 1 + t];
+          p[t] = row_start[columns[j][e - 1 + t]];
+          acc[t] = values[end[t]];
+          common = std::min(common, end[t] - p[t]);
+        }
+        if (count == 4) {
+          for (int64_t q = 0; q < common; ++q) {
+            for (int t = 0; t < 4; ++t) {
+              const double product = values[p[t] + q] * row_j[pattern[p[t] + q]];
+              acc[t] = acc[t] - product;
+            }
+          }
+          for (int t = 0; t < 4; ++t) p[t] += common;
+        }
+        for (int64_t t = 0; t < count; ++t) {
+          for (int64_t q = p[t]; q < end[t]; ++q) {
+            const double product = values[q] * row_j[pattern[q]];
+            acc[t] = acc[t] - product;
+          }
+          unscaled[end[t]] = acc[t];
+        }
+        return;
+      }
       const int32_t i = columns[j][e - 1];
       const int64_t pos = column_positions[j][e - 1];
       double acc = values[pos];
-      if (dense) {
-        const double* row_j = dense_rows.data() + static_cast<size_t>(dense_slot[j]) * size;
-        for (int64_t p = row_start[i]; p < pos; ++p) {
-          const double product = values[p] * row_j[pattern[p]];
-          acc = acc - product;
-        }
-        unscaled[pos] = acc;
-        return;
-      }
       int64_t p = row_start[i];
       int64_t q = start_j;
       while (p < pos && q < end_j) {
