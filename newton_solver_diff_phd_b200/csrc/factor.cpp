@@ -310,6 +310,9 @@ void ldlt_left_looking(int32_t size, const std::vector<int64_t>& row_start, cons
   // k < j that row j lacks read a zero, and subtracting a signed zero leaves
   // every nonzero value unchanged (an entry that is exactly zero may change
   // the sign of its zero; zero multipliers are skipped by the rows of L^{-1}).
+  // Such a column k may sit at this level or above, where row i still holds
+  // A(i, k): a finite value times zero (`values` is written only by the
+  // division pass that follows each level's entry pass).
   // The dense arrays take at most 2^24 doubles.
   const int32_t kDenseColumns =
       static_cast<int32_t>(std::min<int64_t>(64, std::max<int64_t>(1, (int64_t{1} << 24) / std::max(size, 1))));

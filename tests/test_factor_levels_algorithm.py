@@ -180,8 +180,11 @@ def grouped_rows_by_label(lower, width, group_rows, share):
     return rows_out
 
 
-def left_looking(csr, permutation, lower):
-    """Columns level by level: entry (i, j) = A(i, j) - sum m(i, k) e(j, k) over shared k, ascending."""
+def left_looking(csr, permutation, lower, dense=False):
+    """Columns level by level: entry (i, j) = A(i, j) - sum m(i, k) e(j, k) over shared k, ascending.
+    With ``dense`` (the host's top levels) the sum runs over every column k < j of row i, reading
+    e(j, k) = 0 where row j lacks k; such a column k may not be factored yet, and row i then still
+    holds A(i, k) there, a finite value times zero."""
     n = len(lower)
     permuted = sp.csr_matrix(csr[permutation][:, permutation])
     initial = {(i, int(k)): permuted[i, int(k)] for i in range(n) for k in list(lower[i]) + [i]}
@@ -201,9 +204,9 @@ def left_looking(csr, permutation, lower):
             pivot[j] = acc
             for i in rows_of[j]:
                 acc = initial[(i, j)]
-                shared = [k for k in pattern[i] if k < j and k in lower[j]]
+                shared = [k for k in pattern[i] if k < j and (dense or k in lower[j])]
                 for k in shared:  # ascending: the merge of two sorted patterns
-                    acc = acc - multiplier[(i, k)] * unscaled[(j, k)]
+                    acc = acc - multiplier.get((i, k), initial[(i, k)]) * unscaled.get((j, k), 0.0)
                 unscaled[(i, j)] = acc
         for j in columns:
             for i in rows_of[j]:
@@ -220,9 +223,10 @@ def test_chunked_rows_reproduce_the_row_walk(width):
         assert np.array_equal(np.asarray(vals), np.asarray(ref_vals))
 
 
-def test_left_looking_columns_reproduce_the_right_looking_factor():
+@pytest.mark.parametrize("dense", [False, True])
+def test_left_looking_columns_reproduce_the_right_looking_factor(dense):
     csr, permutation, lower, diagonal = beam(8, 3, 3)
-    multiplier, pivot = left_looking(csr, permutation, lower)
+    multiplier, pivot = left_looking(csr, permutation, lower, dense)
     assert np.array_equal(np.asarray(pivot), diagonal)
     for i, row in enumerate(lower):
         for k, value in row.items():
