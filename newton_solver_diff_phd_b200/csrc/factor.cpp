@@ -453,6 +453,25 @@ __attribute__((target_clones("avx2", "default"))) static void subtract_scaled(do
   }
 }
 
+// dst[u] = (((dst[u] - m0 x0[u]) - m1 x1[u]) - m2 x2[u]) - m3 x3[u]: four
+// updates of each entry in order, every product and difference rounded.
+__attribute__((target_clones("avx2", "default"))) static void subtract_scaled4(
+    double* __restrict dst, const double* __restrict x0, const double* __restrict x1, const double* __restrict x2,
+    const double* __restrict x3, const double* m, int32_t count) {
+  const double m0 = m[0], m1 = m[1], m2 = m[2], m3 = m[3];
+  for (int32_t u = 0; u < count; ++u) {
+    double value = dst[u];
+    const double p0 = m0 * x0[u];
+    value = value - p0;
+    const double p1 = m1 * x1[u];
+    value = value - p1;
+    const double p2 = m2 * x2[u];
+    value = value - p2;
+    const double p3 = m3 * x3[u];
+    dst[u] = value - p3;
+  }
+}
+
 // Rows of L^{-1} over host threads in groups of consecutive rows. Row i of
 // L^{-1} is nonzero only on the labels [lo_i, i] of its elimination subtree
 // (lo_i = min(i, lo_k over its columns k)); with the nested-dissection order
@@ -662,15 +681,53 @@ bool inverse_rows_by_groups(const LowerFactorView& f, InverseRows* out, RowPool&
           if (a + r >= c0 && a + r < c1) row_of(r)[a + r - c0] = 1.0;
         }
         const double* multipliers = plan.outer.data() + plan.outer_start[g];
-        for (int64_t u = plan.u_start[g]; u < plan.u_start[g + 1]; ++u) {
-          const int32_t k = plan.u_cols[u];
-          const int32_t from = std::max(lo[k], c0), to = std::min(k + 1, c1);
-          if (from >= to) continue;
-          const double* source = d + base[k] + (from - lo[k]);
-          const double* column = multipliers + (u - plan.u_start[g]) * rows;
+        // Outside columns meeting the chunk, four at a time: on the labels all
+        // four cover, one pass per row applies them in ascending order (a zero
+        // multiplier subtracts a signed zero there); elsewhere each column
+        // applies alone, in ascending order.
+        int64_t u = plan.u_start[g];
+        const int64_t u_end = plan.u_start[g + 1];
+        while (u < u_end) {
+          int64_t picked[4];
+          int32_t from[4], to[4];
+          int found = 0;
+          for (; u < u_end && found < 4; ++u) {
+            const int32_t k = plan.u_cols[u];
+            from[found] = std::max(lo[k], c0);
+            to[found] = std::min(k + 1, c1);
+            if (from[found] < to[found]) picked[found++] = u;
+          }
+          const double* source[4];
+          const double* column[4];
+          for (int t = 0; t < found; ++t) {
+            const int32_t k = plan.u_cols[picked[t]];
+            source[t] = d + base[k] + (from[t] - lo[k]);
+            column[t] = multipliers + (picked[t] - plan.u_start[g]) * rows;
+          }
+          const int32_t common_from = found == 4 ? std::max(std::max(from[0], from[1]), std::max(from[2], from[3])) : 0;
+          const int32_t common_to = found == 4 ? std::min(std::min(to[0], to[1]), std::min(to[2], to[3])) : 0;
+          const bool blocked = found == 4 && common_from < common_to;
           for (int32_t r = 0; r < rows; ++r) {
-            if (column[r] == 0.0) continue;
-            subtract_scaled(row_of(r) + (from - c0), source, column[r], to - from);
+            double* row = row_of(r);
+            if (!blocked) {
+              for (int t = 0; t < found; ++t) {
+                if (column[t][r] == 0.0) continue;
+                subtract_scaled(row + (from[t] - c0), source[t], column[t][r], to[t] - from[t]);
+              }
+              continue;
+            }
+            const double m[4] = {column[0][r], column[1][r], column[2][r], column[3][r]};
+            if (m[0] == 0.0 && m[1] == 0.0 && m[2] == 0.0 && m[3] == 0.0) continue;
+            for (int t = 0; t < 4; ++t) {
+              if (m[t] == 0.0) continue;
+              if (from[t] < common_from)
+                subtract_scaled(row + (from[t] - c0), source[t], m[t], common_from - from[t]);
+              if (common_to < to[t])
+                subtract_scaled(row + (common_to - c0), source[t] + (common_to - from[t]), m[t], to[t] - common_to);
+            }
+            const double* x[4];
+            for (int t = 0; t < 4; ++t) x[t] = source[t] + (common_from - from[t]);
+            subtract_scaled4(row + (common_from - c0), x[0], x[1], x[2], x[3], m, common_to - common_from);
           }
         }
         const double* own = plan.inner.data() + plan.inner_start[g];
