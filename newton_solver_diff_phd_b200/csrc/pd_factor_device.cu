@@ -19,6 +19,8 @@
 // (__dmul_rn / __dsub_rn: no contraction into fused multiply-adds). The
 // nonzero entries are compacted in ascending label order into a scratch slot,
 // then copied into the row pool at offsets the host assigns from the counts.
+// With pd_factor_device_rows(1) the rows follow the host's grouped dense
+// schedule instead (inverse_rows_group_kernel, at the end of this file).
 #include <cuda_runtime.h>
 
 #include <algorithm>
