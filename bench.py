@@ -1368,7 +1368,8 @@ def main():
     parser.add_argument("--factor-device-rows", type=int, choices=(0, 1), default=0,
                         help="device rows of L^-1 in the factor-build legs: 0 chunked, 1 grouped dense segments")
     parser.add_argument("--profile-factor", action="store_true",
-                        help="run only the factor-build leg (4,961 rows, host then device; for profilers)")
+                        help="run only the factor-build leg (4,961 rows, or the twist matrix with --factor-twist; "
+                             "host then device; for profilers)")
     parser.add_argument("--profile-diffpd", action="store_true",
                         help="run only the SolverDiffPD leg (for profilers; --diffpd-steps sets its length)")
     parser.add_argument("--factor-twist", action="store_true",
@@ -1394,7 +1395,7 @@ def main():
     if args.profile_factor:
         import torch
 
-        print(json.dumps(run_factor_build(torch.device("cuda", 0))))
+        print(json.dumps(run_factor_build(torch.device("cuda", 0), twist=args.factor_twist)))
         return
     if args.impl == "reference":
         run_reference(args)
