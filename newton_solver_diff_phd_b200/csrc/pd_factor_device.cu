@@ -684,6 +684,12 @@ std::string device_ldlt(const SymbolicView& symbolic, double* values, double* di
 // dense array from the start), and the host compacts the dense rows. An
 // order whose dense rows would be too large uses the chunked rows instead.
 std::string device_inverse_rows_grouped(const LowerFactorView& factor, InverseRows* out) {
+  if (factor.size == 0) {
+    out->start.assign(1, 0);
+    out->columns.clear();
+    out->values.clear();
+    return std::string();
+  }
   RowGroups plan;
   if (!plan_row_groups(factor, &plan)) return device_inverse_rows_chunked(factor, out);
   const int32_t n = factor.size;
