@@ -491,6 +491,16 @@ __attribute__((target_clones("avx2", "default"))) static void subtract_scaled4(
 bool plan_row_groups(const LowerFactorView& f, RowGroups* plan) {
   constexpr double kShare = 0.5;  // a row joins when half its outside columns are the group's
   const int32_t n = f.size;
+  if (n == 0) {
+    *plan = RowGroups();
+    plan->base.assign(1, 0);
+    plan->group_start.assign(1, 0);
+    plan->u_start.assign(1, 0);
+    plan->outer_start.assign(1, 0);
+    plan->inner_start.assign(1, 0);
+    plan->level_start.assign(1, 0);
+    return true;
+  }
   std::vector<int32_t>& lo = plan->lo;
   lo.assign(n, 0);
   std::vector<int32_t> parent(n, -1);
