@@ -192,3 +192,18 @@ def test_threaded_ldlt_matches_the_sequential_loop_and_its_errors():
     for key in ARRAYS:
         assert np.array_equal(results[0][key], results[1][key]), key
     assert "positive definite" in messages[0] and messages[0] == messages[1]
+
+
+def test_level_path_handles_empty_and_tiny_matrices():
+    """The level path forced on 0-, 1- and 2-row matrices gives the sequential loops' arrays."""
+    lib = _lib.library()
+    matrices = [np.zeros((0, 0)), np.eye(1) * 2.0, np.array([[4.0, 1.0], [1.0, 3.0]])]
+    sequential = [_lib.inverse_factor(_lib.dense_to_csr(m)) for m in matrices]
+    try:
+        _lib.check(lib.pd_inverse_parallel_levels(0))
+        levels = [_lib.inverse_factor(_lib.dense_to_csr(m)) for m in matrices]
+    finally:
+        _lib.check(lib.pd_inverse_parallel_levels(1 << 15))
+    for a, b in zip(sequential, levels):
+        for key in ARRAYS:
+            assert np.array_equal(a[key], b[key]), key
